@@ -1,0 +1,180 @@
+"""ctypes binding of the C ABI in ``include/cffc_e2d.h``.
+
+This is the reference-side binding a Python caller of the library uses: the
+descriptor structs, the loader for ``libcffc_e2d.so`` (built in-tree next to
+this file) and a thin handle class whose methods are the C entry points.
+There is no fallback: if the shared library is missing or a CUDA device is
+unavailable the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .cases import BlockSet, Scheme
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcffc_e2d.so")
+
+E2D_ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory",
+              -4: "NaN/Inf in residual", -5: "GMRES breakdown"}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+class BlocksDesc(C.Structure):
+    _fields_ = [("nblk", C.c_int32), ("nci", C.c_int32), ("ncj", C.c_int32), ("ng", C.c_int32),
+                ("neighbour", _ip), ("bc_w", _ip), ("bc_e", _ip), ("bc_s", _ip), ("bc_n", _ip),
+                ("node_x", _dp), ("node_y", _dp),
+                ("wo_w", _dp), ("wo_e", _dp), ("wo_s", _dp), ("wo_n", _dp)]
+
+
+class SchemeDesc(C.Structure):
+    _fields_ = [("limiter", C.c_int32), ("flux", C.c_int32), ("n_stage", C.c_int32),
+                ("local_dt", C.c_int32), ("precision", C.c_int32), ("reserved", C.c_int32 * 3),
+                ("cfl", C.c_double), ("gamma", C.c_double)]
+
+
+def ptr(a: np.ndarray | None, kind=_dp):
+    if a is None:
+        return C.cast(None, kind)
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(kind)
+
+
+def make_desc(bs: BlockSet):
+    """Returns (BlocksDesc, keep-alive list)."""
+    bs.contiguous()
+    keep = [bs.neighbour, bs.bc_w, bs.bc_e, bs.bc_s, bs.bc_n, bs.node_x, bs.node_y,
+            bs.wo_w, bs.wo_e, bs.wo_s, bs.wo_n]
+    d = BlocksDesc(bs.nblk, bs.nci, bs.ncj, bs.ng,
+                   ptr(bs.neighbour, _ip), ptr(bs.bc_w, _ip), ptr(bs.bc_e, _ip),
+                   ptr(bs.bc_s, _ip), ptr(bs.bc_n, _ip), ptr(bs.node_x), ptr(bs.node_y),
+                   ptr(bs.wo_w), ptr(bs.wo_e), ptr(bs.wo_s), ptr(bs.wo_n))
+    return d, keep
+
+
+def make_scheme(sc: Scheme) -> SchemeDesc:
+    s = SchemeDesc()
+    s.limiter, s.flux, s.n_stage, s.local_dt, s.precision = (
+        sc.limiter, sc.flux, sc.n_stage, sc.local_dt, sc.precision)
+    s.cfl, s.gamma = sc.cfl, sc.gamma
+    return s
+
+
+def declare(lib, prefix: str) -> None:
+    """Argument/return types of the handle API under `prefix` (e2d_ or e2d_oracle_)."""
+    vp = C.c_void_p
+    sig = {
+        "set_state": [vp, _dp], "get_state": [vp, _dp, _dp], "fill_ghosts": [vp],
+        "residual": [vp, _dp], "get_reconstruction": [vp, _dp, _dp, _dp],
+        "rk_steps": [vp, C.c_int, _dp],
+    }
+    for name, args in sig.items():
+        f = getattr(lib, prefix + name)
+        f.argtypes = args
+        f.restype = C.c_int
+    getattr(lib, prefix + "destroy").argtypes = [vp]
+    getattr(lib, prefix + "destroy").restype = None
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libcffc_e2d.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build it with __graft_entry__.build()")
+        lib = C.CDLL(path)
+        declare(lib, "e2d_")
+        lib.e2d_create.argtypes = [C.POINTER(BlocksDesc), C.POINTER(SchemeDesc), C.c_int,
+                                   C.POINTER(C.c_int)]
+        lib.e2d_create.restype = C.c_void_p
+        for name in ("norms",):
+            getattr(lib, "e2d_" + name).argtypes = [C.c_void_p, _dp]
+            getattr(lib, "e2d_" + name).restype = C.c_int
+        lib.e2d_status.argtypes = [C.c_void_p]
+        lib.e2d_status.restype = C.c_int
+        lib.e2d_device_state.argtypes = [C.c_void_p, C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp)]
+        lib.e2d_device_state.restype = C.c_int
+        _lib = lib
+    return _lib
+
+
+class Handle:
+    """A block set resident on the GPU (one e2d_handle)."""
+
+    prefix = "e2d_"
+
+    def __init__(self, bs: BlockSet, device: int = 0, lib=None):
+        self.lib = lib or load_library()
+        self.bs = bs
+        self._desc, self._keep = make_desc(bs)
+        self._scheme = make_scheme(bs.scheme)
+        self.h = self._create(device)
+
+    def _create(self, device):
+        err = C.c_int(0)
+        h = self.lib.e2d_create(C.byref(self._desc), C.byref(self._scheme), device, C.byref(err))
+        if not h:
+            raise RuntimeError(f"e2d_create failed: {E2D_ERRORS.get(err.value, err.value)}")
+        return h
+
+    def _call(self, name, *args):
+        rc = getattr(self.lib, self.prefix + name)(self.h, *args)
+        if rc < 0:
+            raise RuntimeError(f"{self.prefix}{name} failed: {E2D_ERRORS.get(rc, rc)}")
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            getattr(self.lib, self.prefix + "destroy")(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- entry points -----------------------------------------------------
+    def set_state(self, W: np.ndarray | None = None) -> None:
+        W = np.ascontiguousarray(self.bs.W if W is None else W, dtype=np.float64)
+        self._call("set_state", ptr(W))
+
+    def get_state(self):
+        W = np.empty(self.bs.cell_shape())
+        U = np.empty(self.bs.cell_shape())
+        self._call("get_state", ptr(W), ptr(U))
+        return W, U
+
+    def fill_ghosts(self) -> None:
+        self._call("fill_ghosts")
+
+    def residual(self) -> np.ndarray:
+        out = np.empty(self.bs.cell_shape())
+        self._call("residual", ptr(out))
+        return out
+
+    def reconstruction(self):
+        a, b, c = (np.empty(self.bs.cell_shape()) for _ in range(3))
+        self._call("get_reconstruction", ptr(a), ptr(b), ptr(c))
+        return a, b, c
+
+    def rk_steps(self, n: int, history: bool = True):
+        hist = np.zeros((n, 4)) if history else None
+        rc = self._call("rk_steps", n, ptr(hist))
+        return rc, hist
+
+    def norms(self):
+        out = np.zeros(3)
+        self._call("norms", ptr(out))
+        return out
+
+    def status(self) -> int:
+        return self.lib.e2d_status(self.h)

@@ -1,0 +1,158 @@
+/*
+ * cffc_e2d.h — C ABI of the B200 Euler2D finite-volume library
+ * (libcffc_e2d.so, built from cffc_b200/csrc).
+ *
+ * This is the boundary a caller of the CFFC reference's Euler2D path binds
+ * (cgo / ctypes / JNI / a C++ host layer): plain pointers and sizes, no
+ * framework types.  Each entry point names the reference interface it
+ * replaces (paths relative to the CFFC source tree).
+ *
+ * Data layout (host arrays passed in or out, and the device arrays behind a
+ * handle): one record per block, SoA per variable, rows of i:
+ *     cell arrays  [nblk][4][NCj][NCi]   NCi = nci + 2*ng, NCj = ncj + 2*ng
+ *     node arrays  [nblk][NNj][NNi]      NNi = NCi + 1,   NNj = NCj + 1
+ * Cell (i, j) of a block is the reference's SolnBlk.W[i][j] with the same
+ * index origin (ghost cells at i < ICl = ng and i > ICu = ng + nci - 1), and
+ * node (i, j) is Grid.Node[i][j].  Primitive variables are (rho, u, v, p),
+ * conserved (rho, rho*u, rho*v, E).  All state is FP64 (the reference is
+ * FP64); the FP32 reconstruction/flux variant is selected per handle.
+ *
+ * Conventions mirror the reference's error_flag: 0 = success; a positive
+ * return is a reference-style failure (e.g. 1 + the linear index of the first
+ * cell whose density or energy went non-positive, where
+ * Update_Solution_Multistage_Explicit returns the cell's i index); negative
+ * returns are library errors (E2D_ERR_*).  One CUDA stream per handle; a
+ * handle is not thread-safe.  The library owns device memory; host buffers
+ * belong to the caller.
+ */
+#ifndef CFFC_E2D_H
+#define CFFC_E2D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Boundary-condition codes: the reference's values (src_2D/CFD/CFD.h:270-351). */
+#define E2D_BC_NONE 0
+#define E2D_BC_CONSTANT_EXTRAPOLATION 4001
+#define E2D_BC_PERIODIC 6000
+#define E2D_BC_REFLECTION 7001
+#define E2D_BC_CHARACTERISTIC 8001
+#define E2D_BC_FIXED 11000
+
+/* Limiter codes (src_2D/CFD/CFD.h:750-762). */
+#define E2D_LIMITER_ONE (-1)
+#define E2D_LIMITER_ZERO 0
+#define E2D_LIMITER_BARTH_JESPERSEN 8
+#define E2D_LIMITER_VENKATAKRISHNAN 9
+
+/* Flux function codes (src_2D/CFD/CFD.h:769). */
+#define E2D_FLUX_ROE 2
+#define E2D_FLUX_HLLE 4
+
+/* Precision of reconstruction and flux evaluation. */
+#define E2D_PREC_FP64 0
+#define E2D_PREC_FP32 1 /* FP32 reconstruction + flux, FP64 state/accumulation */
+
+/* Library error codes (negative returns). */
+#define E2D_ERR_ARG (-1)      /* invalid argument or unsupported option     */
+#define E2D_ERR_CUDA (-2)     /* a CUDA call failed                          */
+#define E2D_ERR_NOMEM (-3)    /* device allocation failed                    */
+#define E2D_ERR_NAN (-4)      /* NaN/Inf detected in a residual norm         */
+#define E2D_ERR_GMRES (-5)    /* GMRES breakdown                             */
+
+/* Block-set description: geometry, topology and boundary data of all blocks.
+ * Mirrors what Euler2D_Quad_Block / Grid2D_Quad_Block_HO hold for the path
+ * (src_2D/Euler2D/Euler2DQuad.h:140-599, src_2D/Grid/HO_Grid2DQuad.h:277-305):
+ * nodes including ghost nodes, the per-edge BC type arrays BCtypeW/E/S/N and
+ * reference states WoW/E/S/N.  neighbour[b*8 + k] gives the same-resolution
+ * neighbour across edge/corner k = W, E, S, N, SW, SE, NW, NE (-1: none);
+ * it is the block connectivity the reference keeps in its quadtree
+ * (src_2D/AMR/QuadTree.cc:363). */
+typedef struct e2d_blocks_desc {
+  int32_t nblk, nci, ncj, ng; /* ng must be 2 (Euler2DQuad.h:655 asserts > 1) */
+  const int32_t *neighbour;   /* [nblk][8]                                     */
+  const int32_t *bc_w, *bc_e; /* [nblk][NCj]                                   */
+  const int32_t *bc_s, *bc_n; /* [nblk][NCi]                                   */
+  const double *node_x;       /* [nblk][NNj][NNi]                              */
+  const double *node_y;       /* [nblk][NNj][NNi]                              */
+  const double *wo_w, *wo_e;  /* [nblk][4][NCj] primitive reference states     */
+  const double *wo_s, *wo_n;  /* [nblk][4][NCi]                                */
+} e2d_blocks_desc;
+
+/* Numerical scheme: the subset of Euler2D_Input_Parameters the path reads
+ * (src_2D/Euler2D/Euler2DInput.h:41-120). */
+typedef struct e2d_scheme {
+  int32_t limiter;   /* i_Limiter                                         */
+  int32_t flux;      /* i_Flux_Function (Roe)                             */
+  int32_t n_stage;   /* N_Stage of TIME_STEPPING_EXPLICIT_RUNGE_KUTTA: 1, 2 */
+  int32_t local_dt;  /* Local_Time_Stepping: 0 global, 1 scalar local     */
+  int32_t precision; /* E2D_PREC_*                                        */
+  int32_t reserved[3];
+  double cfl;        /* CFL_Number                                        */
+  double gamma;      /* specific-heat ratio g (GAMMA_AIR = 1.4)           */
+} e2d_scheme;
+
+typedef struct e2d_handle e2d_handle;
+
+/* Allocates device state for the block set and uploads geometry; computes
+ * cell centroids/areas as Grid2D_Quad_Block_HO::Update_Cells does
+ * (src_2D/Grid/HO_Grid2DQuad.cc:9832, Math.h:311 quadCentroid).  Replaces
+ * Euler2D_Quad_Block::allocate + grid set-up (Euler2DQuad.h:655).
+ * Returns NULL on failure with *err set. */
+e2d_handle *e2d_create(const e2d_blocks_desc *desc, const e2d_scheme *scheme,
+                       int device, int *err);
+
+/* Releases the handle (Euler2D_Quad_Block::deallocate, Euler2DQuad.h:~700). */
+void e2d_destroy(e2d_handle *h);
+
+/* Uploads the primitive state W of every cell [nblk][4][NCj][NCi] (host
+ * memory) and sets U = U(W); ghost values are kept until the next ghost fill.
+ * Replaces the ICs / Uo assignment loops (Euler2DQuadSingleBlock.cc:1689). */
+int e2d_set_state(e2d_handle *h, const double *W);
+
+/* Downloads W and/or U (either may be NULL). */
+int e2d_get_state(e2d_handle *h, double *W, double *U);
+
+/* Ghost exchange between blocks followed by the BCs of every block:
+ * Send_All_Messages (src_2D/AMR/AdaptiveBlock2D_MessagePassing.h:7883) then
+ * BCs (src_2D/Euler2D/Euler2DQuadSingleBlock.cc:2354). */
+int e2d_fill_ghosts(e2d_handle *h);
+
+/* dUdt_Residual_Evaluation for all blocks (Euler2DQuadSingleBlock.cc:5095 ->
+ * Euler2DQuad.cc:814): ghost fill, least-squares reconstruction with the
+ * limiter, flux per face, flux divergence into dUdt.  dUdt (host, may be
+ * NULL) receives [nblk][4][NCj][NCi] with zero ghost entries. */
+int e2d_residual(e2d_handle *h, double *dUdt);
+
+/* Gradients and limiter values of the last reconstruction (SolnBlk.dWdx,
+ * dWdy, phi), each [nblk][4][NCj][NCi]; any may be NULL. */
+int e2d_get_reconstruction(e2d_handle *h, double *dWdx, double *dWdy, double *phi);
+
+/* n_steps explicit multistage time steps, each in the order of the
+ * reference's explicit loop (src_2D/Euler2D/Euler2DQuadSolvers.cc:657-898):
+ * CFL + global minimum, Set_Global_TimeStep (global dt), residual norms,
+ * then per stage ghost fill, dUdt_Multistage_Explicit (Euler2DQuad.cc:1235)
+ * and Update_Solution_Multistage_Explicit (Euler2DQuadSingleBlock.cc:5300).
+ * hist (host, may be NULL) receives [n_steps][4] = dt_min, L1, L2, Max of
+ * the density residual as the loop computes them before each step. */
+int e2d_rk_steps(e2d_handle *h, int n_steps, double *hist);
+
+/* L1, L2 and max norms of the density residual dUdt[...][0][1] over all
+ * interior cells (Euler2DQuadMultiBlock.cc:1017-1190). */
+int e2d_norms(e2d_handle *h, double out[3]);
+
+/* Device status word: 0 or the first error a kernel recorded. */
+int e2d_status(e2d_handle *h);
+
+/* Device pointers of the resident state (for callers that keep data in HBM):
+ * W, U, dUdt as [nblk][4][NCj][NCi] doubles. */
+int e2d_device_state(e2d_handle *h, double **W, double **U, double **dUdt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFFC_E2D_H */
