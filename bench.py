@@ -1,0 +1,314 @@
+"""Benchmark of the Euler2D explicit path on B200.
+
+Workload (one bench "step"): the curvilinear Mach-2 case — 256 blocks of
+64x64 cells (1,048,576 cells, [0,4]x[0,1], seeded sinusoidal node
+displacement, 5% seeded density perturbation, periodic) advanced by 500
+explicit RK2 time steps (Roe flux, least-squares reconstruction,
+Venkatakrishnan limiter, CFL 0.5, global time step), FP64.
+Metric: Mcell-updates/s (interior cells x time steps / second).
+
+  value     device time (CUDA events) with the state resident in HBM
+  e2e       the same through the C ABI from pinned host memory: upload W,
+            500 steps, download U, every bench step
+  roofline  the fused stage kernel: algorithmic bytes per launch (80 B/cell
+            for RK stage 1, 112 B/cell for stage 2) / mean launch time,
+            against the measured HBM copy bandwidth
+  cpu_baseline  the compiled CFFC reference (oracle/_ref) on the host cores
+
+With --gpus N (torchrun) every rank runs its own replica (the path's blocks
+live on one GPU; independent cases are the unit of scale-out): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+RK_STEPS = 500
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "exact"])
+    p.add_argument("--rk-steps", type=int, default=RK_STEPS)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.rows = []
+        self.stop = threading.Event()
+        self.th = threading.Thread(target=self.run, daemon=True)
+
+    def run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.th.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.th.join(timeout=10)
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 5 + k and r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def cpu_reference_run(bs, nsteps, threads):
+    """Times the compiled reference's explicit loop (oracle/_ref harness)."""
+    from cffc_b200 import cases
+    harness = os.path.join(ROOT, "oracle", "_ref", "e2d_ref_harness")
+    if not os.path.exists(harness):
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.bin")
+        cases.write_case(cp, bs)
+        out = subprocess.run([harness, "time", cp, str(nsteps), str(threads)], capture_output=True,
+                             text=True, check=True).stdout
+    return json.loads(out.strip().splitlines()[-1])
+
+
+def cpu_port_run(bs, nsteps):
+    """Fallback when the compiled reference is absent: the C restatement."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import e2d_oracle
+    o = e2d_oracle.Oracle(bs)
+    o.set_state()
+    t0 = time.perf_counter()
+    rc, _ = o.rk_steps(nsteps)
+    s = time.perf_counter() - t0
+    return {"seconds": s, "steps": nsteps, "cells": bs.n_interior, "threads": 1,
+            "mcell_updates_per_s": bs.n_interior * nsteps / s * 1e-6, "error": rc}
+
+
+def cpu_baseline(bs, nsteps=12):
+    threads = os.cpu_count() or 1
+    r = cpu_reference_run(bs, nsteps, threads)
+    kind = "reference"
+    if r is None:
+        r = cpu_port_run(bs, max(2, nsteps // 4))
+        kind = "port"
+    sample = (f"{r['steps']} RK2 steps of the same 1,048,576-cell block set "
+              f"({r['cells'] * r['steps'] / 1e6:.1f} M cell-updates, {r['seconds']:.1f} s)")
+    return {"value": round(r["mcell_updates_per_s"], 4), "unit": "Mcell-updates/s",
+            "cores": r["threads"], "kind": kind, "sample": sample}
+
+
+def workload():
+    from cffc_b200 import cases
+    return cases.curvilinear_mach2()
+
+
+def config(bs, n, args):
+    return {"workload": f"curvilinear Mach-2, {bs.nblk} blocks x {bs.nci}x{bs.ncj} cells "
+                        f"({bs.n_interior} cells), {args.rk_steps} RK2 steps per bench step",
+            "blocks": bs.nblk, "cells_per_block": [bs.nci, bs.ncj], "cells": bs.n_interior,
+            "rk_steps_per_step": args.rk_steps, "scheme": "Roe + LSQ + Venkatakrishnan, RK2, CFL 0.5",
+            "precision": args.precision, "parallelism": f"replicas x{n}",
+            "l2": "working set (~170 MB per stage) larger than the 126 MB L2; no flush"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    bs = workload()
+    vals = []
+    sample_steps = 4
+    for k in range(args.warmup + args.steps):
+        r = cpu_reference_run(bs, sample_steps, os.cpu_count() or 1)
+        kind = "reference"
+        if r is None:
+            r = cpu_port_run(bs, 2)
+            kind = "port"
+        if k >= args.warmup:
+            vals.append(r)
+    v = statistics.median(x["mcell_updates_per_s"] for x in vals)
+    ms = statistics.median(x["seconds"] / x["steps"] * args.rk_steps * 1e3 for x in vals)
+    line = {"impl": "reference", "metric": "Mcell-updates/s (Roe+limiter residual, explicit RK2)",
+            "value": round(v, 4), "unit": "Mcell-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": config(bs, 1, args),
+            "cpu_baseline": {"value": round(v, 4), "unit": "Mcell-updates/s",
+                             "cores": vals[0]["threads"], "kind": kind,
+                             "sample": f"{sample_steps} RK2 steps of the 1,048,576-cell block set per bench step"},
+            "e2e": {"value": round(v, 4), "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from cffc_b200 import capi
+    bs = workload()
+    bs.scheme.precision = 2 if args.precision == "exact" else 0
+    h = capi.Handle(bs, device=local)
+    stream = torch.cuda.current_stream()
+    h.lib.e2d_set_stream.argtypes = [capi.C.c_void_p, capi.C.c_void_p]
+    h.lib.e2d_set_stream(h.h, capi.C.c_void_p(stream.cuda_stream))
+    h.set_state()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        rc, _ = h.rk_steps(args.rk_steps, history=False)
+        assert rc == 0, rc
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            rc, _ = h.rk_steps(args.rk_steps, history=False)
+            assert rc == 0, rc
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    cell_updates = bs.n_interior * args.rk_steps
+    value = world * cell_updates / (ms * 1e-3) * 1e-6
+
+    # per-kernel device times of the fused stage kernel (launch by launch)
+    kt = np.zeros(6)
+    h.lib.e2d_kernel_times.argtypes = [capi.C.c_void_p, capi.C.c_int, capi._dp]
+    rc = h.lib.e2d_kernel_times(h.h, 20, capi.ptr(kt))
+    assert rc == 0, rc
+    hbm, peak_kind = peaks()
+    stage_ms = 0.5 * (kt[1] + kt[2])
+    stage_bytes = bs.n_interior * 0.5 * (80 + 112)  # per launch, mean of the two stages
+    achieved = stage_bytes / (stage_ms * 1e-3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # end to end through the C ABI: pinned host W in, U out, every step
+    Wh = torch.from_numpy(np.ascontiguousarray(bs.W)).pin_memory()
+    Uh = torch.empty(bs.cell_shape(), dtype=torch.float64).pin_memory()
+    Wp = capi.C.cast(Wh.data_ptr(), capi._dp)
+    Up = capi.C.cast(Uh.data_ptr(), capi._dp)
+    nbytes = Wh.numel() * 8
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        assert h.lib.e2d_set_state(h.h, Wp) == 0
+        rc, _ = h.rk_steps(args.rk_steps, history=False)
+        assert rc == 0
+        assert h.lib.e2d_get_state(h.h, capi.C.cast(None, capi._dp), Up) == 0
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * cell_updates / (e2e_ms * 1e-3) * 1e-6
+
+    line = None
+    if rank == 0:
+        launches_per_rk = 4 + 2 * bs.scheme.n_stage + 1
+        line = {
+            "metric": "Mcell-updates/s (Roe+limiter residual, explicit RK2)",
+            "value": round(value, 3), "unit": "Mcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded curvilinear grid and perturbation)",
+            "config": config(bs, world, args),
+            "e2e": {"value": round(e2e, 3), "unit": "Mcell-updates/s",
+                    "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+            "roofline": {"bound": "hbm", "kernel": "stage_kernel (fused LSQ+limiter+Roe+update)",
+                         "achieved": round(achieved, 2), "peak": hbm, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": traffic,
+                         "algorithmic_bytes_per_launch": stage_bytes,
+                         "launch_ms": {"ghost_fill": round(kt[0], 5), "stage1": round(kt[1], 5),
+                                       "stage2": round(kt[2], 5), "cfl": round(kt[3], 5),
+                                       "norms": round(kt[4], 5), "step": round(kt[5], 5)}},
+            "path_roofline": {"bytes_per_cell_update": 240,
+                              "achieved_gbs": round(240 * cell_updates / (ms * 1e-3) / 1e9, 2),
+                              "frac": round(240 * cell_updates / (ms * 1e-3) / 1e9 / hbm, 4)},
+            "gpu_launches": args.steps * args.rk_steps * launches_per_rk,
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(bs)
+        print(json.dumps(line), flush=True)
+    h.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

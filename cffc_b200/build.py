@@ -1,0 +1,63 @@
+"""Builds libcffc_e2d.so in-tree with nvcc for sm_100a.
+
+Per-file flags matter: the exact FP64 kernels (and the ghost-fill, time-step,
+norm and state-conversion kernels every path shares) are compiled with
+-fmad=false so they round as the reference's x86-64 build does; the fast
+FP64 kernels are compiled with contraction on.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libcffc_e2d.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+          "--expt-relaxed-constexpr"]
+SOURCES = {
+    "e2d_exact.cu": ["-fmad=false"],
+    "e2d_fast.cu": ["-fmad=true"],
+    "e2d_capi.cu": ["-fmad=false"],
+}
+HEADERS = ["e2d_device.cuh", "e2d_stage.cuh", "e2d_aux.cuh", "e2d_launch.h",
+           os.path.join("..", "..", "include", "cffc_e2d.h")]
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose: bool = False, ptxas_info: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    headers = [os.path.join(CSRC, h) for h in HEADERS]
+    objs = []
+    for src, flags in SOURCES.items():
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        objs.append(o)
+        if ptxas_info or _newer(o, [s, __file__] + headers):
+            cmd = [NVCC, *ARCH, *COMMON, *flags, "-c", s, "-o", o]
+            if ptxas_info:
+                cmd += ["-Xptxas", "-v"]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
+    if _newer(LIB, objs):
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, ptxas_info="-v" in sys.argv)

@@ -1,0 +1,395 @@
+// e2d_capi.cu — the C ABI of include/cffc_e2d.h: handle life cycle, device
+// memory, and the launch sequences of the reference's per-block routines.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/cffc_e2d.h"
+#include "e2d_launch.h"
+
+using namespace e2d;
+
+struct e2d_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream the work is enqueued on
+  cudaStream_t own_stream = nullptr;  // the handle's own stream
+  e2d_scheme sc{};
+  Blocks B{};
+  size_t ncell = 0, nnode = 0;
+  // device allocations (owned)
+  std::vector<void*> allocs;
+  double* hist = nullptr;  // [hist_cap][4]
+  int hist_cap = 0;
+  int* step = nullptr;     // device step counter
+  double* part = nullptr;  // [nblk][3] norm partials
+  bool recon_out = false;  // dWdx/dWdy/phi arrays allocated
+  // captured explicit step
+  cudaGraphExec_t step_graph = nullptr;
+};
+
+namespace {
+
+#define CK(call)                                                               \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      fprintf(stderr, "cffc_e2d: %s failed: %s\n", #call, cudaGetErrorString(e_)); \
+      return E2D_ERR_CUDA;                                                     \
+    }                                                                          \
+  } while (0)
+
+template <class T> int dalloc(e2d_handle* h, T** p, size_t n) {
+  void* q = nullptr;
+  if (cudaMalloc(&q, sizeof(T) * (n ? n : 1)) != cudaSuccess) return E2D_ERR_NOMEM;
+  h->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return 0;
+}
+
+template <class T> int upload(e2d_handle* h, T** p, const T* src, size_t n) {
+  int rc = dalloc(h, p, n);
+  if (rc) return rc;
+  CK(cudaMemcpy(*p, src, sizeof(T) * n, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int check_status(e2d_handle* h) {
+  int st[2] = {0, 0};
+  CK(cudaMemcpyAsync(st, h->B.status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (st[0] == ST_NEGATIVE) return 1 + st[1];
+  return st[0] ? E2D_ERR_CUDA : 0;
+}
+
+cudaError_t launch_stage_any(e2d_handle* h, int mode) {
+  StageArgs a{};
+  a.B = h->B;
+  a.mode = mode;
+  a.hist = h->hist;
+  a.step = h->step;
+  const bool exact = h->sc.precision == E2D_PREC_FP64_EXACT;
+  const int ti = exact ? exact::tile_i() : fast::tile_i();
+  const int tj = exact ? exact::tile_j() : fast::tile_j();
+  a.tiles_i = (h->B.nci + ti - 1) / ti;
+  a.tiles_j = (h->B.ncj + tj - 1) / tj;
+  return exact ? exact::launch_stage(a, h->stream) : fast::launch_stage(a, h->stream);
+}
+
+int ensure_recon(e2d_handle* h) {
+  if (h->recon_out) return 0;
+  int rc;
+  if ((rc = dalloc(h, &h->B.dWdx, 4 * h->ncell))) return rc;
+  if ((rc = dalloc(h, &h->B.dWdy, 4 * h->ncell))) return rc;
+  if ((rc = dalloc(h, &h->B.phi, 4 * h->ncell))) return rc;
+  CK(cudaMemsetAsync(h->B.dWdx, 0, sizeof(double) * 4 * h->ncell, h->stream));
+  CK(cudaMemsetAsync(h->B.dWdy, 0, sizeof(double) * 4 * h->ncell, h->stream));
+  CK(cudaMemsetAsync(h->B.phi, 0, sizeof(double) * 4 * h->ncell, h->stream));
+  h->recon_out = true;
+  return 0;
+}
+
+int ensure_hist(e2d_handle* h, int n) {
+  if (n <= h->hist_cap) return 0;
+  int cap = n < 64 ? 64 : n;
+  double* p = nullptr;
+  if (cudaMalloc(&p, sizeof(double) * 4 * cap) != cudaSuccess) return E2D_ERR_NOMEM;
+  if (h->hist) {
+    for (auto& q : h->allocs)
+      if (q == h->hist) { cudaFree(q); q = p; }
+  } else {
+    h->allocs.push_back(p);
+  }
+  h->hist = p;
+  h->hist_cap = cap;
+  if (h->step_graph) { cudaGraphExecDestroy(h->step_graph); h->step_graph = nullptr; }
+  return 0;
+}
+
+// One explicit time step in the reference's order (Euler2DQuadSolvers.cc:657-898).
+cudaError_t enqueue_step(e2d_handle* h) {
+  cudaError_t e;
+  if ((e = launch_step_begin(h->hist, h->step, h->stream))) return e;
+  if ((e = launch_cfl(h->B, h->hist, h->step, h->stream))) return e;
+  if ((e = launch_norms(h->B, h->part, h->hist, h->step, h->stream))) return e;
+  for (int stage = 1; stage <= h->sc.n_stage; ++stage) {
+    if ((e = launch_ghost_fill(h->B, h->stream))) return e;
+    if ((e = launch_stage_any(h, stage))) return e;
+  }
+  return launch_step_end(h->step, h->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+e2d_handle* e2d_create(const e2d_blocks_desc* d, const e2d_scheme* sc, int device, int* err) {
+  auto fail = [&](int code, e2d_handle* h) -> e2d_handle* {
+    if (err) *err = code;
+    if (h) e2d_destroy(h);
+    return nullptr;
+  };
+  if (err) *err = 0;
+  if (!d || !sc || d->nblk < 1 || d->nci < 2 || d->ncj < 2 || d->ng != NG) return fail(E2D_ERR_ARG, nullptr);
+  if (sc->n_stage != 1 && sc->n_stage != 2) return fail(E2D_ERR_ARG, nullptr);
+  if (sc->flux != E2D_FLUX_ROE) return fail(E2D_ERR_ARG, nullptr);
+  if (sc->precision != E2D_PREC_FP64 && sc->precision != E2D_PREC_FP64_EXACT) return fail(E2D_ERR_ARG, nullptr);
+  if (sc->limiter != E2D_LIMITER_VENKATAKRISHNAN && sc->limiter != E2D_LIMITER_BARTH_JESPERSEN &&
+      sc->limiter != E2D_LIMITER_ONE && sc->limiter != E2D_LIMITER_ZERO)
+    return fail(E2D_ERR_ARG, nullptr);
+  const int NCi = d->nci + 2 * NG, NCj = d->ncj + 2 * NG;
+  // Supported BC codes only (others would need reference code paths not built here).
+  auto bc_ok = [](const int32_t* a, size_t n) {
+    for (size_t q = 0; q < n; ++q) {
+      const int c = a[q];
+      if (c != E2D_BC_NONE && c != E2D_BC_CONSTANT_EXTRAPOLATION && c != E2D_BC_PERIODIC &&
+          c != E2D_BC_REFLECTION && c != E2D_BC_CHARACTERISTIC && c != E2D_BC_FIXED)
+        return false;
+    }
+    return true;
+  };
+  if (!bc_ok(d->bc_w, size_t(d->nblk) * NCj) || !bc_ok(d->bc_e, size_t(d->nblk) * NCj) ||
+      !bc_ok(d->bc_s, size_t(d->nblk) * NCi) || !bc_ok(d->bc_n, size_t(d->nblk) * NCi))
+    return fail(E2D_ERR_ARG, nullptr);
+  for (int q = 0; q < 8 * d->nblk; ++q)
+    if (d->neighbour[q] < -1 || d->neighbour[q] >= d->nblk) return fail(E2D_ERR_ARG, nullptr);
+  if (cudaSetDevice(device) != cudaSuccess) return fail(E2D_ERR_CUDA, nullptr);
+
+  e2d_handle* h = new e2d_handle;
+  h->device = device;
+  h->sc = *sc;
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(E2D_ERR_CUDA, h);
+  h->stream = h->own_stream;
+  Blocks& B = h->B;
+  B.nblk = d->nblk; B.nci = d->nci; B.ncj = d->ncj;
+  B.NCi = NCi; B.NCj = NCj; B.NNi = NCi + 1; B.NNj = NCj + 1;
+  h->ncell = size_t(B.nblk) * NCi * NCj;
+  h->nnode = size_t(B.nblk) * B.NNi * B.NNj;
+  B.g = sc->gamma; B.gm1 = B.g - 1.0; B.gm1i = 1.0 / B.gm1;
+  B.cfl = sc->cfl; B.limiter = sc->limiter; B.n_stage = sc->n_stage; B.local_dt = sc->local_dt;
+  int rc = 0;
+  int *neigh, *bcw, *bce, *bcs, *bcn;
+  double *X, *Y, *wow, *woe, *wos, *won;
+  if ((rc = upload(h, &neigh, d->neighbour, size_t(8) * B.nblk)) ||
+      (rc = upload(h, &bcw, d->bc_w, size_t(B.nblk) * NCj)) || (rc = upload(h, &bce, d->bc_e, size_t(B.nblk) * NCj)) ||
+      (rc = upload(h, &bcs, d->bc_s, size_t(B.nblk) * NCi)) || (rc = upload(h, &bcn, d->bc_n, size_t(B.nblk) * NCi)) ||
+      (rc = upload(h, &X, d->node_x, h->nnode)) || (rc = upload(h, &Y, d->node_y, h->nnode)) ||
+      (rc = upload(h, &wow, d->wo_w, size_t(B.nblk) * 4 * NCj)) ||
+      (rc = upload(h, &woe, d->wo_e, size_t(B.nblk) * 4 * NCj)) ||
+      (rc = upload(h, &wos, d->wo_s, size_t(B.nblk) * 4 * NCi)) ||
+      (rc = upload(h, &won, d->wo_n, size_t(B.nblk) * 4 * NCi)))
+    return fail(rc, h);
+  B.neigh = neigh; B.bcw = bcw; B.bce = bce; B.bcs = bcs; B.bcn = bcn;
+  B.X = X; B.Y = Y; B.wow = wow; B.woe = woe; B.wos = wos; B.won = won;
+  if ((rc = dalloc(h, &B.W, 4 * h->ncell)) || (rc = dalloc(h, &B.U, 4 * h->ncell)) ||
+      (rc = dalloc(h, &B.Uo, 4 * h->ncell)) || (rc = dalloc(h, &B.dUdt, 4 * h->ncell)) ||
+      (rc = dalloc(h, &B.dt, h->ncell)) || (rc = dalloc(h, &B.status, 2)) ||
+      (rc = dalloc(h, &h->step, 1)) || (rc = dalloc(h, &h->part, size_t(3) * B.nblk)))
+    return fail(rc, h);
+  if (cudaMemset(B.W, 0, sizeof(double) * 4 * h->ncell) || cudaMemset(B.U, 0, sizeof(double) * 4 * h->ncell) ||
+      cudaMemset(B.Uo, 0, sizeof(double) * 4 * h->ncell) || cudaMemset(B.dUdt, 0, sizeof(double) * 4 * h->ncell) ||
+      cudaMemset(B.dt, 0, sizeof(double) * h->ncell) || cudaMemset(B.status, 0, sizeof(int) * 2) ||
+      cudaMemset(h->step, 0, sizeof(int)))
+    return fail(E2D_ERR_CUDA, h);
+  if ((rc = ensure_hist(h, 64))) return fail(rc, h);
+  B.dWdx = B.dWdy = B.phi = nullptr;
+  return h;
+}
+
+void e2d_destroy(e2d_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+}
+
+// U = U(W) for every cell (Euler2D_pState::U, Euler2DState.h:1748).
+__global__ void u_of_w_kernel(Blocks B, long long ncell) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    const long long b = q / ((long long)B.NCi * B.NCj), r = q % ((long long)B.NCi * B.NCj);
+    const size_t s = size_t(B.NCi) * B.NCj;
+    const size_t base = size_t(b) * 4 * s + size_t(r);
+    PState<double> w{B.W[base], B.W[base + s], B.W[base + 2 * s], B.W[base + 3 * s]};
+    const CState<double> u = U_of_W(w, B.gm1i);
+    B.U[base] = u.d; B.U[base + s] = u.mx; B.U[base + 2 * s] = u.my; B.U[base + 3 * s] = u.E;
+  }
+}
+
+int e2d_set_state(e2d_handle* h, const double* W) {
+  if (!h || !W) return E2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(h->B.W, W, sizeof(double) * 4 * h->ncell, cudaMemcpyHostToDevice, h->stream));
+  int grid = int((h->ncell + 255) / 256);
+  if (grid > 4096) grid = 4096;
+  u_of_w_kernel<<<grid, 256, 0, h->stream>>>(h->B, (long long)h->ncell);
+  CK(cudaGetLastError());
+  CK(cudaMemsetAsync(h->B.status, 0, sizeof(int) * 2, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int e2d_get_state(e2d_handle* h, double* W, double* U) {
+  if (!h) return E2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  if (W) CK(cudaMemcpyAsync(W, h->B.W, sizeof(double) * 4 * h->ncell, cudaMemcpyDeviceToHost, h->stream));
+  if (U) CK(cudaMemcpyAsync(U, h->B.U, sizeof(double) * 4 * h->ncell, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int e2d_fill_ghosts(e2d_handle* h) {
+  if (!h) return E2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(launch_ghost_fill(h->B, h->stream));
+  return check_status(h);
+}
+
+int e2d_residual(e2d_handle* h, double* dUdt) {
+  if (!h) return E2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int rc = ensure_recon(h);
+  if (rc) return rc;
+  CK(launch_ghost_fill(h->B, h->stream));
+  CK(launch_stage_any(h, 0));
+  if (dUdt) CK(cudaMemcpyAsync(dUdt, h->B.dUdt, sizeof(double) * 4 * h->ncell, cudaMemcpyDeviceToHost, h->stream));
+  return check_status(h);
+}
+
+int e2d_get_reconstruction(e2d_handle* h, double* dWdx, double* dWdy, double* phi) {
+  if (!h) return E2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int rc = ensure_recon(h);
+  if (rc) return rc;
+  const size_t n = sizeof(double) * 4 * h->ncell;
+  if (dWdx) CK(cudaMemcpyAsync(dWdx, h->B.dWdx, n, cudaMemcpyDeviceToHost, h->stream));
+  if (dWdy) CK(cudaMemcpyAsync(dWdy, h->B.dWdy, n, cudaMemcpyDeviceToHost, h->stream));
+  if (phi) CK(cudaMemcpyAsync(phi, h->B.phi, n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int e2d_rk_steps(e2d_handle* h, int n_steps, double* hist) {
+  if (!h || n_steps < 0) return E2D_ERR_ARG;
+  if (n_steps == 0) return 0;
+  CK(cudaSetDevice(h->device));
+  int rc = ensure_hist(h, n_steps);
+  if (rc) return rc;
+  // the stage kernels do not write the optional reconstruction arrays
+  const Blocks saved = h->B;
+  h->B.dWdx = h->B.dWdy = h->B.phi = nullptr;
+  CK(cudaMemsetAsync(h->step, 0, sizeof(int), h->stream));
+  if (!h->step_graph) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue_step(h);
+    cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      h->B = saved;
+      fprintf(stderr, "cffc_e2d: step capture failed: %s\n", cudaGetErrorString(e ? e : e2));
+      return E2D_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&h->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { h->B = saved; h->step_graph = nullptr; return E2D_ERR_CUDA; }
+  }
+  h->B = saved;
+  for (int s = 0; s < n_steps; ++s) CK(cudaGraphLaunch(h->step_graph, h->stream));
+  if (hist) CK(cudaMemcpyAsync(hist, h->hist, sizeof(double) * 4 * n_steps, cudaMemcpyDeviceToHost, h->stream));
+  return check_status(h);
+}
+
+int e2d_norms(e2d_handle* h, double out[3]) {
+  if (!h || !out) return E2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemsetAsync(h->step, 0, sizeof(int), h->stream));
+  CK(launch_norms(h->B, h->part, h->hist, h->step, h->stream));
+  double tmp[4];
+  CK(cudaMemcpyAsync(tmp, h->hist, sizeof(tmp), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  out[0] = tmp[1]; out[1] = tmp[2]; out[2] = tmp[3];
+  return 0;
+}
+
+int e2d_status(e2d_handle* h) {
+  if (!h) return E2D_ERR_ARG;
+  return check_status(h);
+}
+
+int e2d_device_state(e2d_handle* h, double** W, double** U, double** dUdt) {
+  if (!h) return E2D_ERR_ARG;
+  if (W) *W = h->B.W;
+  if (U) *U = h->B.U;
+  if (dUdt) *dUdt = h->B.dUdt;
+  return 0;
+}
+
+int e2d_set_stream(e2d_handle* h, void* stream) {
+  if (!h) return E2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  if (!h->own_stream) {
+    CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+  }
+  h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+  return 0;
+}
+
+int e2d_kernel_times(e2d_handle* h, int n_steps, double out[6]) {
+  if (!h || !out || n_steps < 1) return E2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int rc = ensure_hist(h, n_steps);
+  if (rc) return rc;
+  const Blocks saved = h->B;
+  h->B.dWdx = h->B.dWdy = h->B.phi = nullptr;
+  cudaEvent_t ev[10];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  CK(cudaMemsetAsync(h->step, 0, sizeof(int), h->stream));
+  for (int s = 0; s < n_steps; ++s) {
+    CK(cudaEventRecord(ev[0], h->stream));
+    CK(launch_step_begin(h->hist, h->step, h->stream));
+    CK(launch_cfl(h->B, h->hist, h->step, h->stream));
+    CK(cudaEventRecord(ev[1], h->stream));
+    CK(launch_norms(h->B, h->part, h->hist, h->step, h->stream));
+    CK(cudaEventRecord(ev[2], h->stream));
+    CK(launch_ghost_fill(h->B, h->stream));
+    CK(cudaEventRecord(ev[3], h->stream));
+    CK(launch_stage_any(h, 1));
+    CK(cudaEventRecord(ev[4], h->stream));
+    if (h->sc.n_stage == 2) {
+      CK(launch_ghost_fill(h->B, h->stream));
+      CK(cudaEventRecord(ev[5], h->stream));
+      CK(launch_stage_any(h, 2));
+      CK(cudaEventRecord(ev[6], h->stream));
+    }
+    CK(launch_step_end(h->step, h->stream));
+    CK(cudaEventRecord(ev[7], h->stream));
+    CK(cudaEventSynchronize(ev[7]));
+    float t[8] = {0};
+    for (int k = 1; k <= 7; ++k)
+      if (h->sc.n_stage == 2 || (k != 5 && k != 6)) CK(cudaEventElapsedTime(&t[k], ev[0], ev[k]));
+    acc[3] += t[1];
+    acc[4] += t[2] - t[1];
+    acc[0] += t[3] - t[2];
+    acc[1] += t[4] - t[3];
+    if (h->sc.n_stage == 2) {
+      acc[0] += t[5] - t[4];
+      acc[2] += t[6] - t[5];
+    }
+    acc[5] += t[7];
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  h->B = saved;
+  const double gf = h->sc.n_stage == 2 ? 2.0 * n_steps : double(n_steps);
+  out[0] = acc[0] / gf;
+  for (int k = 1; k < 6; ++k) out[k] = acc[k] / n_steps;
+  return check_status(h);
+}
+
+}  // extern "C"

@@ -1,0 +1,26 @@
+// Host-side declarations of the kernel launchers (one set per precision path).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "e2d_device.cuh"
+
+namespace e2d {
+namespace exact {
+cudaError_t launch_stage(const StageArgs& a, cudaStream_t st);
+size_t stage_smem_bytes();
+int tile_i();
+int tile_j();
+}  // namespace exact
+namespace fast {
+cudaError_t launch_stage(const StageArgs& a, cudaStream_t st);
+size_t stage_smem_bytes();
+int tile_i();
+int tile_j();
+}  // namespace fast
+cudaError_t launch_ghost_fill(const Blocks& B, cudaStream_t st);
+cudaError_t launch_cfl(const Blocks& B, double* hist, const int* step, cudaStream_t st);
+cudaError_t launch_norms(const Blocks& B, double* part, double* hist, const int* step, cudaStream_t st);
+cudaError_t launch_step_begin(double* hist, int* step, cudaStream_t st);
+cudaError_t launch_step_end(int* step, cudaStream_t st);
+cudaError_t launch_fill(double* p, long long n, double v, cudaStream_t st);
+}  // namespace e2d

@@ -1,0 +1,448 @@
+// e2d_stage.cuh — the fused residual / explicit-stage kernel.
+//
+// One CTA per TI x TJ tile of interior cells of one block.  The CTA stages the
+// tile's primitive state with its two-cell halo and the tile's nodes in
+// shared memory, computes cell centroids, the least-squares gradients and
+// limiter of every cell that touches a tile face, the Roe flux of every face
+// of the tile exactly once, and then, per interior cell, the flux divergence
+// and (for an RK stage) the solution update — one pass over HBM per stage.
+//
+// It restates, fused:
+//   Linear_Reconstruction_LeastSquares   src_2D/Euler2D/Euler2DQuadSingleBlock.cc:3678-4087
+//   Euler2D_Quad_Block::dUdt_Residual_Evaluation   src_2D/Euler2D/Euler2DQuad.cc:814-1227
+//   Euler2D_Quad_Block::dUdt_Multistage_Explicit   src_2D/Euler2D/Euler2DQuad.cc:1235-1727
+//   Update_Solution_Multistage_Explicit   src_2D/Euler2D/Euler2DQuadSingleBlock.cc:5300-5507
+// with each cell's residual accumulated in the reference's loop order
+// (west + , east - , south + , north -).
+//
+// This header is compiled twice: with -fmad=false (namespace e2d::exact,
+// bit-identical to the FP64 reference) and with contraction on
+// (namespace e2d::fast).  E2D_NS names the namespace.
+#pragma once
+#include "e2d_device.cuh"
+
+#ifndef E2D_NS
+#error "E2D_NS must name the kernel namespace"
+#endif
+
+namespace e2d {
+namespace E2D_NS {
+
+constexpr int TI = 32, TJ = 8;          // interior cells per tile
+constexpr int HI = TI + 4, HJ = TJ + 4; // W tile with 2-cell halo
+constexpr int NI = TI + 5, NJ = TJ + 5; // nodes of the halo tile
+constexpr int RI = TI + 2, RJ = TJ + 2; // cells reconstructed (tile + 1 ring)
+constexpr int NTHREADS = TI * TJ;
+
+struct Smem {
+  double W[4][HJ][HI];
+  double X[NJ][NI], Y[NJ][NI];
+  double xc[HJ][HI], yc[HJ][HI];
+  double px[4][RJ][RI], py[4][RJ][RI];   // phi^dWdx, phi^dWdy
+  double Fi[4][TJ][TI + 1], Fj[4][TJ + 1][TI];  // face fluxes
+  double li[TJ][TI + 1], lj[TJ + 1][TI];        // face lengths
+};
+
+__device__ __forceinline__ bool face_bc(int bc) {
+  return bc == E2D_BC_REFLECTION || bc == E2D_BC_CHARACTERISTIC;
+}
+
+// Outward normal of the edge a->c with the reference's degenerate-edge test
+// (l > NANO * perimeter of the owning cell, else ihat).
+__device__ __forceinline__ void edge_normal(double ax, double ay, double cx, double cy, double l,
+                                            double perim, double& nx, double& ny) {
+  if (l > NANO * perim) {
+    const double dx = ax - cx, dy = ay - cy;
+    const double n = sqrt(dx * dx + dy * dy);
+    nx = (ay - cy) / n;
+    ny = -(ax - cx) / n;
+  } else {
+    nx = 1.0; ny = 0.0;
+  }
+}
+__device__ __forceinline__ double edge_len(double ax, double ay, double cx, double cy) {
+  const double dx = ax - cx, dy = ay - cy;
+  return sqrt(dx * dx + dy * dy);
+}
+
+// Perimeter of halo cell (hi, hj) in the reference's order lE + lN + lW + lS.
+__device__ __forceinline__ double cell_perimeter(const Smem& s, int hi, int hj) {
+  const double lE = edge_len(s.X[hj][hi + 1], s.Y[hj][hi + 1], s.X[hj + 1][hi + 1], s.Y[hj + 1][hi + 1]);
+  const double lN = edge_len(s.X[hj + 1][hi], s.Y[hj + 1][hi], s.X[hj + 1][hi + 1], s.Y[hj + 1][hi + 1]);
+  const double lW = edge_len(s.X[hj][hi], s.Y[hj][hi], s.X[hj + 1][hi], s.Y[hj + 1][hi]);
+  const double lS = edge_len(s.X[hj][hi], s.Y[hj][hi], s.X[hj][hi + 1], s.Y[hj][hi + 1]);
+  return lE + lN + lW + lS;
+}
+// A cheap upper bound of the perimeter (sum of |dx|+|dy| of the edges): when
+// l exceeds NANO times it, the exact test passes too.
+__device__ __forceinline__ double perimeter_bound(const Smem& s, int hi, int hj) {
+  const double x0 = s.X[hj][hi], y0 = s.Y[hj][hi], x1 = s.X[hj][hi + 1], y1 = s.Y[hj][hi + 1];
+  const double x2 = s.X[hj + 1][hi + 1], y2 = s.Y[hj + 1][hi + 1], x3 = s.X[hj + 1][hi], y3 = s.Y[hj + 1][hi];
+  return 2.0 * (fabs(x1 - x0) + fabs(y1 - y0) + fabs(x2 - x1) + fabs(y2 - y1) + fabs(x3 - x2) +
+                fabs(y3 - y2) + fabs(x0 - x3) + fabs(y0 - y3));
+}
+__device__ __forceinline__ double perim_for_test(const Smem& s, int hi, int hj, double l) {
+  const double pb = perimeter_bound(s, hi, hj);
+  return (l > NANO * pb) ? 0.0 : cell_perimeter(s, hi, hj);
+}
+
+// Least-squares stencil (Euler2DQuadSingleBlock.cc:3692-3990) of array cell
+// (I, J).  Writes offsets (di, dj) relative to the cell; returns n_pts.
+__device__ __forceinline__ int lsq_stencil(const Blocks& B, int b, int I, int J, int* di, int* dj) {
+  const int ICl = NG, ICu = B.nci + NG - 1, JCl = NG, JCu = B.ncj + NG - 1;
+  int n = 0;
+#define P(a, c) (di[n] = (a), dj[n] = (c), ++n)
+#define FULL8 P(-1,-1); P(0,-1); P(1,-1); P(-1,0); P(1,0); P(-1,1); P(0,1); P(1,1)
+#define EXTRAP(t) ((t) == E2D_BC_PERIODIC || (t) == E2D_BC_CONSTANT_EXTRAPOLATION || (t) == 4002 || (t) == E2D_BC_CHARACTERISTIC)
+  if (I == ICl - NG || I == ICu + NG || J == JCl - NG || J == JCu + NG) return 0;
+  const bool westG = (I == ICl - NG + 1), eastG = (I == ICu + NG - 1);
+  const bool southG = (J == JCl - NG + 1), northG = (J == JCu + NG - 1);
+  if (!(westG || eastG || southG || northG)) { FULL8; return n; }
+  const int bw = B.bcw[size_t(b) * B.NCj + J], be = B.bce[size_t(b) * B.NCj + J];
+  const int bs = B.bcs[size_t(b) * B.NCi + I], bn = B.bcn[size_t(b) * B.NCi + I];
+  if (westG && bw != E2D_BC_NONE) {
+    if (southG || northG) return 0;
+    if (EXTRAP(bw)) {
+      if (J == JCl) { P(-1,0); P(1,0); P(-1,1); P(0,1); P(1,1); }
+      else if (J == JCu) { P(-1,-1); P(0,-1); P(1,-1); P(-1,0); P(1,0); }
+      else { FULL8; }
+    } else {
+      if (J == JCl) { P(1,0); P(0,1); P(1,1); }
+      else if (J == JCu) { P(0,-1); P(1,-1); P(1,0); }
+      else { P(0,-1); P(1,-1); P(1,0); P(0,1); P(1,1); }
+    }
+  } else if (eastG && be != E2D_BC_NONE) {
+    if (southG || northG) return 0;
+    if (EXTRAP(be)) {
+      if (J == JCl) { P(-1,0); P(1,0); P(-1,1); P(0,1); P(1,1); }
+      else if (J == JCu) { P(-1,-1); P(0,-1); P(1,-1); P(-1,0); P(1,0); }
+      else { FULL8; }
+    } else {
+      if (J == JCl) { P(-1,0); P(-1,1); P(0,1); }
+      else if (J == JCu) { P(-1,-1); P(0,-1); P(-1,0); }
+      else { P(-1,-1); P(0,-1); P(-1,0); P(-1,1); P(0,1); }
+    }
+  } else if (southG && bs != E2D_BC_NONE) {
+    if (westG || eastG) return 0;
+    if (EXTRAP(bs)) {
+      if (I == ICl) { P(0,-1); P(1,-1); P(1,0); P(0,1); P(1,1); }
+      else if (I == ICu) { P(-1,-1); P(0,-1); P(-1,0); P(-1,1); P(0,1); }
+      else { FULL8; }
+    } else {
+      if (I == ICl) { P(1,0); P(0,1); P(1,1); }
+      else if (I == ICu) { P(-1,0); P(-1,1); P(0,1); }
+      else { P(-1,0); P(1,0); P(-1,1); P(0,1); P(1,1); }
+    }
+  } else if (northG && bn != E2D_BC_NONE) {
+    if (westG || eastG) return 0;
+    if (EXTRAP(bn)) {
+      if (I == ICl) { P(0,-1); P(1,-1); P(1,0); P(0,1); P(1,1); }
+      else if (I == ICu) { P(-1,-1); P(0,-1); P(-1,0); P(-1,1); P(0,1); }
+      else { FULL8; }
+    } else {
+      if (I == ICl) { P(0,-1); P(1,-1); P(1,0); }
+      else if (I == ICu) { P(-1,-1); P(0,-1); P(-1,0); }
+      else { P(-1,-1); P(0,-1); P(1,-1); P(-1,0); P(1,0); }
+    }
+  } else {
+    FULL8;
+  }
+#undef P
+#undef FULL8
+#undef EXTRAP
+  return n;
+}
+
+// Limited linear face state of halo cell (hi, hj) (recon index hi-1, hj-1)
+// at face point (fx, fy): W + (phi^dWdx)*dx + (phi^dWdy)*dy.
+__device__ __forceinline__ PState<double> face_state(const Smem& s, int hi, int hj, double fx, double fy) {
+  const double dx = fx - s.xc[hj][hi], dy = fy - s.yc[hj][hi];
+  PState<double> w;
+  w.d = s.W[0][hj][hi] + s.px[0][hj - 1][hi - 1] * dx + s.py[0][hj - 1][hi - 1] * dy;
+  w.u = s.W[1][hj][hi] + s.px[1][hj - 1][hi - 1] * dx + s.py[1][hj - 1][hi - 1] * dy;
+  w.v = s.W[2][hj][hi] + s.px[2][hj - 1][hi - 1] * dx + s.py[2][hj - 1][hi - 1] * dy;
+  w.p = s.W[3][hj][hi] + s.px[3][hj - 1][hi - 1] * dx + s.py[3][hj - 1][hi - 1] * dy;
+  return w;
+}
+
+__device__ __forceinline__ PState<double> load_wo(const double* wo, int b, int len, int k) {
+  const double* p = wo + size_t(b) * 4 * len;
+  PState<double> w;
+  w.d = p[k]; w.u = p[len + k]; w.v = p[2 * len + k]; w.p = p[3 * len + k];
+  return w;
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem& s = *reinterpret_cast<Smem*>(smem_raw);
+  const Blocks& B = a.B;
+  const int tid = threadIdx.x;
+  const int tiles = a.tiles_i * a.tiles_j;
+  const int b = blockIdx.x / tiles;
+  const int t = blockIdx.x % tiles;
+  const int i0 = (t % a.tiles_i) * TI;   // interior index of the tile's first cell
+  const int j0 = (t / a.tiles_i) * TJ;   // == array index of the halo origin
+  if (B.status[0] != 0) return;  // an earlier kernel failed: stop marching
+  const double* dtmin_p = a.hist ? a.hist + 4 * (*a.step) : nullptr;
+  const double g = B.g, gm1 = B.gm1, gm1i = B.gm1i;
+
+  // ---- stage W and nodes (halo tile) --------------------------------------
+  for (int q = tid; q < 4 * HJ * HI; q += NTHREADS) {
+    const int v = q / (HJ * HI), r = q % (HJ * HI), hj = r / HI, hi = r % HI;
+    const int I = i0 + hi, J = j0 + hj;
+    s.W[v][hj][hi] = (I < B.NCi && J < B.NCj) ? B.W[cell_var(B, b, v, J, I)] : 0.0;
+  }
+  for (int q = tid; q < NJ * NI; q += NTHREADS) {
+    const int nj = q / NI, ni = q % NI, I = i0 + ni, J = j0 + nj;
+    const bool in = I < B.NNi && J < B.NNj;
+    s.X[nj][ni] = in ? B.X[node_ix(B, b, J, I)] : 0.0;
+    s.Y[nj][ni] = in ? B.Y[node_ix(B, b, J, I)] : 0.0;
+  }
+  __syncthreads();
+
+  // ---- centroids of the halo tile ------------------------------------------
+  for (int q = tid; q < HJ * HI; q += NTHREADS) {
+    const int hj = q / HI, hi = q % HI;
+    double xc, yc, area;
+    quad_centroid(s.X[hj][hi], s.Y[hj][hi], s.X[hj][hi + 1], s.Y[hj][hi + 1], s.X[hj + 1][hi + 1],
+                  s.Y[hj + 1][hi + 1], s.X[hj + 1][hi], s.Y[hj + 1][hi], xc, yc, area);
+    s.xc[hj][hi] = xc;
+    s.yc[hj][hi] = yc;
+  }
+  __syncthreads();
+
+  // ---- least-squares gradients and limiter of the ring-1 region -----------
+  const int nci_t = min(TI, B.nci - i0), ncj_t = min(TJ, B.ncj - j0);
+  for (int q = tid; q < RJ * RI; q += NTHREADS) {
+    const int rj = q / RI, ri = q % RI;
+    const int hi = ri + 1, hj = rj + 1;
+    const int I = i0 + hi, J = j0 + hj;
+    if (ri > nci_t + 1 || rj > ncj_t + 1) continue;
+    int di[8], dj[8];
+    const int n = lsq_stencil(B, b, I, J, di, dj);
+    if (n == 0) {
+      for (int v = 0; v < 4; ++v) { s.px[v][rj][ri] = 0.0; s.py[v][rj][ri] = 0.0; }
+      if (B.dWdx)
+        for (int v = 0; v < 4; ++v) {
+          const size_t o = cell_var(B, b, v, J, I);
+          B.dWdx[o] = 0.0; B.dWdy[o] = 0.0; B.phi[o] = 0.0;
+        }
+      continue;
+    }
+    double DUDx[4] = {0, 0, 0, 0}, DUDy[4] = {0, 0, 0, 0}, DxDx = 0, DxDy = 0, DyDy = 0;
+    const double xc0 = s.xc[hj][hi], yc0 = s.yc[hj][hi];
+    for (int k = 0; k < n; ++k) {
+      const double dx = s.xc[hj + dj[k]][hi + di[k]] - xc0;
+      const double dy = s.yc[hj + dj[k]][hi + di[k]] - yc0;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const double DU = s.W[v][hj + dj[k]][hi + di[k]] - s.W[v][hj][hi];
+        DUDx[v] += DU * dx;
+        DUDy[v] += DU * dy;
+      }
+      DxDx += dx * dx; DxDy += dx * dy; DyDy += dy * dy;
+    }
+    const double dn = double(n);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) { DUDx[v] = DUDx[v] / dn; DUDy[v] = DUDy[v] / dn; }
+    DxDx = DxDx / dn; DxDy = DxDy / dn; DyDy = DyDy / dn;
+    const double det = DxDx * DyDy - DxDy * DxDy;
+    // face midpoints E, W, N, S of the cell
+    const double fx[4] = {HALF * (s.X[hj][hi + 1] + s.X[hj + 1][hi + 1]), HALF * (s.X[hj][hi] + s.X[hj + 1][hi]),
+                          HALF * (s.X[hj + 1][hi] + s.X[hj + 1][hi + 1]), HALF * (s.X[hj][hi] + s.X[hj][hi + 1])};
+    const double fy[4] = {HALF * (s.Y[hj][hi + 1] + s.Y[hj + 1][hi + 1]), HALF * (s.Y[hj][hi] + s.Y[hj + 1][hi]),
+                          HALF * (s.Y[hj + 1][hi] + s.Y[hj + 1][hi + 1]), HALF * (s.Y[hj][hi] + s.Y[hj][hi + 1])};
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const double gx = (DUDx[v] * DyDy - DUDy[v] * DxDy) / det;
+      const double gy = (DUDy[v] * DxDx - DUDx[v] * DxDy) / det;
+      const double u0 = s.W[v][hj][hi];
+      double umin = u0, umax = u0;
+      for (int k = 0; k < n; ++k) {
+        const double w = s.W[v][hj + dj[k]][hi + di[k]];
+        umin = dmin(umin, w);
+        umax = dmax(umax, w);
+      }
+      double uq[4];
+#pragma unroll
+      for (int q2 = 0; q2 < 4; ++q2) uq[q2] = u0 + gx * (fx[q2] - xc0) + gy * (fy[q2] - yc0);
+      const double phi = limiter(B.limiter, uq, u0, umin, umax);
+      s.px[v][rj][ri] = phi * gx;
+      s.py[v][rj][ri] = phi * gy;
+      if (B.dWdx) {
+        const size_t o = cell_var(B, b, v, J, I);
+        B.dWdx[o] = gx; B.dWdy[o] = gy; B.phi[o] = phi;
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- face fluxes -----------------------------------------------------------
+  const int ICl = NG, ICu = B.nci + NG - 1, JCl = NG, JCu = B.ncj + NG - 1;
+  const int nfi = (TI + 1) * TJ, nfj = TI * (TJ + 1);
+  for (int q = tid; q < nfi + nfj; q += NTHREADS) {
+    PState<double> wl, wr;
+    double nx, ny, l;
+    int fi, fj;
+    bool is_i = q < nfi;
+    if (is_i) {
+      fj = q / (TI + 1); fi = q % (TI + 1);
+      if (fi > nci_t || fj >= ncj_t) continue;
+      // face between halo cells (fi+1, fj+2) and (fi+2, fj+2): east face of the left cell
+      const int hl = fi + 1, hj = fj + 2, I = i0 + hl, J = j0 + hj;
+      const double ax = s.X[hj + 1][hl + 1], ay = s.Y[hj + 1][hl + 1];  // node (I+1, J+1)
+      const double cx = s.X[hj][hl + 1], cy = s.Y[hj][hl + 1];          // node (I+1, J)
+      l = edge_len(cx, cy, ax, ay);
+      edge_normal(ax, ay, cx, cy, l, perim_for_test(s, hl, hj, l), nx, ny);
+      const double mx = HALF * (cx + ax), my = HALF * (cy + ay);
+      const int bw = B.bcw[size_t(b) * B.NCj + J], be = B.bce[size_t(b) * B.NCj + J];
+      if (I == ICl - 1 && face_bc(bw)) {
+        wr = face_state(s, hl + 1, hj, mx, my);
+        // nfaceW(ICl, J) with the right cell's perimeter
+        double wx, wy;
+        edge_normal(cx, cy, ax, ay, l, perim_for_test(s, hl + 1, hj, l), wx, wy);
+        wl = (bw == E2D_BC_REFLECTION) ? reflect(wr, wx, wy)
+                                       : bc_char_pressure(wr, load_wo(B.wow, b, B.NCj, J), wx, wy, g, gm1i);
+      } else if (I == ICu && face_bc(be)) {
+        wl = face_state(s, hl, hj, mx, my);
+        wr = (be == E2D_BC_REFLECTION) ? reflect(wl, nx, ny)
+                                       : bc_char_pressure(wl, load_wo(B.woe, b, B.NCj, J), nx, ny, g, gm1i);
+      } else {
+        wl = face_state(s, hl, hj, mx, my);
+        wr = face_state(s, hl + 1, hj, mx, my);
+      }
+    } else {
+      const int q2 = q - nfi;
+      fj = q2 / TI; fi = q2 % TI;
+      if (fi >= nci_t || fj > ncj_t) continue;
+      // face between halo cells (fi+2, fj+1) and (fi+2, fj+2): north face of the lower cell
+      const int hi = fi + 2, hl = fj + 1, I = i0 + hi, J = j0 + hl;
+      const double ax = s.X[hl + 1][hi], ay = s.Y[hl + 1][hi];          // node (I, J+1)
+      const double cx = s.X[hl + 1][hi + 1], cy = s.Y[hl + 1][hi + 1];  // node (I+1, J+1)
+      l = edge_len(ax, ay, cx, cy);
+      edge_normal(ax, ay, cx, cy, l, perim_for_test(s, hi, hl, l), nx, ny);
+      const double mx = HALF * (ax + cx), my = HALF * (ay + cy);
+      const int bs = B.bcs[size_t(b) * B.NCi + I], bn = B.bcn[size_t(b) * B.NCi + I];
+      if (J == JCl - 1 && face_bc(bs)) {
+        wr = face_state(s, hi, hl + 1, mx, my);
+        double sx, sy;  // nfaceS(I, JCl): edge (I+1,J+1)->(I,J+1) of the upper cell
+        edge_normal(cx, cy, ax, ay, l, perim_for_test(s, hi, hl + 1, l), sx, sy);
+        wl = (bs == E2D_BC_REFLECTION) ? reflect(wr, sx, sy)
+                                       : bc_char_pressure(wr, load_wo(B.wos, b, B.NCi, I), sx, sy, g, gm1i);
+      } else if (J == JCu && face_bc(bn)) {
+        wl = face_state(s, hi, hl, mx, my);
+        wr = (bn == E2D_BC_REFLECTION) ? reflect(wl, nx, ny)
+                                       : bc_char_pressure(wl, load_wo(B.won, b, B.NCi, I), nx, ny, g, gm1i);
+      } else {
+        wl = face_state(s, hi, hl, mx, my);
+        wr = face_state(s, hi, hl + 1, mx, my);
+      }
+    }
+    const CState<double> F = flux_roe_n(wl, wr, nx, ny, g, gm1, gm1i);
+    if (is_i) {
+      s.Fi[0][fj][fi] = F.d; s.Fi[1][fj][fi] = F.mx; s.Fi[2][fj][fi] = F.my; s.Fi[3][fj][fi] = F.E;
+      s.li[fj][fi] = l;
+    } else {
+      s.Fj[0][fj][fi] = F.d; s.Fj[1][fj][fi] = F.mx; s.Fj[2][fj][fi] = F.my; s.Fj[3][fj][fi] = F.E;
+      s.lj[fj][fi] = l;
+    }
+  }
+  __syncthreads();
+
+  // ---- flux divergence and update, one interior cell per thread -------------
+  const int ti = tid % TI, tj = tid / TI;
+  if (ti >= nci_t || tj >= ncj_t) return;
+  const int hi = ti + 2, hj = tj + 2, I = i0 + hi, J = j0 + hj;
+  double xc, yc, A;
+  quad_centroid(s.X[hj][hi], s.Y[hj][hi], s.X[hj][hi + 1], s.Y[hj][hi + 1], s.X[hj + 1][hi + 1],
+                s.Y[hj + 1][hi + 1], s.X[hj + 1][hi], s.Y[hj + 1][hi], xc, yc, A);
+  const double lW = s.li[tj][ti], lE = s.li[tj][ti + 1], lS = s.lj[tj][ti], lN = s.lj[tj + 1][ti];
+  const size_t c = cell_sc(B, b, J, I);
+  double k = 1.0;
+  if (a.mode != 0) k = B.cfl * (B.local_dt ? B.dt[c] : *dtmin_p);
+  double res[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    double d = (a.mode == 2) ? B.dUdt[cell_var(B, b, v, J, I)] : 0.0;
+    if (a.mode != 0) {
+      d += k * s.Fi[v][tj][ti] * lW / A;
+      d -= k * s.Fi[v][tj][ti + 1] * lE / A;
+      d += k * s.Fj[v][tj][ti] * lS / A;
+      d -= k * s.Fj[v][tj + 1][ti] * lN / A;
+    } else {
+      d += s.Fi[v][tj][ti] * lW / A;
+      d -= s.Fi[v][tj][ti + 1] * lE / A;
+      d += s.Fj[v][tj][ti] * lS / A;
+      d -= s.Fj[v][tj + 1][ti] * lN / A;
+    }
+    res[v] = d;
+  }
+  if (a.mode == 0) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, b, v, J, I)] = res[v];
+    return;
+  }
+  // Update_Solution_Multistage_Explicit: U = Uo + omega*dUdt
+  CState<double> uo;
+  if (a.mode == 1) {
+    uo.d = B.U[cell_var(B, b, 0, J, I)]; uo.mx = B.U[cell_var(B, b, 1, J, I)];
+    uo.my = B.U[cell_var(B, b, 2, J, I)]; uo.E = B.U[cell_var(B, b, 3, J, I)];
+    B.Uo[cell_var(B, b, 0, J, I)] = uo.d; B.Uo[cell_var(B, b, 1, J, I)] = uo.mx;
+    B.Uo[cell_var(B, b, 2, J, I)] = uo.my; B.Uo[cell_var(B, b, 3, J, I)] = uo.E;
+  } else {
+    uo.d = B.Uo[cell_var(B, b, 0, J, I)]; uo.mx = B.Uo[cell_var(B, b, 1, J, I)];
+    uo.my = B.Uo[cell_var(B, b, 2, J, I)]; uo.E = B.Uo[cell_var(B, b, 3, J, I)];
+  }
+  const double omega = (B.n_stage == 2 && a.mode == 2) ? HALF * 1.0 : 1.0;
+  CState<double> u;
+  u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
+  u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
+  if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) {
+    if (!B.local_dt) {
+      set_status(B.status, ST_NEGATIVE, int(c));
+    } else {
+      double rrf = 1.0, dtc = B.dt[c];
+      for (int nr = 1; nr <= 10; ++nr) {
+        rrf = HALF * rrf;
+        dtc = rrf * dtc;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) res[v] = rrf * res[v];
+        u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
+        u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
+        if (u.d > 0.0 && u.E > 0.0 && e_of_U(u) > 0.0) break;
+      }
+      B.dt[c] = dtc;
+      if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) set_status(B.status, ST_NEGATIVE, int(c));
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, b, v, J, I)] = res[v];
+  const PState<double> w = W_of_U(u, gm1);
+  B.U[cell_var(B, b, 0, J, I)] = u.d; B.U[cell_var(B, b, 1, J, I)] = u.mx;
+  B.U[cell_var(B, b, 2, J, I)] = u.my; B.U[cell_var(B, b, 3, J, I)] = u.E;
+  B.W[cell_var(B, b, 0, J, I)] = w.d; B.W[cell_var(B, b, 1, J, I)] = w.u;
+  B.W[cell_var(B, b, 2, J, I)] = w.v; B.W[cell_var(B, b, 3, J, I)] = w.p;
+}
+
+}  // namespace E2D_NS
+}  // namespace e2d
+
+namespace e2d {
+namespace E2D_NS {
+size_t stage_smem_bytes() { return sizeof(Smem); }
+cudaError_t launch_stage(const StageArgs& a, cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(sizeof(Smem)));
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const int grid = a.B.nblk * a.tiles_i * a.tiles_j;
+  stage_kernel<<<grid, NTHREADS, sizeof(Smem), st>>>(a);
+  return cudaGetLastError();
+}
+int tile_i() { return TI; }
+int tile_j() { return TJ; }
+}  // namespace E2D_NS
+}  // namespace e2d

@@ -54,8 +54,10 @@ extern "C" {
 #define E2D_FLUX_HLLE 4
 
 /* Precision of reconstruction and flux evaluation. */
-#define E2D_PREC_FP64 0
-#define E2D_PREC_FP32 1 /* FP32 reconstruction + flux, FP64 state/accumulation */
+#define E2D_PREC_FP64 0       /* FP64, FMA contraction allowed                   */
+#define E2D_PREC_FP32 1       /* FP32 reconstruction + flux, FP64 state/update   */
+#define E2D_PREC_FP64_EXACT 2 /* FP64 in the reference's rounding order, no FMA:
+                                 bit-identical to the reference's x86-64 build  */
 
 /* Library error codes (negative returns). */
 #define E2D_ERR_ARG (-1)      /* invalid argument or unsupported option     */
@@ -151,6 +153,18 @@ int e2d_status(e2d_handle *h);
 /* Device pointers of the resident state (for callers that keep data in HBM):
  * W, U, dUdt as [nblk][4][NCj][NCi] doubles. */
 int e2d_device_state(e2d_handle *h, double **W, double **U, double **dUdt);
+
+/* Runs the handle's work on the caller's CUDA stream (a cudaStream_t; NULL
+ * restores the handle's own stream).  No reference counterpart: the
+ * reference is single-threaded host code. */
+int e2d_set_stream(e2d_handle *h, void *stream);
+
+/* Runs n_steps explicit steps launch by launch with CUDA events around each
+ * kernel and returns the mean device time in milliseconds per launch of each
+ * kernel kind: out[0] ghost fill, out[1] RK stage 1, out[2] RK stage 2,
+ * out[3] CFL, out[4] norms (partial + final), out[5] whole step.  The state
+ * advances as with e2d_rk_steps.  Profiling aid; no reference counterpart. */
+int e2d_kernel_times(e2d_handle *h, int n_steps, double out[6]);
 
 #ifdef __cplusplus
 }
