@@ -64,18 +64,39 @@ int check_status(e2d_handle* h) {
   return st[0] ? E2D_ERR_CUDA : 0;
 }
 
+// Stage launch with the double-buffered state (see StageArgs): mode 0 reads
+// (W, U); stage 1 reads (W, U) and writes (W2, U2); stage 2 reads the halo
+// from W2 and U^0 from U and writes (W, U).
 cudaError_t launch_stage_any(e2d_handle* h, int mode) {
   StageArgs a{};
   a.B = h->B;
   a.mode = mode;
   a.hist = h->hist;
   a.step = h->step;
+  a.Win = mode == 2 ? h->B.W2 : h->B.W;
+  a.Ubase = h->B.U;
+  a.Wout = mode == 1 ? h->B.W2 : h->B.W;
+  a.Uout = mode == 1 ? h->B.U2 : h->B.U;
   const bool exact = h->sc.precision == E2D_PREC_FP64_EXACT;
   const int ti = exact ? exact::tile_i() : fast::tile_i();
   const int tj = exact ? exact::tile_j() : fast::tile_j();
   a.tiles_i = (h->B.nci + ti - 1) / ti;
   a.tiles_j = (h->B.ncj + tj - 1) / tj;
-  return exact ? exact::launch_stage(a, h->stream) : fast::launch_stage(a, h->stream);
+  cudaError_t e = exact ? exact::launch_stage(a, h->stream) : fast::launch_stage(a, h->stream);
+  if (e == cudaSuccess && mode == 1 && h->sc.n_stage == 1) {
+    // single-stage scheme: the stage-1 result is the new solution
+    const size_t n = sizeof(double) * 4 * h->ncell;
+    e = cudaMemcpyAsync(h->B.W, h->B.W2, n, cudaMemcpyDeviceToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->B.U, h->B.U2, n, cudaMemcpyDeviceToDevice, h->stream);
+  }
+  return e;
+}
+
+// Ghost fill of the state the given stage reads (stage 2 reads W2, U2).
+cudaError_t ghost_fill_for(e2d_handle* h, int mode) {
+  Blocks B = h->B;
+  if (mode == 2) { B.W = h->B.W2; B.U = h->B.U2; }
+  return launch_ghost_fill(B, h->stream);
 }
 
 int ensure_recon(e2d_handle* h) {
@@ -115,7 +136,7 @@ cudaError_t enqueue_step(e2d_handle* h) {
   if ((e = launch_cfl(h->B, h->hist, h->step, h->stream))) return e;
   if ((e = launch_norms(h->B, h->part, h->hist, h->step, h->stream))) return e;
   for (int stage = 1; stage <= h->sc.n_stage; ++stage) {
-    if ((e = launch_ghost_fill(h->B, h->stream))) return e;
+    if ((e = ghost_fill_for(h, stage))) return e;
     if ((e = launch_stage_any(h, stage))) return e;
   }
   return launch_step_end(h->step, h->stream);
@@ -184,12 +205,14 @@ e2d_handle* e2d_create(const e2d_blocks_desc* d, const e2d_scheme* sc, int devic
   B.neigh = neigh; B.bcw = bcw; B.bce = bce; B.bcs = bcs; B.bcn = bcn;
   B.X = X; B.Y = Y; B.wow = wow; B.woe = woe; B.wos = wos; B.won = won;
   if ((rc = dalloc(h, &B.W, 4 * h->ncell)) || (rc = dalloc(h, &B.U, 4 * h->ncell)) ||
-      (rc = dalloc(h, &B.Uo, 4 * h->ncell)) || (rc = dalloc(h, &B.dUdt, 4 * h->ncell)) ||
+      (rc = dalloc(h, &B.W2, 4 * h->ncell)) || (rc = dalloc(h, &B.U2, 4 * h->ncell)) ||
+      (rc = dalloc(h, &B.dUdt, 4 * h->ncell)) ||
       (rc = dalloc(h, &B.dt, h->ncell)) || (rc = dalloc(h, &B.status, 2)) ||
       (rc = dalloc(h, &h->step, 1)) || (rc = dalloc(h, &h->part, size_t(3) * B.nblk)))
     return fail(rc, h);
   if (cudaMemset(B.W, 0, sizeof(double) * 4 * h->ncell) || cudaMemset(B.U, 0, sizeof(double) * 4 * h->ncell) ||
-      cudaMemset(B.Uo, 0, sizeof(double) * 4 * h->ncell) || cudaMemset(B.dUdt, 0, sizeof(double) * 4 * h->ncell) ||
+      cudaMemset(B.W2, 0, sizeof(double) * 4 * h->ncell) ||
+      cudaMemset(B.U2, 0, sizeof(double) * 4 * h->ncell) || cudaMemset(B.dUdt, 0, sizeof(double) * 4 * h->ncell) ||
       cudaMemset(B.dt, 0, sizeof(double) * h->ncell) || cudaMemset(B.status, 0, sizeof(int) * 2) ||
       cudaMemset(h->step, 0, sizeof(int)))
     return fail(E2D_ERR_CUDA, h);
@@ -358,12 +381,12 @@ int e2d_kernel_times(e2d_handle* h, int n_steps, double out[6]) {
     CK(cudaEventRecord(ev[1], h->stream));
     CK(launch_norms(h->B, h->part, h->hist, h->step, h->stream));
     CK(cudaEventRecord(ev[2], h->stream));
-    CK(launch_ghost_fill(h->B, h->stream));
+    CK(ghost_fill_for(h, 1));
     CK(cudaEventRecord(ev[3], h->stream));
     CK(launch_stage_any(h, 1));
     CK(cudaEventRecord(ev[4], h->stream));
     if (h->sc.n_stage == 2) {
-      CK(launch_ghost_fill(h->B, h->stream));
+      CK(ghost_fill_for(h, 2));
       CK(cudaEventRecord(ev[5], h->stream));
       CK(launch_stage_any(h, 2));
       CK(cudaEventRecord(ev[6], h->stream));

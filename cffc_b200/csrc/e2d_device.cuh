@@ -43,7 +43,8 @@ struct Blocks {
   const int *bcw, *bce, *bcs, *bcn;
   const double *X, *Y;             // nodes
   const double *wow, *woe, *wos, *won;
-  double *W, *U, *Uo, *dUdt;       // cell state
+  double *W, *U, *dUdt;            // cell state (the solution lives in W, U)
+  double *W2, *U2;                 // intermediate RK stage state
   double *dWdx, *dWdy, *phi;       // optional reconstruction output (may be null)
   double* dt;                      // local time step per cell (local dt only)
   int* status;                     // device status word (2 ints: code, cell)
@@ -55,12 +56,21 @@ struct Blocks {
 // 1 = RK stage 1, 2 = RK stage 2.  The global time step of the current
 // explicit step is hist[4 * *step] (the step history lives on the device so
 // that a captured step replays without host involvement).
+//
+// A stage never updates the array it reads its halo from (tiles read their
+// neighbours' cells while those are being updated): stage 1 reads (W, U) and
+// writes (W2, U2); stage 2 reads the halo from W2 and the stage-1 base state
+// U^0 from U, and writes (W, U).  U^0 is the reference's Uo.
 struct StageArgs {
   Blocks B;
   int mode;
   int tiles_i, tiles_j;
   const double* hist;
   const int* step;
+  const double* Win;   // primitive state the residual is evaluated on
+  const double* Ubase; // U^0 of the update U = U^0 + omega * dUdt
+  double* Wout;        // updated state
+  double* Uout;
 };
 
 __host__ __device__ inline size_t cell_var(const Blocks& B, int b, int v, int j, int i) {
@@ -254,19 +264,32 @@ __device__ __forceinline__ T limiter(int kind, const T* uq, T u0, T umin, T umax
   return phi;
 }
 
-// quadCentroid on (SW, SE, NE, NW): area and centroid.
+// quadCentroid on (SW, SE, NE, NW): area and centroid.  The cross products
+// of absolute node coordinates cancel heavily away from the origin (the
+// reference's own reason for its optional local-coordinate mode), so every
+// build evaluates them with explicitly rounded operations: a fused
+// multiply-add here would move centroids by ~1e-11 and the residual by
+// ~1e-8 relative on the benchmark grid.
+__device__ __forceinline__ double rn_cross(double a, double b, double c, double d) {
+  return __dsub_rn(__dmul_rn(a, b), __dmul_rn(c, d));  // a*b - c*d
+}
 __device__ __forceinline__ void quad_centroid(double x0, double y0, double x1, double y1,
                                               double x2, double y2, double x3, double y3,
                                               double& xc, double& yc, double& area) {
   double ai, atmp = 0, xt = 0, yt = 0;
-  ai = x3 * y0 - x0 * y3; atmp += ai; xt += (x0 + x3) * ai; yt += (y0 + y3) * ai;
-  ai = x0 * y1 - x1 * y0; atmp += ai; xt += (x1 + x0) * ai; yt += (y1 + y0) * ai;
-  ai = x1 * y2 - x2 * y1; atmp += ai; xt += (x2 + x1) * ai; yt += (y2 + y1) * ai;
-  ai = x2 * y3 - x3 * y2; atmp += ai; xt += (x3 + x2) * ai; yt += (y3 + y2) * ai;
-  area = 0.5 * atmp;
+  ai = rn_cross(x3, y0, x0, y3); atmp = __dadd_rn(atmp, ai);
+  xt = __dadd_rn(xt, __dmul_rn(__dadd_rn(x0, x3), ai)); yt = __dadd_rn(yt, __dmul_rn(__dadd_rn(y0, y3), ai));
+  ai = rn_cross(x0, y1, x1, y0); atmp = __dadd_rn(atmp, ai);
+  xt = __dadd_rn(xt, __dmul_rn(__dadd_rn(x1, x0), ai)); yt = __dadd_rn(yt, __dmul_rn(__dadd_rn(y1, y0), ai));
+  ai = rn_cross(x1, y2, x2, y1); atmp = __dadd_rn(atmp, ai);
+  xt = __dadd_rn(xt, __dmul_rn(__dadd_rn(x2, x1), ai)); yt = __dadd_rn(yt, __dmul_rn(__dadd_rn(y2, y1), ai));
+  ai = rn_cross(x2, y3, x3, y2); atmp = __dadd_rn(atmp, ai);
+  xt = __dadd_rn(xt, __dmul_rn(__dadd_rn(x3, x2), ai)); yt = __dadd_rn(yt, __dmul_rn(__dadd_rn(y3, y2), ai));
+  area = __dmul_rn(0.5, atmp);
   if (atmp != 0) {
-    xc = xt / (3 * atmp);
-    yc = yt / (3 * atmp);
+    const double a3 = __dmul_rn(3.0, atmp);
+    xc = xt / a3;
+    yc = yt / a3;
   } else {
     xc = 0; yc = 0;
   }

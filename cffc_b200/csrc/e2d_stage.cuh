@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
   for (int q = tid; q < 4 * HJ * HI; q += NTHREADS) {
     const int v = q / (HJ * HI), r = q % (HJ * HI), hj = r / HI, hi = r % HI;
     const int I = i0 + hi, J = j0 + hj;
-    s.W[v][hj][hi] = (I < B.NCi && J < B.NCj) ? B.W[cell_var(B, b, v, J, I)] : 0.0;
+    s.W[v][hj][hi] = (I < B.NCi && J < B.NCj) ? a.Win[cell_var(B, b, v, J, I)] : 0.0;
   }
   for (int q = tid; q < NJ * NI; q += NTHREADS) {
     const int nj = q / NI, ni = q % NI, I = i0 + ni, J = j0 + nj;
@@ -384,15 +384,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
   }
   // Update_Solution_Multistage_Explicit: U = Uo + omega*dUdt
   CState<double> uo;
-  if (a.mode == 1) {
-    uo.d = B.U[cell_var(B, b, 0, J, I)]; uo.mx = B.U[cell_var(B, b, 1, J, I)];
-    uo.my = B.U[cell_var(B, b, 2, J, I)]; uo.E = B.U[cell_var(B, b, 3, J, I)];
-    B.Uo[cell_var(B, b, 0, J, I)] = uo.d; B.Uo[cell_var(B, b, 1, J, I)] = uo.mx;
-    B.Uo[cell_var(B, b, 2, J, I)] = uo.my; B.Uo[cell_var(B, b, 3, J, I)] = uo.E;
-  } else {
-    uo.d = B.Uo[cell_var(B, b, 0, J, I)]; uo.mx = B.Uo[cell_var(B, b, 1, J, I)];
-    uo.my = B.Uo[cell_var(B, b, 2, J, I)]; uo.E = B.Uo[cell_var(B, b, 3, J, I)];
-  }
+  uo.d = a.Ubase[cell_var(B, b, 0, J, I)]; uo.mx = a.Ubase[cell_var(B, b, 1, J, I)];
+  uo.my = a.Ubase[cell_var(B, b, 2, J, I)]; uo.E = a.Ubase[cell_var(B, b, 3, J, I)];
   const double omega = (B.n_stage == 2 && a.mode == 2) ? HALF * 1.0 : 1.0;
   CState<double> u;
   u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
@@ -418,10 +411,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
 #pragma unroll
   for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, b, v, J, I)] = res[v];
   const PState<double> w = W_of_U(u, gm1);
-  B.U[cell_var(B, b, 0, J, I)] = u.d; B.U[cell_var(B, b, 1, J, I)] = u.mx;
-  B.U[cell_var(B, b, 2, J, I)] = u.my; B.U[cell_var(B, b, 3, J, I)] = u.E;
-  B.W[cell_var(B, b, 0, J, I)] = w.d; B.W[cell_var(B, b, 1, J, I)] = w.u;
-  B.W[cell_var(B, b, 2, J, I)] = w.v; B.W[cell_var(B, b, 3, J, I)] = w.p;
+  a.Uout[cell_var(B, b, 0, J, I)] = u.d; a.Uout[cell_var(B, b, 1, J, I)] = u.mx;
+  a.Uout[cell_var(B, b, 2, J, I)] = u.my; a.Uout[cell_var(B, b, 3, J, I)] = u.E;
+  a.Wout[cell_var(B, b, 0, J, I)] = w.d; a.Wout[cell_var(B, b, 1, J, I)] = w.u;
+  a.Wout[cell_var(B, b, 2, J, I)] = w.v; a.Wout[cell_var(B, b, 3, J, I)] = w.p;
 }
 
 }  // namespace E2D_NS
