@@ -24,6 +24,7 @@ SOURCES = {
     "e2d_exact.cu": ["-fmad=false"],
     "e2d_fast.cu": ["-fmad=true"],
     "e2d_capi.cu": ["-fmad=false"],
+    "e2d_noalloc.cu": ["-fmad=false"],
 }
 HEADERS = ["e2d_device.cuh", "e2d_stage.cuh", "e2d_aux.cuh", "e2d_launch.h",
            os.path.join("..", "..", "include", "cffc_e2d.h")]

@@ -166,6 +166,29 @@ int e2d_set_stream(e2d_handle *h, void *stream);
  * advances as with e2d_rk_steps.  Profiling aid; no reference counterpart. */
 int e2d_kernel_times(e2d_handle *h, int n_steps, double out[6]);
 
+/* Largest block count e2d_residual_norms_static serves. */
+#define E2D_NORMS_STATIC_MAX_BLOCKS 4096
+
+/* L1, L2 and max norms of the density residual of a caller-owned device
+ * array, computed without allocating any device memory.  No counterpart in
+ * the reference: it is for callers that cannot allocate when they need the
+ * norms (allocation may stall or synchronise the device mid-loop, their
+ * process's allocator owns all device memory, or they forbid allocation
+ * after start-up).  Same result as e2d_norms, within reduction-order
+ * rounding.
+ *   dUdt    device pointer, [nblk][4][NCj][NCi] with two ghost layers
+ *           (NCi = nci + 4, NCj = ncj + 4); only interior density is read
+ *   out     device pointer to 3 doubles: L1, L2, Max
+ *   stream  cudaStream_t to run on (NULL: the default stream)
+ * The scratch is a fixed device array of 3 * E2D_NORMS_STATIC_MAX_BLOCKS
+ * doubles (96 KiB), held on every GPU that loads the library until exit;
+ * nblk above E2D_NORMS_STATIC_MAX_BLOCKS is rejected with E2D_ERR_ARG.
+ * The first call on a device looks up the array's device address (with that
+ * device current); make that first call before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race. */
+int e2d_residual_norms_static(const double *dUdt, int32_t nblk, int32_t nci, int32_t ncj,
+                              double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
