@@ -279,7 +279,9 @@ def main():
 
     line = None
     if rank == 0:
-        launches_per_rk = 4 + 2 * bs.scheme.n_stage + 1
+        # per time step: slot init, (ghost fill + stage) per stage, step end;
+        # per e2d_rk_steps call: slot init, CFL, two norm kernels
+        launches_per_rk = 2 + 2 * bs.scheme.n_stage
         line = {
             "metric": "Mcell-updates/s (Roe+limiter residual, explicit RK2)",
             "value": round(value, 3), "unit": "Mcell-updates/s", "n_gpus": world,
@@ -299,7 +301,7 @@ def main():
             "path_roofline": {"bytes_per_cell_update": 240,
                               "achieved_gbs": round(240 * cell_updates / (ms * 1e-3) / 1e9, 2),
                               "frac": round(240 * cell_updates / (ms * 1e-3) / 1e9 / hbm, 4)},
-            "gpu_launches": args.steps * args.rk_steps * launches_per_rk,
+            "gpu_launches": args.steps * (args.rk_steps * launches_per_rk + 4),
             "clocks": clk.summary(),
         }
         if world == 1 and not args.no_cpu_baseline:

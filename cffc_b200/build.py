@@ -27,7 +27,7 @@ SOURCES = {
     "e2d_noalloc.cu": ["-fmad=false"],
 }
 HEADERS = ["e2d_device.cuh", "e2d_stage.cuh", "e2d_aux.cuh", "e2d_launch.h",
-           os.path.join("..", "..", "include", "cffc_e2d.h")]
+           "e2d_fastmath.cuh", os.path.join("..", "..", "include", "cffc_e2d.h")]
 
 
 def _newer(target, deps):

@@ -170,7 +170,10 @@ __device__ void bc_horizontal(const Blocks& B, int b, int i, int side) {
 __global__ void __launch_bounds__(AUX_THREADS) ghost_fill_kernel(Blocks B) {
   const int b = blockIdx.x;
   const int ICl = NG, ICu = B.nci + NG - 1, JCl = NG, JCu = B.ncj + NG - 1;
-  if (B.status[0] != 0) return;
+  __shared__ int failed;
+  if (threadIdx.x == 0) failed = *(volatile int*)B.status;
+  __syncthreads();
+  if (failed) return;  // uniform per CTA
   // exchange: edges (2 layers) and corners (2x2) from the 8 neighbours
   const int ne = NG * B.ncj, nn = NG * B.nci, nc = NG * NG;
   const int total = 2 * ne + 2 * nn + 4 * nc;
@@ -295,18 +298,26 @@ __global__ void __launch_bounds__(AUX_THREADS) norm_partial_kernel(Blocks B, dou
 
 // Combines the per-block partials in block order as the multi-block norms
 // and the solver loop do; out = (L1, L2, Max).
+// One warp: lane l sums blocks l, l+32, ...; the lanes are then combined.
 __global__ void norm_final_kernel(int nblk, const double* part, double* hist, const int* step) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double* out = hist + 4 * (*step) + 1;
+  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
   double l1 = 0, l2 = 0, mx = 0;
-  for (int b = 0; b < nblk; ++b) {
+  for (int b = threadIdx.x; b < nblk; b += 32) {
     l1 += part[3 * b];
     l2 += sqr(sqrt(part[3 * b + 1]));
     mx = dmax(mx, part[3 * b + 2]);
   }
-  out[0] = l1;
-  out[1] = sqrt(sqr(sqrt(l2)));
-  out[2] = mx;
+  for (int o = 16; o > 0; o >>= 1) {
+    l1 += __shfl_xor_sync(0xffffffffu, l1, o);
+    l2 += __shfl_xor_sync(0xffffffffu, l2, o);
+    mx = dmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if (threadIdx.x == 0) {
+    double* out = hist + 4 * (*step) + 1;
+    out[0] = l1;
+    out[1] = sqrt(sqr(sqrt(l2)));
+    out[2] = mx;
+  }
 }
 
 __global__ void fill_kernel(double* p, long long n, double v) {
@@ -316,8 +327,19 @@ __global__ void fill_kernel(double* p, long long n, double v) {
 
 // Explicit-step bookkeeping: the step index lives on the device so that one
 // captured step graph replays for every step.
-__global__ void step_begin_kernel(double* hist, const int* step) { hist[4 * (*step)] = MILLION; }
-__global__ void step_end_kernel(int* step) { *step += 1; }
+// Slot of step *step + offset: dt = MILLION (min-reduced), norms = 0 (summed).
+__global__ void slot_init_kernel(double* hist, const int* step, int offset) {
+  double* h = hist + 4 * (*step + offset);
+  h[0] = MILLION; h[1] = 0.0; h[2] = 0.0; h[3] = 0.0;
+}
+// End of a step: the fused epilogue summed r^2 into the next slot's L2 entry.
+__global__ void step_end_kernel(double* hist, int* step, int fused) {
+  if (fused) {
+    double* h = hist + 4 * (*step + 1);
+    h[2] = sqrt(h[2]);
+  }
+  *step += 1;
+}
 
 cudaError_t launch_ghost_fill(const Blocks& B, cudaStream_t st) {
   ghost_fill_kernel<<<B.nblk, AUX_THREADS, 0, st>>>(B);
@@ -338,12 +360,12 @@ cudaError_t launch_norms(const Blocks& B, double* part, double* hist, const int*
   return cudaGetLastError();
 }
 
-cudaError_t launch_step_begin(double* hist, int* step, cudaStream_t st) {
-  step_begin_kernel<<<1, 1, 0, st>>>(hist, step);
+cudaError_t launch_slot_init(double* hist, const int* step, int offset, cudaStream_t st) {
+  slot_init_kernel<<<1, 1, 0, st>>>(hist, step, offset);
   return cudaGetLastError();
 }
-cudaError_t launch_step_end(int* step, cudaStream_t st) {
-  step_end_kernel<<<1, 1, 0, st>>>(step);
+cudaError_t launch_step_end(double* hist, int* step, int fused, cudaStream_t st) {
+  step_end_kernel<<<1, 1, 0, st>>>(hist, step, fused);
   return cudaGetLastError();
 }
 cudaError_t launch_fill(double* p, long long n, double v, cudaStream_t st) {

@@ -67,10 +67,11 @@ int check_status(e2d_handle* h) {
 // Stage launch with the double-buffered state (see StageArgs): mode 0 reads
 // (W, U); stage 1 reads (W, U) and writes (W2, U2); stage 2 reads the halo
 // from W2 and U^0 from U and writes (W, U).
-cudaError_t launch_stage_any(e2d_handle* h, int mode) {
+cudaError_t launch_stage_any(e2d_handle* h, int mode, int fuse_next = 0) {
   StageArgs a{};
   a.B = h->B;
   a.mode = mode;
+  a.fuse_next = fuse_next;
   a.hist = h->hist;
   a.step = h->step;
   a.Win = mode == 2 ? h->B.W2 : h->B.W;
@@ -129,17 +130,28 @@ int ensure_hist(e2d_handle* h, int n) {
   return 0;
 }
 
-// One explicit time step in the reference's order (Euler2DQuadSolvers.cc:657-898).
+// CFL + global minimum and the residual norms of the current state into the
+// current step's history slot: the head of the reference's explicit step
+// (Euler2DQuadSolvers.cc:657-696).  Needed before the first step only; every
+// step's last stage computes them for the following step.
+cudaError_t enqueue_step_head(e2d_handle* h) {
+  cudaError_t e;
+  if ((e = launch_slot_init(h->hist, h->step, 0, h->stream))) return e;
+  if ((e = launch_cfl(h->B, h->hist, h->step, h->stream))) return e;
+  return launch_norms(h->B, h->part, h->hist, h->step, h->stream);
+}
+
+// One explicit time step in the reference's order (Euler2DQuadSolvers.cc:657-898):
+// per stage ghost fill + fused residual/update; the last stage also reduces
+// the next step's CFL minimum and residual norms.
 cudaError_t enqueue_step(e2d_handle* h) {
   cudaError_t e;
-  if ((e = launch_step_begin(h->hist, h->step, h->stream))) return e;
-  if ((e = launch_cfl(h->B, h->hist, h->step, h->stream))) return e;
-  if ((e = launch_norms(h->B, h->part, h->hist, h->step, h->stream))) return e;
+  if ((e = launch_slot_init(h->hist, h->step, 1, h->stream))) return e;
   for (int stage = 1; stage <= h->sc.n_stage; ++stage) {
     if ((e = ghost_fill_for(h, stage))) return e;
-    if ((e = launch_stage_any(h, stage))) return e;
+    if ((e = launch_stage_any(h, stage, stage == h->sc.n_stage))) return e;
   }
-  return launch_step_end(h->step, h->stream);
+  return launch_step_end(h->hist, h->step, 1, h->stream);
 }
 
 }  // namespace
@@ -300,12 +312,13 @@ int e2d_rk_steps(e2d_handle* h, int n_steps, double* hist) {
   if (!h || n_steps < 0) return E2D_ERR_ARG;
   if (n_steps == 0) return 0;
   CK(cudaSetDevice(h->device));
-  int rc = ensure_hist(h, n_steps);
+  int rc = ensure_hist(h, n_steps + 1);  // the last step fills slot n_steps
   if (rc) return rc;
   // the stage kernels do not write the optional reconstruction arrays
   const Blocks saved = h->B;
   h->B.dWdx = h->B.dWdy = h->B.phi = nullptr;
   CK(cudaMemsetAsync(h->step, 0, sizeof(int), h->stream));
+  CK(enqueue_step_head(h));
   if (!h->step_graph) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -366,7 +379,7 @@ int e2d_set_stream(e2d_handle* h, void* stream) {
 int e2d_kernel_times(e2d_handle* h, int n_steps, double out[6]) {
   if (!h || !out || n_steps < 1) return E2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
-  int rc = ensure_hist(h, n_steps);
+  int rc = ensure_hist(h, n_steps + 1);
   if (rc) return rc;
   const Blocks saved = h->B;
   h->B.dWdx = h->B.dWdy = h->B.phi = nullptr;
@@ -375,23 +388,26 @@ int e2d_kernel_times(e2d_handle* h, int n_steps, double out[6]) {
   double acc[6] = {0, 0, 0, 0, 0, 0};
   CK(cudaMemsetAsync(h->step, 0, sizeof(int), h->stream));
   for (int s = 0; s < n_steps; ++s) {
+    // the standalone CFL and norm kernels run before the first step only in
+    // e2d_rk_steps; they are timed on every step here for the record
     CK(cudaEventRecord(ev[0], h->stream));
-    CK(launch_step_begin(h->hist, h->step, h->stream));
+    CK(launch_slot_init(h->hist, h->step, 0, h->stream));
     CK(launch_cfl(h->B, h->hist, h->step, h->stream));
     CK(cudaEventRecord(ev[1], h->stream));
     CK(launch_norms(h->B, h->part, h->hist, h->step, h->stream));
     CK(cudaEventRecord(ev[2], h->stream));
+    CK(launch_slot_init(h->hist, h->step, 1, h->stream));
     CK(ghost_fill_for(h, 1));
     CK(cudaEventRecord(ev[3], h->stream));
-    CK(launch_stage_any(h, 1));
+    CK(launch_stage_any(h, 1, h->sc.n_stage == 1));
     CK(cudaEventRecord(ev[4], h->stream));
     if (h->sc.n_stage == 2) {
       CK(ghost_fill_for(h, 2));
       CK(cudaEventRecord(ev[5], h->stream));
-      CK(launch_stage_any(h, 2));
+      CK(launch_stage_any(h, 2, 1));
       CK(cudaEventRecord(ev[6], h->stream));
     }
-    CK(launch_step_end(h->step, h->stream));
+    CK(launch_step_end(h->hist, h->step, 1, h->stream));
     CK(cudaEventRecord(ev[7], h->stream));
     CK(cudaEventSynchronize(ev[7]));
     float t[8] = {0};

@@ -71,6 +71,8 @@ struct StageArgs {
   const double* Ubase; // U^0 of the update U = U^0 + omega * dUdt
   double* Wout;        // updated state
   double* Uout;
+  int fuse_next;       // last stage of a step: also accumulate the next step's
+                       // CFL minimum and residual norms into hist[4*(*step+1)..]
 };
 
 __host__ __device__ inline size_t cell_var(const Blocks& B, int b, int v, int j, int i) {
@@ -272,6 +274,20 @@ __device__ __forceinline__ T limiter(int kind, const T* uq, T u0, T umin, T umax
 // ~1e-8 relative on the benchmark grid.
 __device__ __forceinline__ double rn_cross(double a, double b, double c, double d) {
   return __dsub_rn(__dmul_rn(a, b), __dmul_rn(c, d));  // a*b - c*d
+}
+__device__ __forceinline__ void quad_moments(double x0, double y0, double x1, double y1,
+                                             double x2, double y2, double x3, double y3,
+                                             double& atmp, double& xt, double& yt) {
+  double ai;
+  atmp = 0; xt = 0; yt = 0;
+  ai = rn_cross(x3, y0, x0, y3); atmp = __dadd_rn(atmp, ai);
+  xt = __dadd_rn(xt, __dmul_rn(__dadd_rn(x0, x3), ai)); yt = __dadd_rn(yt, __dmul_rn(__dadd_rn(y0, y3), ai));
+  ai = rn_cross(x0, y1, x1, y0); atmp = __dadd_rn(atmp, ai);
+  xt = __dadd_rn(xt, __dmul_rn(__dadd_rn(x1, x0), ai)); yt = __dadd_rn(yt, __dmul_rn(__dadd_rn(y1, y0), ai));
+  ai = rn_cross(x1, y2, x2, y1); atmp = __dadd_rn(atmp, ai);
+  xt = __dadd_rn(xt, __dmul_rn(__dadd_rn(x2, x1), ai)); yt = __dadd_rn(yt, __dmul_rn(__dadd_rn(y2, y1), ai));
+  ai = rn_cross(x2, y3, x3, y2); atmp = __dadd_rn(atmp, ai);
+  xt = __dadd_rn(xt, __dmul_rn(__dadd_rn(x3, x2), ai)); yt = __dadd_rn(yt, __dmul_rn(__dadd_rn(y3, y2), ai));
 }
 __device__ __forceinline__ void quad_centroid(double x0, double y0, double x1, double y1,
                                               double x2, double y2, double x3, double y3,

@@ -1,0 +1,190 @@
+// e2d_fastmath.cuh — the fast FP64 path's arithmetic: reciprocal and
+// reciprocal square root by Newton–Raphson refinement of the PTX approximate
+// instructions, and division-lean restatements of the Roe flux, the
+// least-squares gradient and the limiters.
+//
+// Refinement (Newton–Raphson on f(r) = 1/r - x and f(r) = 1/r^2 - x; each step
+// squares the relative error): starting from rcp.approx / rsqrt.approx
+// (relative error below 2^-22), two steps reach the double-precision
+// rounding level.  tests/test_gpu_fastmath.py bounds the error against IEEE
+// division and square root.
+//
+// The algebra keeps the reference's quantities but removes divisions:
+//   c^2 = g p / d,  h = c^2/(g-1) + |v|^2/2,  u H = d u h,
+//   Roe average: a_a^2 = (g-1)(h_a - |v_a|^2/2), and g p_a / d_a = a_a^2, so
+//   lp_x(1|4) = (0, -+d_a/(2 a_a), 0, 1/(2 a_a^2)),  lp_x(2) = (1, 0, 0, -1/a_a^2),
+//   rc_x(1|4) = (1, u_a -+ a_a, v_a, h_a -+ u_a a_a)  (h of the Roe state is h_a);
+//   least-squares: the 1/n averaging cancels in the gradient;
+//   limiters: phi(y) with y = a/b is compared as the fraction
+//   (a^2 + 2ab)/(a^2 + ab + 2b^2) (Venkatakrishnan) or min(|a|,|b|)/|b|
+//   (Barth–Jespersen), the minimum over the face points taken by
+//   cross-multiplication, and one division at the end.
+#pragma once
+#include "e2d_device.cuh"
+
+namespace e2d {
+namespace fm {
+
+__device__ __forceinline__ double rcp_approx(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  return r;
+}
+__device__ __forceinline__ double rsqrt_approx(double x) {
+  double r;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  return r;
+}
+// 1/x for normal, non-zero x.
+__device__ __forceinline__ double rcp(double x) {
+  double r = rcp_approx(x);
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
+// 1/sqrt(x) for normal x > 0.
+__device__ __forceinline__ double rsqrt(double x) {
+  double r = rsqrt_approx(x);
+  const double h = 0.5 * x;
+  double e = fma(-h * r, r, 0.5);
+  r = fma(r, e, r);
+  e = fma(-h * r, r, 0.5);
+  return fma(r, e, r);
+}
+// sqrt(x) = x / sqrt(x) with one Newton correction; x > 0.
+__device__ __forceinline__ double sqrt_from_rsqrt(double x, double r) {
+  const double s = x * r;
+  const double d = fma(-s, s, x);
+  return fma(0.5 * r, d, s);
+}
+
+__device__ __forceinline__ double harten_delta(double la, double ll, double lr) {
+  double delta = dmax(0.0, 2.0 * (lr - ll));
+  if (fabs(la) > delta || delta < TOLER) return 0.0;
+  return 0.5 * (la * la * rcp(delta) + delta) - fabs(la);
+}
+
+// FluxRoe_n in the frame of the unit normal (c, s), division-lean form.
+__device__ __forceinline__ CState<double> flux_roe_n(const PState<double>& wl0, const PState<double>& wr0,
+                                                     double c, double s, double g, double gm1,
+                                                     double gm1i) {
+  const double dl = wl0.d, pl = wl0.p, dr = wr0.d, pr = wr0.p;
+  const double ul = wl0.u * c + wl0.v * s, vl = -wl0.u * s + wl0.v * c;
+  const double ur = wr0.u * c + wr0.v * s, vr = -wr0.u * s + wr0.v * c;
+  const double rsdl = rsqrt(dl), rsdr = rsqrt(dr);
+  const double sdl = sqrt_from_rsqrt(dl, rsdl), sdr = sqrt_from_rsqrt(dr, rsdr);
+  const double cl2 = g * pl * (rsdl * rsdl), cr2 = g * pr * (rsdr * rsdr);
+  const double cl = sqrt_from_rsqrt(cl2, rsqrt(cl2)), cr = sqrt_from_rsqrt(cr2, rsqrt(cr2));
+  const double hl = cl2 * gm1i + 0.5 * (ul * ul + vl * vl);
+  const double hr = cr2 * gm1i + 0.5 * (ur * ur + vr * vr);
+  const double inv = rcp(sdl + sdr);
+  const double ua = (sdl * ul + sdr * ur) * inv;
+  const double va = (sdl * vl + sdr * vr) * inv;
+  const double ha = (sdl * hl + sdr * hr) * inv;
+  const double qa2 = ua * ua + va * va;
+  const double aa2 = gm1 * (ha - 0.5 * qa2);
+  const double rca = rsqrt(aa2);
+  const double ca = sqrt_from_rsqrt(aa2, rca);
+  const double da = sdl * sdr;
+  const double dW0 = dr - dl, dW1 = ur - ul, dW2 = vr - vl, dW3 = pr - pl;
+  const bool up = ua >= 0.0;
+  const double d = up ? dl : dr, u = up ? ul : ur, v = up ? vl : vr, p = up ? pl : pr;
+  const double h = up ? hl : hr;
+  const double du = d * u;
+  double F0 = du, F1 = du * u + p, F2 = du * v, F3 = du * h;
+  const double la0 = ua - ca, la3 = ua + ca;
+  const double d0 = harten_delta(la0, ul - cl, ur - cr);
+  const double d3 = harten_delta(la3, ul + cl, ur + cr);
+  double ws0, ws1, ws3;
+  if (up) {
+    ws0 = 0.5 * (la0 - fabs(la0) - d0);
+    ws1 = 0.5 * (ua - fabs(ua));
+    ws3 = 0.5 * (la3 - fabs(la3) - d3);
+  } else {
+    ws0 = 0.5 * (la0 + fabs(la0) + d0);
+    ws1 = 0.5 * (ua + fabs(ua));
+    ws3 = 0.5 * (la3 + fabs(la3) + d3);
+  }
+  const double sg = up ? 1.0 : -1.0;
+  const double rca2 = rca * rca;
+  const double hdr = 0.5 * da * rca * dW1, pdr = 0.5 * rca2 * dW3;
+  // Each wave contributes only where the reference's upwind test selects it;
+  // a wave speed of exactly zero contributes nothing either way.
+  const bool on0 = up ? (ws0 < 0.0) : (ws0 > 0.0);
+  const bool on1 = up ? (ws1 < 0.0) : (ws1 > 0.0);
+  const bool on3 = up ? (ws3 < 0.0) : (ws3 > 0.0);
+  if (on0) {
+    const double k = sg * ws0 * (pdr - hdr);
+    F0 += k; F1 += k * (ua - ca); F2 += k * va; F3 += k * (ha - ua * ca);
+  }
+  if (on1) {
+    const double k1 = sg * ws1 * (dW0 - rca2 * dW3);
+    F0 += k1; F1 += k1 * ua; F2 += k1 * va; F3 += k1 * (0.5 * qa2);
+    const double k2 = sg * ws1 * dW2;
+    F2 += k2 * da; F3 += k2 * (da * va);
+  }
+  if (on3) {
+    const double k = sg * ws3 * (pdr + hdr);
+    F0 += k; F1 += k * (ua + ca); F2 += k * va; F3 += k * (ha + ua * ca);
+  }
+  CState<double> R;
+  R.d = F0;
+  R.mx = F1 * c - F2 * s;
+  R.my = F1 * s + F2 * c;
+  R.E = F3;
+  return R;
+}
+
+// Limiter over the 4 face points, one division.
+__device__ __forceinline__ double limiter(int kind, const double* uq, double u0, double umin, double umax) {
+  if (kind == E2D_LIMITER_ONE) return 1.0;
+  if (kind == E2D_LIMITER_ZERO) return 0.0;
+  double bn = 1.0, bd = 1.0;  // best fraction bn/bd, starts at phi = 1
+  const bool venk = kind == E2D_LIMITER_VENKATAKRISHNAN;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const double b = uq[q] - u0;
+    if (b > TOLER || b < -TOLER) {
+      const double a = (b > 0.0 ? umax : umin) - u0;  // y = a / b >= 0
+      double n, dd;
+      if (venk) {
+        n = a * a + 2.0 * a * b;
+        dd = a * a + a * b + 2.0 * b * b;
+      } else {
+        const double aa = fabs(a), ab = fabs(b);
+        n = aa < ab ? aa : ab;  // min(1, y) = min(|a|, |b|) / |b|
+        dd = ab;
+      }
+      if (n * bd < bn * dd) { bn = n; bd = dd; }
+    }
+  }
+  return bn == bd ? 1.0 : bn * rcp(bd);
+}
+
+// quadCentroid with the reference-rounded moments and one reciprocal.
+__device__ __forceinline__ void quad_centroid(double x0, double y0, double x1, double y1,
+                                              double x2, double y2, double x3, double y3,
+                                              double& xc, double& yc, double& area) {
+  double atmp, xt, yt;
+  quad_moments(x0, y0, x1, y1, x2, y2, x3, y3, atmp, xt, yt);
+  area = 0.5 * atmp;
+  if (atmp != 0) {
+    const double r = rcp(3.0 * atmp);
+    xc = xt * r;
+    yc = yt * r;
+  } else {
+    xc = 0; yc = 0;
+  }
+}
+
+__device__ __forceinline__ PState<double> W_of_U(const CState<double>& u, double gm1) {
+  const double rd = rcp(u.d);
+  PState<double> w;
+  w.d = u.d; w.u = u.mx * rd; w.v = u.my * rd;
+  w.p = gm1 * (u.E - 0.5 * (u.mx * u.mx + u.my * u.my) * rd);
+  return w;
+}
+
+}  // namespace fm
+}  // namespace e2d

@@ -25,6 +25,19 @@
 #error "E2D_NS must name the kernel namespace"
 #endif
 
+// The fast path (E2D_FAST) replaces IEEE division and square root by the
+// Newton-refined reciprocal / reciprocal square root of e2d_fastmath.cuh and
+// uses the division-lean flux, gradient and limiter forms; it is tuned for
+// two CTAs per SM.
+#ifdef E2D_FAST
+#include "e2d_fastmath.cuh"
+#define E2D_MIN_CTAS 2
+#define E2D_QC fm::quad_centroid
+#else
+#define E2D_MIN_CTAS 1
+#define E2D_QC quad_centroid
+#endif
+
 namespace e2d {
 namespace E2D_NS {
 
@@ -53,16 +66,27 @@ __device__ __forceinline__ void edge_normal(double ax, double ay, double cx, dou
                                             double perim, double& nx, double& ny) {
   if (l > NANO * perim) {
     const double dx = ax - cx, dy = ay - cy;
+#ifdef E2D_FAST
+    const double rn = fm::rsqrt(dx * dx + dy * dy);
+    nx = dy * rn;
+    ny = -dx * rn;
+#else
     const double n = sqrt(dx * dx + dy * dy);
     nx = (ay - cy) / n;
     ny = -(ax - cx) / n;
+#endif
   } else {
     nx = 1.0; ny = 0.0;
   }
 }
 __device__ __forceinline__ double edge_len(double ax, double ay, double cx, double cy) {
   const double dx = ax - cx, dy = ay - cy;
+#ifdef E2D_FAST
+  const double q = dx * dx + dy * dy;
+  return fm::sqrt_from_rsqrt(q, fm::rsqrt(q));
+#else
   return sqrt(dx * dx + dy * dy);
+#endif
 }
 
 // Perimeter of halo cell (hi, hj) in the reference's order lE + lN + lW + lS.
@@ -87,7 +111,9 @@ __device__ __forceinline__ double perim_for_test(const Smem& s, int hi, int hj, 
 }
 
 // Least-squares stencil (Euler2DQuadSingleBlock.cc:3692-3990) of array cell
-// (I, J).  Writes offsets (di, dj) relative to the cell; returns n_pts.
+// (I, J).  Writes offsets (di, dj) relative to the cell in the reference's
+// order; returns n_pts.  (Measured: this indexed form runs ~11% faster on
+// B200 than an unrolled bit-mask form of the same stencils.)
 __device__ __forceinline__ int lsq_stencil(const Blocks& B, int b, int I, int J, int* di, int* dj) {
   const int ICl = NG, ICu = B.nci + NG - 1, JCl = NG, JCu = B.ncj + NG - 1;
   int n = 0;
@@ -165,6 +191,35 @@ __device__ __forceinline__ PState<double> face_state(const Smem& s, int hi, int 
   return w;
 }
 
+constexpr double MILLION_D = 1000000.0;
+
+// CFL time step of halo cell (hi, hj) (Euler2DQuadSingleBlock.cc:3038-3048):
+// dt = min(d_i / (a + |v_i|), d_j / (a + |v_j|)), d = 2A / (l + l'),
+// v_i = v.(n_E - n_W)/2, v_j = v.(n_N - n_S)/2, normals with the cell's own
+// degenerate-edge test.
+__device__ __forceinline__ double cell_dt(const Smem& s, int hi, int hj, double A, double lE, double lW,
+                                          double lN, double lS, const PState<double>& w, double g) {
+  const double per = lE + lN + lW + lS;
+  double nEx, nEy, nWx, nWy, nNx, nNy, nSx, nSy;
+  edge_normal(s.X[hj + 1][hi + 1], s.Y[hj + 1][hi + 1], s.X[hj][hi + 1], s.Y[hj][hi + 1], lE, per, nEx, nEy);
+  edge_normal(s.X[hj][hi], s.Y[hj][hi], s.X[hj + 1][hi], s.Y[hj + 1][hi], lW, per, nWx, nWy);
+  edge_normal(s.X[hj + 1][hi], s.Y[hj + 1][hi], s.X[hj + 1][hi + 1], s.Y[hj + 1][hi + 1], lN, per, nNx, nNy);
+  edge_normal(s.X[hj][hi + 1], s.Y[hj][hi + 1], s.X[hj][hi], s.Y[hj][hi], lS, per, nSx, nSy);
+  const double v_i = HALF * (w.u * (nEx - nWx) + w.v * (nEy - nWy));
+  const double v_j = HALF * (w.u * (nNx - nSx) + w.v * (nNy - nSy));
+#ifdef E2D_FAST
+  const double c2 = g * w.p * fm::rcp(w.d);
+  const double a = fm::sqrt_from_rsqrt(c2, fm::rsqrt(c2));
+  const double d_i = 2.0 * A * fm::rcp(lE + lW), d_j = 2.0 * A * fm::rcp(lN + lS);
+  const double ti = d_i * fm::rcp(a + fabs(v_i)), tj = d_j * fm::rcp(a + fabs(v_j));
+#else
+  const double a = a_of(w, g);
+  const double d_i = 2.0 * (A / (lE + lW)), d_j = 2.0 * (A / (lN + lS));
+  const double ti = d_i / (a + fabs(v_i)), tj = d_j / (a + fabs(v_j));
+#endif
+  return dmin(ti, tj);
+}
+
 __device__ __forceinline__ PState<double> load_wo(const double* wo, int b, int len, int k) {
   const double* p = wo + size_t(b) * 4 * len;
   PState<double> w;
@@ -172,7 +227,8 @@ __device__ __forceinline__ PState<double> load_wo(const double* wo, int b, int l
   return w;
 }
 
-__global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
+template <int MODE, bool FUSE>
+__global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& s = *reinterpret_cast<Smem*>(smem_raw);
   const Blocks& B = a.B;
@@ -182,7 +238,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
   const int t = blockIdx.x % tiles;
   const int i0 = (t % a.tiles_i) * TI;   // interior index of the tile's first cell
   const int j0 = (t / a.tiles_i) * TJ;   // == array index of the halo origin
-  if (B.status[0] != 0) return;  // an earlier kernel failed: stop marching
+  __shared__ int failed;
+  if (tid == 0) failed = *(volatile int*)B.status;
+  __syncthreads();
+  if (failed) return;  // an earlier kernel failed: stop marching (uniform per CTA)
   const double* dtmin_p = a.hist ? a.hist + 4 * (*a.step) : nullptr;
   const double g = B.g, gm1 = B.gm1, gm1i = B.gm1i;
 
@@ -204,7 +263,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
   for (int q = tid; q < HJ * HI; q += NTHREADS) {
     const int hj = q / HI, hi = q % HI;
     double xc, yc, area;
-    quad_centroid(s.X[hj][hi], s.Y[hj][hi], s.X[hj][hi + 1], s.Y[hj][hi + 1], s.X[hj + 1][hi + 1],
+    E2D_QC(s.X[hj][hi], s.Y[hj][hi], s.X[hj][hi + 1], s.Y[hj][hi + 1], s.X[hj + 1][hi + 1],
                   s.Y[hj + 1][hi + 1], s.X[hj + 1][hi], s.Y[hj + 1][hi], xc, yc, area);
     s.xc[hj][hi] = xc;
     s.yc[hj][hi] = yc;
@@ -242,11 +301,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
       }
       DxDx += dx * dx; DxDy += dx * dy; DyDy += dy * dy;
     }
+#ifdef E2D_FAST
+    // the 1/n averaging cancels in the gradient
+    const double rdet = fm::rcp(DxDx * DyDy - DxDy * DxDy);
+#else
     const double dn = double(n);
 #pragma unroll
     for (int v = 0; v < 4; ++v) { DUDx[v] = DUDx[v] / dn; DUDy[v] = DUDy[v] / dn; }
     DxDx = DxDx / dn; DxDy = DxDy / dn; DyDy = DyDy / dn;
     const double det = DxDx * DyDy - DxDy * DxDy;
+#endif
     // face midpoints E, W, N, S of the cell
     const double fx[4] = {HALF * (s.X[hj][hi + 1] + s.X[hj + 1][hi + 1]), HALF * (s.X[hj][hi] + s.X[hj + 1][hi]),
                           HALF * (s.X[hj + 1][hi] + s.X[hj + 1][hi + 1]), HALF * (s.X[hj][hi] + s.X[hj][hi + 1])};
@@ -254,8 +318,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
                           HALF * (s.Y[hj + 1][hi] + s.Y[hj + 1][hi + 1]), HALF * (s.Y[hj][hi] + s.Y[hj][hi + 1])};
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
+#ifdef E2D_FAST
+      const double gx = (DUDx[v] * DyDy - DUDy[v] * DxDy) * rdet;
+      const double gy = (DUDy[v] * DxDx - DUDx[v] * DxDy) * rdet;
+#else
       const double gx = (DUDx[v] * DyDy - DUDy[v] * DxDy) / det;
       const double gy = (DUDy[v] * DxDx - DUDx[v] * DxDy) / det;
+#endif
       const double u0 = s.W[v][hj][hi];
       double umin = u0, umax = u0;
       for (int k = 0; k < n; ++k) {
@@ -266,7 +335,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
       double uq[4];
 #pragma unroll
       for (int q2 = 0; q2 < 4; ++q2) uq[q2] = u0 + gx * (fx[q2] - xc0) + gy * (fy[q2] - yc0);
+#ifdef E2D_FAST
+      const double phi = fm::limiter(B.limiter, uq, u0, umin, umax);
+#else
       const double phi = limiter(B.limiter, uq, u0, umin, umax);
+#endif
       s.px[v][rj][ri] = phi * gx;
       s.py[v][rj][ri] = phi * gy;
       if (B.dWdx) {
@@ -338,7 +411,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
         wr = face_state(s, hi, hl + 1, mx, my);
       }
     }
+#ifdef E2D_FAST
+    const CState<double> F = fm::flux_roe_n(wl, wr, nx, ny, g, gm1, gm1i);
+#else
     const CState<double> F = flux_roe_n(wl, wr, nx, ny, g, gm1, gm1i);
+#endif
     if (is_i) {
       s.Fi[0][fj][fi] = F.d; s.Fi[1][fj][fi] = F.mx; s.Fi[2][fj][fi] = F.my; s.Fi[3][fj][fi] = F.E;
       s.li[fj][fi] = l;
@@ -351,70 +428,128 @@ __global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
 
   // ---- flux divergence and update, one interior cell per thread -------------
   const int ti = tid % TI, tj = tid / TI;
-  if (ti >= nci_t || tj >= ncj_t) return;
+  const bool active = ti < nci_t && tj < ncj_t;
   const int hi = ti + 2, hj = tj + 2, I = i0 + hi, J = j0 + hj;
-  double xc, yc, A;
-  quad_centroid(s.X[hj][hi], s.Y[hj][hi], s.X[hj][hi + 1], s.Y[hj][hi + 1], s.X[hj + 1][hi + 1],
-                s.Y[hj + 1][hi + 1], s.X[hj + 1][hi], s.Y[hj + 1][hi], xc, yc, A);
-  const double lW = s.li[tj][ti], lE = s.li[tj][ti + 1], lS = s.lj[tj][ti], lN = s.lj[tj + 1][ti];
-  const size_t c = cell_sc(B, b, J, I);
-  double k = 1.0;
-  if (a.mode != 0) k = B.cfl * (B.local_dt ? B.dt[c] : *dtmin_p);
-  double res[4];
+  // contributions of this cell to the next step's CFL minimum and residual norms
+  double dt_next = MILLION_D, n1 = 0.0, n2 = 0.0, nmax = 0.0;
+  if (active) {
+    double xc, yc, A;
+    E2D_QC(s.X[hj][hi], s.Y[hj][hi], s.X[hj][hi + 1], s.Y[hj][hi + 1], s.X[hj + 1][hi + 1],
+           s.Y[hj + 1][hi + 1], s.X[hj + 1][hi], s.Y[hj + 1][hi], xc, yc, A);
+    const double lW = s.li[tj][ti], lE = s.li[tj][ti + 1], lS = s.lj[tj][ti], lN = s.lj[tj + 1][ti];
+#ifdef E2D_FAST
+    const double rA = fm::rcp(A);
+#endif
+    const size_t c = cell_sc(B, b, J, I);
+    double k = 1.0;
+    if (MODE != 0) k = B.cfl * (B.local_dt ? B.dt[c] : *dtmin_p);
+    double res[4];
 #pragma unroll
-  for (int v = 0; v < 4; ++v) {
-    double d = (a.mode == 2) ? B.dUdt[cell_var(B, b, v, J, I)] : 0.0;
-    if (a.mode != 0) {
-      d += k * s.Fi[v][tj][ti] * lW / A;
-      d -= k * s.Fi[v][tj][ti + 1] * lE / A;
-      d += k * s.Fj[v][tj][ti] * lS / A;
-      d -= k * s.Fj[v][tj + 1][ti] * lN / A;
-    } else {
-      d += s.Fi[v][tj][ti] * lW / A;
-      d -= s.Fi[v][tj][ti + 1] * lE / A;
-      d += s.Fj[v][tj][ti] * lS / A;
-      d -= s.Fj[v][tj + 1][ti] * lN / A;
-    }
-    res[v] = d;
-  }
-  if (a.mode == 0) {
-#pragma unroll
-    for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, b, v, J, I)] = res[v];
-    return;
-  }
-  // Update_Solution_Multistage_Explicit: U = Uo + omega*dUdt
-  CState<double> uo;
-  uo.d = a.Ubase[cell_var(B, b, 0, J, I)]; uo.mx = a.Ubase[cell_var(B, b, 1, J, I)];
-  uo.my = a.Ubase[cell_var(B, b, 2, J, I)]; uo.E = a.Ubase[cell_var(B, b, 3, J, I)];
-  const double omega = (B.n_stage == 2 && a.mode == 2) ? HALF * 1.0 : 1.0;
-  CState<double> u;
-  u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
-  u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
-  if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) {
-    if (!B.local_dt) {
-      set_status(B.status, ST_NEGATIVE, int(c));
-    } else {
-      double rrf = 1.0, dtc = B.dt[c];
-      for (int nr = 1; nr <= 10; ++nr) {
-        rrf = HALF * rrf;
-        dtc = rrf * dtc;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) res[v] = rrf * res[v];
-        u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
-        u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
-        if (u.d > 0.0 && u.E > 0.0 && e_of_U(u) > 0.0) break;
+    for (int v = 0; v < 4; ++v) {
+      double d = (MODE == 2) ? B.dUdt[cell_var(B, b, v, J, I)] : 0.0;
+      if (MODE != 0) {
+#ifdef E2D_FAST
+        d += k * s.Fi[v][tj][ti] * lW * rA;
+        d -= k * s.Fi[v][tj][ti + 1] * lE * rA;
+        d += k * s.Fj[v][tj][ti] * lS * rA;
+        d -= k * s.Fj[v][tj + 1][ti] * lN * rA;
+#else
+        d += k * s.Fi[v][tj][ti] * lW / A;
+        d -= k * s.Fi[v][tj][ti + 1] * lE / A;
+        d += k * s.Fj[v][tj][ti] * lS / A;
+        d -= k * s.Fj[v][tj + 1][ti] * lN / A;
+#endif
+      } else {
+#ifdef E2D_FAST
+        d += s.Fi[v][tj][ti] * lW * rA;
+        d -= s.Fi[v][tj][ti + 1] * lE * rA;
+        d += s.Fj[v][tj][ti] * lS * rA;
+        d -= s.Fj[v][tj + 1][ti] * lN * rA;
+#else
+        d += s.Fi[v][tj][ti] * lW / A;
+        d -= s.Fi[v][tj][ti + 1] * lE / A;
+        d += s.Fj[v][tj][ti] * lS / A;
+        d -= s.Fj[v][tj + 1][ti] * lN / A;
+#endif
       }
-      B.dt[c] = dtc;
-      if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) set_status(B.status, ST_NEGATIVE, int(c));
+      res[v] = d;
+    }
+    if (MODE == 0) {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, b, v, J, I)] = res[v];
+    } else {
+      // Update_Solution_Multistage_Explicit: U = Uo + omega*dUdt
+      CState<double> uo;
+      uo.d = a.Ubase[cell_var(B, b, 0, J, I)]; uo.mx = a.Ubase[cell_var(B, b, 1, J, I)];
+      uo.my = a.Ubase[cell_var(B, b, 2, J, I)]; uo.E = a.Ubase[cell_var(B, b, 3, J, I)];
+      const double omega = (B.n_stage == 2 && MODE == 2) ? HALF * 1.0 : 1.0;
+      CState<double> u;
+      u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
+      u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
+      if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) {
+        if (!B.local_dt) {
+          set_status(B.status, ST_NEGATIVE, int(c));
+        } else {
+          double rrf = 1.0, dtc = B.dt[c];
+          for (int nr = 1; nr <= 10; ++nr) {
+            rrf = HALF * rrf;
+            dtc = rrf * dtc;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) res[v] = rrf * res[v];
+            u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
+            u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
+            if (u.d > 0.0 && u.E > 0.0 && e_of_U(u) > 0.0) break;
+          }
+          B.dt[c] = dtc;
+          if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) set_status(B.status, ST_NEGATIVE, int(c));
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, b, v, J, I)] = res[v];
+#ifdef E2D_FAST
+      const PState<double> w = fm::W_of_U(u, gm1);
+#else
+      const PState<double> w = W_of_U(u, gm1);
+#endif
+      a.Uout[cell_var(B, b, 0, J, I)] = u.d; a.Uout[cell_var(B, b, 1, J, I)] = u.mx;
+      a.Uout[cell_var(B, b, 2, J, I)] = u.my; a.Uout[cell_var(B, b, 3, J, I)] = u.E;
+      a.Wout[cell_var(B, b, 0, J, I)] = w.d; a.Wout[cell_var(B, b, 1, J, I)] = w.u;
+      a.Wout[cell_var(B, b, 2, J, I)] = w.v; a.Wout[cell_var(B, b, 3, J, I)] = w.p;
+      if (FUSE) {
+        // CFL of the updated cell (Euler2DQuadSingleBlock.cc:3019-3080) and its
+        // density residual, for the next explicit step.
+        dt_next = cell_dt(s, hi, hj, A, lE, lW, lN, lS, w, g);
+        if (B.local_dt) B.dt[c] = dt_next;
+        n1 = fabs(res[0]);
+        n2 = res[0] * res[0];
+        nmax = n1;
+      }
     }
   }
-#pragma unroll
-  for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, b, v, J, I)] = res[v];
-  const PState<double> w = W_of_U(u, gm1);
-  a.Uout[cell_var(B, b, 0, J, I)] = u.d; a.Uout[cell_var(B, b, 1, J, I)] = u.mx;
-  a.Uout[cell_var(B, b, 2, J, I)] = u.my; a.Uout[cell_var(B, b, 3, J, I)] = u.E;
-  a.Wout[cell_var(B, b, 0, J, I)] = w.d; a.Wout[cell_var(B, b, 1, J, I)] = w.u;
-  a.Wout[cell_var(B, b, 2, J, I)] = w.v; a.Wout[cell_var(B, b, 3, J, I)] = w.p;
+  if (FUSE) {
+    // CTA reduction, then one atomic per quantity into the next step's slot
+    __shared__ double red[4][NTHREADS / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+      dt_next = dmin(dt_next, __shfl_xor_sync(0xffffffffu, dt_next, o));
+      n1 += __shfl_xor_sync(0xffffffffu, n1, o);
+      n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+      nmax = dmax(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+    }
+    if ((tid & 31) == 0) {
+      red[0][tid >> 5] = dt_next; red[1][tid >> 5] = n1; red[2][tid >> 5] = n2; red[3][tid >> 5] = nmax;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int w2 = 1; w2 < NTHREADS / 32; ++w2) {
+        dt_next = dmin(dt_next, red[0][w2]); n1 += red[1][w2]; n2 += red[2][w2]; nmax = dmax(nmax, red[3][w2]);
+      }
+      double* next = const_cast<double*>(a.hist) + 4 * (*a.step + 1);
+      atomicMin(reinterpret_cast<unsigned long long*>(next), (unsigned long long)__double_as_longlong(dt_next));
+      atomicAdd(next + 1, n1);
+      atomicAdd(next + 2, n2);
+      atomicMax(reinterpret_cast<unsigned long long*>(next + 3), (unsigned long long)__double_as_longlong(nmax));
+    }
+  }
 }
 
 }  // namespace E2D_NS
@@ -423,17 +558,28 @@ __global__ void __launch_bounds__(NTHREADS, 1) stage_kernel(StageArgs a) {
 namespace e2d {
 namespace E2D_NS {
 size_t stage_smem_bytes() { return sizeof(Smem); }
-cudaError_t launch_stage(const StageArgs& a, cudaStream_t st) {
+template <int MODE, bool FUSE>
+cudaError_t launch_one(const StageArgs& a, cudaStream_t st) {
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(sizeof(Smem)));
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<MODE, FUSE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(Smem)));
     if (e != cudaSuccess) return e;
     configured = true;
   }
   const int grid = a.B.nblk * a.tiles_i * a.tiles_j;
-  stage_kernel<<<grid, NTHREADS, sizeof(Smem), st>>>(a);
+  stage_kernel<MODE, FUSE><<<grid, NTHREADS, sizeof(Smem), st>>>(a);
   return cudaGetLastError();
+}
+cudaError_t launch_stage(const StageArgs& a, cudaStream_t st) {
+  switch (a.mode * 2 + (a.fuse_next ? 1 : 0)) {
+    case 0: return launch_one<0, false>(a, st);
+    case 2: return launch_one<1, false>(a, st);
+    case 3: return launch_one<1, true>(a, st);
+    case 4: return launch_one<2, false>(a, st);
+    case 5: return launch_one<2, true>(a, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 int tile_i() { return TI; }
 int tile_j() { return TJ; }

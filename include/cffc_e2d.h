@@ -166,6 +166,12 @@ int e2d_set_stream(e2d_handle *h, void *stream);
  * advances as with e2d_rk_steps.  Profiling aid; no reference counterpart. */
 int e2d_kernel_times(e2d_handle *h, int n_steps, double out[6]);
 
+/* Self-test of the fast FP64 path's Newton-refined reciprocal, reciprocal
+ * square root and square root against IEEE division / sqrt on n device
+ * inputs x (> 0): out[0..2] receive the largest relative errors (host).
+ * No reference counterpart. */
+int e2d_fastmath_check(const double *x, int n, double *out);
+
 /* Largest block count e2d_residual_norms_static serves. */
 #define E2D_NORMS_STATIC_MAX_BLOCKS 4096
 
