@@ -81,6 +81,9 @@ class BlockSet:
     scheme: Scheme = dataclasses.field(default_factory=Scheme)
     name: str = ""
     ng: int = NG
+    nbi: int = 0          # structured block layout (0: not a structured layout)
+    nbj: int = 0
+    periodic: int = 0     # 1: periodic in both directions (periodic-box wiring)
 
     @property
     def nblk(self) -> int:
@@ -183,7 +186,8 @@ def structured(nbi, nbj, nci, ncj, node_fn, periodic_i=False, periodic_j=False,
                 yc = 0.25 * (y[:-1, :-1] + y[:-1, 1:] + y[1:, 1:] + y[1:, :-1])
                 W[b] = W_fn(xc, yc, b)
     return BlockSet(nci, ncj, neighbour, bc_w, bc_e, bc_s, bc_n, node_x, node_y,
-                    wo_w, wo_e, wo_s, wo_n, W, scheme or Scheme(), name).contiguous()
+                    wo_w, wo_e, wo_s, wo_n, W, scheme or Scheme(), name, NG, nbi, nbj,
+                    int(periodic_i and periodic_j)).contiguous()
 
 
 def periodic_box_bumps(nb=4, nc=32, n_bumps=8, seed=20261203, scheme=None) -> BlockSet:
@@ -295,7 +299,8 @@ def write_case(path: str, bs: BlockSet, W: np.ndarray | None = None) -> None:
     with open(path, "wb") as f:
         f.write(struct.pack("<2i", _MAGIC, 1))
         f.write(struct.pack("<4i", bs.nblk, bs.nci, bs.ncj, bs.ng))
-        f.write(struct.pack("<8i", sc.limiter, sc.flux, sc.n_stage, sc.local_dt, 1, 0, 0, 0))
+        f.write(struct.pack("<8i", sc.limiter, sc.flux, sc.n_stage, sc.local_dt, 1,
+                            bs.nbi, bs.nbj, bs.periodic))
         f.write(struct.pack("<4d", sc.cfl, 0.0, 0.0, 0.0))
         for b in range(bs.nblk):
             f.write(bs.neighbour[b].astype("<i4").tobytes())

@@ -4,62 +4,111 @@
 // pins the C restatement (oracle/e2d_oracle.c) and times the reference's CPU
 // path.  The product never links or runs it.
 //
-// Every numerical step is the reference's own per-block routine:
-//   BCs                                src_2D/Euler2D/Euler2DQuadSingleBlock.cc:2354
-//   dUdt_Residual_Evaluation           src_2D/Euler2D/Euler2DQuadSingleBlock.cc:5095
-//                                      -> Euler2DQuad.cc:814
-//   dUdt_Multistage_Explicit           Euler2DQuadSingleBlock.cc:5117 -> Euler2DQuad.cc:1235
-//   Update_Solution_Multistage_Explicit Euler2DQuadSingleBlock.cc:5300
-//   CFL / Set_Global_TimeStep          Euler2DQuadSingleBlock.cc:3019, :3089
-//   L1/L2/Max_Norm_Residual            Euler2DQuadSingleBlock.cc:3111-3167
-//   Grid2D_Quad_Block_HO::Update_Cells src_2D/Grid/HO_Grid2DQuad.cc:9832
-// The one step restated here is the same-resolution ghost exchange between
-// blocks, a plain copy of the neighbours' two edge layers of U followed by
-// W = U.W(), as Euler2D_Quad_Block::LoadSendBuffer / UnloadReceiveBuffer do
-// (src_2D/Euler2D/Euler2DQuad.h:1570-1650) for Send_All_Messages
-// (src_2D/AMR/AdaptiveBlock2D_MessagePassing.h:7883).
+// The block set is handed to the reference as its initial multi-block mesh:
+// one Grid2D_Quad_Block_HO per block with the case's nodes (ghost nodes
+// included) and BC types, geometry from Grid2D_Quad_Block_HO::Update_Cells
+// (src_2D/Grid/HO_Grid2DQuad.cc:9832).  The reference's own
+// Create_Initial_Solution_Blocks (src_2D/AMR/AMR.h:40) then builds the
+// quadtree, the neighbour lists (periodic-box wiring, src_2D/AMR/QuadTree.cc:363,
+// when the case is periodic) and the message buffers, so every step below is
+// the reference's own code:
+//   residual   Send_All_Messages (AMR/AdaptiveBlock2D_MessagePassing.h:7883),
+//              BCs (Euler2DQuadMultiBlock.cc:937),
+//              dUdt_Residual_Evaluation (Euler2DQuadSingleBlock.cc:5095)
+//   explicit   the explicit loop of Euler2DQuadSolvers.cc:657-898 with the
+//              multi-block CFL, Set_Global_TimeStep, L1/L2/Max norms,
+//              dUdt_Multistage_Explicit, Update_Solution_Multistage_Explicit
+//   nks        Newton_Krylov_Schwarz_Solver (NewtonKrylovSchwarz2D/NKS2D.h:136)
+// The "time" mode runs the explicit step with the reference's per-block
+// routines on POSIX threads (blocks are independent between ghost
+// exchanges, as on the reference's MPI ranks) and a restated same-resolution
+// exchange, a plain copy of the neighbours' two edge layers of U followed by
+// W = U.W() (Euler2D_Quad_Block::LoadSendBuffer/UnloadReceiveBuffer,
+// src_2D/Euler2D/Euler2DQuad.h:1570-1650); the golden tests show the two agree.
 //
 // usage:
 //   e2d_ref_harness residual CASE OUT
-//   e2d_ref_harness explicit CASE NSTEPS OUT [threads]
+//   e2d_ref_harness explicit CASE NSTEPS OUT
+//   e2d_ref_harness nks      CASE OUT MAX_NEWTON GMRES_RESTART MAX_GMRES CFL0 OVERALL_TOL
 //   e2d_ref_harness time     CASE NSTEPS THREADS      (prints one JSON line)
 //
-// Case file (little endian), shared with cffc_b200/case_io.py:
+// Case file (little endian), shared with cffc_b200/cases.py:
 //   int32 magic 0x43443245, version 1
 //   int32 nblk, nci, ncj, ng
-//   int32 limiter, flux, n_stage, local_dt, time_accurate, 0, 0, 0
+//   int32 limiter, flux, n_stage, local_dt, time_accurate, nbi, nbj, periodic
 //   f64   cfl, 0, 0, 0
-//   per block:
+//   per block (b = bj * nbi + bi):
 //     int32 neighbour[8]           W, E, S, N, SW, SE, NW, NE (-1 = none)
 //     int32 bcW[NCj], bcE[NCj], bcS[NCi], bcN[NCi]      reference BC codes
 //     f64   X[NNj][NNi], Y[NNj][NNi]                    nodes incl. ghosts
 //     f64   WoW[4][NCj], WoE[4][NCj], WoS[4][NCi], WoN[4][NCi]
 //     f64   W[4][NCj][NCi]                              (rho, u, v, p)
 // with NCi = nci + 2 ng, NNi = NCi + 1 (likewise j).  Arrays are [var][j][i].
+#include <pthread.h>
 #include <time.h>
+
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <vector>
-#include <pthread.h>
 
 #include "Euler2D/Euler2DQuad.h"
 #include "Euler2D/Euler2DInput.h"
+#include "AMR/AMR.h"
+#include "NewtonKrylovSchwarz2D/NKS2D.h"
+#include "Euler2D/Euler2DQuadNKS.h"
 
 namespace {
 
+struct BlockData {
+  int neigh[8];
+  std::vector<int> bcw, bce, bcs, bcn;
+  std::vector<double> X, Y, wow, woe, wos, won, W;
+};
+
 struct Case {
-  int nblk, nci, ncj, ng;
-  int limiter, flux, n_stage, local_dt, time_accurate;
+  int nblk, nci, ncj, ng, NCi, NCj, NNi, NNj;
+  int limiter, flux, n_stage, local_dt, time_accurate, nbi, nbj, periodic;
   double cfl;
-  std::vector<int> neigh;  // nblk * 8
-  std::vector<Euler2D_Quad_Block*> blk;  // the reference block has no public copy
+  std::vector<BlockData> data;
 };
 
 template <class T> void rd(FILE* f, T* p, size_t n) {
   if (fread(p, sizeof(T), n, f) != n) { fprintf(stderr, "short read\n"); exit(2); }
 }
 template <class T> void wr(FILE* f, const T* p, size_t n) { fwrite(p, sizeof(T), n, f); }
+
+void read_case(const char* path, Case& c) {
+  FILE* f = fopen(path, "rb");
+  if (!f) { perror(path); exit(2); }
+  int hdr[2], dims[4], opts[8];
+  double dopts[4];
+  rd(f, hdr, 2);
+  if (hdr[0] != 0x43443245 || hdr[1] != 1) { fprintf(stderr, "bad case file\n"); exit(2); }
+  rd(f, dims, 4); rd(f, opts, 8); rd(f, dopts, 4);
+  c.nblk = dims[0]; c.nci = dims[1]; c.ncj = dims[2]; c.ng = dims[3];
+  c.NCi = c.nci + 2 * c.ng; c.NCj = c.ncj + 2 * c.ng; c.NNi = c.NCi + 1; c.NNj = c.NCj + 1;
+  c.limiter = opts[0]; c.flux = opts[1]; c.n_stage = opts[2]; c.local_dt = opts[3];
+  c.time_accurate = opts[4]; c.nbi = opts[5]; c.nbj = opts[6]; c.periodic = opts[7];
+  c.cfl = dopts[0];
+  if (c.nbi * c.nbj != c.nblk) { fprintf(stderr, "case has no structured block layout\n"); exit(2); }
+  c.data.resize(c.nblk);
+  for (int b = 0; b < c.nblk; ++b) {
+    BlockData& d = c.data[b];
+    rd(f, d.neigh, 8);
+    d.bcw.resize(c.NCj); d.bce.resize(c.NCj); d.bcs.resize(c.NCi); d.bcn.resize(c.NCi);
+    rd(f, &d.bcw[0], c.NCj); rd(f, &d.bce[0], c.NCj); rd(f, &d.bcs[0], c.NCi); rd(f, &d.bcn[0], c.NCi);
+    d.X.resize(c.NNi * c.NNj); d.Y.resize(c.NNi * c.NNj);
+    rd(f, &d.X[0], d.X.size()); rd(f, &d.Y[0], d.Y.size());
+    d.wow.resize(4 * c.NCj); d.woe.resize(4 * c.NCj); d.wos.resize(4 * c.NCi); d.won.resize(4 * c.NCi);
+    rd(f, &d.wow[0], d.wow.size()); rd(f, &d.woe[0], d.woe.size());
+    rd(f, &d.wos[0], d.wos.size()); rd(f, &d.won[0], d.won.size());
+    d.W.resize(4 * c.NCi * c.NCj);
+    rd(f, &d.W[0], d.W.size());
+  }
+  fclose(f);
+}
 
 void set_input(const Case& c, Euler2D_Input_Parameters& IP) {
   Set_Default_Input_Parameters(IP);
@@ -73,94 +122,79 @@ void set_input(const Case& c, Euler2D_Input_Parameters& IP) {
   IP.Time_Accurate = c.time_accurate;
   IP.Axisymmetric = 0;
   IP.Number_of_Ghost_Cells = c.ng;
+  IP.Number_of_Blocks_Idir = c.nbi;
+  IP.Number_of_Blocks_Jdir = c.nbj;
+  IP.Number_of_Processors = 1;
+  IP.Number_of_Blocks_Per_Processor = c.nblk;
+  IP.Maximum_Refinement_Level = 1;
+  IP.Minimum_Refinement_Level = 1;
+  IP.i_Grid = c.periodic ? GRID_PERIODIC_BOX : GRID_RECTANGULAR_BOX;
 }
 
-void read_case(const char* path, Case& c) {
-  FILE* f = fopen(path, "rb");
-  if (!f) { perror(path); exit(2); }
-  int hdr[2], dims[4], opts[8];
-  double dopts[4];
-  rd(f, hdr, 2);
-  if (hdr[0] != 0x43443245 || hdr[1] != 1) { fprintf(stderr, "bad case file\n"); exit(2); }
-  rd(f, dims, 4); rd(f, opts, 8); rd(f, dopts, 4);
-  c.nblk = dims[0]; c.nci = dims[1]; c.ncj = dims[2]; c.ng = dims[3];
-  c.limiter = opts[0]; c.flux = opts[1]; c.n_stage = opts[2];
-  c.local_dt = opts[3]; c.time_accurate = opts[4]; c.cfl = dopts[0];
-  c.neigh.resize(8 * c.nblk);
-  c.blk.resize(c.nblk);
-  for (int b = 0; b < c.nblk; ++b) c.blk[b] = new Euler2D_Quad_Block;
-  const int NCi = c.nci + 2 * c.ng, NCj = c.ncj + 2 * c.ng;
-  const int NNi = NCi + 1, NNj = NCj + 1;
-  std::vector<double> X(NNi * NNj), Y(NNi * NNj), Wo(4 * (NCi > NCj ? NCi : NCj));
-  std::vector<double> W(4 * NCi * NCj);
-  for (int b = 0; b < c.nblk; ++b) {
-    Euler2D_Quad_Block& B = *c.blk[b];
-    B.allocate(c.nci, c.ncj, c.ng);
-    rd(f, &c.neigh[8 * b], 8);
-    rd(f, B.Grid.BCtypeW, NCj); rd(f, B.Grid.BCtypeE, NCj);
-    rd(f, B.Grid.BCtypeS, NCi); rd(f, B.Grid.BCtypeN, NCi);
-    rd(f, &X[0], X.size()); rd(f, &Y[0], Y.size());
-    for (int j = 0; j < NNj; ++j)
-      for (int i = 0; i < NNi; ++i) {
-        B.Grid.Node[i][j].X.x = X[j * NNi + i];
-        B.Grid.Node[i][j].X.y = Y[j * NNi + i];
-      }
-    B.Grid.Schedule_Interior_Mesh_Update();
-    B.Grid.Schedule_Ghost_Cells_Update();
-    B.Grid.Update_Cells();
-    Euler2D_pState* Wo_dst[4] = {B.WoW, B.WoE, B.WoS, B.WoN};
-    const int Wo_len[4] = {NCj, NCj, NCi, NCi};
-    for (int e = 0; e < 4; ++e) {
-      rd(f, &Wo[0], 4 * Wo_len[e]);
-      for (int k = 0; k < Wo_len[e]; ++k)
-        Wo_dst[e][k] = Euler2D_pState(Wo[k], Wo[Wo_len[e] + k], Wo[2 * Wo_len[e] + k],
-                                      Wo[3 * Wo_len[e] + k]);
+// Fills one block's state from the case.
+void load_state(const Case& c, const BlockData& d, Euler2D_Quad_Block& B) {
+  const int s = c.NCi * c.NCj;
+  for (int j = 0; j < c.NCj; ++j)
+    for (int i = 0; i < c.NCi; ++i) {
+      const int q = j * c.NCi + i;
+      B.W[i][j] = Euler2D_pState(d.W[q], d.W[s + q], d.W[2 * s + q], d.W[3 * s + q]);
+      B.U[i][j] = U(B.W[i][j]);
     }
-    rd(f, &W[0], W.size());
-    for (int j = 0; j < NCj; ++j)
-      for (int i = 0; i < NCi; ++i) {
-        const int q = j * NCi + i, s = NCi * NCj;
-        B.W[i][j] = Euler2D_pState(W[q], W[s + q], W[2 * s + q], W[3 * s + q]);
-        B.U[i][j] = U(B.W[i][j]);
-      }
-    B.Freeze_Limiter = OFF;
-    B.Axisymmetric = 0;
+  Euler2D_pState* Wo_dst[4] = {B.WoW, B.WoE, B.WoS, B.WoN};
+  const std::vector<double>* Wo_src[4] = {&d.wow, &d.woe, &d.wos, &d.won};
+  const int Wo_len[4] = {c.NCj, c.NCj, c.NCi, c.NCi};
+  for (int e = 0; e < 4; ++e) {
+    const std::vector<double>& w = *Wo_src[e];
+    const int L = Wo_len[e];
+    for (int k = 0; k < L; ++k) Wo_dst[e][k] = Euler2D_pState(w[k], w[L + k], w[2 * L + k], w[3 * L + k]);
   }
-  fclose(f);
+  B.Freeze_Limiter = OFF;
+  B.Axisymmetric = 0;
 }
 
-// Same-resolution ghost exchange (see the header comment).
-void exchange(Case& c) {
-  const int g = c.ng;
-  for (int b = 0; b < c.nblk; ++b) {
-    Euler2D_Quad_Block& B = *c.blk[b];
-    const int* nb = &c.neigh[8 * b];
-    const int ICl = B.ICl, ICu = B.ICu, JCl = B.JCl, JCu = B.JCu;
-    for (int k = 0; k < 8; ++k) {
-      if (nb[k] < 0) continue;
-      Euler2D_Quad_Block& S = *c.blk[nb[k]];
-      // ghost index range in this block and the source offset in S
-      int i0, i1, j0, j1, di, dj;
-      const int wi = (k == 0 || k == 4 || k == 6), ei = (k == 1 || k == 5 || k == 7);
-      const int sj = (k == 2 || k == 4 || k == 5), nj = (k == 3 || k == 6 || k == 7);
-      if (wi) { i0 = ICl - g; i1 = ICl - 1; di = (S.ICu + 1) - ICl; }
-      else if (ei) { i0 = ICu + 1; i1 = ICu + g; di = S.ICl - (ICu + 1); }
-      else { i0 = ICl; i1 = ICu; di = 0; }
-      if (sj) { j0 = JCl - g; j1 = JCl - 1; dj = (S.JCu + 1) - JCl; }
-      else if (nj) { j0 = JCu + 1; j1 = JCu + g; dj = S.JCl - (JCu + 1); }
-      else { j0 = JCl; j1 = JCu; dj = 0; }
-      for (int j = j0; j <= j1; ++j)
-        for (int i = i0; i <= i1; ++i) {
-          B.U[i][j] = S.U[i + di][j + dj];
-          B.W[i][j] = B.U[i][j].W();
-        }
+void set_grid(const Case& c, const BlockData& d, Grid2D_Quad_Block_HO& G) {
+  for (int j = 0; j < c.NNj; ++j)
+    for (int i = 0; i < c.NNi; ++i) {
+      G.Node[i][j].X.x = d.X[j * c.NNi + i];
+      G.Node[i][j].X.y = d.Y[j * c.NNi + i];
     }
-  }
+  for (int j = 0; j < c.NCj; ++j) { G.BCtypeW[j] = d.bcw[j]; G.BCtypeE[j] = d.bce[j]; }
+  for (int i = 0; i < c.NCi; ++i) { G.BCtypeS[i] = d.bcs[i]; G.BCtypeN[i] = d.bcn[i]; }
+  G.Schedule_Interior_Mesh_Update();
+  G.Schedule_Ghost_Cells_Update();
+  G.Update_Cells();
 }
 
-void fill_ghosts(Case& c, Euler2D_Input_Parameters& IP) {
-  exchange(c);
-  for (int b = 0; b < c.nblk; ++b) BCs(*c.blk[b], IP);
+// The reference's own multi-block set-up.  order[b] = solution block index
+// of case block b.
+struct RefSet {
+  Euler2D_Input_Parameters IP;
+  QuadTreeBlock_DataStructure QuadTree;
+  AdaptiveBlockResourceList Global;
+  AdaptiveBlock2D_List Local;
+  Euler2D_Quad_Block* Soln;
+  std::vector<int> order;
+};
+
+void build_reference_blocks(const Case& c, RefSet& R) {
+  set_input(c, R.IP);
+  Grid2D_Quad_Block_HO** M = new Grid2D_Quad_Block_HO*[c.nbi];
+  for (int bi = 0; bi < c.nbi; ++bi) M[bi] = new Grid2D_Quad_Block_HO[c.nbj];
+  for (int bj = 0; bj < c.nbj; ++bj)
+    for (int bi = 0; bi < c.nbi; ++bi) {
+      M[bi][bj].allocate(c.nci, c.ncj, c.ng);
+      set_grid(c, c.data[bj * c.nbi + bi], M[bi][bj]);
+    }
+  R.Soln = NULL;
+  R.Soln = Create_Initial_Solution_Blocks(M, R.Soln, R.IP, R.QuadTree, R.Global, R.Local);
+  if (!R.Soln) { fprintf(stderr, "Create_Initial_Solution_Blocks failed\n"); exit(3); }
+  R.order.resize(c.nblk);
+  for (int bj = 0; bj < c.nbj; ++bj)
+    for (int bi = 0; bi < c.nbi; ++bi) {
+      const int n = R.QuadTree.Roots[bi][bj].block.info.blknum;
+      R.order[bj * c.nbi + bi] = n;
+      load_state(c, c.data[bj * c.nbi + bi], R.Soln[n]);
+    }
 }
 
 void dump_p(FILE* f, Euler2D_Quad_Block& B, Euler2D_pState** A) {
@@ -190,70 +224,112 @@ double wall_seconds() {
   return ts.tv_sec + 1e-9 * ts.tv_nsec;
 }
 
-// Runs fn(block) for every block on n_threads POSIX threads (blocks are
-// independent once their ghosts are filled; the reference runs them on
-// separate MPI ranks the same way).
-int n_threads = 1;
-struct ParJob { Case* c; void (*fn)(Case&, int, void*); void* arg; int t, nt; };
-void* par_worker(void* p) {
-  ParJob* j = (ParJob*)p;
-  for (int b = j->t; b < j->c->nblk; b += j->nt) j->fn(*j->c, b, j->arg);
+struct StepLog { double dt, l1, l2, lmax; };
+
+// One explicit multistage step in the order of Euler2DQuadSolvers.cc:657-898.
+int explicit_step_reference(RefSet& R, StepLog& log) {
+  Euler2D_Input_Parameters& IP = R.IP;
+  double dTime = CFL(R.Soln, R.Local, IP);
+  if (!IP.Local_Time_Stepping) Set_Global_TimeStep(R.Soln, R.Local, dTime);
+  double l1 = L1_Norm_Residual(R.Soln, R.Local);
+  double l2 = L2_Norm_Residual(R.Soln, R.Local);
+  l2 = sqrt(sqr(l2));
+  double lmax = Max_Norm_Residual(R.Soln, R.Local);
+  log.dt = dTime; log.l1 = l1; log.l2 = l2; log.lmax = lmax;
+  for (int stage = 1; stage <= IP.N_Stage; ++stage) {
+    int err = Send_All_Messages(R.Soln, R.Local, NUM_VAR_EULER2D, OFF);
+    if (err) return err;
+    BCs(R.Soln, R.Local, IP);
+    err = dUdt_Multistage_Explicit(R.Soln, R.Global, R.Local, IP, stage);
+    if (err) return err;
+    err = Send_Conservative_Flux_Corrections(R.Soln, R.Local, NUM_VAR_EULER2D);
+    if (err) return err;
+    Apply_Boundary_Flux_Corrections_Multistage_Explicit(R.Soln, R.Local, IP, stage);
+    err = Update_Solution_Multistage_Explicit(R.Soln, R.Local, IP, stage);
+    if (err) return err;
+  }
   return 0;
 }
-void parallel_blocks(Case& c, void (*fn)(Case&, int, void*), void* arg) {
-  const int nt = n_threads < c.nblk ? n_threads : c.nblk;
+
+// ---- threaded timing mode (per-block reference routines, restated exchange)
+struct TimedSet {
+  const Case* c;
+  Euler2D_Input_Parameters IP;
+  std::vector<Euler2D_Quad_Block*> blk;
+};
+int n_threads = 1;
+
+void exchange_restated(TimedSet& T) {
+  const Case& c = *T.c;
+  const int g = c.ng;
+  for (int b = 0; b < c.nblk; ++b) {
+    Euler2D_Quad_Block& B = *T.blk[b];
+    const int* nb = c.data[b].neigh;
+    const int ICl = B.ICl, ICu = B.ICu, JCl = B.JCl, JCu = B.JCu;
+    for (int k = 0; k < 8; ++k) {
+      if (nb[k] < 0) continue;
+      Euler2D_Quad_Block& S = *T.blk[nb[k]];
+      int i0, i1, j0, j1, di, dj;
+      const int wi = (k == 0 || k == 4 || k == 6), ei = (k == 1 || k == 5 || k == 7);
+      const int sj = (k == 2 || k == 4 || k == 5), nj = (k == 3 || k == 6 || k == 7);
+      if (wi) { i0 = ICl - g; i1 = ICl - 1; di = (S.ICu + 1) - ICl; }
+      else if (ei) { i0 = ICu + 1; i1 = ICu + g; di = S.ICl - (ICu + 1); }
+      else { i0 = ICl; i1 = ICu; di = 0; }
+      if (sj) { j0 = JCl - g; j1 = JCl - 1; dj = (S.JCu + 1) - JCl; }
+      else if (nj) { j0 = JCu + 1; j1 = JCu + g; dj = S.JCl - (JCu + 1); }
+      else { j0 = JCl; j1 = JCu; dj = 0; }
+      for (int j = j0; j <= j1; ++j)
+        for (int i = i0; i <= i1; ++i) {
+          B.U[i][j] = S.U[i + di][j + dj];
+          B.W[i][j] = B.U[i][j].W();
+        }
+    }
+  }
+}
+
+struct ParJob { TimedSet* T; void (*fn)(TimedSet&, int, void*); void* arg; int t, nt; };
+void* par_worker(void* p) {
+  ParJob* j = (ParJob*)p;
+  for (int b = j->t; b < j->T->c->nblk; b += j->nt) j->fn(*j->T, b, j->arg);
+  return 0;
+}
+void parallel_blocks(TimedSet& T, void (*fn)(TimedSet&, int, void*), void* arg) {
+  const int nt = n_threads < T.c->nblk ? n_threads : T.c->nblk;
   std::vector<pthread_t> th(nt);
   std::vector<ParJob> jobs(nt);
   for (int t = 0; t < nt; ++t) {
-    ParJob j = {&c, fn, arg, t, nt};
+    ParJob j = {&T, fn, arg, t, nt};
     jobs[t] = j;
     if (t > 0) pthread_create(&th[t], 0, par_worker, &jobs[t]);
   }
   par_worker(&jobs[0]);
   for (int t = 1; t < nt; ++t) pthread_join(th[t], 0);
 }
-
-struct StepLog { double dt, l1, l2, lmax; };
-
-struct CflArg { Euler2D_Input_Parameters* IP; double* dt; };
-void cfl_block(Case& c, int b, void* a) {
-  CflArg* x = (CflArg*)a;
-  x->dt[b] = CFL(*c.blk[b], *x->IP);
-}
-struct StageArg { Euler2D_Input_Parameters* IP; int stage; int* err; };
-void stage_block(Case& c, int b, void* a) {
+struct CflArg { double* dt; };
+void cfl_block(TimedSet& T, int b, void* a) { ((CflArg*)a)->dt[b] = CFL(*T.blk[b], T.IP); }
+struct StageArg { int stage; int* err; };
+void stage_block(TimedSet& T, int b, void* a) {
   StageArg* x = (StageArg*)a;
-  BCs(*c.blk[b], *x->IP);
-  int e = dUdt_Multistage_Explicit(*c.blk[b], x->stage, *x->IP);
-  if (!e) e = Update_Solution_Multistage_Explicit(*c.blk[b], x->stage, *x->IP) ? 1 : 0;
+  BCs(*T.blk[b], T.IP);
+  int e = dUdt_Multistage_Explicit(*T.blk[b], x->stage, T.IP);
+  if (!e) e = Update_Solution_Multistage_Explicit(*T.blk[b], x->stage, T.IP) ? 1 : 0;
   x->err[b] = e;
 }
 
-// One explicit multistage time step in the order of the reference's solver
-// loop (src_2D/Euler2D/Euler2DQuadSolvers.cc:657-898).
-int explicit_step(Case& c, Euler2D_Input_Parameters& IP, StepLog& log) {
-  const int nb = c.nblk;
-  double dtmin = MILLION;
+int explicit_step_threaded(TimedSet& T) {
+  const int nb = T.c->nblk;
   std::vector<double> dtb(nb);
-  CflArg ca = {&IP, &dtb[0]};
-  parallel_blocks(c, cfl_block, &ca);
+  CflArg ca = {&dtb[0]};
+  parallel_blocks(T, cfl_block, &ca);
+  double dtmin = MILLION;
   for (int b = 0; b < nb; ++b) dtmin = min(dtmin, dtb[b]);
-  if (!IP.Local_Time_Stepping)
-    for (int b = 0; b < nb; ++b) Set_Global_TimeStep(*c.blk[b], dtmin);
-  double l1 = 0, l2 = 0, lmax = 0;
-  for (int b = 0; b < nb; ++b) {
-    l1 += L1_Norm_Residual(*c.blk[b], 1);
-    l2 += sqr(L2_Norm_Residual(*c.blk[b], 1));
-    lmax = max(lmax, Max_Norm_Residual(*c.blk[b], 1));
-  }
-  // multi-block L2 (Euler2DQuadMultiBlock.cc:1049) is squared, summed over
-  // ranks and rooted again by the solver loop (Euler2DQuadSolvers.cc:690-693)
-  log.dt = dtmin; log.l1 = l1; log.l2 = sqrt(sqr(sqrt(l2))); log.lmax = lmax;
+  if (!T.IP.Local_Time_Stepping)
+    for (int b = 0; b < nb; ++b) Set_Global_TimeStep(*T.blk[b], dtmin);
   std::vector<int> errb(nb, 0);
-  for (int stage = 1; stage <= IP.N_Stage; ++stage) {
-    exchange(c);
-    StageArg sa = {&IP, stage, &errb[0]};
-    parallel_blocks(c, stage_block, &sa);
+  for (int stage = 1; stage <= T.IP.N_Stage; ++stage) {
+    exchange_restated(T);
+    StageArg sa = {stage, &errb[0]};
+    parallel_blocks(T, stage_block, &sa);
     for (int b = 0; b < nb; ++b)
       if (errb[b]) return errb[b];
   }
@@ -264,21 +340,22 @@ int explicit_step(Case& c, Euler2D_Input_Parameters& IP, StepLog& log) {
 
 int main(int argc, char** argv) {
   if (argc < 4) {
-    fprintf(stderr, "usage: %s residual|explicit|time CASE ...\n", argv[0]);
+    fprintf(stderr, "usage: %s residual|explicit|nks|time CASE ...\n", argv[0]);
     return 2;
   }
   Case c;
   read_case(argv[2], c);
-  Euler2D_Input_Parameters IP;
-  set_input(c, IP);
   const char* mode = argv[1];
 
   if (!strcmp(mode, "residual")) {
-    fill_ghosts(c, IP);
-    for (int b = 0; b < c.nblk; ++b) dUdt_Residual_Evaluation(*c.blk[b], IP);
+    RefSet R;
+    build_reference_blocks(c, R);
+    Send_All_Messages(R.Soln, R.Local, NUM_VAR_EULER2D, OFF);
+    BCs(R.Soln, R.Local, R.IP);
+    for (int b = 0; b < c.nblk; ++b) dUdt_Residual_Evaluation(R.Soln[R.order[b]], R.IP);
     FILE* f = fopen(argv[3], "wb");
     for (int b = 0; b < c.nblk; ++b) {
-      Euler2D_Quad_Block& B = *c.blk[b];
+      Euler2D_Quad_Block& B = R.Soln[R.order[b]];
       dump_p(f, B, B.W);
       dump_c(f, B, 0);
       dump_p(f, B, B.dWdx);
@@ -289,38 +366,85 @@ int main(int argc, char** argv) {
     return 0;
   }
 
-  if (!strcmp(mode, "explicit") || !strcmp(mode, "time")) {
+  if (!strcmp(mode, "explicit")) {
     const int nsteps = atoi(argv[3]);
-    const int timing = !strcmp(mode, "time");
-    int threads = 1;
-    if (timing && argc > 4) threads = atoi(argv[4]);
-    if (!timing && argc > 5) threads = atoi(argv[5]);
-    if (threads < 1) threads = 1;
-    n_threads = threads;
-    fill_ghosts(c, IP);
+    RefSet R;
+    build_reference_blocks(c, R);
+    Send_All_Messages(R.Soln, R.Local, NUM_VAR_EULER2D, OFF);
+    BCs(R.Soln, R.Local, R.IP);
     std::vector<StepLog> hist(nsteps);
-    const double t0 = wall_seconds();
     int err = 0, n = 0;
-    for (; n < nsteps && !err; ++n) err = explicit_step(c, IP, hist[n]);
-    const double t1 = wall_seconds();
+    for (; n < nsteps && !err; ++n) err = explicit_step_reference(R, hist[n]);
     if (err) fprintf(stderr, "explicit step %d failed (error %d)\n", n, err);
-    if (timing) {
-      const double s = t1 - t0;
-      const double cells = double(c.nblk) * c.nci * c.ncj;
-      printf("{\"seconds\": %.6f, \"steps\": %d, \"cells\": %.0f, \"threads\": %d, "
-             "\"mcell_updates_per_s\": %.6f, \"error\": %d}\n",
-             s, n, cells, threads, cells * n / s * 1e-6, err);
-      return err ? 1 : 0;
-    }
     FILE* f = fopen(argv[4], "wb");
     int hdr[2] = {n, err};
     wr(f, hdr, 2);
     for (int k = 0; k < n; ++k) wr(f, &hist[k].dt, 4);
     for (int b = 0; b < c.nblk; ++b) {
-      dump_c(f, *c.blk[b], -1);
-      dump_c(f, *c.blk[b], 0);
+      dump_c(f, R.Soln[R.order[b]], -1);
+      dump_c(f, R.Soln[R.order[b]], 0);
     }
     fclose(f);
+    return err ? 1 : 0;
+  }
+
+  if (!strcmp(mode, "nks")) {
+    if (argc < 10) { fprintf(stderr, "nks CASE OUT MAX_NEWTON RESTART MAX_GMRES CFL0 TOL\n"); return 2; }
+    RefSet R;
+    build_reference_blocks(c, R);
+    NKS_Input_Parameters& N = R.IP.NKS_IP;
+    N.Maximum_Number_of_NKS_Iterations = atoi(argv[4]);
+    N.GMRES_Restart = atoi(argv[5]);
+    N.Maximum_Number_of_GMRES_Iterations = atoi(argv[6]);
+    N.Finite_Time_Step_Initial_CFL = atof(argv[7]);
+    N.Overall_Tolerance = atof(argv[8]);
+    Send_All_Messages(R.Soln, R.Local, NUM_VAR_EULER2D, OFF);
+    BCs(R.Soln, R.Local, R.IP);
+    std::string hist_path = std::string(argv[3]) + ".hist";
+    std::ofstream hist(hist_path.c_str());
+    CPUTime cpu;
+    int nexp = 0;
+    double ptime = 0.0;
+    const double t0 = wall_seconds();
+    int err = Newton_Krylov_Schwarz_Solver<Euler2D_pState, Euler2D_Quad_Block, Euler2D_Input_Parameters>(
+        cpu, hist, nexp, ptime, R.Soln, R.QuadTree, R.Global, R.Local, R.IP);
+    const double t1 = wall_seconds();
+    hist.close();
+    fprintf(stderr, "nks: error %d, %.3f s\n", err, t1 - t0);
+    FILE* f = fopen(argv[3], "wb");
+    int hdr[2] = {err, 0};
+    wr(f, hdr, 2);
+    const double secs = t1 - t0;
+    wr(f, &secs, 1);
+    for (int b = 0; b < c.nblk; ++b) dump_c(f, R.Soln[R.order[b]], -1);
+    fclose(f);
+    return err ? 1 : 0;
+  }
+
+  if (!strcmp(mode, "time")) {
+    const int nsteps = atoi(argv[3]);
+    n_threads = argc > 4 ? atoi(argv[4]) : 1;
+    if (n_threads < 1) n_threads = 1;
+    TimedSet T;
+    T.c = &c;
+    set_input(c, T.IP);
+    T.blk.resize(c.nblk);
+    for (int b = 0; b < c.nblk; ++b) {
+      T.blk[b] = new Euler2D_Quad_Block;
+      T.blk[b]->allocate(c.nci, c.ncj, c.ng);
+      set_grid(c, c.data[b], T.blk[b]->Grid);
+      load_state(c, c.data[b], *T.blk[b]);
+    }
+    exchange_restated(T);
+    for (int b = 0; b < c.nblk; ++b) BCs(*T.blk[b], T.IP);
+    const double t0 = wall_seconds();
+    int err = 0, n = 0;
+    for (; n < nsteps && !err; ++n) err = explicit_step_threaded(T);
+    const double s = wall_seconds() - t0;
+    const double cells = double(c.nblk) * c.nci * c.ncj;
+    printf("{\"seconds\": %.6f, \"steps\": %d, \"cells\": %.0f, \"threads\": %d, "
+           "\"mcell_updates_per_s\": %.6f, \"error\": %d}\n",
+           s, n, cells, n_threads, cells * n / s * 1e-6, err);
     return err ? 1 : 0;
   }
   fprintf(stderr, "unknown mode %s\n", mode);

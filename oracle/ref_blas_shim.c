@@ -121,6 +121,86 @@ void dgetri_(const int *n, double *a, const int *lda, const int *ipiv,
 }
 #undef A_
 
+/* C = alpha*op(A)*op(B) + beta*C, column-major, with the loop order of the
+ * reference BLAS (BPKIT's DenseMat products call it for the block-Jacobi
+ * preconditioner apply). */
+void dgemm_(const char *ta, const char *tb, const int *m, const int *n, const int *k,
+            const double *alpha, const double *a, const int *lda, const double *b,
+            const int *ldb, const double *beta, double *c, const int *ldc) {
+  int i, j, l;
+  const int nota = (*ta == 'N' || *ta == 'n'), notb = (*tb == 'N' || *tb == 'n');
+#define A(i, j) a[(i) + (j) * (*lda)]
+#define B(i, j) b[(i) + (j) * (*ldb)]
+#define C(i, j) c[(i) + (j) * (*ldc)]
+  if (*m == 0 || *n == 0) return;
+  if (*alpha == 0.0) {
+    for (j = 0; j < *n; ++j)
+      for (i = 0; i < *m; ++i) C(i, j) = (*beta == 0.0) ? 0.0 : *beta * C(i, j);
+    return;
+  }
+  if (notb) {
+    if (nota) {
+      for (j = 0; j < *n; ++j) {
+        if (*beta == 0.0) for (i = 0; i < *m; ++i) C(i, j) = 0.0;
+        else if (*beta != 1.0) for (i = 0; i < *m; ++i) C(i, j) = *beta * C(i, j);
+        for (l = 0; l < *k; ++l) {
+          const double t = *alpha * B(l, j);
+          for (i = 0; i < *m; ++i) C(i, j) += t * A(i, l);
+        }
+      }
+    } else {
+      for (j = 0; j < *n; ++j)
+        for (i = 0; i < *m; ++i) {
+          double t = 0.0;
+          for (l = 0; l < *k; ++l) t += A(l, i) * B(l, j);
+          C(i, j) = (*beta == 0.0) ? *alpha * t : *alpha * t + *beta * C(i, j);
+        }
+    }
+  } else {
+    if (nota) {
+      for (j = 0; j < *n; ++j) {
+        if (*beta == 0.0) for (i = 0; i < *m; ++i) C(i, j) = 0.0;
+        else if (*beta != 1.0) for (i = 0; i < *m; ++i) C(i, j) = *beta * C(i, j);
+        for (l = 0; l < *k; ++l) {
+          const double t = *alpha * B(j, l);
+          for (i = 0; i < *m; ++i) C(i, j) += t * A(i, l);
+        }
+      }
+    } else {
+      for (j = 0; j < *n; ++j)
+        for (i = 0; i < *m; ++i) {
+          double t = 0.0;
+          for (l = 0; l < *k; ++l) t += A(l, i) * B(j, l);
+          C(i, j) = (*beta == 0.0) ? *alpha * t : *alpha * t + *beta * C(i, j);
+        }
+    }
+  }
+#undef A
+#undef B
+#undef C
+}
+
+/* Solve A X = B with the LU factors of dgetrf (no transpose only). */
+void dgetrs_(const char *tr, const int *n, const int *nrhs, const double *a, const int *lda,
+             const int *ipiv, double *b, const int *ldb, int *info) {
+  int i, j, k;
+  *info = 0;
+  if (!(*tr == 'N' || *tr == 'n')) { fprintf(stderr, "dgetrs_: transpose off path\n"); abort(); }
+  for (k = 0; k < *nrhs; ++k) {
+    double *x = b + k * (*ldb);
+    for (i = 0; i < *n; ++i) {
+      const int p = ipiv[i] - 1;
+      if (p != i) { double t = x[i]; x[i] = x[p]; x[p] = t; }
+    }
+    for (j = 0; j < *n; ++j)
+      for (i = j + 1; i < *n; ++i) x[i] -= x[j] * a[i + j * (*lda)];
+    for (j = *n - 1; j >= 0; --j) {
+      x[j] /= a[j + j * (*lda)];
+      for (i = 0; i < j; ++i) x[i] -= x[j] * a[i + j * (*lda)];
+    }
+  }
+}
+
 static void off_path(const char *name) {
   fprintf(stderr, "e2d_ref_harness: %s is off the Euler2D path and not linked\n", name);
   abort();
@@ -137,3 +217,4 @@ OFF_PATH(bpilutp_)
 OFF_PATH(bpilutstat_)
 OFF_PATH(bplusol_)
 OFF_PATH(readhb_)
+OFF_PATH(dgels_)
