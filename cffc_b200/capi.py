@@ -65,6 +65,34 @@ def make_scheme(sc: Scheme) -> SchemeDesc:
     return s
 
 
+class NksParams(C.Structure):
+    """e2d_nks_params: the NKS_Input_Parameters fields the solver reads
+    (NewtonKrylovSchwarz2D/NKSInput2D.h:125-172 for the defaults)."""
+    _fields_ = [("max_newton", C.c_int32), ("gmres_restart", C.c_int32), ("max_gmres", C.c_int32),
+                ("reserved", C.c_int32), ("overall_tol", C.c_double), ("cfl0", C.c_double),
+                ("gmres_tol_initial", C.c_double), ("gmres_tol_final", C.c_double),
+                ("epsilon0", C.c_double), ("min_ratio", C.c_double)]
+
+
+class NksStep(C.Structure):
+    """e2d_nks_step: one Newton step of the history."""
+    _fields_ = [("l1", C.c_double), ("l2", C.c_double), ("lmax", C.c_double), ("ratio", C.c_double),
+                ("cfl", C.c_double), ("gmres_resid0", C.c_double), ("gmres_relres", C.c_double),
+                ("gmres_iters", C.c_int32), ("gmres_restarts", C.c_int32), ("gmres_failed", C.c_int32),
+                ("pad", C.c_int32)]
+
+
+def nks_params(max_newton: int, gmres_restart: int = 30, max_gmres: int = 100, overall_tol: float = 1e-5,
+               cfl0: float = 1.0, gmres_tol: float = 1e-5, gmres_tol_final: float | None = None,
+               epsilon0: float = 1e-6, min_ratio: float = 1e-10) -> NksParams:
+    p = NksParams()
+    p.max_newton, p.gmres_restart, p.max_gmres, p.reserved = max_newton, gmres_restart, max_gmres, 0
+    p.overall_tol, p.cfl0, p.gmres_tol_initial = overall_tol, cfl0, gmres_tol
+    p.gmres_tol_final = gmres_tol if gmres_tol_final is None else gmres_tol_final
+    p.epsilon0, p.min_ratio = epsilon0, min_ratio
+    return p
+
+
 def declare(lib, prefix: str) -> None:
     """Argument/return types of the handle API under `prefix` (e2d_ or e2d_oracle_)."""
     vp = C.c_void_p
@@ -102,6 +130,8 @@ def load_library(path: str = LIB_PATH):
         lib.e2d_status.restype = C.c_int
         lib.e2d_device_state.argtypes = [C.c_void_p, C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp)]
         lib.e2d_device_state.restype = C.c_int
+        lib.e2d_nks.argtypes = [C.c_void_p, C.POINTER(NksParams), C.POINTER(NksStep), C.POINTER(C.c_int)]
+        lib.e2d_nks.restype = C.c_int
         _lib = lib
     return _lib
 
@@ -175,6 +205,15 @@ class Handle:
         out = np.zeros(3)
         self._call("norms", ptr(out))
         return out
+
+    def nks(self, params: NksParams):
+        """Newton-Krylov steady solve from the resident state.  Returns
+        (rc, history) with one dict per Newton step evaluated."""
+        steps = (NksStep * max(params.max_newton, 1))()
+        n = C.c_int(0)
+        rc = self._call("nks", C.byref(params), steps, C.byref(n))
+        hist = [{f: getattr(steps[k], f) for f, _ in NksStep._fields_ if f != "pad"} for k in range(n.value)]
+        return rc, hist
 
     def status(self) -> int:
         return self.lib.e2d_status(self.h)

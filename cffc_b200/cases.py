@@ -287,6 +287,41 @@ def channel(nbi=2, nbj=2, nci=8, ncj=6, bc=None, seed=7, mach=0.5, scheme=None,
                       name=f"channel_{nbi}x{nbj}x{nci}x{ncj}")
 
 
+def bump_channel(nbi=12, nbj=4, nci=64, ncj=32, h=0.1, mach=0.5, bc=None, scheme=None,
+                 stretch=0.0) -> BlockSet:
+    """Channel [-1.5,1.5]x[0,1] with a bump y = h*sin^2(pi*(x+0.5)) on the
+    lower wall for |x| <= 0.5; nbi x nbj blocks of nci x ncj cells.  Nodes:
+    x uniform, y = y_w(x) + eta*(1 - y_w(x)), eta = J/(nbj*ncj) (optionally
+    clustered to the wall by `stretch`); ghost nodes continue the same map.
+    Freestream rho = p = 1 at `mach`.  Default BCs: characteristic inflow /
+    outflow (W, E) with the freestream as reference state, reflecting walls
+    (S, N).  Steady-state scheme: local time stepping."""
+    nx, ny = nbi * nci, nbj * ncj
+    a = np.sqrt(GAMMA_AIR)
+    free = (1.0, mach * a, 0.0, 1.0)
+    bc = bc or dict(W=BC_CHARACTERISTIC, E=BC_CHARACTERISTIC, S=BC_REFLECTION, N=BC_REFLECTION)
+
+    def wall(x):
+        return np.where(np.abs(x) <= 0.5, h * np.sin(np.pi * (x + 0.5)) ** 2, 0.0)
+
+    def nodes(I, J):
+        x = -1.5 + 3.0 * I / nx
+        eta = J / ny
+        if stretch:
+            eta = np.sinh(stretch * eta) / np.sinh(stretch)
+        yw = wall(x)
+        return x, yw + eta * (1.0 - yw)
+
+    def W_fn(x, y, b):
+        return np.stack([np.full_like(x, free[0]), np.full_like(x, free[1]),
+                         np.full_like(x, free[2]), np.full_like(x, free[3])])
+
+    return structured(nbi, nbj, nci, ncj, nodes, False, False, bc=bc,
+                      wo=dict(W=free, E=free, S=free, N=free), W_fn=W_fn,
+                      scheme=scheme or Scheme(cfl=1.0, n_stage=2, local_dt=1),
+                      name=f"bump_channel_{nbi}x{nbj}x{nci}x{ncj}")
+
+
 # ---------------------------------------------------------------------------
 # Case-file serialisation (the format read by the reference harness; the
 # layout is documented in the harness source).

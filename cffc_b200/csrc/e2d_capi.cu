@@ -8,29 +8,11 @@
 #include <vector>
 
 #include "../../include/cffc_e2d.h"
-#include "e2d_launch.h"
+#include "e2d_handle.h"
 
 using namespace e2d;
 
-struct e2d_handle {
-  int device = 0;
-  cudaStream_t stream = nullptr;      // stream the work is enqueued on
-  cudaStream_t own_stream = nullptr;  // the handle's own stream
-  e2d_scheme sc{};
-  Blocks B{};
-  size_t ncell = 0, nnode = 0;
-  // device allocations (owned)
-  std::vector<void*> allocs;
-  double* hist = nullptr;  // [hist_cap][4]
-  int hist_cap = 0;
-  int* step = nullptr;     // device step counter
-  double* part = nullptr;  // [nblk][3] norm partials
-  bool recon_out = false;  // dWdx/dWdy/phi arrays allocated
-  // captured explicit step
-  cudaGraphExec_t step_graph = nullptr;
-};
-
-namespace {
+namespace e2d_host {
 
 #define CK(call)                                                               \
   do {                                                                         \
@@ -41,13 +23,6 @@ namespace {
     }                                                                          \
   } while (0)
 
-template <class T> int dalloc(e2d_handle* h, T** p, size_t n) {
-  void* q = nullptr;
-  if (cudaMalloc(&q, sizeof(T) * (n ? n : 1)) != cudaSuccess) return E2D_ERR_NOMEM;
-  h->allocs.push_back(q);
-  *p = static_cast<T*>(q);
-  return 0;
-}
 
 template <class T> int upload(e2d_handle* h, T** p, const T* src, size_t n) {
   int rc = dalloc(h, p, n);
@@ -67,7 +42,7 @@ int check_status(e2d_handle* h) {
 // Stage launch with the double-buffered state (see StageArgs): mode 0 reads
 // (W, U); stage 1 reads (W, U) and writes (W2, U2); stage 2 reads the halo
 // from W2 and U^0 from U and writes (W, U).
-cudaError_t launch_stage_any(e2d_handle* h, int mode, int fuse_next = 0) {
+cudaError_t launch_stage_any(e2d_handle* h, int mode, int fuse_next) {
   StageArgs a{};
   a.B = h->B;
   a.mode = mode;
@@ -154,7 +129,9 @@ cudaError_t enqueue_step(e2d_handle* h) {
   return launch_step_end(h->hist, h->step, 1, h->stream);
 }
 
-}  // namespace
+}  // namespace e2d_host
+
+using namespace e2d_host;
 
 extern "C" {
 
@@ -238,6 +215,7 @@ void e2d_destroy(e2d_handle* h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+  nks_free(h);
   for (void* p : h->allocs) cudaFree(p);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
@@ -290,7 +268,7 @@ int e2d_residual(e2d_handle* h, double* dUdt) {
   int rc = ensure_recon(h);
   if (rc) return rc;
   CK(launch_ghost_fill(h->B, h->stream));
-  CK(launch_stage_any(h, 0));
+  CK(launch_stage_any(h, 0, 0));
   if (dUdt) CK(cudaMemcpyAsync(dUdt, h->B.dUdt, sizeof(double) * 4 * h->ncell, cudaMemcpyDeviceToHost, h->stream));
   return check_status(h);
 }

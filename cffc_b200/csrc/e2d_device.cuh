@@ -73,6 +73,15 @@ struct StageArgs {
   double* Uout;
   int fuse_next;       // last stage of a step: also accumulate the next step's
                        // CFL minimum and residual norms into hist[4*(*step+1)..]
+  // mode 3 (Frechet Jacobian-vector product of the NKS, GMRES2D.h:445-488):
+  // v = (R(U)/normR - b)/eps - (z/dt)*normU/normR on interior cells, with the
+  // GMRES vectors b, z, v in the reference's cell-major layout
+  // [nblk][NCj][NCi][4].
+  const double* nks_b;
+  const double* nks_z;
+  double* nks_v;
+  const double* nks_eps;  // device scalar
+  double normU[4], normR[4];
 };
 
 __host__ __device__ inline size_t cell_var(const Blocks& B, int b, int v, int j, int i) {

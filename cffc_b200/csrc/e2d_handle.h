@@ -1,0 +1,58 @@
+// e2d_handle.h — the library's handle (internal; the C ABI sees it as an
+// opaque pointer) and the host helpers the translation units share.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <vector>
+
+#include "../../include/cffc_e2d.h"
+#include "e2d_launch.h"
+
+struct e2d_nks_state;  // NKS work arrays (e2d_nks.cu)
+
+struct e2d_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream the work is enqueued on
+  cudaStream_t own_stream = nullptr;  // the handle's own stream
+  e2d_scheme sc{};
+  e2d::Blocks B{};
+  size_t ncell = 0, nnode = 0;
+  // device allocations (owned)
+  std::vector<void*> allocs;
+  double* hist = nullptr;  // [hist_cap][4]
+  int hist_cap = 0;
+  int* step = nullptr;     // device step counter
+  double* part = nullptr;  // [nblk][3] norm partials
+  bool recon_out = false;  // dWdx/dWdy/phi arrays allocated
+  // captured explicit step
+  cudaGraphExec_t step_graph = nullptr;
+  e2d_nks_state* nks = nullptr;
+};
+
+#define E2D_CK(call)                                                           \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      fprintf(stderr, "cffc_e2d: %s failed: %s\n", #call, cudaGetErrorString(e_)); \
+      return E2D_ERR_CUDA;                                                     \
+    }                                                                          \
+  } while (0)
+
+namespace e2d_host {
+
+template <class T> int dalloc(e2d_handle* h, T** p, size_t n) {
+  void* q = nullptr;
+  if (cudaMalloc(&q, sizeof(T) * (n ? n : 1)) != cudaSuccess) return E2D_ERR_NOMEM;
+  h->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return 0;
+}
+
+int check_status(e2d_handle* h);
+cudaError_t launch_stage_any(e2d_handle* h, int mode, int fuse_next);
+cudaError_t ghost_fill_for(e2d_handle* h, int mode);
+int ensure_hist(e2d_handle* h, int n);
+void nks_free(e2d_handle* h);
+
+}  // namespace e2d_host

@@ -1,0 +1,795 @@
+// e2d_nks.cu — pseudo-transient Newton-Krylov steady solver on the device:
+// the Newton loop of Internal_Newton_Krylov_Schwarz_Solver
+// (NewtonKrylovSchwarz2D/NKS2D.h:412-1258), right-preconditioned restarted
+// matrix-free GMRES (NewtonKrylovSchwarz2D/GMRES2D.h:790-1544), the block
+// Jacobi preconditioner on the first-order HLLE Jacobian
+// (NewtonKrylovSchwarz2D/Block_Preconditioner2D.h:352-584) and the Euler2D
+// Newton_Update with positivity back-off (Euler2D/Euler2DQuadNKS.h:23-92).
+//
+// Layout.  Krylov vectors are the reference's per-block GMRES vectors laid
+// end to end: [nblk][NCj][NCi][4] doubles (GMRES_Block::index,
+// GMRES2D.h:84), ghost entries held at zero.  The preconditioner keeps one
+// 4x4 inverse per cell, row-major [nblk][NCj][NCi][16] (identity on ghost
+// cells, as Create_Preconditioner leaves them).
+//
+// Reductions (dot products, 2-norms) are two-level and deterministic: a
+// fixed grid writes per-CTA partials and the last CTA to finish sums them in
+// CTA order.  The GMRES Hessenberg column comes back to the host once per
+// inner iteration for the Givens rotations and the convergence test, which
+// the reference also does on the host (identically on every block).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "e2d_geom.cuh"
+#include "e2d_handle.h"
+
+using namespace e2d;
+
+namespace {
+
+constexpr int VT = 256;           // threads of the vector kernels
+constexpr int VGRID = 148 * 4;    // CTAs of the vector kernels (fixed: determinism)
+constexpr double RHO_STD = 1.225;       // Euler2D_W_STDATM.d
+constexpr double P_STD = 101325.0;      // Euler2D_W_STDATM.p
+
+enum Final { FIN_SUM = 0, FIN_SQRT = 1, FIN_EPS = 2 };
+
+// Block-level sum followed by the grid-level combine in the last CTA.
+// out = sum, sqrt(sum) or eps0 / sqrt(sum).
+__device__ void reduce_finalize(double v, double* partial, unsigned* counter, double* out, int fin,
+                                double eps0) {
+  __shared__ double red[VT / 32];
+  __shared__ bool last;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < VT / 32; ++w) s += red[w];
+    partial[blockIdx.x] = s;
+    __threadfence();
+    const unsigned done = atomicAdd(counter, 1u);
+    last = (done == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // the last CTA: sum the partials in CTA order (strided per lane, then a
+  // fixed tree), so the result does not depend on which CTA finished last
+  double s = 0.0;
+  for (int q = threadIdx.x; q < gridDim.x; q += VT) s += ((volatile double*)partial)[q];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < VT / 32; ++w) t += red[w];
+    *out = fin == FIN_SUM ? t : (fin == FIN_SQRT ? sqrt(t) : eps0 / sqrt(t));
+    *counter = 0u;
+  }
+}
+
+// out = reduce(sum a*b)
+__global__ void __launch_bounds__(VT) dot_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                                                 long long n2, double* partial, unsigned* counter, double* out,
+                                                 int fin, double eps0) {
+  const double2* a2 = reinterpret_cast<const double2*>(a);
+  const double2* b2 = reinterpret_cast<const double2*>(b);
+  double s = 0.0;
+  for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n2; q += (long long)gridDim.x * VT) {
+    const double2 x = a2[q], y = b2[q];
+    s += x.x * y.x;
+    s += x.y * y.y;
+  }
+  reduce_finalize(s, partial, counter, out, fin, eps0);
+}
+
+// y += alpha * x with alpha = sign * (*alpha_dev) (device scalar) or alpha_host.
+__global__ void __launch_bounds__(VT) axpy_kernel(double* __restrict__ y, const double* __restrict__ x, long long n2,
+                                                  const double* alpha_dev, double sign, double alpha_host) {
+  const double alpha = alpha_dev ? sign * (*alpha_dev) : alpha_host;
+  double2* y2 = reinterpret_cast<double2*>(y);
+  const double2* x2 = reinterpret_cast<const double2*>(x);
+  for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n2; q += (long long)gridDim.x * VT) {
+    double2 v = y2[q];
+    const double2 u = x2[q];
+    v.x = v.x + alpha * u.x;
+    v.y = v.y + alpha * u.y;
+    y2[q] = v;
+  }
+}
+
+// y *= f with f = 1 / (*s_dev) (dscal by ONE/H, GMRES2D.h:1246) or f_host.
+__global__ void __launch_bounds__(VT) scale_kernel(double* __restrict__ y, long long n2, const double* s_dev,
+                                                   double f_host) {
+  const double f = s_dev ? 1.0 / (*s_dev) : f_host;
+  double2* y2 = reinterpret_cast<double2*>(y);
+  for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n2; q += (long long)gridDim.x * VT) {
+    double2 v = y2[q];
+    v.x = f * v.x;
+    v.y = f * v.y;
+    y2[q] = v;
+  }
+}
+
+// x = x + s_0 Z_0 + s_1 Z_1 + ... in the reference's daxpy order
+// (GMRES2D.h:1300-1304).
+__global__ void __launch_bounds__(VT) update_x_kernel(double* __restrict__ x, const double* __restrict__ Z, long long n,
+                                                      const double* __restrict__ s, int k) {
+  for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n; q += (long long)gridDim.x * VT) {
+    double v = x[q];
+    for (int j = 0; j < k; ++j) v = v + s[j] * Z[size_t(j) * n + q];
+    x[q] = v;
+  }
+}
+
+// z = Minv v per cell, with eps = eps0 / ||z|| (calculate_epsilon,
+// GMRES2D.h:1628-1640) reduced on the fly.
+__global__ void __launch_bounds__(VT) precon_apply_kernel(const double* __restrict__ Minv, const double* __restrict__ v,
+                                                          double* __restrict__ z, long long ncell, double* partial,
+                                                          unsigned* counter, double* eps_out, double eps0) {
+  double s = 0.0;
+  for (long long c = blockIdx.x * (long long)VT + threadIdx.x; c < ncell; c += (long long)gridDim.x * VT) {
+    const double2* v2 = reinterpret_cast<const double2*>(v + 4 * c);
+    const double2 va = v2[0], vb = v2[1];
+    const double* M = Minv + 16 * c;
+    double o[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      double t = 0.0;
+      t = t + va.x * M[4 * r + 0];
+      t = t + va.y * M[4 * r + 1];
+      t = t + vb.x * M[4 * r + 2];
+      t = t + vb.y * M[4 * r + 3];
+      o[r] = t;
+      s += t * t;
+    }
+    double2* z2 = reinterpret_cast<double2*>(z + 4 * c);
+    z2[0] = make_double2(o[0], o[1]);
+    z2[1] = make_double2(o[2], o[3]);
+  }
+  reduce_finalize(s, partial, counter, eps_out, FIN_EPS, eps0);
+}
+
+struct Norm4 {
+  double u[4], r[4];
+};
+
+// U = Uo + (eps * dir) * normU on every cell, ghosts included, and W = W(U)
+// (calculate_perturbed_residual, GMRES2D.h:388-409).
+__global__ void __launch_bounds__(VT) perturb_kernel(Blocks B, const double* __restrict__ Uo,
+                                                     const double* __restrict__ dir, const double* eps_dev, Norm4 nm) {
+  const double eps = *eps_dev;
+  const long long ncell = (long long)B.nblk * B.NCj * B.NCi;
+  const int per = B.NCj * B.NCi;
+  for (long long c = blockIdx.x * (long long)VT + threadIdx.x; c < ncell; c += (long long)gridDim.x * VT) {
+    const int b = int(c / per), r = int(c % per);
+    const int j = r / B.NCi, i = r % B.NCi;
+    double uv[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) uv[v] = Uo[cell_var(B, b, v, j, i)] + (eps * dir[4 * c + v]) * nm.u[v];
+    CState<double> u;
+    u.d = uv[0]; u.mx = uv[1]; u.my = uv[2]; u.E = uv[3];
+    stU(B, b, i, j, u);
+    stW(B, b, i, j, W_of_U(u, B.gm1));
+  }
+}
+
+// b = normalizeR(dUdt) on interior cells (GMRES_Block::Initialize, GMRES2D.h:374-380).
+__global__ void __launch_bounds__(VT) load_b_kernel(Blocks B, double* __restrict__ bvec, Norm4 nm) {
+  const long long n = (long long)B.nblk * B.nci * B.ncj;
+  const int per = B.nci * B.ncj;
+  for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n; q += (long long)gridDim.x * VT) {
+    const int b = int(q / per), r = int(q % per);
+    const int i = NG + r % B.nci, j = NG + r / B.nci;
+    const size_t c = cell_sc(B, b, j, i);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) bvec[4 * c + v] = B.dUdt[cell_var(B, b, v, j, i)] / nm.r[v];
+  }
+}
+
+// Time step of the Newton step: the CFL-limited local step scaled by the
+// finite-time-step CFL, or the global minimum times it (NKS2D.h:913-930).
+__global__ void __launch_bounds__(VT) set_dt_kernel(Blocks B, const double* dtmin, double cfl) {
+  const long long n = (long long)B.nblk * B.nci * B.ncj;
+  const int per = B.nci * B.ncj;
+  const double dg = (*dtmin) * cfl;
+  for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n; q += (long long)gridDim.x * VT) {
+    const int b = int(q / per), r = int(q % per);
+    const int i = NG + r % B.nci, j = NG + r / B.nci;
+    const size_t c = cell_sc(B, b, j, i);
+    B.dt[c] = B.local_dt ? B.dt[c] * cfl : dg;
+  }
+}
+
+// Newton_Update (Euler2DQuadNKS.h:23-92): U = Uo + relax * x * normU on
+// interior cells, halving the update up to ten times while the density,
+// total energy or internal energy is not positive; W = W(U).
+__global__ void __launch_bounds__(VT) newton_update_kernel(Blocks B, const double* __restrict__ Uo,
+                                                           const double* __restrict__ x, Norm4 nm, double relax) {
+  const long long n = (long long)B.nblk * B.nci * B.ncj;
+  const int per = B.nci * B.ncj;
+  for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n; q += (long long)gridDim.x * VT) {
+    const int b = int(q / per), r = int(q % per);
+    const int i = NG + r % B.nci, j = NG + r / B.nci;
+    const size_t c = cell_sc(B, b, j, i);
+    double uo[4], du[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      uo[v] = Uo[cell_var(B, b, v, j, i)];
+      du[v] = x[4 * c + v] * nm.u[v];  // GMRES.deltaU = denormalizeU(x)
+    }
+    CState<double> u;
+    u.d = uo[0] + relax * du[0]; u.mx = uo[1] + relax * du[1];
+    u.my = uo[2] + relax * du[2]; u.E = uo[3] + relax * du[3];
+    if (u.d <= 0.0 || e_of_U(u) <= 0.0 || u.E <= 0.0) {
+      double f = 1.0;
+      for (int k = 1; k <= 10; ++k) {
+        f = HALF * f;
+        u.d = uo[0] + du[0] * f; u.mx = uo[1] + du[1] * f;
+        u.my = uo[2] + du[2] * f; u.E = uo[3] + du[3] * f;
+        if (u.d > 0.0 && u.E > 0.0 && e_of_U(u) > 0.0) break;
+      }
+      if (u.d <= 0.0 || e_of_U(u) <= 0.0) set_status(B.status, ST_NEGATIVE, int(c));
+    }
+    stU(B, b, i, j, u);
+    stW(B, b, i, j, W_of_U(u, B.gm1));
+  }
+}
+
+// ---- block Jacobi preconditioner ------------------------------------------
+
+__device__ __forceinline__ PState<double> rotate(const PState<double>& w, double nx, double ny) {
+  PState<double> r;
+  r.d = w.d;
+  r.u = w.u * nx + w.v * ny;
+  r.v = -w.u * ny + w.v * nx;
+  r.p = w.p;
+  return r;
+}
+
+// HLLE_wavespeeds (Euler2D/Euler2DState.cc:3199-3230): (lambda-, lambda+)
+// of the rotated Riemann problem.
+__device__ void hlle_wavespeeds(const PState<double>& wl0, const PState<double>& wr0, double nx, double ny,
+                                double g, double gm1, double& lm, double& lp) {
+  const PState<double> wl = rotate(wl0, nx, ny), wr = rotate(wr0, nx, ny);
+  const double hl = h_of(wl, g, gm1), hr = h_of(wr, g, gm1);
+  const double sdl = sqrt(wl.d), sdr = sqrt(wr.d);
+  PState<double> wa;
+  wa.d = sdl * sdr;
+  wa.u = (sdl * wl.u + sdr * wr.u) / (sdl + sdr);
+  wa.v = (sdl * wl.v + sdr * wr.v) / (sdl + sdr);
+  const double ha = (sdl * hl + sdr * hr) / (sdl + sdr);
+  const double aa2 = gm1 * (ha - HALF * (sqr(wa.u) + sqr(wa.v)));
+  wa.p = wa.d * aa2 / g;
+  lm = dmin(wl.u - a_of(wl, g), wa.u - a_of(wa, g));
+  lp = dmax(wr.u + a_of(wr, g), wa.u + a_of(wa, g));
+  lm = dmin(lm, 0.0);
+  lp = dmax(lp, 0.0);
+}
+
+// Euler2D_pState::dFdU (Euler2D/Euler2DState.h:1792-1806) of a rotated state.
+__device__ void dfdu(const PState<double>& w, double g, double gm1, double gm1i, double m[4][4]) {
+  const double ux = w.u, uy = w.v;
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) m[r][c] = 0.0;
+  m[0][1] = 1.0;
+  m[1][0] = HALF * (sqr(ux) * (g - 3.0) + sqr(uy) * gm1);
+  m[1][1] = -(ux * (g - 3.0));
+  m[1][2] = -(uy * gm1);
+  m[1][3] = gm1;
+  m[2][0] = -(ux * uy);
+  m[2][1] = uy;
+  m[2][2] = ux;
+  m[3][0] = HALF * gm1i * ux * (w.d * (2.0 + g * g - 3.0 * g) * (sqr(ux) + sqr(uy)) - 2.0 * w.p * g) / w.d;
+  m[3][1] = HALF * gm1i * (sqr(ux) * w.d * (5.0 * g - 3.0 - 2.0 * g * g) + sqr(uy) * w.d * gm1 + 2.0 * w.p * g) / w.d;
+  m[3][2] = -(ux * uy * gm1);
+  m[3][3] = g * ux;
+}
+
+// One face's block l * AI * (beta dFdU(Rotate(Wc, n)) + gamma I) * A
+// (First_Order_Inviscid_Jacobian_HLLE, Block_Preconditioner2D.h:491-584),
+// accumulated into acc.
+__device__ void face_jacobian(const PState<double>& wc, const PState<double>& wn, double nx, double ny, double l,
+                              double g, double gm1, double gm1i, double acc[4][4]) {
+  double lm, lp;
+  hlle_wavespeeds(wn, wc, nx, ny, g, gm1, lm, lp);
+  const double gam = (lm * lp) / (lp - lm);
+  const double bet = -lm / (lp - lm);
+  double d[4][4];
+  dfdu(rotate(wc, nx, ny), g, gm1, gm1i, d);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) d[r][c] = bet * d[r][c];
+    d[r][r] = d[r][r] + gam;
+  }
+  // rotation matrices: A = identity with A(1,1)=c, A(1,2)=s, A(2,1)=-s,
+  // A(2,2)=c; AI is its transpose (Rotation_Matrix, Block_Preconditioner2D.h:862)
+  double Am[4][4] = {{1, 0, 0, 0}, {0, nx, ny, 0}, {0, -ny, nx, 0}, {0, 0, 0, 1}};
+  double AI[4][4] = {{1, 0, 0, 0}, {0, nx, -ny, 0}, {0, ny, nx, 0}, {0, 0, 0, 1}};
+  double t[4][4], u[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) t[r][c] = l * AI[r][c];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s += t[r][k] * d[k][c];
+      u[r][c] = s;
+    }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s += u[r][k] * Am[k][c];
+      acc[r][c] += s;
+    }
+}
+
+// In-place inverse of a 4x4 matrix by LU with partial pivoting (the
+// LAPACK dgetrf/dgetri pair BPKIT's LP_INVERSE calls).  Returns false on a
+// zero pivot.
+__device__ bool invert4(double a[4][4]) {
+  int piv[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    int p = k;
+    double best = fabs(a[k][k]);
+#pragma unroll
+    for (int r = k + 1; r < 4; ++r)
+      if (fabs(a[r][k]) > best) { best = fabs(a[r][k]); p = r; }
+    piv[k] = p;
+    if (best == 0.0) return false;
+    if (p != k) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) { const double t = a[k][c]; a[k][c] = a[p][c]; a[p][c] = t; }
+    }
+    const double rp = 1.0 / a[k][k];
+#pragma unroll
+    for (int r = k + 1; r < 4; ++r) {
+      a[r][k] *= rp;
+#pragma unroll
+      for (int c = k + 1; c < 4; ++c) a[r][c] -= a[r][k] * a[k][c];
+    }
+  }
+  // inverse of U in place (upper triangle)
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    a[j][j] = 1.0 / a[j][j];
+    const double ajj = -a[j][j];
+#pragma unroll
+    for (int r = 0; r < j; ++r) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = r; k < j; ++k) s += a[r][k] * a[k][j];
+      a[r][j] = s;
+    }
+#pragma unroll
+    for (int r = 0; r < j; ++r) a[r][j] *= ajj;
+  }
+  // solve inv(A) * L = inv(U) for inv(A), columns from the right
+  double w[4];
+#pragma unroll
+  for (int j = 2; j >= 0; --j) {
+#pragma unroll
+    for (int r = j + 1; r < 4; ++r) { w[r] = a[r][j]; a[r][j] = 0.0; }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      double s = a[r][j];
+#pragma unroll
+      for (int k = j + 1; k < 4; ++k) s -= a[r][k] * w[k];
+      a[r][j] = s;
+    }
+  }
+  // undo the row interchanges as column interchanges
+#pragma unroll
+  for (int j = 2; j >= 0; --j) {
+    const int p = piv[j];
+    if (p != j) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) { const double t = a[r][j]; a[r][j] = a[r][p]; a[r][p] = t; }
+    }
+  }
+  return true;
+}
+
+// Diagonal block of the approximate Jacobian for each interior cell,
+// normalized (normalize_Preconditioner_dFdU, Euler2DQuadNKS.h:115-137) and
+// inverted: CENTER = -I / dt + (J_N + J_S + J_E + J_W) / A.
+__global__ void __launch_bounds__(128) precon_build_kernel(Blocks B, double* __restrict__ Minv, double ao) {
+  const long long n = (long long)B.nblk * B.nci * B.ncj;
+  const int per = B.nci * B.ncj;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int b = int(q / per), r = int(q % per);
+    const int i = NG + r % B.nci, j = NG + r / B.nci;
+    const size_t c = cell_sc(B, b, j, i);
+    const PState<double> wc = ldW(B, b, i, j);
+    double acc[4][4];
+#pragma unroll
+    for (int rr = 0; rr < 4; ++rr)
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) acc[rr][cc] = 0.0;
+    double nx, ny;
+    // N: the north face of the cell below, pointing into this cell
+    nfaceN(B, b, i, j - 1, nx, ny);
+    face_jacobian(wc, ldW(B, b, i, j - 1), nx, ny, glen(B, b, i, j, i + 1, j), B.g, B.gm1, B.gm1i, acc);
+    nfaceS(B, b, i, j + 1, nx, ny);
+    face_jacobian(wc, ldW(B, b, i, j + 1), nx, ny, glen(B, b, i, j + 1, i + 1, j + 1), B.g, B.gm1, B.gm1i, acc);
+    nfaceE(B, b, i - 1, j, nx, ny);
+    face_jacobian(wc, ldW(B, b, i - 1, j), nx, ny, glen(B, b, i, j, i, j + 1), B.g, B.gm1, B.gm1i, acc);
+    nfaceW(B, b, i + 1, j, nx, ny);
+    face_jacobian(wc, ldW(B, b, i + 1, j), nx, ny, glen(B, b, i + 1, j, i + 1, j + 1), B.g, B.gm1, B.gm1i, acc);
+    double xc, yc, A;
+    quad_centroid(nodeX(B, b, i, j), nodeY(B, b, i, j), nodeX(B, b, i + 1, j), nodeY(B, b, i + 1, j),
+                  nodeX(B, b, i + 1, j + 1), nodeY(B, b, i + 1, j + 1), nodeX(B, b, i, j + 1),
+                  nodeY(B, b, i, j + 1), xc, yc, A);
+    const double lhs = 1.0 / B.dt[c];
+    double m[4][4];
+#pragma unroll
+    for (int rr = 0; rr < 4; ++rr)
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) m[rr][cc] = (rr == cc ? -lhs : 0.0) + acc[rr][cc] / A;
+    const double ia = 1.0 / ao, ia2 = 1.0 / (ao * ao), ia3 = 1.0 / (ao * ao * ao);
+    m[0][0] *= ia; m[0][3] *= ao;
+    m[1][0] *= ia2; m[1][1] *= ia; m[1][2] *= ia;
+    m[2][0] *= ia2; m[2][1] *= ia; m[2][2] *= ia;
+    m[3][0] *= ia3; m[3][1] *= ia2; m[3][2] *= ia2; m[3][3] *= ia;
+    if (!invert4(m)) set_status(B.status, 3, int(c));
+    double* o = Minv + 16 * c;
+#pragma unroll
+    for (int rr = 0; rr < 4; ++rr)
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) o[4 * rr + cc] = m[rr][cc];
+  }
+}
+
+__global__ void identity_blocks_kernel(double* Minv, long long ncell) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < 16 * ncell;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int e = int(q % 16);
+    Minv[q] = (e / 4 == e % 4) ? 1.0 : 0.0;
+  }
+}
+
+}  // namespace
+
+struct e2d_nks_state {
+  int m = 0;                 // restart length the buffers are sized for
+  long long n = 0;           // vector length (4 * cells, ghosts included)
+  double* Uo = nullptr;      // [nblk][4][NCj][NCi]
+  double* Minv = nullptr;    // [cells][16]
+  double* bvec = nullptr;
+  double* x = nullptr;
+  double* V = nullptr;       // (m + 1) * n
+  double* Z = nullptr;       // m * n
+  double* partial = nullptr; // [VGRID]
+  unsigned* counter = nullptr;
+  double* scal = nullptr;    // [0] eps, [1] norm, [2 ..] Hessenberg column, s
+  double* hist4 = nullptr;   // CFL / norm slot
+  int* step0 = nullptr;
+  double* host = nullptr;    // pinned: Hessenberg column, norms
+  std::vector<void*> allocs;
+};
+
+namespace e2d_host {
+
+void nks_free(e2d_handle* h) {
+  if (!h->nks) return;
+  for (void* p : h->nks->allocs) cudaFree(p);
+  if (h->nks->host) cudaFreeHost(h->nks->host);
+  delete h->nks;
+  h->nks = nullptr;
+}
+
+}  // namespace e2d_host
+
+namespace {
+
+using namespace e2d_host;
+
+template <class T> int nalloc(e2d_nks_state* s, T** p, size_t n) {
+  void* q = nullptr;
+  if (cudaMalloc(&q, sizeof(T) * (n ? n : 1)) != cudaSuccess) return E2D_ERR_NOMEM;
+  s->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return 0;
+}
+
+int nks_setup(e2d_handle* h, int m) {
+  if (h->nks && h->nks->m >= m) return 0;
+  nks_free(h);
+  e2d_nks_state* s = new e2d_nks_state;
+  h->nks = s;
+  s->m = m;
+  s->n = 4 * (long long)h->ncell;
+  const size_t n = size_t(s->n);
+  int rc;
+  if ((rc = nalloc(s, &s->Uo, n)) || (rc = nalloc(s, &s->Minv, 16 * h->ncell)) || (rc = nalloc(s, &s->bvec, n)) ||
+      (rc = nalloc(s, &s->x, n)) || (rc = nalloc(s, &s->V, (m + 1) * n)) || (rc = nalloc(s, &s->Z, m * n)) ||
+      (rc = nalloc(s, &s->partial, VGRID)) || (rc = nalloc(s, &s->counter, 4)) ||
+      (rc = nalloc(s, &s->scal, 2 * m + 8)) || (rc = nalloc(s, &s->hist4, 4)) || (rc = nalloc(s, &s->step0, 1))) {
+    nks_free(h);
+    return rc;
+  }
+  if (cudaMallocHost(&s->host, sizeof(double) * (2 * m + 8)) != cudaSuccess) {
+    nks_free(h);
+    return E2D_ERR_NOMEM;
+  }
+  E2D_CK(cudaMemsetAsync(s->V, 0, sizeof(double) * (m + 1) * n, h->stream));
+  E2D_CK(cudaMemsetAsync(s->Z, 0, sizeof(double) * m * n, h->stream));
+  E2D_CK(cudaMemsetAsync(s->bvec, 0, sizeof(double) * n, h->stream));
+  E2D_CK(cudaMemsetAsync(s->counter, 0, sizeof(unsigned) * 4, h->stream));
+  E2D_CK(cudaMemsetAsync(s->step0, 0, sizeof(int), h->stream));
+  identity_blocks_kernel<<<VGRID, VT, 0, h->stream>>>(s->Minv, (long long)h->ncell);
+  E2D_CK(cudaGetLastError());
+  return 0;
+}
+
+int grid_for(long long n) {
+  long long g = (n + VT - 1) / VT;
+  if (g > VGRID) g = VGRID;
+  return int(g < 1 ? 1 : g);
+}
+
+// Stage kernel in Frechet mode: v = (R(U)/normR - b)/eps - (z/dt) normU/normR.
+cudaError_t launch_frechet(e2d_handle* h, const double* z, double* v, const Norm4& nm) {
+  StageArgs a{};
+  a.B = h->B;
+  a.mode = 3;
+  a.fuse_next = 0;
+  a.hist = h->hist;
+  a.step = h->step;
+  a.Win = h->B.W;
+  a.Ubase = h->B.U;
+  a.Wout = h->B.W;
+  a.Uout = h->B.U;
+  a.nks_b = h->nks->bvec;
+  a.nks_z = z;
+  a.nks_v = v;
+  a.nks_eps = h->nks->scal + 0;
+  for (int k = 0; k < 4; ++k) { a.normU[k] = nm.u[k]; a.normR[k] = nm.r[k]; }
+  const bool exact = h->sc.precision == E2D_PREC_FP64_EXACT;
+  const int ti = exact ? exact::tile_i() : fast::tile_i();
+  const int tj = exact ? exact::tile_j() : fast::tile_j();
+  a.tiles_i = (h->B.nci + ti - 1) / ti;
+  a.tiles_j = (h->B.ncj + tj - 1) / tj;
+  return exact ? exact::launch_stage(a, h->stream) : fast::launch_stage(a, h->stream);
+}
+
+// Perturbed residual + Frechet product: U = Uo + eps*dir (all cells), ghost
+// exchange and BCs, residual, v = J dir (GMRES2D.h:1106-1221).
+int matvec(e2d_handle* h, const double* dir, double* v, const Norm4& nm) {
+  e2d_nks_state* s = h->nks;
+  perturb_kernel<<<grid_for((long long)h->ncell), VT, 0, h->stream>>>(h->B, s->Uo, dir, s->scal + 0, nm);
+  E2D_CK(cudaGetLastError());
+  E2D_CK(ghost_fill_for(h, 0));
+  E2D_CK(launch_frechet(h, dir, v, nm));
+  return 0;
+}
+
+int dot(e2d_handle* h, const double* a, const double* b, double* out, int fin, double eps0 = 0.0) {
+  e2d_nks_state* s = h->nks;
+  dot_kernel<<<VGRID, VT, 0, h->stream>>>(a, b, s->n / 2, s->partial, s->counter, out, fin, eps0);
+  E2D_CK(cudaGetLastError());
+  return 0;
+}
+
+int axpy(e2d_handle* h, double* y, const double* x, const double* alpha_dev, double sign, double alpha_host) {
+  axpy_kernel<<<VGRID, VT, 0, h->stream>>>(y, x, h->nks->n / 2, alpha_dev, sign, alpha_host);
+  E2D_CK(cudaGetLastError());
+  return 0;
+}
+
+int scale(e2d_handle* h, double* y, const double* s_dev, double f_host) {
+  scale_kernel<<<VGRID, VT, 0, h->stream>>>(y, h->nks->n / 2, s_dev, f_host);
+  E2D_CK(cudaGetLastError());
+  return 0;
+}
+
+int fetch(e2d_handle* h, const double* dev, int count, double* out) {
+  E2D_CK(cudaMemcpyAsync(h->nks->host, dev, sizeof(double) * count, cudaMemcpyDeviceToHost, h->stream));
+  E2D_CK(cudaStreamSynchronize(h->stream));
+  memcpy(out, h->nks->host, sizeof(double) * count);
+  return 0;
+}
+
+void generate_rotation(double dx, double dy, double& cs, double& sn) {
+  if (dy == 0.0) {
+    cs = 1.0; sn = 0.0;
+  } else if (fabs(dy) > fabs(dx)) {
+    const double t = dx / dy;
+    sn = 1.0 / sqrt(1.0 + t * t);
+    cs = t * sn;
+  } else {
+    const double t = dy / dx;
+    cs = 1.0 / sqrt(1.0 + t * t);
+    sn = t * cs;
+  }
+}
+void apply_rotation(double& dx, double& dy, double cs, double sn) {
+  const double t = cs * dx + sn * dy;
+  dy = -sn * dx + cs * dy;
+  dx = t;
+}
+
+struct GmresOut {
+  double resid0 = 0, relres = 0;
+  int iters = 0;
+  bool restarted = false, failed = false;
+};
+
+// GMRES_RightPrecon_MatrixFree::solve (GMRES2D.h:790-1544) with the
+// default options: first-order Frechet derivative, no GMRES check.
+int gmres(e2d_handle* h, const e2d_nks_params& p, double tol, const Norm4& nm, GmresOut& out) {
+  e2d_nks_state* s = h->nks;
+  const int m = p.gmres_restart;
+  const long long n = s->n;
+  const size_t nb = sizeof(double) * size_t(n);
+  std::vector<double> H(size_t(m) * (m + 1), 0.0), cs(m, 0.0), sn(m, 0.0), sv(m + 1, 0.0), col(m + 2);
+  int rc;
+  E2D_CK(cudaMemsetAsync(s->x, 0, nb, h->stream));
+  // V(0) = b (the Initialize'd V(0) is zero; daxpy adds b)
+  E2D_CK(cudaMemcpyAsync(s->V, s->bvec, nb, cudaMemcpyDeviceToDevice, h->stream));
+  double resid0 = 0.0, relres = 0.0;
+  int iters = 0;
+  bool met = false, failed = false, restarted = false, first = true;
+  for (;;) {
+    if (!first) {
+      // V(0) = J x + b with eps = eps0 / ||x|| (GMRES2D.h:838-1000)
+      if ((rc = dot(h, s->x, s->x, s->scal + 0, FIN_EPS, p.epsilon0))) return rc;
+      if ((rc = matvec(h, s->x, s->V, nm))) return rc;
+      if ((rc = axpy(h, s->V, s->bvec, nullptr, 0.0, 1.0))) return rc;
+    }
+    if ((rc = dot(h, s->V, s->V, s->scal + 1, FIN_SQRT))) return rc;
+    double beta;
+    if ((rc = fetch(h, s->scal + 1, 1, &beta))) return rc;
+    if (!(beta > 0.0) || !std::isfinite(beta)) return E2D_ERR_GMRES;
+    if ((rc = scale(h, s->V, nullptr, -1.0 / beta))) return rc;
+    for (int q = 1; q < m + 1; ++q) sv[q] = 0.0;
+    sv[0] = beta;
+    if (iters == 0) resid0 = beta;
+    int j = -1;
+    for (;;) {
+      ++j;
+      ++iters;
+      double* Vj = s->V + size_t(j) * n;
+      double* Vn = s->V + size_t(j + 1) * n;
+      double* Zj = s->Z + size_t(j) * n;
+      precon_apply_kernel<<<VGRID, VT, 0, h->stream>>>(s->Minv, Vj, Zj, (long long)h->ncell, s->partial, s->counter,
+                                                       s->scal + 0, p.epsilon0);
+      E2D_CK(cudaGetLastError());
+      if ((rc = matvec(h, Zj, Vn, nm))) return rc;
+      // modified Gram-Schmidt (GMRES2D.h:1224-1240)
+      for (int k = 0; k <= j; ++k) {
+        double* hk = s->scal + 2 + k;
+        if ((rc = dot(h, Vn, s->V + size_t(k) * n, hk, FIN_SUM))) return rc;
+        if ((rc = axpy(h, Vn, s->V + size_t(k) * n, hk, -1.0, 0.0))) return rc;
+      }
+      if ((rc = dot(h, Vn, Vn, s->scal + 2 + j + 1, FIN_SQRT))) return rc;
+      if ((rc = scale(h, Vn, s->scal + 2 + j + 1, 0.0))) return rc;
+      if ((rc = fetch(h, s->scal + 2, j + 2, col.data()))) return rc;
+      double* Hj = &H[size_t(j) * (m + 1)];
+      for (int k = 0; k <= j + 1; ++k) Hj[k] = col[k];
+      if (!std::isfinite(Hj[j + 1])) return E2D_ERR_NAN;
+      for (int k = 0; k < j; ++k) apply_rotation(Hj[k], Hj[k + 1], cs[k], sn[k]);
+      generate_rotation(Hj[j], Hj[j + 1], cs[j], sn[j]);
+      apply_rotation(Hj[j], Hj[j + 1], cs[j], sn[j]);
+      apply_rotation(sv[j], sv[j + 1], cs[j], sn[j]);
+      relres = fabs(sv[j + 1]) / resid0;
+      if (relres <= tol) { met = true; break; }
+      if (iters >= p.max_gmres) { failed = true; break; }
+      if (j >= m - 1) { restarted = true; break; }
+    }
+    // back substitution and x += sum s_k Z_k (GMRES2D.h:1290-1304)
+    for (int jj = j; jj >= 0; --jj) {
+      sv[jj] /= H[size_t(jj) * (m + 1) + jj];
+      for (int k = jj - 1; k >= 0; --k) sv[k] -= H[size_t(jj) * (m + 1) + k] * sv[jj];
+    }
+    memcpy(s->host, sv.data(), sizeof(double) * (j + 1));
+    E2D_CK(cudaMemcpyAsync(s->scal + 2 + m + 2, s->host, sizeof(double) * (j + 1), cudaMemcpyHostToDevice, h->stream));
+    update_x_kernel<<<VGRID, VT, 0, h->stream>>>(s->x, s->Z, n, s->scal + 2 + m + 2, j + 1);
+    E2D_CK(cudaGetLastError());
+    // the pinned buffer is reused by the next fetch: wait for this copy
+    E2D_CK(cudaStreamSynchronize(h->stream));
+    if (met || failed) break;
+    first = false;
+  }
+  out.resid0 = resid0;
+  out.relres = relres;
+  out.iters = iters;
+  out.restarted = restarted;
+  out.failed = failed;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int e2d_nks(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, int* n_steps) {
+  if (n_steps) *n_steps = 0;
+  if (!h || !p || p->max_newton < 0 || p->gmres_restart < 1 || p->gmres_restart > 500 || p->max_gmres < 1 ||
+      !(p->epsilon0 > 0.0) || !(p->cfl0 > 0.0) || !(p->gmres_tol_initial > 0.0) || !(p->gmres_tol_final > 0.0) ||
+      !(p->min_ratio > 0.0))
+    return E2D_ERR_ARG;
+  if (cudaSetDevice(h->device) != cudaSuccess) return E2D_ERR_CUDA;
+  int rc;
+  if ((rc = nks_setup(h, p->gmres_restart))) return rc;
+  e2d_nks_state* s = h->nks;
+  Blocks& B = h->B;
+  const long long nint = (long long)B.nblk * B.nci * B.ncj;
+  // normalisation by the standard atmosphere (GMRES_Block::set_normalize_values,
+  // Euler2DQuadNKS.h:148-166)
+  const double ao = sqrt(h->sc.gamma * P_STD / RHO_STD);
+  const double rho = RHO_STD;
+  Norm4 nm;
+  nm.u[0] = rho; nm.u[1] = rho * ao; nm.u[2] = rho * ao; nm.u[3] = rho * ao * ao;
+  nm.r[0] = rho * ao; nm.r[1] = rho * ao * ao; nm.r[2] = rho * ao * ao; nm.r[3] = rho * ao * ao * ao;
+  // GMRES forcing: tol = min(0.9, tol_i * ratio^(log(f/i)/log(max(L, eps))))
+  const double L = p->overall_tol > 1e-18 ? p->overall_tol : 1e-18;
+  const double forcing = log(p->gmres_tol_final / p->gmres_tol_initial) / log(L);
+  // the caller's state: exchange and BCs first (as before the solver call)
+  E2D_CK(launch_ghost_fill(B, h->stream));
+  double l2_first = -1.0;
+  int nsteps = 0;
+  for (int newton = 1; newton <= p->max_newton; ++newton) {
+    // residual and its density norms (NKS2D.h:552-593)
+    E2D_CK(launch_stage_any(h, 0, 0));
+    E2D_CK(launch_slot_init(s->hist4, s->step0, 0, h->stream));
+    E2D_CK(launch_norms(B, h->part, s->hist4, s->step0, h->stream));
+    double nrm[4];
+    if ((rc = fetch(h, s->hist4, 4, nrm))) return rc;
+    if ((rc = check_status(h))) return rc;
+    if (!std::isfinite(nrm[2])) return E2D_ERR_NAN;
+    if (l2_first <= 0.0) l2_first = nrm[2];
+    const double ratio = nrm[2] / l2_first;
+    e2d_nks_step st{};
+    st.l1 = nrm[1]; st.l2 = nrm[2]; st.lmax = nrm[3]; st.ratio = ratio;
+    if (!(ratio > p->overall_tol)) {
+      if (hist) hist[nsteps] = st;
+      ++nsteps;
+      break;
+    }
+    // SER finite time step (Finite_Time_Step, NKS2D.h:1316-1340)
+    const double cfl = ratio > p->min_ratio ? p->cfl0 * pow(std::max(1.0, 1.0 / ratio), 1.0) : p->cfl0 / p->min_ratio;
+    st.cfl = cfl;
+    E2D_CK(launch_slot_init(s->hist4, s->step0, 0, h->stream));
+    E2D_CK(launch_cfl(B, s->hist4, s->step0, h->stream));
+    set_dt_kernel<<<grid_for(nint), VT, 0, h->stream>>>(B, s->hist4, cfl);
+    E2D_CK(cudaGetLastError());
+    // Uo = U (ghosts included) and the preconditioner at Uo
+    E2D_CK(cudaMemcpyAsync(s->Uo, B.U, sizeof(double) * 4 * h->ncell, cudaMemcpyDeviceToDevice, h->stream));
+    precon_build_kernel<<<grid_for(nint) * 2, 128, 0, h->stream>>>(B, s->Minv, ao);
+    E2D_CK(cudaGetLastError());
+    load_b_kernel<<<grid_for(nint), VT, 0, h->stream>>>(B, s->bvec, nm);
+    E2D_CK(cudaGetLastError());
+    const double tol = std::min(0.9, p->gmres_tol_initial * pow(ratio, forcing));
+    GmresOut g;
+    if ((rc = gmres(h, *p, tol, nm, g))) return rc;
+    st.gmres_resid0 = g.resid0; st.gmres_relres = g.relres; st.gmres_iters = g.iters;
+    st.gmres_restarts = g.restarted ? 1 : 0; st.gmres_failed = g.failed ? 1 : 0;
+    if (hist) hist[nsteps] = st;
+    ++nsteps;
+    // U = Uo + x, exchange and BCs (NKS2D.h:1058-1090)
+    newton_update_kernel<<<grid_for(nint), VT, 0, h->stream>>>(B, s->Uo, s->x, nm, 1.0);
+    E2D_CK(cudaGetLastError());
+    E2D_CK(launch_ghost_fill(B, h->stream));
+    if ((rc = check_status(h))) { if (n_steps) *n_steps = nsteps; return rc; }
+  }
+  if (n_steps) *n_steps = nsteps;
+  E2D_CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}

@@ -442,12 +442,12 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
 #endif
     const size_t c = cell_sc(B, b, J, I);
     double k = 1.0;
-    if (MODE != 0) k = B.cfl * (B.local_dt ? B.dt[c] : *dtmin_p);
+    if (MODE == 1 || MODE == 2) k = B.cfl * (B.local_dt ? B.dt[c] : *dtmin_p);
     double res[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
       double d = (MODE == 2) ? B.dUdt[cell_var(B, b, v, J, I)] : 0.0;
-      if (MODE != 0) {
+      if (MODE == 1 || MODE == 2) {
 #ifdef E2D_FAST
         d += k * s.Fi[v][tj][ti] * lW * rA;
         d -= k * s.Fi[v][tj][ti + 1] * lE * rA;
@@ -477,6 +477,18 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
     if (MODE == 0) {
 #pragma unroll
       for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, b, v, J, I)] = res[v];
+    } else if (MODE == 3) {
+      // Frechet derivative: calculate_Matrix_Free (GMRES2D.h:445-488),
+      // V = (normalizeR(R) - b)/eps - normalizeUtoR(z * (1/dt))
+      const double eps = *a.nks_eps;
+      const double rdt = 1.0 / B.dt[c];
+      const size_t q = c * 4;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        double val = (res[v] / a.normR[v] - a.nks_b[q + v]) / eps;
+        val -= (a.nks_z[q + v] * rdt) * a.normU[v] / a.normR[v];
+        a.nks_v[q + v] = val;
+      }
     } else {
       // Update_Solution_Multistage_Explicit: U = Uo + omega*dUdt
       CState<double> uo;
@@ -578,6 +590,7 @@ cudaError_t launch_stage(const StageArgs& a, cudaStream_t st) {
     case 3: return launch_one<1, true>(a, st);
     case 4: return launch_one<2, false>(a, st);
     case 5: return launch_one<2, true>(a, st);
+    case 6: return launch_one<3, false>(a, st);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -147,6 +147,43 @@ int e2d_rk_steps(e2d_handle *h, int n_steps, double *hist);
  * interior cells (Euler2DQuadMultiBlock.cc:1017-1190). */
 int e2d_norms(e2d_handle *h, double out[3]);
 
+/* Newton-Krylov-Schwarz parameters: the NKS_Input_Parameters fields the
+ * Euler2D steady path reads (src_2D/NewtonKrylovSchwarz2D/NKSInput2D.h:128-172;
+ * defaults in brackets).  The preconditioner is block Jacobi on the
+ * first-order HLLE Jacobian, the Frechet derivative first order. */
+typedef struct e2d_nks_params {
+  int32_t max_newton;        /* Maximum_Number_of_NKS_Iterations            */
+  int32_t gmres_restart;     /* GMRES_Restart                       [30]    */
+  int32_t max_gmres;         /* Maximum_Number_of_GMRES_Iterations          */
+  int32_t reserved;
+  double overall_tol;        /* Overall_Tolerance, L2 density drop [1e-5]   */
+  double cfl0;               /* Finite_Time_Step_Initial_CFL        [1]     */
+  double gmres_tol_initial;  /* GMRES_Initial_Tolerance             [1e-5]  */
+  double gmres_tol_final;    /* GMRES_Final_Tolerance               [1e-5]  */
+  double epsilon0;           /* Epsilon_Naught                      [1e-6]  */
+  double min_ratio;          /* Min_Finite_Time_Step_Norm_Ratio     [1e-10] */
+} e2d_nks_params;
+
+/* One Newton step of the history (the values the reference prints). */
+typedef struct e2d_nks_step {
+  double l1, l2, lmax;       /* density residual norms before the step      */
+  double ratio;              /* L2 / L2 of the first step                   */
+  double cfl;                /* finite-time-step CFL of the step            */
+  double gmres_resid0, gmres_relres; /* initial residual, final ratio       */
+  int32_t gmres_iters, gmres_restarts, gmres_failed, pad;
+} e2d_nks_step;
+
+/* Steady solve by pseudo-transient Newton-Krylov: the Newton loop of
+ * Internal_Newton_Krylov_Schwarz_Solver (NKS2D.h:412-1258) with SER CFL
+ * (Finite_Time_Step, NKS2D.h:1316), the block-Jacobi preconditioner of
+ * Block_Preconditioner (Block_Preconditioner2D.h:352-584, BPKIT BJacobi with
+ * LP_INVERSE), right-preconditioned restarted matrix-free GMRES with modified
+ * Gram-Schmidt (GMRES2D.h:790-1544) and Newton_Update with positivity
+ * back-off (Euler2DQuadNKS.h:23-92).  hist (host, may be NULL) receives one
+ * entry per Newton step evaluated, *n_steps their count.  Returns 0, or a
+ * negative library error. */
+int e2d_nks(e2d_handle *h, const e2d_nks_params *p, e2d_nks_step *hist, int *n_steps);
+
 /* Device status word: 0 or the first error a kernel recorded. */
 int e2d_status(e2d_handle *h);
 

@@ -389,7 +389,7 @@ int main(int argc, char** argv) {
   }
 
   if (!strcmp(mode, "nks")) {
-    if (argc < 10) { fprintf(stderr, "nks CASE OUT MAX_NEWTON RESTART MAX_GMRES CFL0 TOL\n"); return 2; }
+    if (argc < 9) { fprintf(stderr, "nks CASE OUT MAX_NEWTON RESTART MAX_GMRES CFL0 TOL\n"); return 2; }
     RefSet R;
     build_reference_blocks(c, R);
     NKS_Input_Parameters& N = R.IP.NKS_IP;

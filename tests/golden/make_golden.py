@@ -8,9 +8,16 @@ not need to rebuild the case bit for bit) and what the reference computed:
 * residual fixtures: W after ghost fill, dUdt, dWdx, dWdy, phi
   (dUdt_Residual_Evaluation, src_2D/Euler2D/Euler2DQuad.cc:814);
 * explicit fixtures: final U, last dUdt and the per-step dt/L1/L2/Max history
-  of the explicit loop (src_2D/Euler2D/Euler2DQuadSolvers.cc:657-898).
+  of the explicit loop (src_2D/Euler2D/Euler2DQuadSolvers.cc:657-898);
+* nks fixtures: final U of Newton_Krylov_Schwarz_Solver
+  (src_2D/NewtonKrylovSchwarz2D/NKS2D.h:136) and, per Newton step, the L2
+  norm, ratio and CFL and the GMRES iterations / resid0 / resid / relative
+  residual it prints (10 significant digits, NKS2D.h:938-945 and
+  GMRES2D.h:1515-1520); plus the same run from the initial density scaled
+  by (1 + 2^-46) ("pert_"), which measures how far the reference's own
+  history moves under a round-off-sized change of its input.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [NAME ...]
 """
 from __future__ import annotations
 
@@ -52,6 +59,38 @@ def run_explicit(bs, nsteps):
     return dict(U=rest[:, 0], dUdt=rest[:, 1], hist=hist, err=np.int32(err))
 
 
+def run_nks(bs, params):
+    """params: (max_newton, restart, max_gmres, cfl0, overall_tol)."""
+    res = run_nks_once(bs, params)
+    W = bs.W.copy()
+    W[:, 0] *= 1.0 + 2.0 ** -46
+    pert = run_nks_once(dataclasses.replace(bs, W=W), params)
+    res.update({"pert_" + k: pert[k] for k in ("U", "newton", "gmres")})
+    return res
+
+
+def run_nks_once(bs, params):
+    with tempfile.TemporaryDirectory() as td:
+        cp, op = os.path.join(td, "c.bin"), os.path.join(td, "o.bin")
+        cases.write_case(cp, bs)
+        r = subprocess.run([HARNESS, "nks", cp, op] + [str(v) for v in params], check=True,
+                           capture_output=True, text=True)
+        buf = open(op, "rb").read()
+    err = np.frombuffer(buf[:8], dtype="<i4")[0]
+    U = np.frombuffer(buf[16:], dtype="<f8").reshape(bs.nblk, 4, bs.NCj, bs.NCi)
+    newton, gmres = [], []
+    for line in r.stdout.split("\n"):
+        t = line.split()
+        if line.strip().startswith("Newton Step (Outer It.)"):
+            newton.append([float(t[t.index("L2norm") + 2]), float(t[t.index("L2norm_ratio") + 2]),
+                           float(t[t.index("CFL") + 2])])
+        elif line.strip().startswith("Finished GMRES"):
+            gmres.append([float(t[t.index("Iterations)") + 2]), float(t[t.index("resid0") + 2]),
+                          float(t[t.index("resid") + 2]), float(t[t.index("relative_residual") + 2])])
+    return dict(U=U, newton=np.array(newton), gmres=np.array(gmres), err=np.int32(err),
+                params=np.array(params, dtype=np.float64))
+
+
 def case_arrays(bs):
     d = {f.name: getattr(bs, f.name) for f in dataclasses.fields(bs)
          if isinstance(getattr(bs, f.name), np.ndarray)}
@@ -73,6 +112,9 @@ def golden_cases():
     ch_bj = cases.channel(seed=9, scheme=cases.Scheme(limiter=cases.LIMITER_BARTH_JESPERSEN,
                                                       cfl=0.4, n_stage=2, local_dt=1))
     curv = cases.curvilinear_mach2(nbi=4, nbj=2, nc=16, seed=5)
+    bump = cases.bump_channel(nbi=6, nbj=2, nci=16, ncj=16)
+    bump_bj = cases.bump_channel(nbi=4, nbj=2, nci=16, ncj=8, mach=0.6,
+                                 scheme=cases.Scheme(limiter=cases.LIMITER_BARTH_JESPERSEN, local_dt=0))
     return [
         ("residual_box_2x2x8", small_box, "residual", 0),
         ("residual_box_4x4x32", box, "residual", 0),
@@ -83,15 +125,26 @@ def golden_cases():
         ("explicit_channel_local_bj_40", ch_bj, "explicit", 40),
         ("explicit_channel_char_40", ch_char, "explicit", 40),
         ("explicit_curv_4x2x16_30", curv, "explicit", 30),
+        # Newton steps, GMRES restart, GMRES iteration cap, initial CFL, tolerance
+        ("nks_bump_6x2x16_6", bump, "nks", (6, 30, 60, 1.0, 1e-10)),
+        # global time step, Barth-Jespersen, GMRES restarts and its iteration cap
+        ("nks_bump_bj_global_4", bump_bj, "nks", (4, 10, 25, 5.0, 1e-10)),
     ]
 
 
 def main():
     if not os.path.exists(HARNESS):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "reference"], check=True)
+    only = set(sys.argv[1:])
     for name, bs, kind, steps in golden_cases():
+        if only and name not in only:
+            continue
         out = case_arrays(bs)
-        res = run_residual(bs) if kind == "residual" else run_explicit(bs, steps)
+        if kind == "nks":
+            res = run_nks(bs, steps)
+            steps = steps[0]
+        else:
+            res = run_residual(bs) if kind == "residual" else run_explicit(bs, steps)
         if bs.nblk * bs.nci * bs.ncj > 8192:
             # keep the large fixtures small: the interior of the main output only
             keep = "dUdt" if kind == "residual" else "U"
