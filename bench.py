@@ -36,13 +36,40 @@ sys.path.insert(0, ROOT)
 RK_STEPS = 500
 
 
+PRECISION = {"fp64": 0, "fp32": 1, "exact": 2}  # E2D_PREC_*
+
+
+def fp32_error(bs, nsteps, device):
+    """Relative L2 error of density and total energy after nsteps of the FP32
+    reconstruction/flux path against the FP64 path, same initial state."""
+    import dataclasses
+
+    import numpy as np
+
+    from cffc_b200 import capi
+    out = {}
+    for prec in (0, 1):
+        b2 = dataclasses.replace(bs, scheme=dataclasses.replace(bs.scheme, precision=prec))
+        h = capi.Handle(b2, device=device)
+        h.set_state()
+        rc, _ = h.rk_steps(nsteps, history=False)
+        assert rc == 0, rc
+        out[prec] = bs.interior(h.get_state()[1])
+        h.close()
+    err = {}
+    for name, v in (("density", 0), ("energy", 3)):
+        ref, x = out[0][:, v], out[1][:, v]
+        err[name] = float(np.sqrt(np.sum((x - ref) ** 2) / np.sum(ref ** 2)))
+    return err
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--precision", default="fp64", choices=["fp64", "exact"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "exact", "fp32"])
     p.add_argument("--rk-steps", type=int, default=RK_STEPS)
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -175,7 +202,8 @@ def run_reference(args):
     line = {"impl": "reference", "metric": "Mcell-updates/s (Roe+limiter residual, explicit RK2)",
             "value": round(v, 4), "unit": "Mcell-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 reconstruction+flux / f64 state" if args.precision == "fp32" else "f64",
             "data": "synthetic (seeded)", "config": config(bs, 1, args),
             "cpu_baseline": {"value": round(v, 4), "unit": "Mcell-updates/s",
                              "cores": vals[0]["threads"], "kind": kind,
@@ -204,7 +232,7 @@ def main():
 
     from cffc_b200 import capi
     bs = workload()
-    bs.scheme.precision = 2 if args.precision == "exact" else 0
+    bs.scheme.precision = PRECISION[args.precision]
     h = capi.Handle(bs, device=local)
     stream = torch.cuda.current_stream()
     h.lib.e2d_set_stream.argtypes = [capi.C.c_void_p, capi.C.c_void_p]
@@ -286,7 +314,8 @@ def main():
             "metric": "Mcell-updates/s (Roe+limiter residual, explicit RK2)",
             "value": round(value, 3), "unit": "Mcell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 reconstruction+flux / f64 state" if args.precision == "fp32" else "f64",
             "data": "synthetic (seeded curvilinear grid and perturbation)",
             "config": config(bs, world, args),
             "e2e": {"value": round(e2e, 3), "unit": "Mcell-updates/s",
@@ -304,6 +333,8 @@ def main():
             "gpu_launches": args.steps * (args.rk_steps * launches_per_rk + 4),
             "clocks": clk.summary(),
         }
+        if args.precision == "fp32":
+            line["l2_error_vs_fp64"] = dict(fp32_error(bs, args.rk_steps, local), steps=args.rk_steps)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(bs)
         print(json.dumps(line), flush=True)

@@ -23,6 +23,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 SOURCES = {
     "e2d_exact.cu": ["-fmad=false"],
     "e2d_fast.cu": ["-fmad=true"],
+    "e2d_f32.cu": ["-fmad=true", "-prec-div=false", "-prec-sqrt=false"],
     "e2d_capi.cu": ["-fmad=false"],
     "e2d_noalloc.cu": ["-fmad=false"],
     "e2d_nks.cu": ["-fmad=false"],

@@ -53,12 +53,11 @@ cudaError_t launch_stage_any(e2d_handle* h, int mode, int fuse_next) {
   a.Ubase = h->B.U;
   a.Wout = mode == 1 ? h->B.W2 : h->B.W;
   a.Uout = mode == 1 ? h->B.U2 : h->B.U;
-  const bool exact = h->sc.precision == E2D_PREC_FP64_EXACT;
-  const int ti = exact ? exact::tile_i() : fast::tile_i();
-  const int tj = exact ? exact::tile_j() : fast::tile_j();
+  int ti, tj;
+  stage_tile(h->sc.precision, &ti, &tj);
   a.tiles_i = (h->B.nci + ti - 1) / ti;
   a.tiles_j = (h->B.ncj + tj - 1) / tj;
-  cudaError_t e = exact ? exact::launch_stage(a, h->stream) : fast::launch_stage(a, h->stream);
+  cudaError_t e = launch_stage_prec(h->sc.precision, a, h->stream);
   if (e == cudaSuccess && mode == 1 && h->sc.n_stage == 1) {
     // single-stage scheme: the stage-1 result is the new solution
     const size_t n = sizeof(double) * 4 * h->ncell;
@@ -145,7 +144,8 @@ e2d_handle* e2d_create(const e2d_blocks_desc* d, const e2d_scheme* sc, int devic
   if (!d || !sc || d->nblk < 1 || d->nci < 2 || d->ncj < 2 || d->ng != NG) return fail(E2D_ERR_ARG, nullptr);
   if (sc->n_stage != 1 && sc->n_stage != 2) return fail(E2D_ERR_ARG, nullptr);
   if (sc->flux != E2D_FLUX_ROE) return fail(E2D_ERR_ARG, nullptr);
-  if (sc->precision != E2D_PREC_FP64 && sc->precision != E2D_PREC_FP64_EXACT) return fail(E2D_ERR_ARG, nullptr);
+  if (sc->precision != E2D_PREC_FP64 && sc->precision != E2D_PREC_FP64_EXACT && sc->precision != E2D_PREC_FP32)
+    return fail(E2D_ERR_ARG, nullptr);
   if (sc->limiter != E2D_LIMITER_VENKATAKRISHNAN && sc->limiter != E2D_LIMITER_BARTH_JESPERSEN &&
       sc->limiter != E2D_LIMITER_ONE && sc->limiter != E2D_LIMITER_ZERO)
     return fail(E2D_ERR_ARG, nullptr);

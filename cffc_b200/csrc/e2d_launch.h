@@ -17,6 +17,24 @@ size_t stage_smem_bytes();
 int tile_i();
 int tile_j();
 }  // namespace fast
+namespace f32 {
+cudaError_t launch_stage(const StageArgs& a, cudaStream_t st);
+size_t stage_smem_bytes();
+int tile_i();
+int tile_j();
+}  // namespace f32
+
+// The stage kernel of a precision (E2D_PREC_*): launch and tile shape.
+inline cudaError_t launch_stage_prec(int precision, const StageArgs& a, cudaStream_t st) {
+  if (precision == E2D_PREC_FP64_EXACT) return exact::launch_stage(a, st);
+  if (precision == E2D_PREC_FP32) return f32::launch_stage(a, st);
+  return fast::launch_stage(a, st);
+}
+inline void stage_tile(int precision, int* ti, int* tj) {
+  if (precision == E2D_PREC_FP64_EXACT) { *ti = exact::tile_i(); *tj = exact::tile_j(); }
+  else if (precision == E2D_PREC_FP32) { *ti = f32::tile_i(); *tj = f32::tile_j(); }
+  else { *ti = fast::tile_i(); *tj = fast::tile_j(); }
+}
 cudaError_t launch_ghost_fill(const Blocks& B, cudaStream_t st);
 cudaError_t launch_cfl(const Blocks& B, double* hist, const int* step, cudaStream_t st);
 cudaError_t launch_norms(const Blocks& B, double* part, double* hist, const int* step, cudaStream_t st);

@@ -563,12 +563,11 @@ cudaError_t launch_frechet(e2d_handle* h, const double* z, double* v, const Norm
   a.nks_v = v;
   a.nks_eps = h->nks->scal + 0;
   for (int k = 0; k < 4; ++k) { a.normU[k] = nm.u[k]; a.normR[k] = nm.r[k]; }
-  const bool exact = h->sc.precision == E2D_PREC_FP64_EXACT;
-  const int ti = exact ? exact::tile_i() : fast::tile_i();
-  const int tj = exact ? exact::tile_j() : fast::tile_j();
+  int ti, tj;
+  stage_tile(h->sc.precision, &ti, &tj);
   a.tiles_i = (h->B.nci + ti - 1) / ti;
   a.tiles_j = (h->B.ncj + tj - 1) / tj;
-  return exact ? exact::launch_stage(a, h->stream) : fast::launch_stage(a, h->stream);
+  return launch_stage_prec(h->sc.precision, a, h->stream);
 }
 
 // Perturbed residual + Frechet product: U = Uo + eps*dir (all cells), ghost

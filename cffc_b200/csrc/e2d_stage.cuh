@@ -15,9 +15,12 @@
 // with each cell's residual accumulated in the reference's loop order
 // (west + , east - , south + , north -).
 //
-// This header is compiled twice: with -fmad=false (namespace e2d::exact,
-// bit-identical to the FP64 reference) and with contraction on
-// (namespace e2d::fast).  E2D_NS names the namespace.
+// This header is compiled three times: with -fmad=false (namespace
+// e2d::exact, bit-identical to the FP64 reference), with contraction on
+// (namespace e2d::fast), and with the reconstruction and flux in FP32
+// (namespace e2d::f32, E2D_FP32: the staged state, gradients, limiter, face
+// states and Roe flux are float; geometry, the flux divergence, the RK update,
+// the CFL step and the norms stay FP64).  E2D_NS names the namespace.
 #pragma once
 #include "e2d_device.cuh"
 
@@ -41,6 +44,12 @@
 namespace e2d {
 namespace E2D_NS {
 
+#ifdef E2D_FP32
+using RT = float;   // reconstruction and flux arithmetic
+#else
+using RT = double;
+#endif
+
 constexpr int TI = 32, TJ = 8;          // interior cells per tile
 constexpr int HI = TI + 4, HJ = TJ + 4; // W tile with 2-cell halo
 constexpr int NI = TI + 5, NJ = TJ + 5; // nodes of the halo tile
@@ -48,12 +57,12 @@ constexpr int RI = TI + 2, RJ = TJ + 2; // cells reconstructed (tile + 1 ring)
 constexpr int NTHREADS = TI * TJ;
 
 struct Smem {
-  double W[4][HJ][HI];
+  RT W[4][HJ][HI];
   double X[NJ][NI], Y[NJ][NI];
   double xc[HJ][HI], yc[HJ][HI];
-  double px[4][RJ][RI], py[4][RJ][RI];   // phi^dWdx, phi^dWdy
-  double Fi[4][TJ][TI + 1], Fj[4][TJ + 1][TI];  // face fluxes
-  double li[TJ][TI + 1], lj[TJ + 1][TI];        // face lengths
+  RT px[4][RJ][RI], py[4][RJ][RI];   // phi^dWdx, phi^dWdy
+  RT Fi[4][TJ][TI + 1], Fj[4][TJ + 1][TI];  // face fluxes
+  double li[TJ][TI + 1], lj[TJ + 1][TI];    // face lengths
 };
 
 __device__ __forceinline__ bool face_bc(int bc) {
@@ -181,9 +190,9 @@ __device__ __forceinline__ int lsq_stencil(const Blocks& B, int b, int I, int J,
 
 // Limited linear face state of halo cell (hi, hj) (recon index hi-1, hj-1)
 // at face point (fx, fy): W + (phi^dWdx)*dx + (phi^dWdy)*dy.
-__device__ __forceinline__ PState<double> face_state(const Smem& s, int hi, int hj, double fx, double fy) {
-  const double dx = fx - s.xc[hj][hi], dy = fy - s.yc[hj][hi];
-  PState<double> w;
+__device__ __forceinline__ PState<RT> face_state(const Smem& s, int hi, int hj, double fx, double fy) {
+  const RT dx = RT(fx - s.xc[hj][hi]), dy = RT(fy - s.yc[hj][hi]);
+  PState<RT> w;
   w.d = s.W[0][hj][hi] + s.px[0][hj - 1][hi - 1] * dx + s.py[0][hj - 1][hi - 1] * dy;
   w.u = s.W[1][hj][hi] + s.px[1][hj - 1][hi - 1] * dx + s.py[1][hj - 1][hi - 1] * dy;
   w.v = s.W[2][hj][hi] + s.px[2][hj - 1][hi - 1] * dx + s.py[2][hj - 1][hi - 1] * dy;
@@ -220,11 +229,29 @@ __device__ __forceinline__ double cell_dt(const Smem& s, int hi, int hj, double 
   return dmin(ti, tj);
 }
 
-__device__ __forceinline__ PState<double> load_wo(const double* wo, int b, int len, int k) {
+__device__ __forceinline__ PState<RT> load_wo(const double* wo, int b, int len, int k) {
   const double* p = wo + size_t(b) * 4 * len;
-  PState<double> w;
-  w.d = p[k]; w.u = p[len + k]; w.v = p[2 * len + k]; w.p = p[3 * len + k];
+  PState<RT> w;
+  w.d = RT(p[k]); w.u = RT(p[len + k]); w.v = RT(p[2 * len + k]); w.p = RT(p[3 * len + k]);
   return w;
+}
+
+// Flux and limiter of the reconstruction type: the division-lean FP64 forms
+// on the fast path, the reference's forms otherwise (FP32 included).
+__device__ __forceinline__ CState<RT> face_flux(const PState<RT>& wl, const PState<RT>& wr, RT nx, RT ny, RT g,
+                                                RT gm1, RT gm1i) {
+#if defined(E2D_FAST) && !defined(E2D_FP32)
+  return fm::flux_roe_n(wl, wr, nx, ny, g, gm1, gm1i);
+#else
+  return flux_roe_n(wl, wr, nx, ny, g, gm1, gm1i);
+#endif
+}
+__device__ __forceinline__ RT cell_limiter(int kind, const RT* uq, RT u0, RT umin, RT umax) {
+#if defined(E2D_FAST) && !defined(E2D_FP32)
+  return fm::limiter(kind, uq, u0, umin, umax);
+#else
+  return limiter(kind, uq, u0, umin, umax);
+#endif
 }
 
 template <int MODE, bool FUSE>
@@ -249,7 +276,7 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
   for (int q = tid; q < 4 * HJ * HI; q += NTHREADS) {
     const int v = q / (HJ * HI), r = q % (HJ * HI), hj = r / HI, hi = r % HI;
     const int I = i0 + hi, J = j0 + hj;
-    s.W[v][hj][hi] = (I < B.NCi && J < B.NCj) ? a.Win[cell_var(B, b, v, J, I)] : 0.0;
+    s.W[v][hj][hi] = RT((I < B.NCi && J < B.NCj) ? a.Win[cell_var(B, b, v, J, I)] : 0.0);
   }
   for (int q = tid; q < NJ * NI; q += NTHREADS) {
     const int nj = q / NI, ni = q % NI, I = i0 + ni, J = j0 + nj;
@@ -280,7 +307,7 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
     int di[8], dj[8];
     const int n = lsq_stencil(B, b, I, J, di, dj);
     if (n == 0) {
-      for (int v = 0; v < 4; ++v) { s.px[v][rj][ri] = 0.0; s.py[v][rj][ri] = 0.0; }
+      for (int v = 0; v < 4; ++v) { s.px[v][rj][ri] = RT(0); s.py[v][rj][ri] = RT(0); }
       if (B.dWdx)
         for (int v = 0; v < 4; ++v) {
           const size_t o = cell_var(B, b, v, J, I);
@@ -288,20 +315,22 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
         }
       continue;
     }
-    double DUDx[4] = {0, 0, 0, 0}, DUDy[4] = {0, 0, 0, 0}, DxDx = 0, DxDy = 0, DyDy = 0;
+    RT DUDx[4] = {0, 0, 0, 0}, DUDy[4] = {0, 0, 0, 0}, DxDx = 0, DxDy = 0, DyDy = 0;
     const double xc0 = s.xc[hj][hi], yc0 = s.yc[hj][hi];
     for (int k = 0; k < n; ++k) {
-      const double dx = s.xc[hj + dj[k]][hi + di[k]] - xc0;
-      const double dy = s.yc[hj + dj[k]][hi + di[k]] - yc0;
+      const RT dx = RT(s.xc[hj + dj[k]][hi + di[k]] - xc0);
+      const RT dy = RT(s.yc[hj + dj[k]][hi + di[k]] - yc0);
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        const double DU = s.W[v][hj + dj[k]][hi + di[k]] - s.W[v][hj][hi];
+        const RT DU = s.W[v][hj + dj[k]][hi + di[k]] - s.W[v][hj][hi];
         DUDx[v] += DU * dx;
         DUDy[v] += DU * dy;
       }
       DxDx += dx * dx; DxDy += dx * dy; DyDy += dy * dy;
     }
-#ifdef E2D_FAST
+#if defined(E2D_FP32)
+    const RT rdet = RT(1) / (DxDx * DyDy - DxDy * DxDy);
+#elif defined(E2D_FAST)
     // the 1/n averaging cancels in the gradient
     const double rdet = fm::rcp(DxDx * DyDy - DxDy * DxDy);
 #else
@@ -316,30 +345,29 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
                           HALF * (s.X[hj + 1][hi] + s.X[hj + 1][hi + 1]), HALF * (s.X[hj][hi] + s.X[hj][hi + 1])};
     const double fy[4] = {HALF * (s.Y[hj][hi + 1] + s.Y[hj + 1][hi + 1]), HALF * (s.Y[hj][hi] + s.Y[hj + 1][hi]),
                           HALF * (s.Y[hj + 1][hi] + s.Y[hj + 1][hi + 1]), HALF * (s.Y[hj][hi] + s.Y[hj][hi + 1])};
+    RT ofx[4], ofy[4];
+#pragma unroll
+    for (int q2 = 0; q2 < 4; ++q2) { ofx[q2] = RT(fx[q2] - xc0); ofy[q2] = RT(fy[q2] - yc0); }
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-#ifdef E2D_FAST
-      const double gx = (DUDx[v] * DyDy - DUDy[v] * DxDy) * rdet;
-      const double gy = (DUDy[v] * DxDx - DUDx[v] * DxDy) * rdet;
+#if defined(E2D_FAST) || defined(E2D_FP32)
+      const RT gx = (DUDx[v] * DyDy - DUDy[v] * DxDy) * rdet;
+      const RT gy = (DUDy[v] * DxDx - DUDx[v] * DxDy) * rdet;
 #else
       const double gx = (DUDx[v] * DyDy - DUDy[v] * DxDy) / det;
       const double gy = (DUDy[v] * DxDx - DUDx[v] * DxDy) / det;
 #endif
-      const double u0 = s.W[v][hj][hi];
-      double umin = u0, umax = u0;
+      const RT u0 = s.W[v][hj][hi];
+      RT umin = u0, umax = u0;
       for (int k = 0; k < n; ++k) {
-        const double w = s.W[v][hj + dj[k]][hi + di[k]];
+        const RT w = s.W[v][hj + dj[k]][hi + di[k]];
         umin = dmin(umin, w);
         umax = dmax(umax, w);
       }
-      double uq[4];
+      RT uq[4];
 #pragma unroll
-      for (int q2 = 0; q2 < 4; ++q2) uq[q2] = u0 + gx * (fx[q2] - xc0) + gy * (fy[q2] - yc0);
-#ifdef E2D_FAST
-      const double phi = fm::limiter(B.limiter, uq, u0, umin, umax);
-#else
-      const double phi = limiter(B.limiter, uq, u0, umin, umax);
-#endif
+      for (int q2 = 0; q2 < 4; ++q2) uq[q2] = u0 + gx * ofx[q2] + gy * ofy[q2];
+      const RT phi = cell_limiter(B.limiter, uq, u0, umin, umax);
       s.px[v][rj][ri] = phi * gx;
       s.py[v][rj][ri] = phi * gy;
       if (B.dWdx) {
@@ -354,7 +382,7 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
   const int ICl = NG, ICu = B.nci + NG - 1, JCl = NG, JCu = B.ncj + NG - 1;
   const int nfi = (TI + 1) * TJ, nfj = TI * (TJ + 1);
   for (int q = tid; q < nfi + nfj; q += NTHREADS) {
-    PState<double> wl, wr;
+    PState<RT> wl, wr;
     double nx, ny, l;
     int fi, fj;
     bool is_i = q < nfi;
@@ -374,12 +402,12 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
         // nfaceW(ICl, J) with the right cell's perimeter
         double wx, wy;
         edge_normal(cx, cy, ax, ay, l, perim_for_test(s, hl + 1, hj, l), wx, wy);
-        wl = (bw == E2D_BC_REFLECTION) ? reflect(wr, wx, wy)
-                                       : bc_char_pressure(wr, load_wo(B.wow, b, B.NCj, J), wx, wy, g, gm1i);
+        wl = (bw == E2D_BC_REFLECTION) ? reflect(wr, RT(wx), RT(wy))
+                                       : bc_char_pressure(wr, load_wo(B.wow, b, B.NCj, J), RT(wx), RT(wy), RT(g), RT(gm1i));
       } else if (I == ICu && face_bc(be)) {
         wl = face_state(s, hl, hj, mx, my);
-        wr = (be == E2D_BC_REFLECTION) ? reflect(wl, nx, ny)
-                                       : bc_char_pressure(wl, load_wo(B.woe, b, B.NCj, J), nx, ny, g, gm1i);
+        wr = (be == E2D_BC_REFLECTION) ? reflect(wl, RT(nx), RT(ny))
+                                       : bc_char_pressure(wl, load_wo(B.woe, b, B.NCj, J), RT(nx), RT(ny), RT(g), RT(gm1i));
       } else {
         wl = face_state(s, hl, hj, mx, my);
         wr = face_state(s, hl + 1, hj, mx, my);
@@ -400,22 +428,18 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
         wr = face_state(s, hi, hl + 1, mx, my);
         double sx, sy;  // nfaceS(I, JCl): edge (I+1,J+1)->(I,J+1) of the upper cell
         edge_normal(cx, cy, ax, ay, l, perim_for_test(s, hi, hl + 1, l), sx, sy);
-        wl = (bs == E2D_BC_REFLECTION) ? reflect(wr, sx, sy)
-                                       : bc_char_pressure(wr, load_wo(B.wos, b, B.NCi, I), sx, sy, g, gm1i);
+        wl = (bs == E2D_BC_REFLECTION) ? reflect(wr, RT(sx), RT(sy))
+                                       : bc_char_pressure(wr, load_wo(B.wos, b, B.NCi, I), RT(sx), RT(sy), RT(g), RT(gm1i));
       } else if (J == JCu && face_bc(bn)) {
         wl = face_state(s, hi, hl, mx, my);
-        wr = (bn == E2D_BC_REFLECTION) ? reflect(wl, nx, ny)
-                                       : bc_char_pressure(wl, load_wo(B.won, b, B.NCi, I), nx, ny, g, gm1i);
+        wr = (bn == E2D_BC_REFLECTION) ? reflect(wl, RT(nx), RT(ny))
+                                       : bc_char_pressure(wl, load_wo(B.won, b, B.NCi, I), RT(nx), RT(ny), RT(g), RT(gm1i));
       } else {
         wl = face_state(s, hi, hl, mx, my);
         wr = face_state(s, hi, hl + 1, mx, my);
       }
     }
-#ifdef E2D_FAST
-    const CState<double> F = fm::flux_roe_n(wl, wr, nx, ny, g, gm1, gm1i);
-#else
-    const CState<double> F = flux_roe_n(wl, wr, nx, ny, g, gm1, gm1i);
-#endif
+    const CState<RT> F = face_flux(wl, wr, RT(nx), RT(ny), RT(g), RT(gm1), RT(gm1i));
     if (is_i) {
       s.Fi[0][fj][fi] = F.d; s.Fi[1][fj][fi] = F.mx; s.Fi[2][fj][fi] = F.my; s.Fi[3][fj][fi] = F.E;
       s.li[fj][fi] = l;

@@ -29,7 +29,7 @@
 // usage:
 //   e2d_ref_harness residual CASE OUT
 //   e2d_ref_harness explicit CASE NSTEPS OUT
-//   e2d_ref_harness nks      CASE OUT MAX_NEWTON GMRES_RESTART MAX_GMRES CFL0 OVERALL_TOL
+//   e2d_ref_harness nks      CASE OUT MAX_NEWTON GMRES_RESTART MAX_GMRES CFL0 OVERALL_TOL [GMRES_TOL]
 //   e2d_ref_harness time     CASE NSTEPS THREADS      (prints one JSON line)
 //
 // Case file (little endian), shared with cffc_b200/cases.py:
@@ -398,6 +398,7 @@ int main(int argc, char** argv) {
     N.Maximum_Number_of_GMRES_Iterations = atoi(argv[6]);
     N.Finite_Time_Step_Initial_CFL = atof(argv[7]);
     N.Overall_Tolerance = atof(argv[8]);
+    if (argc > 9) N.GMRES_Initial_Tolerance = N.GMRES_Final_Tolerance = atof(argv[9]);
     Send_All_Messages(R.Soln, R.Local, NUM_VAR_EULER2D, OFF);
     BCs(R.Soln, R.Local, R.IP);
     std::string hist_path = std::string(argv[3]) + ".hist";

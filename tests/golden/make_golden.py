@@ -13,7 +13,8 @@ not need to rebuild the case bit for bit) and what the reference computed:
   (src_2D/NewtonKrylovSchwarz2D/NKS2D.h:136) and, per Newton step, the L2
   norm, ratio and CFL and the GMRES iterations / resid0 / resid / relative
   residual it prints (10 significant digits, NKS2D.h:938-945 and
-  GMRES2D.h:1515-1520); plus the same run from the initial density scaled
+  GMRES2D.h:1515-1520), and the closing "End of Newton Steps" line (steps
+  taken, final L2 and ratio, NKS2D.h:1150-1153); plus the same run from the initial density scaled
   by (1 + 2^-46) ("pert_"), which measures how far the reference's own
   history moves under a round-off-sized change of its input.
 
@@ -60,12 +61,12 @@ def run_explicit(bs, nsteps):
 
 
 def run_nks(bs, params):
-    """params: (max_newton, restart, max_gmres, cfl0, overall_tol)."""
+    """params: (max_newton, restart, max_gmres, cfl0, overall_tol[, gmres_tol])."""
     res = run_nks_once(bs, params)
     W = bs.W.copy()
     W[:, 0] *= 1.0 + 2.0 ** -46
     pert = run_nks_once(dataclasses.replace(bs, W=W), params)
-    res.update({"pert_" + k: pert[k] for k in ("U", "newton", "gmres")})
+    res.update({"pert_" + k: pert[k] for k in ("U", "newton", "gmres", "final")})
     return res
 
 
@@ -78,17 +79,20 @@ def run_nks_once(bs, params):
         buf = open(op, "rb").read()
     err = np.frombuffer(buf[:8], dtype="<i4")[0]
     U = np.frombuffer(buf[16:], dtype="<f8").reshape(bs.nblk, 4, bs.NCj, bs.NCi)
-    newton, gmres = [], []
+    newton, gmres, final = [], [], []
     for line in r.stdout.split("\n"):
         t = line.split()
         if line.strip().startswith("Newton Step (Outer It.)"):
             newton.append([float(t[t.index("L2norm") + 2]), float(t[t.index("L2norm_ratio") + 2]),
                            float(t[t.index("CFL") + 2])])
+        elif line.strip().startswith("End of Newton Steps"):
+            final = [float(t[t.index("Steps") + 2]), float(t[t.index("L2norm") + 2]),
+                     float(t[t.index("L2norm_ratio") + 2])]
         elif line.strip().startswith("Finished GMRES"):
             gmres.append([float(t[t.index("Iterations)") + 2]), float(t[t.index("resid0") + 2]),
                           float(t[t.index("resid") + 2]), float(t[t.index("relative_residual") + 2])])
-    return dict(U=U, newton=np.array(newton), gmres=np.array(gmres), err=np.int32(err),
-                params=np.array(params, dtype=np.float64))
+    return dict(U=U, newton=np.array(newton), gmres=np.array(gmres), final=np.array(final),
+                err=np.int32(err), params=np.array(params, dtype=np.float64))
 
 
 def case_arrays(bs):
@@ -115,6 +119,8 @@ def golden_cases():
     bump = cases.bump_channel(nbi=6, nbj=2, nci=16, ncj=16)
     bump_bj = cases.bump_channel(nbi=4, nbj=2, nci=16, ncj=8, mach=0.6,
                                  scheme=cases.Scheme(limiter=cases.LIMITER_BARTH_JESPERSEN, local_dt=0))
+    bump_m14 = cases.bump_channel(nbi=6, nbj=2, nci=16, ncj=16, mach=1.4, h=0.04,
+                                  scheme=cases.Scheme(limiter=cases.LIMITER_ZERO, local_dt=1))
     return [
         ("residual_box_2x2x8", small_box, "residual", 0),
         ("residual_box_4x4x32", box, "residual", 0),
@@ -129,6 +135,8 @@ def golden_cases():
         ("nks_bump_6x2x16_6", bump, "nks", (6, 30, 60, 1.0, 1e-10)),
         # global time step, Barth-Jespersen, GMRES restarts and its iteration cap
         ("nks_bump_bj_global_4", bump_bj, "nks", (4, 10, 25, 5.0, 1e-10)),
+        # supersonic, first order, inexact Newton (GMRES tolerance 0.1): converges to 1e-10
+        ("nks_bump_m14_converged", bump_m14, "nks", (30, 30, 120, 10.0, 1e-10, 0.1)),
     ]
 
 

@@ -1,0 +1,63 @@
+"""GPU mixed-precision path (E2D_PREC_FP32: least-squares reconstruction,
+limiter and Roe flux in FP32; geometry, flux divergence, RK accumulation,
+CFL and norms in FP64) against the reference's FP64 golden vectors.
+
+Stated tolerances (float has a 6e-8 unit round-off; a residual is a
+difference of fluxes, so its relative error is larger where fluxes cancel):
+
+* residual, per cell: helpers.rel_err <= 1e-3 (measured: 5e-6 .. 3e-5 on
+  Cartesian grids, 3e-4 on the curvilinear grid, where the cell-centroid
+  offsets entering the float gradients are least regular);
+* explicit runs: relative L2 error of density and total energy over the
+  interior after the fixture's steps <= 1e-5;
+* the FP32 path must really differ from FP64 (error > 1e-12), i.e. it is
+  not the FP64 kernel.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from cffc_b200 import capi
+from helpers import fixtures, load, rel_err
+
+pytestmark = pytest.mark.gpu
+
+FP32 = 1
+
+
+def fp32(bs):
+    return dataclasses.replace(bs, scheme=dataclasses.replace(bs.scheme, precision=FP32))
+
+
+def l2_rel(x, ref):
+    return float(np.sqrt(np.sum((x - ref) ** 2) / np.sum(ref ** 2)))
+
+
+@pytest.mark.parametrize("name", fixtures("residual"))
+def test_fp32_residual_close_to_reference(name):
+    bs, ref, _, lean = load(name)
+    h = capi.Handle(fp32(bs))
+    h.set_state()
+    dUdt = h.residual()
+    h.close()
+    got = bs.interior(dUdt)
+    want = ref["dUdt"] if lean else bs.interior(ref["dUdt"])
+    err = rel_err(got, want)
+    assert 1e-12 < err <= 1e-3, err
+
+
+@pytest.mark.parametrize("name", fixtures("explicit"))
+def test_fp32_explicit_density_energy_l2(name):
+    bs, ref, steps, lean = load(name)
+    h = capi.Handle(fp32(bs))
+    h.set_state()
+    rc, _ = h.rk_steps(steps)
+    _, U = h.get_state()
+    h.close()
+    assert rc == 0
+    want = ref["U"] if lean else bs.interior(ref["U"])
+    got = bs.interior(U)
+    for v in (0, 3):
+        err = l2_rel(got[:, v], want[:, v])
+        assert 1e-12 < err <= 1e-5, (v, err)

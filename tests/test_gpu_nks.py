@@ -8,16 +8,22 @@ device sums them in a fixed two-level tree, so the two differ in the last
 bits of every reduction and the Krylov recurrences carry that forward.  How
 far round-off alone moves the reference's history is measured by the
 fixture itself: the reference run again from the initial density scaled by
-(1 + 2^-46) ("pert_").  For every quantity the device result must lie
-within ENVELOPE times that self-divergence of the reference, with a floor:
+(1 + 2^-46) ("pert_").  A round-off difference grows along the Newton
+sequence, so the envelope of step k is the largest self-divergence of the
+reference over steps 0..k.  For every quantity the device result must lie
+within ENVELOPE times that envelope, with a floor:
 
 * per Newton step: L2 norm, ratio, CFL and GMRES resid0, floor 1e-8
   relative (the reference prints 10 significant digits);
-* GMRES inner iterations: equal (the perturbed reference run matches too);
+* GMRES inner iterations: equal, up to the first step at which the
+  perturbed reference run's count differs (after it, the counts are
+  round-off-sensitive for the reference itself);
 * GMRES final relative residual: floor 1e-6 relative and 10x the envelope
   (RELRES_ENVELOPE): it is the end value of a GMRES recurrence that, on the
   later steps, stops at its iteration cap unconverged, and one perturbed run
   underestimates its spread (the device has been seen at up to 17x);
+* converged runs: the same number of Newton steps, and the final L2 within
+  the envelope of the whole run;
 * final conserved state: helpers.rel_err, floor 1e-10.
 """
 import dataclasses
@@ -39,11 +45,12 @@ RELRES_ENVELOPE = 100.0
 def run(name, precision):
     bs, ref, steps, _ = load(name)
     bs = dataclasses.replace(bs, scheme=dataclasses.replace(bs.scheme, precision=precision))
-    max_newton, restart, max_gmres, cfl0, tol = ref["params"]
+    max_newton, restart, max_gmres, cfl0, tol = ref["params"][:5]
+    gmres_tol = float(ref["params"][5]) if len(ref["params"]) > 5 else 1e-5
     h = capi.Handle(bs)
     h.set_state()
     p = capi.nks_params(int(max_newton), gmres_restart=int(restart), max_gmres=int(max_gmres),
-                        overall_tol=float(tol), cfl0=float(cfl0))
+                        overall_tol=float(tol), cfl0=float(cfl0), gmres_tol=gmres_tol)
     rc, hist = h.nks(p)
     _, U = h.get_state()
     h.close()
@@ -60,21 +67,35 @@ def test_nks_matches_reference(name, precision):
     bs, ref, rc, hist, U = run(name, precision)
     assert rc == 0
     newton, gmres = ref["newton"], ref["gmres"]
-    assert len(hist) == len(newton)
     pn, pg = ref["pert_newton"], ref["pert_gmres"]
+    tol = ref["params"][4]
+    converged = ref["final"][2] <= tol
+    # the reference prints a Newton line only for steps it takes; a converged
+    # run ends with one more evaluation, which the history records
+    assert len(hist) == len(newton) + (1 if converged else 0)
     rows, bad = [], []
-    for k, st in enumerate(hist):
+    floor = [1e-8, 1e-8, 1e-8, 1e-8, 1e-6]
+    env = [ENVELOPE] * 4 + [RELRES_ENVELOPE]
+    span = [0.0] * 5           # running max of the reference's self-divergence
+    chaotic = False            # the perturbed reference's GMRES count has differed
+    for k, st in enumerate(hist[:len(newton)]):
         got = [st["l2"], st["ratio"], st["cfl"], st["gmres_resid0"], st["gmres_relres"]]
         want = [newton[k, 0], newton[k, 1], newton[k, 2], gmres[k, 1], gmres[k, 3]]
         pert = [pn[k, 0], pn[k, 1], pn[k, 2], pg[k, 1], pg[k, 3]]
-        floor = [1e-8, 1e-8, 1e-8, 1e-8, 1e-6]
+        span = [max(sp, rel(p, w)) for sp, p, w in zip(span, pert, want)]
         devs = [rel(g, w) for g, w in zip(got, want)]
-        env = [ENVELOPE] * 4 + [RELRES_ENVELOPE]
-        lims = [max(f, e * rel(p, w)) for f, e, p, w in zip(floor, env, pert, want)]
+        lims = [max(f, e * sp) for f, e, sp in zip(floor, env, span)]
         rows.append((k, st["gmres_iters"] - int(gmres[k, 0])) + tuple(devs))
         bad += [(k, q) for q in range(5) if not devs[q] <= lims[q]]
-        if st["gmres_iters"] != int(gmres[k, 0]):
+        chaotic = chaotic or int(pg[k, 0]) != int(gmres[k, 0])
+        if st["gmres_iters"] != int(gmres[k, 0]) and not chaotic:
             bad.append((k, "iters"))
+    if converged:
+        last = hist[-1]
+        assert last["ratio"] <= tol and last["gmres_iters"] == 0
+        lim = max(1e-8, ENVELOPE * max(span[0], rel(ref["pert_final"][1], ref["final"][1])))
+        if not rel(last["l2"], ref["final"][1]) <= lim:
+            bad.append(("final", last["l2"], ref["final"][1], lim))
     u_err = rel_err(bs.interior(U), bs.interior(ref["U"]))
     u_lim = max(1e-10, ENVELOPE * rel_err(bs.interior(ref["pert_U"]), bs.interior(ref["U"])))
     table = "\n".join("step %d: iters %+d l2 %.1e ratio %.1e cfl %.1e resid0 %.1e relres %.1e" % r for r in rows)
