@@ -3,7 +3,9 @@
 Per-file flags matter: the exact FP64 kernels (and the ghost-fill, time-step,
 norm and state-conversion kernels every path shares) are compiled with
 -fmad=false so they round as the reference's x86-64 build does; the fast
-FP64 kernels are compiled with contraction on.
+FP64 kernels are compiled with contraction on.  The C++ host layer
+(cffc_b200/host, include/cffc_euler2d.hpp) is compiled with the host compiler
+and linked into the same library.
 """
 from __future__ import annotations
 
@@ -16,6 +18,10 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcffc_e2d.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CXX = os.environ.get("CXX", "g++")
+HOST = os.path.join(HERE, "host")
+ROOT_DIR = os.path.dirname(HERE)
+HOST_SOURCES = ["euler2d_host.cc"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
@@ -51,6 +57,17 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
             cmd = [NVCC, *ARCH, *COMMON, *flags, "-c", s, "-o", o]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
+    # C++ host layer (include/cffc_euler2d.hpp): plain host code
+    inc = os.path.join(ROOT_DIR, "include")
+    for src in HOST_SOURCES:
+        s = os.path.join(HOST, src)
+        o = os.path.join(BUILD, src.replace(".cc", ".o"))
+        objs.append(o)
+        if _newer(o, [s, __file__, os.path.join(inc, "cffc_euler2d.hpp"), os.path.join(inc, "cffc_e2d.h")]):
+            cmd = [CXX, "-O2", "-std=c++17", "-fPIC", "-I", inc, "-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)

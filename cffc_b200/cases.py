@@ -24,6 +24,7 @@ Seeds use numpy's PCG64 generator; the draw order is documented per builder.
 from __future__ import annotations
 
 import dataclasses
+import os
 import struct
 
 import numpy as np
@@ -346,3 +347,42 @@ def write_case(path: str, bs: BlockSet, W: np.ndarray | None = None) -> None:
             for a in (bs.wo_w, bs.wo_e, bs.wo_s, bs.wo_n):
                 f.write(a[b].astype("<f8").tobytes())
             f.write(np.ascontiguousarray(W[b]).astype("<f8").tobytes())
+
+
+def read_case(path: str) -> BlockSet:
+    """Reads a case file written by write_case (or by the C++ host layer's
+    Write_Case_File) back into a BlockSet."""
+    buf = open(path, "rb").read()
+    magic, version = struct.unpack_from("<2i", buf, 0)
+    if magic != _MAGIC or version != 1:
+        raise ValueError(f"{path}: not a case file")
+    nblk, nci, ncj, ng = struct.unpack_from("<4i", buf, 8)
+    limiter, flux, n_stage, local_dt, _, nbi, nbj, periodic = struct.unpack_from("<8i", buf, 24)
+    cfl = struct.unpack_from("<d", buf, 56)[0]
+    NCi, NCj = nci + 2 * ng, ncj + 2 * ng
+    NNi, NNj = NCi + 1, NCj + 1
+    off = 88
+    arrays = {k: [] for k in ("neighbour", "bc_w", "bc_e", "bc_s", "bc_n", "node_x", "node_y",
+                              "wo_w", "wo_e", "wo_s", "wo_n", "W")}
+
+    def take(dtype, shape):
+        nonlocal off
+        n = int(np.prod(shape))
+        a = np.frombuffer(buf, dtype=dtype, count=n, offset=off).reshape(shape)
+        off += n * np.dtype(dtype).itemsize
+        return a.copy()
+
+    for _ in range(nblk):
+        arrays["neighbour"].append(take("<i4", (8,)))
+        for k, n in (("bc_w", NCj), ("bc_e", NCj), ("bc_s", NCi), ("bc_n", NCi)):
+            arrays[k].append(take("<i4", (n,)))
+        arrays["node_x"].append(take("<f8", (NNj, NNi)))
+        arrays["node_y"].append(take("<f8", (NNj, NNi)))
+        for k, n in (("wo_w", NCj), ("wo_e", NCj), ("wo_s", NCi), ("wo_n", NCi)):
+            arrays[k].append(take("<f8", (4, n)))
+        arrays["W"].append(take("<f8", (4, NCj, NCi)))
+    a = {k: np.stack(v) for k, v in arrays.items()}
+    scheme = Scheme(limiter=limiter, flux=flux, n_stage=n_stage, local_dt=local_dt, cfl=cfl)
+    return BlockSet(nci, ncj, a["neighbour"], a["bc_w"], a["bc_e"], a["bc_s"], a["bc_n"], a["node_x"],
+                    a["node_y"], a["wo_w"], a["wo_e"], a["wo_s"], a["wo_n"], a["W"], scheme,
+                    os.path.basename(path), ng, nbi, nbj, periodic).contiguous()

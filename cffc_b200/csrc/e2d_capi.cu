@@ -330,6 +330,22 @@ int e2d_norms(e2d_handle* h, double out[3]) {
   return 0;
 }
 
+int e2d_cfl(e2d_handle* h, double* dt, double* dtmin) {
+  if (!h) return E2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemsetAsync(h->step, 0, sizeof(int), h->stream));
+  CK(launch_slot_init(h->hist, h->step, 0, h->stream));
+  Blocks B = h->B;
+  B.local_dt = 1;  // every interior cell's step into B.dt
+  CK(launch_cfl(B, h->hist, h->step, h->stream));
+  double tmp[4];
+  CK(cudaMemcpyAsync(tmp, h->hist, sizeof(tmp), cudaMemcpyDeviceToHost, h->stream));
+  if (dt) CK(cudaMemcpyAsync(dt, h->B.dt, sizeof(double) * h->ncell, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (dtmin) *dtmin = tmp[0];
+  return 0;
+}
+
 int e2d_status(e2d_handle* h) {
   if (!h) return E2D_ERR_ARG;
   return check_status(h);

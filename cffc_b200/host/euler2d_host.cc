@@ -1,0 +1,626 @@
+// euler2d_host.cc — the C++ host surface of include/cffc_euler2d.hpp: the
+// reference's Euler2D state and block types, the input-deck parser of the
+// path, grid / initial-solution builders, and the solver driver, all on top
+// of the C ABI of cffc_e2d.h.  Host-side only: no CUDA code here.
+#include "cffc_euler2d.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <istream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace cffc_b200 {
+
+namespace {
+constexpr double HALF = 0.5;
+constexpr double PI = 3.14159265358979323846;
+constexpr int INVALID_INPUT_CODE = -1, EXECUTE_CODE = 1, TERMINATE_CODE = 2;
+}  // namespace
+
+// ---- states (Euler2DState.h:1055-1095, :1741-1760, :3414-3430) -------------
+double Euler2D_pState::g = 1.4;
+double Euler2D_pState::gm1 = 0.4;
+double Euler2D_pState::gm1i = 1.0 / 0.4;
+double Euler2D_pState::R = 287.0636;
+
+double Euler2D_pState::a() const { return std::sqrt(g * p / d); }
+double Euler2D_pState::h() const { return g * p / (gm1 * d) + HALF * (v.x * v.x + v.y * v.y); }
+double Euler2D_pState::E() const { return p * gm1i + HALF * d * (v.x * v.x + v.y * v.y); }
+Euler2D_cState Euler2D_pState::U() const { return Euler2D_cState(d, d * v.x, d * v.y, E()); }
+double& Euler2D_pState::operator[](int index) {
+  switch (index) {
+    case 1: return d;
+    case 2: return v.x;
+    case 3: return v.y;
+    default: return p;
+  }
+}
+const double& Euler2D_pState::operator[](int index) const {
+  return const_cast<Euler2D_pState*>(this)->operator[](index);
+}
+
+double Euler2D_cState::e() const { return E / d - HALF * (dv.x * dv.x + dv.y * dv.y) / (d * d); }
+Euler2D_pState Euler2D_cState::W() const {
+  return Euler2D_pState(d, dv.x / d, dv.y / d,
+                        Euler2D_pState::gm1 * (E - HALF * (dv.x * dv.x + dv.y * dv.y) / d));
+}
+double& Euler2D_cState::operator[](int index) {
+  switch (index) {
+    case 1: return d;
+    case 2: return dv.x;
+    case 3: return dv.y;
+    default: return E;
+  }
+}
+const double& Euler2D_cState::operator[](int index) const {
+  return const_cast<Euler2D_cState*>(this)->operator[](index);
+}
+
+// ---- block (Euler2D_Quad_Block::allocate, Euler2DQuad.h:655-760) -----------
+void Euler2D_Quad_Block::allocate(int Ni, int Nj, int Ng) {
+  Nghost = Ng;
+  NCi = Ni + 2 * Ng; ICl = Ng; ICu = Ni + Ng - 1;
+  NCj = Nj + 2 * Ng; JCl = Ng; JCu = Nj + Ng - 1;
+  W.assign(NCi, std::vector<Euler2D_pState>(NCj));
+  U.assign(NCi, std::vector<Euler2D_cState>(NCj));
+  dUdt.assign(NCi, std::vector<Euler2D_cState>(NCj, Euler2D_cState(0, 0, 0, 0)));
+  dt.assign(NCi, std::vector<double>(NCj, 0.0));
+  WoN.assign(NCi, Euler2D_pState()); WoS.assign(NCi, Euler2D_pState());
+  WoE.assign(NCj, Euler2D_pState()); WoW.assign(NCj, Euler2D_pState());
+  Grid.Nghost = Ng;
+  Grid.NNi = NCi + 1; Grid.NNj = NCj + 1;
+  Grid.Node.assign(Grid.NNi, std::vector<Vector2D>(Grid.NNj));
+  Grid.BCtypeN.assign(NCi, E2D_BC_NONE); Grid.BCtypeS.assign(NCi, E2D_BC_NONE);
+  Grid.BCtypeE.assign(NCj, E2D_BC_NONE); Grid.BCtypeW.assign(NCj, E2D_BC_NONE);
+}
+
+// ---- input deck --------------------------------------------------------------
+Euler2D_Input_Parameters::Euler2D_Input_Parameters() {
+  // NKS_Input_Parameters defaults (NKSInput2D.h:125-172)
+  NKS.max_newton = 0;
+  NKS.gmres_restart = 30;
+  NKS.max_gmres = 100;
+  NKS.overall_tol = 1e-5;
+  NKS.cfl0 = 1.0;
+  NKS.gmres_tol_initial = 1e-5;
+  NKS.gmres_tol_final = 1e-5;
+  NKS.epsilon0 = 1e-6;
+  NKS.min_ratio = 1e-10;
+  set_freestream();
+}
+
+// Wo from Pressure, Temperature, Mach_Number and Flow_Angle (the updates of
+// Euler2DInput.cc:2558-2611).
+void Euler2D_Input_Parameters::set_freestream() {
+  Wo = Euler2D_pState(Pressure / (Euler2D_pState::R * Temperature), 0.0, 0.0, Pressure);
+  Wo.v.x = Mach_Number * Wo.a() * std::cos(2.0 * PI * Flow_Angle / 360.00);
+  Wo.v.y = Mach_Number * Wo.a() * std::sin(2.0 * PI * Flow_Angle / 360.00);
+}
+
+namespace {
+
+// Get_Next_Input_Control_Parameter (Euler2DInput.cc:100-144): the first
+// token (up to blank, tab or '=') of the next line that is neither empty nor
+// a '#' comment.
+bool next_token(std::istream& in, int& line, std::string& tok) {
+  std::string buf;
+  while (std::getline(in, buf)) {
+    ++line;
+    size_t i = buf.find_first_not_of(" \t");
+    if (i == std::string::npos || buf[i] == '#' || buf[i] == '\r') continue;
+    size_t e = buf.find_first_of(" \t=\r", i);
+    tok = buf.substr(i, e == std::string::npos ? std::string::npos : e - i);
+    return true;
+  }
+  return false;
+}
+
+// A numeric value on the next line (IP.Input_File >> value; getline).
+template <class T> bool next_value(std::istream& in, int& line, T& v) {
+  std::string buf;
+  if (!std::getline(in, buf)) return false;
+  ++line;
+  std::istringstream ss(buf);
+  return static_cast<bool>(ss >> v);
+}
+
+}  // namespace
+
+// Parse_Next_Input_Control_Parameter (Euler2DInput.cc:1759-3920,
+// NKSInput2D.h:378-640) for the keywords of this path.  Returns 0 for a
+// keyword taken, EXECUTE_CODE / TERMINATE_CODE, or INVALID_INPUT_CODE.
+int Parse_Next_Input_Control_Parameter(Euler2D_Input_Parameters& IP, std::istream& in, const std::string& code) {
+  int& L = IP.Line_Number;
+  std::string s;
+  auto str = [&](std::string& dst) { return next_token(in, L, dst) ? 0 : INVALID_INPUT_CODE; };
+  if (code == "Execute") return EXECUTE_CODE;
+  if (code == "Terminate") return TERMINATE_CODE;
+  if (code == "Continue" || code == "Write_Output" || code == "Write_Output_Cells") return 0;
+  if (code == "Time_Integration_Type") {
+    if (str(IP.Time_Integration_Type)) return INVALID_INPUT_CODE;
+    const std::string& t = IP.Time_Integration_Type;
+    if (t == "Explicit_Euler") IP.N_Stage = 1;
+    else if (t == "Explicit_Predictor_Corrector") IP.N_Stage = 2;
+    else if (t == "Explicit_Runge_Kutta") IP.N_Stage = 4;
+    else return INVALID_INPUT_CODE;  // optimal smoothing, multigrid, DTS: outside this path
+    return 0;
+  }
+  if (code == "Reconstruction_Type") {
+    if (str(IP.Reconstruction_Type)) return INVALID_INPUT_CODE;
+    return IP.Reconstruction_Type == "Least_Squares" ? 0 : INVALID_INPUT_CODE;
+  }
+  if (code == "Limiter_Type") {
+    if (str(IP.Limiter_Type)) return INVALID_INPUT_CODE;
+    const std::string& t = IP.Limiter_Type;
+    if (t == "One") IP.i_Limiter = E2D_LIMITER_ONE;
+    else if (t == "Zero") IP.i_Limiter = E2D_LIMITER_ZERO;
+    else if (t == "Barth_Jespersen") IP.i_Limiter = E2D_LIMITER_BARTH_JESPERSEN;
+    else if (t == "Venkatakrishnan") IP.i_Limiter = E2D_LIMITER_VENKATAKRISHNAN;
+    else return INVALID_INPUT_CODE;
+    return 0;
+  }
+  if (code == "Flux_Function_Type") {
+    if (str(IP.Flux_Function_Type)) return INVALID_INPUT_CODE;
+    return IP.Flux_Function_Type == "Roe" ? 0 : INVALID_INPUT_CODE;
+  }
+  if (code == "ICs_Type") {
+    if (str(IP.ICs_Type)) return INVALID_INPUT_CODE;
+    return (IP.ICs_Type == "Uniform" || IP.ICs_Type == "Constant") ? 0 : INVALID_INPUT_CODE;
+  }
+  if (code == "Grid_Type") {
+    if (str(IP.Grid_Type)) return INVALID_INPUT_CODE;
+    const std::string& t = IP.Grid_Type;
+    return (t == "Rectangular_Box" || t == "Periodic_Box" || t == "Sine_Squared_Bump_Channel") ? 0
+                                                                                                : INVALID_INPUT_CODE;
+  }
+  if (code == "Output_File_Name") return str(IP.Output_File_Name);
+  if (code == "GPU_Precision") {
+    if (str(s)) return INVALID_INPUT_CODE;
+    if (s == "FP64") IP.Precision = E2D_PREC_FP64;
+    else if (s == "FP64_Exact") IP.Precision = E2D_PREC_FP64_EXACT;
+    else if (s == "FP32") IP.Precision = E2D_PREC_FP32;
+    else return INVALID_INPUT_CODE;
+    return 0;
+  }
+  // numeric keywords: (name, pointer, validity)
+  auto num_i = [&](int& v, int lo) { return (next_value(in, L, v) && v >= lo) ? 0 : INVALID_INPUT_CODE; };
+  auto num_d = [&](double& v, bool positive) {
+    return (next_value(in, L, v) && (!positive || v > 0.0)) ? 0 : INVALID_INPUT_CODE;
+  };
+  if (code == "N_Stage") {
+    int rc = num_i(IP.N_Stage, 0);
+    return rc ? rc : ((IP.N_Stage == 1 || IP.N_Stage == 2) ? 0 : INVALID_INPUT_CODE);
+  }
+  if (code == "CFL_Number") return num_d(IP.CFL_Number, true);
+  if (code == "Time_Accurate") return num_i(IP.Time_Accurate, 0);
+  if (code == "Local_Time_Stepping") {
+    int rc = num_i(IP.Local_Time_Stepping, 0);
+    if (IP.Local_Time_Stepping > 1) IP.Local_Time_Stepping = 1;  // scalar local time stepping
+    return rc;
+  }
+  if (code == "Maximum_Number_of_Time_Steps") return num_i(IP.Maximum_Number_of_Time_Steps, 0);
+  if (code == "Time_Max") {
+    int rc = num_d(IP.Time_Max, false);
+    IP.Time_Max = IP.Time_Max / 1000.0;  // ms -> s
+    return rc;
+  }
+  if (code == "Box_Width") return num_d(IP.Box_Width, true);
+  if (code == "Box_Height") return num_d(IP.Box_Height, true);
+  if (code == "Bump_Height") return num_d(IP.Bump_Height, false);
+  if (code == "Number_of_Cells_Idir") return num_i(IP.Number_of_Cells_Idir, 1);
+  if (code == "Number_of_Cells_Jdir") return num_i(IP.Number_of_Cells_Jdir, 1);
+  if (code == "Number_of_Blocks_Idir") return num_i(IP.Number_of_Blocks_Idir, 1);
+  if (code == "Number_of_Blocks_Jdir") return num_i(IP.Number_of_Blocks_Jdir, 1);
+  if (code == "Number_of_Ghost_Cells") {
+    int rc = num_i(IP.Number_of_Ghost_Cells, 1);
+    return rc ? rc : (IP.Number_of_Ghost_Cells == 2 ? 0 : INVALID_INPUT_CODE);
+  }
+  if (code == "Mach_Number") {
+    int rc = num_d(IP.Mach_Number, false);
+    IP.set_freestream();
+    return rc;
+  }
+  if (code == "Flow_Angle") {
+    int rc = num_d(IP.Flow_Angle, false);
+    IP.set_freestream();
+    return rc;
+  }
+  if (code == "Pressure") {
+    int rc = num_d(IP.Pressure, true);
+    IP.Pressure = IP.Pressure * 1000.0;  // kPa -> Pa
+    IP.set_freestream();
+    return rc;
+  }
+  if (code == "Temperature") {
+    int rc = num_d(IP.Temperature, true);
+    IP.set_freestream();
+    return rc;
+  }
+  // NKS_Input_Parameters::Parse_Next_Input_Control_Parameter (NKSInput2D.h:378-640)
+  e2d_nks_params& N = IP.NKS;
+  if (code == "Maximum_Number_of_NKS_Iterations") return num_i(N.max_newton, 0);
+  if (code == "NKS_Overall_Tolerance") return num_d(N.overall_tol, false);
+  if (code == "NKS_Finite_Time_Step_Initial_CFL") return num_d(N.cfl0, true);
+  if (code == "Maximum_Number_of_GMRES_Iterations") return num_i(N.max_gmres, 1);
+  if (code == "GMRES_Restart") return num_i(N.gmres_restart, 1);
+  if (code == "GMRES_Tolerance") {
+    int rc = num_d(N.gmres_tol_initial, true);
+    N.gmres_tol_final = N.gmres_tol_initial;  // backward compatible keyword
+    return rc;
+  }
+  if (code == "GMRES_Initial_Tolerance") return num_d(N.gmres_tol_initial, true);
+  if (code == "GMRES_Final_Tolerance") return num_d(N.gmres_tol_final, true);
+  if (code == "GMRES_Epsilon_Naught") return num_d(N.epsilon0, true);
+  if (code == "NKS_Min_Finite_Time_Step_Norm_Ratio") return num_d(N.min_ratio, true);
+  // Any other keyword belongs to parts of the reference outside this path:
+  // its value line is skipped and the keyword recorded.
+  IP.Ignored.push_back(code);
+  std::string skip;
+  std::getline(in, skip);
+  ++L;
+  return 0;
+}
+
+int Euler2D_Input_Parameters::Process_Input_Control_Parameter_File(const std::string& path) {
+  std::ifstream in(path);
+  if (!in.good()) return -1;
+  Line_Number = 0;
+  std::string code;
+  while (next_token(in, Line_Number, code)) {
+    const int rc = Parse_Next_Input_Control_Parameter(*this, in, code);
+    if (rc == EXECUTE_CODE || rc == TERMINATE_CODE) break;
+    if (rc == INVALID_INPUT_CODE) return Line_Number > 0 ? Line_Number : 1;
+  }
+  set_freestream();
+  return 0;
+}
+
+// ---- grids and initial solution -----------------------------------------------
+int Create_Initial_Solution_Blocks(const Euler2D_Input_Parameters& IP, std::vector<Euler2D_Quad_Block>& blocks,
+                                   std::vector<int>& neighbour) {
+  const int nbi = IP.Number_of_Blocks_Idir, nbj = IP.Number_of_Blocks_Jdir, ng = IP.Number_of_Ghost_Cells;
+  if (IP.Number_of_Cells_Idir % nbi || IP.Number_of_Cells_Jdir % nbj) return 1;
+  const int nci = IP.Number_of_Cells_Idir / nbi, ncj = IP.Number_of_Cells_Jdir / nbj;
+  const int Nx = IP.Number_of_Cells_Idir, Ny = IP.Number_of_Cells_Jdir;
+  const bool periodic = IP.Grid_Type == "Periodic_Box";
+  const bool bump = IP.Grid_Type == "Sine_Squared_Bump_Channel";
+  int bcW = E2D_BC_REFLECTION, bcE = E2D_BC_REFLECTION, bcS = E2D_BC_REFLECTION, bcN = E2D_BC_REFLECTION;
+  if (periodic) bcW = bcE = bcS = bcN = E2D_BC_NONE;
+  if (bump) bcW = bcE = E2D_BC_CHARACTERISTIC;
+  // node map of global node indices (ghost nodes continue the same map)
+  auto node = [&](int I, int J) -> Vector2D {
+    const double x = -0.5 * IP.Box_Width + IP.Box_Width * double(I) / double(Nx);
+    if (!bump) return Vector2D(x, -0.5 * IP.Box_Height + IP.Box_Height * double(J) / double(Ny));
+    // channel [-1.5, 1.5] x [0, 1] over a sin^2 bump on |x| <= 0.5
+    const double xb = -1.5 + 3.0 * double(I) / double(Nx);
+    const double yw = std::fabs(xb) <= 0.5 ? IP.Bump_Height * std::pow(std::sin(PI * (xb + 0.5)), 2) : 0.0;
+    const double eta = double(J) / double(Ny);
+    return Vector2D(xb, yw + eta * (1.0 - yw));
+  };
+  static const int off[8][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}, {-1, -1}, {1, -1}, {-1, 1}, {1, 1}};
+  blocks.assign(size_t(nbi) * nbj, Euler2D_Quad_Block());
+  neighbour.assign(size_t(8) * nbi * nbj, -1);
+  for (int bj = 0; bj < nbj; ++bj)
+    for (int bi = 0; bi < nbi; ++bi) {
+      const int b = bj * nbi + bi;
+      Euler2D_Quad_Block& B = blocks[b];
+      B.allocate(nci, ncj, ng);
+      for (int k = 0; k < 8; ++k) {
+        int ni = bi + off[k][0], nj = bj + off[k][1];
+        if (periodic) { ni = (ni + nbi) % nbi; nj = (nj + nbj) % nbj; }
+        if (ni >= 0 && ni < nbi && nj >= 0 && nj < nbj) neighbour[8 * b + k] = nj * nbi + ni;
+      }
+      for (int i = 0; i < B.Grid.NNi; ++i)
+        for (int j = 0; j < B.Grid.NNj; ++j) B.Grid.Node[i][j] = node(bi * nci + i - ng, bj * ncj + j - ng);
+      if (bi == 0) std::fill(B.Grid.BCtypeW.begin(), B.Grid.BCtypeW.end(), bcW);
+      if (bi == nbi - 1) std::fill(B.Grid.BCtypeE.begin(), B.Grid.BCtypeE.end(), bcE);
+      if (bj == 0) std::fill(B.Grid.BCtypeS.begin(), B.Grid.BCtypeS.end(), bcS);
+      if (bj == nbj - 1) std::fill(B.Grid.BCtypeN.begin(), B.Grid.BCtypeN.end(), bcN);
+      for (auto& w : B.WoN) w = IP.Wo;
+      for (auto& w : B.WoS) w = IP.Wo;
+      for (auto& w : B.WoE) w = IP.Wo;
+      for (auto& w : B.WoW) w = IP.Wo;
+      // ICs_Type Uniform / Constant: the freestream everywhere (ICs,
+      // Euler2DQuadSingleBlock.cc:1689)
+      for (int i = 0; i < B.NCi; ++i)
+        for (int j = 0; j < B.NCj; ++j) {
+          B.W[i][j] = IP.Wo;
+          B.U[i][j] = IP.Wo.U();
+        }
+    }
+  return 0;
+}
+
+// ---- device block set --------------------------------------------------------
+namespace {
+
+struct Packed {
+  std::vector<int32_t> neighbour, bcw, bce, bcs, bcn;
+  std::vector<double> X, Y, wow, woe, wos, won;
+  e2d_blocks_desc desc{};
+};
+
+void pack_blocks(const std::vector<Euler2D_Quad_Block>& blocks, const std::vector<int>& neighbour, Packed& P) {
+  const int nblk = int(blocks.size());
+  const Euler2D_Quad_Block& B0 = blocks[0];
+  const int NCi = B0.NCi, NCj = B0.NCj, NNi = NCi + 1, NNj = NCj + 1;
+  P.neighbour.assign(neighbour.begin(), neighbour.end());
+  P.bcw.resize(size_t(nblk) * NCj); P.bce.resize(size_t(nblk) * NCj);
+  P.bcs.resize(size_t(nblk) * NCi); P.bcn.resize(size_t(nblk) * NCi);
+  P.X.resize(size_t(nblk) * NNi * NNj); P.Y.resize(P.X.size());
+  P.wow.resize(size_t(nblk) * 4 * NCj); P.woe.resize(P.wow.size());
+  P.wos.resize(size_t(nblk) * 4 * NCi); P.won.resize(P.wos.size());
+  for (int b = 0; b < nblk; ++b) {
+    const Euler2D_Quad_Block& B = blocks[b];
+    for (int j = 0; j < NCj; ++j) {
+      P.bcw[size_t(b) * NCj + j] = B.Grid.BCtypeW[j];
+      P.bce[size_t(b) * NCj + j] = B.Grid.BCtypeE[j];
+      for (int v = 1; v <= 4; ++v) {
+        P.wow[(size_t(b) * 4 + v - 1) * NCj + j] = B.WoW[j][v];
+        P.woe[(size_t(b) * 4 + v - 1) * NCj + j] = B.WoE[j][v];
+      }
+    }
+    for (int i = 0; i < NCi; ++i) {
+      P.bcs[size_t(b) * NCi + i] = B.Grid.BCtypeS[i];
+      P.bcn[size_t(b) * NCi + i] = B.Grid.BCtypeN[i];
+      for (int v = 1; v <= 4; ++v) {
+        P.wos[(size_t(b) * 4 + v - 1) * NCi + i] = B.WoS[i][v];
+        P.won[(size_t(b) * 4 + v - 1) * NCi + i] = B.WoN[i][v];
+      }
+    }
+    for (int j = 0; j < NNj; ++j)
+      for (int i = 0; i < NNi; ++i) {
+        P.X[(size_t(b) * NNj + j) * NNi + i] = B.Grid.Node[i][j].x;
+        P.Y[(size_t(b) * NNj + j) * NNi + i] = B.Grid.Node[i][j].y;
+      }
+  }
+  e2d_blocks_desc& d = P.desc;
+  d.nblk = nblk; d.nci = NCi - 2 * B0.Nghost; d.ncj = NCj - 2 * B0.Nghost; d.ng = B0.Nghost;
+  d.neighbour = P.neighbour.data();
+  d.bc_w = P.bcw.data(); d.bc_e = P.bce.data(); d.bc_s = P.bcs.data(); d.bc_n = P.bcn.data();
+  d.node_x = P.X.data(); d.node_y = P.Y.data();
+  d.wo_w = P.wow.data(); d.wo_e = P.woe.data(); d.wo_s = P.wos.data(); d.wo_n = P.won.data();
+}
+
+e2d_scheme scheme_of(const Euler2D_Input_Parameters& IP) {
+  e2d_scheme s{};
+  s.limiter = IP.i_Limiter;
+  s.flux = E2D_FLUX_ROE;
+  s.n_stage = IP.N_Stage;
+  s.local_dt = IP.Local_Time_Stepping ? 1 : 0;
+  s.precision = IP.Precision;
+  s.cfl = IP.CFL_Number;
+  s.gamma = Euler2D_pState::g;
+  return s;
+}
+
+// host blocks <-> SoA [nblk][4][NCj][NCi]
+void gather_W(const std::vector<Euler2D_Quad_Block>& blocks, std::vector<double>& W) {
+  const int NCi = blocks[0].NCi, NCj = blocks[0].NCj;
+  W.resize(blocks.size() * 4 * size_t(NCi) * NCj);
+  for (size_t b = 0; b < blocks.size(); ++b)
+    for (int v = 1; v <= 4; ++v)
+      for (int j = 0; j < NCj; ++j)
+        for (int i = 0; i < NCi; ++i) W[((b * 4 + v - 1) * NCj + j) * NCi + i] = blocks[b].W[i][j][v];
+}
+
+}  // namespace
+
+Euler2D_Device_Blocks::Euler2D_Device_Blocks(std::vector<Euler2D_Quad_Block>& blocks, const std::vector<int>& neighbour,
+                                             const Euler2D_Input_Parameters& IP, int device)
+    : blocks_(blocks) {
+  if (blocks.empty()) return;
+  Packed P;
+  pack_blocks(blocks, neighbour, P);
+  const e2d_scheme s = scheme_of(IP);
+  int err = 0;
+  h_ = e2d_create(&P.desc, &s, device, &err);
+  nci_ = P.desc.nci; ncj_ = P.desc.ncj; ng_ = P.desc.ng;
+  if (h_) upload();
+}
+
+Euler2D_Device_Blocks::~Euler2D_Device_Blocks() {
+  if (h_) e2d_destroy(h_);
+}
+
+int Euler2D_Device_Blocks::upload() {
+  if (!h_) return E2D_ERR_ARG;
+  std::vector<double> W;
+  gather_W(blocks_, W);
+  return e2d_set_state(h_, W.data());
+}
+
+int Euler2D_Device_Blocks::download() {
+  if (!h_) return E2D_ERR_ARG;
+  const int NCi = blocks_[0].NCi, NCj = blocks_[0].NCj;
+  const size_t n = blocks_.size() * 4 * size_t(NCi) * NCj;
+  std::vector<double> W(n), U(n);
+  const int rc = e2d_get_state(h_, W.data(), U.data());
+  if (rc) return rc;
+  for (size_t b = 0; b < blocks_.size(); ++b)
+    for (int j = 0; j < NCj; ++j)
+      for (int i = 0; i < NCi; ++i) {
+        Euler2D_Quad_Block& B = blocks_[b];
+        for (int v = 1; v <= 4; ++v) {
+          const size_t q = ((b * 4 + v - 1) * NCj + j) * NCi + i;
+          B.W[i][j][v] = W[q];
+          B.U[i][j][v] = U[q];
+        }
+      }
+  return 0;
+}
+
+int Euler2D_Device_Blocks::residual() {
+  if (!h_) return E2D_ERR_ARG;
+  const int NCi = blocks_[0].NCi, NCj = blocks_[0].NCj;
+  std::vector<double> R(blocks_.size() * 4 * size_t(NCi) * NCj);
+  const int rc = e2d_residual(h_, R.data());
+  if (rc) return rc;
+  for (size_t b = 0; b < blocks_.size(); ++b)
+    for (int v = 1; v <= 4; ++v)
+      for (int j = 0; j < NCj; ++j)
+        for (int i = 0; i < NCi; ++i) blocks_[b].dUdt[i][j][v] = R[((b * 4 + v - 1) * NCj + j) * NCi + i];
+  return 0;
+}
+
+int Euler2D_Device_Blocks::explicit_steps(int n, std::vector<double>* hist) {
+  if (!h_) return E2D_ERR_ARG;
+  if (hist) hist->assign(size_t(4) * (n > 0 ? n : 1), 0.0);
+  return e2d_rk_steps(h_, n, hist ? hist->data() : nullptr);
+}
+
+int Euler2D_Device_Blocks::nks(const e2d_nks_params& p, std::vector<e2d_nks_step>* hist) {
+  if (!h_) return E2D_ERR_ARG;
+  std::vector<e2d_nks_step> local(p.max_newton > 0 ? p.max_newton : 1);
+  int n = 0;
+  const int rc = e2d_nks(h_, &p, local.data(), &n);
+  if (hist) hist->assign(local.begin(), local.begin() + n);
+  return rc;
+}
+
+int Write_Case_File(const std::string& path, const std::vector<Euler2D_Quad_Block>& blocks,
+                    const std::vector<int>& neighbour, const Euler2D_Input_Parameters& IP) {
+  if (blocks.empty()) return E2D_ERR_ARG;
+  Packed P;
+  pack_blocks(blocks, neighbour, P);
+  std::vector<double> W;
+  gather_W(blocks, W);
+  FILE* f = fopen(path.c_str(), "wb");
+  if (!f) return E2D_ERR_ARG;
+  const e2d_blocks_desc& d = P.desc;
+  const e2d_scheme s = scheme_of(IP);
+  const int NCi = d.nci + 2 * d.ng, NCj = d.ncj + 2 * d.ng, NNi = NCi + 1, NNj = NCj + 1;
+  const int32_t head[14] = {0x43443245, 1, d.nblk, d.nci, d.ncj, d.ng, s.limiter, s.flux, s.n_stage, s.local_dt, 1,
+                            IP.Number_of_Blocks_Idir, IP.Number_of_Blocks_Jdir,
+                            IP.Grid_Type == "Periodic_Box" ? 1 : 0};
+  const double headf[4] = {s.cfl, 0.0, 0.0, 0.0};
+  fwrite(head, sizeof(int32_t), 14, f);
+  fwrite(headf, sizeof(double), 4, f);
+  for (int b = 0; b < d.nblk; ++b) {
+    fwrite(P.neighbour.data() + 8 * b, sizeof(int32_t), 8, f);
+    fwrite(P.bcw.data() + size_t(b) * NCj, sizeof(int32_t), NCj, f);
+    fwrite(P.bce.data() + size_t(b) * NCj, sizeof(int32_t), NCj, f);
+    fwrite(P.bcs.data() + size_t(b) * NCi, sizeof(int32_t), NCi, f);
+    fwrite(P.bcn.data() + size_t(b) * NCi, sizeof(int32_t), NCi, f);
+    fwrite(P.X.data() + size_t(b) * NNi * NNj, sizeof(double), size_t(NNi) * NNj, f);
+    fwrite(P.Y.data() + size_t(b) * NNi * NNj, sizeof(double), size_t(NNi) * NNj, f);
+    fwrite(P.wow.data() + size_t(b) * 4 * NCj, sizeof(double), size_t(4) * NCj, f);
+    fwrite(P.woe.data() + size_t(b) * 4 * NCj, sizeof(double), size_t(4) * NCj, f);
+    fwrite(P.wos.data() + size_t(b) * 4 * NCi, sizeof(double), size_t(4) * NCi, f);
+    fwrite(P.won.data() + size_t(b) * 4 * NCi, sizeof(double), size_t(4) * NCi, f);
+    fwrite(W.data() + size_t(b) * 4 * NCi * NCj, sizeof(double), size_t(4) * NCi * NCj, f);
+  }
+  return fclose(f) == 0 ? 0 : E2D_ERR_ARG;
+}
+
+// ---- single-block entry points ----------------------------------------------
+int dUdt_Residual_Evaluation(Euler2D_Quad_Block& SolnBlk, const Euler2D_Input_Parameters& IP) {
+  std::vector<Euler2D_Quad_Block> one(1, SolnBlk);
+  std::vector<int> nb(8, -1);
+  Euler2D_Device_Blocks dev(one, nb, IP);
+  if (!dev.handle()) return E2D_ERR_CUDA;
+  int rc = dev.residual();
+  if (rc) return rc;
+  SolnBlk.dUdt = one[0].dUdt;
+  return 0;
+}
+
+// CFL (Euler2DQuadSingleBlock.cc:3019-3080): the device evaluates every
+// interior cell's step into SolnBlk.dt; returns the block minimum (or a
+// negative library error).
+double CFL(Euler2D_Quad_Block& SolnBlk, const Euler2D_Input_Parameters& IP) {
+  std::vector<Euler2D_Quad_Block> one(1, SolnBlk);
+  std::vector<int> nb(8, -1);
+  Euler2D_Device_Blocks dev(one, nb, IP);
+  if (!dev.handle()) return E2D_ERR_CUDA;
+  const int NCi = SolnBlk.NCi, NCj = SolnBlk.NCj;
+  std::vector<double> dt(size_t(NCi) * NCj);
+  double dtmin = 0.0;
+  const int rc = e2d_cfl(dev.handle(), dt.data(), &dtmin);
+  if (rc) return rc;
+  for (int j = 0; j < NCj; ++j)
+    for (int i = 0; i < NCi; ++i) SolnBlk.dt[i][j] = dt[size_t(j) * NCi + i];
+  return dtmin;
+}
+
+double L1_Norm_Residual(const Euler2D_Quad_Block& B) {
+  double s = 0.0;
+  for (int j = B.JCl; j <= B.JCu; ++j)
+    for (int i = B.ICl; i <= B.ICu; ++i) s += std::fabs(B.dUdt[i][j].d);
+  return s;
+}
+double L2_Norm_Residual(const Euler2D_Quad_Block& B) {
+  double s = 0.0;
+  for (int j = B.JCl; j <= B.JCu; ++j)
+    for (int i = B.ICl; i <= B.ICu; ++i) s += B.dUdt[i][j].d * B.dUdt[i][j].d;
+  return std::sqrt(s);
+}
+double Max_Norm_Residual(const Euler2D_Quad_Block& B) {
+  double m = 0.0;
+  for (int j = B.JCl; j <= B.JCu; ++j)
+    for (int i = B.ICl; i <= B.ICu; ++i) m = std::fmax(m, std::fabs(B.dUdt[i][j].d));
+  return m;
+}
+
+// ---- solver driver (Euler2DQuadSolver, Euler2DQuadSolvers.cc:26-1100) --------
+int Euler2DQuadSolver(const char* Input_File_Name_ptr, int batch_flag) {
+  Euler2D_Input_Parameters IP;
+  int rc = IP.Process_Input_Control_Parameter_File(Input_File_Name_ptr);
+  if (rc) {
+    if (!batch_flag) fprintf(stderr, "Euler2DQuadSolver: error reading %s at line %d\n", Input_File_Name_ptr, rc);
+    return rc > 0 ? rc : E2D_ERR_ARG;
+  }
+  std::vector<Euler2D_Quad_Block> blocks;
+  std::vector<int> neighbour;
+  if ((rc = Create_Initial_Solution_Blocks(IP, blocks, neighbour))) return E2D_ERR_ARG;
+  Euler2D_Device_Blocks dev(blocks, neighbour, IP);
+  if (!dev.handle()) return E2D_ERR_CUDA;
+  std::vector<double> hist;
+  if (IP.Maximum_Number_of_Time_Steps > 0) {
+    if ((rc = dev.explicit_steps(IP.Maximum_Number_of_Time_Steps, &hist))) return rc;
+  }
+  std::vector<e2d_nks_step> nks_hist;
+  if (IP.NKS.max_newton > 0) {
+    if ((rc = dev.nks(IP.NKS, &nks_hist))) return rc;
+  }
+  if ((rc = dev.download())) return rc;
+  // cell-centred output: one zone per block (x, y of the cell centroid
+  // average of its nodes; rho, u, v, p)
+  FILE* f = fopen(IP.Output_File_Name.c_str(), "w");
+  if (!f) return E2D_ERR_ARG;
+  fprintf(f, "TITLE = \"Euler2D solution\"\nVARIABLES = \"x\" \"y\" \"rho\" \"u\" \"v\" \"p\"\n");
+  for (size_t b = 0; b < blocks.size(); ++b) {
+    const Euler2D_Quad_Block& B = blocks[b];
+    fprintf(f, "ZONE T = \"Block %zu\" I = %d J = %d F = POINT\n", b, B.ICu - B.ICl + 1, B.JCu - B.JCl + 1);
+    for (int j = B.JCl; j <= B.JCu; ++j)
+      for (int i = B.ICl; i <= B.ICu; ++i) {
+        const auto& N = B.Grid.Node;
+        const double x = 0.25 * (N[i][j].x + N[i + 1][j].x + N[i + 1][j + 1].x + N[i][j + 1].x);
+        const double y = 0.25 * (N[i][j].y + N[i + 1][j].y + N[i + 1][j + 1].y + N[i][j + 1].y);
+        const Euler2D_pState& w = B.W[i][j];
+        fprintf(f, "%.17g %.17g %.17g %.17g %.17g %.17g\n", x, y, w.d, w.v.x, w.v.y, w.p);
+      }
+  }
+  fclose(f);
+  if (!batch_flag) {
+    if (!hist.empty())
+      printf("explicit: %d steps, last L2 = %.10g\n", IP.Maximum_Number_of_Time_Steps, hist[hist.size() - 2]);
+    for (size_t k = 0; k < nks_hist.size(); ++k)
+      printf("Newton Step %zu L2norm = %.10g L2norm_ratio = %.10g CFL = %.10g GMRES = %d\n", k + 1, nks_hist[k].l2,
+             nks_hist[k].ratio, nks_hist[k].cfl, nks_hist[k].gmres_iters);
+  }
+  return 0;
+}
+
+}  // namespace cffc_b200
+
+// C entry of the deck-driven solve (for callers without C++ linkage).
+extern "C" int e2d_solver_run(const char* input_file, int batch_flag) {
+  if (!input_file) return E2D_ERR_ARG;
+  return cffc_b200::Euler2DQuadSolver(input_file, batch_flag);
+}

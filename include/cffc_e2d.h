@@ -147,6 +147,19 @@ int e2d_rk_steps(e2d_handle *h, int n_steps, double *hist);
  * interior cells (Euler2DQuadMultiBlock.cc:1017-1190). */
 int e2d_norms(e2d_handle *h, double out[3]);
 
+/* CFL (Euler2DQuadSingleBlock.cc:3019-3080) of the current state: the
+ * stability time step of every interior cell into dt (host, may be NULL;
+ * [nblk][NCj][NCi], ghost entries untouched) and their minimum over all
+ * blocks into *dtmin (CFL of Euler2DQuadMultiBlock.cc:963 with
+ * CFFC_Minimum_MPI). */
+int e2d_cfl(e2d_handle *h, double *dt, double *dtmin);
+
+/* Deck-driven solve: Euler2DQuadSolver(char *Input_File_Name, int
+ * batch_flag) (Euler2DQuadSolvers.cc:26) through the C++ host layer of
+ * cffc_euler2d.hpp.  Returns 0, the line number of the first invalid deck
+ * entry, or a library error. */
+int e2d_solver_run(const char *input_file, int batch_flag);
+
 /* Newton-Krylov-Schwarz parameters: the NKS_Input_Parameters fields the
  * Euler2D steady path reads (src_2D/NewtonKrylovSchwarz2D/NKSInput2D.h:128-172;
  * defaults in brackets).  The preconditioner is block Jacobi on the
