@@ -72,6 +72,7 @@ def parse():
     p.add_argument("--precision", default="fp64", choices=["fp64", "exact", "fp32"])
     p.add_argument("--rk-steps", type=int, default=RK_STEPS)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-nks", action="store_true", help="skip the Newton-Krylov s-to-steady measurement")
     return p.parse_args()
 
 
@@ -166,6 +167,61 @@ def cpu_baseline(bs, nsteps=12):
               f"({r['cells'] * r['steps'] / 1e6:.1f} M cell-updates, {r['seconds']:.1f} s)")
     return {"value": round(r["mcell_updates_per_s"], 4), "unit": "Mcell-updates/s",
             "cores": r["threads"], "kind": kind, "sample": sample}
+
+
+NKS_PARAMS = dict(max_newton=40, gmres_restart=30, max_gmres=200, overall_tol=1e-10, cfl0=10.0,
+                  gmres_tol=0.1)
+
+
+def nks_workload():
+    """Steady supersonic (Mach 1.4) flow over a 4 % sin^2 bump, first order
+    (limiter zero), local time stepping: 6 x 2 blocks of 32 x 32 cells.  The
+    reference's block-Jacobi Newton-Krylov converges this case to a 1e-10
+    L2 drop (it stalls on the subsonic bump and on larger grids)."""
+    from cffc_b200 import cases
+    return cases.bump_channel(nbi=6, nbj=2, nci=32, ncj=32, mach=1.4, h=0.04,
+                              scheme=cases.Scheme(limiter=cases.LIMITER_ZERO, local_dt=1))
+
+
+def nks_measure(precision, device, cpu):
+    """Seconds to a 1e-10 L2 density drop: the device solve end to end (host
+    W in, Newton loop with its per-iteration host round trips), and the
+    compiled reference's Newton_Krylov_Schwarz_Solver on one host core."""
+    from cffc_b200 import capi
+    bs = nks_workload()
+    bs.scheme.precision = precision
+    p = capi.nks_params(**NKS_PARAMS)
+    h = capi.Handle(bs, device=device)
+    h.set_state()
+    h.nks(capi.nks_params(2, gmres_restart=30, max_gmres=20))  # warm-up: allocation, first launches
+    t0 = time.perf_counter()
+    h.set_state()
+    rc, hist = h.nks(p)
+    secs = time.perf_counter() - t0
+    h.close()
+    iters = sum(st["gmres_iters"] for st in hist)
+    out = {"workload": "supersonic bump, 6 x 2 blocks x 32x32 (12,288 cells), first order, "
+                       "GMRES(30) tol 0.1, CFL0 10, block-Jacobi",
+           "tolerance": NKS_PARAMS["overall_tol"], "seconds_to_steady": round(secs, 4),
+           "converged": bool(rc == 0 and hist and hist[-1]["ratio"] <= NKS_PARAMS["overall_tol"]),
+           "newton_steps": len(hist) - 1, "gmres_iterations": iters,
+           "residual_evaluations": len(hist) + iters + sum(st["gmres_restarts"] for st in hist),
+           "final_ratio": hist[-1]["ratio"] if hist else None}
+    harness = os.path.join(ROOT, "oracle", "_ref", "e2d_ref_harness")
+    if cpu and os.path.exists(harness):
+        from cffc_b200 import cases
+        with tempfile.TemporaryDirectory() as td:
+            cp, op = os.path.join(td, "c.bin"), os.path.join(td, "o.bin")
+            cases.write_case(cp, bs)
+            a = NKS_PARAMS
+            r = subprocess.run([harness, "nks", cp, op, str(a["max_newton"]), str(a["gmres_restart"]),
+                                str(a["max_gmres"]), str(a["cfl0"]), str(a["overall_tol"]), str(a["gmres_tol"])],
+                               capture_output=True, text=True)
+            secs_ref = float(r.stderr.strip().split(",")[-1].split()[0])
+            end = [l for l in r.stdout.split("\n") if "End of Newton Steps" in l]
+            out["cpu_reference"] = {"seconds_to_steady": round(secs_ref, 3), "cores": 1, "kind": "reference",
+                                    "summary": end[0].strip() if end else None}
+    return out
 
 
 def workload():
@@ -337,6 +393,8 @@ def main():
             line["l2_error_vs_fp64"] = dict(fp32_error(bs, args.rk_steps, local), steps=args.rk_steps)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(bs)
+        if world == 1 and not args.no_nks:
+            line["nks"] = nks_measure(PRECISION[args.precision], local, not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
     h.close()
     if world > 1:
