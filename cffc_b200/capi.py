@@ -217,3 +217,69 @@ class Handle:
 
     def status(self) -> int:
         return self.lib.e2d_status(self.h)
+
+
+class BatchHandle(Handle):
+    """Several independent cases on one handle (e2d_create_batch): their
+    blocks end to end in case order; per-case histories and Newton-Krylov
+    solves.  Block dimensions and the scheme must agree across cases."""
+
+    def __init__(self, cases: list[BlockSet], device: int = 0, lib=None):
+        self.lib = lib or load_library()
+        if not cases:
+            raise ValueError("no cases")
+        self.cases = cases
+        self.bs = cases[0]
+        descs, self._keep = [], []
+        for bs in cases:
+            d, k = make_desc(bs)
+            descs.append(d)
+            self._keep += k
+        self._descs = (BlocksDesc * len(cases))(*descs)
+        self._scheme = make_scheme(cases[0].scheme)
+        self.lib.e2d_create_batch.argtypes = [C.POINTER(BlocksDesc), C.c_int, C.POINTER(SchemeDesc), C.c_int,
+                                              C.POINTER(C.c_int)]
+        self.lib.e2d_create_batch.restype = C.c_void_p
+        err = C.c_int(0)
+        self.h = self.lib.e2d_create_batch(self._descs, len(cases), C.byref(self._scheme), device, C.byref(err))
+        if not self.h:
+            raise RuntimeError(f"e2d_create_batch failed: {E2D_ERRORS.get(err.value, err.value)}")
+        self.nblk = sum(bs.nblk for bs in cases)
+        self.offsets = np.cumsum([0] + [bs.nblk for bs in cases])
+
+    def shape(self):
+        return (self.nblk, 4, self.bs.NCj, self.bs.NCi)
+
+    def split(self, a):
+        return [a[self.offsets[c]:self.offsets[c + 1]] for c in range(len(self.cases))]
+
+    def set_state(self, Ws=None) -> None:
+        Ws = [bs.W for bs in self.cases] if Ws is None else Ws
+        W = np.ascontiguousarray(np.concatenate(Ws, axis=0), dtype=np.float64)
+        self._call("set_state", ptr(W))
+
+    def get_state(self):
+        W, U = np.empty(self.shape()), np.empty(self.shape())
+        self._call("get_state", ptr(W), ptr(U))
+        return list(zip(self.split(W), self.split(U)))
+
+    def residual(self):
+        out = np.empty(self.shape())
+        self._call("residual", ptr(out))
+        return self.split(out)
+
+    def rk_steps(self, n: int, history: bool = True):
+        hist = np.zeros((n, len(self.cases), 4)) if history else None
+        rc = self._call("rk_steps", n, ptr(hist))
+        return rc, hist
+
+    def nks(self, params: NksParams):
+        C_ = len(self.cases)
+        m = max(params.max_newton, 1)
+        steps = (NksStep * (m * C_))()
+        counts = (C.c_int * C_)()
+        self.lib.e2d_nks.argtypes = [C.c_void_p, C.POINTER(NksParams), C.POINTER(NksStep), C.POINTER(C.c_int)]
+        rc = self._call("nks", C.byref(params), steps, counts)
+        hists = [[{f: getattr(steps[c * m + k], f) for f, _ in NksStep._fields_ if f != "pad"}
+                  for k in range(counts[c])] for c in range(C_)]
+        return rc, hists

@@ -151,15 +151,15 @@ __device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
   atomicMax(reinterpret_cast<unsigned long long*>(addr), __double_as_longlong(v));
 }
 
-// Local time step of every interior cell and the global minimum (into *dtmin).
+// Local time step of every interior cell and the minimum of each case (into
+// its slot of the step history).  One CTA per block.
 __global__ void __launch_bounds__(AUX_THREADS) cfl_kernel(Blocks B, double* hist, const int* step) {
   __shared__ double red[AUX_THREADS / 32];
-  double* dtmin = hist + 4 * (*step);
+  const int b = blockIdx.x;
+  double* dtmin = hist + 4 * ((*step) * B.ncase + case_id(B, b));
   const int per = B.nci * B.ncj;
-  const long long n = (long long)B.nblk * per;
   double m = MILLION;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    const int b = int(q / per), r = int(q % per);
+  for (int r = threadIdx.x; r < per; r += blockDim.x) {
     const int i = NG + r % B.nci, j = NG + r / B.nci;
     double xc, yc, A;
     quad_centroid(nodeX(B, b, i, j), nodeY(B, b, i, j), nodeX(B, b, i + 1, j), nodeY(B, b, i + 1, j),
@@ -222,12 +222,15 @@ __global__ void __launch_bounds__(AUX_THREADS) norm_partial_kernel(Blocks B, dou
 }
 
 // Combines the per-block partials in block order as the multi-block norms
-// and the solver loop do; out = (L1, L2, Max).
-// One warp: lane l sums blocks l, l+32, ...; the lanes are then combined.
-__global__ void norm_final_kernel(int nblk, const double* part, double* hist, const int* step) {
-  if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+// and the solver loop do; out = (L1, L2, Max) of each case.
+// One warp per case: lane l sums the case's blocks l, l+32, ...; the lanes
+// are then combined.
+__global__ void norm_final_kernel(Blocks B, const double* part, double* hist, const int* step) {
+  if (threadIdx.x >= 32) return;
+  const int c = blockIdx.x;
+  const int b0 = B.case_start ? B.case_start[c] : 0, b1 = B.case_start ? B.case_start[c + 1] : B.nblk;
   double l1 = 0, l2 = 0, mx = 0;
-  for (int b = threadIdx.x; b < nblk; b += 32) {
+  for (int b = b0 + threadIdx.x; b < b1; b += 32) {
     l1 += part[3 * b];
     l2 += sqr(sqrt(part[3 * b + 1]));
     mx = dmax(mx, part[3 * b + 2]);
@@ -238,7 +241,7 @@ __global__ void norm_final_kernel(int nblk, const double* part, double* hist, co
     mx = dmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   }
   if (threadIdx.x == 0) {
-    double* out = hist + 4 * (*step) + 1;
+    double* out = hist + 4 * ((*step) * B.ncase + c) + 1;
     out[0] = l1;
     out[1] = sqrt(sqr(sqrt(l2)));
     out[2] = mx;
@@ -253,17 +256,21 @@ __global__ void fill_kernel(double* p, long long n, double v) {
 // Explicit-step bookkeeping: the step index lives on the device so that one
 // captured step graph replays for every step.
 // Slot of step *step + offset: dt = MILLION (min-reduced), norms = 0 (summed).
-__global__ void slot_init_kernel(double* hist, const int* step, int offset) {
-  double* h = hist + 4 * (*step + offset);
-  h[0] = MILLION; h[1] = 0.0; h[2] = 0.0; h[3] = 0.0;
-}
-// End of a step: the fused epilogue summed r^2 into the next slot's L2 entry.
-__global__ void step_end_kernel(double* hist, int* step, int fused) {
-  if (fused) {
-    double* h = hist + 4 * (*step + 1);
-    h[2] = sqrt(h[2]);
+__global__ void slot_init_kernel(double* hist, const int* step, int offset, int ncase) {
+  for (int c = threadIdx.x; c < ncase; c += blockDim.x) {
+    double* h = hist + 4 * ((*step + offset) * ncase + c);
+    h[0] = MILLION; h[1] = 0.0; h[2] = 0.0; h[3] = 0.0;
   }
-  *step += 1;
+}
+// End of a step: the fused epilogue summed r^2 into the next slots' L2 entries.
+__global__ void step_end_kernel(double* hist, int* step, int fused, int ncase) {
+  if (fused)
+    for (int c = threadIdx.x; c < ncase; c += blockDim.x) {
+      double* h = hist + 4 * ((*step + 1) * ncase + c);
+      h[2] = sqrt(h[2]);
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) *step += 1;
 }
 
 cudaError_t launch_ghost_fill(const Blocks& B, cudaStream_t st) {
@@ -272,25 +279,22 @@ cudaError_t launch_ghost_fill(const Blocks& B, cudaStream_t st) {
 }
 
 cudaError_t launch_cfl(const Blocks& B, double* hist, const int* step, cudaStream_t st) {
-  const long long n = (long long)B.nblk * B.nci * B.ncj;
-  int grid = int((n + AUX_THREADS - 1) / AUX_THREADS);
-  if (grid > 148 * 8) grid = 148 * 8;
-  cfl_kernel<<<grid, AUX_THREADS, 0, st>>>(B, hist, step);
+  cfl_kernel<<<B.nblk, AUX_THREADS, 0, st>>>(B, hist, step);
   return cudaGetLastError();
 }
 
 cudaError_t launch_norms(const Blocks& B, double* part, double* hist, const int* step, cudaStream_t st) {
   norm_partial_kernel<<<B.nblk, AUX_THREADS, 0, st>>>(B, part);
-  norm_final_kernel<<<1, 32, 0, st>>>(B.nblk, part, hist, step);
+  norm_final_kernel<<<B.ncase, 32, 0, st>>>(B, part, hist, step);
   return cudaGetLastError();
 }
 
-cudaError_t launch_slot_init(double* hist, const int* step, int offset, cudaStream_t st) {
-  slot_init_kernel<<<1, 1, 0, st>>>(hist, step, offset);
+cudaError_t launch_slot_init(double* hist, const int* step, int offset, int ncase, cudaStream_t st) {
+  slot_init_kernel<<<1, 128, 0, st>>>(hist, step, offset, ncase);
   return cudaGetLastError();
 }
-cudaError_t launch_step_end(double* hist, int* step, int fused, cudaStream_t st) {
-  step_end_kernel<<<1, 1, 0, st>>>(hist, step, fused);
+cudaError_t launch_step_end(double* hist, int* step, int fused, int ncase, cudaStream_t st) {
+  step_end_kernel<<<1, 128, 0, st>>>(hist, step, fused, ncase);
   return cudaGetLastError();
 }
 cudaError_t launch_fill(double* p, long long n, double v, cudaStream_t st) {

@@ -91,7 +91,7 @@ int ensure_hist(e2d_handle* h, int n) {
   if (n <= h->hist_cap) return 0;
   int cap = n < 64 ? 64 : n;
   double* p = nullptr;
-  if (cudaMalloc(&p, sizeof(double) * 4 * cap) != cudaSuccess) return E2D_ERR_NOMEM;
+  if (cudaMalloc(&p, sizeof(double) * 4 * size_t(cap) * h->B.ncase) != cudaSuccess) return E2D_ERR_NOMEM;
   if (h->hist) {
     for (auto& q : h->allocs)
       if (q == h->hist) { cudaFree(q); q = p; }
@@ -110,7 +110,7 @@ int ensure_hist(e2d_handle* h, int n) {
 // step's last stage computes them for the following step.
 cudaError_t enqueue_step_head(e2d_handle* h) {
   cudaError_t e;
-  if ((e = launch_slot_init(h->hist, h->step, 0, h->stream))) return e;
+  if ((e = launch_slot_init(h->hist, h->step, 0, h->B.ncase, h->stream))) return e;
   if ((e = launch_cfl(h->B, h->hist, h->step, h->stream))) return e;
   return launch_norms(h->B, h->part, h->hist, h->step, h->stream);
 }
@@ -120,12 +120,12 @@ cudaError_t enqueue_step_head(e2d_handle* h) {
 // the next step's CFL minimum and residual norms.
 cudaError_t enqueue_step(e2d_handle* h) {
   cudaError_t e;
-  if ((e = launch_slot_init(h->hist, h->step, 1, h->stream))) return e;
+  if ((e = launch_slot_init(h->hist, h->step, 1, h->B.ncase, h->stream))) return e;
   for (int stage = 1; stage <= h->sc.n_stage; ++stage) {
     if ((e = ghost_fill_for(h, stage))) return e;
     if ((e = launch_stage_any(h, stage, stage == h->sc.n_stage))) return e;
   }
-  return launch_step_end(h->hist, h->step, 1, h->stream);
+  return launch_step_end(h->hist, h->step, 1, h->B.ncase, h->stream);
 }
 
 }  // namespace e2d_host
@@ -179,6 +179,7 @@ e2d_handle* e2d_create(const e2d_blocks_desc* d, const e2d_scheme* sc, int devic
   h->nnode = size_t(B.nblk) * B.NNi * B.NNj;
   B.g = sc->gamma; B.gm1 = B.g - 1.0; B.gm1i = 1.0 / B.gm1;
   B.cfl = sc->cfl; B.limiter = sc->limiter; B.n_stage = sc->n_stage; B.local_dt = sc->local_dt;
+  B.case_of = nullptr; B.case_start = nullptr; B.ncase = 1; B.case_active = nullptr;
   int rc = 0;
   int *neigh, *bcw, *bce, *bcs, *bcn;
   double *X, *Y, *wow, *woe, *wos, *won;
@@ -209,6 +210,77 @@ e2d_handle* e2d_create(const e2d_blocks_desc* d, const e2d_scheme* sc, int devic
   B.dWdx = B.dWdy = B.phi = nullptr;
   return h;
 }
+
+e2d_handle* e2d_create_batch(const e2d_blocks_desc* cases, int ncase, const e2d_scheme* sc, int device, int* err) {
+  if (err) *err = 0;
+  if (!cases || ncase < 1 || !sc) {
+    if (err) *err = E2D_ERR_ARG;
+    return nullptr;
+  }
+  const int nci = cases[0].nci, ncj = cases[0].ncj, ng = cases[0].ng;
+  int nblk = 0;
+  for (int c = 0; c < ncase; ++c) {
+    if (cases[c].nci != nci || cases[c].ncj != ncj || cases[c].ng != ng || cases[c].nblk < 1) {
+      if (err) *err = E2D_ERR_ARG;
+      return nullptr;
+    }
+    nblk += cases[c].nblk;
+  }
+  const size_t NCi = nci + 2 * ng, NCj = ncj + 2 * ng, NN = (NCi + 1) * (NCj + 1);
+  std::vector<int32_t> nb, bcw, bce, bcs, bcn, case_of, case_start(1, 0);
+  std::vector<double> X, Y, wow, woe, wos, won;
+  auto app = [](auto& v, const auto* p, size_t n) { v.insert(v.end(), p, p + n); };
+  for (int c = 0; c < ncase; ++c) {
+    const e2d_blocks_desc& d = cases[c];
+    const int b0 = case_start.back();
+    for (int q = 0; q < 8 * d.nblk; ++q) {
+      const int v = d.neighbour[q];
+      if (v < -1 || v >= d.nblk) {
+        if (err) *err = E2D_ERR_ARG;
+        return nullptr;
+      }
+      nb.push_back(v < 0 ? -1 : v + b0);  // neighbours never cross cases
+    }
+    app(bcw, d.bc_w, d.nblk * NCj); app(bce, d.bc_e, d.nblk * NCj);
+    app(bcs, d.bc_s, d.nblk * NCi); app(bcn, d.bc_n, d.nblk * NCi);
+    app(X, d.node_x, d.nblk * NN); app(Y, d.node_y, d.nblk * NN);
+    app(wow, d.wo_w, d.nblk * 4 * NCj); app(woe, d.wo_e, d.nblk * 4 * NCj);
+    app(wos, d.wo_s, d.nblk * 4 * NCi); app(won, d.wo_n, d.nblk * 4 * NCi);
+    for (int b = 0; b < d.nblk; ++b) case_of.push_back(c);
+    case_start.push_back(b0 + d.nblk);
+  }
+  e2d_blocks_desc all = cases[0];
+  all.nblk = nblk;
+  all.neighbour = nb.data();
+  all.bc_w = bcw.data(); all.bc_e = bce.data(); all.bc_s = bcs.data(); all.bc_n = bcn.data();
+  all.node_x = X.data(); all.node_y = Y.data();
+  all.wo_w = wow.data(); all.wo_e = woe.data(); all.wo_s = wos.data(); all.wo_n = won.data();
+  e2d_handle* h = e2d_create(&all, sc, device, err);
+  if (!h) return nullptr;
+  int* dcase = nullptr;
+  int* dstart = nullptr;
+  int rc;
+  if ((rc = upload(h, &dcase, case_of.data(), case_of.size())) ||
+      (rc = upload(h, &dstart, case_start.data(), case_start.size()))) {
+    if (err) *err = rc;
+    e2d_destroy(h);
+    return nullptr;
+  }
+  h->B.case_of = dcase;
+  h->B.case_start = dstart;
+  h->B.ncase = ncase;
+  // the step history holds one slot per case and step
+  const int cap = h->hist_cap;
+  h->hist_cap = 0;
+  if ((rc = ensure_hist(h, cap))) {
+    if (err) *err = rc;
+    e2d_destroy(h);
+    return nullptr;
+  }
+  return h;
+}
+
+int e2d_batch_cases(e2d_handle* h) { return h ? h->B.ncase : E2D_ERR_ARG; }
 
 void e2d_destroy(e2d_handle* h) {
   if (!h) return;
@@ -314,19 +386,22 @@ int e2d_rk_steps(e2d_handle* h, int n_steps, double* hist) {
   }
   h->B = saved;
   for (int s = 0; s < n_steps; ++s) CK(cudaGraphLaunch(h->step_graph, h->stream));
-  if (hist) CK(cudaMemcpyAsync(hist, h->hist, sizeof(double) * 4 * n_steps, cudaMemcpyDeviceToHost, h->stream));
+  if (hist)
+    CK(cudaMemcpyAsync(hist, h->hist, sizeof(double) * 4 * size_t(n_steps) * h->B.ncase, cudaMemcpyDeviceToHost,
+                       h->stream));
   return check_status(h);
 }
 
-int e2d_norms(e2d_handle* h, double out[3]) {
+int e2d_norms(e2d_handle* h, double* out) {
   if (!h || !out) return E2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
   CK(cudaMemsetAsync(h->step, 0, sizeof(int), h->stream));
   CK(launch_norms(h->B, h->part, h->hist, h->step, h->stream));
-  double tmp[4];
-  CK(cudaMemcpyAsync(tmp, h->hist, sizeof(tmp), cudaMemcpyDeviceToHost, h->stream));
+  std::vector<double> tmp(4 * size_t(h->B.ncase));
+  CK(cudaMemcpyAsync(tmp.data(), h->hist, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  out[0] = tmp[1]; out[1] = tmp[2]; out[2] = tmp[3];
+  for (int c = 0; c < h->B.ncase; ++c)
+    for (int k = 0; k < 3; ++k) out[3 * c + k] = tmp[4 * c + 1 + k];
   return 0;
 }
 
@@ -334,15 +409,16 @@ int e2d_cfl(e2d_handle* h, double* dt, double* dtmin) {
   if (!h) return E2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
   CK(cudaMemsetAsync(h->step, 0, sizeof(int), h->stream));
-  CK(launch_slot_init(h->hist, h->step, 0, h->stream));
+  CK(launch_slot_init(h->hist, h->step, 0, h->B.ncase, h->stream));
   Blocks B = h->B;
   B.local_dt = 1;  // every interior cell's step into B.dt
   CK(launch_cfl(B, h->hist, h->step, h->stream));
-  double tmp[4];
-  CK(cudaMemcpyAsync(tmp, h->hist, sizeof(tmp), cudaMemcpyDeviceToHost, h->stream));
+  std::vector<double> tmp(4 * size_t(h->B.ncase));
+  CK(cudaMemcpyAsync(tmp.data(), h->hist, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost, h->stream));
   if (dt) CK(cudaMemcpyAsync(dt, h->B.dt, sizeof(double) * h->ncell, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  if (dtmin) *dtmin = tmp[0];
+  if (dtmin)
+    for (int c = 0; c < h->B.ncase; ++c) dtmin[c] = tmp[4 * c];
   return 0;
 }
 
@@ -385,12 +461,12 @@ int e2d_kernel_times(e2d_handle* h, int n_steps, double out[6]) {
     // the standalone CFL and norm kernels run before the first step only in
     // e2d_rk_steps; they are timed on every step here for the record
     CK(cudaEventRecord(ev[0], h->stream));
-    CK(launch_slot_init(h->hist, h->step, 0, h->stream));
+    CK(launch_slot_init(h->hist, h->step, 0, h->B.ncase, h->stream));
     CK(launch_cfl(h->B, h->hist, h->step, h->stream));
     CK(cudaEventRecord(ev[1], h->stream));
     CK(launch_norms(h->B, h->part, h->hist, h->step, h->stream));
     CK(cudaEventRecord(ev[2], h->stream));
-    CK(launch_slot_init(h->hist, h->step, 1, h->stream));
+    CK(launch_slot_init(h->hist, h->step, 1, h->B.ncase, h->stream));
     CK(ghost_fill_for(h, 1));
     CK(cudaEventRecord(ev[3], h->stream));
     CK(launch_stage_any(h, 1, h->sc.n_stage == 1));
@@ -401,7 +477,7 @@ int e2d_kernel_times(e2d_handle* h, int n_steps, double out[6]) {
       CK(launch_stage_any(h, 2, 1));
       CK(cudaEventRecord(ev[6], h->stream));
     }
-    CK(launch_step_end(h->hist, h->step, 1, h->stream));
+    CK(launch_step_end(h->hist, h->step, 1, h->B.ncase, h->stream));
     CK(cudaEventRecord(ev[7], h->stream));
     CK(cudaEventSynchronize(ev[7]));
     float t[8] = {0};

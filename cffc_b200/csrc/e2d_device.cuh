@@ -50,7 +50,17 @@ struct Blocks {
   int* status;                     // device status word (2 ints: code, cell)
   double g, gm1, gm1i, cfl;
   int limiter, n_stage, local_dt;
+  // Batches of independent cases: the blocks of case c are
+  // case_start[c] .. case_start[c+1]-1 and case_of[b] names the case of block b
+  // (null for a single case).  Per-case quantities (time-step minimum, residual
+  // norms) live in slot (step, case) of the step history: hist + 4*(step*ncase + case).
+  const int* case_of;
+  const int* case_start;
+  int ncase;
+  const int* case_active;  // per case, null = all: residual/JVP stages skip inactive cases
 };
+
+__host__ __device__ inline int case_id(const Blocks& B, int b) { return B.case_of ? B.case_of[b] : 0; }
 
 // Arguments of the fused stage kernel.  mode: 0 = dUdt_Residual_Evaluation,
 // 1 = RK stage 1, 2 = RK stage 2.  The global time step of the current

@@ -38,7 +38,7 @@ inline void stage_tile(int precision, int* ti, int* tj) {
 cudaError_t launch_ghost_fill(const Blocks& B, cudaStream_t st);
 cudaError_t launch_cfl(const Blocks& B, double* hist, const int* step, cudaStream_t st);
 cudaError_t launch_norms(const Blocks& B, double* part, double* hist, const int* step, cudaStream_t st);
-cudaError_t launch_slot_init(double* hist, const int* step, int offset, cudaStream_t st);
-cudaError_t launch_step_end(double* hist, int* step, int fused, cudaStream_t st);
+cudaError_t launch_slot_init(double* hist, const int* step, int offset, int ncase, cudaStream_t st);
+cudaError_t launch_step_end(double* hist, int* step, int fused, int ncase, cudaStream_t st);
 cudaError_t launch_fill(double* p, long long n, double v, cudaStream_t st);
 }  // namespace e2d

@@ -6,17 +6,21 @@
 // (NewtonKrylovSchwarz2D/Block_Preconditioner2D.h:352-584) and the Euler2D
 // Newton_Update with positivity back-off (Euler2D/Euler2DQuadNKS.h:23-92).
 //
+// Batches.  A handle may hold several independent cases (e2d_create_batch).
+// Every case runs its own Newton loop and GMRES — own norms, CFL, epsilon,
+// Hessenberg matrix, Givens rotations and stopping decisions — while the
+// device work of all cases still iterating runs in the same launches, in
+// lockstep: all cases start GMRES together, a case that meets its tolerance
+// drops out (its blocks are skipped through the per-case active mask) and
+// the restarted cases go on together.  Reductions are per block, then per
+// case in block order, so a case gives the same bits in a batch as alone.
+//
 // Layout.  Krylov vectors are the reference's per-block GMRES vectors laid
 // end to end: [nblk][NCj][NCi][4] doubles (GMRES_Block::index,
 // GMRES2D.h:84), ghost entries held at zero.  The preconditioner keeps one
 // 4x4 inverse per cell, row-major [nblk][NCj][NCi][16] (identity on ghost
-// cells, as Create_Preconditioner leaves them).
-//
-// Reductions (dot products, 2-norms) are two-level and deterministic: a
-// fixed grid writes per-CTA partials and the last CTA to finish sums them in
-// CTA order.  The GMRES Hessenberg column comes back to the host once per
-// inner iteration for the Givens rotations and the convergence test, which
-// the reference also does on the host (identically on every block).
+// cells, as Create_Preconditioner leaves them).  Per-case scalars are
+// [ncase] arrays; the Hessenberg column of iteration j is [j+2][ncase].
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,69 +37,66 @@ using namespace e2d;
 namespace {
 
 constexpr int VT = 256;           // threads of the vector kernels
-constexpr int VGRID = 148 * 4;    // CTAs of the vector kernels (fixed: determinism)
+constexpr int VGRID = 148 * 4;    // CTAs of the grid-stride kernels
 constexpr double RHO_STD = 1.225;       // Euler2D_W_STDATM.d
 constexpr double P_STD = 101325.0;      // Euler2D_W_STDATM.p
 
 enum Final { FIN_SUM = 0, FIN_SQRT = 1, FIN_EPS = 2 };
 
-// Block-level sum followed by the grid-level combine in the last CTA.
-// out = sum, sqrt(sum) or eps0 / sqrt(sum).
-__device__ void reduce_finalize(double v, double* partial, unsigned* counter, double* out, int fin,
-                                double eps0) {
+__device__ __forceinline__ bool case_on(const Blocks& B, int c) { return !B.case_active || B.case_active[c]; }
+
+// CTA sum of v (fixed order: warp shuffles, then the warps in order).
+__device__ double cta_sum(double v) {
   __shared__ double red[VT / 32];
-  __shared__ bool last;
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < VT / 32; ++w) s += red[w];
-    partial[blockIdx.x] = s;
-    __threadfence();
-    const unsigned done = atomicAdd(counter, 1u);
-    last = (done == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  // the last CTA: sum the partials in CTA order (strided per lane, then a
-  // fixed tree), so the result does not depend on which CTA finished last
   double s = 0.0;
-  for (int q = threadIdx.x; q < gridDim.x; q += VT) s += ((volatile double*)partial)[q];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < VT / 32; ++w) t += red[w];
-    *out = fin == FIN_SUM ? t : (fin == FIN_SQRT ? sqrt(t) : eps0 / sqrt(t));
-    *counter = 0u;
-  }
+  if (threadIdx.x == 0)
+    for (int w = 0; w < VT / 32; ++w) s += red[w];
+  return s;  // valid in thread 0
 }
 
-// out = reduce(sum a*b)
-__global__ void __launch_bounds__(VT) dot_kernel(const double* __restrict__ a, const double* __restrict__ b,
-                                                 long long n2, double* partial, unsigned* counter, double* out,
-                                                 int fin, double eps0) {
-  const double2* a2 = reinterpret_cast<const double2*>(a);
-  const double2* b2 = reinterpret_cast<const double2*>(b);
+// partial[b] = sum over block b of a*b (one CTA per block; nper2 double2
+// entries per block).
+__global__ void __launch_bounds__(VT) blk_dot_kernel(const double* __restrict__ a, const double* __restrict__ bv,
+                                                     int nper2, double* partial, Blocks B) {
+  const int blk = blockIdx.x;
+  if (!case_on(B, case_id(B, blk))) return;  // uniform per CTA
+  const double2* a2 = reinterpret_cast<const double2*>(a) + size_t(blk) * nper2;
+  const double2* b2 = reinterpret_cast<const double2*>(bv) + size_t(blk) * nper2;
   double s = 0.0;
-  for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n2; q += (long long)gridDim.x * VT) {
+  for (int q = threadIdx.x; q < nper2; q += VT) {
     const double2 x = a2[q], y = b2[q];
     s += x.x * y.x;
     s += x.y * y.y;
   }
-  reduce_finalize(s, partial, counter, out, fin, eps0);
+  s = cta_sum(s);
+  if (threadIdx.x == 0) partial[blk] = s;
 }
 
-// y += alpha * x with alpha = sign * (*alpha_dev) (device scalar) or alpha_host.
+// out[c] = f(sum of the case's block partials in block order): the sum,
+// its square root, or eps0 / sqrt (calculate_epsilon, GMRES2D.h:1628-1640).
+// One warp per case.
+__global__ void case_final_kernel(const double* partial, Blocks B, double* out, int fin, double eps0) {
+  const int c = blockIdx.x;
+  if (threadIdx.x >= 32 || !case_on(B, c)) return;
+  const int b0 = B.case_start ? B.case_start[c] : 0, b1 = B.case_start ? B.case_start[c + 1] : B.nblk;
+  double s = 0.0;
+  for (int b = b0 + threadIdx.x; b < b1; b += 32) s += partial[b];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) out[c] = fin == FIN_SUM ? s : (fin == FIN_SQRT ? sqrt(s) : eps0 / sqrt(s));
+}
+
+// y += alpha * x, alpha = sign * coef[case] (device, per case) or alpha_h.
 __global__ void __launch_bounds__(VT) axpy_kernel(double* __restrict__ y, const double* __restrict__ x, long long n2,
-                                                  const double* alpha_dev, double sign, double alpha_host) {
-  const double alpha = alpha_dev ? sign * (*alpha_dev) : alpha_host;
+                                                  int nper2, const double* coef, double sign, double alpha_h, Blocks B) {
   double2* y2 = reinterpret_cast<double2*>(y);
   const double2* x2 = reinterpret_cast<const double2*>(x);
   for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n2; q += (long long)gridDim.x * VT) {
+    const int c = case_id(B, int(q / nper2));
+    if (!case_on(B, c)) continue;
+    const double alpha = coef ? sign * coef[c] : alpha_h;
     double2 v = y2[q];
     const double2 u = x2[q];
     v.x = v.x + alpha * u.x;
@@ -104,12 +105,14 @@ __global__ void __launch_bounds__(VT) axpy_kernel(double* __restrict__ y, const 
   }
 }
 
-// y *= f with f = 1 / (*s_dev) (dscal by ONE/H, GMRES2D.h:1246) or f_host.
-__global__ void __launch_bounds__(VT) scale_kernel(double* __restrict__ y, long long n2, const double* s_dev,
-                                                   double f_host) {
-  const double f = s_dev ? 1.0 / (*s_dev) : f_host;
+// y *= sign / s[case] (dscal by ONE/H or -ONE/beta, GMRES2D.h:1080, :1246).
+__global__ void __launch_bounds__(VT) scale_kernel(double* __restrict__ y, long long n2, int nper2, const double* s,
+                                                   double sign, Blocks B) {
   double2* y2 = reinterpret_cast<double2*>(y);
   for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n2; q += (long long)gridDim.x * VT) {
+    const int c = case_id(B, int(q / nper2));
+    if (!case_on(B, c)) continue;
+    const double f = sign / s[c];
     double2 v = y2[q];
     v.x = f * v.x;
     v.y = f * v.y;
@@ -117,43 +120,51 @@ __global__ void __launch_bounds__(VT) scale_kernel(double* __restrict__ y, long 
   }
 }
 
-// x = x + s_0 Z_0 + s_1 Z_1 + ... in the reference's daxpy order
-// (GMRES2D.h:1300-1304).
+// x = x + s_0 Z_0 + ... + s_{k-1} Z_{k-1} per case, in the reference's daxpy
+// order (GMRES2D.h:1300-1304); k = kcount[case] (0: x unchanged).
 __global__ void __launch_bounds__(VT) update_x_kernel(double* __restrict__ x, const double* __restrict__ Z, long long n,
-                                                      const double* __restrict__ s, int k) {
+                                                      int nper, const double* __restrict__ s, const int* kcount,
+                                                      int m, Blocks B) {
   for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n; q += (long long)gridDim.x * VT) {
+    const int c = case_id(B, int(q / nper));
+    const int k = kcount[c];
+    if (k == 0) continue;
     double v = x[q];
-    for (int j = 0; j < k; ++j) v = v + s[j] * Z[size_t(j) * n + q];
+    for (int j = 0; j < k; ++j) v = v + s[size_t(c) * m + j] * Z[size_t(j) * n + q];
     x[q] = v;
   }
 }
 
-// z = Minv v per cell, with eps = eps0 / ||z|| (calculate_epsilon,
-// GMRES2D.h:1628-1640) reduced on the fly.
+// z = Minv v per cell of block blockIdx.x, and partial[b] = sum z^2 (the
+// numerator of eps = eps0 / ||z||).
 __global__ void __launch_bounds__(VT) precon_apply_kernel(const double* __restrict__ Minv, const double* __restrict__ v,
-                                                          double* __restrict__ z, long long ncell, double* partial,
-                                                          unsigned* counter, double* eps_out, double eps0) {
+                                                          double* __restrict__ z, int cells_per_block, double* partial,
+                                                          Blocks B) {
+  const int blk = blockIdx.x;
+  if (!case_on(B, case_id(B, blk))) return;
   double s = 0.0;
-  for (long long c = blockIdx.x * (long long)VT + threadIdx.x; c < ncell; c += (long long)gridDim.x * VT) {
+  for (int r = threadIdx.x; r < cells_per_block; r += VT) {
+    const size_t c = size_t(blk) * cells_per_block + r;
     const double2* v2 = reinterpret_cast<const double2*>(v + 4 * c);
     const double2 va = v2[0], vb = v2[1];
     const double* M = Minv + 16 * c;
     double o[4];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
+    for (int row = 0; row < 4; ++row) {
       double t = 0.0;
-      t = t + va.x * M[4 * r + 0];
-      t = t + va.y * M[4 * r + 1];
-      t = t + vb.x * M[4 * r + 2];
-      t = t + vb.y * M[4 * r + 3];
-      o[r] = t;
+      t = t + va.x * M[4 * row + 0];
+      t = t + va.y * M[4 * row + 1];
+      t = t + vb.x * M[4 * row + 2];
+      t = t + vb.y * M[4 * row + 3];
+      o[row] = t;
       s += t * t;
     }
     double2* z2 = reinterpret_cast<double2*>(z + 4 * c);
     z2[0] = make_double2(o[0], o[1]);
     z2[1] = make_double2(o[2], o[3]);
   }
-  reduce_finalize(s, partial, counter, eps_out, FIN_EPS, eps0);
+  s = cta_sum(s);
+  if (threadIdx.x == 0) partial[blk] = s;
 }
 
 struct Norm4 {
@@ -163,12 +174,14 @@ struct Norm4 {
 // U = Uo + (eps * dir) * normU on every cell, ghosts included, and W = W(U)
 // (calculate_perturbed_residual, GMRES2D.h:388-409).
 __global__ void __launch_bounds__(VT) perturb_kernel(Blocks B, const double* __restrict__ Uo,
-                                                     const double* __restrict__ dir, const double* eps_dev, Norm4 nm) {
-  const double eps = *eps_dev;
+                                                     const double* __restrict__ dir, const double* eps_case, Norm4 nm) {
   const long long ncell = (long long)B.nblk * B.NCj * B.NCi;
   const int per = B.NCj * B.NCi;
   for (long long c = blockIdx.x * (long long)VT + threadIdx.x; c < ncell; c += (long long)gridDim.x * VT) {
     const int b = int(c / per), r = int(c % per);
+    const int cs = case_id(B, b);
+    if (!case_on(B, cs)) continue;
+    const double eps = eps_case[cs];
     const int j = r / B.NCi, i = r % B.NCi;
     double uv[4];
 #pragma unroll
@@ -186,6 +199,7 @@ __global__ void __launch_bounds__(VT) load_b_kernel(Blocks B, double* __restrict
   const int per = B.nci * B.ncj;
   for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n; q += (long long)gridDim.x * VT) {
     const int b = int(q / per), r = int(q % per);
+    if (!case_on(B, case_id(B, b))) continue;
     const int i = NG + r % B.nci, j = NG + r / B.nci;
     const size_t c = cell_sc(B, b, j, i);
 #pragma unroll
@@ -194,16 +208,18 @@ __global__ void __launch_bounds__(VT) load_b_kernel(Blocks B, double* __restrict
 }
 
 // Time step of the Newton step: the CFL-limited local step scaled by the
-// finite-time-step CFL, or the global minimum times it (NKS2D.h:913-930).
-__global__ void __launch_bounds__(VT) set_dt_kernel(Blocks B, const double* dtmin, double cfl) {
+// case's finite-time-step CFL, or the case's minimum times it (NKS2D.h:913-930).
+__global__ void __launch_bounds__(VT) set_dt_kernel(Blocks B, const double* slots, const double* cfl_case) {
   const long long n = (long long)B.nblk * B.nci * B.ncj;
   const int per = B.nci * B.ncj;
-  const double dg = (*dtmin) * cfl;
   for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n; q += (long long)gridDim.x * VT) {
     const int b = int(q / per), r = int(q % per);
+    const int cs = case_id(B, b);
+    if (!case_on(B, cs)) continue;
     const int i = NG + r % B.nci, j = NG + r / B.nci;
     const size_t c = cell_sc(B, b, j, i);
-    B.dt[c] = B.local_dt ? B.dt[c] * cfl : dg;
+    const double cfl = cfl_case[cs];
+    B.dt[c] = B.local_dt ? B.dt[c] * cfl : slots[4 * cs] * cfl;
   }
 }
 
@@ -216,6 +232,7 @@ __global__ void __launch_bounds__(VT) newton_update_kernel(Blocks B, const doubl
   const int per = B.nci * B.ncj;
   for (long long q = blockIdx.x * (long long)VT + threadIdx.x; q < n; q += (long long)gridDim.x * VT) {
     const int b = int(q / per), r = int(q % per);
+    if (!case_on(B, case_id(B, b))) continue;
     const int i = NG + r % B.nci, j = NG + r / B.nci;
     const size_t c = cell_sc(B, b, j, i);
     double uo[4], du[4];
@@ -416,6 +433,7 @@ __global__ void __launch_bounds__(128) precon_build_kernel(Blocks B, double* __r
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
        q += (long long)gridDim.x * blockDim.x) {
     const int b = int(q / per), r = int(q % per);
+    if (B.case_active && !B.case_active[case_id(B, b)]) continue;
     const int i = NG + r % B.nci, j = NG + r / B.nci;
     const size_t c = cell_sc(B, b, j, i);
     const PState<double> wc = ldW(B, b, i, j);
@@ -470,19 +488,27 @@ __global__ void identity_blocks_kernel(double* Minv, long long ncell) {
 
 struct e2d_nks_state {
   int m = 0;                 // restart length the buffers are sized for
+  int ncase = 0;
   long long n = 0;           // vector length (4 * cells, ghosts included)
+  int nper4 = 0;             // vector entries per block
   double* Uo = nullptr;      // [nblk][4][NCj][NCi]
   double* Minv = nullptr;    // [cells][16]
   double* bvec = nullptr;
   double* x = nullptr;
   double* V = nullptr;       // (m + 1) * n
   double* Z = nullptr;       // m * n
-  double* partial = nullptr; // [VGRID]
-  unsigned* counter = nullptr;
-  double* scal = nullptr;    // [0] eps, [1] norm, [2 ..] Hessenberg column, s
-  double* hist4 = nullptr;   // CFL / norm slot
+  double* partial = nullptr; // [nblk]
+  double* eps = nullptr;     // [ncase]
+  double* nrm = nullptr;     // [ncase]
+  double* hcol = nullptr;    // [m + 2][ncase]
+  double* svals = nullptr;   // [ncase][m]
+  int* kcount = nullptr;     // [ncase]
+  double* cflv = nullptr;    // [ncase]
+  int* active = nullptr;     // [ncase]
+  double* slots = nullptr;   // [ncase][4]: CFL minimum and residual norms
   int* step0 = nullptr;
-  double* host = nullptr;    // pinned: Hessenberg column, norms
+  double* host = nullptr;    // pinned staging
+  size_t host_n = 0;
   std::vector<void*> allocs;
 };
 
@@ -515,25 +541,30 @@ int nks_setup(e2d_handle* h, int m) {
   nks_free(h);
   e2d_nks_state* s = new e2d_nks_state;
   h->nks = s;
+  const int C = h->B.ncase;
   s->m = m;
+  s->ncase = C;
   s->n = 4 * (long long)h->ncell;
+  s->nper4 = 4 * h->B.NCi * h->B.NCj;
   const size_t n = size_t(s->n);
   int rc;
   if ((rc = nalloc(s, &s->Uo, n)) || (rc = nalloc(s, &s->Minv, 16 * h->ncell)) || (rc = nalloc(s, &s->bvec, n)) ||
       (rc = nalloc(s, &s->x, n)) || (rc = nalloc(s, &s->V, (m + 1) * n)) || (rc = nalloc(s, &s->Z, m * n)) ||
-      (rc = nalloc(s, &s->partial, VGRID)) || (rc = nalloc(s, &s->counter, 4)) ||
-      (rc = nalloc(s, &s->scal, 2 * m + 8)) || (rc = nalloc(s, &s->hist4, 4)) || (rc = nalloc(s, &s->step0, 1))) {
+      (rc = nalloc(s, &s->partial, h->B.nblk)) || (rc = nalloc(s, &s->eps, C)) || (rc = nalloc(s, &s->nrm, C)) ||
+      (rc = nalloc(s, &s->hcol, size_t(m + 2) * C)) || (rc = nalloc(s, &s->svals, size_t(m) * C)) ||
+      (rc = nalloc(s, &s->kcount, C)) || (rc = nalloc(s, &s->cflv, C)) || (rc = nalloc(s, &s->active, C)) ||
+      (rc = nalloc(s, &s->slots, 4 * size_t(C))) || (rc = nalloc(s, &s->step0, 1))) {
     nks_free(h);
     return rc;
   }
-  if (cudaMallocHost(&s->host, sizeof(double) * (2 * m + 8)) != cudaSuccess) {
+  s->host_n = std::max(size_t(m + 2) * C, size_t(m + 1) * C + C) + 8;
+  if (cudaMallocHost(&s->host, sizeof(double) * s->host_n) != cudaSuccess) {
     nks_free(h);
     return E2D_ERR_NOMEM;
   }
   E2D_CK(cudaMemsetAsync(s->V, 0, sizeof(double) * (m + 1) * n, h->stream));
   E2D_CK(cudaMemsetAsync(s->Z, 0, sizeof(double) * m * n, h->stream));
   E2D_CK(cudaMemsetAsync(s->bvec, 0, sizeof(double) * n, h->stream));
-  E2D_CK(cudaMemsetAsync(s->counter, 0, sizeof(unsigned) * 4, h->stream));
   E2D_CK(cudaMemsetAsync(s->step0, 0, sizeof(int), h->stream));
   identity_blocks_kernel<<<VGRID, VT, 0, h->stream>>>(s->Minv, (long long)h->ncell);
   E2D_CK(cudaGetLastError());
@@ -546,13 +577,31 @@ int grid_for(long long n) {
   return int(g < 1 ? 1 : g);
 }
 
+// The per-case active mask the kernels see (and the stage kernel through
+// Blocks::case_active).
+int set_active(e2d_handle* h, const std::vector<int>& on) {
+  e2d_nks_state* s = h->nks;
+  int* hb = reinterpret_cast<int*>(s->host);
+  E2D_CK(cudaStreamSynchronize(h->stream));  // the staging buffer is free
+  for (int c = 0; c < s->ncase; ++c) hb[c] = on[c];
+  E2D_CK(cudaMemcpyAsync(s->active, hb, sizeof(int) * s->ncase, cudaMemcpyHostToDevice, h->stream));
+  E2D_CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+Blocks act(e2d_handle* h) {
+  Blocks B = h->B;
+  B.case_active = h->nks->active;
+  return B;
+}
+
 // Stage kernel in Frechet mode: v = (R(U)/normR - b)/eps - (z/dt) normU/normR.
 cudaError_t launch_frechet(e2d_handle* h, const double* z, double* v, const Norm4& nm) {
   StageArgs a{};
-  a.B = h->B;
+  a.B = act(h);
   a.mode = 3;
   a.fuse_next = 0;
-  a.hist = h->hist;
+  a.hist = nullptr;
   a.step = h->step;
   a.Win = h->B.W;
   a.Ubase = h->B.U;
@@ -561,7 +610,7 @@ cudaError_t launch_frechet(e2d_handle* h, const double* z, double* v, const Norm
   a.nks_b = h->nks->bvec;
   a.nks_z = z;
   a.nks_v = v;
-  a.nks_eps = h->nks->scal + 0;
+  a.nks_eps = h->nks->eps;
   for (int k = 0; k < 4; ++k) { a.normU[k] = nm.u[k]; a.normR[k] = nm.r[k]; }
   int ti, tj;
   stage_tile(h->sc.precision, &ti, &tj);
@@ -574,33 +623,39 @@ cudaError_t launch_frechet(e2d_handle* h, const double* z, double* v, const Norm
 // exchange and BCs, residual, v = J dir (GMRES2D.h:1106-1221).
 int matvec(e2d_handle* h, const double* dir, double* v, const Norm4& nm) {
   e2d_nks_state* s = h->nks;
-  perturb_kernel<<<grid_for((long long)h->ncell), VT, 0, h->stream>>>(h->B, s->Uo, dir, s->scal + 0, nm);
+  perturb_kernel<<<grid_for((long long)h->ncell), VT, 0, h->stream>>>(act(h), s->Uo, dir, s->eps, nm);
   E2D_CK(cudaGetLastError());
   E2D_CK(ghost_fill_for(h, 0));
   E2D_CK(launch_frechet(h, dir, v, nm));
   return 0;
 }
 
+// out[c] = f(dot(a, b) over case c) for the active cases.
 int dot(e2d_handle* h, const double* a, const double* b, double* out, int fin, double eps0 = 0.0) {
   e2d_nks_state* s = h->nks;
-  dot_kernel<<<VGRID, VT, 0, h->stream>>>(a, b, s->n / 2, s->partial, s->counter, out, fin, eps0);
+  const Blocks B = act(h);
+  blk_dot_kernel<<<h->B.nblk, VT, 0, h->stream>>>(a, b, s->nper4 / 2, s->partial, B);
+  E2D_CK(cudaGetLastError());
+  case_final_kernel<<<s->ncase, 32, 0, h->stream>>>(s->partial, B, out, fin, eps0);
   E2D_CK(cudaGetLastError());
   return 0;
 }
 
-int axpy(e2d_handle* h, double* y, const double* x, const double* alpha_dev, double sign, double alpha_host) {
-  axpy_kernel<<<VGRID, VT, 0, h->stream>>>(y, x, h->nks->n / 2, alpha_dev, sign, alpha_host);
+int axpy(e2d_handle* h, double* y, const double* x, const double* coef, double sign, double alpha) {
+  e2d_nks_state* s = h->nks;
+  axpy_kernel<<<VGRID, VT, 0, h->stream>>>(y, x, s->n / 2, s->nper4 / 2, coef, sign, alpha, act(h));
   E2D_CK(cudaGetLastError());
   return 0;
 }
 
-int scale(e2d_handle* h, double* y, const double* s_dev, double f_host) {
-  scale_kernel<<<VGRID, VT, 0, h->stream>>>(y, h->nks->n / 2, s_dev, f_host);
+int scale(e2d_handle* h, double* y, const double* sdev, double sign) {
+  e2d_nks_state* s = h->nks;
+  scale_kernel<<<VGRID, VT, 0, h->stream>>>(y, s->n / 2, s->nper4 / 2, sdev, sign, act(h));
   E2D_CK(cudaGetLastError());
   return 0;
 }
 
-int fetch(e2d_handle* h, const double* dev, int count, double* out) {
+int fetch(e2d_handle* h, const double* dev, size_t count, double* out) {
   E2D_CK(cudaMemcpyAsync(h->nks->host, dev, sizeof(double) * count, cudaMemcpyDeviceToHost, h->stream));
   E2D_CK(cudaStreamSynchronize(h->stream));
   memcpy(out, h->nks->host, sizeof(double) * count);
@@ -626,104 +681,149 @@ void apply_rotation(double& dx, double& dy, double cs, double sn) {
   dx = t;
 }
 
-struct GmresOut {
+struct GmresCase {
   double resid0 = 0, relres = 0;
   int iters = 0;
-  bool restarted = false, failed = false;
+  bool restarted = false, failed = false, met = false, done = false;
+  int jstop = -1;                        // j at which the case left this cycle
+  std::vector<double> H, cs, sn, sv;     // Hessenberg columns [m][m+1], rotations, rhs
 };
 
-// GMRES_RightPrecon_MatrixFree::solve (GMRES2D.h:790-1544) with the
-// default options: first-order Frechet derivative, no GMRES check.
-int gmres(e2d_handle* h, const e2d_nks_params& p, double tol, const Norm4& nm, GmresOut& out) {
+// GMRES_RightPrecon_MatrixFree::solve (GMRES2D.h:790-1544) with the default
+// options (first-order Frechet derivative, no GMRES check), for every case
+// with on[c] set, in lockstep.
+int gmres(e2d_handle* h, const e2d_nks_params& p, const std::vector<double>& tol, const std::vector<int>& on,
+          const Norm4& nm, std::vector<GmresCase>& G) {
   e2d_nks_state* s = h->nks;
-  const int m = p.gmres_restart;
+  const int m = p.gmres_restart, C = s->ncase;
   const long long n = s->n;
   const size_t nb = sizeof(double) * size_t(n);
-  std::vector<double> H(size_t(m) * (m + 1), 0.0), cs(m, 0.0), sn(m, 0.0), sv(m + 1, 0.0), col(m + 2);
   int rc;
+  G.assign(C, GmresCase());
+  for (int c = 0; c < C; ++c) {
+    G[c].H.assign(size_t(m) * (m + 1), 0.0);
+    G[c].cs.assign(m, 0.0); G[c].sn.assign(m, 0.0); G[c].sv.assign(m + 1, 0.0);
+    G[c].done = !on[c];
+  }
   E2D_CK(cudaMemsetAsync(s->x, 0, nb, h->stream));
   // V(0) = b (the Initialize'd V(0) is zero; daxpy adds b)
   E2D_CK(cudaMemcpyAsync(s->V, s->bvec, nb, cudaMemcpyDeviceToDevice, h->stream));
-  double resid0 = 0.0, relres = 0.0;
+  std::vector<double> col(size_t(m + 2) * C), beta(C);
+  std::vector<int> cyc(C), kc(C);
   int iters = 0;
-  bool met = false, failed = false, restarted = false, first = true;
+  bool first = true;
   for (;;) {
+    for (int c = 0; c < C; ++c) { cyc[c] = !G[c].done; G[c].jstop = -1; }
+    if ((rc = set_active(h, cyc))) return rc;
     if (!first) {
       // V(0) = J x + b with eps = eps0 / ||x|| (GMRES2D.h:838-1000)
-      if ((rc = dot(h, s->x, s->x, s->scal + 0, FIN_EPS, p.epsilon0))) return rc;
+      if ((rc = dot(h, s->x, s->x, s->eps, FIN_EPS, p.epsilon0))) return rc;
       if ((rc = matvec(h, s->x, s->V, nm))) return rc;
       if ((rc = axpy(h, s->V, s->bvec, nullptr, 0.0, 1.0))) return rc;
     }
-    if ((rc = dot(h, s->V, s->V, s->scal + 1, FIN_SQRT))) return rc;
-    double beta;
-    if ((rc = fetch(h, s->scal + 1, 1, &beta))) return rc;
-    if (!(beta > 0.0) || !std::isfinite(beta)) return E2D_ERR_GMRES;
-    if ((rc = scale(h, s->V, nullptr, -1.0 / beta))) return rc;
-    for (int q = 1; q < m + 1; ++q) sv[q] = 0.0;
-    sv[0] = beta;
-    if (iters == 0) resid0 = beta;
+    if ((rc = dot(h, s->V, s->V, s->nrm, FIN_SQRT))) return rc;
+    if ((rc = fetch(h, s->nrm, C, beta.data()))) return rc;
+    for (int c = 0; c < C; ++c)
+      if (cyc[c] && (!(beta[c] > 0.0) || !std::isfinite(beta[c]))) return E2D_ERR_GMRES;
+    if ((rc = scale(h, s->V, s->nrm, -1.0))) return rc;
+    for (int c = 0; c < C; ++c) {
+      if (!cyc[c]) continue;
+      for (int q = 1; q < m + 1; ++q) G[c].sv[q] = 0.0;
+      G[c].sv[0] = beta[c];
+      if (iters == 0) G[c].resid0 = beta[c];
+    }
     int j = -1;
+    std::vector<int> inner = cyc;
     for (;;) {
       ++j;
       ++iters;
       double* Vj = s->V + size_t(j) * n;
       double* Vn = s->V + size_t(j + 1) * n;
       double* Zj = s->Z + size_t(j) * n;
-      precon_apply_kernel<<<VGRID, VT, 0, h->stream>>>(s->Minv, Vj, Zj, (long long)h->ncell, s->partial, s->counter,
-                                                       s->scal + 0, p.epsilon0);
+      const Blocks B = act(h);
+      precon_apply_kernel<<<h->B.nblk, VT, 0, h->stream>>>(s->Minv, Vj, Zj, h->B.NCi * h->B.NCj, s->partial, B);
+      E2D_CK(cudaGetLastError());
+      case_final_kernel<<<C, 32, 0, h->stream>>>(s->partial, B, s->eps, FIN_EPS, p.epsilon0);
       E2D_CK(cudaGetLastError());
       if ((rc = matvec(h, Zj, Vn, nm))) return rc;
       // modified Gram-Schmidt (GMRES2D.h:1224-1240)
       for (int k = 0; k <= j; ++k) {
-        double* hk = s->scal + 2 + k;
+        double* hk = s->hcol + size_t(k) * C;
         if ((rc = dot(h, Vn, s->V + size_t(k) * n, hk, FIN_SUM))) return rc;
         if ((rc = axpy(h, Vn, s->V + size_t(k) * n, hk, -1.0, 0.0))) return rc;
       }
-      if ((rc = dot(h, Vn, Vn, s->scal + 2 + j + 1, FIN_SQRT))) return rc;
-      if ((rc = scale(h, Vn, s->scal + 2 + j + 1, 0.0))) return rc;
-      if ((rc = fetch(h, s->scal + 2, j + 2, col.data()))) return rc;
-      double* Hj = &H[size_t(j) * (m + 1)];
-      for (int k = 0; k <= j + 1; ++k) Hj[k] = col[k];
-      if (!std::isfinite(Hj[j + 1])) return E2D_ERR_NAN;
-      for (int k = 0; k < j; ++k) apply_rotation(Hj[k], Hj[k + 1], cs[k], sn[k]);
-      generate_rotation(Hj[j], Hj[j + 1], cs[j], sn[j]);
-      apply_rotation(Hj[j], Hj[j + 1], cs[j], sn[j]);
-      apply_rotation(sv[j], sv[j + 1], cs[j], sn[j]);
-      relres = fabs(sv[j + 1]) / resid0;
-      if (relres <= tol) { met = true; break; }
-      if (iters >= p.max_gmres) { failed = true; break; }
-      if (j >= m - 1) { restarted = true; break; }
+      double* hn = s->hcol + size_t(j + 1) * C;
+      if ((rc = dot(h, Vn, Vn, hn, FIN_SQRT))) return rc;
+      if ((rc = scale(h, Vn, hn, 1.0))) return rc;
+      if ((rc = fetch(h, s->hcol, size_t(j + 2) * C, col.data()))) return rc;
+      bool any = false, changed = false;
+      for (int c = 0; c < C; ++c) {
+        if (!inner[c]) continue;
+        GmresCase& g = G[c];
+        double* Hj = &g.H[size_t(j) * (m + 1)];
+        for (int k = 0; k <= j + 1; ++k) Hj[k] = col[size_t(k) * C + c];
+        if (!std::isfinite(Hj[j + 1])) return E2D_ERR_NAN;
+        for (int k = 0; k < j; ++k) apply_rotation(Hj[k], Hj[k + 1], g.cs[k], g.sn[k]);
+        generate_rotation(Hj[j], Hj[j + 1], g.cs[j], g.sn[j]);
+        apply_rotation(Hj[j], Hj[j + 1], g.cs[j], g.sn[j]);
+        apply_rotation(g.sv[j], g.sv[j + 1], g.cs[j], g.sn[j]);
+        g.relres = fabs(g.sv[j + 1]) / g.resid0;
+        bool stop = false;
+        if (g.relres <= tol[c]) { g.met = true; stop = true; }
+        else if (iters >= p.max_gmres) { g.failed = true; stop = true; }
+        else if (j >= m - 1) { g.restarted = true; stop = true; }
+        if (stop) { g.jstop = j; g.iters = iters; inner[c] = 0; changed = true; }
+        else any = true;
+      }
+      if (!any) break;
+      if (changed && (rc = set_active(h, inner))) return rc;
     }
-    // back substitution and x += sum s_k Z_k (GMRES2D.h:1290-1304)
-    for (int jj = j; jj >= 0; --jj) {
-      sv[jj] /= H[size_t(jj) * (m + 1) + jj];
-      for (int k = jj - 1; k >= 0; --k) sv[k] -= H[size_t(jj) * (m + 1) + k] * sv[jj];
-    }
-    memcpy(s->host, sv.data(), sizeof(double) * (j + 1));
-    E2D_CK(cudaMemcpyAsync(s->scal + 2 + m + 2, s->host, sizeof(double) * (j + 1), cudaMemcpyHostToDevice, h->stream));
-    update_x_kernel<<<VGRID, VT, 0, h->stream>>>(s->x, s->Z, n, s->scal + 2 + m + 2, j + 1);
-    E2D_CK(cudaGetLastError());
-    // the pinned buffer is reused by the next fetch: wait for this copy
+    // back substitution and x += sum s_k Z_k per case (GMRES2D.h:1290-1304)
+    double* hs = s->host;
+    int* hk = reinterpret_cast<int*>(s->host + size_t(m) * C);
     E2D_CK(cudaStreamSynchronize(h->stream));
-    if (met || failed) break;
+    for (int c = 0; c < C; ++c) {
+      kc[c] = 0;
+      if (!cyc[c]) continue;
+      GmresCase& g = G[c];
+      const int jj0 = g.jstop;
+      for (int jj = jj0; jj >= 0; --jj) {
+        g.sv[jj] /= g.H[size_t(jj) * (m + 1) + jj];
+        for (int k = jj - 1; k >= 0; --k) g.sv[k] -= g.H[size_t(jj) * (m + 1) + k] * g.sv[jj];
+      }
+      kc[c] = jj0 + 1;
+      for (int q = 0; q < jj0 + 1; ++q) hs[size_t(c) * m + q] = g.sv[q];
+    }
+    for (int c = 0; c < C; ++c) hk[c] = kc[c];
+    E2D_CK(cudaMemcpyAsync(s->svals, hs, sizeof(double) * size_t(m) * C, cudaMemcpyHostToDevice, h->stream));
+    E2D_CK(cudaMemcpyAsync(s->kcount, hk, sizeof(int) * C, cudaMemcpyHostToDevice, h->stream));
+    update_x_kernel<<<VGRID, VT, 0, h->stream>>>(s->x, s->Z, n, s->nper4, s->svals, s->kcount, m, h->B);
+    E2D_CK(cudaGetLastError());
+    E2D_CK(cudaStreamSynchronize(h->stream));
+    bool more = false;
+    for (int c = 0; c < C; ++c) {
+      if (!cyc[c]) continue;
+      if (G[c].met || G[c].failed) G[c].done = true;
+      else more = true;
+    }
+    if (!more) break;
     first = false;
   }
-  out.resid0 = resid0;
-  out.relres = relres;
-  out.iters = iters;
-  out.restarted = restarted;
-  out.failed = failed;
   return 0;
 }
 
 }  // namespace
 
 extern "C" int e2d_nks(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, int* n_steps) {
-  if (n_steps) *n_steps = 0;
   if (!h || !p || p->max_newton < 0 || p->gmres_restart < 1 || p->gmres_restart > 500 || p->max_gmres < 1 ||
       !(p->epsilon0 > 0.0) || !(p->cfl0 > 0.0) || !(p->gmres_tol_initial > 0.0) || !(p->gmres_tol_final > 0.0) ||
-      !(p->min_ratio > 0.0))
+      !(p->min_ratio > 0.0)) {
+    if (n_steps) *n_steps = 0;
     return E2D_ERR_ARG;
+  }
+  const int C = h->B.ncase;
+  if (n_steps)
+    for (int c = 0; c < C; ++c) n_steps[c] = 0;
   if (cudaSetDevice(h->device) != cudaSuccess) return E2D_ERR_CUDA;
   int rc;
   if ((rc = nks_setup(h, p->gmres_restart))) return rc;
@@ -737,58 +837,85 @@ extern "C" int e2d_nks(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* his
   Norm4 nm;
   nm.u[0] = rho; nm.u[1] = rho * ao; nm.u[2] = rho * ao; nm.u[3] = rho * ao * ao;
   nm.r[0] = rho * ao; nm.r[1] = rho * ao * ao; nm.r[2] = rho * ao * ao; nm.r[3] = rho * ao * ao * ao;
-  // GMRES forcing: tol = min(0.9, tol_i * ratio^(log(f/i)/log(max(L, eps))))
+  // GMRES forcing: tol = min(0.9, tol_i * ratio^(log(f/i)/log(max(L, 1e-18))))
   const double L = p->overall_tol > 1e-18 ? p->overall_tol : 1e-18;
   const double forcing = log(p->gmres_tol_final / p->gmres_tol_initial) / log(L);
+  std::vector<int> on(C, 1), cnt(C, 0);
+  std::vector<double> l2_first(C, -1.0), ratio(C, 1.0), cfl(C, 0.0), tol(C, 0.0), slots(4 * size_t(C));
+  std::vector<e2d_nks_step> cur(C);
+  std::vector<GmresCase> G;
+  auto record = [&](int c) {
+    if (hist) hist[size_t(c) * p->max_newton + cnt[c]] = cur[c];
+    ++cnt[c];
+  };
+  auto finish = [&](int code) {
+    if (n_steps)
+      for (int c = 0; c < C; ++c) n_steps[c] = cnt[c];
+    B.case_active = nullptr;
+    return code;
+  };
   // the caller's state: exchange and BCs first (as before the solver call)
   E2D_CK(launch_ghost_fill(B, h->stream));
-  double l2_first = -1.0;
-  int nsteps = 0;
   for (int newton = 1; newton <= p->max_newton; ++newton) {
+    if ((rc = set_active(h, on))) return finish(rc);
     // residual and its density norms (NKS2D.h:552-593)
-    E2D_CK(launch_stage_any(h, 0, 0));
-    E2D_CK(launch_slot_init(s->hist4, s->step0, 0, h->stream));
-    E2D_CK(launch_norms(B, h->part, s->hist4, s->step0, h->stream));
-    double nrm[4];
-    if ((rc = fetch(h, s->hist4, 4, nrm))) return rc;
-    if ((rc = check_status(h))) return rc;
-    if (!std::isfinite(nrm[2])) return E2D_ERR_NAN;
-    if (l2_first <= 0.0) l2_first = nrm[2];
-    const double ratio = nrm[2] / l2_first;
-    e2d_nks_step st{};
-    st.l1 = nrm[1]; st.l2 = nrm[2]; st.lmax = nrm[3]; st.ratio = ratio;
-    if (!(ratio > p->overall_tol)) {
-      if (hist) hist[nsteps] = st;
-      ++nsteps;
-      break;
+    B.case_active = s->active;
+    const cudaError_t e0 = launch_stage_any(h, 0, 0);
+    B.case_active = nullptr;
+    E2D_CK(e0);
+    E2D_CK(launch_slot_init(s->slots, s->step0, 0, C, h->stream));
+    E2D_CK(launch_norms(B, h->part, s->slots, s->step0, h->stream));
+    if ((rc = fetch(h, s->slots, 4 * size_t(C), slots.data()))) return finish(rc);
+    if ((rc = check_status(h))) return finish(rc);
+    bool any = false;
+    for (int c = 0; c < C; ++c) {
+      if (!on[c]) continue;
+      const double l2 = slots[4 * c + 2];
+      if (!std::isfinite(l2)) return finish(E2D_ERR_NAN);
+      if (l2_first[c] <= 0.0) l2_first[c] = l2;
+      ratio[c] = l2 / l2_first[c];
+      cur[c] = e2d_nks_step{};
+      cur[c].l1 = slots[4 * c + 1]; cur[c].l2 = l2; cur[c].lmax = slots[4 * c + 3]; cur[c].ratio = ratio[c];
+      if (!(ratio[c] > p->overall_tol)) {
+        record(c);  // converged: the loop's stop test (NKS2D.h:902)
+        on[c] = 0;
+        continue;
+      }
+      any = true;
+      // SER finite time step (Finite_Time_Step, NKS2D.h:1316-1340)
+      cfl[c] = ratio[c] > p->min_ratio ? p->cfl0 * pow(std::max(1.0, 1.0 / ratio[c]), 1.0) : p->cfl0 / p->min_ratio;
+      cur[c].cfl = cfl[c];
+      tol[c] = std::min(0.9, p->gmres_tol_initial * pow(ratio[c], forcing));
     }
-    // SER finite time step (Finite_Time_Step, NKS2D.h:1316-1340)
-    const double cfl = ratio > p->min_ratio ? p->cfl0 * pow(std::max(1.0, 1.0 / ratio), 1.0) : p->cfl0 / p->min_ratio;
-    st.cfl = cfl;
-    E2D_CK(launch_slot_init(s->hist4, s->step0, 0, h->stream));
-    E2D_CK(launch_cfl(B, s->hist4, s->step0, h->stream));
-    set_dt_kernel<<<grid_for(nint), VT, 0, h->stream>>>(B, s->hist4, cfl);
+    if (!any) break;
+    if ((rc = set_active(h, on))) return finish(rc);
+    double* hc = s->host;
+    for (int c = 0; c < C; ++c) hc[c] = cfl[c];
+    E2D_CK(cudaMemcpyAsync(s->cflv, hc, sizeof(double) * C, cudaMemcpyHostToDevice, h->stream));
+    E2D_CK(launch_slot_init(s->slots, s->step0, 0, C, h->stream));
+    E2D_CK(launch_cfl(B, s->slots, s->step0, h->stream));
+    set_dt_kernel<<<grid_for(nint), VT, 0, h->stream>>>(act(h), s->slots, s->cflv);
     E2D_CK(cudaGetLastError());
     // Uo = U (ghosts included) and the preconditioner at Uo
     E2D_CK(cudaMemcpyAsync(s->Uo, B.U, sizeof(double) * 4 * h->ncell, cudaMemcpyDeviceToDevice, h->stream));
-    precon_build_kernel<<<grid_for(nint) * 2, 128, 0, h->stream>>>(B, s->Minv, ao);
+    precon_build_kernel<<<grid_for(nint) * 2, 128, 0, h->stream>>>(act(h), s->Minv, ao);
     E2D_CK(cudaGetLastError());
-    load_b_kernel<<<grid_for(nint), VT, 0, h->stream>>>(B, s->bvec, nm);
+    load_b_kernel<<<grid_for(nint), VT, 0, h->stream>>>(act(h), s->bvec, nm);
     E2D_CK(cudaGetLastError());
-    const double tol = std::min(0.9, p->gmres_tol_initial * pow(ratio, forcing));
-    GmresOut g;
-    if ((rc = gmres(h, *p, tol, nm, g))) return rc;
-    st.gmres_resid0 = g.resid0; st.gmres_relres = g.relres; st.gmres_iters = g.iters;
-    st.gmres_restarts = g.restarted ? 1 : 0; st.gmres_failed = g.failed ? 1 : 0;
-    if (hist) hist[nsteps] = st;
-    ++nsteps;
-    // U = Uo + x, exchange and BCs (NKS2D.h:1058-1090)
-    newton_update_kernel<<<grid_for(nint), VT, 0, h->stream>>>(B, s->Uo, s->x, nm, 1.0);
+    if ((rc = gmres(h, *p, tol, on, nm, G))) return finish(rc);
+    for (int c = 0; c < C; ++c) {
+      if (!on[c]) continue;
+      cur[c].gmres_resid0 = G[c].resid0; cur[c].gmres_relres = G[c].relres; cur[c].gmres_iters = G[c].iters;
+      cur[c].gmres_restarts = G[c].restarted ? 1 : 0; cur[c].gmres_failed = G[c].failed ? 1 : 0;
+      record(c);
+    }
+    // U = Uo + x for the cases still stepping, exchange and BCs (NKS2D.h:1058-1090)
+    if ((rc = set_active(h, on))) return finish(rc);
+    newton_update_kernel<<<grid_for(nint), VT, 0, h->stream>>>(act(h), s->Uo, s->x, nm, 1.0);
     E2D_CK(cudaGetLastError());
     E2D_CK(launch_ghost_fill(B, h->stream));
-    if ((rc = check_status(h))) { if (n_steps) *n_steps = nsteps; return rc; }
+    if ((rc = check_status(h))) return finish(rc);
   }
-  if (n_steps) *n_steps = nsteps;
   E2D_CK(cudaStreamSynchronize(h->stream));
-  return 0;
+  return finish(0);
 }

@@ -282,7 +282,9 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
   if (tid == 0) failed = *(volatile int*)B.status;
   __syncthreads();
   if (failed) return;  // an earlier kernel failed: stop marching (uniform per CTA)
-  const double* dtmin_p = a.hist ? a.hist + 4 * (*a.step) : nullptr;
+  const int cs = case_id(B, b);  // the block's case: its slot of the step history
+  if (B.case_active && !B.case_active[cs]) return;  // a finished case of a batch (uniform per CTA)
+  const double* dtmin_p = a.hist ? a.hist + 4 * ((*a.step) * B.ncase + cs) : nullptr;
   const double g = B.g, gm1 = B.gm1, gm1i = B.gm1i;
 
   // ---- stage W and nodes (halo tile) --------------------------------------
@@ -517,7 +519,7 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
     } else if (MODE == 3) {
       // Frechet derivative: calculate_Matrix_Free (GMRES2D.h:445-488),
       // V = (normalizeR(R) - b)/eps - normalizeUtoR(z * (1/dt))
-      const double eps = *a.nks_eps;
+      const double eps = a.nks_eps[cs];  // the case's epsilon
       const double rdt = 1.0 / B.dt[c];
       const size_t q = c * 4;
 #pragma unroll
@@ -592,7 +594,7 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
       for (int w2 = 1; w2 < NTHREADS / 32; ++w2) {
         dt_next = dmin(dt_next, red[0][w2]); n1 += red[1][w2]; n2 += red[2][w2]; nmax = dmax(nmax, red[3][w2]);
       }
-      double* next = const_cast<double*>(a.hist) + 4 * (*a.step + 1);
+      double* next = const_cast<double*>(a.hist) + 4 * ((*a.step + 1) * B.ncase + cs);
       atomicMin(reinterpret_cast<unsigned long long*>(next), (unsigned long long)__double_as_longlong(dt_next));
       atomicAdd(next + 1, n1);
       atomicAdd(next + 2, n2);

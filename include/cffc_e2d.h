@@ -108,6 +108,19 @@ typedef struct e2d_handle e2d_handle;
 e2d_handle *e2d_create(const e2d_blocks_desc *desc, const e2d_scheme *scheme,
                        int device, int *err);
 
+/* One handle over ncase independent cases (each its own block set, as
+ * e2d_create takes it; block counts may differ, block dimensions must not).
+ * Their blocks are laid end to end in case order; every entry point then
+ * works on all cases at once, with per-case time-step minima, residual
+ * norms, histories and Newton-Krylov solves, and gives each case the same
+ * result bit for bit as a handle of that case alone.  No reference
+ * counterpart: the reference runs one case per process. */
+e2d_handle *e2d_create_batch(const e2d_blocks_desc *cases, int ncase, const e2d_scheme *scheme,
+                             int device, int *err);
+
+/* Number of cases of a handle (1 for e2d_create). */
+int e2d_batch_cases(e2d_handle *h);
+
 /* Releases the handle (Euler2D_Quad_Block::deallocate, Euler2DQuad.h:~700). */
 void e2d_destroy(e2d_handle *h);
 
@@ -139,19 +152,21 @@ int e2d_get_reconstruction(e2d_handle *h, double *dWdx, double *dWdy, double *ph
  * CFL + global minimum, Set_Global_TimeStep (global dt), residual norms,
  * then per stage ghost fill, dUdt_Multistage_Explicit (Euler2DQuad.cc:1235)
  * and Update_Solution_Multistage_Explicit (Euler2DQuadSingleBlock.cc:5300).
- * hist (host, may be NULL) receives [n_steps][4] = dt_min, L1, L2, Max of
- * the density residual as the loop computes them before each step. */
+ * hist (host, may be NULL) receives [n_steps][ncase][4] = dt_min, L1, L2,
+ * Max of the density residual of each case as the loop computes them before
+ * each step (ncase = 1 unless the handle is a batch). */
 int e2d_rk_steps(e2d_handle *h, int n_steps, double *hist);
 
 /* L1, L2 and max norms of the density residual dUdt[...][0][1] over all
- * interior cells (Euler2DQuadMultiBlock.cc:1017-1190). */
-int e2d_norms(e2d_handle *h, double out[3]);
+ * interior cells (Euler2DQuadMultiBlock.cc:1017-1190); out receives
+ * [ncase][3] (three values for a single case). */
+int e2d_norms(e2d_handle *h, double *out);
 
 /* CFL (Euler2DQuadSingleBlock.cc:3019-3080) of the current state: the
  * stability time step of every interior cell into dt (host, may be NULL;
  * [nblk][NCj][NCi], ghost entries untouched) and their minimum over all
- * blocks into *dtmin (CFL of Euler2DQuadMultiBlock.cc:963 with
- * CFFC_Minimum_MPI). */
+ * blocks of each case into dtmin[ncase] (CFL of Euler2DQuadMultiBlock.cc:963
+ * with CFFC_Minimum_MPI). */
 int e2d_cfl(e2d_handle *h, double *dt, double *dtmin);
 
 /* Deck-driven solve: Euler2DQuadSolver(char *Input_File_Name, int

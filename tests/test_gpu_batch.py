@@ -1,0 +1,81 @@
+"""Batched handles (e2d_create_batch): several independent cases with uneven
+block counts in one handle.  Every case must come out exactly as it does on
+a handle of its own — explicit steps and Newton-Krylov solves alike (the
+reductions are per block, then per case in block order)."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from cffc_b200 import capi, cases
+
+pytestmark = pytest.mark.gpu
+
+
+def with_scheme(bs, **kw):
+    return dataclasses.replace(bs, scheme=dataclasses.replace(bs.scheme, **kw))
+
+
+def explicit_cases(precision):
+    sc = dict(limiter=cases.LIMITER_VENKATAKRISHNAN, n_stage=2, local_dt=0, cfl=0.5, precision=precision)
+    return [with_scheme(cases.periodic_box_bumps(nb=2, nc=16, seed=31), **sc),
+            with_scheme(cases.periodic_box_bumps(nb=3, nc=16, seed=32), **sc),
+            with_scheme(cases.bump_channel(nbi=4, nbj=2, nci=16, ncj=16), **sc)]
+
+
+@pytest.mark.parametrize("precision", [2, 0])
+def test_batched_explicit_equals_solo(precision):
+    cs = explicit_cases(precision)
+    hb = capi.BatchHandle(cs)
+    hb.set_state()
+    rc, hist = hb.rk_steps(25)
+    assert rc == 0
+    states = hb.get_state()
+    hb.close()
+    for c, bs in enumerate(cs):
+        h = capi.Handle(bs)
+        h.set_state()
+        rc1, h1 = h.rk_steps(25)
+        W1, U1 = h.get_state()
+        h.close()
+        assert rc1 == 0
+        assert np.array_equal(bs.interior(states[c][1]), bs.interior(U1)), c
+        assert np.array_equal(hist[:, c, 0], h1[:, 0])          # time-step minima: exact
+        np.testing.assert_allclose(hist[:, c, 1:], h1[:, 1:], rtol=1e-12, atol=0)  # atomically summed norms
+
+
+def nks_cases():
+    sc = dict(limiter=cases.LIMITER_ZERO, local_dt=1, precision=0)
+    return [with_scheme(cases.bump_channel(nbi=6, nbj=2, nci=16, ncj=16, mach=1.4, h=0.04), **sc),
+            with_scheme(cases.bump_channel(nbi=4, nbj=2, nci=16, ncj=16, mach=1.5, h=0.03), **sc),
+            with_scheme(cases.bump_channel(nbi=6, nbj=3, nci=16, ncj=16, mach=1.3, h=0.05), **sc)]
+
+
+def test_batched_nks_equals_solo():
+    cs = nks_cases()
+    p = capi.nks_params(30, gmres_restart=20, max_gmres=120, overall_tol=1e-10, cfl0=10.0, gmres_tol=0.1)
+    hb = capi.BatchHandle(cs)
+    hb.set_state()
+    rc, hists = hb.nks(p)
+    assert rc == 0
+    states = hb.get_state()
+    hb.close()
+    for c, bs in enumerate(cs):
+        h = capi.Handle(bs)
+        h.set_state()
+        rc1, h1 = h.nks(p)
+        _, U1 = h.get_state()
+        h.close()
+        assert rc1 == 0
+        assert hists[c] == h1, c
+        assert np.array_equal(bs.interior(states[c][1]), bs.interior(U1)), c
+    # cases leave the batch at different Newton steps (converged or not)
+    assert sum(x[-1]["ratio"] <= 1e-10 for x in hists) >= 1
+    assert len({len(x) for x in hists}) > 1
+
+
+def test_batch_rejects_mismatched_blocks():
+    a = cases.periodic_box_bumps(nb=2, nc=16, seed=1)
+    b = cases.periodic_box_bumps(nb=2, nc=8, seed=1)
+    with pytest.raises(RuntimeError):
+        capi.BatchHandle([a, b])
