@@ -224,6 +224,42 @@ def nks_measure(precision, device, cpu):
     return out
 
 
+def nks_batch_measure(precision, device, n_cases=16):
+    """A sweep of steady cases (cases.bump_family: Mach, bump height and
+    block layout drawn per case, 8-48 blocks of 32x32 cells) solved to a
+    1e-10 drop as one batched handle, and one after another on single-case
+    handles (the plain GPU path), from the freestream."""
+    from cffc_b200 import capi, cases
+    fam = cases.bump_family(n_cases, precision=precision)
+    p = capi.nks_params(**NKS_PARAMS)
+    warm = capi.Handle(fam[0], device=device)
+    warm.set_state()
+    warm.nks(capi.nks_params(2, gmres_restart=30, max_gmres=20))
+    warm.close()
+    t0 = time.perf_counter()
+    hb = capi.BatchHandle(fam, device=device)
+    hb.set_state()
+    rc, hists = hb.nks(p)
+    hb.close()
+    t_batch = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    solo_ok = 0
+    for bs in fam:
+        h = capi.Handle(bs, device=device)
+        h.set_state()
+        rc1, h1 = h.nks(p)
+        h.close()
+        solo_ok += int(rc1 == 0 and h1[-1]["ratio"] <= NKS_PARAMS["overall_tol"])
+    t_solo = time.perf_counter() - t0
+    conv = sum(int(x and x[-1]["ratio"] <= NKS_PARAMS["overall_tol"]) for x in hists)
+    return {"workload": f"{n_cases} supersonic bump cases (cases.bump_family, 8-48 blocks of 32x32, "
+                        f"{sum(b.n_interior for b in fam)} cells in all), first order, to a 1e-10 drop",
+            "batched_seconds": round(t_batch, 3), "sequential_seconds": round(t_solo, 3),
+            "speedup": round(t_solo / t_batch, 2), "converged": conv, "converged_sequential": solo_ok,
+            "newton_steps": [len(x) - 1 for x in hists],
+            "gmres_iterations": sum(st["gmres_iters"] for x in hists for st in x)}
+
+
 def workload():
     from cffc_b200 import cases
     return cases.curvilinear_mach2()
@@ -395,6 +431,7 @@ def main():
             line["cpu_baseline"] = cpu_baseline(bs)
         if world == 1 and not args.no_nks:
             line["nks"] = nks_measure(PRECISION[args.precision], local, not args.no_cpu_baseline)
+            line["nks_batch"] = nks_batch_measure(PRECISION[args.precision], local)
         print(json.dumps(line), flush=True)
     h.close()
     if world > 1:

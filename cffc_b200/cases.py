@@ -386,3 +386,25 @@ def read_case(path: str) -> BlockSet:
     return BlockSet(nci, ncj, a["neighbour"], a["bc_w"], a["bc_e"], a["bc_s"], a["bc_n"], a["node_x"],
                     a["node_y"], a["wo_w"], a["wo_e"], a["wo_s"], a["wo_n"], a["W"], scheme,
                     os.path.basename(path), ng, nbi, nbj, periodic).contiguous()
+
+
+def bump_family(n_cases: int, seed: int = 20261205, mach=(1.35, 1.6), height=(0.02, 0.045),
+                layouts=((4, 2), (6, 2), (8, 2), (6, 3), (8, 3), (12, 2), (8, 4), (12, 4)), nc: int = 32,
+                precision: int = 0) -> list:
+    """A sweep of steady supersonic bump-channel cases for batched solves:
+    per case (PCG64(seed), in this order) Mach ~ U(mach), bump height ~
+    U(height) and a block layout drawn from `layouts` (nbi x nbj blocks of
+    nc x nc cells: 8 to 48 blocks).  First order (limiter zero), local time
+    stepping: the configuration the reference's block-Jacobi Newton-Krylov
+    drives to a 1e-10 residual drop."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for k in range(n_cases):
+        m = rng.uniform(*mach)
+        h = rng.uniform(*height)
+        nbi, nbj = layouts[int(rng.integers(len(layouts)))]
+        bs = bump_channel(nbi=nbi, nbj=nbj, nci=nc, ncj=nc, mach=m, h=h,
+                          scheme=Scheme(limiter=LIMITER_ZERO, local_dt=1, precision=precision))
+        bs.name = f"bump_m{m:.3f}_h{h:.4f}_{nbi}x{nbj}"
+        out.append(bs)
+    return out

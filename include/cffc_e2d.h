@@ -175,6 +175,13 @@ int e2d_cfl(e2d_handle *h, double *dt, double *dtmin);
  * entry, or a library error. */
 int e2d_solver_run(const char *input_file, int batch_flag);
 
+/* Self-test of the tensor-core path the warm-start network uses (tcgen05,
+ * BF16 operands in shared memory, FP32 accumulator in TMEM): D[128][N] =
+ * A[128][K] * B[N][K]^T for host BF16 bit patterns A, B and host FP32 D;
+ * 16 <= N <= 256 and 16 <= K <= 128, multiples of 16.  No reference
+ * counterpart. */
+int e2d_tc_selftest(const uint16_t *A, const uint16_t *B, float *D, int N, int K);
+
 /* Newton-Krylov-Schwarz parameters: the NKS_Input_Parameters fields the
  * Euler2D steady path reads (src_2D/NewtonKrylovSchwarz2D/NKSInput2D.h:128-172;
  * defaults in brackets).  The preconditioner is block Jacobi on the
