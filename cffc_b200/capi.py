@@ -71,7 +71,8 @@ class NksParams(C.Structure):
     _fields_ = [("max_newton", C.c_int32), ("gmres_restart", C.c_int32), ("max_gmres", C.c_int32),
                 ("reserved", C.c_int32), ("overall_tol", C.c_double), ("cfl0", C.c_double),
                 ("gmres_tol_initial", C.c_double), ("gmres_tol_final", C.c_double),
-                ("epsilon0", C.c_double), ("min_ratio", C.c_double)]
+                ("epsilon0", C.c_double), ("min_ratio", C.c_double),
+                ("l2_reference", C.POINTER(C.c_double))]
 
 
 class NksStep(C.Structure):
@@ -273,8 +274,12 @@ class BatchHandle(Handle):
         rc = self._call("rk_steps", n, ptr(hist))
         return rc, hist
 
-    def nks(self, params: NksParams):
+    def nks(self, params: NksParams, l2_reference=None):
         C_ = len(self.cases)
+        ref = None
+        if l2_reference is not None:
+            ref = np.ascontiguousarray(l2_reference, dtype=np.float64)
+            params.l2_reference = ref.ctypes.data_as(C.POINTER(C.c_double))
         m = max(params.max_newton, 1)
         steps = (NksStep * (m * C_))()
         counts = (C.c_int * C_)()
@@ -282,4 +287,5 @@ class BatchHandle(Handle):
         rc = self._call("nks", C.byref(params), steps, counts)
         hists = [[{f: getattr(steps[c * m + k], f) for f, _ in NksStep._fields_ if f != "pad"}
                   for k in range(counts[c])] for c in range(C_)]
+        params.l2_reference = None
         return rc, hists

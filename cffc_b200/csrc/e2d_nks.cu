@@ -872,7 +872,8 @@ extern "C" int e2d_nks(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* his
       if (!on[c]) continue;
       const double l2 = slots[4 * c + 2];
       if (!std::isfinite(l2)) return finish(E2D_ERR_NAN);
-      if (l2_first[c] <= 0.0) l2_first[c] = l2;
+      if (l2_first[c] <= 0.0)
+        l2_first[c] = (p->l2_reference && p->l2_reference[c] > 0.0) ? p->l2_reference[c] : l2;
       ratio[c] = l2 / l2_first[c];
       cur[c] = e2d_nks_step{};
       cur[c].l1 = slots[4 * c + 1]; cur[c].l2 = l2; cur[c].lmax = slots[4 * c + 3]; cur[c].ratio = ratio[c];

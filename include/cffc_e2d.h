@@ -182,6 +182,31 @@ int e2d_solver_run(const char *input_file, int batch_flag);
  * counterpart. */
 int e2d_tc_selftest(const uint16_t *A, const uint16_t *B, float *D, int N, int K);
 
+/* ---- Learned warm start (no reference counterpart) ---------------------
+ * A per-cell network, 16 input features -> 128 -> 128 (tanh) -> 4 outputs,
+ * evaluated and trained by tcgen05 kernels (BF16 operands, FP32
+ * accumulation in TMEM).  The caller builds the features and targets (the
+ * normalised converged state of cases the Newton-Krylov solver produced);
+ * its prediction seeds e2d_set_state, and the solver then drives every case
+ * to the same residual tolerance as from the freestream.
+ * Parameters, flat FP32 (e2d_mlp_nparams() of them): W1[128][16], b1[128],
+ * W2[128][128], b2[128], W3[16][128] (rows 4..15 unused), b3[16].
+ * X, T, Y are device pointers: X[n][16], T[n][4], Y[n][4] FP32; stream is a
+ * cudaStream_t or NULL. */
+typedef struct e2d_mlp e2d_mlp;
+e2d_mlp *e2d_mlp_create(uint64_t seed, int *err);  /* Glorot-uniform weights */
+void e2d_mlp_destroy(e2d_mlp *m);
+int e2d_mlp_nparams(void);
+/* out (host, may be NULL) <- parameters; then parameters <- in (may be NULL) */
+int e2d_mlp_params(e2d_mlp *m, float *out, const float *in);
+int e2d_mlp_forward(e2d_mlp *m, const float *X, int n, float *Y, void *stream);
+/* gradient of sum((Y - T)^2) / n into grad (host, may be NULL), loss (host) */
+int e2d_mlp_gradient(e2d_mlp *m, const float *X, const float *T, int n, float *grad, double *loss,
+                     void *stream);
+/* steps of full-batch Adam (0.9, 0.999, 1e-8) at learning rate lr */
+int e2d_mlp_train(e2d_mlp *m, const float *X, const float *T, int n, int steps, float lr, float *loss_hist,
+                  void *stream);
+
 /* Newton-Krylov-Schwarz parameters: the NKS_Input_Parameters fields the
  * Euler2D steady path reads (src_2D/NewtonKrylovSchwarz2D/NKSInput2D.h:128-172;
  * defaults in brackets).  The preconditioner is block Jacobi on the
@@ -197,6 +222,11 @@ typedef struct e2d_nks_params {
   double gmres_tol_final;    /* GMRES_Final_Tolerance               [1e-5]  */
   double epsilon0;           /* Epsilon_Naught                      [1e-6]  */
   double min_ratio;          /* Min_Finite_Time_Step_Norm_Ratio     [1e-10] */
+  /* Per case (host, may be NULL): the L2 the residual ratio, the tolerance
+   * and the SER CFL are measured against instead of the first residual
+   * (library extension; a warm-started case passes its freestream residual
+   * so that it is driven to the same absolute level as a cold start). */
+  const double *l2_reference;
 } e2d_nks_params;
 
 /* One Newton step of the history (the values the reference prints). */

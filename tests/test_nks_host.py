@@ -12,8 +12,9 @@ from helpers import fixtures, load
 
 
 def test_struct_layouts_match_header():
-    # e2d_nks_params: 4 int32 + 6 double; e2d_nks_step: 7 double + 4 int32
-    assert ctypes.sizeof(capi.NksParams) == 64
+    # e2d_nks_params: 4 int32 + 6 double + 1 pointer; e2d_nks_step: 7 double + 4 int32
+    assert ctypes.sizeof(capi.NksParams) == 72
+    assert capi.NksParams.l2_reference.offset == 64
     assert ctypes.sizeof(capi.NksStep) == 72
     assert capi.NksStep.gmres_iters.offset == 56
 
