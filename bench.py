@@ -260,6 +260,50 @@ def nks_batch_measure(precision, device, n_cases=16):
             "gmres_iterations": sum(st["gmres_iters"] for x in hists for st in x)}
 
 
+def nks_learned_measure(device):
+    """Learned + batched against plain: a network trained on 48 solved cases
+    of the family seeds 16 held-out cases; seconds to the same absolute
+    residual level (1e-10 of each case's freestream residual) for the
+    warm-started batch, the cold batch, and cold single-case solves one
+    after another (the plain GPU path)."""
+    import numpy as np
+
+    from cffc_b200 import capi, cases, warmstart
+    p = capi.nks_params(**NKS_PARAMS)
+    net, info = warmstart.train_network(cases.bump_family(48, seed=101), p, device=device)
+    test = cases.bump_family(16, seed=202)
+    warmstart.solve_family(test[:2], p, device=device)  # warm-up of the batch path
+    t0 = time.perf_counter()
+    rc_c, cold, cold_states = warmstart.solve_family(test, p, device=device)
+    t_cold = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    rc_w, warm, warm_states = warmstart.warm_solve(net, test, p, device=device)
+    t_warm = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for bs in test:
+        h = capi.Handle(bs, device=device)
+        h.set_state()
+        h.nks(p)
+        h.close()
+    t_seq = time.perf_counter() - t0
+    err = max(warmstart.l2_cells(bs.interior(a[1]), bs.interior(b[1]))
+              for bs, a, b in zip(test, warm_states, cold_states))
+    tol = NKS_PARAMS["overall_tol"]
+    return {"workload": "16 held-out cases of cases.bump_family (seed 202), network trained on 48 (seed 101)",
+            "training": info,
+            "warm_batched_seconds": round(t_warm, 3), "cold_batched_seconds": round(t_cold, 3),
+            "cold_sequential_seconds": round(t_seq, 3),
+            "speedup_vs_plain_sequential": round(t_seq / t_warm, 2),
+            "speedup_vs_cold_batched": round(t_cold / t_warm, 2),
+            "newton_steps_warm": int(sum(len(x) - 1 for x in warm)),
+            "newton_steps_cold": int(sum(len(x) - 1 for x in cold)),
+            "gmres_iterations_warm": int(sum(st["gmres_iters"] for x in warm for st in x)),
+            "gmres_iterations_cold": int(sum(st["gmres_iters"] for x in cold for st in x)),
+            "converged_warm": int(sum(x[-1]["ratio"] <= tol for x in warm)),
+            "converged_cold": int(sum(x[-1]["ratio"] <= tol for x in cold)),
+            "max_l2_error_warm_vs_cold": float(err), "rc": [rc_w, rc_c]}
+
+
 def workload():
     from cffc_b200 import cases
     return cases.curvilinear_mach2()
@@ -432,6 +476,7 @@ def main():
         if world == 1 and not args.no_nks:
             line["nks"] = nks_measure(PRECISION[args.precision], local, not args.no_cpu_baseline)
             line["nks_batch"] = nks_batch_measure(PRECISION[args.precision], local)
+            line["nks_learned"] = nks_learned_measure(local)
         print(json.dumps(line), flush=True)
     h.close()
     if world > 1:

@@ -207,3 +207,50 @@ def predict_states(net, fam):
 
 def l2_cells(a, b):
     return float(math.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)))
+
+
+def warm_solve(net, fam, params, smooth_steps: int = 150, device=0):
+    """The warm-started batched solve: freestream residuals (the reference
+    level), the network's prediction, smooth_steps explicit local-time-step
+    RK steps that damp its high-frequency error, then Newton-Krylov to the
+    cold start's absolute residual level.  Returns (rc, hists, states)."""
+    l2 = freestream_l2(fam, device=device)
+    Ws = predict_states(net, fam)
+    hb = capi.BatchHandle(fam, device=device)
+    hb.set_state(Ws)
+    if smooth_steps:
+        rc, _ = hb.rk_steps(smooth_steps, history=False)
+        if rc:
+            hb.close()
+            return rc, [], []
+    rc, hists = hb.nks(params, l2)
+    states = hb.get_state()
+    hb.close()
+    return rc, hists, states
+
+
+def train_network(train_fam, params, steps=((3e-3, 1500), (1e-3, 1500), (3e-4, 1000)), seed=11, device=0):
+    """Solves the training cases (batched, from the freestream), builds the
+    per-cell training set from their converged states and trains a network
+    on it.  Returns (net, info)."""
+    import time
+
+    import torch
+    t0 = time.perf_counter()
+    rc, hists, states = solve_family(train_fam, params, device=device)
+    t_solve = time.perf_counter() - t0
+    if rc:
+        raise RuntimeError(f"training-set solve failed: {rc}")
+    X, T = build_training_set(train_fam, states)
+    Xd, Td = torch.from_numpy(X).cuda(device), torch.from_numpy(T).cuda(device)
+    net = Mlp(seed=seed)
+    t0 = time.perf_counter()
+    losses = []
+    for lr, n in steps:
+        losses.append(net.train(Xd, Td, n, lr))
+    t_train = time.perf_counter() - t0
+    loss = np.concatenate(losses)
+    return net, {"cases": len(train_fam), "cells": int(X.shape[0]), "solve_seconds": round(t_solve, 3),
+                 "train_seconds": round(t_train, 3), "adam_steps": int(loss.size),
+                 "loss_first": float(loss[0]), "loss_last": float(loss[-1]),
+                 "converged": int(sum(h[-1]["ratio"] <= params.overall_tol for h in hists))}

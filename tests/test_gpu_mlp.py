@@ -81,9 +81,7 @@ def test_warm_start_reaches_same_solution_faster():
     assert hist[-1] < 0.05 * hist[0]
     rc, cold, cold_states = warmstart.solve_family(test, p)
     assert rc == 0
-    l2_fs = warmstart.freestream_l2(test)
-    Ws = warmstart.predict_states(net, test)
-    rc, warm, warm_states = warmstart.solve_family(test, p, Ws=Ws, l2_ref=l2_fs)
+    rc, warm, warm_states = warmstart.warm_solve(net, test, p)
     assert rc == 0
     for c, bs in enumerate(test):
         assert cold[c][-1]["ratio"] <= 1e-10 and warm[c][-1]["ratio"] <= 1e-10
