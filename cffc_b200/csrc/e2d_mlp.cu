@@ -12,7 +12,9 @@
 //             dW3^T = H2^T dY      (M = h, K = c)     dH2 = dY W3      (M = c)
 //             dZ2 = dH2 (1 - H2^2); dW2 = dZ2^T H1  (M = o, K = c)
 //             dH1 = dZ2 W2; dZ1 = dH1 (1 - H1^2);   dW1 = dZ1^T X   (M = h, K = c)
-// Weight gradients of all tiles are summed with FP32 atomics.
+// Each CTA accumulates its tiles' weight gradients in TMEM (FP32) and
+// writes them to its own slot; the slots are summed in CTA order, so
+// training is deterministic.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -150,7 +152,8 @@ struct MlpSmem {
   uint8_t R[MH * TILE * 2];    // H1T [MH][cells] (B of dW2, train)
   uint8_t S[MH * TILE * 2];    // H2T [MH][cells] (A of dW3^T), then dZ1T (A of dW1) (train)
   float b1[MH], b2[MH], b3[MO];
-  float gb1[MH], gb2[MH], gb3[MO];  // per-CTA bias gradients (train)
+  float gb1[4][MH], gb2[4][MH], gb3[4][MO];  // per-warp bias gradients (train)
+  double lw[4];                                // per-warp loss sums
 };
 
 __device__ __forceinline__ uint16_t f2bf(float x) {
@@ -210,7 +213,8 @@ constexpr uint32_t C_D1 = 0, C_D2 = 128, C_D3 = 0, C_GW3 = 256, C_GW1 = 272, C_G
 // Persistent kernel over tiles of 128 cells.  TRAIN = false: Y = f(X) for the
 // rows of the tiles.  TRAIN = true: the gradient of
 // loss = sum over rows and the four outputs of (y - t)^2 / n_total,
-// accumulated in TMEM over the CTA's tiles and added to grad (FP32 atomics).
+// accumulated in TMEM over the CTA's tiles and written to the CTA's slot of
+// grad (and of loss).
 template <bool TRAIN>
 __global__ void __launch_bounds__(TILE, 1) mlp_kernel(MlpDev w, const float* __restrict__ X,
                                                       const float* __restrict__ T, int n, float inv_n,
@@ -229,10 +233,12 @@ __global__ void __launch_bounds__(TILE, 1) mlp_kernel(MlpDev w, const float* __r
   for (int k = tid; k < MH; k += TILE) {
     s.b1[k] = w.p[P_B1 + k];
     s.b2[k] = w.p[P_B2 + k];
-    s.gb1[k] = 0.0f;
-    s.gb2[k] = 0.0f;
+    for (int q = 0; q < 4; ++q) { s.gb1[q][k] = 0.0f; s.gb2[q][k] = 0.0f; }
   }
-  if (tid < MO) { s.b3[tid] = w.p[P_B3 + tid]; s.gb3[tid] = 0.0f; }
+  if (tid < MO) {
+    s.b3[tid] = w.p[P_B3 + tid];
+    for (int q = 0; q < 4; ++q) s.gb3[q][tid] = 0.0f;
+  }
   if (tid == 0) tc::mbar_init(&bar, 1);
   if (warp == 0) tc::tmem_alloc(&taddr, ncols);
   cta_sync_async();
@@ -316,7 +322,7 @@ __global__ void __launch_bounds__(TILE, 1) mlp_kernel(MlpDev w, const float* __r
 #pragma unroll
     for (int q = 0; q < MO_USED; ++q) {
       const float t = warp_sum(dy[q]);
-      if (lane == 0) atomicAdd(&s.gb3[q], t);
+      if (lane == 0) s.gb3[warp][q] += t;
     }
     stage_rows(s.W23, w.w2t, MH, MH);
     cta_sync_async();
@@ -335,7 +341,7 @@ __global__ void __launch_bounds__(TILE, 1) mlp_kernel(MlpDev w, const float* __r
         const float dz = valid ? v[q] * (1.0f - h2 * h2) : 0.0f;
         st_bf(s.P, tc::kmaj_off(tid, c0 + q, MH), dz);  // dZ2 (H1 is no longer read)
         const float t = warp_sum(dz);
-        if (lane == 0) atomicAdd(&s.gb2[c0 + q], t);
+        if (lane == 0) s.gb2[warp][c0 + q] += t;
       }
     }
     __syncthreads();  // H2 in Q is read no more: dZ2T overwrites it
@@ -358,7 +364,7 @@ __global__ void __launch_bounds__(TILE, 1) mlp_kernel(MlpDev w, const float* __r
         const float dz = valid ? v[q] * (1.0f - h1 * h1) : 0.0f;
         st_bf(s.S, tc::kmaj_off(c0 + q, tid, TILE), dz);  // dZ1T (H2T was consumed by B1)
         const float t = warp_sum(dz);
-        if (lane == 0) atomicAdd(&s.gb1[c0 + q], t);
+        if (lane == 0) s.gb1[warp][c0 + q] += t;
       }
     }
     cta_sync_async();
@@ -371,30 +377,34 @@ __global__ void __launch_bounds__(TILE, 1) mlp_kernel(MlpDev w, const float* __r
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
   } else if (TRAIN && !first) {
-    // the CTA's accumulated weight gradients (TMEM lane = output row)
+    // the CTA's accumulated gradients into its own slot of grad (summed
+    // over the CTAs in CTA order by mlp_reduce_kernel: training is
+    // deterministic); TMEM lane = output row
+    float* gs = grad + size_t(blockIdx.x) * NPARAM;
     const int r = tid;
     float v[16];
     tc::tmem_ld16(tm + lane_base + C_GW3, v);  // dW3^T: row h, columns o
 #pragma unroll
-    for (int q = 0; q < MO_USED; ++q) atomicAdd(&grad[P_W3 + q * MH + r], v[q]);
+    for (int q = 0; q < MO; ++q) gs[P_W3 + q * MH + r] = q < MO_USED ? v[q] : 0.0f;
     tc::tmem_ld16(tm + lane_base + C_GW1, v);  // dW1: row h, columns f
 #pragma unroll
-    for (int q = 0; q < MF; ++q) atomicAdd(&grad[P_W1 + r * MF + q], v[q]);
+    for (int q = 0; q < MF; ++q) gs[P_W1 + r * MF + q] = v[q];
     for (int c0 = 0; c0 < MH; c0 += 16) {       // dW2: row o, columns h
       tc::tmem_ld16(tm + lane_base + C_GW2 + c0, v);
 #pragma unroll
-      for (int q = 0; q < 16; ++q) atomicAdd(&grad[P_W2 + r * MH + c0 + q], v[q]);
+      for (int q = 0; q < 16; ++q) gs[P_W2 + r * MH + c0 + q] = v[q];
     }
     __syncthreads();
-    atomicAdd(&grad[P_B1 + r], s.gb1[r]);
-    atomicAdd(&grad[P_B2 + r], s.gb2[r]);
-    if (r < MO_USED) atomicAdd(&grad[P_B3 + r], s.gb3[r]);
+    gs[P_B1 + r] = ((s.gb1[0][r] + s.gb1[1][r]) + s.gb1[2][r]) + s.gb1[3][r];
+    gs[P_B2 + r] = ((s.gb2[0][r] + s.gb2[1][r]) + s.gb2[2][r]) + s.gb2[3][r];
+    if (r < MO) gs[P_B3 + r] = r < MO_USED ? ((s.gb3[0][r] + s.gb3[1][r]) + s.gb3[2][r]) + s.gb3[3][r] : 0.0f;
   }
   if (TRAIN && ok) {
-    const double t = lsum;
-    double sum = t;
+    double sum = lsum;
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    if (lane == 0) atomicAdd(loss, sum);
+    if (lane == 0) s.lw[warp] = sum;
+    __syncthreads();
+    if (tid == 0) loss[blockIdx.x] = ((s.lw[0] + s.lw[1]) + s.lw[2]) + s.lw[3];
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -432,11 +442,28 @@ __global__ void adam_kernel(float* p, const float* g, float* m, float* v, int n,
   }
 }
 
+// grad[q] = sum over the CTAs' slots in CTA order; loss likewise.
+__global__ void mlp_reduce_kernel(const float* __restrict__ parts, int nparts, float* __restrict__ grad,
+                                  const double* lparts, double* loss) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < NPARAM; q += gridDim.x * blockDim.x) {
+    float t = 0.0f;
+    for (int c = 0; c < nparts; ++c) t += parts[size_t(c) * NPARAM + q];
+    grad[q] = t;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double t = 0.0;
+    for (int c = 0; c < nparts; ++c) t += lparts[c];
+    *loss = t;
+  }
+}
+
 }  // namespace
 
 struct e2d_mlp {
   int device = 0;
   float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+  float* gpart = nullptr;     // [sms][NPARAM] per-CTA gradient slots
+  double* lpart = nullptr;    // [sms] per-CTA loss sums
   uint16_t *w1 = nullptr, *w2 = nullptr, *w3 = nullptr, *w2t = nullptr, *w3t = nullptr;
   double* loss = nullptr;
   int* err = nullptr;
@@ -465,8 +492,14 @@ int mlp_launch(e2d_mlp* mm, const float* X, const float* T, int n, float* Y, cud
   }
   const int ntiles = (n + TILE - 1) / TILE;
   const int grid = ntiles < mm->sms ? ntiles : mm->sms;  // persistent: one CTA per SM
-  mlp_kernel<TRAIN><<<grid, TILE, smem, st>>>(dev_of(mm), X, T, n, 1.0f / float(n), Y, mm->g, mm->loss, mm->err);
-  return cudaGetLastError() == cudaSuccess ? 0 : E2D_ERR_CUDA;
+  mlp_kernel<TRAIN><<<grid, TILE, smem, st>>>(dev_of(mm), X, T, n, 1.0f / float(n), Y, mm->gpart, mm->lpart,
+                                               mm->err);
+  if (cudaGetLastError() != cudaSuccess) return E2D_ERR_CUDA;
+  if (TRAIN) {
+    mlp_reduce_kernel<<<(NPARAM + 255) / 256, 256, 0, st>>>(mm->gpart, grid, mm->g, mm->lpart, mm->loss);
+    if (cudaGetLastError() != cudaSuccess) return E2D_ERR_CUDA;
+  }
+  return 0;
 }
 
 int mlp_check(e2d_mlp* mm, cudaStream_t st) {
@@ -502,6 +535,7 @@ e2d_mlp* e2d_mlp_create(uint64_t seed, int* err) {
              cudaMalloc(&mm->v, 4 * NPARAM) || cudaMalloc(&mm->w1, 2 * MH * MF) || cudaMalloc(&mm->w2, 2 * MH * MH) ||
              cudaMalloc(&mm->w3, 2 * MO * MH) || cudaMalloc(&mm->w2t, 2 * MH * MH) ||
              cudaMalloc(&mm->w3t, 2 * MO * MH) || cudaMalloc(&mm->loss, sizeof(double)) ||
+             cudaMalloc(&mm->gpart, 4 * size_t(NPARAM) * mm->sms) || cudaMalloc(&mm->lpart, sizeof(double) * mm->sms) ||
              cudaMalloc(&mm->err, sizeof(int));
   if (bad) {
     if (err) *err = E2D_ERR_NOMEM;
@@ -530,7 +564,7 @@ e2d_mlp* e2d_mlp_create(uint64_t seed, int* err) {
 
 void e2d_mlp_destroy(e2d_mlp* mm) {
   if (!mm) return;
-  for (void* q : {(void*)mm->p, (void*)mm->g, (void*)mm->m, (void*)mm->v, (void*)mm->w1, (void*)mm->w2,
+  for (void* q : {(void*)mm->gpart, (void*)mm->lpart, (void*)mm->p, (void*)mm->g, (void*)mm->m, (void*)mm->v, (void*)mm->w1, (void*)mm->w2,
                   (void*)mm->w3, (void*)mm->w2t, (void*)mm->w3t, (void*)mm->loss, (void*)mm->err})
     if (q) cudaFree(q);
   delete mm;
@@ -558,9 +592,6 @@ int e2d_mlp_forward(e2d_mlp* mm, const float* X, int n, float* Y, void* stream) 
 int e2d_mlp_gradient(e2d_mlp* mm, const float* X, const float* T, int n, float* grad, double* loss, void* stream) {
   if (!mm || !X || !T || n < 1) return E2D_ERR_ARG;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (cudaMemsetAsync(mm->g, 0, 4 * NPARAM, st) != cudaSuccess ||
-      cudaMemsetAsync(mm->loss, 0, sizeof(double), st) != cudaSuccess)
-    return E2D_ERR_CUDA;
   int rc = mlp_launch<true>(mm, X, T, n, nullptr, st);
   if (rc || (rc = mlp_check(mm, st))) return rc;
   if (grad && cudaMemcpy(grad, mm->g, 4 * NPARAM, cudaMemcpyDeviceToHost) != cudaSuccess) return E2D_ERR_CUDA;

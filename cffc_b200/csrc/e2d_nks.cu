@@ -57,35 +57,54 @@ __device__ double cta_sum(double v) {
   return s;  // valid in thread 0
 }
 
-// partial[b] = sum over block b of a*b (one CTA per block; nper2 double2
-// entries per block).
+// Reductions: each block's entries are split into `ch` chunks, one CTA per
+// chunk; the CTA writes its partial sum to partial[block * ch + chunk], and
+// the last CTA of a case to arrive (per-case counter) sums the case's
+// partials in block and chunk order — a fixed order, whichever CTA is last —
+// and writes out[c] = f(sum): the sum, its square root, or eps0 / sqrt
+// (calculate_epsilon, GMRES2D.h:1628-1640).
+__device__ void partial_done(double s, double* partial, int slot, const Blocks& B, int c, int ch, unsigned* counter,
+                             double* out, int fin, double eps0) {
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    partial[slot] = s;
+    __threadfence();
+    const int b0 = B.case_start ? B.case_start[c] : 0, b1 = B.case_start ? B.case_start[c + 1] : B.nblk;
+    const unsigned n = unsigned((b1 - b0) * ch);
+    last = atomicAdd(&counter[c], 1u) == n - 1;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x >= 32) return;
+  __threadfence();
+  const int b0 = B.case_start ? B.case_start[c] : 0, b1 = B.case_start ? B.case_start[c + 1] : B.nblk;
+  double t = 0.0;
+  for (int q = b0 * ch + threadIdx.x; q < b1 * ch; q += 32) t += ((volatile double*)partial)[q];
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if (threadIdx.x == 0) {
+    out[c] = fin == FIN_SUM ? t : (fin == FIN_SQRT ? sqrt(t) : eps0 / sqrt(t));
+    counter[c] = 0u;
+  }
+}
+
+// out[case] = f(sum of a*b over the case); grid = nblk * ch CTAs, nper2
+// double2 entries per block.
 __global__ void __launch_bounds__(VT) blk_dot_kernel(const double* __restrict__ a, const double* __restrict__ bv,
-                                                     int nper2, double* partial, Blocks B) {
-  const int blk = blockIdx.x;
-  if (!case_on(B, case_id(B, blk))) return;  // uniform per CTA
+                                                     int nper2, int ch, double* partial, unsigned* counter,
+                                                     double* out, int fin, double eps0, Blocks B) {
+  const int blk = blockIdx.x / ch, part = blockIdx.x % ch;
+  const int c = case_id(B, blk);
+  if (!case_on(B, c)) return;  // uniform per CTA
+  const int len = (nper2 + ch - 1) / ch, q0 = part * len, q1 = min(nper2, q0 + len);
   const double2* a2 = reinterpret_cast<const double2*>(a) + size_t(blk) * nper2;
   const double2* b2 = reinterpret_cast<const double2*>(bv) + size_t(blk) * nper2;
   double s = 0.0;
-  for (int q = threadIdx.x; q < nper2; q += VT) {
+  for (int q = q0 + threadIdx.x; q < q1; q += VT) {
     const double2 x = a2[q], y = b2[q];
     s += x.x * y.x;
     s += x.y * y.y;
   }
   s = cta_sum(s);
-  if (threadIdx.x == 0) partial[blk] = s;
-}
-
-// out[c] = f(sum of the case's block partials in block order): the sum,
-// its square root, or eps0 / sqrt (calculate_epsilon, GMRES2D.h:1628-1640).
-// One warp per case.
-__global__ void case_final_kernel(const double* partial, Blocks B, double* out, int fin, double eps0) {
-  const int c = blockIdx.x;
-  if (threadIdx.x >= 32 || !case_on(B, c)) return;
-  const int b0 = B.case_start ? B.case_start[c] : 0, b1 = B.case_start ? B.case_start[c + 1] : B.nblk;
-  double s = 0.0;
-  for (int b = b0 + threadIdx.x; b < b1; b += 32) s += partial[b];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (threadIdx.x == 0) out[c] = fin == FIN_SUM ? s : (fin == FIN_SQRT ? sqrt(s) : eps0 / sqrt(s));
+  partial_done(s, partial, blockIdx.x, B, c, ch, counter, out, fin, eps0);
 }
 
 // y += alpha * x, alpha = sign * coef[case] (device, per case) or alpha_h.
@@ -135,15 +154,18 @@ __global__ void __launch_bounds__(VT) update_x_kernel(double* __restrict__ x, co
   }
 }
 
-// z = Minv v per cell of block blockIdx.x, and partial[b] = sum z^2 (the
-// numerator of eps = eps0 / ||z||).
+// z = Minv v per cell, and eps[case] = eps0 / ||z|| over the case; grid =
+// nblk * ch CTAs, each a chunk of a block's cells.
 __global__ void __launch_bounds__(VT) precon_apply_kernel(const double* __restrict__ Minv, const double* __restrict__ v,
-                                                          double* __restrict__ z, int cells_per_block, double* partial,
-                                                          Blocks B) {
-  const int blk = blockIdx.x;
-  if (!case_on(B, case_id(B, blk))) return;
+                                                          double* __restrict__ z, int cells_per_block, int ch,
+                                                          double* partial, unsigned* counter, double* eps_out,
+                                                          double eps0, Blocks B) {
+  const int blk = blockIdx.x / ch, part = blockIdx.x % ch;
+  const int cs = case_id(B, blk);
+  if (!case_on(B, cs)) return;
+  const int len = (cells_per_block + ch - 1) / ch, r0 = part * len, r1 = min(cells_per_block, r0 + len);
   double s = 0.0;
-  for (int r = threadIdx.x; r < cells_per_block; r += VT) {
+  for (int r = r0 + threadIdx.x; r < r1; r += VT) {
     const size_t c = size_t(blk) * cells_per_block + r;
     const double2* v2 = reinterpret_cast<const double2*>(v + 4 * c);
     const double2 va = v2[0], vb = v2[1];
@@ -164,7 +186,7 @@ __global__ void __launch_bounds__(VT) precon_apply_kernel(const double* __restri
     z2[1] = make_double2(o[2], o[3]);
   }
   s = cta_sum(s);
-  if (threadIdx.x == 0) partial[blk] = s;
+  partial_done(s, partial, blockIdx.x, B, cs, ch, counter, eps_out, FIN_EPS, eps0);
 }
 
 struct Norm4 {
@@ -497,7 +519,9 @@ struct e2d_nks_state {
   double* x = nullptr;
   double* V = nullptr;       // (m + 1) * n
   double* Z = nullptr;       // m * n
-  double* partial = nullptr; // [nblk]
+  double* partial = nullptr; // [nblk * ch]
+  unsigned* counter = nullptr; // [ncase] arrivals of the reduction CTAs
+  int ch_vec = 1, ch_cell = 1; // CTAs per block of the vector / per-cell reductions
   double* eps = nullptr;     // [ncase]
   double* nrm = nullptr;     // [ncase]
   double* hcol = nullptr;    // [m + 2][ncase]
@@ -550,7 +574,8 @@ int nks_setup(e2d_handle* h, int m) {
   int rc;
   if ((rc = nalloc(s, &s->Uo, n)) || (rc = nalloc(s, &s->Minv, 16 * h->ncell)) || (rc = nalloc(s, &s->bvec, n)) ||
       (rc = nalloc(s, &s->x, n)) || (rc = nalloc(s, &s->V, (m + 1) * n)) || (rc = nalloc(s, &s->Z, m * n)) ||
-      (rc = nalloc(s, &s->partial, h->B.nblk)) || (rc = nalloc(s, &s->eps, C)) || (rc = nalloc(s, &s->nrm, C)) ||
+      (rc = nalloc(s, &s->partial, size_t(h->B.nblk) * 16)) || (rc = nalloc(s, &s->counter, C)) ||
+      (rc = nalloc(s, &s->eps, C)) || (rc = nalloc(s, &s->nrm, C)) ||
       (rc = nalloc(s, &s->hcol, size_t(m + 2) * C)) || (rc = nalloc(s, &s->svals, size_t(m) * C)) ||
       (rc = nalloc(s, &s->kcount, C)) || (rc = nalloc(s, &s->cflv, C)) || (rc = nalloc(s, &s->active, C)) ||
       (rc = nalloc(s, &s->slots, 4 * size_t(C))) || (rc = nalloc(s, &s->step0, 1))) {
@@ -566,6 +591,11 @@ int nks_setup(e2d_handle* h, int m) {
   E2D_CK(cudaMemsetAsync(s->Z, 0, sizeof(double) * m * n, h->stream));
   E2D_CK(cudaMemsetAsync(s->bvec, 0, sizeof(double) * n, h->stream));
   E2D_CK(cudaMemsetAsync(s->step0, 0, sizeof(int), h->stream));
+  E2D_CK(cudaMemsetAsync(s->counter, 0, sizeof(unsigned) * C, h->stream));
+  // enough CTAs per block for small block counts (about 2048 double2 / 512
+  // cells per CTA), at most 16
+  s->ch_vec = std::max(1, std::min(16, s->nper4 / 2 / 2048));
+  s->ch_cell = std::max(1, std::min(16, h->B.NCi * h->B.NCj / 512));
   identity_blocks_kernel<<<VGRID, VT, 0, h->stream>>>(s->Minv, (long long)h->ncell);
   E2D_CK(cudaGetLastError());
   return 0;
@@ -634,9 +664,8 @@ int matvec(e2d_handle* h, const double* dir, double* v, const Norm4& nm) {
 int dot(e2d_handle* h, const double* a, const double* b, double* out, int fin, double eps0 = 0.0) {
   e2d_nks_state* s = h->nks;
   const Blocks B = act(h);
-  blk_dot_kernel<<<h->B.nblk, VT, 0, h->stream>>>(a, b, s->nper4 / 2, s->partial, B);
-  E2D_CK(cudaGetLastError());
-  case_final_kernel<<<s->ncase, 32, 0, h->stream>>>(s->partial, B, out, fin, eps0);
+  blk_dot_kernel<<<h->B.nblk * s->ch_vec, VT, 0, h->stream>>>(a, b, s->nper4 / 2, s->ch_vec, s->partial, s->counter,
+                                                               out, fin, eps0, B);
   E2D_CK(cudaGetLastError());
   return 0;
 }
@@ -741,9 +770,8 @@ int gmres(e2d_handle* h, const e2d_nks_params& p, const std::vector<double>& tol
       double* Vn = s->V + size_t(j + 1) * n;
       double* Zj = s->Z + size_t(j) * n;
       const Blocks B = act(h);
-      precon_apply_kernel<<<h->B.nblk, VT, 0, h->stream>>>(s->Minv, Vj, Zj, h->B.NCi * h->B.NCj, s->partial, B);
-      E2D_CK(cudaGetLastError());
-      case_final_kernel<<<C, 32, 0, h->stream>>>(s->partial, B, s->eps, FIN_EPS, p.epsilon0);
+      precon_apply_kernel<<<h->B.nblk * s->ch_cell, VT, 0, h->stream>>>(
+          s->Minv, Vj, Zj, h->B.NCi * h->B.NCj, s->ch_cell, s->partial, s->counter, s->eps, p.epsilon0, B);
       E2D_CK(cudaGetLastError());
       if ((rc = matvec(h, Zj, Vn, nm))) return rc;
       // modified Gram-Schmidt (GMRES2D.h:1224-1240)

@@ -160,27 +160,31 @@ def state_from(bs, out):
     return W
 
 
-def solve_family(fam, params, Ws=None, l2_ref=None, device=0):
+def solve_family(fam, params, Ws=None, l2_ref=None, device=0, handle=None):
     """Batched Newton-Krylov solve of a list of cases from Ws (or the
     freestream); l2_ref: per-case reference L2 for the tolerance and CFL
-    ratio (None: each case's first residual).  Returns (rc, hists, states)."""
-    hb = capi.BatchHandle(fam, device=device)
+    ratio (None: each case's first residual).  Uses `handle` (a BatchHandle
+    of fam) when given.  Returns (rc, hists, states)."""
+    hb = handle or capi.BatchHandle(fam, device=device)
     hb.set_state(Ws)
     rc, hists = hb.nks(params, l2_ref)
     states = hb.get_state()
-    hb.close()
+    if handle is None:
+        hb.close()
     return rc, hists, states
 
 
-def freestream_l2(fam, device=0):
-    """Density-residual L2 of each case at its freestream state."""
-    hb = capi.BatchHandle(fam, device=device)
+def freestream_l2(fam, device=0, handle=None):
+    """Density-residual L2 of each case at its freestream state (on `handle`,
+    a BatchHandle of fam, when given)."""
+    hb = handle or capi.BatchHandle(fam, device=device)
     hb.set_state()
     hb.residual()
     out = np.zeros(3 * len(fam))
     hb.lib.e2d_norms.argtypes = [C.c_void_p, capi._dp]
     rc = hb.lib.e2d_norms(hb.h, capi.ptr(out))
-    hb.close()
+    if handle is None:
+        hb.close()
     if rc:
         raise RuntimeError(f"e2d_norms: {rc}")
     return out.reshape(-1, 3)[:, 1]
@@ -209,24 +213,37 @@ def l2_cells(a, b):
     return float(math.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)))
 
 
-def warm_solve(net, fam, params, smooth_steps: int = 150, device=0):
+def warm_solve(net, fam, params, smooth_steps: int = 150, device=0, handle=None):
     """The warm-started batched solve: freestream residuals (the reference
     level), the network's prediction, smooth_steps explicit local-time-step
     RK steps that damp its high-frequency error, then Newton-Krylov to the
-    cold start's absolute residual level.  Returns (rc, hists, states)."""
-    l2 = freestream_l2(fam, device=device)
-    Ws = predict_states(net, fam)
-    hb = capi.BatchHandle(fam, device=device)
-    hb.set_state(Ws)
+    cold start's absolute residual level.  A case the warm start does not
+    bring to the tolerance is solved again from the freestream (the plain
+    method is the fallback), so every answer meets the tolerance.  Uses
+    `handle` (a BatchHandle of fam) when given.  Returns (rc, hists, states,
+    fallback case indices)."""
+    hb = handle or capi.BatchHandle(fam, device=device)
+    l2 = freestream_l2(fam, handle=hb)
+    hb.set_state(predict_states(net, fam))
+    rc, hists, states = 0, [], []
     if smooth_steps:
         rc, _ = hb.rk_steps(smooth_steps, history=False)
-        if rc:
-            hb.close()
-            return rc, [], []
-    rc, hists = hb.nks(params, l2)
-    states = hb.get_state()
-    hb.close()
-    return rc, hists, states
+    if rc == 0:
+        rc, hists = hb.nks(params, l2)
+        states = hb.get_state()
+    if handle is None:
+        hb.close()
+    if rc:
+        return rc, hists, states, []
+    tol = params.overall_tol
+    bad = [c for c, h in enumerate(hists) if not (h and h[-1]["ratio"] <= tol)]
+    if bad:
+        sub = [fam[c] for c in bad]
+        rc, h2, s2 = solve_family(sub, params, device=device)
+        for k, c in enumerate(bad):
+            hists[c] = hists[c] + h2[k]
+            states[c] = s2[k]
+    return rc, hists, states, bad
 
 
 def train_network(train_fam, params, steps=((3e-3, 1500), (1e-3, 1500), (3e-4, 1000)), seed=11, device=0):

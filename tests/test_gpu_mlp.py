@@ -60,6 +60,17 @@ def test_gradient_matches_oracle():
         k += n
 
 
+def test_training_is_deterministic():
+    import torch
+    X, T = data(20000, 4)
+    Xd, Td = torch.from_numpy(X).cuda(), torch.from_numpy(T).cuda()
+    a = warmstart.Mlp(seed=9)
+    b = warmstart.Mlp(seed=9)
+    a.train(Xd, Td, 20, 1e-3)
+    b.train(Xd, Td, 20, 1e-3)
+    assert np.array_equal(a.params(), b.params())
+
+
 def test_training_reduces_loss():
     import torch
     net = warmstart.Mlp(seed=7)
@@ -81,10 +92,11 @@ def test_warm_start_reaches_same_solution_faster():
     assert hist[-1] < 0.05 * hist[0]
     rc, cold, cold_states = warmstart.solve_family(test, p)
     assert rc == 0
-    rc, warm, warm_states = warmstart.warm_solve(net, test, p)
+    rc, warm, warm_states, fallback = warmstart.warm_solve(net, test, p)
     assert rc == 0
     for c, bs in enumerate(test):
         assert cold[c][-1]["ratio"] <= 1e-10 and warm[c][-1]["ratio"] <= 1e-10
         # the same steady state
         assert warmstart.l2_cells(bs.interior(warm_states[c][1]), bs.interior(cold_states[c][1])) < 1e-7
     assert sum(len(h) for h in warm) < sum(len(h) for h in cold)
+    assert not fallback
