@@ -522,6 +522,9 @@ struct e2d_nks_state {
   double* partial = nullptr; // [nblk * ch]
   unsigned* counter = nullptr; // [ncase] arrivals of the reduction CTAs
   int ch_vec = 1, ch_cell = 1; // CTAs per block of the vector / per-cell reductions
+  std::vector<cudaGraphExec_t> graphs;  // Arnoldi step j, captured on its second use
+  std::vector<int> graph_uses;
+  double graph_eps0 = -1.0;
   double* eps = nullptr;     // [ncase]
   double* nrm = nullptr;     // [ncase]
   double* hcol = nullptr;    // [m + 2][ncase]
@@ -540,6 +543,8 @@ namespace e2d_host {
 
 void nks_free(e2d_handle* h) {
   if (!h->nks) return;
+  for (auto g : h->nks->graphs)
+    if (g) cudaGraphExecDestroy(g);
   for (void* p : h->nks->allocs) cudaFree(p);
   if (h->nks->host) cudaFreeHost(h->nks->host);
   delete h->nks;
@@ -595,6 +600,8 @@ int nks_setup(e2d_handle* h, int m) {
   // enough CTAs per block for small block counts (about 2048 double2 / 512
   // cells per CTA), at most 16
   s->ch_vec = std::max(1, std::min(16, s->nper4 / 2 / 2048));
+  s->graphs.assign(m, nullptr);
+  s->graph_uses.assign(m, 0);
   s->ch_cell = std::max(1, std::min(16, h->B.NCi * h->B.NCj / 512));
   identity_blocks_kernel<<<VGRID, VT, 0, h->stream>>>(s->Minv, (long long)h->ncell);
   E2D_CK(cudaGetLastError());
@@ -710,6 +717,66 @@ void apply_rotation(double& dx, double& dy, double cs, double sn) {
   dx = t;
 }
 
+// One Arnoldi step j of GMRES (GMRES2D.h:1020-1250): z_j = M^-1 v_j with
+// eps = eps0 / ||z_j||, v_{j+1} = J z_j, modified Gram-Schmidt against
+// v_0..v_j into the Hessenberg column, ||v_{j+1}||, v_{j+1} /= it.  Only
+// enqueues device work (it is captured into a graph per j).
+int arnoldi_step(e2d_handle* h, int j, double eps0, const Norm4& nm) {
+  e2d_nks_state* s = h->nks;
+  const int C = s->ncase;
+  const long long n = s->n;
+  int rc;
+  double* Vj = s->V + size_t(j) * n;
+  double* Vn = s->V + size_t(j + 1) * n;
+  double* Zj = s->Z + size_t(j) * n;
+  precon_apply_kernel<<<h->B.nblk * s->ch_cell, VT, 0, h->stream>>>(
+      s->Minv, Vj, Zj, h->B.NCi * h->B.NCj, s->ch_cell, s->partial, s->counter, s->eps, eps0, act(h));
+  E2D_CK(cudaGetLastError());
+  if ((rc = matvec(h, Zj, Vn, nm))) return rc;
+  // modified Gram-Schmidt (GMRES2D.h:1224-1240)
+  for (int k = 0; k <= j; ++k) {
+    double* hk = s->hcol + size_t(k) * C;
+    if ((rc = dot(h, Vn, s->V + size_t(k) * n, hk, FIN_SUM))) return rc;
+    if ((rc = axpy(h, Vn, s->V + size_t(k) * n, hk, -1.0, 0.0))) return rc;
+  }
+  double* hn = s->hcol + size_t(j + 1) * C;
+  if ((rc = dot(h, Vn, Vn, hn, FIN_SQRT))) return rc;
+  return scale(h, Vn, hn, 1.0);
+}
+
+// Arnoldi step j through a CUDA graph: the first use of a j runs eagerly,
+// the second captures the step, later uses replay it (one launch instead of
+// about 2j + 8).  Every pointer the step reads is fixed for the life of the
+// work arrays; the per-case active mask and scalars are read from device
+// memory at run time.
+int run_arnoldi(e2d_handle* h, int j, double eps0, const Norm4& nm) {
+  e2d_nks_state* s = h->nks;
+  if (s->graph_eps0 != eps0) {
+    for (auto& g : s->graphs)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    std::fill(s->graph_uses.begin(), s->graph_uses.end(), 0);
+    s->graph_eps0 = eps0;
+  }
+  if (s->graphs[j]) {
+    E2D_CK(cudaGraphLaunch(s->graphs[j], h->stream));
+    return 0;
+  }
+  if (s->graph_uses[j]++ == 0) return arnoldi_step(h, j, eps0, nm);
+  cudaGraph_t g = nullptr;
+  E2D_CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = arnoldi_step(h, j, eps0, nm);
+  const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  if (rc || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return rc ? rc : E2D_ERR_CUDA;
+  }
+  const cudaError_t e2 = cudaGraphInstantiate(&s->graphs[j], g, 0);
+  cudaGraphDestroy(g);
+  if (e2 != cudaSuccess) { s->graphs[j] = nullptr; return E2D_ERR_CUDA; }
+  E2D_CK(cudaGraphLaunch(s->graphs[j], h->stream));
+  return 0;
+}
+
 struct GmresCase {
   double resid0 = 0, relres = 0;
   int iters = 0;
@@ -766,23 +833,7 @@ int gmres(e2d_handle* h, const e2d_nks_params& p, const std::vector<double>& tol
     for (;;) {
       ++j;
       ++iters;
-      double* Vj = s->V + size_t(j) * n;
-      double* Vn = s->V + size_t(j + 1) * n;
-      double* Zj = s->Z + size_t(j) * n;
-      const Blocks B = act(h);
-      precon_apply_kernel<<<h->B.nblk * s->ch_cell, VT, 0, h->stream>>>(
-          s->Minv, Vj, Zj, h->B.NCi * h->B.NCj, s->ch_cell, s->partial, s->counter, s->eps, p.epsilon0, B);
-      E2D_CK(cudaGetLastError());
-      if ((rc = matvec(h, Zj, Vn, nm))) return rc;
-      // modified Gram-Schmidt (GMRES2D.h:1224-1240)
-      for (int k = 0; k <= j; ++k) {
-        double* hk = s->hcol + size_t(k) * C;
-        if ((rc = dot(h, Vn, s->V + size_t(k) * n, hk, FIN_SUM))) return rc;
-        if ((rc = axpy(h, Vn, s->V + size_t(k) * n, hk, -1.0, 0.0))) return rc;
-      }
-      double* hn = s->hcol + size_t(j + 1) * C;
-      if ((rc = dot(h, Vn, Vn, hn, FIN_SQRT))) return rc;
-      if ((rc = scale(h, Vn, hn, 1.0))) return rc;
+      if ((rc = run_arnoldi(h, j, p.epsilon0, nm))) return rc;
       if ((rc = fetch(h, s->hcol, size_t(j + 2) * C, col.data()))) return rc;
       bool any = false, changed = false;
       for (int c = 0; c < C; ++c) {
