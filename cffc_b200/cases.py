@@ -41,7 +41,16 @@ LIMITER_ONE = -1
 LIMITER_ZERO = 0
 LIMITER_BARTH_JESPERSEN = 8
 LIMITER_VENKATAKRISHNAN = 9
+# i_Flux_Function codes (CFD.h:768-778)
+FLUX_GODUNOV = 1
 FLUX_ROE = 2
+FLUX_RUSANOV = 3
+FLUX_HLLE = 4
+FLUX_LINDE = 5
+FLUX_HLLC = 6
+FLUX_VANLEER = 8
+FLUX_AUSM = 9
+FLUX_AUSMPLUS = 10
 
 GAMMA_AIR = 1.40
 NG = 2

@@ -143,7 +143,7 @@ e2d_handle* e2d_create(const e2d_blocks_desc* d, const e2d_scheme* sc, int devic
   if (err) *err = 0;
   if (!d || !sc || d->nblk < 1 || d->nci < 2 || d->ncj < 2 || d->ng != NG) return fail(E2D_ERR_ARG, nullptr);
   if (sc->n_stage != 1 && sc->n_stage != 2) return fail(E2D_ERR_ARG, nullptr);
-  if (sc->flux != E2D_FLUX_ROE) return fail(E2D_ERR_ARG, nullptr);
+  if (!e2d_flux_supported(sc->flux)) return fail(E2D_ERR_ARG, nullptr);
   if (sc->precision != E2D_PREC_FP64 && sc->precision != E2D_PREC_FP64_EXACT && sc->precision != E2D_PREC_FP32)
     return fail(E2D_ERR_ARG, nullptr);
   if (sc->limiter != E2D_LIMITER_VENKATAKRISHNAN && sc->limiter != E2D_LIMITER_BARTH_JESPERSEN &&
@@ -178,7 +178,7 @@ e2d_handle* e2d_create(const e2d_blocks_desc* d, const e2d_scheme* sc, int devic
   h->ncell = size_t(B.nblk) * NCi * NCj;
   h->nnode = size_t(B.nblk) * B.NNi * B.NNj;
   B.g = sc->gamma; B.gm1 = B.g - 1.0; B.gm1i = 1.0 / B.gm1;
-  B.cfl = sc->cfl; B.limiter = sc->limiter; B.n_stage = sc->n_stage; B.local_dt = sc->local_dt;
+  B.cfl = sc->cfl; B.limiter = sc->limiter; B.flux = sc->flux; B.n_stage = sc->n_stage; B.local_dt = sc->local_dt;
   B.case_of = nullptr; B.case_start = nullptr; B.ncase = 1; B.case_active = nullptr;
   int rc = 0;
   int *neigh, *bcw, *bce, *bcs, *bcn;

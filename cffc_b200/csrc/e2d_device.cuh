@@ -49,7 +49,7 @@ struct Blocks {
   double* dt;                      // local time step per cell (local dt only)
   int* status;                     // device status word (2 ints: code, cell)
   double g, gm1, gm1i, cfl;
-  int limiter, n_stage, local_dt;
+  int limiter, flux, n_stage, local_dt;
   // Batches of independent cases: the blocks of case c are
   // case_start[c] .. case_start[c+1]-1 and case_of[b] names the case of block b
   // (null for a single case).  Per-case quantities (time-step minimum, residual
@@ -61,6 +61,10 @@ struct Blocks {
 };
 
 __host__ __device__ inline int case_id(const Blocks& B, int b) { return B.case_of ? B.case_of[b] : 0; }
+
+// The flux functions of i_Flux_Function built here: all of CFD.h:768-778 but
+// Osher (7, which the reference's Euler2D dispatch does not offer either).
+__host__ __device__ inline bool e2d_flux_supported(int f) { return f >= E2D_FLUX_GODUNOV && f <= E2D_FLUX_AUSMPLUS && f != 7; }
 
 // Arguments of the fused stage kernel.  mode: 0 = dUdt_Residual_Evaluation,
 // 1 = RK stage 1, 2 = RK stage 2.  The global time step of the current
@@ -261,6 +265,366 @@ __device__ inline CState<T> flux_roe_n(const PState<T>& wl0, const PState<T>& wr
   R.my = F.mx * s + F.my * c;
   R.E = F.E;
   return R;
+}
+
+// ---- the other flux functions of i_Flux_Function ----------------------------
+// Each *_n routine of the reference rotates both states into the frame of the
+// unit normal (c, s), evaluates the x-direction flux and rotates the momentum
+// flux back; flux_n does the same around the x-direction functions below.
+
+template <class T> __device__ __forceinline__ PState<T> rotate_in(const PState<T>& w, T c, T s) {
+  PState<T> r;
+  r.d = w.d; r.u = w.u * c + w.v * s; r.v = -w.u * s + w.v * c; r.p = w.p;
+  return r;
+}
+template <class T> __device__ __forceinline__ CState<T> rotate_out(const CState<T>& f, T c, T s) {
+  CState<T> r;
+  r.d = f.d; r.mx = f.mx * c - f.my * s; r.my = f.mx * s + f.my * c; r.E = f.E;
+  return r;
+}
+// Euler2D_pState::H (total enthalpy per volume, Euler2DState.h:1077) and Fx (:1845).
+template <class T> __device__ __forceinline__ T ht_of(const PState<T>& w, T g, T gm1i) {
+  return g * gm1i * w.p + T(HALF) * w.d * (w.u * w.u + w.v * w.v);
+}
+template <class T> __device__ __forceinline__ CState<T> fx_of(const PState<T>& w, T g, T gm1i) {
+  CState<T> F;
+  F.d = w.d * w.u; F.mx = w.d * sqr(w.u) + w.p; F.my = w.d * w.u * w.v; F.E = w.u * ht_of(w, g, gm1i);
+  return F;
+}
+// RoeAverage (Euler2DState.cc:654-683).
+template <class T> __device__ __forceinline__ PState<T> roe_average(const PState<T>& wl, const PState<T>& wr, T g,
+                                                                   T gm1) {
+  const T hl = h_of(wl, g, gm1), hr = h_of(wr, g, gm1);
+  const T sdl = sqrt(wl.d), sdr = sqrt(wr.d);
+  PState<T> wa;
+  wa.d = sdl * sdr;
+  wa.u = (sdl * wl.u + sdr * wr.u) / (sdl + sdr);
+  wa.v = (sdl * wl.v + sdr * wr.v) / (sdl + sdr);
+  const T ha = (sdl * hl + sdr * hr) / (sdl + sdr);
+  const T aa2 = gm1 * (ha - T(HALF) * (sqr(wa.u) + sqr(wa.v)));
+  wa.p = wa.d * aa2 / g;
+  return wa;
+}
+template <class T> __device__ __forceinline__ PState<T> pstate(T d, T u, T v, T p) {
+  PState<T> w;
+  w.d = d; w.u = u; w.v = v; w.p = p;
+  return w;
+}
+
+// Riemann_x (Euler2DState.cc:245-449): exact Riemann solver of Gottlieb and
+// Groth, Newton-Raphson on the intermediate velocity (at most 11 passes),
+// returning the state on the ray x/t = 0.
+template <class T>
+__device__ inline PState<T> riemann_x(const PState<T>& wl, const PState<T>& wr, T g, T gm1) {
+  const T al = a_of(wl, g), ar = a_of(wr, g);
+  const T CL = wl.u + T(2) * al / gm1;
+  const T CR = wr.u - T(2) * ar / gm1;
+  if (CL - CR <= T(0)) return pstate(T(0), T(0), T(0), T(0));
+  const T Z = (ar / al) * pow((wl.p / wr.p), T(HALF) * gm1 / g);
+  T um = (CL * Z + CR) / (T(1) + Z);
+  T pm, aml = T(0), amr = T(0);
+  if (um >= wl.u && um <= wr.u) {  // two rarefactions: exact without iteration
+    if (um >= T(0)) {
+      aml = al - T(HALF) * gm1 * (um - wl.u);
+      pm = wl.p * pow((aml / al), T(2) * g / gm1);
+      if (wl.u - al >= T(0)) return wl;
+      if (um - aml <= T(0)) return pstate(g * pm / sqr(aml), um, wl.v, pm);
+      um = (gm1 * wl.u + T(2) * al) / (g + T(1));
+      pm = wl.p * pow((um / al), T(2) * g / gm1);
+      return pstate(g * pm / sqr(um), um, wl.v, pm);
+    }
+    amr = ar + T(HALF) * gm1 * (um - wr.u);
+    pm = wr.p * pow((amr / ar), T(2) * g / gm1);
+    if (wr.u + ar <= T(0)) return wr;
+    if (um + amr >= T(0)) return pstate(g * pm / sqr(amr), um, wr.v, pm);
+    um = (gm1 * wr.u - T(2) * ar) / (g + T(1));
+    pm = wr.p * pow((-um / ar), T(2) * g / gm1);
+    return pstate(g * pm / sqr(um), um, wr.v, pm);
+  }
+  T msl = T(0), msr = T(0), pml, pmr, dpl, dpr;
+  for (int it = 1;; ++it) {
+    if (um < wl.u) {
+      msl = (g + T(1)) * (um - wl.u) / (T(4) * al);
+      msl = msl - sqrt(T(1) + sqr(msl));
+      pml = wl.p * (T(1) + g * (um - wl.u) * msl / al);
+      dpl = T(2) * g * wl.p * (msl * msl * msl) / (al * (T(1) + sqr(msl)));
+    } else {
+      aml = al - T(HALF) * gm1 * (um - wl.u);
+      pml = wl.p * pow((aml / al), T(2) * g / gm1);
+      dpl = -g * pml / aml;
+    }
+    if (um > wr.u) {
+      msr = (g + T(1)) * (um - wr.u) / (T(4) * ar);
+      msr = msr + sqrt(T(1) + sqr(msr));
+      pmr = wr.p * (T(1) + g * (um - wr.u) * msr / ar);
+      dpr = T(2) * g * wr.p * (msr * msr * msr) / (ar * (T(1) + sqr(msr)));
+    } else {
+      amr = ar + T(HALF) * gm1 * (um - wr.u);
+      pmr = wr.p * pow((amr / ar), T(2) * g / gm1);
+      dpr = g * pmr / amr;
+    }
+    if (fabs(T(1) - pml / pmr) <= T(TOLER)) break;
+    if (it > 10) break;  // the reference reports non-convergence and carries on
+    um = um - (pml - pmr) / (dpl - dpr);
+  }
+  pm = T(HALF) * (pml + pmr);
+  if (um >= T(0)) {
+    if (um < wl.u) {  // left shock
+      aml = al * sqrt(((g + T(1)) + gm1 * pm / wl.p) / ((g + T(1)) + gm1 * wl.p / pm));
+      if (wl.u + msl * al >= T(0)) return wl;
+      return pstate(g * pm / sqr(aml), um, wl.v, pm);
+    }
+    if (wl.u - al >= T(0)) return wl;
+    if (um - aml <= T(0)) return pstate(g * pm / sqr(aml), um, wl.v, pm);
+    um = (gm1 * wl.u + T(2) * al) / (g + T(1));
+    pm = wl.p * pow((um / al), T(2) * g / gm1);
+    return pstate(g * pm / sqr(um), um, wl.v, pm);
+  }
+  if (um > wr.u) {  // right shock
+    amr = ar * sqrt(((g + T(1)) + gm1 * pm / wr.p) / ((g + T(1)) + gm1 * wr.p / pm));
+    if (wr.u + msr * ar <= T(0)) return wr;
+    return pstate(g * pm / sqr(amr), um, wr.v, pm);
+  }
+  if (wr.u + ar <= T(0)) return wr;
+  if (um + amr >= T(0)) return pstate(g * pm / sqr(amr), um, wr.v, pm);
+  um = (gm1 * wr.u - T(2) * ar) / (g + T(1));
+  pm = wr.p * pow((-um / ar), T(2) * g / gm1);
+  return pstate(g * pm / sqr(um), um, wr.v, pm);
+}
+
+// FluxRusanov_x (Euler2DState.cc:2673-2713): central flux less half the
+// largest Harten-fixed |lambda| times the jump in U (HartenFixAbs, CFD.cc:655).
+template <class T>
+__device__ inline CState<T> flux_rusanov_x(const PState<T>& wl, const PState<T>& wr, T g, T gm1, T gm1i) {
+  const PState<T> wa = roe_average(wl, wr, g, gm1);
+  const CState<T> ul = U_of_W(wl, gm1i), ur = U_of_W(wr, gm1i);
+  const CState<T> fl = fx_of(wl, g, gm1i), fr = fx_of(wr, g, gm1i);
+  const T cl = a_of(wl, g), cr = a_of(wr, g), ca = a_of(wa, g);
+  const T la0 = wa.u - ca, la3 = wa.u + ca;
+  T m = fabs(la0) + harten_delta(la0, wl.u - cl, wr.u - cr);
+  m = dmax(m, fabs(wa.u));
+  m = dmax(m, fabs(wa.u));
+  m = dmax(m, fabs(la3) + harten_delta(la3, wl.u + cl, wr.u + cr));
+  const T k = T(HALF) * m;
+  CState<T> F;
+  F.d = T(HALF) * (fl.d + fr.d);
+  F.mx = T(HALF) * (fl.mx + fr.mx);
+  F.my = T(HALF) * (fl.my + fr.my);
+  F.E = T(HALF) * (fl.E + fr.E);
+  F.d -= k * (ur.d - ul.d);
+  F.mx -= k * (ur.mx - ul.mx);
+  F.my -= k * (ur.my - ul.my);
+  F.E -= k * (ur.E - ul.E);
+  return F;
+}
+
+// FluxHLLE_x (Euler2DState.cc:2921-2963) and FluxLinde_x (:3321-3383): HLL
+// flux with the Einfeldt wave-speed bounds; Linde's variant restores part of
+// the contact through the coefficient alpha.
+template <class T, bool LINDE>
+__device__ inline CState<T> flux_hll_x(const PState<T>& wl, const PState<T>& wr, T g, T gm1, T gm1i) {
+  const PState<T> wa = roe_average(wl, wr, g, gm1);
+  const T ca = a_of(wa, g);
+  const T sl = dmin(wl.u - a_of(wl, g), wa.u - ca);
+  const T sr = dmax(wr.u + a_of(wr, g), wa.u + ca);
+  if (sl >= T(0)) return fx_of(wl, g, gm1i);
+  if (sr <= T(0)) return fx_of(wr, g, gm1i);
+  const CState<T> ul = U_of_W(wl, gm1i), ur = U_of_W(wr, gm1i);
+  const CState<T> fl = fx_of(wl, g, gm1i), fr = fx_of(wr, g, gm1i);
+  CState<T> dU;
+  dU.d = ur.d - ul.d; dU.mx = ur.mx - ul.mx; dU.my = ur.my - ul.my; dU.E = ur.E - ul.E;
+  T k = sl * sr;
+  if (LINDE) {
+    const T sm = wa.u, da = wa.d;
+    T du = fabs(dU.d) / da + fabs(dU.mx) / (da * ca) + fabs(dU.my) / (da * ca) + fabs(dU.E) / (da * ca * ca);
+    T alpha;
+    if (du <= T(TOLER)) {
+      alpha = T(0);
+    } else {
+      du = T(1) / du;
+      const T w0 = (fr.d - fl.d) - sm * dU.d, w1 = (fr.mx - fl.mx) - sm * dU.mx;
+      const T w2 = (fr.my - fl.my) - sm * dU.my, w3 = (fr.E - fl.E) - sm * dU.E;
+      alpha = T(1) - (fabs(w0) / (da * ca) + fabs(w1) / (da * ca * ca) + fabs(w2) / (da * ca * ca) +
+                      fabs(w3) / (da * ca * ca * ca)) * du;
+      alpha = dmax(T(0), alpha);
+    }
+    k = k * (T(1) - (T(1) - dmax(sm / sr, sm / sl)) * alpha);
+  }
+  const T den = sr - sl;
+  CState<T> F;
+  F.d = ((sr * fl.d - sl * fr.d) + k * dU.d) / den;
+  F.mx = ((sr * fl.mx - sl * fr.mx) + k * dU.mx) / den;
+  F.my = ((sr * fl.my - sl * fr.my) + k * dU.my) / den;
+  F.E = ((sr * fl.E - sl * fr.E) + k * dU.E) / den;
+  return F;
+}
+
+// FluxHLLC_x (Euler2DState.cc:3630-3694): Toro's HLLC with wave speeds from
+// the two-rarefaction pressure estimate.
+template <class T>
+__device__ inline CState<T> flux_hllc_x(const PState<T>& wl, const PState<T>& wr, T g, T gm1, T gm1i) {
+  const T al = a_of(wl, g), ar = a_of(wr, g);
+  const T CL = wl.u + T(2) * al / gm1;
+  const T CR = wr.u - T(2) * ar / gm1;
+  const T Z = (ar / al) * pow((wl.p / wr.p), T(HALF) * gm1 / g);
+  const T um = (CL * Z + CR) / (T(1) + Z);
+  const T aml = al - T(HALF) * gm1 * (um - wl.u);
+  T pm = wl.p * pow((aml / al), T(2) * g / gm1);
+  const T amr = ar + T(HALF) * gm1 * (um - wr.u);
+  pm = T(HALF) * (pm + wr.p * pow((amr / ar), T(2) * g / gm1));
+  const T ql = (pm / wl.p <= T(1)) ? T(1) : sqrt(T(1) + T(HALF) * ((g + T(1)) / g) * (pm / wl.p));
+  const T sl = wl.u - ql * al;
+  const T qr = (pm / wr.p <= T(1)) ? T(1) : sqrt(T(1) + T(HALF) * ((g + T(1)) / g) * (pm / wr.p));
+  const T sr = wr.u + qr * ar;
+  if (sl >= T(0)) return fx_of(wl, g, gm1i);
+  if (sr <= T(0)) return fx_of(wr, g, gm1i);
+  const bool left = um >= T(0);
+  const PState<T>& w = left ? wl : wr;
+  const T sk = left ? sl : sr;
+  const CState<T> uk = U_of_W(w, gm1i), fk = fx_of(w, g, gm1i);
+  const T f = (sk - w.u) / (sk - um);
+  CState<T> us;  // intermediate state on the upwind side of the contact
+  us.d = w.d * f;
+  us.mx = (w.d * um) * f;
+  us.my = (w.d * w.v) * f;
+  us.E = (uk.E + w.d * (um - w.u) * (um + w.p / (w.d * (sk - w.u)))) * f;
+  CState<T> F;
+  F.d = fk.d + sk * (us.d - uk.d);
+  F.mx = fk.mx + sk * (us.mx - uk.mx);
+  F.my = fk.my + sk * (us.my - uk.my);
+  F.E = fk.E + sk * (us.E - uk.E);
+  return F;
+}
+
+// FluxVanLeer (Euler2DState.cc:3862-3903): flux-vector splitting.
+template <class T>
+__device__ inline CState<T> flux_vanleer_x(const PState<T>& wl, const PState<T>& wr, T g, T gm1, T gm1i) {
+  CState<T> fl, fr;
+  // Euler2D_cState's default value, reached only by a NaN Mach number
+  fl.d = fr.d = T(1.225); fl.mx = fr.mx = fl.my = fr.my = T(0); fl.E = fr.E = T(101325.0 / (1.4 - 1.0));
+  T M = wl.u / a_of(wl, g);
+  if (M < T(-1)) {
+    fl.d = fl.mx = fl.my = fl.E = T(0);
+  } else if (fabs(M) <= T(1)) {
+    const T a = a_of(wl, g);
+    const T Mp = T(0.25) * wl.d * a * sqr(T(1) + M);
+    fl.d = Mp;
+    fl.mx = Mp * ((T(2) * a / g) * (T(HALF) * gm1 * M + T(1)));
+    fl.my = Mp * wl.v;
+    fl.E = Mp * ((T(2) * (g * wl.p / wl.d) / (g * g - T(1))) * sqr(T(HALF) * gm1 * M + T(1)) + T(HALF) * sqr(wl.v));
+  } else if (M > T(1)) {
+    fl = fx_of(wl, g, gm1i);
+  }
+  M = wr.u / a_of(wr, g);
+  if (-M < T(-1)) {
+    fr.d = fr.mx = fr.my = fr.E = T(0);
+  } else if (fabs(M) <= T(1)) {
+    const T a = a_of(wr, g);
+    const T Mn = T(-0.25) * wr.d * a * sqr(T(1) - M);
+    fr.d = Mn;
+    fr.mx = Mn * ((T(2) * a / g) * (T(HALF) * gm1 * M - T(1)));
+    fr.my = Mn * wr.v;
+    fr.E = Mn * ((T(2) * (g * wr.p / wr.d) / (g * g - T(1))) * sqr(T(HALF) * gm1 * M - T(1)) + T(HALF) * sqr(wr.v));
+  } else if (-M > T(1)) {
+    fr = fx_of(wr, g, gm1i);
+  }
+  CState<T> F;
+  F.d = fl.d + fr.d; F.mx = fl.mx + fr.mx; F.my = fl.my + fr.my; F.E = fl.E + fr.E;
+  return F;
+}
+
+// FluxAUSM (Euler2DState.cc:4056-4106, Liou and Steffen) and FluxAUSMplus
+// (:4170-4231, Liou 1994): split Mach numbers and pressures.
+template <class T>
+__device__ inline CState<T> flux_ausm_x(const PState<T>& wl, const PState<T>& wr, T g, T gm1i) {
+  const T al = a_of(wl, g), Ml = wl.u / al;
+  const T ar = a_of(wr, g), Mr = wr.u / ar;
+  T Mplus, pplus, Mminus, pminus;
+  if (fabs(Ml) <= T(1)) {
+    Mplus = T(0.25) * sqr(Ml + T(1));
+    pplus = T(0.25) * wl.p * sqr(Ml + T(1)) * (T(2) - Ml);
+  } else {
+    Mplus = T(0.5) * (Ml + fabs(Ml));
+    pplus = T(0.5) * wl.p * (Ml + fabs(Ml)) / Ml;
+  }
+  if (fabs(Mr) <= T(1)) {
+    Mminus = T(-0.25) * sqr(Mr - T(1));
+    pminus = T(0.25) * wr.p * sqr(Mr - T(1)) * (T(2) + Mr);
+  } else {
+    Mminus = T(0.5) * (Mr - fabs(Mr));
+    pminus = T(0.5) * wr.p * (Mr - fabs(Mr)) / Mr;
+  }
+  const T Mh = Mplus + Mminus, ph = pplus + pminus;
+  const T Hl = ht_of(wl, g, gm1i), Hr = ht_of(wr, g, gm1i);
+  const T k = T(0.5) * Mh, q = T(0.5) * fabs(Mh);
+  CState<T> F;
+  F.d = k * (wl.d * al + wr.d * ar);
+  F.mx = k * (wl.d * al * wl.u + wr.d * ar * wr.u);
+  F.my = k * (wl.d * al * wl.v + wr.d * ar * wr.v);
+  F.E = k * (al * Hl + ar * Hr);
+  F.d -= q * (wr.d * ar - wl.d * al);
+  F.mx -= q * (wr.d * ar * wr.u - wl.d * al * wl.u);
+  F.my -= q * (wr.d * ar * wr.v - wl.d * al * wl.v);
+  F.E -= q * (ar * Hr - al * Hl);
+  F.mx += ph;
+  return F;
+}
+template <class T>
+__device__ inline CState<T> flux_ausmplus_x(const PState<T>& wl, const PState<T>& wr, T g, T gm1i) {
+  const T beta = T(0.125), alpha = T(0.1875);
+  const T ah = T(HALF) * (a_of(wl, g) + a_of(wr, g));
+  const T Ml = wl.u / ah, Mr = wr.u / ah;
+  T Mplus, pplus, Mminus, pminus;
+  if (fabs(Ml) < T(1)) {
+    Mplus = T(0.25) * sqr(Ml + T(1)) + beta * sqr(Ml * Ml - T(1));
+    pplus = (T(0.25) * sqr(Ml + T(1)) * (T(2) - Ml) + alpha * Ml * sqr(Ml * Ml - T(1))) * wl.p;
+  } else {
+    Mplus = T(0.5) * (Ml + fabs(Ml));
+    pplus = T(0.5) * wl.p * (T(1) + ((Ml < T(0)) ? T(-1) : T(1)));
+  }
+  if (fabs(Mr) < T(1)) {
+    Mminus = T(-0.25) * sqr(Mr - T(1)) - beta * sqr(Mr * Mr - T(1));
+    pminus = (T(0.25) * sqr(Mr - T(1)) * (T(2) + Mr) - alpha * Mr * sqr(Mr * Mr - T(1))) * wr.p;
+  } else {
+    Mminus = T(0.5) * (Mr - fabs(Mr));
+    pminus = T(0.5) * wr.p * (T(1) - ((Mr < T(0)) ? T(-1) : T(1)));
+  }
+  const T Mh = Mplus + Mminus, ph = pplus + pminus;
+  const T Hl = ht_of(wl, g, gm1i), Hr = ht_of(wr, g, gm1i);
+  const T k = T(0.5) * Mh, q = T(0.5) * fabs(Mh);
+  CState<T> F;
+  F.d = k * (wl.d + wr.d);
+  F.mx = k * (wl.d * wl.u + wr.d * wr.u);
+  F.my = k * (wl.d * wl.v + wr.d * wr.v);
+  F.E = k * (Hl + Hr);
+  F.d -= q * (wr.d - wl.d);
+  F.mx -= q * (wr.d * wr.u - wl.d * wl.u);
+  F.my -= q * (wr.d * wr.v - wl.d * wl.v);
+  F.E -= q * (Hr - Hl);
+  F.d *= ah; F.mx *= ah; F.my *= ah; F.E *= ah;
+  F.mx += ph;
+  return F;
+}
+
+// Face flux of i_Flux_Function `kind` other than Roe (dispatch of
+// dUdt_Residual_Evaluation, Euler2DQuad.cc:968-1003).  Kept out of line so
+// that the Roe path's register allocation does not carry these.
+template <class T>
+__device__ inline CState<T> flux_n(int kind, PState<T> wl, PState<T> wr, T c, T s, T g, T gm1, T gm1i) {
+  wl = rotate_in(wl, c, s);
+  wr = rotate_in(wr, c, s);
+  CState<T> F;
+  switch (kind) {
+    case E2D_FLUX_GODUNOV: F = fx_of(riemann_x(wl, wr, g, gm1), g, gm1i); break;
+    case E2D_FLUX_RUSANOV: F = flux_rusanov_x(wl, wr, g, gm1, gm1i); break;
+    case E2D_FLUX_HLLE: F = flux_hll_x<T, false>(wl, wr, g, gm1, gm1i); break;
+    case E2D_FLUX_LINDE: F = flux_hll_x<T, true>(wl, wr, g, gm1, gm1i); break;
+    case E2D_FLUX_HLLC: F = flux_hllc_x(wl, wr, g, gm1, gm1i); break;
+    case E2D_FLUX_VANLEER: F = flux_vanleer_x(wl, wr, g, gm1, gm1i); break;
+    case E2D_FLUX_AUSM: F = flux_ausm_x(wl, wr, g, gm1i); break;
+    default: F = flux_ausmplus_x(wl, wr, g, gm1i); break;
+  }
+  return rotate_out(F, c, s);
 }
 
 // Limiter_BarthJespersen / Limiter_Venkatakrishnan over the 4 face points.

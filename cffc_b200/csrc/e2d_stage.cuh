@@ -251,8 +251,12 @@ __device__ __forceinline__ PState<RT> load_wo(const double* wo, int b, int len, 
 
 // Flux and limiter of the reconstruction type: the division-lean FP64 forms
 // on the fast path, the reference's forms otherwise (FP32 included).
-__device__ __forceinline__ CState<RT> face_flux(const PState<RT>& wl, const PState<RT>& wr, RT nx, RT ny, RT g,
-                                                RT gm1, RT gm1i) {
+// ROE: the kernel instance of the Roe flux; the other instance dispatches
+// over the remaining flux functions, so neither carries the other's registers.
+template <bool ROE>
+__device__ __forceinline__ CState<RT> face_flux(int kind, const PState<RT>& wl, const PState<RT>& wr, RT nx, RT ny,
+                                                RT g, RT gm1, RT gm1i) {
+  if (!ROE) return flux_n(kind, wl, wr, nx, ny, g, gm1, gm1i);
 #if defined(E2D_FAST) && !defined(E2D_FP32)
   return fm::flux_roe_n(wl, wr, nx, ny, g, gm1, gm1i);
 #else
@@ -267,7 +271,7 @@ __device__ __forceinline__ RT cell_limiter(int kind, const RT* uq, RT u0, RT umi
 #endif
 }
 
-template <int MODE, bool FUSE>
+template <int MODE, bool FUSE, bool ROE>
 __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& s = *reinterpret_cast<Smem*>(smem_raw);
@@ -454,7 +458,7 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
         wr = face_state(s, hi, hl + 1, mx, my);
       }
     }
-    const CState<RT> F = face_flux(wl, wr, RT(nx), RT(ny), RT(g), RT(gm1), RT(gm1i));
+    const CState<RT> F = face_flux<ROE>(B.flux, wl, wr, RT(nx), RT(ny), RT(g), RT(gm1), RT(gm1i));
     if (is_i) {
       s.Fi[0][fj][fi] = F.d; s.Fi[1][fj][fi] = F.mx; s.Fi[2][fj][fi] = F.my; s.Fi[3][fj][fi] = F.E;
       s.li[fj][fi] = l;
@@ -609,29 +613,33 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
 namespace e2d {
 namespace E2D_NS {
 size_t stage_smem_bytes() { return sizeof(Smem); }
-template <int MODE, bool FUSE>
+template <int MODE, bool FUSE, bool ROE>
 cudaError_t launch_one(const StageArgs& a, cudaStream_t st) {
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel<MODE, FUSE>,
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<MODE, FUSE, ROE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(Smem)));
     if (e != cudaSuccess) return e;
     configured = true;
   }
   const int grid = a.B.nblk * a.tiles_i * a.tiles_j;
-  stage_kernel<MODE, FUSE><<<grid, NTHREADS, sizeof(Smem), st>>>(a);
+  stage_kernel<MODE, FUSE, ROE><<<grid, NTHREADS, sizeof(Smem), st>>>(a);
   return cudaGetLastError();
 }
-cudaError_t launch_stage(const StageArgs& a, cudaStream_t st) {
+template <bool ROE>
+cudaError_t launch_flux(const StageArgs& a, cudaStream_t st) {
   switch (a.mode * 2 + (a.fuse_next ? 1 : 0)) {
-    case 0: return launch_one<0, false>(a, st);
-    case 2: return launch_one<1, false>(a, st);
-    case 3: return launch_one<1, true>(a, st);
-    case 4: return launch_one<2, false>(a, st);
-    case 5: return launch_one<2, true>(a, st);
-    case 6: return launch_one<3, false>(a, st);
+    case 0: return launch_one<0, false, ROE>(a, st);
+    case 2: return launch_one<1, false, ROE>(a, st);
+    case 3: return launch_one<1, true, ROE>(a, st);
+    case 4: return launch_one<2, false, ROE>(a, st);
+    case 5: return launch_one<2, true, ROE>(a, st);
+    case 6: return launch_one<3, false, ROE>(a, st);
     default: return cudaErrorInvalidValue;
   }
+}
+cudaError_t launch_stage(const StageArgs& a, cudaStream_t st) {
+  return a.B.flux == E2D_FLUX_ROE ? launch_flux<true>(a, st) : launch_flux<false>(a, st);
 }
 int tile_i() { return TI; }
 int tile_j() { return TJ; }

@@ -12,6 +12,7 @@
 #include <istream>
 #include <sstream>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace cffc_b200 {
@@ -165,8 +166,19 @@ int Parse_Next_Input_Control_Parameter(Euler2D_Input_Parameters& IP, std::istrea
     return 0;
   }
   if (code == "Flux_Function_Type") {
+    // the names of Euler2DInput.cc:1850-1876; the preconditioned and moving-frame
+    // variants are outside this path
     if (str(IP.Flux_Function_Type)) return INVALID_INPUT_CODE;
-    return IP.Flux_Function_Type == "Roe" ? 0 : INVALID_INPUT_CODE;
+    static const std::pair<const char*, int> names[] = {
+        {"Godunov", E2D_FLUX_GODUNOV}, {"Roe", E2D_FLUX_ROE},         {"Rusanov", E2D_FLUX_RUSANOV},
+        {"HLLE", E2D_FLUX_HLLE},       {"Linde", E2D_FLUX_LINDE},     {"HLLC", E2D_FLUX_HLLC},
+        {"VanLeer", E2D_FLUX_VANLEER}, {"AUSM", E2D_FLUX_AUSM},       {"AUSM+", E2D_FLUX_AUSMPLUS}};
+    for (const auto& n : names)
+      if (IP.Flux_Function_Type == n.first) {
+        IP.i_Flux_Function = n.second;
+        return 0;
+      }
+    return INVALID_INPUT_CODE;
   }
   if (code == "ICs_Type") {
     if (str(IP.ICs_Type)) return INVALID_INPUT_CODE;
@@ -390,7 +402,7 @@ void pack_blocks(const std::vector<Euler2D_Quad_Block>& blocks, const std::vecto
 e2d_scheme scheme_of(const Euler2D_Input_Parameters& IP) {
   e2d_scheme s{};
   s.limiter = IP.i_Limiter;
-  s.flux = E2D_FLUX_ROE;
+  s.flux = IP.i_Flux_Function;
   s.n_stage = IP.N_Stage;
   s.local_dt = IP.Local_Time_Stepping ? 1 : 0;
   s.precision = IP.Precision;

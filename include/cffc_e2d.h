@@ -49,9 +49,16 @@ extern "C" {
 #define E2D_LIMITER_BARTH_JESPERSEN 8
 #define E2D_LIMITER_VENKATAKRISHNAN 9
 
-/* Flux function codes (src_2D/CFD/CFD.h:769). */
-#define E2D_FLUX_ROE 2
+/* Flux function codes (src_2D/CFD/CFD.h:768-778). */
+#define E2D_FLUX_GODUNOV 1  /* exact Riemann solver            */
+#define E2D_FLUX_ROE 2      /* Roe with Harten's entropy fix   */
+#define E2D_FLUX_RUSANOV 3
 #define E2D_FLUX_HLLE 4
+#define E2D_FLUX_LINDE 5    /* HLLL                            */
+#define E2D_FLUX_HLLC 6
+#define E2D_FLUX_VANLEER 8
+#define E2D_FLUX_AUSM 9
+#define E2D_FLUX_AUSMPLUS 10
 
 /* Precision of reconstruction and flux evaluation. */
 #define E2D_PREC_FP64 0       /* FP64, FMA contraction allowed                   */
@@ -89,7 +96,7 @@ typedef struct e2d_blocks_desc {
  * (src_2D/Euler2D/Euler2DInput.h:41-120). */
 typedef struct e2d_scheme {
   int32_t limiter;   /* i_Limiter                                         */
-  int32_t flux;      /* i_Flux_Function (Roe)                             */
+  int32_t flux;      /* i_Flux_Function: E2D_FLUX_* (all but Osher)       */
   int32_t n_stage;   /* N_Stage of TIME_STEPPING_EXPLICIT_RUNGE_KUTTA: 1, 2 */
   int32_t local_dt;  /* Local_Time_Stepping: 0 global, 1 scalar local     */
   int32_t precision; /* E2D_PREC_*                                        */

@@ -107,6 +107,7 @@ struct Euler2D_Input_Parameters {
   std::string Limiter_Type = "Venkatakrishnan";
   int i_Limiter = E2D_LIMITER_VENKATAKRISHNAN;
   std::string Flux_Function_Type = "Roe";
+  int i_Flux_Function = E2D_FLUX_ROE;
   std::string ICs_Type = "Uniform";
   std::string Grid_Type = "Rectangular_Box";
   double Box_Width = 1.0, Box_Height = 1.0;

@@ -273,6 +273,317 @@ static cst flux_roe_n(const e2d_oracle *o, pst wl, pst wr, vec2 n) {
   return F;
 }
 
+/* ---- the other flux functions of i_Flux_Function (Euler2DQuad.cc:968-1003) ----
+ * All evaluate an x-direction flux between states rotated into the frame of
+ * the face normal and rotate the momentum flux back (FluxXxx_n). */
+
+static cst Fx_of(const e2d_oracle *o, pst w) { /* Euler2D_pState::Fx, Euler2DState.h:1845 */
+  cst F;
+  F.d = w.d * w.u; F.mx = w.d * sqr(w.u) + w.p; F.my = w.d * w.u * w.v; F.E = w.u * Ht_of(o, w);
+  return F;
+}
+static pst mkp(double d, double u, double v, double p) { pst w; w.d = d; w.u = u; w.v = v; w.p = p; return w; }
+static cst cdiff(cst a, cst b) { cst r; r.d = a.d - b.d; r.mx = a.mx - b.mx; r.my = a.my - b.my; r.E = a.E - b.E; return r; }
+
+/* RoeAverage (src_2D/Euler2D/Euler2DState.cc:654-683). */
+static pst roe_average(const e2d_oracle *o, pst wl, pst wr) {
+  double hl = h_of(o, wl), hr = h_of(o, wr), sdl = sqrt(wl.d), sdr = sqrt(wr.d), ha, aa2;
+  pst wa;
+  wa.d = sdl * sdr;
+  wa.u = (sdl * wl.u + sdr * wr.u) / (sdl + sdr);
+  wa.v = (sdl * wl.v + sdr * wr.v) / (sdl + sdr);
+  ha = (sdl * hl + sdr * hr) / (sdl + sdr);
+  aa2 = o->gm1 * (ha - HALF * (sqr(wa.u) + sqr(wa.v)));
+  wa.p = wa.d * aa2 / o->g;
+  return wa;
+}
+
+/* Riemann_x (Euler2DState.cc:245-449): exact solver, Newton-Raphson on the
+ * intermediate velocity, state on x/t = 0. */
+static pst riemann_x(const e2d_oracle *o, pst wl, pst wr) {
+  const double g = o->g, gm1 = o->gm1;
+  double al = a_of(o, wl), ar = a_of(o, wr), CL, CR, Z, um, pm, aml = 0.0, amr = 0.0;
+  double msl = 0.0, msr = 0.0, pml = 0.0, pmr = 0.0, dpl, dpr;
+  int it;
+  CL = wl.u + 2.0 * al / gm1;
+  CR = wr.u - 2.0 * ar / gm1;
+  if (CL - CR <= 0.0) return mkp(0.0, 0.0, 0.0, 0.0);
+  Z = (ar / al) * pow((wl.p / wr.p), HALF * gm1 / g);
+  um = (CL * Z + CR) / (1.0 + Z);
+  if (um >= wl.u && um <= wr.u) {
+    if (um >= 0.0) {
+      aml = al - HALF * gm1 * (um - wl.u);
+      pm = wl.p * pow((aml / al), 2.0 * g / gm1);
+      if (wl.u - al >= 0.0) return wl;
+      if (um - aml <= 0.0) return mkp(g * pm / sqr(aml), um, wl.v, pm);
+      um = (gm1 * wl.u + 2.0 * al) / (g + 1.0);
+      pm = wl.p * pow((um / al), 2.0 * g / gm1);
+      return mkp(g * pm / sqr(um), um, wl.v, pm);
+    }
+    amr = ar + HALF * gm1 * (um - wr.u);
+    pm = wr.p * pow((amr / ar), 2.0 * g / gm1);
+    if (wr.u + ar <= 0.0) return wr;
+    if (um + amr >= 0.0) return mkp(g * pm / sqr(amr), um, wr.v, pm);
+    um = (gm1 * wr.u - 2.0 * ar) / (g + 1.0);
+    pm = wr.p * pow((-um / ar), 2.0 * g / gm1);
+    return mkp(g * pm / sqr(um), um, wr.v, pm);
+  }
+  for (it = 1;; ++it) {
+    if (um < wl.u) {
+      msl = (g + 1.0) * (um - wl.u) / (4.0 * al);
+      msl = msl - sqrt(1.0 + sqr(msl));
+      pml = wl.p * (1.0 + g * (um - wl.u) * msl / al);
+      dpl = 2.0 * g * wl.p * (msl * msl * msl) / (al * (1.0 + sqr(msl)));
+    } else {
+      aml = al - HALF * gm1 * (um - wl.u);
+      pml = wl.p * pow((aml / al), 2.0 * g / gm1);
+      dpl = -g * pml / aml;
+    }
+    if (um > wr.u) {
+      msr = (g + 1.0) * (um - wr.u) / (4.0 * ar);
+      msr = msr + sqrt(1.0 + sqr(msr));
+      pmr = wr.p * (1.0 + g * (um - wr.u) * msr / ar);
+      dpr = 2.0 * g * wr.p * (msr * msr * msr) / (ar * (1.0 + sqr(msr)));
+    } else {
+      amr = ar + HALF * gm1 * (um - wr.u);
+      pmr = wr.p * pow((amr / ar), 2.0 * g / gm1);
+      dpr = g * pmr / amr;
+    }
+    if (fabs(1.0 - pml / pmr) <= TOLER) break;
+    if (it > 10) break;
+    um = um - (pml - pmr) / (dpl - dpr);
+  }
+  pm = HALF * (pml + pmr);
+  if (um >= 0.0) {
+    if (um < wl.u) {
+      aml = al * sqrt(((g + 1.0) + gm1 * pm / wl.p) / ((g + 1.0) + gm1 * wl.p / pm));
+      if (wl.u + msl * al >= 0.0) return wl;
+      return mkp(g * pm / sqr(aml), um, wl.v, pm);
+    }
+    if (wl.u - al >= 0.0) return wl;
+    if (um - aml <= 0.0) return mkp(g * pm / sqr(aml), um, wl.v, pm);
+    um = (gm1 * wl.u + 2.0 * al) / (g + 1.0);
+    pm = wl.p * pow((um / al), 2.0 * g / gm1);
+    return mkp(g * pm / sqr(um), um, wl.v, pm);
+  }
+  if (um > wr.u) {
+    amr = ar * sqrt(((g + 1.0) + gm1 * pm / wr.p) / ((g + 1.0) + gm1 * wr.p / pm));
+    if (wr.u + msr * ar <= 0.0) return wr;
+    return mkp(g * pm / sqr(amr), um, wr.v, pm);
+  }
+  if (wr.u + ar <= 0.0) return wr;
+  if (um + amr >= 0.0) return mkp(g * pm / sqr(amr), um, wr.v, pm);
+  um = (gm1 * wr.u - 2.0 * ar) / (g + 1.0);
+  pm = wr.p * pow((-um / ar), 2.0 * g / gm1);
+  return mkp(g * pm / sqr(um), um, wr.v, pm);
+}
+
+/* FluxRusanov_x (Euler2DState.cc:2673-2713) with HartenFixAbs (CFD.cc:655-669). */
+static cst flux_rusanov_x(const e2d_oracle *o, pst wl, pst wr) {
+  pst wa = roe_average(o, wl, wr);
+  cst fl = Fx_of(o, wl), fr = Fx_of(o, wr), dU = cdiff(U_of_W(o, wr), U_of_W(o, wl)), F;
+  double cl = a_of(o, wl), cr = a_of(o, wr), ca = a_of(o, wa), ws[4], m;
+  int k;
+  ws[0] = fabs(wa.u - ca) + harten_delta(wa.u - ca, wl.u - cl, wr.u - cr);
+  ws[1] = fabs(wa.u);
+  ws[2] = fabs(wa.u);
+  ws[3] = fabs(wa.u + ca) + harten_delta(wa.u + ca, wl.u + cl, wr.u + cr);
+  m = ws[0];
+  for (k = 1; k < 4; ++k) m = dmax(m, ws[k]);
+  F.d = HALF * (fl.d + fr.d); F.mx = HALF * (fl.mx + fr.mx);
+  F.my = HALF * (fl.my + fr.my); F.E = HALF * (fl.E + fr.E);
+  F.d -= HALF * m * dU.d; F.mx -= HALF * m * dU.mx; F.my -= HALF * m * dU.my; F.E -= HALF * m * dU.E;
+  return F;
+}
+
+/* FluxHLLE_x (Euler2DState.cc:2921-2963); linde != 0: FluxLinde_x (:3321-3383). */
+static cst flux_hll_x(const e2d_oracle *o, pst wl, pst wr, int linde) {
+  pst wa = roe_average(o, wl, wr);
+  double ca = a_of(o, wa), sl, sr, k, alpha, du, sm, da;
+  cst fl, fr, dU, dF, F;
+  sl = dmin(wl.u - a_of(o, wl), wa.u - ca);
+  sr = dmax(wr.u + a_of(o, wr), wa.u + ca);
+  if (sl >= 0.0) return Fx_of(o, wl);
+  if (sr <= 0.0) return Fx_of(o, wr);
+  fl = Fx_of(o, wl); fr = Fx_of(o, wr);
+  dU = cdiff(U_of_W(o, wr), U_of_W(o, wl));
+  k = sl * sr;
+  if (linde) {
+    sm = wa.u; da = wa.d;
+    du = fabs(dU.d) / da + fabs(dU.mx) / (da * ca) + fabs(dU.my) / (da * ca) + fabs(dU.E) / (da * ca * ca);
+    if (du <= TOLER) {
+      alpha = 0.0;
+    } else {
+      du = 1.0 / du;
+      dF = cdiff(fr, fl);
+      dF.d = dF.d - sm * dU.d; dF.mx = dF.mx - sm * dU.mx; dF.my = dF.my - sm * dU.my; dF.E = dF.E - sm * dU.E;
+      alpha = 1.0 - (fabs(dF.d) / (da * ca) + fabs(dF.mx) / (da * ca * ca) + fabs(dF.my) / (da * ca * ca) +
+                     fabs(dF.E) / (da * ca * ca * ca)) * du;
+      alpha = dmax(0.0, alpha);
+    }
+    k = k * (1.0 - (1.0 - dmax(sm / sr, sm / sl)) * alpha);
+  }
+  F.d = ((sr * fl.d - sl * fr.d) + k * dU.d) / (sr - sl);
+  F.mx = ((sr * fl.mx - sl * fr.mx) + k * dU.mx) / (sr - sl);
+  F.my = ((sr * fl.my - sl * fr.my) + k * dU.my) / (sr - sl);
+  F.E = ((sr * fl.E - sl * fr.E) + k * dU.E) / (sr - sl);
+  return F;
+}
+
+/* FluxHLLC_x (Euler2DState.cc:3630-3694). */
+static cst flux_hllc_x(const e2d_oracle *o, pst wl, pst wr) {
+  const double g = o->g, gm1 = o->gm1;
+  double al = a_of(o, wl), ar = a_of(o, wr), CL, CR, Z, um, aml, amr, pm, ql, qr, sl, sr, sk, f;
+  pst w;
+  cst uk, fk, us, F;
+  CL = wl.u + 2.0 * al / gm1;
+  CR = wr.u - 2.0 * ar / gm1;
+  Z = (ar / al) * pow((wl.p / wr.p), HALF * gm1 / g);
+  um = (CL * Z + CR) / (1.0 + Z);
+  aml = al - HALF * gm1 * (um - wl.u);
+  pm = wl.p * pow((aml / al), 2.0 * g / gm1);
+  amr = ar + HALF * gm1 * (um - wr.u);
+  pm = HALF * (pm + wr.p * pow((amr / ar), 2.0 * g / gm1));
+  ql = (pm / wl.p <= 1.0) ? 1.0 : sqrt(1.0 + HALF * ((g + 1.0) / g) * (pm / wl.p));
+  sl = wl.u - ql * al;
+  qr = (pm / wr.p <= 1.0) ? 1.0 : sqrt(1.0 + HALF * ((g + 1.0) / g) * (pm / wr.p));
+  sr = wr.u + qr * ar;
+  if (sl >= 0.0) return Fx_of(o, wl);
+  if (sr <= 0.0) return Fx_of(o, wr);
+  if (um >= 0.0) { w = wl; sk = sl; } else { w = wr; sk = sr; }
+  uk = U_of_W(o, w); fk = Fx_of(o, w);
+  f = (sk - w.u) / (sk - um);
+  us.d = w.d * f;
+  us.mx = (w.d * um) * f;
+  us.my = (w.d * w.v) * f;
+  us.E = (uk.E + w.d * (um - w.u) * (um + w.p / (w.d * (sk - w.u)))) * f;
+  F.d = fk.d + sk * (us.d - uk.d);
+  F.mx = fk.mx + sk * (us.mx - uk.mx);
+  F.my = fk.my + sk * (us.my - uk.my);
+  F.E = fk.E + sk * (us.E - uk.E);
+  return F;
+}
+
+/* FluxVanLeer (Euler2DState.cc:3862-3903). */
+static cst flux_vanleer_x(const e2d_oracle *o, pst wl, pst wr) {
+  const double g = o->g, gm1 = o->gm1;
+  cst fl, fr, F;
+  double M, a, m;
+  /* Euler2D_cState() defaults: only a NaN Mach number leaves them */
+  fl.d = fr.d = 1.225; fl.mx = fr.mx = fl.my = fr.my = 0.0; fl.E = fr.E = 101325.0 / (1.4 - 1.0);
+  M = wl.u / a_of(o, wl);
+  if (M < -1.0) {
+    fl.d = fl.mx = fl.my = fl.E = 0.0;
+  } else if (fabs(M) <= 1.0) {
+    a = a_of(o, wl);
+    m = 0.25 * wl.d * a * sqr(1.0 + M);
+    fl.d = m;
+    fl.mx = m * ((2.0 * a / g) * (HALF * gm1 * M + 1.0));
+    fl.my = m * wl.v;
+    fl.E = m * ((2.0 * (g * wl.p / wl.d) / (g * g - 1.0)) * sqr(HALF * gm1 * M + 1.0) + HALF * sqr(wl.v));
+  } else if (M > 1.0) {
+    fl = Fx_of(o, wl);
+  }
+  M = wr.u / a_of(o, wr);
+  if (-M < -1.0) {
+    fr.d = fr.mx = fr.my = fr.E = 0.0;
+  } else if (fabs(M) <= 1.0) {
+    a = a_of(o, wr);
+    m = -0.25 * wr.d * a * sqr(1.0 - M);
+    fr.d = m;
+    fr.mx = m * ((2.0 * a / g) * (HALF * gm1 * M - 1.0));
+    fr.my = m * wr.v;
+    fr.E = m * ((2.0 * (g * wr.p / wr.d) / (g * g - 1.0)) * sqr(HALF * gm1 * M - 1.0) + HALF * sqr(wr.v));
+  } else if (-M > 1.0) {
+    fr = Fx_of(o, wr);
+  }
+  F.d = fl.d + fr.d; F.mx = fl.mx + fr.mx; F.my = fl.my + fr.my; F.E = fl.E + fr.E;
+  return F;
+}
+
+/* FluxAUSM (Euler2DState.cc:4056-4106). */
+static cst flux_ausm_x(const e2d_oracle *o, pst wl, pst wr) {
+  double al = a_of(o, wl), Ml = wl.u / al, ar = a_of(o, wr), Mr = wr.u / ar;
+  double Mp, pp, Mn, pn, Mh, ph, Hl, Hr;
+  cst F;
+  if (fabs(Ml) <= 1.0) { Mp = 0.25 * sqr(Ml + 1.0); pp = 0.25 * wl.p * sqr(Ml + 1.0) * (2.0 - Ml); }
+  else { Mp = 0.5 * (Ml + fabs(Ml)); pp = 0.5 * wl.p * (Ml + fabs(Ml)) / Ml; }
+  if (fabs(Mr) <= 1.0) { Mn = -0.25 * sqr(Mr - 1.0); pn = 0.25 * wr.p * sqr(Mr - 1.0) * (2.0 + Mr); }
+  else { Mn = 0.5 * (Mr - fabs(Mr)); pn = 0.5 * wr.p * (Mr - fabs(Mr)) / Mr; }
+  Mh = Mp + Mn; ph = pp + pn;
+  Hl = Ht_of(o, wl); Hr = Ht_of(o, wr);
+  F.d = 0.5 * Mh * (wl.d * al + wr.d * ar);
+  F.mx = 0.5 * Mh * (wl.d * al * wl.u + wr.d * ar * wr.u);
+  F.my = 0.5 * Mh * (wl.d * al * wl.v + wr.d * ar * wr.v);
+  F.E = 0.5 * Mh * (al * Hl + ar * Hr);
+  F.d -= 0.5 * fabs(Mh) * (wr.d * ar - wl.d * al);
+  F.mx -= 0.5 * fabs(Mh) * (wr.d * ar * wr.u - wl.d * al * wl.u);
+  F.my -= 0.5 * fabs(Mh) * (wr.d * ar * wr.v - wl.d * al * wl.v);
+  F.E -= 0.5 * fabs(Mh) * (ar * Hr - al * Hl);
+  F.mx += ph;
+  return F;
+}
+
+/* FluxAUSMplus (Euler2DState.cc:4170-4231). */
+static cst flux_ausmplus_x(const e2d_oracle *o, pst wl, pst wr) {
+  const double beta = 0.125, alpha = 0.1875;
+  double ah = HALF * (a_of(o, wl) + a_of(o, wr)), Ml = wl.u / ah, Mr = wr.u / ah;
+  double Mp, pp, Mn, pn, Mh, ph, Hl, Hr;
+  cst F;
+  if (fabs(Ml) < 1.0) {
+    Mp = 0.25 * sqr(Ml + 1.0) + beta * sqr(Ml * Ml - 1.0);
+    pp = (0.25 * sqr(Ml + 1.0) * (2.0 - Ml) + alpha * Ml * sqr(Ml * Ml - 1.0)) * wl.p;
+  } else {
+    Mp = 0.5 * (Ml + fabs(Ml));
+    pp = 0.5 * wl.p * (1.0 + ((Ml < 0.0) ? -1.0 : 1.0));
+  }
+  if (fabs(Mr) < 1.0) {
+    Mn = -0.25 * sqr(Mr - 1.0) - beta * sqr(Mr * Mr - 1.0);
+    pn = (0.25 * sqr(Mr - 1.0) * (2.0 + Mr) - alpha * Mr * sqr(Mr * Mr - 1.0)) * wr.p;
+  } else {
+    Mn = 0.5 * (Mr - fabs(Mr));
+    pn = 0.5 * wr.p * (1.0 - ((Mr < 0.0) ? -1.0 : 1.0));
+  }
+  Mh = Mp + Mn; ph = pp + pn;
+  Hl = Ht_of(o, wl); Hr = Ht_of(o, wr);
+  F.d = 0.5 * Mh * (wl.d + wr.d);
+  F.mx = 0.5 * Mh * (wl.d * wl.u + wr.d * wr.u);
+  F.my = 0.5 * Mh * (wl.d * wl.v + wr.d * wr.v);
+  F.E = 0.5 * Mh * (Hl + Hr);
+  F.d -= 0.5 * fabs(Mh) * (wr.d - wl.d);
+  F.mx -= 0.5 * fabs(Mh) * (wr.d * wr.u - wl.d * wl.u);
+  F.my -= 0.5 * fabs(Mh) * (wr.d * wr.v - wl.d * wl.v);
+  F.E -= 0.5 * fabs(Mh) * (Hr - Hl);
+  F.d *= ah; F.mx *= ah; F.my *= ah; F.E *= ah;
+  F.mx += ph;
+  return F;
+}
+
+/* Face flux of the scheme's i_Flux_Function (dispatch of Euler2DQuad.cc:968-1003). */
+static cst face_flux_n(const e2d_oracle *o, pst wl, pst wr, vec2 n) {
+  double c = n.x, s = n.y;
+  pst lr, rr;
+  cst Fr, F;
+  if (o->sc.flux == E2D_FLUX_ROE) return flux_roe_n(o, wl, wr, n);
+  lr.d = wl.d; lr.u = wl.u * c + wl.v * s; lr.v = -wl.u * s + wl.v * c; lr.p = wl.p;
+  rr.d = wr.d; rr.u = wr.u * c + wr.v * s; rr.v = -wr.u * s + wr.v * c; rr.p = wr.p;
+  switch (o->sc.flux) {
+    case E2D_FLUX_GODUNOV: Fr = Fx_of(o, riemann_x(o, lr, rr)); break;
+    case E2D_FLUX_RUSANOV: Fr = flux_rusanov_x(o, lr, rr); break;
+    case E2D_FLUX_HLLE: Fr = flux_hll_x(o, lr, rr, 0); break;
+    case E2D_FLUX_LINDE: Fr = flux_hll_x(o, lr, rr, 1); break;
+    case E2D_FLUX_HLLC: Fr = flux_hllc_x(o, lr, rr); break;
+    case E2D_FLUX_VANLEER: Fr = flux_vanleer_x(o, lr, rr); break;
+    case E2D_FLUX_AUSM: Fr = flux_ausm_x(o, lr, rr); break;
+    default: Fr = flux_ausmplus_x(o, lr, rr); break;
+  }
+  F.d = Fr.d;
+  F.mx = Fr.mx * c - Fr.my * s;
+  F.my = Fr.mx * s + Fr.my * c;
+  F.E = Fr.E;
+  return F;
+}
+
 /* Limiter_BarthJespersen / Limiter_Venkatakrishnan (src_2D/CFD/CFD.cc:696-751). */
 static double limiter(int kind, const double *uq, double u0, double umin, double umax) {
   double phi = 1.0, y;
@@ -455,7 +766,7 @@ static cst iface_flux(const e2d_oracle *o, int b, int i, int j) {
     wl = face_state(o, b, i, j, xfaceE(o, b, i, j));
     wr = face_state(o, b, i + 1, j, xfaceW(o, b, i + 1, j));
   }
-  return flux_roe_n(o, wl, wr, nfaceE(o, b, i, j));
+  return face_flux_n(o, wl, wr, nfaceE(o, b, i, j));
 }
 
 /* j-direction face flux between cells (i, j) and (i, j+1). */
@@ -472,7 +783,7 @@ static cst jface_flux(const e2d_oracle *o, int b, int i, int j) {
     wl = face_state(o, b, i, j, xfaceN(o, b, i, j));
     wr = face_state(o, b, i, j + 1, xfaceS(o, b, i, j + 1));
   }
-  return flux_roe_n(o, wl, wr, nfaceN(o, b, i, j));
+  return face_flux_n(o, wl, wr, nfaceN(o, b, i, j));
 }
 
 /* Residual of one block: dUdt_Residual_Evaluation (stage == 0,
@@ -750,7 +1061,8 @@ e2d_oracle *e2d_oracle_create(const e2d_blocks_desc *d, const e2d_scheme *sc, in
   size_t ncell, nnode;
   if (err) *err = 0;
   if (!d || !sc || d->nblk < 1 || d->nci < 2 || d->ncj < 2 || d->ng != 2 ||
-      (sc->n_stage != 1 && sc->n_stage != 2) || sc->flux != E2D_FLUX_ROE) {
+      (sc->n_stage != 1 && sc->n_stage != 2) || sc->flux < E2D_FLUX_GODUNOV || sc->flux > E2D_FLUX_AUSMPLUS ||
+      sc->flux == 7) {
     if (err) *err = E2D_ERR_ARG;
     return NULL;
   }

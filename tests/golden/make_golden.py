@@ -137,7 +137,27 @@ def golden_cases():
         ("nks_bump_bj_global_4", bump_bj, "nks", (4, 10, 25, 5.0, 1e-10)),
         # supersonic, first order, inexact Newton (GMRES tolerance 0.1): converges to 1e-10
         ("nks_bump_m14_converged", bump_m14, "nks", (30, 30, 120, 10.0, 1e-10, 0.1)),
+        # the same solve with the HLLE flux in the residual
+        ("nks_bump_m14_hlle", with_flux(bump_m14, cases.FLUX_HLLE), "nks", (30, 30, 120, 10.0, 1e-10, 0.1)),
+    ] + [
+        # every other flux function: a supersonic curvilinear residual, explicit
+        # steps in the subsonic channel with fixed inflow and reflecting walls,
+        # and in the channel with characteristic inflow/outflow
+        case for f, nm in FLUX_NAMES.items() for case in (
+            (f"residual_{nm}_curv_4x2x8", with_flux(cases.curvilinear_mach2(nbi=4, nbj=2, nc=8, seed=6), f),
+             "residual", 0),
+            (f"explicit_{nm}_channel_20", with_flux(ch, f), "explicit", 20),
+            (f"explicit_{nm}_channel_char_20", with_flux(ch_char, f), "explicit", 20))
     ]
+
+
+FLUX_NAMES = {cases.FLUX_GODUNOV: "godunov", cases.FLUX_RUSANOV: "rusanov", cases.FLUX_HLLE: "hlle",
+              cases.FLUX_LINDE: "linde", cases.FLUX_HLLC: "hllc", cases.FLUX_VANLEER: "vanleer",
+              cases.FLUX_AUSM: "ausm", cases.FLUX_AUSMPLUS: "ausmplus"}
+
+
+def with_flux(bs, flux):
+    return dataclasses.replace(bs, scheme=dataclasses.replace(bs.scheme, flux=flux))
 
 
 def main():

@@ -15,6 +15,39 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 # variable over the block set (so cells where the residual nearly cancels are
 # judged against the field's magnitude, not their own).
 RTOL_FP64 = 1e-12
+# The other flux functions have more cancellation in their dissipation terms
+# (differences of products, then scaled): FMA contraction moves their
+# residuals by up to 3.3e-12 (Godunov), 2e-12 (AUSM+, HLLC), 1.7e-12 (Linde)
+# on the curvilinear Mach-2 grid.
+RTOL_FP64_OTHER_FLUX = 1e-11
+
+# Paths through pow.  CUDA's pow and glibc's pow are both faithfully rounded
+# but need not round to the same neighbour (glibc's own pow differs from the
+# correctly rounded power in about 5 of 10^4 calls on the arguments these
+# paths take), so a case that reaches pow -- the characteristic boundary
+# condition, the Godunov and HLLC fluxes -- reproduces the reference up to
+# those one-ulp differences and what the steps carry them into (measured
+# 1e-15 .. 1.2e-13 after 20 steps); every other case is bit for bit.
+RTOL_POW = 1e-12
+
+
+def reaches_pow(bs):
+    if bs.scheme.flux in (cases.FLUX_GODUNOV, cases.FLUX_HLLC):
+        return True
+    return any(np.any(np.asarray(a) == cases.BC_CHARACTERISTIC) for a in (bs.bc_w, bs.bc_e, bs.bc_s, bs.bc_n))
+
+
+def rtol_fast(bs):
+    return RTOL_FP64 if bs.scheme.flux == cases.FLUX_ROE else RTOL_FP64_OTHER_FLUX
+
+
+def assert_exact(bs, got, want):
+    """Bit for bit, or within RTOL_POW where the case reaches pow."""
+    if reaches_pow(bs):
+        err = rel_err(got, want)
+        assert err <= RTOL_POW, err
+    else:
+        assert np.array_equal(got, want)
 
 
 def fixtures(kind=None):

@@ -129,6 +129,18 @@ def test_unsupported_scheme_is_rejected(driver, tmp_path):
     assert r.returncode == 3
 
 
+@pytest.mark.parametrize("name,code", [("Godunov", 1), ("Roe", 2), ("Rusanov", 3), ("HLLE", 4), ("Linde", 5),
+                                       ("HLLC", 6), ("VanLeer", 8), ("AUSM", 9), ("AUSM+", 10)])
+def test_flux_function_keywords(driver, tmp_path, name, code):
+    """The Flux_Function_Type names of Euler2DInput.cc:1850-1872 select the
+    reference's i_Flux_Function codes."""
+    text = DECK.replace("Flux_Function_Type =\nRoe", "Flux_Function_Type =\n" + name)
+    deck = write_deck(tmp_path / "f.in", text=text)
+    case = str(tmp_path / "f.case")
+    subprocess.run([driver, "parse", deck, case], check=True, capture_output=True)
+    assert cases.read_case(case).scheme.flux == code
+
+
 @pytest.mark.gpu
 def test_deck_run_matches_oracle_bitwise(driver, tmp_path):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
