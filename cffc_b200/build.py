@@ -61,14 +61,15 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
-    # C++ host layer (include/cffc_euler2d.hpp): plain host code
+    # C++ host layer (include/cffc_euler2d.hpp): plain host code, without
+    # contraction so the restart files' cell geometry is the reference's
     inc = os.path.join(ROOT_DIR, "include")
     for src in HOST_SOURCES:
         s = os.path.join(HOST, src)
         o = os.path.join(BUILD, src.replace(".cc", ".o"))
         objs.append(o)
         if _newer(o, [s, __file__, os.path.join(inc, "cffc_euler2d.hpp"), os.path.join(inc, "cffc_e2d.h")]):
-            cmd = [CXX, "-O2", "-std=c++17", "-fPIC", "-I", inc, "-c", s, "-o", o]
+            cmd = [CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", inc, "-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)

@@ -318,6 +318,48 @@ int e2d_set_state(e2d_handle* h, const double* W) {
   return 0;
 }
 
+// Ghost cells of (W2, U2) into (W, U); interior cells untouched.
+__global__ void ghost_from_stage_kernel(Blocks B, long long ncell) {
+  const long long per = (long long)B.NCi * B.NCj;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    const long long b = q / per, r = q % per;
+    const int i = int(r % B.NCi), j = int(r / B.NCi);
+    if (i >= NG && i < NG + B.nci && j >= NG && j < NG + B.ncj) continue;
+    const size_t s = size_t(per);
+    const size_t base = size_t(b) * 4 * s + size_t(r);
+    for (int v = 0; v < 4; ++v) {
+      B.W[base + v * s] = B.W2[base + v * s];
+      B.U[base + v * s] = B.U2[base + v * s];
+    }
+  }
+}
+
+// W = W(U) for every cell (Euler2D_cState::W, Euler2DState.h:1741; the
+// state a restart file's U gives, Euler2DQuad.h:1359-1362).
+__global__ void w_of_u_kernel(Blocks B, long long ncell) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    const long long b = q / ((long long)B.NCi * B.NCj), r = q % ((long long)B.NCi * B.NCj);
+    const size_t s = size_t(B.NCi) * B.NCj;
+    const size_t base = size_t(b) * 4 * s + size_t(r);
+    CState<double> u{B.U[base], B.U[base + s], B.U[base + 2 * s], B.U[base + 3 * s]};
+    const PState<double> w = W_of_U(u, B.gm1);
+    B.W[base] = w.d; B.W[base + s] = w.u; B.W[base + 2 * s] = w.v; B.W[base + 3 * s] = w.p;
+  }
+}
+
+int e2d_set_conserved(e2d_handle* h, const double* U) {
+  if (!h || !U) return E2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(h->B.U, U, sizeof(double) * 4 * h->ncell, cudaMemcpyHostToDevice, h->stream));
+  int grid = int((h->ncell + 255) / 256);
+  if (grid > 4096) grid = 4096;
+  w_of_u_kernel<<<grid, 256, 0, h->stream>>>(h->B, (long long)h->ncell);
+  CK(cudaGetLastError());
+  CK(cudaMemsetAsync(h->B.status, 0, sizeof(int) * 2, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
 int e2d_get_state(e2d_handle* h, double* W, double* U) {
   if (!h) return E2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
@@ -386,6 +428,15 @@ int e2d_rk_steps(e2d_handle* h, int n_steps, double* hist) {
   }
   h->B = saved;
   for (int s = 0; s < n_steps; ++s) CK(cudaGraphLaunch(h->step_graph, h->stream));
+  if (h->sc.n_stage == 2) {
+    // The reference keeps one state array, so after a two-stage step its
+    // ghost cells hold the last stage's exchange and BCs; here those went
+    // to the stage buffers.  Copy them so the final state matches the
+    // reference's in every cell (what a restart file records).
+    const int grid = int(std::min<size_t>((h->ncell + 255) / 256, 4096));
+    ghost_from_stage_kernel<<<grid, 256, 0, h->stream>>>(h->B, (long long)h->ncell);
+    CK(cudaGetLastError());
+  }
   if (hist)
     CK(cudaMemcpyAsync(hist, h->hist, sizeof(double) * 4 * size_t(n_steps) * h->B.ncase, cudaMemcpyDeviceToHost,
                        h->stream));

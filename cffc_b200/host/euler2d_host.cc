@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <ctime>
 #include <fstream>
 #include <istream>
 #include <sstream>
@@ -24,9 +25,11 @@ constexpr int INVALID_INPUT_CODE = -1, EXECUTE_CODE = 1, TERMINATE_CODE = 2;
 }  // namespace
 
 // ---- states (Euler2DState.h:1055-1095, :1741-1760, :3414-3430) -------------
+// gm1 = g - 1 and gm1i = 1/gm1 as Euler2D_pState::setgas derives them (the
+// double g - 1 is not the double nearest 0.4)
 double Euler2D_pState::g = 1.4;
-double Euler2D_pState::gm1 = 0.4;
-double Euler2D_pState::gm1i = 1.0 / 0.4;
+double Euler2D_pState::gm1 = 1.4 - 1.0;
+double Euler2D_pState::gm1i = 1.0 / (1.4 - 1.0);
 double Euler2D_pState::R = 287.0636;
 
 double Euler2D_pState::a() const { return std::sqrt(g * p / d); }
@@ -182,15 +185,22 @@ int Parse_Next_Input_Control_Parameter(Euler2D_Input_Parameters& IP, std::istrea
   }
   if (code == "ICs_Type") {
     if (str(IP.ICs_Type)) return INVALID_INPUT_CODE;
-    return (IP.ICs_Type == "Uniform" || IP.ICs_Type == "Constant") ? 0 : INVALID_INPUT_CODE;
+    const std::string& t = IP.ICs_Type;
+    return (t == "Uniform" || t == "Constant" || t == "Restart") ? 0 : INVALID_INPUT_CODE;
   }
   if (code == "Grid_Type") {
-    if (str(IP.Grid_Type)) return INVALID_INPUT_CODE;
-    const std::string& t = IP.Grid_Type;
-    return (t == "Rectangular_Box" || t == "Periodic_Box" || t == "Sine_Squared_Bump_Channel") ? 0
-                                                                                                : INVALID_INPUT_CODE;
+    // any of the reference's grid names: a restart run (ICs_Type Restart)
+    // takes its grid from the restart files; otherwise
+    // Create_Initial_Solution_Blocks builds Rectangular_Box, Periodic_Box and
+    // Sine_Squared_Bump_Channel and rejects the rest
+    return str(IP.Grid_Type);
   }
   if (code == "Output_File_Name") return str(IP.Output_File_Name);
+  if (code == "Restart_File_Name") {  // Euler2DInput.cc:2186-2191
+    if (str(IP.Restart_File_Name)) return INVALID_INPUT_CODE;
+    IP.Restart_File_Name += ".soln";
+    return 0;
+  }
   if (code == "GPU_Precision") {
     if (str(s)) return INVALID_INPUT_CODE;
     if (s == "FP64") IP.Precision = E2D_PREC_FP64;
@@ -210,6 +220,7 @@ int Parse_Next_Input_Control_Parameter(Euler2D_Input_Parameters& IP, std::istrea
   }
   if (code == "CFL_Number") return num_d(IP.CFL_Number, true);
   if (code == "Time_Accurate") return num_i(IP.Time_Accurate, 0);
+  if (code == "Restart_Solution_Save_Frequency") return num_i(IP.Restart_Solution_Save_Frequency, 1);
   if (code == "Local_Time_Stepping") {
     int rc = num_i(IP.Local_Time_Stepping, 0);
     if (IP.Local_Time_Stepping > 1) IP.Local_Time_Stepping = 1;  // scalar local time stepping
@@ -228,6 +239,7 @@ int Parse_Next_Input_Control_Parameter(Euler2D_Input_Parameters& IP, std::istrea
   if (code == "Number_of_Cells_Jdir") return num_i(IP.Number_of_Cells_Jdir, 1);
   if (code == "Number_of_Blocks_Idir") return num_i(IP.Number_of_Blocks_Idir, 1);
   if (code == "Number_of_Blocks_Jdir") return num_i(IP.Number_of_Blocks_Jdir, 1);
+  if (code == "Number_of_Blocks_Per_Processor") return num_i(IP.Number_of_Blocks_Per_Processor, 1);
   if (code == "Number_of_Ghost_Cells") {
     int rc = num_i(IP.Number_of_Ghost_Cells, 1);
     return rc ? rc : (IP.Number_of_Ghost_Cells == 2 ? 0 : INVALID_INPUT_CODE);
@@ -285,7 +297,13 @@ int Euler2D_Input_Parameters::Process_Input_Control_Parameter_File(const std::st
   std::string code;
   while (next_token(in, Line_Number, code)) {
     const int rc = Parse_Next_Input_Control_Parameter(*this, in, code);
-    if (rc == EXECUTE_CODE || rc == TERMINATE_CODE) break;
+    if (rc == TERMINATE_CODE) break;
+    if (rc == EXECUTE_CODE) {
+      // the commands that follow (Write_Restart, Write_Output, ...) up to
+      // Terminate, for the driver to carry out after the solve
+      while (next_token(in, Line_Number, code) && code != "Terminate") Commands.push_back(code);
+      break;
+    }
     if (rc == INVALID_INPUT_CODE) return Line_Number > 0 ? Line_Number : 1;
   }
   set_freestream();
@@ -296,6 +314,8 @@ int Euler2D_Input_Parameters::Process_Input_Control_Parameter_File(const std::st
 int Create_Initial_Solution_Blocks(const Euler2D_Input_Parameters& IP, std::vector<Euler2D_Quad_Block>& blocks,
                                    std::vector<int>& neighbour) {
   const int nbi = IP.Number_of_Blocks_Idir, nbj = IP.Number_of_Blocks_Jdir, ng = IP.Number_of_Ghost_Cells;
+  const std::string& t = IP.Grid_Type;
+  if (t != "Rectangular_Box" && t != "Periodic_Box" && t != "Sine_Squared_Bump_Channel") return 1;
   if (IP.Number_of_Cells_Idir % nbi || IP.Number_of_Cells_Jdir % nbj) return 1;
   const int nci = IP.Number_of_Cells_Idir / nbi, ncj = IP.Number_of_Cells_Jdir / nbj;
   const int Nx = IP.Number_of_Cells_Idir, Ny = IP.Number_of_Cells_Jdir;
@@ -421,6 +441,15 @@ void gather_W(const std::vector<Euler2D_Quad_Block>& blocks, std::vector<double>
         for (int i = 0; i < NCi; ++i) W[((b * 4 + v - 1) * NCj + j) * NCi + i] = blocks[b].W[i][j][v];
 }
 
+void gather_U(const std::vector<Euler2D_Quad_Block>& blocks, std::vector<double>& U) {
+  const int NCi = blocks[0].NCi, NCj = blocks[0].NCj;
+  U.resize(blocks.size() * 4 * size_t(NCi) * NCj);
+  for (size_t b = 0; b < blocks.size(); ++b)
+    for (int v = 1; v <= 4; ++v)
+      for (int j = 0; j < NCj; ++j)
+        for (int i = 0; i < NCi; ++i) U[((b * 4 + v - 1) * NCj + j) * NCi + i] = blocks[b].U[i][j][v];
+}
+
 }  // namespace
 
 Euler2D_Device_Blocks::Euler2D_Device_Blocks(std::vector<Euler2D_Quad_Block>& blocks, const std::vector<int>& neighbour,
@@ -445,6 +474,13 @@ int Euler2D_Device_Blocks::upload() {
   std::vector<double> W;
   gather_W(blocks_, W);
   return e2d_set_state(h_, W.data());
+}
+
+int Euler2D_Device_Blocks::upload_conserved() {
+  if (!h_) return E2D_ERR_ARG;
+  std::vector<double> U;
+  gather_U(blocks_, U);
+  return e2d_set_conserved(h_, U.data());
 }
 
 int Euler2D_Device_Blocks::download() {
@@ -579,6 +615,352 @@ double Max_Norm_Residual(const Euler2D_Quad_Block& B) {
   return m;
 }
 
+// ---- restart files --------------------------------------------------------------
+namespace {
+
+// Restart_File_Name up to its first ' ' or '.' (Euler2DQuadMultiBlock.cc:160-168).
+std::string restart_prefix(const Euler2D_Input_Parameters& IP) {
+  return IP.Restart_File_Name.substr(0, IP.Restart_File_Name.find_first_of(" ."));
+}
+std::string soln_file(const Euler2D_Input_Parameters& IP, int gblknum) {
+  char ext[32];
+  snprintf(ext, sizeof(ext), "%.6d.soln", gblknum);
+  return restart_prefix(IP) + "_blk" + ext;
+}
+std::string tree_file(const Euler2D_Input_Parameters& IP) { return restart_prefix(IP) + "_quadtree.tree"; }
+
+// quadCentroid (Math.h:311-351) on (SW, SE, NE, NW): the cell centroid and
+// area Grid2D_Quad_Block_HO::Update_Cells stores and the restart file lists.
+void quad_centroid(const Vector2D& p0, const Vector2D& p1, const Vector2D& p2, const Vector2D& p3, Vector2D& c,
+                   double& area) {
+  const Vector2D p[4] = {p0, p1, p2, p3};
+  double atmp = 0.0, xt = 0.0, yt = 0.0;
+  for (int k = 0; k < 4; ++k) {
+    const Vector2D& a = p[(k + 3) % 4];
+    const Vector2D& b = p[k];
+    const double ai = a.x * b.y - b.x * a.y;
+    atmp += ai;
+    xt += (b.x + a.x) * ai;
+    yt += (b.y + a.y) * ai;
+  }
+  area = 0.5 * atmp;
+  if (atmp != 0.0) {
+    c.x = xt / (3.0 * atmp);
+    c.y = yt / (3.0 * atmp);
+  } else {
+    c.x = c.y = 0.0;
+  }
+}
+
+// Stream forms of the reference's types (Vector2D, Euler2D_pState /
+// cState: a leading blank, scientific; Math/Vector2D.h:433,
+// Euler2DState.h:1349, 1724).
+void put_vec(std::ostream& o, double x, double y) {
+  o.setf(std::ios::scientific);
+  o << " " << x << " " << y;
+  o.unsetf(std::ios::scientific);
+}
+void put_state(std::ostream& o, double a, double b, double c, double d) {
+  o.setf(std::ios::scientific);
+  o << " " << a << " " << b << " " << c << " " << d;
+  o.unsetf(std::ios::scientific);
+}
+
+// One block in the layout of operator<<(ostream&, Euler2D_Quad_Block)
+// (Euler2DQuad.h:1306-1336) around operator<<(ostream&, Grid2D_Quad_Block_HO)
+// (Grid/HO_Grid2DQuad.cc:13763-13990) of a first-order geometry without
+// boundary splines or stretching.
+void put_block(std::ostream& o, const Euler2D_Quad_Block& B) {
+  const Grid2D_Quad_Block& G = B.Grid;
+  const int ng = B.Nghost, NCi = B.NCi, NCj = B.NCj;
+  o << G.NNi << " " << ng << " " << G.NNi - ng - 1 << "\n";
+  o << G.NNj << " " << ng << " " << G.NNj - ng - 1 << "\n";
+  o << ng << "\n" << 0 << "\n" << 0 << "\n";
+  o << NCi << " " << B.ICl << " " << B.ICu << "\n";
+  o << NCj << " " << B.JCl << " " << B.JCu << "\n";
+  o.precision(15);
+  for (int j = 0; j < G.NNj; ++j)
+    for (int i = 0; i < G.NNi; ++i) {
+      put_vec(o, G.Node[i][j].x, G.Node[i][j].y);
+      o << "\n";
+    }
+  for (int j = 0; j < NCj; ++j)
+    for (int i = 0; i < NCi; ++i) {
+      Vector2D c;
+      double A;
+      quad_centroid(G.Node[i][j], G.Node[i + 1][j], G.Node[i + 1][j + 1], G.Node[i][j + 1], c, A);
+      o << " " << i << " " << j;
+      put_vec(o, c.x, c.y);
+      o.setf(std::ios::scientific);
+      o << " " << A << "\n";
+      o.unsetf(std::ios::scientific);
+      // geometric moments of order 0: the single moment (0, 0) = 1
+      // (TaylorDerivatives2D.h:143-150, 808-817)
+      o << " ";
+      o.width(4);
+      o << 0 << std::endl;
+      o.width(4);
+      o << 0;
+      o.width(4);
+      o << 0;
+      o.precision(15);
+      o.width(25);
+      o << 1.0 << std::endl;
+      o << "\n";
+    }
+  for (int i = 0; i < NCi; ++i) o << G.BCtypeN[i] << " " << G.BCtypeS[i] << "\n";
+  for (int j = 0; j < NCj; ++j) o << G.BCtypeE[j] << " " << G.BCtypeW[j] << "\n";
+  for (int k = 0; k < 12; ++k) o << 0 << "\n" << 0 << "\n";  // no boundary splines
+  o.setf(std::ios::scientific);
+  o << 0.0 << " " << 0.0 << " " << 0.0 << " " << 0.0 << "\n";
+  o << 0.0 << " " << 0.0 << " " << 0.0 << " " << 0.0 << "\n";
+  o << 0 << " " << 1.0 << " " << 1.0 << "\n";
+  o << 0 << " " << 1.0 << " " << 1.0 << "\n";
+  o.unsetf(std::ios::scientific);
+  o << 1 << " " << 1 << " " << 1 << " " << 1 << "\n";
+  o << NCi << " " << B.ICl << " " << B.ICu << " " << ng << "\n";
+  o << NCj << " " << B.JCl << " " << B.JCu << "\n";
+  o << 0 << "\n";  // Axisymmetric
+  for (int j = 0; j < NCj; ++j)
+    for (int i = 0; i < NCi; ++i) {
+      const Euler2D_cState& U = B.U[i][j];
+      put_state(o, U.d, U.dv.x, U.dv.y, U.E);
+      o << "\n";
+    }
+  for (int j = 0; j < NCj; ++j) {
+    put_state(o, B.WoW[j].d, B.WoW[j].v.x, B.WoW[j].v.y, B.WoW[j].p);
+    o << "\n";
+    put_state(o, B.WoE[j].d, B.WoE[j].v.x, B.WoE[j].v.y, B.WoE[j].p);
+    o << "\n";
+  }
+  for (int i = 0; i < NCi; ++i) {
+    put_state(o, B.WoS[i].d, B.WoS[i].v.x, B.WoS[i].v.y, B.WoS[i].p);
+    o << "\n";
+    put_state(o, B.WoN[i].d, B.WoN[i].v.x, B.WoN[i].v.y, B.WoN[i].p);
+    o << "\n";
+  }
+  o << 0 << "\n";  // NumberOfHighOrderVariables
+}
+
+// Whitespace-separated reading, as the reference's istream >> with skipws.
+template <class T> bool get(std::istream& in, T& v) { return static_cast<bool>(in >> v); }
+bool skip(std::istream& in, long n) {
+  std::string t;
+  for (long k = 0; k < n; ++k)
+    if (!(in >> t)) return false;
+  return true;
+}
+
+// Spline2D_HO and its Spline2DInterval_HO list (Grid/HO_Spline2D.h:808-830,
+// Grid/HO_Spline2DInterval.h:271-330): read and dropped.
+bool skip_spline(std::istream& in) {
+  long np, n;
+  if (!get(in, np)) return false;
+  if (np != 0 && !skip(in, 4 + 4 * np)) return false;
+  if (!get(in, n)) return false;
+  for (long k = 0; k < n; ++k) {
+    long nsub, ngq;
+    if (!get(in, nsub) || !get(in, ngq)) return false;
+    // lengths; per Gauss point its position and normal; per contour-integral
+    // point (3 per subinterval) its position and dy/ds
+    if (!skip(in, nsub + 4 * nsub * ngq + 3 * 3 * nsub)) return false;
+  }
+  return true;
+}
+
+// operator>>(istream&, Euler2D_Quad_Block) (Euler2DQuad.h:1338-1400).
+bool get_block(std::istream& in, Euler2D_Quad_Block& B) {
+  int nni, inl, inu, nnj, jnl, jnu, ng, rec, bflag, nci, icl, icu, ncj, jcl, jcu;
+  if (!(in >> nni >> inl >> inu >> nnj >> jnl >> jnu >> ng >> rec >> bflag)) return false;
+  if (nni == 0 || nnj == 0) return false;
+  if (!(in >> nci >> icl >> icu >> ncj >> jcl >> jcu)) return false;
+  if (nci != nni - 1 || ncj != nnj - 1 || nci <= 2 * ng || ncj <= 2 * ng) return false;
+  B.allocate(nci - 2 * ng, ncj - 2 * ng, ng);
+  Grid2D_Quad_Block& G = B.Grid;
+  for (int j = 0; j < nnj; ++j)
+    for (int i = 0; i < nni; ++i)
+      if (!(in >> G.Node[i][j].x >> G.Node[i][j].y)) return false;
+  const long moments = long(rec + 1) * (rec + 2) / 2;
+  for (int j = 0; j < ncj; ++j)
+    for (int i = 0; i < nci; ++i) {
+      int order;
+      if (!skip(in, 5) || !get(in, order) || order != rec || !skip(in, 3 * moments)) return false;
+    }
+  for (int i = 0; i < nci; ++i)
+    if (!(in >> G.BCtypeN[i] >> G.BCtypeS[i])) return false;
+  for (int j = 0; j < ncj; ++j)
+    if (!(in >> G.BCtypeE[j] >> G.BCtypeW[j])) return false;
+  for (int k = 0; k < 12; ++k)
+    if (!skip_spline(in)) return false;
+  if (!skip(in, 8 + 6 + 4)) return false;  // Smin/Smax, stretching, orthogonality flags
+  int ni, il, iu, g2, nj, jl, ju, axi;
+  if (!(in >> ni >> il >> iu >> g2 >> nj >> jl >> ju >> axi)) return false;
+  if (ni != nci || nj != ncj || g2 != ng) return false;
+  for (int j = 0; j < ncj; ++j)
+    for (int i = 0; i < nci; ++i) {
+      Euler2D_cState& U = B.U[i][j];
+      if (!(in >> U.d >> U.dv.x >> U.dv.y >> U.E)) return false;
+      B.W[i][j] = U.W();
+    }
+  for (int j = 0; j < ncj; ++j) {
+    Euler2D_pState& w = B.WoW[j];
+    Euler2D_pState& e = B.WoE[j];
+    if (!(in >> w.d >> w.v.x >> w.v.y >> w.p >> e.d >> e.v.x >> e.v.y >> e.p)) return false;
+  }
+  for (int i = 0; i < nci; ++i) {
+    Euler2D_pState& s = B.WoS[i];
+    Euler2D_pState& n = B.WoN[i];
+    if (!(in >> s.d >> s.v.x >> s.v.y >> s.p >> n.d >> n.v.x >> n.v.y >> n.p)) return false;
+  }
+  int n_ho;
+  return get(in, n_ho) && n_ho == 0;  // high-order variables are outside this path
+}
+
+// One node of the block tree (QuadTreeBlock::read, AMR/QuadTree.h:357-385,
+// with AdaptiveBlock2D operator>>, AMR/AdaptiveBlock.h:720-760).
+struct TreeLeaf {
+  int gblknum, cpu, blknum, level;
+  int n[8];          // neighbour counts N S E W NW NE SE SW
+  int ncpu[8], nblk[8], nlevel[8];
+};
+bool read_tree_node(std::istream& in, std::vector<TreeLeaf>& leaves) {
+  int used, gbl, cpu, blk, di, dj, dg, sector, level;
+  if (!(in >> used >> gbl >> cpu >> blk >> di >> dj >> dg >> sector >> level)) return false;
+  TreeLeaf L{};
+  L.gblknum = gbl; L.cpu = cpu; L.blknum = blk; L.level = level;
+  for (int s = 0; s < 8; ++s) {
+    if (!get(in, L.n[s])) return false;
+    for (int k = 0; k < L.n[s]; ++k) {
+      int c, b, i, j, g, sec, lev;
+      if (!(in >> c >> b >> i >> j >> g >> sec >> lev)) return false;
+      if (k == 0) { L.ncpu[s] = c; L.nblk[s] = b; L.nlevel[s] = lev; }
+    }
+  }
+  int children;
+  if (!get(in, children)) return false;
+  if (used) leaves.push_back(L);
+  if (!used && children > 0)
+    for (int k = 0; k < 4; ++k)
+      if (!read_tree_node(in, leaves)) return false;
+  return true;
+}
+
+// AdaptiveBlock2D_Info of a same-level root block on CPU 0 (AMR/AdaptiveBlock.h:502-509).
+void put_info(std::ostream& o, int blknum, const Euler2D_Quad_Block& B) {
+  o << " " << 0 << " " << blknum << " " << B.ICu - B.ICl + 1 << " " << B.JCu - B.JCl + 1 << " " << B.Nghost
+    << " " << -1 << " " << 0;
+}
+
+}  // namespace
+
+int Write_QuadTree(const std::vector<Euler2D_Quad_Block>& blocks, const std::vector<int>& neighbour,
+                   const Euler2D_Input_Parameters& IP) {
+  const int nbi = IP.Number_of_Blocks_Idir, nbj = IP.Number_of_Blocks_Jdir;
+  const int nblk = static_cast<int>(blocks.size());
+  if (nbi * nbj != nblk || neighbour.size() != size_t(8) * nblk) return 1;
+  std::ofstream o(tree_file(IP));
+  if (!o.good()) return 1;
+  o << nbi << " " << nbj << " " << 1 << " "
+    << std::max(nblk, IP.Number_of_Blocks_Per_Processor) << "\n";
+  // neighbour slots in the tree's order N S E W NW NE SE SW (ours: W E S N SW SE NW NE)
+  static const int slot[8] = {3, 2, 1, 0, 6, 7, 5, 4};
+  for (int b = 0; b < nblk; ++b) {
+    o << " " << 1 << " " << b;
+    put_info(o, b, blocks[b]);
+    for (int s = 0; s < 8; ++s) {
+      const int nb = neighbour[8 * b + slot[s]];
+      o << "\n " << (nb >= 0 ? 1 : 0);
+      if (nb >= 0) {
+        o << " ";
+        put_info(o, nb, blocks[nb]);
+      }
+    }
+    o << "\n" << " " << 0 << "\n";
+  }
+  return o.good() ? 0 : 1;
+}
+
+int Write_Restart_Solution(const std::vector<Euler2D_Quad_Block>& blocks, const Euler2D_Input_Parameters& IP,
+                           int Number_of_Time_Steps, double Time, double CPU_Time) {
+  for (size_t b = 0; b < blocks.size(); ++b) {
+    std::ofstream o(soln_file(IP, static_cast<int>(b)));
+    if (!o.good()) return 1;
+    o.setf(std::ios::scientific);
+    o.precision(14);
+    o << Number_of_Time_Steps << " " << Time << " ";
+    o << " " << CPU_Time << "\n";
+    o.unsetf(std::ios::scientific);
+    o << IP.Gas_Type << "\n";
+    o.precision(14);
+    put_block(o, blocks[b]);
+    if (!o.good()) return 1;
+  }
+  return 0;
+}
+
+int Read_QuadTree(std::vector<Euler2D_Quad_Block>& blocks, std::vector<int>& neighbour,
+                  Euler2D_Input_Parameters& IP) {
+  std::ifstream in(tree_file(IP));
+  if (!in.good()) return 1;
+  int nri, nrj, ncpu, nblk;
+  if (!(in >> nri >> nrj >> ncpu >> nblk) || nri < 1 || nrj < 1) return 1;
+  IP.Number_of_Blocks_Idir = nri;
+  IP.Number_of_Blocks_Jdir = nrj;
+  IP.Number_of_Blocks_Per_Processor = nblk;
+  std::vector<TreeLeaf> leaves;
+  for (int r = 0; r < nri * nrj; ++r)
+    if (!read_tree_node(in, leaves)) return 1;
+  const int n = static_cast<int>(leaves.size());
+  std::vector<int> order(n, -1);  // gblknum -> leaf
+  for (int k = 0; k < n; ++k) {
+    const int g = leaves[k].gblknum;
+    if (g < 0 || g >= n || order[g] >= 0 || leaves[k].level != leaves[0].level) return 1;
+    order[g] = k;
+  }
+  auto find = [&](int cpu, int blk) {
+    for (int k = 0; k < n; ++k)
+      if (leaves[k].cpu == cpu && leaves[k].blknum == blk) return leaves[k].gblknum;
+    return -1;
+  };
+  static const int slot[8] = {3, 2, 1, 0, 6, 7, 5, 4};  // tree side -> W E S N SW SE NW NE
+  neighbour.assign(size_t(8) * n, -1);
+  for (int g = 0; g < n; ++g) {
+    const TreeLeaf& L = leaves[order[g]];
+    for (int s = 0; s < 8; ++s) {
+      if (L.n[s] == 0) continue;
+      if (L.n[s] != 1 || L.nlevel[s] != L.level) return 1;  // a resolution change
+      const int nb = find(L.ncpu[s], L.nblk[s]);
+      if (nb < 0) return 1;
+      neighbour[8 * g + slot[s]] = nb;
+    }
+  }
+  blocks.assign(n, Euler2D_Quad_Block());
+  return 0;
+}
+
+int Read_Restart_Solution(std::vector<Euler2D_Quad_Block>& blocks, Euler2D_Input_Parameters& IP,
+                          int& Number_of_Time_Steps, double& Time, double& CPU_Time) {
+  for (size_t b = 0; b < blocks.size(); ++b) {
+    std::ifstream in(soln_file(IP, static_cast<int>(b)));
+    if (!in.good()) return 1;
+    int nsteps;
+    double t, cpu;
+    std::string rest, gas;
+    if (!(in >> nsteps >> t >> cpu)) return 1;
+    std::getline(in, rest);
+    std::getline(in, gas);
+    if (b == 0) {
+      Number_of_Time_Steps = nsteps;
+      IP.Maximum_Number_of_Time_Steps += nsteps;
+      Time = t;
+      CPU_Time = cpu;
+      if (gas != IP.Gas_Type) IP.Gas_Type = gas;
+    }
+    if (!get_block(in, blocks[b])) return 1;
+  }
+  return 0;
+}
+
 // ---- solver driver (Euler2DQuadSolver, Euler2DQuadSolvers.cc:26-1100) --------
 int Euler2DQuadSolver(const char* Input_File_Name_ptr, int batch_flag) {
   Euler2D_Input_Parameters IP;
@@ -589,18 +971,50 @@ int Euler2DQuadSolver(const char* Input_File_Name_ptr, int batch_flag) {
   }
   std::vector<Euler2D_Quad_Block> blocks;
   std::vector<int> neighbour;
-  if ((rc = Create_Initial_Solution_Blocks(IP, blocks, neighbour))) return E2D_ERR_ARG;
+  int number_of_time_steps = 0;
+  double Time = 0.0, cpu_time = 0.0;
+  const bool restart = IP.ICs_Type == "Restart";
+  if (restart) {  // Euler2DQuadSolvers.cc:223-270
+    if (Read_QuadTree(blocks, neighbour, IP) ||
+        Read_Restart_Solution(blocks, IP, number_of_time_steps, Time, cpu_time))
+      return E2D_ERR_ARG;
+  } else if ((rc = Create_Initial_Solution_Blocks(IP, blocks, neighbour))) {
+    return E2D_ERR_ARG;
+  }
   Euler2D_Device_Blocks dev(blocks, neighbour, IP);
   if (!dev.handle()) return E2D_ERR_CUDA;
+  if (restart && (rc = dev.upload_conserved())) return rc;
+  const std::clock_t c0 = std::clock();
+  auto save = [&]() -> bool {  // Write_QuadTree + Write_Restart_Solution of the current state
+    if (dev.download()) return true;
+    const double cpu = cpu_time + double(std::clock() - c0) / CLOCKS_PER_SEC;
+    return Write_QuadTree(blocks, neighbour, IP) != 0 ||
+           Write_Restart_Solution(blocks, IP, number_of_time_steps, Time, cpu) != 0;
+  };
+  // the explicit loop in chunks that end where the reference saves restart
+  // files (every Restart_Solution_Save_Frequency steps, not at its first step)
   std::vector<double> hist;
-  if (IP.Maximum_Number_of_Time_Steps > 0) {
-    if ((rc = dev.explicit_steps(IP.Maximum_Number_of_Time_Steps, &hist))) return rc;
+  const int first = number_of_time_steps, freq = IP.Restart_Solution_Save_Frequency;
+  while (number_of_time_steps < IP.Maximum_Number_of_Time_Steps) {
+    const int n = std::min(IP.Maximum_Number_of_Time_Steps - number_of_time_steps,
+                           freq - number_of_time_steps % freq);
+    std::vector<double> h;
+    if ((rc = dev.explicit_steps(n, &h))) return rc;
+    for (int k = 0; k < n; ++k) Time += IP.CFL_Number * h[4 * k];
+    hist.insert(hist.end(), h.begin(), h.begin() + 4 * n);
+    number_of_time_steps += n;
+    if (number_of_time_steps % freq == 0 && number_of_time_steps > first && save()) return E2D_ERR_ARG;
   }
+  // ghost exchange and BCs of the final explicit state (Euler2DQuadSolvers.cc:901-925)
+  if (number_of_time_steps > first && (rc = e2d_fill_ghosts(dev.handle()))) return rc;
   std::vector<e2d_nks_step> nks_hist;
   if (IP.NKS.max_newton > 0) {
     if ((rc = dev.nks(IP.NKS, &nks_hist))) return rc;
   }
   if ((rc = dev.download())) return rc;
+  // commands after Execute (Euler2DQuadSolvers.cc:1317-1360 for Write_Restart)
+  for (const std::string& c : IP.Commands)
+    if (c == "Write_Restart" && save()) return E2D_ERR_ARG;
   // cell-centred output: one zone per block (x, y of the cell centroid
   // average of its nodes; rho, u, v, p)
   FILE* f = fopen(IP.Output_File_Name.c_str(), "w");

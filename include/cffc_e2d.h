@@ -136,6 +136,11 @@ void e2d_destroy(e2d_handle *h);
  * Replaces the ICs / Uo assignment loops (Euler2DQuadSingleBlock.cc:1689). */
 int e2d_set_state(e2d_handle *h, const double *W);
 
+/* Uploads the conserved state U of every cell [nblk][4][NCj][NCi] and sets
+ * W = W(U): the state a restart file holds (operator>> of
+ * Euler2D_Quad_Block reads U and derives W, Euler2DQuad.h:1356-1362). */
+int e2d_set_conserved(e2d_handle *h, const double *U);
+
 /* Downloads W and/or U (either may be NULL). */
 int e2d_get_state(e2d_handle *h, double *W, double *U);
 

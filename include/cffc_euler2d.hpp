@@ -114,11 +114,16 @@ struct Euler2D_Input_Parameters {
   double Bump_Height = 0.1;
   int Number_of_Cells_Idir = 100, Number_of_Cells_Jdir = 100;
   int Number_of_Blocks_Idir = 1, Number_of_Blocks_Jdir = 1;
+  int Number_of_Blocks_Per_Processor = 0;  // 0: the block count (the quadtree's capacity)
   int Number_of_Ghost_Cells = 2;
   double Mach_Number = 0.0, Flow_Angle = 0.0;
   double Pressure = 101325.0, Temperature = 288.16;
   Euler2D_pState Wo;               // freestream (from Pressure, Temperature, Mach, angle)
   std::string Output_File_Name = "outputfile.dat";
+  std::string Restart_File_Name = "restartfile.soln";  // the keyword's value + ".soln"
+  std::string Gas_Type = "AIR";
+  int Restart_Solution_Save_Frequency = 1000;
+  std::vector<std::string> Commands;  // commands after Execute (Write_Restart, Write_Output, ...)
   int Precision = E2D_PREC_FP64;   // GPU_Precision keyword (library extension)
   e2d_nks_params NKS{};            // Maximum_Number_of_NKS_Iterations, GMRES_*, NKS_*
   std::vector<std::string> Ignored; // keywords of the reference outside this path
@@ -141,6 +146,7 @@ class Euler2D_Device_Blocks {
   Euler2D_Device_Blocks(const Euler2D_Device_Blocks&) = delete;
   Euler2D_Device_Blocks& operator=(const Euler2D_Device_Blocks&) = delete;
   int upload();                         // W of the host blocks -> device (U = U(W))
+  int upload_conserved();               // U of the host blocks -> device (W = W(U)), as after a restart
   int download();                       // device W, U -> host blocks
   int residual();                       // ghost fill + dUdt_Residual_Evaluation
   int explicit_steps(int n, std::vector<double>* hist);  // hist: n x (dt, L1, L2, Max)
@@ -178,8 +184,39 @@ double L1_Norm_Residual(const Euler2D_Quad_Block& SolnBlk);
 double L2_Norm_Residual(const Euler2D_Quad_Block& SolnBlk);
 double Max_Norm_Residual(const Euler2D_Quad_Block& SolnBlk);
 
-// Whole solve from a deck: grid, ICs, explicit steps, then Newton-Krylov
-// when Maximum_Number_of_NKS_Iterations > 0; writes Output_File_Name.
+// ---- restart files -------------------------------------------------------
+// The reference's checkpoint format: PREFIX_quadtree.tree (the block tree,
+// Write_QuadTree / Read_QuadTree, AMR/AMR.h:163-340) and one
+// PREFIX_blkNNNNNN.soln per block, NNNNNN the global block number
+// (Write_Restart_Solution / Read_Restart_Solution,
+// Euler2DQuadMultiBlock.cc:145-300), PREFIX = Restart_File_Name up to its
+// first '.' or ' '.  Files written here are the reference's byte for byte
+// for a block set without boundary splines (the reference's own writer
+// prints 16 significant digits, so a round trip moves a value by at most
+// one unit in its 16th digit).  Blocks are numbered b = j * nbi + i over the
+// Number_of_Blocks_Idir x Number_of_Blocks_Jdir roots, one CPU.  Reading
+// takes any tree whose used blocks all sit at one refinement level (no
+// resolution changes) and files with or without boundary splines, whose
+// data is skipped.  Return 0, or 1 when a file cannot be opened or parsed.
+int Write_QuadTree(const std::vector<Euler2D_Quad_Block>& blocks, const std::vector<int>& neighbour,
+                   const Euler2D_Input_Parameters& IP);
+int Write_Restart_Solution(const std::vector<Euler2D_Quad_Block>& blocks, const Euler2D_Input_Parameters& IP,
+                           int Number_of_Time_Steps, double Time, double CPU_Time);
+// Fills neighbour (indexed by global block number), sizes blocks, and sets
+// the root layout Number_of_Blocks_Idir/Jdir and Number_of_Blocks_Per_Processor
+// from the tree.
+int Read_QuadTree(std::vector<Euler2D_Quad_Block>& blocks, std::vector<int>& neighbour,
+                  Euler2D_Input_Parameters& IP);
+// Reads every block of the tree; as the reference does, adds the stored
+// step count to Maximum_Number_of_Time_Steps.
+int Read_Restart_Solution(std::vector<Euler2D_Quad_Block>& blocks, Euler2D_Input_Parameters& IP,
+                          int& Number_of_Time_Steps, double& Time, double& CPU_Time);
+
+// Whole solve from a deck: grid and ICs (or, for ICs_Type Restart, the
+// restart files), explicit steps (restart files every
+// Restart_Solution_Save_Frequency steps), then Newton-Krylov when
+// Maximum_Number_of_NKS_Iterations > 0; writes Output_File_Name, and the
+// restart files when the deck's commands after Execute hold Write_Restart.
 int Euler2DQuadSolver(const char* Input_File_Name_ptr, int batch_flag);
 
 }  // namespace cffc_b200

@@ -339,8 +339,15 @@ int explicit_step_threaded(TimedSet& T) {
 }  // namespace
 
 int main(int argc, char** argv) {
+  if (argc == 3 && !strcmp(argv[1], "solve")) {
+    // the reference's own deck-driven solver, as its command line runs it
+    // (Euler2DQuadSolver, Euler2DQuadSolvers.cc:26), in batch mode, after
+    // the process set-up of its main (one processor, Euler2D.cc)
+    CFFC_Initialize_MPI(argc, argv);
+    return Euler2DQuadSolver(argv[2], 1);
+  }
   if (argc < 4) {
-    fprintf(stderr, "usage: %s residual|explicit|nks|time CASE ...\n", argv[0]);
+    fprintf(stderr, "usage: %s residual|explicit|nks|time CASE ... | solve DECK\n", argv[0]);
     return 2;
   }
   Case c;
@@ -420,6 +427,82 @@ int main(int argc, char** argv) {
     for (int b = 0; b < c.nblk; ++b) dump_c(f, R.Soln[R.order[b]], -1);
     fclose(f);
     return err ? 1 : 0;
+  }
+
+  if (!strcmp(mode, "restart_write")) {
+    // Write_Restart_Solution + Write_QuadTree (Euler2DQuadMultiBlock.cc:218,
+    // AMR/AMR.h:296) of the case's block set, PREFIX_blkNNNNNN.soln and
+    // PREFIX_quadtree.tree, with time step count NSTEPS and time TIME.
+    if (argc < 6) { fprintf(stderr, "restart_write CASE PREFIX NSTEPS TIME\n"); return 2; }
+    RefSet R;
+    build_reference_blocks(c, R);
+    snprintf(R.IP.Restart_File_Name, sizeof(R.IP.Restart_File_Name), "%s.soln", argv[3]);
+    CPUTime cpu;
+    cpu.cput = 1.5;
+    int err = Write_Restart_Solution(R.Soln, R.Local, R.IP, atoi(argv[4]), atof(argv[5]), cpu);
+    err = err || Write_QuadTree(R.QuadTree, R.IP);
+    return err ? 1 : 0;
+  }
+
+  if (!strcmp(mode, "restart_read")) {
+    // Read_QuadTree + Read_Restart_Solution (AMR/AMR.h:169,
+    // Euler2DQuadMultiBlock.cc:145) of PREFIX; the case file gives the grid
+    // type (periodic wiring) and the block count.  OUT: int32 nsteps, int32
+    // nblk, f64 time, f64 cpu time, then per root block (j outer, i inner):
+    // int32 gblknum, nW, nE, nS, nN and the local numbers of the first
+    // neighbour on each side (-1: none), int32 BCtypeW/E/S/N, f64 nodes X, Y,
+    // f64 WoW/E/S/N [4][n], f64 U [4][NCj][NCi].
+    if (argc < 5) { fprintf(stderr, "restart_read CASE PREFIX OUT\n"); return 2; }
+    Euler2D_Input_Parameters IP;
+    set_input(c, IP);
+    snprintf(IP.Restart_File_Name, sizeof(IP.Restart_File_Name), "%s.soln", argv[3]);
+    QuadTreeBlock_DataStructure QT;
+    AdaptiveBlockResourceList Global;
+    AdaptiveBlock2D_List Local;
+    Euler2D_Quad_Block* Soln = new Euler2D_Quad_Block[c.nblk];
+    int nsteps = 0;
+    double time = 0.0;
+    CPUTime cpu;
+    if (Read_QuadTree(QT, Global, Local, IP)) { fprintf(stderr, "Read_QuadTree failed\n"); return 1; }
+    if (Read_Restart_Solution(Soln, Local, IP, nsteps, time, cpu)) { fprintf(stderr, "Read_Restart_Solution failed\n"); return 1; }
+    FILE* f = fopen(argv[4], "wb");
+    int hdr[2] = {nsteps, c.nblk};
+    wr(f, hdr, 2);
+    wr(f, &time, 1);
+    wr(f, &cpu.cput, 1);
+    for (int bj = 0; bj < QT.NRj; ++bj)
+      for (int bi = 0; bi < QT.NRi; ++bi) {
+        const int n = QT.Roots[bi][bj].block.info.blknum;
+        const AdaptiveBlock2D& A = Local.Block[n];
+        Euler2D_Quad_Block& B = Soln[n];
+        int nb[9] = {A.gblknum, A.nW, A.nE, A.nS, A.nN,
+                     A.nW ? A.infoW[0].blknum : -1, A.nE ? A.infoE[0].blknum : -1,
+                     A.nS ? A.infoS[0].blknum : -1, A.nN ? A.infoN[0].blknum : -1};
+        wr(f, nb, 9);
+        std::vector<int> bc;
+        for (int j = 0; j < B.NCj; ++j) bc.push_back(B.Grid.BCtypeW[j]);
+        for (int j = 0; j < B.NCj; ++j) bc.push_back(B.Grid.BCtypeE[j]);
+        for (int i = 0; i < B.NCi; ++i) bc.push_back(B.Grid.BCtypeS[i]);
+        for (int i = 0; i < B.NCi; ++i) bc.push_back(B.Grid.BCtypeN[i]);
+        wr(f, &bc[0], bc.size());
+        std::vector<double> xy;
+        for (int j = 0; j < B.NCj + 1; ++j)
+          for (int i = 0; i < B.NCi + 1; ++i) xy.push_back(B.Grid.Node[i][j].X.x);
+        for (int j = 0; j < B.NCj + 1; ++j)
+          for (int i = 0; i < B.NCi + 1; ++i) xy.push_back(B.Grid.Node[i][j].X.y);
+        wr(f, &xy[0], xy.size());
+        Euler2D_pState* Wo[4] = {B.WoW, B.WoE, B.WoS, B.WoN};
+        const int L[4] = {B.NCj, B.NCj, B.NCi, B.NCi};
+        for (int e = 0; e < 4; ++e) {
+          std::vector<double> w(4 * L[e]);
+          for (int k = 0; k < L[e]; ++k)
+            for (int v = 0; v < 4; ++v) w[v * L[e] + k] = Wo[e][k][v + 1];
+          wr(f, &w[0], w.size());
+        }
+        dump_c(f, B, -1);
+      }
+    fclose(f);
+    return 0;
   }
 
   if (!strcmp(mode, "time")) {

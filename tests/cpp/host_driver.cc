@@ -11,6 +11,7 @@
 //
 // Prints one line "ok <n ignored keywords> <Wo.d> <Wo.u> <Wo.p>" on success.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -32,12 +33,117 @@ static void write_R(FILE* f, const Euler2D_Quad_Block& B) {
       for (int i = 0; i < B.NCi; ++i) fwrite(&B.dUdt[i][j][v], sizeof(double), 1, f);
 }
 
+// The block set of a case file (the layout cffc_b200.cases.write_case writes),
+// with U = U(W) as the reference's harness sets it.
+static bool read_case(const char* path, std::vector<Euler2D_Quad_Block>& blocks, std::vector<int>& neighbour,
+                      Euler2D_Input_Parameters& IP) {
+  FILE* f = fopen(path, "rb");
+  if (!f) return false;
+  int hdr[2], dims[4], opts[8];
+  double dopts[4];
+  bool ok = fread(hdr, 4, 2, f) == 2 && fread(dims, 4, 4, f) == 4 && fread(opts, 4, 8, f) == 8 &&
+            fread(dopts, 8, 4, f) == 4;
+  const int nblk = dims[0], nci = dims[1], ncj = dims[2], ng = dims[3];
+  const int NCi = nci + 2 * ng, NCj = ncj + 2 * ng, NNi = NCi + 1, NNj = NCj + 1;
+  IP.Number_of_Blocks_Idir = opts[5];
+  IP.Number_of_Blocks_Jdir = opts[6];
+  blocks.assign(nblk, Euler2D_Quad_Block());
+  neighbour.assign(size_t(8) * nblk, -1);
+  auto rd = [&](void* p, size_t sz, size_t n) { ok = ok && fread(p, sz, n, f) == n; };
+  for (int b = 0; ok && b < nblk; ++b) {
+    Euler2D_Quad_Block& B = blocks[b];
+    B.allocate(nci, ncj, ng);
+    rd(&neighbour[8 * b], 4, 8);
+    std::vector<int> bc(2 * NCj + 2 * NCi);
+    rd(bc.data(), 4, bc.size());
+    for (int j = 0; j < NCj; ++j) { B.Grid.BCtypeW[j] = bc[j]; B.Grid.BCtypeE[j] = bc[NCj + j]; }
+    for (int i = 0; i < NCi; ++i) { B.Grid.BCtypeS[i] = bc[2 * NCj + i]; B.Grid.BCtypeN[i] = bc[2 * NCj + NCi + i]; }
+    std::vector<double> xy(2 * NNi * NNj);
+    rd(xy.data(), 8, xy.size());
+    for (int j = 0; j < NNj; ++j)
+      for (int i = 0; i < NNi; ++i) B.Grid.Node[i][j] = Vector2D(xy[j * NNi + i], xy[NNi * NNj + j * NNi + i]);
+    std::vector<Euler2D_pState>* wo[4] = {&B.WoW, &B.WoE, &B.WoS, &B.WoN};
+    const int L[4] = {NCj, NCj, NCi, NCi};
+    for (int e = 0; e < 4; ++e) {
+      std::vector<double> w(4 * L[e]);
+      rd(w.data(), 8, w.size());
+      for (int k = 0; k < L[e]; ++k) (*wo[e])[k] = Euler2D_pState(w[k], w[L[e] + k], w[2 * L[e] + k], w[3 * L[e] + k]);
+    }
+    std::vector<double> W(4 * NCi * NCj);
+    rd(W.data(), 8, W.size());
+    const int s = NCi * NCj;
+    for (int j = 0; j < NCj; ++j)
+      for (int i = 0; i < NCi; ++i) {
+        const int q = j * NCi + i;
+        B.W[i][j] = Euler2D_pState(W[q], W[s + q], W[2 * s + q], W[3 * s + q]);
+        B.U[i][j] = B.W[i][j].U();
+      }
+  }
+  fclose(f);
+  return ok;
+}
+
+// The restart test modes (no deck):
+//   host_driver restart_write CASE PREFIX NSTEPS TIME   Write_QuadTree + Write_Restart_Solution
+//   host_driver restart_read PREFIX OUT                 Read_QuadTree + Read_Restart_Solution; OUT in
+//                                                       the layout of the reference harness's
+//                                                       restart_read
+static int restart_modes(int argc, char** argv) {
+  const std::string mode = argv[1];
+  Euler2D_Input_Parameters IP;
+  std::vector<Euler2D_Quad_Block> blocks;
+  std::vector<int> neighbour;
+  if (mode == "restart_write") {
+    if (argc < 6 || !read_case(argv[2], blocks, neighbour, IP)) return 2;
+    IP.Restart_File_Name = std::string(argv[3]) + ".soln";
+    if (Write_QuadTree(blocks, neighbour, IP) || Write_Restart_Solution(blocks, IP, atoi(argv[4]), atof(argv[5]), 1.5))
+      return 5;
+    printf("ok\n");
+    return 0;
+  }
+  IP.Restart_File_Name = std::string(argv[2]) + ".soln";
+  int nsteps = 0;
+  double time = 0.0, cpu = 0.0;
+  if (Read_QuadTree(blocks, neighbour, IP) || Read_Restart_Solution(blocks, IP, nsteps, time, cpu)) return 5;
+  FILE* f = fopen(argv[3], "wb");
+  if (!f) return 10;
+  const int hdr[2] = {nsteps, static_cast<int>(blocks.size())};
+  fwrite(hdr, 4, 2, f);
+  fwrite(&time, 8, 1, f);
+  fwrite(&cpu, 8, 1, f);
+  for (size_t b = 0; b < blocks.size(); ++b) {
+    const Euler2D_Quad_Block& B = blocks[b];
+    const int* nb = &neighbour[8 * b];
+    const int rec[9] = {static_cast<int>(b), nb[0] >= 0, nb[1] >= 0, nb[2] >= 0, nb[3] >= 0, nb[0], nb[1], nb[2], nb[3]};
+    fwrite(rec, 4, 9, f);
+    for (int j = 0; j < B.NCj; ++j) fwrite(&B.Grid.BCtypeW[j], 4, 1, f);
+    for (int j = 0; j < B.NCj; ++j) fwrite(&B.Grid.BCtypeE[j], 4, 1, f);
+    for (int i = 0; i < B.NCi; ++i) fwrite(&B.Grid.BCtypeS[i], 4, 1, f);
+    for (int i = 0; i < B.NCi; ++i) fwrite(&B.Grid.BCtypeN[i], 4, 1, f);
+    for (int j = 0; j < B.Grid.NNj; ++j)
+      for (int i = 0; i < B.Grid.NNi; ++i) fwrite(&B.Grid.Node[i][j].x, 8, 1, f);
+    for (int j = 0; j < B.Grid.NNj; ++j)
+      for (int i = 0; i < B.Grid.NNi; ++i) fwrite(&B.Grid.Node[i][j].y, 8, 1, f);
+    const std::vector<Euler2D_pState>* wo[4] = {&B.WoW, &B.WoE, &B.WoS, &B.WoN};
+    for (int e = 0; e < 4; ++e)
+      for (int v = 1; v <= 4; ++v)
+        for (const Euler2D_pState& w : *wo[e]) fwrite(&w[v], 8, 1, f);
+    for (int v = 1; v <= 4; ++v)
+      for (int j = 0; j < B.NCj; ++j)
+        for (int i = 0; i < B.NCi; ++i) fwrite(&B.U[i][j][v], 8, 1, f);
+  }
+  fclose(f);
+  printf("ok %d\n", nsteps);
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc < 4) {
     fprintf(stderr, "usage: host_driver parse|run|residual1 DECK OUT [STATE_OUT]\n");
     return 2;
   }
   const std::string mode = argv[1];
+  if (mode == "restart_write" || mode == "restart_read") return restart_modes(argc, argv);
   Euler2D_Input_Parameters IP;
   const int line = IP.Process_Input_Control_Parameter_File(argv[2]);
   if (line) {

@@ -160,10 +160,104 @@ def with_flux(bs, flux):
     return dataclasses.replace(bs, scheme=dataclasses.replace(bs.scheme, flux=flux))
 
 
+# Decks of the restart fixture, run by the reference's own solver
+# (Euler2DQuadSolver).  A: the reference's Bump_Channel_Flow grid (4 x 2
+# blocks of 8 x 4 cells, circular-arc bump spline), 20 predictor-corrector
+# steps from the Mach 1.4 freestream, restart files written at the end.
+# B: a restart from A's files for 10 more steps.
+RESTART_DECK = """# supersonic bump channel, explicit predictor-corrector
+Time_Integration_Type =
+Explicit_Predictor_Corrector
+Time_Accurate =
+0
+Local_Time_Stepping =
+1
+CFL_Number =
+0.5
+Maximum_Number_of_Time_Steps =
+{steps}
+Reconstruction_Type =
+Least_Squares
+Limiter_Type =
+Venkatakrishnan
+Flux_Function_Type =
+Roe
+ICs_Type =
+{ics}
+Mach_Number =
+1.40
+Grid_Type =
+Bump_Channel_Flow
+Smooth_Bump =
+OFF
+Number_of_Cells_Idir =
+8
+Number_of_Cells_Jdir =
+4
+Number_of_Blocks_Per_Processor =
+8
+Restart_File_Name =
+bump
+Output_File_Name =
+bump
+{extra}Execute
+Write_Restart
+Terminate
+"""
+
+
+def restart_deck(restart, extra=""):
+    return RESTART_DECK.format(steps=10 if restart else 20, ics="Restart" if restart else "Uniform", extra=extra)
+
+
+def make_restart_fixture():
+    """tests/golden/restart.tar.gz: restart files the reference wrote and what
+    its own reader (Read_QuadTree + Read_Restart_Solution) makes of them
+    (read.bin, layout of the harness's restart_read):
+      chan/   Write_Restart_Solution of the channel case with characteristic
+              inflow/outflow (17 steps, time 0.25)
+      bump0/  deck A's restart files (boundary splines in the grid)
+      bump1/  deck B's, a restart from bump0 continued for 10 steps
+    and the two decks."""
+    import shutil
+    import tarfile
+    ch_char = cases.channel(bc=dict(W=cases.BC_CHARACTERISTIC, E=cases.BC_CHARACTERISTIC,
+                                    S=cases.BC_REFLECTION, N=cases.BC_CONSTANT_EXTRAPOLATION), seed=8)
+    with tempfile.TemporaryDirectory() as td:
+        root = os.path.join(td, "restart")
+        for d in ("chan", "bump0", "bump1"):
+            os.makedirs(os.path.join(root, d))
+        chan = os.path.join(root, "chan")
+        cp = os.path.join(td, "chan.case")
+        cases.write_case(cp, ch_char)
+        subprocess.run([HARNESS, "restart_write", cp, "chan", "17", "0.25"], cwd=chan, check=True)
+        subprocess.run([HARNESS, "restart_read", cp, "chan", "read.bin"], cwd=chan, check=True)
+        for name, restart in (("deck_a.in", False), ("deck_b.in", True)):
+            with open(os.path.join(root, name), "w") as f:
+                f.write(restart_deck(restart))
+        dummy = os.path.join(td, "bump.case")  # block count and wiring for restart_read
+        cases.write_case(dummy, cases.channel(nbi=4, nbj=2))
+        run = os.path.join(td, "run")
+        os.makedirs(run)
+        for stage, deck in (("bump0", "deck_a.in"), ("bump1", "deck_b.in")):
+            subprocess.run([HARNESS, "solve", os.path.join(root, deck)], cwd=run, check=True,
+                           capture_output=True)
+            dst = os.path.join(root, stage)
+            for fn in sorted(os.listdir(run)):
+                if fn.startswith("bump_blk") or fn == "bump_quadtree.tree":
+                    shutil.copy(os.path.join(run, fn), dst)
+            subprocess.run([HARNESS, "restart_read", dummy, "bump", "read.bin"], cwd=dst, check=True)
+        with tarfile.open(os.path.join(OUT, "restart.tar.gz"), "w:gz") as t:
+            t.add(root, arcname="restart")
+    print("restart.tar.gz")
+
+
 def main():
     if not os.path.exists(HARNESS):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "reference"], check=True)
     only = set(sys.argv[1:])
+    if not only or "restart" in only:
+        make_restart_fixture()
     for name, bs, kind, steps in golden_cases():
         if only and name not in only:
             continue

@@ -64,17 +64,6 @@ Execute
 """
 
 
-@pytest.fixture(scope="session")
-def driver(tmp_path_factory):
-    capi.load_library()  # the library must exist (built by __graft_entry__.build)
-    exe = str(tmp_path_factory.mktemp("host") / "host_driver")
-    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"),
-           os.path.join(ROOT, "tests", "cpp", "host_driver.cc"), "-o", exe, "-L", LIBDIR, "-lcffc_e2d",
-           "-Wl,-rpath," + LIBDIR]
-    subprocess.run(cmd, check=True)
-    return exe
-
-
 def write_deck(path, steps=10, precision="FP64_Exact", text=DECK):
     with open(path, "w") as f:
         f.write(text.format(steps=steps, precision=precision))
