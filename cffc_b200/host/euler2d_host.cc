@@ -30,7 +30,7 @@ constexpr int INVALID_INPUT_CODE = -1, EXECUTE_CODE = 1, TERMINATE_CODE = 2;
 double Euler2D_pState::g = 1.4;
 double Euler2D_pState::gm1 = 1.4 - 1.0;
 double Euler2D_pState::gm1i = 1.0 / (1.4 - 1.0);
-double Euler2D_pState::R = 287.0636;
+double Euler2D_pState::R = 8.314511 / (28.9640 * 0.001);  // R_UNIVERSAL / (MOLE_WT_AIR * MILLI)
 
 double Euler2D_pState::a() const { return std::sqrt(g * p / d); }
 double Euler2D_pState::h() const { return g * p / (gm1 * d) + HALF * (v.x * v.x + v.y * v.y); }
@@ -95,15 +95,28 @@ Euler2D_Input_Parameters::Euler2D_Input_Parameters() {
   NKS.gmres_tol_final = 1e-5;
   NKS.epsilon0 = 1e-6;
   NKS.min_ratio = 1e-10;
-  set_freestream();
+  // freestream defaults (Set_Default_Input_Parameters, Euler2DInput.cc:304-313):
+  // the standard atmosphere, its temperature, Mach 0.8 along x
+  Wo = Euler2D_pState(1.225, 0.0, 0.0, 101325.00);
+  Pressure = Wo.p;
+  Temperature = Wo.p / (Wo.d * Euler2D_pState::R);
+  Mach_Number = 0.80;
+  Flow_Angle = 0.0;
+  set_velocity();
 }
 
-// Wo from Pressure, Temperature, Mach_Number and Flow_Angle (the updates of
-// Euler2DInput.cc:2558-2611).
-void Euler2D_Input_Parameters::set_freestream() {
-  Wo = Euler2D_pState(Pressure / (Euler2D_pState::R * Temperature), 0.0, 0.0, Pressure);
+// Wo.v from Mach_Number and Flow_Angle at the current sound speed (the update
+// every freestream keyword makes, Euler2DInput.cc:2558-2611).
+void Euler2D_Input_Parameters::set_velocity() {
   Wo.v.x = Mach_Number * Wo.a() * std::cos(2.0 * PI * Flow_Angle / 360.00);
   Wo.v.y = Mach_Number * Wo.a() * std::sin(2.0 * PI * Flow_Angle / 360.00);
+}
+
+// Wo = (Pressure / (R Temperature), 0, 0, Pressure), then its velocity (the
+// Pressure and Temperature keywords).
+void Euler2D_Input_Parameters::set_freestream() {
+  Wo = Euler2D_pState(Pressure / (Euler2D_pState::R * Temperature), 0.0, 0.0, Pressure);
+  set_velocity();
 }
 
 namespace {
@@ -195,7 +208,21 @@ int Parse_Next_Input_Control_Parameter(Euler2D_Input_Parameters& IP, std::istrea
     // Sine_Squared_Bump_Channel and rejects the rest
     return str(IP.Grid_Type);
   }
-  if (code == "Output_File_Name") return str(IP.Output_File_Name);
+  if (code == "Output_File_Name") {  // Euler2DInput.cc:2157-2174: names every output file
+    std::string v;
+    if (str(v)) return INVALID_INPUT_CODE;
+    IP.Output_File_Name = v + ".dat";
+    IP.Grid_File_Name = v + ".grid";
+    IP.Grid_Definition_File_Name = v + ".griddef";
+    IP.Restart_File_Name = v + ".soln";
+    return 0;
+  }
+  if (code == "Grid_File_Name") {  // Euler2DInput.cc:2176-2184
+    if (str(IP.Grid_File_Name)) return INVALID_INPUT_CODE;
+    IP.Grid_Definition_File_Name = IP.Grid_File_Name + ".griddef";
+    IP.Grid_File_Name += ".grid";
+    return 0;
+  }
   if (code == "Restart_File_Name") {  // Euler2DInput.cc:2186-2191
     if (str(IP.Restart_File_Name)) return INVALID_INPUT_CODE;
     IP.Restart_File_Name += ".soln";
@@ -246,12 +273,12 @@ int Parse_Next_Input_Control_Parameter(Euler2D_Input_Parameters& IP, std::istrea
   }
   if (code == "Mach_Number") {
     int rc = num_d(IP.Mach_Number, false);
-    IP.set_freestream();
+    if (!rc) IP.set_velocity();
     return rc;
   }
   if (code == "Flow_Angle") {
     int rc = num_d(IP.Flow_Angle, false);
-    IP.set_freestream();
+    if (!rc) IP.set_velocity();
     return rc;
   }
   if (code == "Pressure") {
@@ -306,7 +333,6 @@ int Euler2D_Input_Parameters::Process_Input_Control_Parameter_File(const std::st
     }
     if (rc == INVALID_INPUT_CODE) return Line_Number > 0 ? Line_Number : 1;
   }
-  set_freestream();
   return 0;
 }
 
@@ -315,6 +341,19 @@ int Create_Initial_Solution_Blocks(const Euler2D_Input_Parameters& IP, std::vect
                                    std::vector<int>& neighbour) {
   const int nbi = IP.Number_of_Blocks_Idir, nbj = IP.Number_of_Blocks_Jdir, ng = IP.Number_of_Ghost_Cells;
   const std::string& t = IP.Grid_Type;
+  if (t == "Read_From_Data_File") {  // the reference's grid data file (Grid_File_Name)
+    if (Read_Multi_Block_Grid(IP.Grid_File_Name, blocks, neighbour)) return 1;
+    for (Euler2D_Quad_Block& B : blocks) {
+      for (auto* wo : {&B.WoN, &B.WoS, &B.WoE, &B.WoW})
+        for (auto& w : *wo) w = IP.Wo;
+      for (int i = 0; i < B.NCi; ++i)
+        for (int j = 0; j < B.NCj; ++j) {
+          B.W[i][j] = IP.Wo;
+          B.U[i][j] = IP.Wo.U();
+        }
+    }
+    return 0;
+  }
   if (t != "Rectangular_Box" && t != "Periodic_Box" && t != "Sine_Squared_Bump_Channel") return 1;
   if (IP.Number_of_Cells_Idir % nbi || IP.Number_of_Cells_Jdir % nbj) return 1;
   const int nci = IP.Number_of_Cells_Idir / nbi, ncj = IP.Number_of_Cells_Jdir / nbj;
@@ -666,11 +705,10 @@ void put_state(std::ostream& o, double a, double b, double c, double d) {
   o.unsetf(std::ios::scientific);
 }
 
-// One block in the layout of operator<<(ostream&, Euler2D_Quad_Block)
-// (Euler2DQuad.h:1306-1336) around operator<<(ostream&, Grid2D_Quad_Block_HO)
-// (Grid/HO_Grid2DQuad.cc:13763-13990) of a first-order geometry without
-// boundary splines or stretching.
-void put_block(std::ostream& o, const Euler2D_Quad_Block& B) {
+// operator<<(ostream&, Grid2D_Quad_Block_HO) (Grid/HO_Grid2DQuad.cc:
+// 13763-13990) of a first-order geometry without boundary splines or
+// stretching; it leaves the stream at precision 15.
+void put_grid(std::ostream& o, const Euler2D_Quad_Block& B) {
   const Grid2D_Quad_Block& G = B.Grid;
   const int ng = B.Nghost, NCi = B.NCi, NCj = B.NCj;
   o << G.NNi << " " << ng << " " << G.NNi - ng - 1 << "\n";
@@ -718,6 +756,13 @@ void put_block(std::ostream& o, const Euler2D_Quad_Block& B) {
   o << 0 << " " << 1.0 << " " << 1.0 << "\n";
   o.unsetf(std::ios::scientific);
   o << 1 << " " << 1 << " " << 1 << " " << 1 << "\n";
+}
+
+// One block in the layout of operator<<(ostream&, Euler2D_Quad_Block)
+// (Euler2DQuad.h:1306-1336).
+void put_block(std::ostream& o, const Euler2D_Quad_Block& B) {
+  const int ng = B.Nghost, NCi = B.NCi, NCj = B.NCj;
+  put_grid(o, B);
   o << NCi << " " << B.ICl << " " << B.ICu << " " << ng << "\n";
   o << NCj << " " << B.JCl << " " << B.JCu << "\n";
   o << 0 << "\n";  // Axisymmetric
@@ -768,8 +813,10 @@ bool skip_spline(std::istream& in) {
   return true;
 }
 
-// operator>>(istream&, Euler2D_Quad_Block) (Euler2DQuad.h:1338-1400).
-bool get_block(std::istream& in, Euler2D_Quad_Block& B) {
+// operator>>(istream&, Grid2D_Quad_Block_HO) (Grid/HO_Grid2DQuad.cc:
+// 14006-14200): nodes and BC codes kept, cell data and splines dropped;
+// allocates the block.
+bool get_grid(std::istream& in, Euler2D_Quad_Block& B) {
   int nni, inl, inu, nnj, jnl, jnu, ng, rec, bflag, nci, icl, icu, ncj, jcl, jcu;
   if (!(in >> nni >> inl >> inu >> nnj >> jnl >> jnu >> ng >> rec >> bflag)) return false;
   if (nni == 0 || nnj == 0) return false;
@@ -792,7 +839,13 @@ bool get_block(std::istream& in, Euler2D_Quad_Block& B) {
     if (!(in >> G.BCtypeE[j] >> G.BCtypeW[j])) return false;
   for (int k = 0; k < 12; ++k)
     if (!skip_spline(in)) return false;
-  if (!skip(in, 8 + 6 + 4)) return false;  // Smin/Smax, stretching, orthogonality flags
+  return skip(in, 8 + 6 + 4);  // Smin/Smax, stretching, orthogonality flags
+}
+
+// operator>>(istream&, Euler2D_Quad_Block) (Euler2DQuad.h:1338-1400).
+bool get_block(std::istream& in, Euler2D_Quad_Block& B) {
+  if (!get_grid(in, B)) return false;
+  const int nci = B.NCi, ncj = B.NCj, ng = B.Nghost;
   int ni, il, iu, g2, nj, jl, ju, axi;
   if (!(in >> ni >> il >> iu >> g2 >> nj >> jl >> ju >> axi)) return false;
   if (ni != nci || nj != ncj || g2 != ng) return false;
@@ -853,11 +906,83 @@ void put_info(std::ostream& o, int blknum, const Euler2D_Quad_Block& B) {
 
 }  // namespace
 
+namespace {
+// The nbi x nbj root layout of a block set numbered b = j * nbi + i: the
+// deck's, or (for a grid read from a file) the run of east neighbours from
+// block 0.
+bool root_layout(const std::vector<int>& neighbour, int nblk, const Euler2D_Input_Parameters& IP, int& nbi,
+                 int& nbj) {
+  nbi = IP.Number_of_Blocks_Idir;
+  nbj = IP.Number_of_Blocks_Jdir;
+  if (nbi * nbj == nblk) return true;
+  if (neighbour.size() != size_t(8) * nblk) return false;
+  nbi = 1;
+  for (int b = 0; neighbour[8 * b + 1] > b; b = neighbour[8 * b + 1]) ++nbi;
+  nbj = nblk / nbi;
+  return nbi * nbj == nblk;
+}
+
+// i_Grid codes of the grid names this library builds or reads (CFD/CFD.h:800-860).
+int grid_code(const std::string& t) {
+  if (t == "Rectangular_Box") return 2;
+  if (t == "Bump_Channel_Flow") return 16;
+  if (t == "Periodic_Box") return 55;
+  return 10001;  // GRID_READ_FROM_GRID_DATA_FILE
+}
+}  // namespace
+
+int Write_Multi_Block_Grid(const std::string& path, const std::vector<Euler2D_Quad_Block>& blocks,
+                           const Euler2D_Input_Parameters& IP) {
+  const int nbi = IP.Number_of_Blocks_Idir, nbj = IP.Number_of_Blocks_Jdir;
+  if (blocks.empty() || size_t(nbi) * nbj != blocks.size()) return 1;
+  std::ofstream o(path);
+  if (!o.good()) return 1;
+  o << IP.Grid_Type << "\n" << grid_code(IP.Grid_Type) << "\n";
+  o << nbi << " " << nbj << "\n";
+  for (const Euler2D_Quad_Block& B : blocks) {
+    o.precision(14);  // Grid2D_Quad_Block_HO::Write_Quad_Block
+    put_grid(o, B);
+    o.precision(6);
+  }
+  return o.good() ? 0 : 1;
+}
+
+int Read_Multi_Block_Grid(const std::string& path, std::vector<Euler2D_Quad_Block>& blocks,
+                          std::vector<int>& neighbour, std::string* grid_type, int* nbi_out, int* nbj_out) {
+  std::ifstream in(path);
+  if (!in.good()) return 1;
+  std::string type;
+  int code, nbi, nbj;
+  std::getline(in, type);
+  if (!(in >> code >> nbi >> nbj) || nbi < 1 || nbj < 1) return 1;
+  if (grid_type) *grid_type = type;
+  if (nbi_out) *nbi_out = nbi;
+  if (nbj_out) *nbj_out = nbj;
+  blocks.assign(size_t(nbi) * nbj, Euler2D_Quad_Block());
+  for (Euler2D_Quad_Block& B : blocks)
+    if (!get_grid(in, B)) return 1;
+  for (const Euler2D_Quad_Block& B : blocks)
+    if (B.NCi != blocks[0].NCi || B.NCj != blocks[0].NCj) return 1;
+  // root blocks of the layout (Find_Neighbours_of_Root_Solution_Blocks,
+  // AMR/QuadTree.cc:363, with the periodic-box wiring of GRID_PERIODIC_BOX)
+  const bool periodic = code == 55;
+  static const int off[8][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}, {-1, -1}, {1, -1}, {-1, 1}, {1, 1}};
+  neighbour.assign(size_t(8) * nbi * nbj, -1);
+  for (int bj = 0; bj < nbj; ++bj)
+    for (int bi = 0; bi < nbi; ++bi)
+      for (int k = 0; k < 8; ++k) {
+        int ni = bi + off[k][0], nj = bj + off[k][1];
+        if (periodic) { ni = (ni + nbi) % nbi; nj = (nj + nbj) % nbj; }
+        if (ni >= 0 && ni < nbi && nj >= 0 && nj < nbj) neighbour[8 * (bj * nbi + bi) + k] = nj * nbi + ni;
+      }
+  return 0;
+}
+
 int Write_QuadTree(const std::vector<Euler2D_Quad_Block>& blocks, const std::vector<int>& neighbour,
                    const Euler2D_Input_Parameters& IP) {
-  const int nbi = IP.Number_of_Blocks_Idir, nbj = IP.Number_of_Blocks_Jdir;
   const int nblk = static_cast<int>(blocks.size());
-  if (nbi * nbj != nblk || neighbour.size() != size_t(8) * nblk) return 1;
+  int nbi, nbj;
+  if (!root_layout(neighbour, nblk, IP, nbi, nbj)) return 1;
   std::ofstream o(tree_file(IP));
   if (!o.good()) return 1;
   o << nbi << " " << nbj << " " << 1 << " "

@@ -36,7 +36,8 @@ struct Vector2D {
 
 class Euler2D_cState;
 
-// Primitive state (rho, u, v, p); gamma = 1.4, R = 287.0636 J/(kg K)
+// Primitive state (rho, u, v, p); gamma = 1.4, R = R_universal / M_air
+// = 8.314511 / 0.028964 J/(kg K)
 // (Euler2DState.h:972-977).  operator[] is 1-based as in the reference.
 class Euler2D_pState {
  public:
@@ -121,6 +122,8 @@ struct Euler2D_Input_Parameters {
   Euler2D_pState Wo;               // freestream (from Pressure, Temperature, Mach, angle)
   std::string Output_File_Name = "outputfile.dat";
   std::string Restart_File_Name = "restartfile.soln";  // the keyword's value + ".soln"
+  std::string Grid_File_Name = "gridfile.grid";        // Grid_File_Name keyword + ".grid"
+  std::string Grid_Definition_File_Name = "gridfile.griddef";
   std::string Gas_Type = "AIR";
   int Restart_Solution_Save_Frequency = 1000;
   std::vector<std::string> Commands;  // commands after Execute (Write_Restart, Write_Output, ...)
@@ -129,7 +132,8 @@ struct Euler2D_Input_Parameters {
   std::vector<std::string> Ignored; // keywords of the reference outside this path
   int Line_Number = 0;
   Euler2D_Input_Parameters();
-  void set_freestream();
+  void set_freestream();  // Wo from Pressure and Temperature, then set_velocity()
+  void set_velocity();    // Wo.v from Mach_Number and Flow_Angle at Wo's sound speed
   // Reads a whole deck up to Execute / Terminate; returns 0 or the
   // (positive) line number of the first invalid entry.
   int Process_Input_Control_Parameter_File(const std::string& path);
@@ -183,6 +187,21 @@ double CFL(Euler2D_Quad_Block& SolnBlk, const Euler2D_Input_Parameters& IP);
 double L1_Norm_Residual(const Euler2D_Quad_Block& SolnBlk);
 double L2_Norm_Residual(const Euler2D_Quad_Block& SolnBlk);
 double Max_Norm_Residual(const Euler2D_Quad_Block& SolnBlk);
+
+// ---- grid data files ------------------------------------------------------
+// The reference's multi-block grid data file (Write_Multi_Block_Grid_Using_IP /
+// Read_Multi_Block_Grid_Using_IP, Grid/HO_Grid2DQuadMultiBlock.h:3160-3210):
+// the Grid_Type line, its i_Grid code, "nbi nbj", then every block's grid
+// (j outer, i inner) as the restart files hold it.  Reading keeps nodes and
+// BC codes (cell data and boundary splines are dropped) and wires the
+// nbi x nbj root blocks as the reference does (periodic for Periodic_Box).
+// Grid_Type Read_From_Data_File builds the initial blocks from
+// Grid_File_Name.  Return 0, or 1 when the file cannot be opened or parsed.
+int Write_Multi_Block_Grid(const std::string& path, const std::vector<Euler2D_Quad_Block>& blocks,
+                           const Euler2D_Input_Parameters& IP);
+int Read_Multi_Block_Grid(const std::string& path, std::vector<Euler2D_Quad_Block>& blocks,
+                          std::vector<int>& neighbour, std::string* grid_type = nullptr, int* nbi = nullptr,
+                          int* nbj = nullptr);
 
 // ---- restart files -------------------------------------------------------
 // The reference's checkpoint format: PREFIX_quadtree.tree (the block tree,

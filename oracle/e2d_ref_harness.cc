@@ -444,6 +444,24 @@ int main(int argc, char** argv) {
     return err ? 1 : 0;
   }
 
+  if (!strcmp(mode, "grid_write")) {
+    // the grid data file of the case's blocks in the layout of
+    // Write_Multi_Block_Grid_Using_IP (Grid/HO_Grid2DQuadMultiBlock.h:3160):
+    // grid type line, i_Grid, "nbi nbj", Write_Quad_Block of every block
+    std::ofstream out(argv[3]);
+    out << (c.periodic ? "Periodic_Box" : "Rectangular_Box") << "\n"
+        << (c.periodic ? GRID_PERIODIC_BOX : GRID_RECTANGULAR_BOX) << "\n";
+    out << c.nbi << " " << c.nbj << "\n";
+    for (int bj = 0; bj < c.nbj; ++bj)
+      for (int bi = 0; bi < c.nbi; ++bi) {
+        Grid2D_Quad_Block_HO G;
+        G.allocate(c.nci, c.ncj, c.ng);
+        set_grid(c, c.data[bj * c.nbi + bi], G);
+        G.Write_Quad_Block(out);
+      }
+    return out.good() ? 0 : 1;
+  }
+
   if (!strcmp(mode, "restart_read")) {
     // Read_QuadTree + Read_Restart_Solution (AMR/AMR.h:169,
     // Euler2DQuadMultiBlock.cc:145) of PREFIX; the case file gives the grid
@@ -465,6 +483,14 @@ int main(int argc, char** argv) {
     CPUTime cpu;
     if (Read_QuadTree(QT, Global, Local, IP)) { fprintf(stderr, "Read_QuadTree failed\n"); return 1; }
     if (Read_Restart_Solution(Soln, Local, IP, nsteps, time, cpu)) { fprintf(stderr, "Read_Restart_Solution failed\n"); return 1; }
+    if (argc > 5) {
+      // restart_read CASE PREFIX OUT GRIDFILE: also the blocks' grids as a
+      // grid data file of type Bump_Channel_Flow (Write_Quad_Block per root)
+      std::ofstream g(argv[5]);
+      g << "Bump_Channel_Flow\n" << GRID_BUMP_CHANNEL_FLOW << "\n" << QT.NRi << " " << QT.NRj << "\n";
+      for (int bj = 0; bj < QT.NRj; ++bj)
+        for (int bi = 0; bi < QT.NRi; ++bi) Soln[QT.Roots[bi][bj].block.info.blknum].Grid.Write_Quad_Block(g);
+    }
     FILE* f = fopen(argv[4], "wb");
     int hdr[2] = {nsteps, c.nblk};
     wr(f, hdr, 2);

@@ -47,6 +47,7 @@ static bool read_case(const char* path, std::vector<Euler2D_Quad_Block>& blocks,
   const int NCi = nci + 2 * ng, NCj = ncj + 2 * ng, NNi = NCi + 1, NNj = NCj + 1;
   IP.Number_of_Blocks_Idir = opts[5];
   IP.Number_of_Blocks_Jdir = opts[6];
+  IP.Grid_Type = opts[7] ? "Periodic_Box" : "Rectangular_Box";
   blocks.assign(nblk, Euler2D_Quad_Block());
   neighbour.assign(size_t(8) * nblk, -1);
   auto rd = [&](void* p, size_t sz, size_t n) { ok = ok && fread(p, sz, n, f) == n; };
@@ -93,6 +94,35 @@ static int restart_modes(int argc, char** argv) {
   Euler2D_Input_Parameters IP;
   std::vector<Euler2D_Quad_Block> blocks;
   std::vector<int> neighbour;
+  if (mode == "grid_write") {
+    if (!read_case(argv[2], blocks, neighbour, IP)) return 2;
+    if (Write_Multi_Block_Grid(argv[3], blocks, IP)) return 5;
+    printf("ok\n");
+    return 0;
+  }
+  if (mode == "grid_read") {
+    // nodes X, Y of every block, then BC codes W E S N, then neighbours [nblk][8]
+    std::string type;
+    if (Read_Multi_Block_Grid(argv[2], blocks, neighbour, &type)) return 5;
+    FILE* f = fopen(argv[3], "wb");
+    if (!f) return 10;
+    for (const Euler2D_Quad_Block& B : blocks) {
+      for (int j = 0; j < B.Grid.NNj; ++j)
+        for (int i = 0; i < B.Grid.NNi; ++i) fwrite(&B.Grid.Node[i][j].x, 8, 1, f);
+      for (int j = 0; j < B.Grid.NNj; ++j)
+        for (int i = 0; i < B.Grid.NNi; ++i) fwrite(&B.Grid.Node[i][j].y, 8, 1, f);
+    }
+    for (const Euler2D_Quad_Block& B : blocks) {
+      fwrite(B.Grid.BCtypeW.data(), 4, B.NCj, f);
+      fwrite(B.Grid.BCtypeE.data(), 4, B.NCj, f);
+      fwrite(B.Grid.BCtypeS.data(), 4, B.NCi, f);
+      fwrite(B.Grid.BCtypeN.data(), 4, B.NCi, f);
+    }
+    fwrite(neighbour.data(), 4, neighbour.size(), f);
+    fclose(f);
+    printf("ok %s %zu\n", type.c_str(), blocks.size());
+    return 0;
+  }
   if (mode == "restart_write") {
     if (argc < 6 || !read_case(argv[2], blocks, neighbour, IP)) return 2;
     IP.Restart_File_Name = std::string(argv[3]) + ".soln";
@@ -143,7 +173,8 @@ int main(int argc, char** argv) {
     return 2;
   }
   const std::string mode = argv[1];
-  if (mode == "restart_write" || mode == "restart_read") return restart_modes(argc, argv);
+  if (mode == "restart_write" || mode == "restart_read" || mode == "grid_write" || mode == "grid_read")
+    return restart_modes(argc, argv);
   Euler2D_Input_Parameters IP;
   const int line = IP.Process_Input_Control_Parameter_File(argv[2]);
   if (line) {

@@ -186,11 +186,7 @@ ICs_Type =
 {ics}
 Mach_Number =
 1.40
-Grid_Type =
-Bump_Channel_Flow
-Smooth_Bump =
-OFF
-Number_of_Cells_Idir =
+{grid}Number_of_Cells_Idir =
 8
 Number_of_Cells_Jdir =
 4
@@ -206,8 +202,15 @@ Terminate
 """
 
 
-def restart_deck(restart, extra=""):
-    return RESTART_DECK.format(steps=10 if restart else 20, ics="Restart" if restart else "Uniform", extra=extra)
+BUMP_GRID = "Grid_Type =\nBump_Channel_Flow\nSmooth_Bump =\nOFF\n"
+# (Grid_File_Name after Output_File_Name, which also sets the grid file name)
+DATA_GRID = "Grid_Type =\nRead_From_Data_File\n"
+DATA_GRID_FILE = "Grid_File_Name =\nbumpgrid\n"
+
+
+def restart_deck(restart, extra="", grid=BUMP_GRID):
+    return RESTART_DECK.format(steps=10 if restart else 20, ics="Restart" if restart else "Uniform", extra=extra,
+                               grid=grid)
 
 
 def make_restart_fixture():
@@ -218,35 +221,48 @@ def make_restart_fixture():
               inflow/outflow (17 steps, time 0.25)
       bump0/  deck A's restart files (boundary splines in the grid)
       bump1/  deck B's, a restart from bump0 continued for 10 steps
-    and the two decks."""
+      bump2/  deck C's: deck A on the grid data file bumpgrid.grid (bump0's
+              grids as Write_Quad_Block writes them) read back by the
+              reference (Grid_Type Read_From_Data_File)
+      grid/   grid data files of the channel case and of a periodic box
+    and the three decks."""
     import shutil
     import tarfile
     ch_char = cases.channel(bc=dict(W=cases.BC_CHARACTERISTIC, E=cases.BC_CHARACTERISTIC,
                                     S=cases.BC_REFLECTION, N=cases.BC_CONSTANT_EXTRAPOLATION), seed=8)
     with tempfile.TemporaryDirectory() as td:
         root = os.path.join(td, "restart")
-        for d in ("chan", "bump0", "bump1"):
+        for d in ("chan", "bump0", "bump1", "bump2", "grid"):
             os.makedirs(os.path.join(root, d))
+        grid = os.path.join(root, "grid")
+        for name, bs in (("chan", ch_char), ("box", cases.periodic_box_bumps(nb=2, nc=8, seed=11))):
+            cp = os.path.join(td, name + ".case")
+            cases.write_case(cp, bs)
+            subprocess.run([HARNESS, "grid_write", cp, os.path.join(grid, name + ".grid")], check=True)
         chan = os.path.join(root, "chan")
         cp = os.path.join(td, "chan.case")
         cases.write_case(cp, ch_char)
         subprocess.run([HARNESS, "restart_write", cp, "chan", "17", "0.25"], cwd=chan, check=True)
         subprocess.run([HARNESS, "restart_read", cp, "chan", "read.bin"], cwd=chan, check=True)
-        for name, restart in (("deck_a.in", False), ("deck_b.in", True)):
+        for name, text in (("deck_a.in", restart_deck(False)), ("deck_b.in", restart_deck(True)),
+                           ("deck_c.in", restart_deck(False, extra=DATA_GRID_FILE, grid=DATA_GRID))):
             with open(os.path.join(root, name), "w") as f:
-                f.write(restart_deck(restart))
+                f.write(text)
         dummy = os.path.join(td, "bump.case")  # block count and wiring for restart_read
         cases.write_case(dummy, cases.channel(nbi=4, nbj=2))
         run = os.path.join(td, "run")
         os.makedirs(run)
-        for stage, deck in (("bump0", "deck_a.in"), ("bump1", "deck_b.in")):
+        for stage, deck in (("bump0", "deck_a.in"), ("bump1", "deck_b.in"), ("bump2", "deck_c.in")):
             subprocess.run([HARNESS, "solve", os.path.join(root, deck)], cwd=run, check=True,
                            capture_output=True)
             dst = os.path.join(root, stage)
             for fn in sorted(os.listdir(run)):
                 if fn.startswith("bump_blk") or fn == "bump_quadtree.tree":
                     shutil.copy(os.path.join(run, fn), dst)
-            subprocess.run([HARNESS, "restart_read", dummy, "bump", "read.bin"], cwd=dst, check=True)
+            extra = [os.path.join(run, "bumpgrid.grid")] if stage == "bump0" else []
+            subprocess.run([HARNESS, "restart_read", dummy, "bump", "read.bin"] + extra, cwd=dst, check=True)
+            if extra:
+                shutil.copy(extra[0], os.path.join(root, "bump2"))
         with tarfile.open(os.path.join(OUT, "restart.tar.gz"), "w:gz") as t:
             t.add(root, arcname="restart")
     print("restart.tar.gz")

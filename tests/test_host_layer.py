@@ -16,7 +16,7 @@ from cffc_b200 import capi, cases
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIBDIR = os.path.join(ROOT, "cffc_b200")
-R_AIR = 287.0636
+R_AIR = 8.314511 / (28.9640 * 0.001)  # R_UNIVERSAL / (MOLE_WT_AIR * MILLI)
 
 DECK = """# periodic box, 2 x 2 blocks of 16 x 16 cells
 Time_Integration_Type =
@@ -175,9 +175,9 @@ def test_solver_entry_point_writes_output(tmp_path):
     lib = capi.load_library()
     text = DECK + ""
     deck = write_deck(tmp_path / "s.in", steps=5)
-    outname = str(tmp_path / "s.dat")
+    outname = str(tmp_path / "s.dat")  # the keyword's value + ".dat", as the reference names it
     with open(deck) as f:
-        body = f.read().replace("Execute", "Output_File_Name =\n%s\nExecute" % outname)
+        body = f.read().replace("Execute", "Output_File_Name =\n%s\nExecute" % outname[:-4])
     with open(deck, "w") as f:
         f.write(body)
     lib.e2d_solver_run.argtypes = [capi.C.c_char_p, capi.C.c_int]

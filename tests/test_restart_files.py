@@ -98,32 +98,90 @@ def test_reader_matches_reference_reader(driver, restart_dir, tmp_path, stage, p
     assert len(blocks) == (4 if stage == "chan" else 8)
 
 
+@pytest.mark.parametrize("name", ["chan", "box"])
+def test_grid_file_writer_matches_reference_bytes(driver, restart_dir, tmp_path, name):
+    bs = channel_case() if name == "chan" else cases.periodic_box_bumps(nb=2, nc=8, seed=11)
+    case = str(tmp_path / "c.case")
+    cases.write_case(case, bs)
+    out = str(tmp_path / "ours.grid")
+    subprocess.run([driver, "grid_write", case, out], check=True, capture_output=True)
+    assert open(out, "rb").read() == open(os.path.join(restart_dir, "grid", name + ".grid"), "rb").read()
+
+
+@pytest.mark.parametrize("name", ["chan", "box"])
+def test_grid_file_reader(driver, restart_dir, tmp_path, name):
+    """Nodes as the file prints them (16 significant digits), BC codes and the
+    root-block wiring (periodic for the periodic box) of the case."""
+    bs = channel_case() if name == "chan" else cases.periodic_box_bumps(nb=2, nc=8, seed=11)
+    out = str(tmp_path / "read.bin")
+    r = subprocess.run([driver, "grid_read", os.path.join(restart_dir, "grid", name + ".grid"), out], check=True,
+                       capture_output=True, text=True)
+    assert r.stdout.split()[1] == ("Rectangular_Box" if name == "chan" else "Periodic_Box")
+    raw = open(out, "rb").read()
+    nn = bs.nblk * 2 * bs.node_x[0].size
+    nodes = np.frombuffer(raw[:8 * nn], "<f8").reshape(bs.nblk, 2, *bs.node_x.shape[1:])
+    printed = np.vectorize(lambda x: float("%.15e" % x))
+    assert np.array_equal(nodes[:, 0], printed(bs.node_x))
+    assert np.array_equal(nodes[:, 1], printed(bs.node_y))
+    nbc = 2 * bs.NCj + 2 * bs.NCi
+    bc = np.frombuffer(raw[8 * nn:8 * nn + 4 * nbc * bs.nblk], "<i4").reshape(bs.nblk, nbc)
+    want = np.concatenate([bs.bc_w, bs.bc_e, bs.bc_s, bs.bc_n], axis=1)
+    assert np.array_equal(bc, want)
+    neigh = np.frombuffer(raw[8 * nn + 4 * nbc * bs.nblk:], "<i4").reshape(bs.nblk, 8)
+    assert np.array_equal(neigh, bs.neighbour)
+
+
 def test_reader_rejects_missing_files(driver, tmp_path):
     r = subprocess.run([driver, "restart_read", str(tmp_path / "none"), str(tmp_path / "x.bin")],
                        capture_output=True)
     assert r.returncode != 0
 
 
-@pytest.mark.gpu
-def test_restart_continues_as_the_reference(driver, restart_dir, tmp_path):
+def solve_deck(driver, restart_dir, tmp_path, deck, inputs):
+    """Runs the deck-driven solver (e2d_solver_run, FP64_Exact) in a fresh
+    directory holding the given fixture files; returns what the restart
+    files it writes at the end hold."""
     run = tmp_path / "run"
-    shutil.copytree(os.path.join(restart_dir, "bump0"), run)
-    os.remove(run / "read.bin")
-    deck = open(os.path.join(restart_dir, "deck_b.in")).read()
-    deck = deck.replace("Execute\n", "GPU_Precision =\nFP64_Exact\nExecute\n")
-    with open(run / "deck_b.in", "w") as f:
-        f.write(deck)
+    run.mkdir()
+    for src in inputs:
+        shutil.copy(os.path.join(restart_dir, src), run)
+    text = open(os.path.join(restart_dir, deck)).read()
+    with open(run / deck, "w") as f:
+        f.write(text.replace("Execute\n", "GPU_Precision =\nFP64_Exact\nExecute\n"))
     lib = capi.load_library()
     lib.e2d_solver_run.argtypes = [capi.C.c_char_p, capi.C.c_int]
     cwd = os.getcwd()
     try:
-        os.chdir(run)  # the restart files are named relative to the working directory
-        assert lib.e2d_solver_run(b"deck_b.in", 1) == 0
+        os.chdir(run)  # the files are named relative to the working directory
+        assert lib.e2d_solver_run(deck.encode(), 1) == 0
     finally:
         os.chdir(cwd)
     ours = str(tmp_path / "ours.bin")
     subprocess.run([driver, "restart_read", str(run / "bump"), ours], check=True, capture_output=True)
-    n1, t1, _, got = parse_read(ours, 8, 4)
+    return parse_read(ours, 8, 4)
+
+
+@pytest.mark.gpu
+def test_deck_on_grid_data_file_as_the_reference(driver, restart_dir, tmp_path):
+    """Grid_Type Read_From_Data_File: the reference's Bump_Channel_Flow grid
+    from a grid data file, 20 steps from the freestream."""
+    n1, t1, _, got = solve_deck(driver, restart_dir, tmp_path, "deck_c.in", ["bump2/bumpgrid.grid"])
+    n2, t2, _, want = parse_read(os.path.join(restart_dir, "bump2", "read.bin"), 8, 4)
+    assert n1 == n2 == 20
+    assert t1 == t2
+    assert_same_blocks(got, want, ("ids", "bc", "wo"))
+    for x, y in zip(got, want):
+        # one ulp of the domain's largest coordinate (|x| < 4)
+        np.testing.assert_allclose(x["nodes"], y["nodes"], rtol=0, atol=np.spacing(4.0))
+        ua, ub = x["U"].reshape(4, -1), y["U"].reshape(4, -1)
+        for v in range(4):
+            assert np.max(np.abs(ua[v] - ub[v])) <= 1e-13 * np.max(np.abs(ub[v])), v
+
+
+@pytest.mark.gpu
+def test_restart_continues_as_the_reference(driver, restart_dir, tmp_path):
+    inputs = ["bump0/" + n for n in os.listdir(os.path.join(restart_dir, "bump0")) if n != "read.bin"]
+    n1, t1, _, got = solve_deck(driver, restart_dir, tmp_path, "deck_b.in", inputs)
     n2, t2, _, want = parse_read(os.path.join(restart_dir, "bump1", "read.bin"), 8, 4)
     assert n1 == n2 == 30
     assert t1 == t2
@@ -135,7 +193,8 @@ def test_restart_continues_as_the_reference(driver, restart_dir, tmp_path):
     # the states (measured: at most 1.3e-14 of a block's largest value of the
     # variable after 10 steps).
     for x, y in zip(got, want):
-        np.testing.assert_allclose(x["nodes"], y["nodes"], rtol=0, atol=2e-16)
+        # one ulp of the domain's largest coordinate (|x| < 4)
+        np.testing.assert_allclose(x["nodes"], y["nodes"], rtol=0, atol=np.spacing(4.0))
         ua, ub = x["U"].reshape(4, -1), y["U"].reshape(4, -1)
         for v in range(4):
             assert np.max(np.abs(ua[v] - ub[v])) <= 1e-13 * np.max(np.abs(ub[v])), v
