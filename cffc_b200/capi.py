@@ -34,8 +34,10 @@ class BlocksDesc(C.Structure):
 
 class SchemeDesc(C.Structure):
     _fields_ = [("limiter", C.c_int32), ("flux", C.c_int32), ("n_stage", C.c_int32),
-                ("local_dt", C.c_int32), ("precision", C.c_int32), ("reserved", C.c_int32 * 3),
-                ("cfl", C.c_double), ("gamma", C.c_double)]
+                ("local_dt", C.c_int32), ("precision", C.c_int32), ("time_integration", C.c_int32),
+                ("rs_iterations", C.c_int32), ("freeze_limiter", C.c_int32),
+                ("cfl", C.c_double), ("gamma", C.c_double), ("rs_epsilon", C.c_double),
+                ("freeze_level", C.c_double)]
 
 
 def ptr(a: np.ndarray | None, kind=_dp):
@@ -61,7 +63,9 @@ def make_scheme(sc: Scheme) -> SchemeDesc:
     s = SchemeDesc()
     s.limiter, s.flux, s.n_stage, s.local_dt, s.precision = (
         sc.limiter, sc.flux, sc.n_stage, sc.local_dt, sc.precision)
-    s.cfl, s.gamma = sc.cfl, sc.gamma
+    s.time_integration, s.rs_iterations, s.freeze_limiter = (
+        sc.time_integration, sc.rs_iterations, sc.freeze_limiter)
+    s.cfl, s.gamma, s.rs_epsilon, s.freeze_level = sc.cfl, sc.gamma, sc.rs_epsilon, sc.freeze_level
     return s
 
 

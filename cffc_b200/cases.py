@@ -41,6 +41,11 @@ LIMITER_ONE = -1
 LIMITER_ZERO = 0
 LIMITER_BARTH_JESPERSEN = 8
 LIMITER_VENKATAKRISHNAN = 9
+# i_Time_Integration codes of the explicit schemes (CFD.h:651-659)
+TIME_EXPLICIT_EULER = 0
+TIME_PREDICTOR_CORRECTOR = 3
+TIME_OPTIMAL_SMOOTHING = 7
+TIME_RUNGE_KUTTA = 8
 # i_Flux_Function codes (CFD.h:768-778)
 FLUX_GODUNOV = 1
 FLUX_ROE = 2
@@ -70,6 +75,11 @@ class Scheme:
     precision: int = 0
     cfl: float = 0.5
     gamma: float = GAMMA_AIR
+    time_integration: int = 0   # i_Time_Integration (TIME_* below)
+    rs_epsilon: float = 0.0     # Residual_Smoothing_Epsilon (> 0: on)
+    rs_iterations: int = 2      # Residual_Smoothing_Gauss_Seidel_Iterations
+    freeze_limiter: int = 0     # Freeze_Limiter
+    freeze_level: float = 0.0   # Freeze_Limiter_Residual_Level
 
 
 @dataclasses.dataclass
@@ -342,11 +352,12 @@ def write_case(path: str, bs: BlockSet, W: np.ndarray | None = None) -> None:
     sc = bs.scheme
     W = bs.W if W is None else W
     with open(path, "wb") as f:
-        f.write(struct.pack("<2i", _MAGIC, 1))
+        f.write(struct.pack("<2i", _MAGIC, 2))
         f.write(struct.pack("<4i", bs.nblk, bs.nci, bs.ncj, bs.ng))
         f.write(struct.pack("<8i", sc.limiter, sc.flux, sc.n_stage, sc.local_dt, 1,
                             bs.nbi, bs.nbj, bs.periodic))
-        f.write(struct.pack("<4d", sc.cfl, 0.0, 0.0, 0.0))
+        f.write(struct.pack("<4d", sc.cfl, sc.rs_epsilon, sc.freeze_level, 0.0))
+        f.write(struct.pack("<4i", sc.time_integration, sc.rs_iterations, sc.freeze_limiter, 0))
         for b in range(bs.nblk):
             f.write(bs.neighbour[b].astype("<i4").tobytes())
             for a in (bs.bc_w, bs.bc_e, bs.bc_s, bs.bc_n):
@@ -363,14 +374,15 @@ def read_case(path: str) -> BlockSet:
     Write_Case_File) back into a BlockSet."""
     buf = open(path, "rb").read()
     magic, version = struct.unpack_from("<2i", buf, 0)
-    if magic != _MAGIC or version != 1:
+    if magic != _MAGIC or version not in (1, 2):
         raise ValueError(f"{path}: not a case file")
     nblk, nci, ncj, ng = struct.unpack_from("<4i", buf, 8)
     limiter, flux, n_stage, local_dt, _, nbi, nbj, periodic = struct.unpack_from("<8i", buf, 24)
-    cfl = struct.unpack_from("<d", buf, 56)[0]
+    cfl, rs_eps, fz_level, _ = struct.unpack_from("<4d", buf, 56)
+    tint, rs_it, fz = struct.unpack_from("<3i", buf, 88) if version == 2 else (0, 2, 0)
     NCi, NCj = nci + 2 * ng, ncj + 2 * ng
     NNi, NNj = NCi + 1, NCj + 1
-    off = 88
+    off = 104 if version == 2 else 88
     arrays = {k: [] for k in ("neighbour", "bc_w", "bc_e", "bc_s", "bc_n", "node_x", "node_y",
                               "wo_w", "wo_e", "wo_s", "wo_n", "W")}
 
@@ -391,7 +403,9 @@ def read_case(path: str) -> BlockSet:
             arrays[k].append(take("<f8", (4, n)))
         arrays["W"].append(take("<f8", (4, NCj, NCi)))
     a = {k: np.stack(v) for k, v in arrays.items()}
-    scheme = Scheme(limiter=limiter, flux=flux, n_stage=n_stage, local_dt=local_dt, cfl=cfl)
+    scheme = Scheme(limiter=limiter, flux=flux, n_stage=n_stage, local_dt=local_dt, cfl=cfl,
+                    time_integration=tint, rs_epsilon=rs_eps, rs_iterations=rs_it, freeze_limiter=fz,
+                    freeze_level=fz_level)
     return BlockSet(nci, ncj, a["neighbour"], a["bc_w"], a["bc_e"], a["bc_s"], a["bc_n"], a["node_x"],
                     a["node_y"], a["wo_w"], a["wo_e"], a["wo_s"], a["wo_n"], a["W"], scheme,
                     os.path.basename(path), ng, nbi, nbj, periodic).contiguous()

@@ -2,6 +2,7 @@
 // memory, and the launch sequences of the reference's per-block routines.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -9,6 +10,7 @@
 
 #include "../../include/cffc_e2d.h"
 #include "e2d_handle.h"
+#include "e2d_smooth.cuh"
 
 using namespace e2d;
 
@@ -39,9 +41,112 @@ int check_status(e2d_handle* h) {
   return st[0] ? E2D_ERR_CUDA : 0;
 }
 
-// Stage launch with the double-buffered state (see StageArgs): mode 0 reads
-// (W, U); stage 1 reads (W, U) and writes (W2, U2); stage 2 reads the halo
-// from W2 and U^0 from U and writes (W, U).
+// Runge_Kutta (CFD.cc:901-940) and MultiStage_Optimally_Smoothing
+// (CFD.cc:953-1031): the update coefficient of stage s of an n-stage scheme.
+// The optimally smoothing values are van Leer, Tai and Powell's published
+// coefficients (product of the stage factor and the scheme's CFL factor).
+double rk_coefficient(int s, int n) {
+  double beta = 1.0;
+  if (n == 2 && s == 2) beta = 0.5 * beta;
+  if (n == 4) {
+    if (s == 1 || s == 2) beta = 0.5 * beta;
+    if (s == 4) beta = beta / 6.0;
+  }
+  if (n == 5) {
+    static const double f[4] = {0.059, 0.14, 0.273, 0.5};
+    if (s <= 4) beta *= f[s - 1];
+  }
+  return beta;
+}
+double os_coefficient(int s, int n, int limiter) {
+  static const double zero_lim[7][6] = {{0}, {1.0}, {1.0, 0.3333}, {1.50, 0.1481, 0.4000},
+                                        {2.00, 0.0833, 0.2069, 0.4265}, {2.50, 0.0533, 0.1263, 0.2375, 0.4414},
+                                        {3.00, 0.0370, 0.0851, 0.1521, 0.2562, 0.4512}};
+  static const double lim[7][6] = {{0}, {1.0}, {0.4693, 0.4242}, {0.6936, 0.1918, 0.4929},
+                                   {0.9214, 0.1084, 0.2602, 0.5052}, {1.1508, 0.0695, 0.1602, 0.2898, 0.5060},
+                                   {1.3805, 0.0482, 0.1085, 0.1885, 0.3050, 0.5063}};
+  if (n < 1 || n > 6) return 1.0;
+  const double(&t)[6] = limiter == E2D_LIMITER_ZERO ? zero_lim[n] : lim[n];
+  double beta = t[0];
+  if (s < n) beta = t[s] * beta;  // stage s < n scales the scheme's factor
+  return beta;
+}
+
+// Is the stage sequence of (time_integration, n_stage) one this library runs?
+bool scheme_supported(const e2d_scheme* sc) {
+  switch (sc->time_integration) {
+    case E2D_TIME_EXPLICIT_EULER: return sc->n_stage == 1 || sc->n_stage == 2;
+    case E2D_TIME_PREDICTOR_CORRECTOR: return sc->n_stage == 2;
+    case E2D_TIME_RUNGE_KUTTA: return sc->n_stage == 1 || sc->n_stage == 2 || sc->n_stage == 4 || sc->n_stage == 5;
+    case E2D_TIME_OPTIMAL_SMOOTHING: return sc->n_stage >= 1 && sc->n_stage <= 6;
+    default: return false;
+  }
+}
+
+// Stage s of the handle's scheme: the state it reads (in) and writes (out)
+// -- 0 = (W, U), 1 = (W2, U2), 2 = (W3, U3) -- its update coefficient, the
+// residual slot it stores (0 = dUdt, 1 = R1, 2 = R2) and whether its
+// residual starts from the stored one (the two-stage Runge-Kutta and
+// predictor-corrector schemes, and RK4's last stage; every other stage
+// starts from zero, dUdt_Multistage_Explicit, Euler2DQuad.cc:1304-1342).
+// A stage never writes the state it reads its halo from; the last one
+// writes (W, U) (one-stage schemes copy their result there).
+struct StagePlan {
+  int mode, in, out, slot;
+  bool rk4;
+  double omega;
+};
+StagePlan stage_plan(const e2d_scheme& sc, int s) {
+  const int n = sc.n_stage;
+  const bool os = sc.time_integration == E2D_TIME_OPTIMAL_SMOOTHING;
+  StagePlan p{1, 0, 1, 0, false, os ? os_coefficient(s, n, sc.limiter) : rk_coefficient(s, n)};
+  if (s == 1) return p;
+  p.in = (s == 2) ? 1 : ((s % 2 == 0) ? 1 : 2);
+  p.out = (s == n) ? 0 : (p.in == 1 ? 2 : 1);
+  if (!os && n == 2) p.mode = 2;
+  if (!os && n == 4) {
+    p.slot = s - 1;
+    if (s == 4) { p.mode = 2; p.slot = 0; p.rk4 = true; }
+  }
+  return p;
+}
+
+// (W, U) <- (sW, sU) on the ghost cells (ghost) or the interior cells (!ghost).
+__global__ void copy_cells_kernel(Blocks B, const double* sW, const double* sU, long long ncell, int ghost) {
+  const long long per = (long long)B.NCi * B.NCj;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    const long long b = q / per, r = q % per;
+    const int i = int(r % B.NCi), j = int(r / B.NCi);
+    const bool interior = i >= NG && i < NG + B.nci && j >= NG && j < NG + B.ncj;
+    if (interior == bool(ghost)) continue;
+    const size_t s = size_t(per);
+    const size_t base = size_t(b) * 4 * s + size_t(r);
+    for (int v = 0; v < 4; ++v) {
+      B.W[base + v * s] = sW[base + v * s];
+      B.U[base + v * s] = sU[base + v * s];
+    }
+  }
+}
+cudaError_t copy_cells(e2d_handle* h, const double* sW, const double* sU, bool ghost) {
+  const int grid = int(std::min<size_t>((h->ncell + 255) / 256, 4096));
+  copy_cells_kernel<<<grid, 256, 0, h->stream>>>(h->B, sW, sU, (long long)h->ncell, ghost ? 1 : 0);
+  return cudaGetLastError();
+}
+
+void stage_buffers(e2d_handle* h, int k, double*& W, double*& U) {
+  W = k == 0 ? h->B.W : (k == 1 ? h->B.W2 : h->W3);
+  U = k == 0 ? h->B.U : (k == 1 ? h->B.U2 : h->U3);
+}
+
+cudaError_t launch_stage_args(e2d_handle* h, StageArgs& a) {
+  int ti, tj;
+  stage_tile(h->sc.precision, &ti, &tj);
+  a.tiles_i = (h->B.nci + ti - 1) / ti;
+  a.tiles_j = (h->B.ncj + tj - 1) / tj;
+  return launch_stage_prec(h->sc.precision, a, h->stream);
+}
+
+// Residual (mode 0) or Frechet product (mode 3) of the state (W, U).
 cudaError_t launch_stage_any(e2d_handle* h, int mode, int fuse_next) {
   StageArgs a{};
   a.B = h->B;
@@ -49,28 +154,42 @@ cudaError_t launch_stage_any(e2d_handle* h, int mode, int fuse_next) {
   a.fuse_next = fuse_next;
   a.hist = h->hist;
   a.step = h->step;
-  a.Win = mode == 2 ? h->B.W2 : h->B.W;
+  a.Win = h->B.W;
   a.Ubase = h->B.U;
-  a.Wout = mode == 1 ? h->B.W2 : h->B.W;
-  a.Uout = mode == 1 ? h->B.U2 : h->B.U;
-  int ti, tj;
-  stage_tile(h->sc.precision, &ti, &tj);
-  a.tiles_i = (h->B.nci + ti - 1) / ti;
-  a.tiles_j = (h->B.ncj + tj - 1) / tj;
-  cudaError_t e = launch_stage_prec(h->sc.precision, a, h->stream);
-  if (e == cudaSuccess && mode == 1 && h->sc.n_stage == 1) {
-    // single-stage scheme: the stage-1 result is the new solution
-    const size_t n = sizeof(double) * 4 * h->ncell;
-    e = cudaMemcpyAsync(h->B.W, h->B.W2, n, cudaMemcpyDeviceToDevice, h->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h->B.U, h->B.U2, n, cudaMemcpyDeviceToDevice, h->stream);
-  }
+  a.Wout = h->B.W;
+  a.Uout = h->B.U;
+  a.res_out = h->B.dUdt;
+  a.omega = 1.0;
+  return launch_stage_args(h, a);
+}
+
+// Explicit stage s (1-based) of the handle's scheme, per its StagePlan.
+cudaError_t launch_explicit_stage(e2d_handle* h, int s, int fuse_next) {
+  const StagePlan p = stage_plan(h->sc, s);
+  StageArgs a{};
+  a.B = h->B;
+  a.mode = p.mode;
+  a.fuse_next = fuse_next;
+  a.hist = h->hist;
+  a.step = h->step;
+  double *W_in, *U_in;
+  stage_buffers(h, p.in, W_in, U_in);
+  a.Win = W_in;
+  a.Ubase = h->B.U;
+  stage_buffers(h, p.out, a.Wout, a.Uout);
+  a.omega = p.omega;
+  a.res_out = p.slot == 0 ? h->B.dUdt : (p.slot == 1 ? h->R1 : h->R2);
+  if (p.rk4) { a.acc1 = h->R1; a.acc2 = h->R2; }
+  cudaError_t e = launch_stage_args(h, a);
+  // single-stage scheme: the stage's interior result is the new solution
+  if (e == cudaSuccess && h->sc.n_stage == 1) e = copy_cells(h, h->B.W2, h->B.U2, false);
   return e;
 }
 
-// Ghost fill of the state the given stage reads (stage 2 reads W2, U2).
-cudaError_t ghost_fill_for(e2d_handle* h, int mode) {
+// Ghost fill of the state stage s reads (s = 0: the solution (W, U)).
+cudaError_t ghost_fill_for(e2d_handle* h, int s) {
   Blocks B = h->B;
-  if (mode == 2) { B.W = h->B.W2; B.U = h->B.U2; }
+  if (s > 0) stage_buffers(h, stage_plan(h->sc, s).in, B.W, B.U);
   return launch_ghost_fill(B, h->stream);
 }
 
@@ -115,17 +234,96 @@ cudaError_t enqueue_step_head(e2d_handle* h) {
   return launch_norms(h->B, h->part, h->hist, h->step, h->stream);
 }
 
+// The frozen flags ([ncase], cleared), the first-step flag (set) and the
+// stored limiters of a scheme with Freeze_Limiter.
+int alloc_freeze(e2d_handle* h) {
+  if (!h->sc.freeze_limiter) return 0;
+  int rc;
+  if ((rc = dalloc(h, &h->freeze, size_t(h->B.ncase))) || (rc = dalloc(h, &h->first, 1))) return rc;
+  if (!h->B.phi_keep) {
+    if ((rc = dalloc(h, &h->B.phi_keep, 4 * h->ncell))) return rc;
+    CK(cudaMemset(h->B.phi_keep, 0, sizeof(double) * 4 * h->ncell));
+  }
+  const int one = 1;
+  CK(cudaMemset(h->freeze, 0, sizeof(int) * h->B.ncase));
+  CK(cudaMemcpy(h->first, &one, sizeof(int), cudaMemcpyHostToDevice));
+  h->B.freeze = h->freeze;
+  return 0;
+}
+
+// A new initial state starts a new run: limiters unfrozen, first step next.
+int reset_run(e2d_handle* h) {
+  if (!h->freeze) return 0;
+  const int one = 1;
+  CK(cudaMemsetAsync(h->freeze, 0, sizeof(int) * h->B.ncase, h->stream));
+  CK(cudaMemcpyAsync(h->first, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  return 0;
+}
+
+cudaError_t launch_freeze_check(e2d_handle* h) {
+  if (!h->freeze) return cudaSuccess;
+  freeze_check_kernel<<<1, 32, 0, h->stream>>>(h->hist, h->step, h->B.ncase, h->sc.freeze_level, h->freeze,
+                                                h->first);
+  return cudaGetLastError();
+}
+
+// Stage s with residual smoothing: the stage's residual (no update), the
+// Gauss-Seidel smoothing of it, then the update.
+cudaError_t launch_smoothed_stage(e2d_handle* h, int s) {
+  const StagePlan p = stage_plan(h->sc, s);
+  StageArgs a{};
+  a.B = h->B;
+  a.mode = p.mode;
+  a.fuse_next = 0;
+  a.hist = h->hist;
+  a.step = h->step;
+  double *W_in, *U_in, *W_out, *U_out;
+  stage_buffers(h, p.in, W_in, U_in);
+  stage_buffers(h, p.out, W_out, U_out);
+  a.Win = W_in;
+  a.Ubase = h->B.U;
+  a.Wout = W_out;
+  a.Uout = U_out;
+  a.omega = p.omega;
+  a.res_out = h->B.dUdt;
+  a.no_update = 1;
+  cudaError_t e = launch_stage_args(h, a);
+  if (e != cudaSuccess) return e;
+  if (h->smooth_smem)
+    residual_smoothing_kernel<true><<<h->B.nblk, SMOOTH_THREADS, h->smooth_smem, h->stream>>>(
+        h->B, h->B.dUdt, nullptr, h->sc.rs_epsilon, h->sc.rs_iterations);
+  else
+    residual_smoothing_kernel<false><<<h->B.nblk, SMOOTH_THREADS, 0, h->stream>>>(
+        h->B, h->B.dUdt, h->smooth_scratch, h->sc.rs_epsilon, h->sc.rs_iterations);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const long long n = (long long)h->B.nblk * h->B.nci * h->B.ncj;
+  const int grid = int(std::min<long long>((n + 255) / 256, 4096));
+  stage_update_kernel<<<grid, 256, 0, h->stream>>>(h->B, h->B.U, h->B.dUdt, p.omega, W_out, U_out);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (h->sc.n_stage == 1) e = copy_cells(h, h->B.W2, h->B.U2, false);
+  return e;
+}
+
 // One explicit time step in the reference's order (Euler2DQuadSolvers.cc:657-898):
-// per stage ghost fill + fused residual/update; the last stage also reduces
-// the next step's CFL minimum and residual norms.
+// limiter-freezing test, then per stage ghost fill + fused residual/update;
+// the last stage also reduces the next step's CFL minimum and residual
+// norms.  With residual smoothing the stages are split (residual,
+// smoothing, update) and every step starts with its own CFL and norms.
 cudaError_t enqueue_step(e2d_handle* h) {
   cudaError_t e;
+  const bool smooth = h->sc.rs_epsilon > 0.0;
+  if (smooth && (e = enqueue_step_head(h))) return e;
   if ((e = launch_slot_init(h->hist, h->step, 1, h->B.ncase, h->stream))) return e;
+  if ((e = launch_freeze_check(h))) return e;
   for (int stage = 1; stage <= h->sc.n_stage; ++stage) {
     if ((e = ghost_fill_for(h, stage))) return e;
-    if ((e = launch_stage_any(h, stage, stage == h->sc.n_stage))) return e;
+    if (smooth) {
+      if ((e = launch_smoothed_stage(h, stage))) return e;
+    } else if ((e = launch_explicit_stage(h, stage, stage == h->sc.n_stage))) {
+      return e;
+    }
   }
-  return launch_step_end(h->hist, h->step, 1, h->B.ncase, h->stream);
+  return launch_step_end(h->hist, h->step, smooth ? 0 : 1, h->B.ncase, h->stream);
 }
 
 }  // namespace e2d_host
@@ -142,7 +340,11 @@ e2d_handle* e2d_create(const e2d_blocks_desc* d, const e2d_scheme* sc, int devic
   };
   if (err) *err = 0;
   if (!d || !sc || d->nblk < 1 || d->nci < 2 || d->ncj < 2 || d->ng != NG) return fail(E2D_ERR_ARG, nullptr);
-  if (sc->n_stage != 1 && sc->n_stage != 2) return fail(E2D_ERR_ARG, nullptr);
+  if (!scheme_supported(sc)) return fail(E2D_ERR_ARG, nullptr);
+  // residual smoothing keeps its scratch in the reference's residual slot
+  // k_residual+1, which RK4's stages occupy: not a combination to run
+  if (sc->rs_epsilon > 0.0 && (sc->rs_iterations < 0 || stage_plan(*sc, sc->n_stage).rk4))
+    return fail(E2D_ERR_ARG, nullptr);
   if (!e2d_flux_supported(sc->flux)) return fail(E2D_ERR_ARG, nullptr);
   if (sc->precision != E2D_PREC_FP64 && sc->precision != E2D_PREC_FP64_EXACT && sc->precision != E2D_PREC_FP32)
     return fail(E2D_ERR_ARG, nullptr);
@@ -206,6 +408,32 @@ e2d_handle* e2d_create(const e2d_blocks_desc* d, const e2d_scheme* sc, int devic
       cudaMemset(B.dt, 0, sizeof(double) * h->ncell) || cudaMemset(B.status, 0, sizeof(int) * 2) ||
       cudaMemset(h->step, 0, sizeof(int)))
     return fail(E2D_ERR_CUDA, h);
+  if (sc->n_stage >= 3) {
+    if ((rc = dalloc(h, &h->W3, 4 * h->ncell)) || (rc = dalloc(h, &h->U3, 4 * h->ncell))) return fail(rc, h);
+    if (cudaMemset(h->W3, 0, sizeof(double) * 4 * h->ncell) || cudaMemset(h->U3, 0, sizeof(double) * 4 * h->ncell))
+      return fail(E2D_ERR_CUDA, h);
+  }
+  if (stage_plan(*sc, sc->n_stage).rk4) {
+    if ((rc = dalloc(h, &h->R1, 4 * h->ncell)) || (rc = dalloc(h, &h->R2, 4 * h->ncell))) return fail(rc, h);
+    if (cudaMemset(h->R1, 0, sizeof(double) * 4 * h->ncell) || cudaMemset(h->R2, 0, sizeof(double) * 4 * h->ncell))
+      return fail(E2D_ERR_CUDA, h);
+  }
+  if (sc->rs_epsilon > 0.0) {
+    // the smoothing region and its zero ring, [4][ncj][nci] doubles per block,
+    // in shared memory when it fits
+    const size_t bytes = sizeof(double) * 4 * size_t(d->nci) * d->ncj;
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (bytes <= size_t(max_smem) &&
+        cudaFuncSetAttribute(residual_smoothing_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(bytes)) == cudaSuccess) {
+      h->smooth_smem = bytes;
+    } else {
+      cudaGetLastError();
+      if ((rc = dalloc(h, &h->smooth_scratch, 4 * size_t(d->nci) * d->ncj * B.nblk))) return fail(rc, h);
+    }
+  }
+  if ((rc = alloc_freeze(h))) return fail(rc, h);
   if ((rc = ensure_hist(h, 64))) return fail(rc, h);
   B.dWdx = B.dWdy = B.phi = nullptr;
   return h;
@@ -272,7 +500,7 @@ e2d_handle* e2d_create_batch(const e2d_blocks_desc* cases, int ncase, const e2d_
   // the step history holds one slot per case and step
   const int cap = h->hist_cap;
   h->hist_cap = 0;
-  if ((rc = ensure_hist(h, cap))) {
+  if ((rc = ensure_hist(h, cap)) || (rc = alloc_freeze(h))) {
     if (err) *err = rc;
     e2d_destroy(h);
     return nullptr;
@@ -314,24 +542,9 @@ int e2d_set_state(e2d_handle* h, const double* W) {
   u_of_w_kernel<<<grid, 256, 0, h->stream>>>(h->B, (long long)h->ncell);
   CK(cudaGetLastError());
   CK(cudaMemsetAsync(h->B.status, 0, sizeof(int) * 2, h->stream));
+  if (int rc = reset_run(h)) return rc;
   CK(cudaStreamSynchronize(h->stream));
   return 0;
-}
-
-// Ghost cells of (W2, U2) into (W, U); interior cells untouched.
-__global__ void ghost_from_stage_kernel(Blocks B, long long ncell) {
-  const long long per = (long long)B.NCi * B.NCj;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
-    const long long b = q / per, r = q % per;
-    const int i = int(r % B.NCi), j = int(r / B.NCi);
-    if (i >= NG && i < NG + B.nci && j >= NG && j < NG + B.ncj) continue;
-    const size_t s = size_t(per);
-    const size_t base = size_t(b) * 4 * s + size_t(r);
-    for (int v = 0; v < 4; ++v) {
-      B.W[base + v * s] = B.W2[base + v * s];
-      B.U[base + v * s] = B.U2[base + v * s];
-    }
-  }
 }
 
 // W = W(U) for every cell (Euler2D_cState::W, Euler2DState.h:1741; the
@@ -356,6 +569,7 @@ int e2d_set_conserved(e2d_handle* h, const double* U) {
   w_of_u_kernel<<<grid, 256, 0, h->stream>>>(h->B, (long long)h->ncell);
   CK(cudaGetLastError());
   CK(cudaMemsetAsync(h->B.status, 0, sizeof(int) * 2, h->stream));
+  if (int rc = reset_run(h)) return rc;
   CK(cudaStreamSynchronize(h->stream));
   return 0;
 }
@@ -428,14 +642,14 @@ int e2d_rk_steps(e2d_handle* h, int n_steps, double* hist) {
   }
   h->B = saved;
   for (int s = 0; s < n_steps; ++s) CK(cudaGraphLaunch(h->step_graph, h->stream));
-  if (h->sc.n_stage == 2) {
-    // The reference keeps one state array, so after a two-stage step its
+  if (h->sc.n_stage >= 2) {
+    // The reference keeps one state array, so after a multistage step its
     // ghost cells hold the last stage's exchange and BCs; here those went
-    // to the stage buffers.  Copy them so the final state matches the
-    // reference's in every cell (what a restart file records).
-    const int grid = int(std::min<size_t>((h->ncell + 255) / 256, 4096));
-    ghost_from_stage_kernel<<<grid, 256, 0, h->stream>>>(h->B, (long long)h->ncell);
-    CK(cudaGetLastError());
+    // to the buffer that stage read.  Copy them so the final state matches
+    // the reference's in every cell (what a restart file records).
+    double *W, *U;
+    stage_buffers(h, stage_plan(h->sc, h->sc.n_stage).in, W, U);
+    CK(copy_cells(h, W, U, true));
   }
   if (hist)
     CK(cudaMemcpyAsync(hist, h->hist, sizeof(double) * 4 * size_t(n_steps) * h->B.ncase, cudaMemcpyDeviceToHost,
@@ -520,12 +734,12 @@ int e2d_kernel_times(e2d_handle* h, int n_steps, double out[6]) {
     CK(launch_slot_init(h->hist, h->step, 1, h->B.ncase, h->stream));
     CK(ghost_fill_for(h, 1));
     CK(cudaEventRecord(ev[3], h->stream));
-    CK(launch_stage_any(h, 1, h->sc.n_stage == 1));
+    CK(launch_explicit_stage(h, 1, h->sc.n_stage == 1));
     CK(cudaEventRecord(ev[4], h->stream));
     if (h->sc.n_stage == 2) {
       CK(ghost_fill_for(h, 2));
       CK(cudaEventRecord(ev[5], h->stream));
-      CK(launch_stage_any(h, 2, 1));
+      CK(launch_explicit_stage(h, 2, 1));
       CK(cudaEventRecord(ev[6], h->stream));
     }
     CK(launch_step_end(h->hist, h->step, 1, h->B.ncase, h->stream));

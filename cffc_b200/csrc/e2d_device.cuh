@@ -58,6 +58,12 @@ struct Blocks {
   const int* case_start;
   int ncase;
   const int* case_active;  // per case, null = all: residual/JVP stages skip inactive cases
+  // Limiter freezing (Freeze_Limiter): with freeze set, *freeze != 0 means
+  // the limiters are frozen and every reconstruction takes phi from
+  // phi_keep; while *freeze == 0 each reconstruction stores its phi there
+  // (cells of the tiles and their one-cell rings).  freeze null: off.
+  const int* freeze;
+  double* phi_keep;
 };
 
 __host__ __device__ inline int case_id(const Blocks& B, int b) { return B.case_of ? B.case_of[b] : 0; }
@@ -87,6 +93,15 @@ struct StageArgs {
   double* Uout;
   int fuse_next;       // last stage of a step: also accumulate the next step's
                        // CFL minimum and residual norms into hist[4*(*step+1)..]
+  // explicit stages (modes 1, 2): U = Ubase + omega*dUdt, the stage's dUdt
+  // stored to res_out; mode 2 starts dUdt from res_out's previous content
+  // (the two-stage schemes) or, with acc1/acc2 set, from
+  // res_out + 2*acc1 + 2*acc2 (stage 4 of RK4, Euler2DQuad.cc:1322-1334)
+  double omega;
+  double* res_out;
+  const double* acc1;
+  const double* acc2;
+  int no_update;  // modes 1, 2: store the stage's residual only (residual smoothing follows)
   // mode 3 (Frechet Jacobian-vector product of the NKS, GMRES2D.h:445-488):
   // v = (R(U)/normR - b)/eps - (z/dt)*normU/normR on interior cells, with the
   // GMRES vectors b, z, v in the reference's cell-major layout

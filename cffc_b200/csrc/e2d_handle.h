@@ -25,6 +25,15 @@ struct e2d_handle {
   int* step = nullptr;     // device step counter
   double* part = nullptr;  // [nblk][3] norm partials
   bool recon_out = false;  // dWdx/dWdy/phi arrays allocated
+  // third stage state (schemes of three or more stages) and the second and
+  // third residual slots of RK4 (dUdt[i][j][1..2] of the reference)
+  double *W3 = nullptr, *U3 = nullptr, *R1 = nullptr, *R2 = nullptr;
+  // limiter freezing: per-case frozen flags and the "first step of the run"
+  // flag (device); residual smoothing: global scratch when a block's
+  // smoothing region does not fit in shared memory
+  int *freeze = nullptr, *first = nullptr;
+  double* smooth_scratch = nullptr;
+  size_t smooth_smem = 0;
   // captured explicit step
   cudaGraphExec_t step_graph = nullptr;
   e2d_nks_state* nks = nullptr;

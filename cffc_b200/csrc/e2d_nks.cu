@@ -893,7 +893,22 @@ int gmres(e2d_handle* h, const e2d_nks_params& p, const std::vector<double>& tol
 
 }  // namespace
 
+static int nks_run(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, int* n_steps);
+
+// The Newton-Krylov solve starts with the limiters unfrozen and never
+// freezes them (Evaluate_Limiters, NKS2D.h:90; its freezing code is
+// disabled): the solve runs without the freezing machinery.
 extern "C" int e2d_nks(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, int* n_steps) {
+  if (!h) return nks_run(h, p, hist, n_steps);
+  if (h->freeze && cudaMemset(h->freeze, 0, sizeof(int) * h->B.ncase) != cudaSuccess) return E2D_ERR_CUDA;
+  const int* saved = h->B.freeze;
+  h->B.freeze = nullptr;
+  const int rc = nks_run(h, p, hist, n_steps);
+  h->B.freeze = saved;
+  return rc;
+}
+
+static int nks_run(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, int* n_steps) {
   if (!h || !p || p->max_newton < 0 || p->gmres_restart < 1 || p->gmres_restart > 500 || p->max_gmres < 1 ||
       !(p->epsilon0 > 0.0) || !(p->cfl0 > 0.0) || !(p->gmres_tol_initial > 0.0) || !(p->gmres_tol_final > 0.0) ||
       !(p->min_ratio > 0.0)) {

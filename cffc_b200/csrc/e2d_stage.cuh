@@ -282,8 +282,11 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
   const int t = blockIdx.x % tiles;
   const int i0 = (t % a.tiles_i) * TI;   // interior index of the tile's first cell
   const int j0 = (t / a.tiles_i) * TJ;   // == array index of the halo origin
-  __shared__ int failed;
-  if (tid == 0) failed = *(volatile int*)B.status;
+  __shared__ int failed, frozen;
+  if (tid == 0) {
+    failed = *(volatile int*)B.status;
+    frozen = B.freeze ? B.freeze[case_id(B, b)] : 0;
+  }
   __syncthreads();
   if (failed) return;  // an earlier kernel failed: stop marching (uniform per CTA)
   const int cs = case_id(B, b);  // the block's case: its slot of the step history
@@ -386,7 +389,13 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
       RT uq[4];
 #pragma unroll
       for (int q2 = 0; q2 < 4; ++q2) uq[q2] = u0 + gx * ofx[q2] + gy * ofy[q2];
-      const RT phi = cell_limiter(B.limiter, uq, u0, umin, umax);
+      RT phi;
+      if (frozen) {  // Freeze_Limiter: the limiter of the last reconstruction before freezing
+        phi = RT(B.phi_keep[cell_var(B, b, v, J, I)]);
+      } else {
+        phi = cell_limiter(B.limiter, uq, u0, umin, umax);
+        if (B.freeze) B.phi_keep[cell_var(B, b, v, J, I)] = double(phi);
+      }
       s.px[v][rj][ri] = phi * gx;
       s.py[v][rj][ri] = phi * gy;
       if (B.dWdx) {
@@ -489,7 +498,12 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
     double res[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-      double d = (MODE == 2) ? B.dUdt[cell_var(B, b, v, J, I)] : 0.0;
+      double d = 0.0;
+      if (MODE == 2) {
+        const size_t q = cell_var(B, b, v, J, I);
+        d = a.res_out[q];
+        if (a.acc1) d = d + 2.0 * a.acc1[q] + 2.0 * a.acc2[q];
+      }
       if (MODE == 1 || MODE == 2) {
 #ifdef E2D_FAST
         d += k * s.Fi[v][tj][ti] * lW * rA;
@@ -532,12 +546,16 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
         val -= (a.nks_z[q + v] * rdt) * a.normU[v] / a.normR[v];
         a.nks_v[q + v] = val;
       }
+    } else if (a.no_update) {
+      // the stage's residual only: residual smoothing and the update follow
+#pragma unroll
+      for (int v = 0; v < 4; ++v) a.res_out[cell_var(B, b, v, J, I)] = res[v];
     } else {
       // Update_Solution_Multistage_Explicit: U = Uo + omega*dUdt
       CState<double> uo;
       uo.d = a.Ubase[cell_var(B, b, 0, J, I)]; uo.mx = a.Ubase[cell_var(B, b, 1, J, I)];
       uo.my = a.Ubase[cell_var(B, b, 2, J, I)]; uo.E = a.Ubase[cell_var(B, b, 3, J, I)];
-      const double omega = (B.n_stage == 2 && MODE == 2) ? HALF * 1.0 : 1.0;
+      const double omega = a.omega;
       CState<double> u;
       u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
       u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
@@ -560,7 +578,7 @@ __global__ void __launch_bounds__(NTHREADS, E2D_MIN_CTAS) stage_kernel(StageArgs
         }
       }
 #pragma unroll
-      for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, b, v, J, I)] = res[v];
+      for (int v = 0; v < 4; ++v) a.res_out[cell_var(B, b, v, J, I)] = res[v];
 #ifdef E2D_FAST
       const PState<double> w = fm::W_of_U(u, gm1);
 #else

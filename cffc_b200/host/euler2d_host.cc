@@ -160,11 +160,14 @@ int Parse_Next_Input_Control_Parameter(Euler2D_Input_Parameters& IP, std::istrea
   if (code == "Continue" || code == "Write_Output" || code == "Write_Output_Cells") return 0;
   if (code == "Time_Integration_Type") {
     if (str(IP.Time_Integration_Type)) return INVALID_INPUT_CODE;
+    // Euler2DInput.cc:1782-1794; multigrid and the implicit schemes are
+    // outside this path
     const std::string& t = IP.Time_Integration_Type;
-    if (t == "Explicit_Euler") IP.N_Stage = 1;
-    else if (t == "Explicit_Predictor_Corrector") IP.N_Stage = 2;
-    else if (t == "Explicit_Runge_Kutta") IP.N_Stage = 4;
-    else return INVALID_INPUT_CODE;  // optimal smoothing, multigrid, DTS: outside this path
+    if (t == "Explicit_Euler") { IP.i_Time_Integration = E2D_TIME_EXPLICIT_EULER; IP.N_Stage = 1; }
+    else if (t == "Explicit_Predictor_Corrector") { IP.i_Time_Integration = E2D_TIME_PREDICTOR_CORRECTOR; IP.N_Stage = 2; }
+    else if (t == "Explicit_Runge_Kutta") { IP.i_Time_Integration = E2D_TIME_RUNGE_KUTTA; IP.N_Stage = 4; }
+    else if (t == "Multistage_Optimal_Smoothing") { IP.i_Time_Integration = E2D_TIME_OPTIMAL_SMOOTHING; IP.N_Stage = 4; }
+    else return INVALID_INPUT_CODE;
     return 0;
   }
   if (code == "Reconstruction_Type") {
@@ -241,11 +244,20 @@ int Parse_Next_Input_Control_Parameter(Euler2D_Input_Parameters& IP, std::istrea
   auto num_d = [&](double& v, bool positive) {
     return (next_value(in, L, v) && (!positive || v > 0.0)) ? 0 : INVALID_INPUT_CODE;
   };
-  if (code == "N_Stage") {
-    int rc = num_i(IP.N_Stage, 0);
-    return rc ? rc : ((IP.N_Stage == 1 || IP.N_Stage == 2) ? 0 : INVALID_INPUT_CODE);
-  }
+  if (code == "N_Stage") return num_i(IP.N_Stage, 1);  // the scheme's stage counts are checked at e2d_create
   if (code == "CFL_Number") return num_d(IP.CFL_Number, true);
+  if (code == "Residual_Smoothing_Epsilon") {  // Euler2DInput.cc:2958-2969 (<= 0: off)
+    int rc = num_d(IP.Residual_Smoothing_Epsilon, false);
+    if (!rc && IP.Residual_Smoothing_Epsilon <= 0.0) IP.Residual_Smoothing_Epsilon = 0.0;
+    return rc;
+  }
+  if (code == "Residual_Smoothing_Gauss_Seidel_Iterations") {
+    int rc = num_i(IP.Residual_Smoothing_Gauss_Seidel_Iterations, -1000000);
+    if (!rc && IP.Residual_Smoothing_Gauss_Seidel_Iterations < 0) IP.Residual_Smoothing_Gauss_Seidel_Iterations = 0;
+    return rc;
+  }
+  if (code == "Freeze_Limiter") return num_i(IP.Freeze_Limiter, 0);
+  if (code == "Freeze_Limiter_Residual_Level") return num_d(IP.Freeze_Limiter_Residual_Level, false);
   if (code == "Time_Accurate") return num_i(IP.Time_Accurate, 0);
   if (code == "Restart_Solution_Save_Frequency") return num_i(IP.Restart_Solution_Save_Frequency, 1);
   if (code == "Local_Time_Stepping") {
@@ -465,8 +477,13 @@ e2d_scheme scheme_of(const Euler2D_Input_Parameters& IP) {
   s.n_stage = IP.N_Stage;
   s.local_dt = IP.Local_Time_Stepping ? 1 : 0;
   s.precision = IP.Precision;
+  s.time_integration = IP.i_Time_Integration;
+  s.rs_iterations = IP.Residual_Smoothing_Gauss_Seidel_Iterations;
+  s.freeze_limiter = IP.Freeze_Limiter ? 1 : 0;
   s.cfl = IP.CFL_Number;
   s.gamma = Euler2D_pState::g;
+  s.rs_epsilon = IP.Residual_Smoothing_Epsilon;
+  s.freeze_level = IP.Freeze_Limiter_Residual_Level;
   return s;
 }
 
@@ -582,12 +599,14 @@ int Write_Case_File(const std::string& path, const std::vector<Euler2D_Quad_Bloc
   const e2d_blocks_desc& d = P.desc;
   const e2d_scheme s = scheme_of(IP);
   const int NCi = d.nci + 2 * d.ng, NCj = d.ncj + 2 * d.ng, NNi = NCi + 1, NNj = NCj + 1;
-  const int32_t head[14] = {0x43443245, 1, d.nblk, d.nci, d.ncj, d.ng, s.limiter, s.flux, s.n_stage, s.local_dt, 1,
+  const int32_t head[14] = {0x43443245, 2, d.nblk, d.nci, d.ncj, d.ng, s.limiter, s.flux, s.n_stage, s.local_dt, 1,
                             IP.Number_of_Blocks_Idir, IP.Number_of_Blocks_Jdir,
                             IP.Grid_Type == "Periodic_Box" ? 1 : 0};
-  const double headf[4] = {s.cfl, 0.0, 0.0, 0.0};
+  const double headf[4] = {s.cfl, s.rs_epsilon, s.freeze_level, 0.0};
+  const int32_t head2[4] = {s.time_integration, s.rs_iterations, s.freeze_limiter, 0};
   fwrite(head, sizeof(int32_t), 14, f);
   fwrite(headf, sizeof(double), 4, f);
+  fwrite(head2, sizeof(int32_t), 4, f);
   for (int b = 0; b < d.nblk; ++b) {
     fwrite(P.neighbour.data() + 8 * b, sizeof(int32_t), 8, f);
     fwrite(P.bcw.data() + size_t(b) * NCj, sizeof(int32_t), NCj, f);

@@ -92,17 +92,34 @@ typedef struct e2d_blocks_desc {
   const double *wo_s, *wo_n;  /* [nblk][4][NCi]                                */
 } e2d_blocks_desc;
 
+/* Explicit time-stepping schemes (i_Time_Integration, src_2D/CFD/CFD.h:651-659)
+ * and their stage counts:
+ *   E2D_TIME_EXPLICIT_EULER / PREDICTOR_CORRECTOR / RUNGE_KUTTA: N_Stage 1, 2
+ *     (residuals accumulated over the stages), 4 (classical RK4), 5
+ *     (the reference's 5-stage coefficients);
+ *   E2D_TIME_OPTIMAL_SMOOTHING: N_Stage 1-6, the optimally smoothing
+ *     multistage coefficients of van Leer, Tai and Powell (CFD.cc:953).
+ * Code 0 (the structure's zero value) is the Runge-Kutta family. */
+#define E2D_TIME_EXPLICIT_EULER 0
+#define E2D_TIME_PREDICTOR_CORRECTOR 3
+#define E2D_TIME_OPTIMAL_SMOOTHING 7
+#define E2D_TIME_RUNGE_KUTTA 8
+
 /* Numerical scheme: the subset of Euler2D_Input_Parameters the path reads
  * (src_2D/Euler2D/Euler2DInput.h:41-120). */
 typedef struct e2d_scheme {
   int32_t limiter;   /* i_Limiter                                         */
   int32_t flux;      /* i_Flux_Function: E2D_FLUX_* (all but Osher)       */
-  int32_t n_stage;   /* N_Stage of TIME_STEPPING_EXPLICIT_RUNGE_KUTTA: 1, 2 */
+  int32_t n_stage;   /* N_Stage (see E2D_TIME_*)                          */
   int32_t local_dt;  /* Local_Time_Stepping: 0 global, 1 scalar local     */
   int32_t precision; /* E2D_PREC_*                                        */
-  int32_t reserved[3];
+  int32_t time_integration;  /* i_Time_Integration: E2D_TIME_*            */
+  int32_t rs_iterations;     /* Residual_Smoothing_Gauss_Seidel_Iterations */
+  int32_t freeze_limiter;    /* Freeze_Limiter: 0 off, 1 on               */
   double cfl;        /* CFL_Number                                        */
   double gamma;      /* specific-heat ratio g (GAMMA_AIR = 1.4)           */
+  double rs_epsilon; /* Residual_Smoothing_Epsilon (> 0: smoothing on)    */
+  double freeze_level;       /* Freeze_Limiter_Residual_Level             */
 } e2d_scheme;
 
 typedef struct e2d_handle e2d_handle;

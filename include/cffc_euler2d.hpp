@@ -98,7 +98,12 @@ class Euler2D_Quad_Block {
 // (Pressure in kPa, Time_Max in ms), stored in SI as the reference does.
 struct Euler2D_Input_Parameters {
   std::string Time_Integration_Type = "Explicit_Euler";
+  int i_Time_Integration = E2D_TIME_EXPLICIT_EULER;
   int N_Stage = 1;
+  double Residual_Smoothing_Epsilon = 0.0;  // > 0 turns implicit residual smoothing on
+  int Residual_Smoothing_Gauss_Seidel_Iterations = 2;
+  int Freeze_Limiter = 0;
+  double Freeze_Limiter_Residual_Level = 1e-4;
   double CFL_Number = 0.5;
   int Time_Accurate = 0;
   int Local_Time_Stepping = 0;

@@ -31,6 +31,8 @@ struct e2d_oracle {
   double *X, *Y, *wow, *woe, *wos, *won;
   double *xc, *yc, *A;                                  /* [nblk][NCj][NCi] */
   double *W, *U, *Uo, *dUdt, *dWdx, *dWdy, *phi, *dt;  /* cell arrays */
+  double *dUdt1, *dUdt2;  /* residual slots 1, 2 (dUdt[i][j][1..2], RK4) */
+  int frozen, first;      /* limiters frozen; next explicit step is a run's first */
 };
 
 static inline double dmin(double x, double y) { return (x < y) ? x : y; } /* Math.h */
@@ -712,7 +714,9 @@ static void lsq_cell(e2d_oracle *o, int b, int i, int j) {
           const double dx = xf[q].x - o->xc[c], dy = xf[q].y - o->yc[c];
           uq[q] = u0 + dWx[v] * dx + dWy[v] * dy;
         }
-        o->phi[CV(o, b, v, j, i)] = limiter(o->sc.limiter, uq, u0, umin, umax);
+        /* Freeze_Limiter: a frozen block keeps its stored phi
+           (Linear_Reconstruction_LeastSquares, Euler2DQuadSingleBlock.cc:3572) */
+        if (!o->frozen) o->phi[CV(o, b, v, j, i)] = limiter(o->sc.limiter, uq, u0, umin, umax);
       }
     }
   } else {
@@ -786,17 +790,66 @@ static cst jface_flux(const e2d_oracle *o, int b, int i, int j) {
   return face_flux_n(o, wl, wr, nfaceN(o, b, i, j));
 }
 
+/* The explicit schemes' stage structure (dUdt_Multistage_Explicit and
+ * Update_Solution_Multistage_Explicit, Euler2DQuad.cc:1235-1342,
+ * Euler2DQuadSingleBlock.cc:5300-5350): the update coefficient of stage s
+ * (Runge_Kutta, CFD.cc:901-940; MultiStage_Optimally_Smoothing, CFD.cc:953-1031),
+ * the residual slot k_residual it fills, and how its residual starts: 0
+ * from zero, 1 from the stored slot-0 residual (the two-stage Runge-Kutta
+ * and predictor-corrector schemes), 2 from slot0 + 2 slot1 + 2 slot2 (RK4's
+ * last stage). */
+static double stage_omega(const e2d_scheme *sc, int s) {
+  const int n = sc->n_stage;
+  double beta = 1.0;
+  if (sc->time_integration == E2D_TIME_OPTIMAL_SMOOTHING) {
+    static const double z[7][6] = {{0}, {1.0}, {1.0, 0.3333}, {1.50, 0.1481, 0.4000},
+                                   {2.00, 0.0833, 0.2069, 0.4265}, {2.50, 0.0533, 0.1263, 0.2375, 0.4414},
+                                   {3.00, 0.0370, 0.0851, 0.1521, 0.2562, 0.4512}};
+    static const double l[7][6] = {{0}, {1.0}, {0.4693, 0.4242}, {0.6936, 0.1918, 0.4929},
+                                   {0.9214, 0.1084, 0.2602, 0.5052}, {1.1508, 0.0695, 0.1602, 0.2898, 0.5060},
+                                   {1.3805, 0.0482, 0.1085, 0.1885, 0.3050, 0.5063}};
+    const double *t = sc->limiter == E2D_LIMITER_ZERO ? z[n] : l[n];
+    beta = t[0];
+    if (s < n) beta = t[s] * beta;
+    return beta;
+  }
+  if (n == 2 && s == 2) beta = HALF * beta;
+  if (n == 4) {
+    if (s == 1 || s == 2) beta = HALF * beta;
+    if (s == 4) beta = beta / 6.0;
+  }
+  if (n == 5) {
+    static const double f[4] = {0.059, 0.14, 0.273, 0.5};
+    if (s <= 4) beta *= f[s - 1];
+  }
+  return beta;
+}
+static int stage_slot(const e2d_scheme *sc, int s) {
+  return (sc->time_integration != E2D_TIME_OPTIMAL_SMOOTHING && sc->n_stage == 4 && s < 4) ? s - 1 : 0;
+}
+static int stage_start(const e2d_scheme *sc, int s) {
+  if (s == 1 || sc->time_integration == E2D_TIME_OPTIMAL_SMOOTHING) return 0;
+  if (sc->n_stage == 2) return 1;
+  if (sc->n_stage == 4 && s == 4) return 2;
+  return 0;
+}
+static double *slot_array(e2d_oracle *o, int slot) {
+  return slot == 0 ? o->dUdt : (slot == 1 ? o->dUdt1 : o->dUdt2);
+}
+
 /* Residual of one block: dUdt_Residual_Evaluation (stage == 0,
  * src_2D/Euler2D/Euler2DQuad.cc:814-1227) or stage `stage` of
- * dUdt_Multistage_Explicit (:1235-1727; RK with N_Stage 1 or 2, k_residual 0).
- * Each interior cell accumulates, in the reference's loop order,
- * D + west - east + south - north, with D = 0 except at RK2 stage 2. */
+ * dUdt_Multistage_Explicit (:1235-1727).  Each interior cell accumulates, in
+ * the reference's loop order, D + west - east + south - north into the
+ * stage's residual slot, D per stage_start. */
 static void residual_block(e2d_oracle *o, int b, int stage) {
   const int ICl = o->ICl, ICu = o->ICu, JCl = o->JCl, JCu = o->JCu;
   int i, j, v;
   cst *Fi = (cst *)malloc(sizeof(cst) * (size_t)(ICu - ICl + 2) * (JCu - JCl + 1));
   cst *Fj = (cst *)malloc(sizeof(cst) * (size_t)(ICu - ICl + 1) * (JCu - JCl + 2));
   const int ni = ICu - ICl + 2, nj = JCu - JCl + 2;
+  const int start = stage ? stage_start(&o->sc, stage) : 0;
+  double *R = slot_array(o, stage ? stage_slot(&o->sc, stage) : 0);
   for (j = JCl - 1; j <= JCu + 1; ++j)
     for (i = ICl - 1; i <= ICu + 1; ++i) lsq_cell(o, b, i, j);
   if (stage == 1) {
@@ -813,7 +866,7 @@ static void residual_block(e2d_oracle *o, int b, int stage) {
     for (i = 0; i < o->NCi; ++i) {
       const int interior = (i >= ICl && i <= ICu && j >= JCl && j <= JCu);
       if (!interior) {
-        for (v = 0; v < 4; ++v) o->dUdt[CV(o, b, v, j, i)] = 0.0;
+        for (v = 0; v < 4; ++v) R[CV(o, b, v, j, i)] = 0.0;
         continue;
       }
       {
@@ -829,7 +882,10 @@ static void residual_block(e2d_oracle *o, int b, int stage) {
         const double fwv[4] = {fw.d, fw.mx, fw.my, fw.E}, fev[4] = {fe.d, fe.mx, fe.my, fe.E};
         const double fsv[4] = {fs.d, fs.mx, fs.my, fs.E}, fnv[4] = {fn.d, fn.mx, fn.my, fn.E};
         for (v = 0; v < 4; ++v) {
-          double d = (stage == 2) ? o->dUdt[CV(o, b, v, j, i)] : 0.0;
+          const size_t q = CV(o, b, v, j, i);
+          double d = 0.0;
+          if (start == 1) d = o->dUdt[q];
+          if (start == 2) d = o->dUdt[q] + 2.0 * o->dUdt1[q] + 2.0 * o->dUdt2[q];
           if (stage) {
             d += k * fwv[v] * lW / A;
             d -= k * fev[v] * lE / A;
@@ -841,7 +897,7 @@ static void residual_block(e2d_oracle *o, int b, int stage) {
             d += fsv[v] * lS / A;
             d -= fnv[v] * lN / A;
           }
-          o->dUdt[CV(o, b, v, j, i)] = d;
+          R[q] = d;
         }
       }
     }
@@ -1020,16 +1076,46 @@ static double cfl_block(e2d_oracle *o, int b) {
   return dtMin;
 }
 
+/* Residual_Smoothing (src_2D/Euler2D/Euler2DQuadSingleBlock.cc:4521-4563):
+ * Gauss-Seidel sweeps in lexicographic order over the cells one away from
+ * the block edges, on a copy whose other entries are zero (the reference's
+ * second residual slot, never written on this path); the result replaces
+ * the residual there. */
+static void residual_smoothing_block(e2d_oracle *o, int b, double *R) {
+  const int il = o->ICl + 1, iu = o->ICu - 1, jl = o->JCl + 1, ju = o->JCu - 1;
+  const double eps = o->sc.rs_epsilon;
+  const size_t n = 4 * (size_t)o->NCi * o->NCj;
+  double *S = (double *)calloc(n, sizeof(double));
+  int i, j, v, it;
+  /* S indexed as R of block 0 */
+  for (v = 0; v < 4; ++v)
+    for (j = jl; j <= ju; ++j)
+      for (i = il; i <= iu; ++i) S[CV(o, 0, v, j, i)] = R[CV(o, b, v, j, i)];
+  for (it = 1; it <= o->sc.rs_iterations; ++it)
+    for (j = jl; j <= ju; ++j)
+      for (i = il; i <= iu; ++i)
+        for (v = 0; v < 4; ++v)
+          S[CV(o, 0, v, j, i)] = (R[CV(o, b, v, j, i)] +
+                                  eps * (S[CV(o, 0, v, j - 1, i)] + S[CV(o, 0, v, j, i - 1)] +
+                                         S[CV(o, 0, v, j, i + 1)] + S[CV(o, 0, v, j + 1, i)])) /
+                                 (1.0 + 4.0 * eps);
+  for (v = 0; v < 4; ++v)
+    for (j = jl; j <= ju; ++j)
+      for (i = il; i <= iu; ++i) R[CV(o, b, v, j, i)] = S[CV(o, 0, v, j, i)];
+  free(S);
+}
+
 /* Update_Solution_Multistage_Explicit for RK (src_2D/Euler2D/Euler2DQuadSingleBlock.cc:5300-5507)
  * and Runge_Kutta (src_2D/CFD/CFD.cc:901-937).  Returns 0 or 1 + the linear
  * cell index of the failing cell. */
 static int update_block(e2d_oracle *o, int b, int stage) {
-  const double omega = (o->sc.n_stage == 2 && stage == 2) ? HALF * 1.0 : 1.0;
+  const double omega = stage_omega(&o->sc, stage);
+  double *R = slot_array(o, stage_slot(&o->sc, stage));
   int i, j, v, nr;
   for (j = o->JCl; j <= o->JCu; ++j)
     for (i = o->ICl; i <= o->ICu; ++i) {
       const size_t c = SC(o, b, j, i);
-      cst uo = getU(o, o->Uo, b, i, j), du = getU(o, o->dUdt, b, i, j), u;
+      cst uo = getU(o, o->Uo, b, i, j), du = getU(o, R, b, i, j), u;
       u.d = uo.d + omega * du.d; u.mx = uo.mx + omega * du.mx;
       u.my = uo.my + omega * du.my; u.E = uo.E + omega * du.E;
       if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) {
@@ -1044,7 +1130,7 @@ static int update_block(e2d_oracle *o, int b, int stage) {
             u.my = uo.my + omega * du.my; u.E = uo.E + omega * du.E;
             if (u.d > 0.0 && u.E > 0.0 && e_of_U(u) > 0.0) break;
           }
-          putU(o, o->dUdt, b, i, j, du);
+          putU(o, R, b, i, j, du);
           if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) return 1 + (int)c;
         }
       }
@@ -1061,7 +1147,7 @@ e2d_oracle *e2d_oracle_create(const e2d_blocks_desc *d, const e2d_scheme *sc, in
   size_t ncell, nnode;
   if (err) *err = 0;
   if (!d || !sc || d->nblk < 1 || d->nci < 2 || d->ncj < 2 || d->ng != 2 ||
-      (sc->n_stage != 1 && sc->n_stage != 2) || sc->flux < E2D_FLUX_GODUNOV || sc->flux > E2D_FLUX_AUSMPLUS ||
+      sc->n_stage < 1 || sc->n_stage > 6 || sc->flux < E2D_FLUX_GODUNOV || sc->flux > E2D_FLUX_AUSMPLUS ||
       sc->flux == 7) {
     if (err) *err = E2D_ERR_ARG;
     return NULL;
@@ -1096,6 +1182,8 @@ e2d_oracle *e2d_oracle_create(const e2d_blocks_desc *d, const e2d_scheme *sc, in
   o->U = (double *)calloc(4 * ncell, sizeof(double));
   o->Uo = (double *)calloc(4 * ncell, sizeof(double));
   o->dUdt = (double *)calloc(4 * ncell, sizeof(double));
+  o->dUdt1 = (double *)calloc(4 * ncell, sizeof(double));
+  o->dUdt2 = (double *)calloc(4 * ncell, sizeof(double));
   o->dWdx = (double *)calloc(4 * ncell, sizeof(double));
   o->dWdy = (double *)calloc(4 * ncell, sizeof(double));
   o->phi = (double *)calloc(4 * ncell, sizeof(double));
@@ -1116,6 +1204,7 @@ void e2d_oracle_destroy(e2d_oracle *o) {
   free(o->X); free(o->Y); free(o->wow); free(o->woe); free(o->wos); free(o->won);
   free(o->xc); free(o->yc); free(o->A); free(o->dt);
   free(o->W); free(o->U); free(o->Uo); free(o->dUdt); free(o->dWdx); free(o->dWdy); free(o->phi);
+  free(o->dUdt1); free(o->dUdt2);
   free(o);
 }
 
@@ -1125,6 +1214,8 @@ int e2d_oracle_set_state(e2d_oracle *o, const double *W) {
   for (b = 0; b < o->nblk; ++b)
     for (j = 0; j < o->NCj; ++j)
       for (i = 0; i < o->NCi; ++i) putU(o, o->U, b, i, j, U_of_W(o, getW(o, o->W, b, i, j)));
+  o->frozen = 0;
+  o->first = 1;
   return 0;
 }
 
@@ -1194,9 +1285,15 @@ int e2d_oracle_rk_steps(e2d_oracle *o, int n_steps, double *hist) {
        rooted again by the solver loop (Euler2DQuadSolvers.cc:690-693) */
       hist[4 * n] = dtmin; hist[4 * n + 1] = l1; hist[4 * n + 2] = sqrt(sqr(sqrt(l2))); hist[4 * n + 3] = lmax;
     }
+    /* limiter freezing at the head of every step but a run's first
+       (Euler2DQuadSolvers.cc:794-803) */
+    if (!o->first && o->sc.freeze_limiter && sqrt(sqr(sqrt(l2))) <= o->sc.freeze_level) o->frozen = 1;
+    o->first = 0;
     for (stage = 1; stage <= o->sc.n_stage; ++stage) {
       e2d_oracle_fill_ghosts(o);
       for (b = 0; b < o->nblk; ++b) residual_block(o, b, stage);
+      if (o->sc.rs_epsilon > 0.0)
+        for (b = 0; b < o->nblk; ++b) residual_smoothing_block(o, b, slot_array(o, stage_slot(&o->sc, stage)));
       for (b = 0; b < o->nblk; ++b) {
         err = update_block(o, b, stage);
         if (err) return err;

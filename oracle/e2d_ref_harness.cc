@@ -71,6 +71,9 @@ struct Case {
   int nblk, nci, ncj, ng, NCi, NCj, NNi, NNj;
   int limiter, flux, n_stage, local_dt, time_accurate, nbi, nbj, periodic;
   double cfl;
+  // version 2: scheme, residual smoothing and limiter freezing
+  int time_integration = 0, rs_iterations = 2, freeze_limiter = 0;
+  double rs_epsilon = 0.0, freeze_level = 1e-4;
   std::vector<BlockData> data;
 };
 
@@ -85,8 +88,14 @@ void read_case(const char* path, Case& c) {
   int hdr[2], dims[4], opts[8];
   double dopts[4];
   rd(f, hdr, 2);
-  if (hdr[0] != 0x43443245 || hdr[1] != 1) { fprintf(stderr, "bad case file\n"); exit(2); }
+  if (hdr[0] != 0x43443245 || (hdr[1] != 1 && hdr[1] != 2)) { fprintf(stderr, "bad case file\n"); exit(2); }
   rd(f, dims, 4); rd(f, opts, 8); rd(f, dopts, 4);
+  if (hdr[1] == 2) {
+    int opts2[4];
+    rd(f, opts2, 4);
+    c.time_integration = opts2[0]; c.rs_iterations = opts2[1]; c.freeze_limiter = opts2[2];
+    c.rs_epsilon = dopts[1]; c.freeze_level = dopts[2];
+  }
   c.nblk = dims[0]; c.nci = dims[1]; c.ncj = dims[2]; c.ng = dims[3];
   c.NCi = c.nci + 2 * c.ng; c.NCj = c.ncj + 2 * c.ng; c.NNi = c.NCi + 1; c.NNj = c.NCj + 1;
   c.limiter = opts[0]; c.flux = opts[1]; c.n_stage = opts[2]; c.local_dt = opts[3];
@@ -115,8 +124,14 @@ void set_input(const Case& c, Euler2D_Input_Parameters& IP) {
   IP.i_Reconstruction = RECONSTRUCTION_LEAST_SQUARES;
   IP.i_Limiter = c.limiter;
   IP.i_Flux_Function = c.flux;
-  IP.i_Time_Integration = TIME_STEPPING_EXPLICIT_RUNGE_KUTTA;
+  // scheme code 0 runs as the Runge-Kutta family (N_Stage 1 or 2)
+  IP.i_Time_Integration = c.time_integration == 0 ? TIME_STEPPING_EXPLICIT_RUNGE_KUTTA : c.time_integration;
   IP.N_Stage = c.n_stage;
+  IP.Residual_Smoothing = c.rs_epsilon > 0.0 ? 1 : 0;
+  IP.Residual_Smoothing_Epsilon = c.rs_epsilon;
+  IP.Residual_Smoothing_Gauss_Seidel_Iterations = c.rs_iterations;
+  IP.Freeze_Limiter = c.freeze_limiter;
+  IP.Freeze_Limiter_Residual_Level = c.freeze_level;
   IP.CFL_Number = c.cfl;
   IP.Local_Time_Stepping = c.local_dt ? SCALAR_LOCAL_TIME_STEPPING : GLOBAL_TIME_STEPPING;
   IP.Time_Accurate = c.time_accurate;
@@ -174,6 +189,7 @@ struct RefSet {
   AdaptiveBlock2D_List Local;
   Euler2D_Quad_Block* Soln;
   std::vector<int> order;
+  bool first_step = true;
 };
 
 void build_reference_blocks(const Case& c, RefSet& R) {
@@ -236,6 +252,8 @@ int explicit_step_reference(RefSet& R, StepLog& log) {
   l2 = sqrt(sqr(l2));
   double lmax = Max_Norm_Residual(R.Soln, R.Local);
   log.dt = dTime; log.l1 = l1; log.l2 = l2; log.lmax = lmax;
+  // limiter freezing (Euler2DQuadSolvers.cc:794-803)
+  if (!R.first_step && IP.Freeze_Limiter && l2 <= IP.Freeze_Limiter_Residual_Level) Freeze_Limiters(R.Soln, R.Local);
   for (int stage = 1; stage <= IP.N_Stage; ++stage) {
     int err = Send_All_Messages(R.Soln, R.Local, NUM_VAR_EULER2D, OFF);
     if (err) return err;
@@ -245,9 +263,11 @@ int explicit_step_reference(RefSet& R, StepLog& log) {
     err = Send_Conservative_Flux_Corrections(R.Soln, R.Local, NUM_VAR_EULER2D);
     if (err) return err;
     Apply_Boundary_Flux_Corrections_Multistage_Explicit(R.Soln, R.Local, IP, stage);
+    if (IP.Residual_Smoothing) Residual_Smoothing(R.Soln, R.Local, IP, stage);
     err = Update_Solution_Multistage_Explicit(R.Soln, R.Local, IP, stage);
     if (err) return err;
   }
+  R.first_step = false;
   return 0;
 }
 

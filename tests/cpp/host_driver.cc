@@ -43,6 +43,8 @@ static bool read_case(const char* path, std::vector<Euler2D_Quad_Block>& blocks,
   double dopts[4];
   bool ok = fread(hdr, 4, 2, f) == 2 && fread(dims, 4, 4, f) == 4 && fread(opts, 4, 8, f) == 8 &&
             fread(dopts, 8, 4, f) == 4;
+  int opts2[4] = {0, 2, 0, 0};
+  if (ok && hdr[1] == 2) ok = fread(opts2, 4, 4, f) == 4;  // version 2: scheme extras
   const int nblk = dims[0], nci = dims[1], ncj = dims[2], ng = dims[3];
   const int NCi = nci + 2 * ng, NCj = ncj + 2 * ng, NNi = NCi + 1, NNj = NCj + 1;
   IP.Number_of_Blocks_Idir = opts[5];

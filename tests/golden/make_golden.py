@@ -99,8 +99,9 @@ def case_arrays(bs):
     d = {f.name: getattr(bs, f.name) for f in dataclasses.fields(bs)
          if isinstance(getattr(bs, f.name), np.ndarray)}
     sc = bs.scheme
-    d["scheme"] = np.array([sc.limiter, sc.flux, sc.n_stage, sc.local_dt, sc.precision], np.int32)
-    d["scheme_f"] = np.array([sc.cfl, sc.gamma])
+    d["scheme"] = np.array([sc.limiter, sc.flux, sc.n_stage, sc.local_dt, sc.precision, sc.time_integration,
+                            sc.rs_iterations, sc.freeze_limiter], np.int32)
+    d["scheme_f"] = np.array([sc.cfl, sc.gamma, sc.rs_epsilon, sc.freeze_level])
     d["dims"] = np.array([bs.nci, bs.ncj, bs.ng], np.int32)
     return d
 
@@ -121,6 +122,8 @@ def golden_cases():
                                  scheme=cases.Scheme(limiter=cases.LIMITER_BARTH_JESPERSEN, local_dt=0))
     bump_m14 = cases.bump_channel(nbi=6, nbj=2, nci=16, ncj=16, mach=1.4, h=0.04,
                                   scheme=cases.Scheme(limiter=cases.LIMITER_ZERO, local_dt=1))
+    ch_ms = cases.channel(nbi=2, nbj=2, nci=12, ncj=10, seed=9,
+                          scheme=cases.Scheme(limiter=cases.LIMITER_VENKATAKRISHNAN, cfl=0.8, n_stage=4, local_dt=1))
     return [
         ("residual_box_2x2x8", small_box, "residual", 0),
         ("residual_box_4x4x32", box, "residual", 0),
@@ -139,6 +142,27 @@ def golden_cases():
         ("nks_bump_m14_converged", bump_m14, "nks", (30, 30, 120, 10.0, 1e-10, 0.1)),
         # the same solve with the HLLE flux in the residual
         ("nks_bump_m14_hlle", with_flux(bump_m14, cases.FLUX_HLLE), "nks", (30, 30, 120, 10.0, 1e-10, 0.1)),
+    ] + [
+        # the other explicit schemes (optimally smoothing multistage, RK4, RK5),
+        # implicit residual smoothing and limiter freezing
+        (name, dataclasses.replace(ch_ms, scheme=dataclasses.replace(ch_ms.scheme, **kw)), "explicit", steps)
+        for name, kw, steps in (
+            ("explicit_os4_channel_30", dict(time_integration=cases.TIME_OPTIMAL_SMOOTHING, n_stage=4), 30),
+            ("explicit_os5_zero_channel_30", dict(time_integration=cases.TIME_OPTIMAL_SMOOTHING, n_stage=5,
+                                                  limiter=cases.LIMITER_ZERO), 30),
+            ("explicit_os2_global_channel_30", dict(time_integration=cases.TIME_OPTIMAL_SMOOTHING, n_stage=2,
+                                                    local_dt=0, cfl=0.4), 30),
+            ("explicit_rk4_channel_20", dict(time_integration=cases.TIME_RUNGE_KUTTA, n_stage=4, local_dt=0), 20),
+            ("explicit_rk5_channel_20", dict(time_integration=cases.TIME_RUNGE_KUTTA, n_stage=5), 20),
+            ("explicit_os3_smoothing_channel_30", dict(time_integration=cases.TIME_OPTIMAL_SMOOTHING, n_stage=3,
+                                                       rs_epsilon=0.125, rs_iterations=2), 30),
+            ("explicit_pc_smoothing_channel_30", dict(time_integration=cases.TIME_PREDICTOR_CORRECTOR, n_stage=2,
+                                                      rs_epsilon=0.25, rs_iterations=1, cfl=0.6), 30),
+            ("explicit_os4_freeze_channel_30", dict(time_integration=cases.TIME_OPTIMAL_SMOOTHING, n_stage=4,
+                                                    freeze_limiter=1, freeze_level=0.0463), 30),
+            ("explicit_os5_smoothing_freeze_channel_30", dict(
+                time_integration=cases.TIME_OPTIMAL_SMOOTHING, n_stage=5, rs_epsilon=0.125, rs_iterations=2,
+                freeze_limiter=1, freeze_level=0.0484), 30))
     ] + [
         # every other flux function: a supersonic curvilinear residual, explicit
         # steps in the subsonic channel with fixed inflow and reflecting walls,

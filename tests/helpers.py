@@ -63,6 +63,10 @@ def load(name):
     scheme = cases.Scheme(limiter=int(sc[0]), flux=int(sc[1]), n_stage=int(sc[2]),
                           local_dt=int(sc[3]), precision=int(sc[4]), cfl=float(scf[0]),
                           gamma=float(scf[1]))
+    if len(sc) > 5:  # time integration, residual smoothing, limiter freezing
+        scheme = cases.Scheme(**{**scheme.__dict__, "time_integration": int(sc[5]), "rs_iterations": int(sc[6]),
+                                 "freeze_limiter": int(sc[7]), "rs_epsilon": float(scf[2]),
+                                 "freeze_level": float(scf[3])})
     bs = cases.BlockSet(nci, ncj, z["neighbour"], z["bc_w"], z["bc_e"], z["bc_s"], z["bc_n"],
                         z["node_x"], z["node_y"], z["wo_w"], z["wo_e"], z["wo_s"], z["wo_n"],
                         z["W"], scheme, name, ng).contiguous()

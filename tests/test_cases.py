@@ -42,4 +42,4 @@ def test_case_file_roundtrip_size(tmp_path):
     cases.write_case(str(p), bs)
     per_block = (8 + 2 * bs.NCj + 2 * bs.NCi) * 4 + 8 * (2 * (bs.NCi + 1) * (bs.NCj + 1)
                                                            + 8 * bs.NCj + 8 * bs.NCi + 4 * bs.NCi * bs.NCj)
-    assert p.stat().st_size == 8 + 16 + 32 + 32 + bs.nblk * per_block
+    assert p.stat().st_size == 8 + 16 + 32 + 32 + 16 + bs.nblk * per_block

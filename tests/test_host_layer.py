@@ -46,8 +46,8 @@ Number_of_Blocks_Jdir =
 Number_of_Ghost_Cells =
 2
 # keywords of the reference outside this path are skipped
-Residual_Smoothing_Epsilon =
-0.125
+Number_of_Initial_Mesh_Refinements =
+0
    Mach_Number =
 0.5
 Pressure =
@@ -92,7 +92,7 @@ def test_deck_parses_and_builds_the_blocks(driver, tmp_path):
     deck = write_deck(tmp_path / "box.in")
     case = str(tmp_path / "box.case")
     out = subprocess.run([driver, "parse", deck, case], capture_output=True, text=True, check=True).stdout.split()
-    assert out[0] == "ok" and int(out[1]) == 1  # Residual_Smoothing_Epsilon
+    assert out[0] == "ok" and int(out[1]) == 1  # Number_of_Initial_Mesh_Refinements
     got = cases.read_case(case)
     want, (rho, u, p) = expected_blocks()
     assert float(out[2]) == rho and float(out[3]) == u and float(out[4]) == p
