@@ -31,12 +31,17 @@
 //   e2d_ref_harness explicit CASE NSTEPS OUT
 //   e2d_ref_harness nks      CASE OUT MAX_NEWTON GMRES_RESTART MAX_GMRES CFL0 OVERALL_TOL [GMRES_TOL]
 //   e2d_ref_harness time     CASE NSTEPS THREADS      (prints one JSON line)
+//   e2d_ref_harness restart_write CASE PREFIX NSTEPS TIME  (Write_QuadTree + Write_Restart_Solution)
+//   e2d_ref_harness restart_read  CASE PREFIX OUT [GRIDFILE]
+//   e2d_ref_harness grid_write    CASE GRIDFILE
+//   e2d_ref_harness solve    DECK                      (Euler2DQuadSolver in batch mode)
 //
 // Case file (little endian), shared with cffc_b200/cases.py:
-//   int32 magic 0x43443245, version 1
+//   int32 magic 0x43443245, version 1 or 2
 //   int32 nblk, nci, ncj, ng
 //   int32 limiter, flux, n_stage, local_dt, time_accurate, nbi, nbj, periodic
-//   f64   cfl, 0, 0, 0
+//   f64   cfl, rs_epsilon, freeze_level, 0         (version 1: cfl, 0, 0, 0)
+//   int32 time_integration, rs_iterations, freeze_limiter, 0   (version 2 only)
 //   per block (b = bj * nbi + bi):
 //     int32 neighbour[8]           W, E, S, N, SW, SE, NW, NE (-1 = none)
 //     int32 bcW[NCj], bcE[NCj], bcS[NCi], bcN[NCi]      reference BC codes
