@@ -73,10 +73,17 @@ class NksParams(C.Structure):
     """e2d_nks_params: the NKS_Input_Parameters fields the solver reads
     (NewtonKrylovSchwarz2D/NKSInput2D.h:125-172 for the defaults)."""
     _fields_ = [("max_newton", C.c_int32), ("gmres_restart", C.c_int32), ("max_gmres", C.c_int32),
-                ("reserved", C.c_int32), ("overall_tol", C.c_double), ("cfl0", C.c_double),
+                ("block_preconditioner", C.c_int32), ("overall_tol", C.c_double), ("cfl0", C.c_double),
                 ("gmres_tol_initial", C.c_double), ("gmres_tol_final", C.c_double),
                 ("epsilon0", C.c_double), ("min_ratio", C.c_double),
-                ("l2_reference", C.POINTER(C.c_double))]
+                ("l2_reference", C.POINTER(C.c_double)), ("ilu_level_of_fill", C.c_int32),
+                ("jacobian_order", C.c_int32)]
+
+
+PRECON_BLOCK_JACOBI = 0    # GMRES_Block_Preconditioner Diagonal
+PRECON_BLOCK_ILUK = 1      # GMRES_Block_Preconditioner ILUK
+JACOBIAN_FIRST_ORDER_HLLE = 0
+JACOBIAN_SOURCE_TERMS_ONLY = 1
 
 
 class NksStep(C.Structure):
@@ -89,9 +96,14 @@ class NksStep(C.Structure):
 
 def nks_params(max_newton: int, gmres_restart: int = 30, max_gmres: int = 100, overall_tol: float = 1e-5,
                cfl0: float = 1.0, gmres_tol: float = 1e-5, gmres_tol_final: float | None = None,
-               epsilon0: float = 1e-6, min_ratio: float = 1e-10) -> NksParams:
+               epsilon0: float = 1e-6, min_ratio: float = 1e-10, ilu_level: int | None = None,
+               jacobian_order: int = 0) -> NksParams:
+    """ilu_level None: block Jacobi (the reference's default); k: ILU(k)."""
     p = NksParams()
-    p.max_newton, p.gmres_restart, p.max_gmres, p.reserved = max_newton, gmres_restart, max_gmres, 0
+    p.max_newton, p.gmres_restart, p.max_gmres = max_newton, gmres_restart, max_gmres
+    p.block_preconditioner = PRECON_BLOCK_JACOBI if ilu_level is None else PRECON_BLOCK_ILUK
+    p.ilu_level_of_fill = 0 if ilu_level is None else ilu_level
+    p.jacobian_order = jacobian_order
     p.overall_tol, p.cfl0, p.gmres_tol_initial = overall_tol, cfl0, gmres_tol
     p.gmres_tol_final = gmres_tol if gmres_tol_final is None else gmres_tol_final
     p.epsilon0, p.min_ratio = epsilon0, min_ratio
@@ -219,6 +231,19 @@ class Handle:
         rc = self._call("nks", C.byref(params), steps, C.byref(n))
         hist = [{f: getattr(steps[k], f) for f, _ in NksStep._fields_ if f != "pad"} for k in range(n.value)]
         return rc, hist
+
+    def block_precon_apply(self, params: NksParams, cfl: float, v: np.ndarray) -> np.ndarray:
+        """e2d_block_precon_apply: z = M^-1 v with the Newton step's
+        preconditioner at the current state (dt = cfl x the CFL step); v, z
+        in the GMRES layout [nblk][NCj][NCi][4]."""
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        z = np.zeros_like(v)
+        self.lib.e2d_block_precon_apply.argtypes = [C.c_void_p, C.POINTER(NksParams), C.c_double,
+                                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        rc = self.lib.e2d_block_precon_apply(self.h, C.byref(params), cfl, ptr(v), ptr(z))
+        if rc != 0:
+            raise RuntimeError(f"e2d_block_precon_apply failed: {rc}")
+        return z
 
     def status(self) -> int:
         return self.lib.e2d_status(self.h)

@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <vector>
 
 #include "e2d_geom.cuh"
@@ -446,10 +447,20 @@ __device__ bool invert4(double a[4][4]) {
   return true;
 }
 
+// normalize_Preconditioner_dFdU (Euler2D/Euler2DQuadNKS.h:115-137)
+__device__ __forceinline__ void normalize_block(double m[4][4], double ao) {
+  const double ia = 1.0 / ao, ia2 = 1.0 / (ao * ao), ia3 = 1.0 / (ao * ao * ao);
+  m[0][0] *= ia; m[0][3] *= ao;
+  m[1][0] *= ia2; m[1][1] *= ia; m[1][2] *= ia;
+  m[2][0] *= ia2; m[2][1] *= ia; m[2][2] *= ia;
+  m[3][0] *= ia3; m[3][1] *= ia2; m[3][2] *= ia2; m[3][3] *= ia;
+}
+
 // Diagonal block of the approximate Jacobian for each interior cell,
 // normalized (normalize_Preconditioner_dFdU, Euler2DQuadNKS.h:115-137) and
 // inverted: CENTER = -I / dt + (J_N + J_S + J_E + J_W) / A.
-__global__ void __launch_bounds__(128) precon_build_kernel(Blocks B, double* __restrict__ Minv, double ao) {
+// order E2D_JACOBIAN_SOURCE_TERMS_ONLY keeps -I / dt alone.
+__global__ void __launch_bounds__(128) precon_build_kernel(Blocks B, double* __restrict__ Minv, double ao, int order) {
   const long long n = (long long)B.nblk * B.nci * B.ncj;
   const int per = B.nci * B.ncj;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
@@ -465,6 +476,7 @@ __global__ void __launch_bounds__(128) precon_build_kernel(Blocks B, double* __r
 #pragma unroll
       for (int cc = 0; cc < 4; ++cc) acc[rr][cc] = 0.0;
     double nx, ny;
+    if (order == E2D_JACOBIAN_FIRST_ORDER_HLLE) {
     // N: the north face of the cell below, pointing into this cell
     nfaceN(B, b, i, j - 1, nx, ny);
     face_jacobian(wc, ldW(B, b, i, j - 1), nx, ny, glen(B, b, i, j, i + 1, j), B.g, B.gm1, B.gm1i, acc);
@@ -474,6 +486,7 @@ __global__ void __launch_bounds__(128) precon_build_kernel(Blocks B, double* __r
     face_jacobian(wc, ldW(B, b, i - 1, j), nx, ny, glen(B, b, i, j, i, j + 1), B.g, B.gm1, B.gm1i, acc);
     nfaceW(B, b, i + 1, j, nx, ny);
     face_jacobian(wc, ldW(B, b, i + 1, j), nx, ny, glen(B, b, i + 1, j, i + 1, j + 1), B.g, B.gm1, B.gm1i, acc);
+    }
     double xc, yc, A;
     quad_centroid(nodeX(B, b, i, j), nodeY(B, b, i, j), nodeX(B, b, i + 1, j), nodeY(B, b, i + 1, j),
                   nodeX(B, b, i + 1, j + 1), nodeY(B, b, i + 1, j + 1), nodeX(B, b, i, j + 1),
@@ -483,12 +496,10 @@ __global__ void __launch_bounds__(128) precon_build_kernel(Blocks B, double* __r
 #pragma unroll
     for (int rr = 0; rr < 4; ++rr)
 #pragma unroll
-      for (int cc = 0; cc < 4; ++cc) m[rr][cc] = (rr == cc ? -lhs : 0.0) + acc[rr][cc] / A;
-    const double ia = 1.0 / ao, ia2 = 1.0 / (ao * ao), ia3 = 1.0 / (ao * ao * ao);
-    m[0][0] *= ia; m[0][3] *= ao;
-    m[1][0] *= ia2; m[1][1] *= ia; m[1][2] *= ia;
-    m[2][0] *= ia2; m[2][1] *= ia; m[2][2] *= ia;
-    m[3][0] *= ia3; m[3][1] *= ia2; m[3][2] *= ia2; m[3][3] *= ia;
+      for (int cc = 0; cc < 4; ++cc)
+        m[rr][cc] = order == E2D_JACOBIAN_FIRST_ORDER_HLLE ? (rr == cc ? -lhs : 0.0) + acc[rr][cc] / A
+                                                            : (rr == cc ? -lhs : 0.0);
+    normalize_block(m, ao);
     if (!invert4(m)) set_status(B.status, 3, int(c));
     double* o = Minv + 16 * c;
 #pragma unroll
@@ -506,6 +517,8 @@ __global__ void identity_blocks_kernel(double* Minv, long long ncell) {
   }
 }
 
+#include "e2d_ilu.cuh"
+
 }  // namespace
 
 struct e2d_nks_state {
@@ -515,6 +528,11 @@ struct e2d_nks_state {
   int nper4 = 0;             // vector entries per block
   double* Uo = nullptr;      // [nblk][4][NCj][NCi]
   double* Minv = nullptr;    // [cells][16]
+  IluPattern ilu_pat;        // ILU(k) pattern and schedules (host copy)
+  IluDev ilu{};              // device copies, values and inverted diagonals
+  int ilu_level = -1;        // level the ILU arrays are built for (-1: none)
+  size_t ilu_smem = 0;       // dynamic shared memory of the apply (0: D.work)
+  std::vector<void*> ilu_allocs;
   double* bvec = nullptr;
   double* x = nullptr;
   double* V = nullptr;       // (m + 1) * n
@@ -525,6 +543,7 @@ struct e2d_nks_state {
   std::vector<cudaGraphExec_t> graphs;  // Arnoldi step j, captured on its second use
   std::vector<int> graph_uses;
   double graph_eps0 = -1.0;
+  int graph_ilu = -1;        // preconditioner kind the graphs were captured with
   double* eps = nullptr;     // [ncase]
   double* nrm = nullptr;     // [ncase]
   double* hcol = nullptr;    // [m + 2][ncase]
@@ -546,6 +565,7 @@ void nks_free(e2d_handle* h) {
   for (auto g : h->nks->graphs)
     if (g) cudaGraphExecDestroy(g);
   for (void* p : h->nks->allocs) cudaFree(p);
+  for (void* p : h->nks->ilu_allocs) cudaFree(p);
   if (h->nks->host) cudaFreeHost(h->nks->host);
   delete h->nks;
   h->nks = nullptr;
@@ -612,6 +632,88 @@ int grid_for(long long n) {
   long long g = (n + VT - 1) / VT;
   if (g > VGRID) g = VGRID;
   return int(g < 1 ? 1 : g);
+}
+
+// ILU(k) pattern, schedules and value arrays for the handle's block shape,
+// built once per level of fill.
+int ilu_setup(e2d_handle* h, int level) {
+  e2d_nks_state* s = h->nks;
+  if (s->ilu_level == level) return 0;
+  for (void* p : s->ilu_allocs) cudaFree(p);
+  s->ilu_allocs.clear();
+  s->ilu_level = -1;
+  IluPattern& P = s->ilu_pat;
+  if (!ilu_pattern(h->B.nci, h->B.ncj, level, P)) return E2D_ERR_NOMEM;
+  IluDev& D = s->ilu;
+  D = IluDev{};
+  D.nrow = P.nrow; D.nnz = P.nnz; D.nflev = P.nflev; D.nblev = P.nblev;
+  auto up = [&](const void* src, size_t bytes, void** dst) -> int {
+    void* q = nullptr;
+    if (cudaMalloc(&q, bytes ? bytes : 1) != cudaSuccess) return E2D_ERR_NOMEM;
+    s->ilu_allocs.push_back(q);
+    if (src && bytes && cudaMemcpy(q, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return E2D_ERR_CUDA;
+    *dst = q;
+    return 0;
+  };
+  const int nblk = h->B.nblk;
+  int rc;
+  void *a0, *a1, *a2, *a3, *a4, *a5, *a6, *a7, *a8, *a9, *v0, *v1;
+  if ((rc = up(P.row_ptr.data(), sizeof(int) * P.row_ptr.size(), &a0)) ||
+      (rc = up(P.nlow.data(), sizeof(int) * P.nlow.size(), &a1)) ||
+      (rc = up(P.col.data(), sizeof(int) * P.col.size(), &a2)) ||
+      (rc = up(P.fop_ptr.data(), sizeof(int) * P.fop_ptr.size(), &a3)) ||
+      (rc = up(P.fop.data(), sizeof(int2) * P.fop.size(), &a4)) ||
+      (rc = up(P.flev_ptr.data(), sizeof(int) * P.flev_ptr.size(), &a5)) ||
+      (rc = up(P.flev_rows.data(), sizeof(int) * P.flev_rows.size(), &a6)) ||
+      (rc = up(P.blev_ptr.data(), sizeof(int) * P.blev_ptr.size(), &a7)) ||
+      (rc = up(P.blev_rows.data(), sizeof(int) * P.blev_rows.size(), &a8)) ||
+      (rc = up(P.apos.data(), sizeof(int) * P.apos.size(), &a9)) ||
+      (rc = up(nullptr, sizeof(double) * 16 * size_t(P.nnz) * nblk, &v0)) ||
+      (rc = up(nullptr, sizeof(double) * 16 * size_t(P.nrow) * nblk, &v1)))
+    return rc;
+  D.row_ptr = static_cast<int*>(a0); D.nlow = static_cast<int*>(a1); D.col = static_cast<int*>(a2);
+  D.fop_ptr = static_cast<int*>(a3); D.fop = static_cast<int2*>(a4);
+  D.flev_ptr = static_cast<int*>(a5); D.flev_rows = static_cast<int*>(a6);
+  D.blev_ptr = static_cast<int*>(a7); D.blev_rows = static_cast<int*>(a8); D.apos = static_cast<int*>(a9);
+  D.vals = static_cast<double*>(v0); D.dinv = static_cast<double*>(v1);
+  // a block's vector in shared memory when it fits, else a global work array
+  const size_t smem = sizeof(double) * 4 * size_t(P.nrow);
+  int dev = 0, optin = 0;
+  E2D_CK(cudaGetDevice(&dev));
+  E2D_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (smem <= size_t(optin)) {
+    E2D_CK(cudaFuncSetAttribute(ilu_apply_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    s->ilu_smem = smem;
+  } else {
+    void* w;
+    if ((rc = up(nullptr, sizeof(double) * 4 * size_t(P.nrow) * nblk, &w))) return rc;
+    D.work = static_cast<double*>(w);
+    s->ilu_smem = 0;
+  }
+  s->ilu_level = level;
+  return 0;
+}
+
+bool use_ilu(const e2d_nks_params& p) { return p.block_preconditioner == E2D_PRECON_BLOCK_ILUK; }
+
+// The preconditioner at the current state and dt (Update_Jacobian_and_Preconditioner).
+int precon_build(e2d_handle* h, const e2d_nks_params& p, double ao, const Blocks& B) {
+  e2d_nks_state* s = h->nks;
+  const long long nint = (long long)h->B.nblk * h->B.nci * h->B.ncj;
+  if (use_ilu(p)) {
+    int rc;
+    if ((rc = ilu_setup(h, p.ilu_level_of_fill))) return rc;
+    E2D_CK(cudaMemsetAsync(s->ilu.vals, 0, sizeof(double) * 16 * size_t(s->ilu.nnz) * h->B.nblk, h->stream));
+    ilu_assemble_kernel<<<grid_for(nint) * 2, 128, 0, h->stream>>>(B, s->ilu, ao,
+                                                                   p.jacobian_order == E2D_JACOBIAN_FIRST_ORDER_HLLE);
+    E2D_CK(cudaGetLastError());
+    ilu_factor_kernel<<<h->B.nblk, ILU_THREADS, 0, h->stream>>>(B, s->ilu);
+    E2D_CK(cudaGetLastError());
+    return 0;
+  }
+  precon_build_kernel<<<grid_for(nint) * 2, 128, 0, h->stream>>>(B, s->Minv, ao, p.jacobian_order);
+  E2D_CK(cudaGetLastError());
+  return 0;
 }
 
 // The per-case active mask the kernels see (and the stage kernel through
@@ -717,11 +819,22 @@ void apply_rotation(double& dx, double& dy, double cs, double sn) {
   dx = t;
 }
 
+// z = M^-1 v with the ILU factors, every active block.
+int ilu_apply(e2d_handle* h, const double* v, double* z) {
+  e2d_nks_state* s = h->nks;
+  if (s->ilu_smem)
+    ilu_apply_kernel<true><<<h->B.nblk, ILU_THREADS, s->ilu_smem, h->stream>>>(act(h), s->ilu, v, z);
+  else
+    ilu_apply_kernel<false><<<h->B.nblk, ILU_THREADS, 0, h->stream>>>(act(h), s->ilu, v, z);
+  E2D_CK(cudaGetLastError());
+  return 0;
+}
+
 // One Arnoldi step j of GMRES (GMRES2D.h:1020-1250): z_j = M^-1 v_j with
 // eps = eps0 / ||z_j||, v_{j+1} = J z_j, modified Gram-Schmidt against
 // v_0..v_j into the Hessenberg column, ||v_{j+1}||, v_{j+1} /= it.  Only
 // enqueues device work (it is captured into a graph per j).
-int arnoldi_step(e2d_handle* h, int j, double eps0, const Norm4& nm) {
+int arnoldi_step(e2d_handle* h, int j, double eps0, const Norm4& nm, bool ilu) {
   e2d_nks_state* s = h->nks;
   const int C = s->ncase;
   const long long n = s->n;
@@ -729,9 +842,14 @@ int arnoldi_step(e2d_handle* h, int j, double eps0, const Norm4& nm) {
   double* Vj = s->V + size_t(j) * n;
   double* Vn = s->V + size_t(j + 1) * n;
   double* Zj = s->Z + size_t(j) * n;
-  precon_apply_kernel<<<h->B.nblk * s->ch_cell, VT, 0, h->stream>>>(
-      s->Minv, Vj, Zj, h->B.NCi * h->B.NCj, s->ch_cell, s->partial, s->counter, s->eps, eps0, act(h));
-  E2D_CK(cudaGetLastError());
+  if (ilu) {
+    if ((rc = ilu_apply(h, Vj, Zj))) return rc;
+    if ((rc = dot(h, Zj, Zj, s->eps, FIN_EPS, eps0))) return rc;
+  } else {
+    precon_apply_kernel<<<h->B.nblk * s->ch_cell, VT, 0, h->stream>>>(
+        s->Minv, Vj, Zj, h->B.NCi * h->B.NCj, s->ch_cell, s->partial, s->counter, s->eps, eps0, act(h));
+    E2D_CK(cudaGetLastError());
+  }
   if ((rc = matvec(h, Zj, Vn, nm))) return rc;
   // modified Gram-Schmidt (GMRES2D.h:1224-1240)
   for (int k = 0; k <= j; ++k) {
@@ -749,22 +867,23 @@ int arnoldi_step(e2d_handle* h, int j, double eps0, const Norm4& nm) {
 // about 2j + 8).  Every pointer the step reads is fixed for the life of the
 // work arrays; the per-case active mask and scalars are read from device
 // memory at run time.
-int run_arnoldi(e2d_handle* h, int j, double eps0, const Norm4& nm) {
+int run_arnoldi(e2d_handle* h, int j, double eps0, const Norm4& nm, bool ilu) {
   e2d_nks_state* s = h->nks;
-  if (s->graph_eps0 != eps0) {
+  if (s->graph_eps0 != eps0 || s->graph_ilu != int(ilu)) {
     for (auto& g : s->graphs)
       if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     std::fill(s->graph_uses.begin(), s->graph_uses.end(), 0);
     s->graph_eps0 = eps0;
+    s->graph_ilu = int(ilu);
   }
   if (s->graphs[j]) {
     E2D_CK(cudaGraphLaunch(s->graphs[j], h->stream));
     return 0;
   }
-  if (s->graph_uses[j]++ == 0) return arnoldi_step(h, j, eps0, nm);
+  if (s->graph_uses[j]++ == 0) return arnoldi_step(h, j, eps0, nm, ilu);
   cudaGraph_t g = nullptr;
   E2D_CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  const int rc = arnoldi_step(h, j, eps0, nm);
+  const int rc = arnoldi_step(h, j, eps0, nm, ilu);
   const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
   if (rc || e != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
@@ -833,7 +952,7 @@ int gmres(e2d_handle* h, const e2d_nks_params& p, const std::vector<double>& tol
     for (;;) {
       ++j;
       ++iters;
-      if ((rc = run_arnoldi(h, j, p.epsilon0, nm))) return rc;
+      if ((rc = run_arnoldi(h, j, p.epsilon0, nm, use_ilu(p)))) return rc;
       if ((rc = fetch(h, s->hcol, size_t(j + 2) * C, col.data()))) return rc;
       bool any = false, changed = false;
       for (int c = 0; c < C; ++c) {
@@ -895,6 +1014,12 @@ int gmres(e2d_handle* h, const e2d_nks_params& p, const std::vector<double>& tol
 
 static int nks_run(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, int* n_steps);
 
+static bool params_ok(const e2d_nks_params& p) {
+  return (p.block_preconditioner == E2D_PRECON_BLOCK_JACOBI || p.block_preconditioner == E2D_PRECON_BLOCK_ILUK) &&
+         p.ilu_level_of_fill >= 0 && p.ilu_level_of_fill <= 16 &&
+         (p.jacobian_order == E2D_JACOBIAN_FIRST_ORDER_HLLE || p.jacobian_order == E2D_JACOBIAN_SOURCE_TERMS_ONLY);
+}
+
 // The Newton-Krylov solve starts with the limiters unfrozen and never
 // freezes them (Evaluate_Limiters, NKS2D.h:90; its freezing code is
 // disabled): the solve runs without the freezing machinery.
@@ -911,7 +1036,7 @@ extern "C" int e2d_nks(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* his
 static int nks_run(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, int* n_steps) {
   if (!h || !p || p->max_newton < 0 || p->gmres_restart < 1 || p->gmres_restart > 500 || p->max_gmres < 1 ||
       !(p->epsilon0 > 0.0) || !(p->cfl0 > 0.0) || !(p->gmres_tol_initial > 0.0) || !(p->gmres_tol_final > 0.0) ||
-      !(p->min_ratio > 0.0)) {
+      !(p->min_ratio > 0.0) || !params_ok(*p)) {
     if (n_steps) *n_steps = 0;
     return E2D_ERR_ARG;
   }
@@ -993,8 +1118,7 @@ static int nks_run(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, i
     E2D_CK(cudaGetLastError());
     // Uo = U (ghosts included) and the preconditioner at Uo
     E2D_CK(cudaMemcpyAsync(s->Uo, B.U, sizeof(double) * 4 * h->ncell, cudaMemcpyDeviceToDevice, h->stream));
-    precon_build_kernel<<<grid_for(nint) * 2, 128, 0, h->stream>>>(act(h), s->Minv, ao);
-    E2D_CK(cudaGetLastError());
+    if ((rc = precon_build(h, *p, ao, act(h)))) return finish(rc);
     load_b_kernel<<<grid_for(nint), VT, 0, h->stream>>>(act(h), s->bvec, nm);
     E2D_CK(cudaGetLastError());
     if ((rc = gmres(h, *p, tol, on, nm, G))) return finish(rc);
@@ -1013,4 +1137,47 @@ static int nks_run(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, i
   }
   E2D_CK(cudaStreamSynchronize(h->stream));
   return finish(0);
+}
+
+// The Newton step's preconditioner alone (parity checks and callers that run
+// their own Krylov solver): dt as the Newton loop sets it, the block
+// preconditioner at the current state, z = M^-1 v.  Ghost rows are identity
+// rows, as in the reference's block matrix: ghost entries pass through.
+extern "C" int e2d_block_precon_apply(e2d_handle* h, const e2d_nks_params* p, double cfl, const double* v,
+                                      double* z) {
+  if (!h || !p || !v || !z || !(cfl > 0.0) || !params_ok(*p) || p->gmres_restart < 1 || p->gmres_restart > 500)
+    return E2D_ERR_ARG;
+  if (cudaSetDevice(h->device) != cudaSuccess) return E2D_ERR_CUDA;
+  int rc;
+  if ((rc = nks_setup(h, p->gmres_restart))) return rc;
+  e2d_nks_state* s = h->nks;
+  Blocks& B = h->B;
+  const int C = B.ncase;
+  const long long nint = (long long)B.nblk * B.nci * B.ncj;
+  const double ao = sqrt(h->sc.gamma * P_STD / RHO_STD);
+  if ((rc = set_active(h, std::vector<int>(C, 1)))) return rc;
+  E2D_CK(launch_ghost_fill(B, h->stream));
+  for (int c = 0; c < C; ++c) s->host[c] = cfl;
+  E2D_CK(cudaMemcpyAsync(s->cflv, s->host, sizeof(double) * C, cudaMemcpyHostToDevice, h->stream));
+  E2D_CK(launch_slot_init(s->slots, s->step0, 0, C, h->stream));
+  E2D_CK(launch_cfl(B, s->slots, s->step0, h->stream));
+  set_dt_kernel<<<grid_for(nint), VT, 0, h->stream>>>(act(h), s->slots, s->cflv);
+  E2D_CK(cudaGetLastError());
+  if ((rc = precon_build(h, *p, ao, act(h)))) return rc;
+  const size_t nb = sizeof(double) * size_t(s->n);
+  E2D_CK(cudaMemcpyAsync(s->V, v, nb, cudaMemcpyHostToDevice, h->stream));
+  if (use_ilu(*p)) {
+    E2D_CK(cudaMemcpyAsync(s->Z, s->V, nb, cudaMemcpyDeviceToDevice, h->stream));
+    if ((rc = ilu_apply(h, s->V, s->Z))) return rc;
+  } else {
+    precon_apply_kernel<<<B.nblk * s->ch_cell, VT, 0, h->stream>>>(s->Minv, s->V, s->Z, B.NCi * B.NCj, s->ch_cell,
+                                                                   s->partial, s->counter, s->eps, 1.0, act(h));
+    E2D_CK(cudaGetLastError());
+  }
+  E2D_CK(cudaMemcpyAsync(z, s->Z, nb, cudaMemcpyDeviceToHost, h->stream));
+  E2D_CK(cudaStreamSynchronize(h->stream));
+  // the Krylov buffers start clean for the next solve
+  E2D_CK(cudaMemsetAsync(s->V, 0, nb, h->stream));
+  E2D_CK(cudaMemsetAsync(s->Z, 0, nb, h->stream));
+  return check_status(h);
 }

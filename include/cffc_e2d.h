@@ -238,13 +238,23 @@ int e2d_mlp_train(e2d_mlp *m, const float *X, const float *T, int n, int steps, 
 
 /* Newton-Krylov-Schwarz parameters: the NKS_Input_Parameters fields the
  * Euler2D steady path reads (src_2D/NewtonKrylovSchwarz2D/NKSInput2D.h:128-172;
- * defaults in brackets).  The preconditioner is block Jacobi on the
- * first-order HLLE Jacobian, the Frechet derivative first order. */
+ * defaults in brackets).  The Frechet derivative is first order.  The
+ * preconditioner (Block_Preconditioner, Block_Preconditioner2D.h:261-800)
+ * is block Jacobi or BPKIT's ILU(k) on the approximate Jacobian, both with
+ * exact inverses of the 4x4 diagonal blocks (LP_INVERSE).  Of the reference's
+ * Jacobian orders, Euler2D provides the first-order HLLE Jacobian and the
+ * source-terms-only one; the others end its run (they need specializations
+ * Euler2D does not have) and are not offered here.  Zero-filled fields past
+ * max_gmres select the reference's defaults. */
+#define E2D_PRECON_BLOCK_JACOBI 0   /* GMRES_Block_Preconditioner Diagonal  */
+#define E2D_PRECON_BLOCK_ILUK 1     /* GMRES_Block_Preconditioner ILUK      */
+#define E2D_JACOBIAN_FIRST_ORDER_HLLE 0  /* First_Order_Inviscid_HLLE       */
+#define E2D_JACOBIAN_SOURCE_TERMS_ONLY 1 /* Source_Terms_Only (-I/dt)       */
 typedef struct e2d_nks_params {
   int32_t max_newton;        /* Maximum_Number_of_NKS_Iterations            */
   int32_t gmres_restart;     /* GMRES_Restart                       [30]    */
   int32_t max_gmres;         /* Maximum_Number_of_GMRES_Iterations          */
-  int32_t reserved;
+  int32_t block_preconditioner; /* E2D_PRECON_*                    [Jacobi] */
   double overall_tol;        /* Overall_Tolerance, L2 density drop [1e-5]   */
   double cfl0;               /* Finite_Time_Step_Initial_CFL        [1]     */
   double gmres_tol_initial;  /* GMRES_Initial_Tolerance             [1e-5]  */
@@ -256,6 +266,8 @@ typedef struct e2d_nks_params {
    * (library extension; a warm-started case passes its freestream residual
    * so that it is driven to the same absolute level as a cold start). */
   const double *l2_reference;
+  int32_t ilu_level_of_fill; /* GMRES_ILUK_Level_of_Fill, 0-16         [0]     */
+  int32_t jacobian_order;    /* Jacobian_Order: E2D_JACOBIAN_*   [HLLE]    */
 } e2d_nks_params;
 
 /* One Newton step of the history (the values the reference prints). */
@@ -269,14 +281,24 @@ typedef struct e2d_nks_step {
 
 /* Steady solve by pseudo-transient Newton-Krylov: the Newton loop of
  * Internal_Newton_Krylov_Schwarz_Solver (NKS2D.h:412-1258) with SER CFL
- * (Finite_Time_Step, NKS2D.h:1316), the block-Jacobi preconditioner of
- * Block_Preconditioner (Block_Preconditioner2D.h:352-584, BPKIT BJacobi with
- * LP_INVERSE), right-preconditioned restarted matrix-free GMRES with modified
+ * (Finite_Time_Step, NKS2D.h:1316), the block-Jacobi or ILU(k)
+ * preconditioner of Block_Preconditioner (Block_Preconditioner2D.h:352-800,
+ * BPKIT BJacobi / BILUK with LP_INVERSE), right-preconditioned restarted matrix-free GMRES with modified
  * Gram-Schmidt (GMRES2D.h:790-1544) and Newton_Update with positivity
  * back-off (Euler2DQuadNKS.h:23-92).  hist (host, may be NULL) receives one
  * entry per Newton step evaluated, *n_steps their count.  Returns 0, or a
  * negative library error. */
 int e2d_nks(e2d_handle *h, const e2d_nks_params *p, e2d_nks_step *hist, int *n_steps);
+
+/* The Newton step's preconditioner on its own: each cell's dt is the
+ * CFL-limited step (local or global, as the scheme says) times cfl, as the
+ * Newton loop sets it (NKS2D.h:913-930); then
+ * Block_Preconditioner::Update_Jacobian_and_Preconditioner and
+ * Apply_Preconditioner (Block_Preconditioner2D.h:352, 787) for every block:
+ * z = M^-1 v.  v and z are host arrays in the GMRES vector layout
+ * [nblk][NCj][NCi][4] (ghost entries of v ignored, of z zero).  The state
+ * is left as it was; dt is overwritten.  Returns 0 or a library error. */
+int e2d_block_precon_apply(e2d_handle *h, const e2d_nks_params *p, double cfl, const double *v, double *z);
 
 /* Device status word: 0 or the first error a kernel recorded. */
 int e2d_status(e2d_handle *h);

@@ -29,7 +29,9 @@
 // usage:
 //   e2d_ref_harness residual CASE OUT
 //   e2d_ref_harness explicit CASE NSTEPS OUT
-//   e2d_ref_harness nks      CASE OUT MAX_NEWTON GMRES_RESTART MAX_GMRES CFL0 OVERALL_TOL [GMRES_TOL]
+//   e2d_ref_harness nks      CASE OUT MAX_NEWTON GMRES_RESTART MAX_GMRES CFL0 OVERALL_TOL [GMRES_TOL
+//                            [ILUK|Diagonal LEVEL]]
+//   e2d_ref_harness precon   CASE OUT CFL ILUK|Diagonal LEVEL VFILE
 //   e2d_ref_harness time     CASE NSTEPS THREADS      (prints one JSON line)
 //   e2d_ref_harness restart_write CASE PREFIX NSTEPS TIME  (Write_QuadTree + Write_Restart_Solution)
 //   e2d_ref_harness restart_read  CASE PREFIX OUT [GRIDFILE]
@@ -183,6 +185,13 @@ void set_grid(const Case& c, const BlockData& d, Grid2D_Quad_Block_HO& G) {
   G.Schedule_Interior_Mesh_Update();
   G.Schedule_Ghost_Cells_Update();
   G.Update_Cells();
+}
+
+// GMRES_Block_Preconditioner and GMRES_ILUK_Level_of_Fill as the deck
+// keywords set them (NKSInput2D.h:523-536).
+void set_block_preconditioner(NKS_Input_Parameters& N, const char* kind, const char* level) {
+  N.GMRES_Block_Preconditioner = strcmp(kind, "Diagonal") ? Block_ILUK : Block_Jacobi;
+  N.GMRES_ILUK_Level_of_Fill = atoi(level);
 }
 
 // The reference's own multi-block set-up.  order[b] = solution block index
@@ -420,6 +429,46 @@ int main(int argc, char** argv) {
     return err ? 1 : 0;
   }
 
+  if (!strcmp(mode, "precon")) {
+    // The Newton step's preconditioner alone: dt as the Newton loop sets it
+    // (NKS2D.h:913-930), then per block Create_Preconditioner,
+    // Update_Jacobian_and_Preconditioner and Apply_Preconditioner
+    // (Block_Preconditioner2D.h:261, 352, 787) on the vectors of VFILE
+    // ([nblk][NCj][NCi][4] doubles, GMRES_Block::index order); OUT gets z.
+    if (argc < 8) { fprintf(stderr, "precon CASE OUT CFL ILUK|Diagonal LEVEL VFILE\n"); return 2; }
+    RefSet R;
+    build_reference_blocks(c, R);
+    set_block_preconditioner(R.IP.NKS_IP, argv[5], argv[6]);
+    Send_All_Messages(R.Soln, R.Local, NUM_VAR_EULER2D, OFF);
+    BCs(R.Soln, R.Local, R.IP);
+    const double cfl = atof(argv[4]);
+    double dTime = CFL(R.Soln, R.Local, R.IP);
+    if (R.IP.Local_Time_Stepping == GLOBAL_TIME_STEPPING) {
+      Set_Global_TimeStep(R.Soln, R.Local, dTime * cfl);
+    } else {
+      for (int b = 0; b < c.nblk; ++b) {
+        Euler2D_Quad_Block& B = R.Soln[R.order[b]];
+        for (int i = 0; i < B.NCi; ++i)
+          for (int j = 0; j < B.NCj; ++j) B.dt[i][j] *= cfl;
+      }
+    }
+    const int n = 4 * (c.nci + 2 * c.ng) * (c.ncj + 2 * c.ng);
+    std::vector<double> v(size_t(n) * c.nblk), z(size_t(n) * c.nblk, 0.0);
+    FILE* fv = fopen(argv[7], "rb");
+    if (!fv || fread(v.data(), sizeof(double), v.size(), fv) != v.size()) { fprintf(stderr, "bad VFILE\n"); return 2; }
+    fclose(fv);
+    for (int b = 0; b < c.nblk; ++b) {
+      Block_Preconditioner<Euler2D_pState, Euler2D_Quad_Block, Euler2D_Input_Parameters> P;
+      P.Create_Preconditioner(R.Soln[R.order[b]], R.IP, NUM_VAR_EULER2D);
+      P.Update_Jacobian_and_Preconditioner(0.0);
+      P.Apply_Preconditioner(n, 1, &v[size_t(b) * n], n, &z[size_t(b) * n], n);
+    }
+    FILE* f = fopen(argv[3], "wb");
+    wr(f, z.data(), z.size());
+    fclose(f);
+    return 0;
+  }
+
   if (!strcmp(mode, "nks")) {
     if (argc < 9) { fprintf(stderr, "nks CASE OUT MAX_NEWTON RESTART MAX_GMRES CFL0 TOL\n"); return 2; }
     RefSet R;
@@ -431,6 +480,7 @@ int main(int argc, char** argv) {
     N.Finite_Time_Step_Initial_CFL = atof(argv[7]);
     N.Overall_Tolerance = atof(argv[8]);
     if (argc > 9) N.GMRES_Initial_Tolerance = N.GMRES_Final_Tolerance = atof(argv[9]);
+    if (argc > 11) set_block_preconditioner(N, argv[10], argv[11]);
     Send_All_Messages(R.Soln, R.Local, NUM_VAR_EULER2D, OFF);
     BCs(R.Soln, R.Local, R.IP);
     std::string hist_path = std::string(argv[3]) + ".hist";

@@ -61,7 +61,8 @@ def run_explicit(bs, nsteps):
 
 
 def run_nks(bs, params):
-    """params: (max_newton, restart, max_gmres, cfl0, overall_tol[, gmres_tol])."""
+    """params: (max_newton, restart, max_gmres, cfl0, overall_tol[, gmres_tol[, ilu_level]]);
+    ilu_level k >= 0 selects GMRES_Block_Preconditioner ILUK with level of fill k."""
     res = run_nks_once(bs, params)
     W = bs.W.copy()
     W[:, 0] *= 1.0 + 2.0 ** -46
@@ -74,8 +75,10 @@ def run_nks_once(bs, params):
     with tempfile.TemporaryDirectory() as td:
         cp, op = os.path.join(td, "c.bin"), os.path.join(td, "o.bin")
         cases.write_case(cp, bs)
-        r = subprocess.run([HARNESS, "nks", cp, op] + [str(v) for v in params], check=True,
-                           capture_output=True, text=True)
+        args = [str(v) for v in params[:6]]
+        if len(params) > 6 and params[6] >= 0:
+            args += ["ILUK", str(params[6])]
+        r = subprocess.run([HARNESS, "nks", cp, op] + args, check=True, capture_output=True, text=True)
         buf = open(op, "rb").read()
     err = np.frombuffer(buf[:8], dtype="<i4")[0]
     U = np.frombuffer(buf[16:], dtype="<f8").reshape(bs.nblk, 4, bs.NCj, bs.NCi)
@@ -93,6 +96,30 @@ def run_nks_once(bs, params):
                           float(t[t.index("resid") + 2]), float(t[t.index("relative_residual") + 2])])
     return dict(U=U, newton=np.array(newton), gmres=np.array(gmres), final=np.array(final),
                 err=np.int32(err), params=np.array(params, dtype=np.float64))
+
+
+def precon_vector(bs, seed):
+    """Seeded GMRES-layout vector [nblk][NCj][NCi][4], ghost entries zero."""
+    v = np.zeros((bs.nblk, bs.NCj, bs.NCi, 4))
+    g = bs.ng
+    v[:, g:-g, g:-g, :] = np.random.default_rng(seed).standard_normal((bs.nblk, bs.ncj, bs.nci, 4))
+    return v
+
+
+def run_precon(bs, params):
+    """params: (cfl, ilu_level, seed); ilu_level -1 is block Jacobi.  The
+    reference's Newton-step preconditioner applied to a seeded vector."""
+    cfl, level, seed = params
+    v = precon_vector(bs, int(seed))
+    with tempfile.TemporaryDirectory() as td:
+        cp, op, vp = (os.path.join(td, n) for n in ("c.bin", "o.bin", "v.bin"))
+        cases.write_case(cp, bs)
+        v.astype("<f8").tofile(vp)
+        kind = "ILUK" if level >= 0 else "Diagonal"
+        subprocess.run([HARNESS, "precon", cp, op, repr(float(cfl)), kind, str(max(int(level), 0)), vp],
+                       check=True, capture_output=True, text=True)
+        z = np.fromfile(op, dtype="<f8").reshape(v.shape)
+    return dict(v=v, z=z, params=np.array(params, dtype=np.float64))
 
 
 def case_arrays(bs):
@@ -142,6 +169,19 @@ def golden_cases():
         ("nks_bump_m14_converged", bump_m14, "nks", (30, 30, 120, 10.0, 1e-10, 0.1)),
         # the same solve with the HLLE flux in the residual
         ("nks_bump_m14_hlle", with_flux(bump_m14, cases.FLUX_HLLE), "nks", (30, 30, 120, 10.0, 1e-10, 0.1)),
+        # the subsonic bump that stalls under block Jacobi, with the ILU(4)
+        # preconditioner of the reference's NKS example decks
+        ("nks_bump_iluk4", bump, "nks", (12, 30, 120, 10.0, 1e-10, 0.1, 4)),
+        # global time step, Barth-Jespersen, restarts, with ILU(0)
+        ("nks_bump_bj_global_iluk0", bump_bj, "nks", (4, 10, 25, 5.0, 1e-10, 1e-5, 0)),
+        # the Newton step's preconditioner alone: (CFL, ILU level or -1 for
+        # block Jacobi, vector seed)
+        ("precon_bump_jacobi", bump, "precon", (10.0, -1, 1)),
+        ("precon_bump_iluk0", bump, "precon", (10.0, 0, 2)),
+        ("precon_bump_iluk2", bump, "precon", (10.0, 2, 3)),
+        ("precon_bump_iluk4", bump, "precon", (100.0, 4, 4)),
+        ("precon_bump_bj_global_iluk1", bump_bj, "precon", (5.0, 1, 5)),
+        ("precon_curv_iluk3", curv, "precon", (3.0, 3, 6)),
     ] + [
         # the other explicit schemes (optimally smoothing multistage, RK4, RK5),
         # implicit residual smoothing and limiter freezing
@@ -305,6 +345,9 @@ def main():
         if kind == "nks":
             res = run_nks(bs, steps)
             steps = steps[0]
+        elif kind == "precon":
+            res = run_precon(bs, steps)
+            steps = 0
         else:
             res = run_residual(bs) if kind == "residual" else run_explicit(bs, steps)
         if bs.nblk * bs.nci * bs.ncj > 8192:

@@ -47,10 +47,12 @@ def run(name, precision):
     bs = dataclasses.replace(bs, scheme=dataclasses.replace(bs.scheme, precision=precision))
     max_newton, restart, max_gmres, cfl0, tol = ref["params"][:5]
     gmres_tol = float(ref["params"][5]) if len(ref["params"]) > 5 else 1e-5
+    level = int(ref["params"][6]) if len(ref["params"]) > 6 else -1
     h = capi.Handle(bs)
     h.set_state()
     p = capi.nks_params(int(max_newton), gmres_restart=int(restart), max_gmres=int(max_gmres),
-                        overall_tol=float(tol), cfl0=float(cfl0), gmres_tol=gmres_tol)
+                        overall_tol=float(tol), cfl0=float(cfl0), gmres_tol=gmres_tol,
+                        ilu_level=None if level < 0 else level)
     rc, hist = h.nks(p)
     _, U = h.get_state()
     h.close()
