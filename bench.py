@@ -183,17 +183,18 @@ def nks_workload():
                               scheme=cases.Scheme(limiter=cases.LIMITER_ZERO, local_dt=1))
 
 
-def nks_measure(precision, device, cpu):
+def nks_measure(precision, device, cpu, ilu_level=None):
     """Seconds to a 1e-10 L2 density drop: the device solve end to end (host
     W in, Newton loop with its per-iteration host round trips), and the
-    compiled reference's Newton_Krylov_Schwarz_Solver on one host core."""
+    compiled reference's Newton_Krylov_Schwarz_Solver on one host core, both
+    with block Jacobi (ilu_level None) or ILU(ilu_level)."""
     from cffc_b200 import capi
     bs = nks_workload()
     bs.scheme.precision = precision
-    p = capi.nks_params(**NKS_PARAMS)
+    p = capi.nks_params(**NKS_PARAMS, ilu_level=ilu_level)
     h = capi.Handle(bs, device=device)
     h.set_state()
-    h.nks(capi.nks_params(2, gmres_restart=30, max_gmres=20))  # warm-up: allocation, first launches
+    h.nks(capi.nks_params(2, gmres_restart=30, max_gmres=20, ilu_level=ilu_level))  # warm-up: allocation, first launches
     t0 = time.perf_counter()
     h.set_state()
     rc, hist = h.nks(p)
@@ -201,7 +202,8 @@ def nks_measure(precision, device, cpu):
     h.close()
     iters = sum(st["gmres_iters"] for st in hist)
     out = {"workload": "supersonic bump, 6 x 2 blocks x 32x32 (12,288 cells), first order, "
-                       "GMRES(30) tol 0.1, CFL0 10, block-Jacobi",
+                       "GMRES(30) tol 0.1, CFL0 10, " + ("block-Jacobi" if ilu_level is None else
+                                                         "ILU(%d)" % ilu_level),
            "tolerance": NKS_PARAMS["overall_tol"], "seconds_to_steady": round(secs, 4),
            "converged": bool(rc == 0 and hist and hist[-1]["ratio"] <= NKS_PARAMS["overall_tol"]),
            "newton_steps": len(hist) - 1, "gmres_iterations": iters,
@@ -214,9 +216,10 @@ def nks_measure(precision, device, cpu):
             cp, op = os.path.join(td, "c.bin"), os.path.join(td, "o.bin")
             cases.write_case(cp, bs)
             a = NKS_PARAMS
+            extra = [] if ilu_level is None else ["ILUK", str(ilu_level)]
             r = subprocess.run([harness, "nks", cp, op, str(a["max_newton"]), str(a["gmres_restart"]),
-                                str(a["max_gmres"]), str(a["cfl0"]), str(a["overall_tol"]), str(a["gmres_tol"])],
-                               capture_output=True, text=True)
+                                str(a["max_gmres"]), str(a["cfl0"]), str(a["overall_tol"]), str(a["gmres_tol"])]
+                               + extra, capture_output=True, text=True)
             secs_ref = float(r.stderr.strip().split(",")[-1].split()[0])
             end = [l for l in r.stdout.split("\n") if "End of Newton Steps" in l]
             out["cpu_reference"] = {"seconds_to_steady": round(secs_ref, 3), "cores": 1, "kind": "reference",
@@ -487,6 +490,7 @@ def main():
             line["cpu_baseline"] = cpu_baseline(bs)
         if world == 1 and not args.no_nks:
             line["nks"] = nks_measure(PRECISION[args.precision], local, not args.no_cpu_baseline)
+            line["nks_iluk"] = nks_measure(PRECISION[args.precision], local, not args.no_cpu_baseline, ilu_level=2)
             line["nks_batch"] = nks_batch_measure(PRECISION[args.precision], local)
             line["nks_learned"] = nks_learned_measure(local)
         print(json.dumps(line), flush=True)

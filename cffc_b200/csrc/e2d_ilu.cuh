@@ -34,16 +34,18 @@
 // (needs <map> and <vector>, included by e2d_nks.cu at file scope)
 
 struct IluPattern {
-  int nrow = 0, nnz = 0, nflev = 0, nblev = 0, level = -1, nci = 0, ncj = 0;
+  int nrow = 0, nnz = 0, nflev = 0, nblev = 0, maxrow = 0, maxops = 0, level = -1, nci = 0, ncj = 0;
   std::vector<int> row_ptr, nlow, col, fop_ptr, flev_ptr, flev_rows, blev_ptr, blev_rows, apos;
   std::vector<int2> fop;
+  std::vector<int4> fdesc, bdesc;
 };
 
 struct IluDev {
-  int nrow, nnz, nflev, nblev;
+  int nrow, nnz, nflev, nblev, maxrow, maxops;
   const int *row_ptr, *nlow, *col, *fop_ptr;
   const int2* fop;
   const int *flev_ptr, *flev_rows, *blev_ptr, *blev_rows, *apos;
+  const int4 *fdesc, *bdesc;  // per level-ordered row: (row, first entry, end entry, 0)
   double* vals;
   double* dinv;
   double* work;  // [nblk][nrow][4] when a block's vector does not fit shared memory
@@ -106,6 +108,7 @@ inline bool ilu_pattern(int nci, int ncj, int k_fill, IluPattern& P) {
       if (c < r) ++P.nlow[r];
     }
     P.row_ptr[r + 1] = int(P.col.size());
+    P.maxrow = std::max(P.maxrow, P.row_ptr[r + 1] - P.row_ptr[r]);
     if (P.col.size() > (size_t(1) << 26)) return false;
   }
   P.nnz = int(P.col.size());
@@ -127,6 +130,7 @@ inline bool ilu_pattern(int nci, int ncj, int k_fill, IluPattern& P) {
       }
       P.fop_ptr[e + 1] = int(P.fop.size());
     }
+    P.maxops = std::max(P.maxops, P.fop_ptr[P.row_ptr[r + 1]] - P.fop_ptr[P.row_ptr[r]]);
   }
   // level schedules
   std::vector<int> lev(nr, 0);
@@ -161,6 +165,15 @@ inline bool ilu_pattern(int nci, int ncj, int k_fill, IluPattern& P) {
   {
     std::vector<int> fill(P.blev_ptr.begin(), P.blev_ptr.end() - 1);
     for (int r = nr - 1; r >= 0; --r) P.blev_rows[fill[lev[r]]++] = r;
+  }
+  // row descriptors in level order: the L part (forward), the U part past
+  // the diagonal (backward)
+  P.fdesc.resize(nr);
+  P.bdesc.resize(nr);
+  for (int q = 0; q < nr; ++q) {
+    const int i = P.flev_rows[q], k = P.blev_rows[q];
+    P.fdesc[q] = make_int4(i, P.row_ptr[i], P.row_ptr[i] + P.nlow[i], 0);
+    P.bdesc[q] = make_int4(k, P.row_ptr[k] + P.nlow[k] + 1, P.row_ptr[k + 1], 0);
   }
   // where cell c's column blocks go: its diagonal, then the rows of the
   // cells below (j-1), above (j+1), left (i-1), right (i+1) — the reference's
@@ -269,11 +282,17 @@ constexpr int ILU_THREADS = 256;
 
 // BILUK::setup's numeric factorization (BILUK.cc:85-150), one CTA per
 // block, rows level by level; a row is worked by 16 threads, one per element
-// of the 4x4 blocks.  For each L entry in column order: mult = L * inv(D_id)
-// (stored as the L factor), then every pattern entry t of the row that U(id)
-// reaches gets t -= mult * U(id, .); finally the diagonal block is inverted.
-// Products accumulate in the order of the netlib dgemm loops BPKIT calls.
+// of the 4x4 blocks, in shared memory: the row's blocks, columns and
+// elimination work list are staged per 16-thread group (D.maxrow entries,
+// D.maxops updates).  For each L entry in column order: mult = L * inv(D_id)
+// (kept as the L factor), then every pattern entry t of the row that U(id)
+// reaches gets t -= mult * U(id, .); the finished row goes back to global
+// memory and its diagonal block is inverted.  Products accumulate in the
+// order of the netlib dgemm loops BPKIT calls.
+constexpr int ILU_OPS_CHUNK = 8;
+
 __global__ void __launch_bounds__(ILU_THREADS) ilu_factor_kernel(Blocks B, IluDev D) {
+  extern __shared__ double rsh[];
   const int b = blockIdx.x;
   if (B.case_active && !B.case_active[case_id(B, b)]) return;
   double* V = D.vals + (size_t(b) * D.nnz) * 16;
@@ -282,51 +301,179 @@ __global__ void __launch_bounds__(ILU_THREADS) ilu_factor_kernel(Blocks B, IluDe
   const unsigned gmask = 0xFFFFu << (threadIdx.x & 16);
   __shared__ double msh[ILU_THREADS];
   double* mg = msh + (threadIdx.x & ~15);
+  // per group: blocks [maxrow][16], columns [maxrow], op offsets [maxrow + 2], ops [maxops]
+  const size_t per = 16 * size_t(D.maxrow) * sizeof(double) + (2 * size_t(D.maxrow) + 2) * sizeof(int) +
+                     size_t(D.maxops) * sizeof(int2);
+  unsigned char* gbase = reinterpret_cast<unsigned char*>(rsh) + size_t(grp) * per;
+  double* row = reinterpret_cast<double*>(gbase);
+  int* gcol = reinterpret_cast<int*>(row + 16 * D.maxrow);
+  int* gfp = gcol + D.maxrow;
+  int2* gops = reinterpret_cast<int2*>(gfp + D.maxrow + 2);
   for (int L = 0; L < D.nflev; ++L) {
     for (int q = D.flev_ptr[L] + grp; q < D.flev_ptr[L + 1]; q += ILU_THREADS / 16) {
       const int i = D.flev_rows[q];
-      const int e0 = D.row_ptr[i], e1 = e0 + D.nlow[i];
-      for (int e = e0; e < e1; ++e) {
-        const double* Dd = Di + 16 * size_t(D.col[e]);
+      const int e0 = D.row_ptr[i], nL = D.nlow[i], nE = D.row_ptr[i + 1] - e0;
+      const int ob = D.fop_ptr[e0], oe = D.fop_ptr[e0 + nL];
+      for (int e = 0; e < nE; ++e) row[16 * e + lane] = V[16 * size_t(e0 + e) + lane];
+      for (int t = lane; t < nE; t += 16) gcol[t] = D.col[e0 + t];
+      for (int t = lane; t <= nL; t += 16) gfp[t] = D.fop_ptr[e0 + t] - ob;
+      for (int t = lane; t < oe - ob; t += 16) {
+        const int2 o = D.fop[ob + t];
+        gops[t] = make_int2(o.x - e0, o.y);
+      }
+      __syncwarp(gmask);
+      double dn[4] = {0.0, 0.0, 0.0, 0.0};
+      if (nL > 0) {
+        const double* Dd = Di + 16 * size_t(gcol[0]);
+#pragma unroll
+        for (int l = 0; l < 4; ++l) dn[l] = Dd[4 * l + c];
+      }
+      for (int le = 0; le < nL; ++le) {
+        const double d0 = dn[0], d1 = dn[1], d2 = dn[2], d3 = dn[3];
+        if (le + 1 < nL) {  // the next L entry's inverted diagonal, a step ahead
+          const double* Dd = Di + 16 * size_t(gcol[le + 1]);
+#pragma unroll
+          for (int l = 0; l < 4; ++l) dn[l] = Dd[4 * l + c];
+        }
+        double* Le = row + 16 * le;
         __syncwarp(gmask);
-        const double a0 = V[16 * size_t(e) + 4 * r + 0], a1 = V[16 * size_t(e) + 4 * r + 1];
-        const double a2 = V[16 * size_t(e) + 4 * r + 2], a3 = V[16 * size_t(e) + 4 * r + 3];
+        const double a0 = Le[4 * r + 0], a1 = Le[4 * r + 1], a2 = Le[4 * r + 2], a3 = Le[4 * r + 3];
         double m = 0.0;
-        m = m + Dd[0 + c] * a0;
-        m = m + Dd[4 + c] * a1;
-        m = m + Dd[8 + c] * a2;
-        m = m + Dd[12 + c] * a3;
+        m = m + d0 * a0;
+        m = m + d1 * a1;
+        m = m + d2 * a2;
+        m = m + d3 * a3;
         mg[lane] = m;
         __syncwarp(gmask);
-        V[16 * size_t(e) + lane] = m;
+        Le[lane] = m;
         const double m0 = mg[4 * r + 0], m1 = mg[4 * r + 1], m2 = mg[4 * r + 2], m3 = mg[4 * r + 3];
-        for (int o = D.fop_ptr[e]; o < D.fop_ptr[e + 1]; ++o) {
-          const int2 tq = D.fop[o];
-          const double* U = V + 16 * size_t(tq.y);
-          double acc = V[16 * size_t(tq.x) + lane];
-          acc = acc + (-U[0 + c]) * m0;
-          acc = acc + (-U[4 + c]) * m1;
-          acc = acc + (-U[8 + c]) * m2;
-          acc = acc + (-U[12 + c]) * m3;
-          V[16 * size_t(tq.x) + lane] = acc;
+        // the updates of one L entry hit distinct entries: a chunk at a
+        // time, its U loads issued together
+        for (int o = gfp[le]; o < gfp[le + 1]; o += ILU_OPS_CHUNK) {
+          const int n = min(ILU_OPS_CHUNK, gfp[le + 1] - o);
+          double u[ILU_OPS_CHUNK][4];
+#pragma unroll
+          for (int kk = 0; kk < ILU_OPS_CHUNK; ++kk)
+            if (kk < n) {
+              const double* U = V + 16 * size_t(gops[o + kk].y);
+              u[kk][0] = U[0 + c]; u[kk][1] = U[4 + c]; u[kk][2] = U[8 + c]; u[kk][3] = U[12 + c];
+            }
+#pragma unroll
+          for (int kk = 0; kk < ILU_OPS_CHUNK; ++kk)
+            if (kk < n) {
+              double* t = row + 16 * gops[o + kk].x + lane;
+              double acc = *t;
+              acc = acc + (-u[kk][0]) * m0;
+              acc = acc + (-u[kk][1]) * m1;
+              acc = acc + (-u[kk][2]) * m2;
+              acc = acc + (-u[kk][3]) * m3;
+              *t = acc;
+            }
         }
       }
       __syncwarp(gmask);
+      for (int e = 0; e < nE; ++e) V[16 * size_t(e0 + e) + lane] = row[16 * e + lane];
       if (lane == 0) {
         double a[4][4];
 #pragma unroll
         for (int rr = 0; rr < 4; ++rr)
 #pragma unroll
-          for (int cc = 0; cc < 4; ++cc) a[rr][cc] = V[16 * size_t(e1) + 4 * rr + cc];
+          for (int cc = 0; cc < 4; ++cc) a[rr][cc] = row[16 * nL + 4 * rr + cc];
         if (!invert4(a)) set_status(B.status, 3, int(cell_sc(B, b, NG + i / B.nci, NG + i % B.nci)));
 #pragma unroll
         for (int rr = 0; rr < 4; ++rr)
 #pragma unroll
           for (int cc = 0; cc < 4; ++cc) Di[16 * size_t(i) + 4 * rr + cc] = a[rr][cc];
       }
+      __syncwarp(gmask);
     }
     __syncthreads();
   }
+}
+
+// size of ilu_factor_kernel's dynamic shared memory
+inline size_t ilu_factor_smem_bytes(const IluPattern& P) {
+  return size_t(ILU_THREADS / 16) * (16 * size_t(P.maxrow) * sizeof(double) +
+                                     (2 * size_t(P.maxrow) + 2) * sizeof(int) + size_t(P.maxops) * sizeof(int2));
+}
+
+// acc - sum over entries e0..e1 (in order) of block(e) row k . y(col(e)):
+// one row of a triangular solve, the loads of four entries issued together.
+__device__ __forceinline__ double row_solve(const double* __restrict__ V, const double* y, const int* __restrict__ col,
+                                            int e0, int e1, int k, double acc) {
+  int e = e0;
+  for (; e + 4 <= e1; e += 4) {
+    double a[4][4], w[4][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double* Bq = V + 16 * size_t(e + q) + 4 * k;
+      const double* yq = y + 4 * col[e + q];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) { a[q][l] = Bq[l]; w[q][l] = yq[l]; }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int l = 0; l < 4; ++l) acc = acc + (-w[q][l]) * a[q][l];
+  }
+  for (; e < e1; ++e) {
+    const double* Bq = V + 16 * size_t(e) + 4 * k;
+    const double* yq = y + 4 * col[e];
+    acc = acc + (-yq[0]) * Bq[0];
+    acc = acc + (-yq[1]) * Bq[1];
+    acc = acc + (-yq[2]) * Bq[2];
+    acc = acc + (-yq[3]) * Bq[3];
+  }
+  return acc;
+}
+
+// A row of a triangular solve whose first four entries (values, columns
+// and, for the upper solve, the inverted diagonal block) are loaded a level
+// ahead, while the level before it is still being solved.
+struct RowPre {
+  int i, e, end;
+  int col[4];
+  double a[4][4];
+  double dd[4];
+};
+
+template <bool BACK>
+__device__ __forceinline__ void row_prefetch(const int4* desc, const int* lp, int L, int nlev, int grp, int k,
+                                             const double* __restrict__ V, const double* __restrict__ Di,
+                                             const int* __restrict__ col, RowPre& p) {
+  p.i = -1;
+  if (L >= nlev) return;
+  const int q = lp[L] + grp;
+  if (q >= lp[L + 1]) return;
+  const int4 d = desc[q];
+  p.i = d.x; p.e = d.y; p.end = d.z;
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    if (d.y + m < d.z) {
+      p.col[m] = col[d.y + m];
+      const double* Bq = V + 16 * size_t(d.y + m) + 4 * k;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) p.a[m][l] = Bq[l];
+    }
+  }
+  if (BACK) {
+    const double* Dd = Di + 16 * size_t(d.x) + 4 * k;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) p.dd[l] = Dd[l];
+  }
+}
+
+__device__ __forceinline__ double row_finish(const RowPre& p, const double* __restrict__ V, const double* y,
+                                             const int* __restrict__ col, int k, double acc) {
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+    if (p.e + m < p.end) {
+      const double* yq = y + 4 * p.col[m];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) acc = acc + (-yq[l]) * p.a[m][l];
+    }
+  if (p.end > p.e + 4) acc = row_solve(V, y, col, p.e + 4, p.end, k, acc);
+  return acc;
 }
 
 // BILUK::apply (BILUK.cc:152-205): z = inv(U) inv(L) v on the interior
@@ -342,7 +489,23 @@ __global__ void __launch_bounds__(ILU_THREADS) ilu_apply_kernel(Blocks B, IluDev
   if (B.case_active && !B.case_active[case_id(B, b)]) return;
   const double* V = D.vals + (size_t(b) * D.nnz) * 16;
   const double* Di = D.dinv + (size_t(b) * D.nrow) * 16;
+  // shared: the block's vector, the row descriptors in level order and the
+  // level offsets (everything a level reads except the factor values)
   double* y = SHARED ? ysh : D.work + size_t(b) * D.nrow * 4;
+  const int4* fdesc = D.fdesc;
+  const int4* bdesc = D.bdesc;
+  const int* flp = D.flev_ptr;
+  const int* blp = D.blev_ptr;
+  if (SHARED) {
+    int4* fd = reinterpret_cast<int4*>(ysh + 4 * size_t(D.nrow));
+    int4* bd = fd + D.nrow;
+    int* fl = reinterpret_cast<int*>(bd + D.nrow);
+    int* bl = fl + D.nflev + 1;
+    for (int t = threadIdx.x; t < D.nrow; t += ILU_THREADS) { fd[t] = D.fdesc[t]; bd[t] = D.bdesc[t]; }
+    for (int t = threadIdx.x; t <= D.nflev; t += ILU_THREADS) fl[t] = D.flev_ptr[t];
+    for (int t = threadIdx.x; t <= D.nblev; t += ILU_THREADS) bl[t] = D.blev_ptr[t];
+    fdesc = fd; bdesc = bd; flp = fl; blp = bl;
+  }
   const size_t base = size_t(b) * B.NCj * B.NCi;
   for (int t = threadIdx.x; t < 4 * D.nrow; t += ILU_THREADS) {
     const int r = t >> 2;
@@ -351,48 +514,52 @@ __global__ void __launch_bounds__(ILU_THREADS) ilu_apply_kernel(Blocks B, IluDev
   __syncthreads();
   const int grp = threadIdx.x >> 2, k = threadIdx.x & 3;
   const unsigned qmask = 0xFu << (threadIdx.x & 28);
-  // forward solve with the unit lower factor
+  // forward solve with the unit lower factor (level 0 rows have no L part);
+  // a group's first row of each level is prefetched during the level before
+  RowPre cur, nxt;
+  row_prefetch<false>(fdesc, flp, 1, D.nflev, grp, k, V, Di, D.col, cur);
   for (int L = 1; L < D.nflev; ++L) {
-    for (int q = D.flev_ptr[L] + grp; q < D.flev_ptr[L + 1]; q += ILU_THREADS / 4) {
-      const int i = D.flev_rows[q];
-      double acc = y[4 * i + k];
-      for (int e = D.row_ptr[i]; e < D.row_ptr[i] + D.nlow[i]; ++e) {
-        const double* Lb = V + 16 * size_t(e) + 4 * k;
-        const double* yj = y + 4 * D.col[e];
-        acc = acc + (-yj[0]) * Lb[0];
-        acc = acc + (-yj[1]) * Lb[1];
-        acc = acc + (-yj[2]) * Lb[2];
-        acc = acc + (-yj[3]) * Lb[3];
-      }
-      y[4 * i + k] = acc;
+    row_prefetch<false>(fdesc, flp, L + 1, D.nflev, grp, k, V, Di, D.col, nxt);
+    if (cur.i >= 0) y[4 * cur.i + k] = row_finish(cur, V, y, D.col, k, y[4 * cur.i + k]);
+    for (int q = flp[L] + grp + ILU_THREADS / 4; q < flp[L + 1]; q += ILU_THREADS / 4) {
+      const int4 d = fdesc[q];
+      y[4 * d.x + k] = row_solve(V, y, D.col, d.y, d.z, k, y[4 * d.x + k]);
     }
     __syncthreads();
+    cur = nxt;
   }
   // backward solve with U, then the inverted diagonal block
+  row_prefetch<true>(bdesc, blp, 0, D.nblev, grp, k, V, Di, D.col, cur);
   for (int L = 0; L < D.nblev; ++L) {
-    for (int q = D.blev_ptr[L] + grp; q < D.blev_ptr[L + 1]; q += ILU_THREADS / 4) {
-      const int i = D.blev_rows[q];
-      double acc = y[4 * i + k];
-      for (int e = D.row_ptr[i] + D.nlow[i] + 1; e < D.row_ptr[i + 1]; ++e) {
-        const double* Ub = V + 16 * size_t(e) + 4 * k;
-        const double* yj = y + 4 * D.col[e];
-        acc = acc + (-yj[0]) * Ub[0];
-        acc = acc + (-yj[1]) * Ub[1];
-        acc = acc + (-yj[2]) * Ub[2];
-        acc = acc + (-yj[3]) * Ub[3];
-      }
-      y[4 * i + k] = acc;
+    row_prefetch<true>(bdesc, blp, L + 1, D.nblev, grp, k, V, Di, D.col, nxt);
+    if (cur.i >= 0) {
+      const int i = cur.i;
+      y[4 * i + k] = row_finish(cur, V, y, D.col, k, y[4 * i + k]);
       __syncwarp(qmask);
-      const double* Dd = Di + 16 * size_t(i) + 4 * k;
       double x = 0.0;
-      x = x + y[4 * i + 0] * Dd[0];
-      x = x + y[4 * i + 1] * Dd[1];
-      x = x + y[4 * i + 2] * Dd[2];
-      x = x + y[4 * i + 3] * Dd[3];
+      x = x + y[4 * i + 0] * cur.dd[0];
+      x = x + y[4 * i + 1] * cur.dd[1];
+      x = x + y[4 * i + 2] * cur.dd[2];
+      x = x + y[4 * i + 3] * cur.dd[3];
       __syncwarp(qmask);
       y[4 * i + k] = x;
     }
+    for (int q = blp[L] + grp + ILU_THREADS / 4; q < blp[L + 1]; q += ILU_THREADS / 4) {
+      const int4 d = bdesc[q];
+      const double* Dd = Di + 16 * size_t(d.x) + 4 * k;
+      const double d0 = Dd[0], d1 = Dd[1], d2 = Dd[2], d3 = Dd[3];
+      y[4 * d.x + k] = row_solve(V, y, D.col, d.y, d.z, k, y[4 * d.x + k]);
+      __syncwarp(qmask);
+      double x = 0.0;
+      x = x + y[4 * d.x + 0] * d0;
+      x = x + y[4 * d.x + 1] * d1;
+      x = x + y[4 * d.x + 2] * d2;
+      x = x + y[4 * d.x + 3] * d3;
+      __syncwarp(qmask);
+      y[4 * d.x + k] = x;
+    }
     __syncthreads();
+    cur = nxt;
   }
   for (int t = threadIdx.x; t < 4 * D.nrow; t += ILU_THREADS) {
     const int r = t >> 2;

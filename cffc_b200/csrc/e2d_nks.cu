@@ -532,6 +532,7 @@ struct e2d_nks_state {
   IluDev ilu{};              // device copies, values and inverted diagonals
   int ilu_level = -1;        // level the ILU arrays are built for (-1: none)
   size_t ilu_smem = 0;       // dynamic shared memory of the apply (0: D.work)
+  size_t ilu_factor_smem = 0; // dynamic shared memory of the factorization
   std::vector<void*> ilu_allocs;
   double* bvec = nullptr;
   double* x = nullptr;
@@ -646,7 +647,8 @@ int ilu_setup(e2d_handle* h, int level) {
   if (!ilu_pattern(h->B.nci, h->B.ncj, level, P)) return E2D_ERR_NOMEM;
   IluDev& D = s->ilu;
   D = IluDev{};
-  D.nrow = P.nrow; D.nnz = P.nnz; D.nflev = P.nflev; D.nblev = P.nblev;
+  D.nrow = P.nrow; D.nnz = P.nnz; D.nflev = P.nflev; D.nblev = P.nblev; D.maxrow = P.maxrow;
+  D.maxops = P.maxops;
   auto up = [&](const void* src, size_t bytes, void** dst) -> int {
     void* q = nullptr;
     if (cudaMalloc(&q, bytes ? bytes : 1) != cudaSuccess) return E2D_ERR_NOMEM;
@@ -657,7 +659,7 @@ int ilu_setup(e2d_handle* h, int level) {
   };
   const int nblk = h->B.nblk;
   int rc;
-  void *a0, *a1, *a2, *a3, *a4, *a5, *a6, *a7, *a8, *a9, *v0, *v1;
+  void *a0, *a1, *a2, *a3, *a4, *a5, *a6, *a7, *a8, *a9, *d0, *d1, *v0, *v1;
   if ((rc = up(P.row_ptr.data(), sizeof(int) * P.row_ptr.size(), &a0)) ||
       (rc = up(P.nlow.data(), sizeof(int) * P.nlow.size(), &a1)) ||
       (rc = up(P.col.data(), sizeof(int) * P.col.size(), &a2)) ||
@@ -668,6 +670,8 @@ int ilu_setup(e2d_handle* h, int level) {
       (rc = up(P.blev_ptr.data(), sizeof(int) * P.blev_ptr.size(), &a7)) ||
       (rc = up(P.blev_rows.data(), sizeof(int) * P.blev_rows.size(), &a8)) ||
       (rc = up(P.apos.data(), sizeof(int) * P.apos.size(), &a9)) ||
+      (rc = up(P.fdesc.data(), sizeof(int4) * P.fdesc.size(), &d0)) ||
+      (rc = up(P.bdesc.data(), sizeof(int4) * P.bdesc.size(), &d1)) ||
       (rc = up(nullptr, sizeof(double) * 16 * size_t(P.nnz) * nblk, &v0)) ||
       (rc = up(nullptr, sizeof(double) * 16 * size_t(P.nrow) * nblk, &v1)))
     return rc;
@@ -675,9 +679,11 @@ int ilu_setup(e2d_handle* h, int level) {
   D.fop_ptr = static_cast<int*>(a3); D.fop = static_cast<int2*>(a4);
   D.flev_ptr = static_cast<int*>(a5); D.flev_rows = static_cast<int*>(a6);
   D.blev_ptr = static_cast<int*>(a7); D.blev_rows = static_cast<int*>(a8); D.apos = static_cast<int*>(a9);
+  D.fdesc = static_cast<int4*>(d0); D.bdesc = static_cast<int4*>(d1);
   D.vals = static_cast<double*>(v0); D.dinv = static_cast<double*>(v1);
   // a block's vector in shared memory when it fits, else a global work array
-  const size_t smem = sizeof(double) * 4 * size_t(P.nrow);
+  const size_t smem = sizeof(double) * 4 * size_t(P.nrow) + sizeof(int4) * 2 * size_t(P.nrow) +
+                      sizeof(int) * size_t(P.nflev + P.nblev + 2);
   int dev = 0, optin = 0;
   E2D_CK(cudaGetDevice(&dev));
   E2D_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -690,6 +696,11 @@ int ilu_setup(e2d_handle* h, int level) {
     D.work = static_cast<double*>(w);
     s->ilu_smem = 0;
   }
+  // one row (blocks, columns, work list) per 16-thread group
+  s->ilu_factor_smem = ilu_factor_smem_bytes(P);
+  if (s->ilu_factor_smem > size_t(optin)) return E2D_ERR_ARG;
+  E2D_CK(cudaFuncSetAttribute(ilu_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(s->ilu_factor_smem)));
   s->ilu_level = level;
   return 0;
 }
@@ -707,7 +718,7 @@ int precon_build(e2d_handle* h, const e2d_nks_params& p, double ao, const Blocks
     ilu_assemble_kernel<<<grid_for(nint) * 2, 128, 0, h->stream>>>(B, s->ilu, ao,
                                                                    p.jacobian_order == E2D_JACOBIAN_FIRST_ORDER_HLLE);
     E2D_CK(cudaGetLastError());
-    ilu_factor_kernel<<<h->B.nblk, ILU_THREADS, 0, h->stream>>>(B, s->ilu);
+    ilu_factor_kernel<<<h->B.nblk, ILU_THREADS, s->ilu_factor_smem, h->stream>>>(B, s->ilu);
     E2D_CK(cudaGetLastError());
     return 0;
   }

@@ -320,6 +320,31 @@ int Parse_Next_Input_Control_Parameter(Euler2D_Input_Parameters& IP, std::istrea
   if (code == "GMRES_Final_Tolerance") return num_d(N.gmres_tol_final, true);
   if (code == "GMRES_Epsilon_Naught") return num_d(N.epsilon0, true);
   if (code == "NKS_Min_Finite_Time_Step_Norm_Ratio") return num_d(N.min_ratio, true);
+  if (code == "GMRES_Block_Preconditioner") {
+    // "Diagonal" is block Jacobi; "ILUK" and any other value ILU(k)
+    std::string v;
+    if (str(v)) return INVALID_INPUT_CODE;
+    N.block_preconditioner = v == "Diagonal" ? E2D_PRECON_BLOCK_JACOBI : E2D_PRECON_BLOCK_ILUK;
+    return 0;
+  }
+  if (code == "GMRES_ILUK_Level_of_Fill") {
+    int rc = num_i(N.ilu_level_of_fill, 0);
+    return (rc || N.ilu_level_of_fill > 16) ? INVALID_INPUT_CODE : 0;
+  }
+  if (code == "Jacobian_Order") {
+    // Euler2D has the first-order HLLE and the source-terms-only Jacobians;
+    // the Roe, AUSM+up and second-order diamond-path ones stop the
+    // reference's run (no Euler2D specialization) and are rejected here; an
+    // unknown name falls back to first-order HLLE, as the reference's does.
+    std::string v;
+    if (str(v)) return INVALID_INPUT_CODE;
+    if (v == "Source_Terms_Only") N.jacobian_order = E2D_JACOBIAN_SOURCE_TERMS_ONLY;
+    else if (v == "First_Order_Inviscid_Roe" || v == "First_Order_Inviscid_AUSM_plus_up" ||
+             v.rfind("Second_Order_Diamond_Path_with_", 0) == 0)
+      return INVALID_INPUT_CODE;
+    else N.jacobian_order = E2D_JACOBIAN_FIRST_ORDER_HLLE;
+    return 0;
+  }
   // Any other keyword belongs to parts of the reference outside this path:
   // its value line is skipped and the keyword recorded.
   IP.Ignored.push_back(code);

@@ -228,6 +228,7 @@ int main(int argc, char** argv) {
     }
     fclose(f);
   }
-  printf("ok %zu %.17g %.17g %.17g\n", IP.Ignored.size(), IP.Wo.d, IP.Wo.v.x, IP.Wo.p);
+  printf("ok %zu %.17g %.17g %.17g %d %d %d\n", IP.Ignored.size(), IP.Wo.d, IP.Wo.v.x, IP.Wo.p,
+         IP.NKS.block_preconditioner, IP.NKS.ilu_level_of_fill, IP.NKS.jacobian_order);
   return 0;
 }

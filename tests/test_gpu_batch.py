@@ -51,9 +51,13 @@ def nks_cases():
             with_scheme(cases.bump_channel(nbi=6, nbj=3, nci=16, ncj=16, mach=1.3, h=0.05), **sc)]
 
 
-def test_batched_nks_equals_solo():
+@pytest.mark.parametrize("ilu_level", [None, 2])
+def test_batched_nks_equals_solo(ilu_level):
+    """Block Jacobi and ILU(k) alike: the preconditioner is built and applied
+    block by block, so a case's solve is the same in a batch as alone."""
     cs = nks_cases()
-    p = capi.nks_params(30, gmres_restart=20, max_gmres=120, overall_tol=1e-10, cfl0=10.0, gmres_tol=0.1)
+    p = capi.nks_params(30, gmres_restart=20, max_gmres=120, overall_tol=1e-10, cfl0=10.0, gmres_tol=0.1,
+                        ilu_level=ilu_level)
     hb = capi.BatchHandle(cs)
     hb.set_state()
     rc, hists = hb.nks(p)

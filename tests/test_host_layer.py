@@ -186,3 +186,30 @@ def test_solver_entry_point_writes_output(tmp_path):
     assert len(rows) == 32 * 32
     vals = np.array([[float(x) for x in r.split()] for r in rows])
     assert np.all(vals[:, 2] > 0) and np.all(vals[:, 5] > 0)
+
+
+@pytest.mark.parametrize("lines,want", [
+    ("", (0, 0, 0)),
+    ("GMRES_Block_Preconditioner =\nILUK\nGMRES_ILUK_Level_of_Fill =\n4\n", (1, 4, 0)),
+    ("GMRES_Block_Preconditioner =\nDiagonal\n", (0, 0, 0)),
+    ("GMRES_Block_Preconditioner =\nAnything\nJacobian_Order =\nSource_Terms_Only\n", (1, 0, 1)),
+    ("Jacobian_Order =\nFirst_Order_Inviscid_HLLE\n", (0, 0, 0)),
+    ("Jacobian_Order =\nSomething_Unknown\n", (0, 0, 0)),
+])
+def test_block_preconditioner_keywords(driver, tmp_path, lines, want):
+    """GMRES_Block_Preconditioner, GMRES_ILUK_Level_of_Fill and Jacobian_Order
+    as NKS_Input_Parameters parses them (NKSInput2D.h:523-560): "Diagonal" is
+    block Jacobi, any other value ILU(k); an unknown Jacobian order is
+    first-order HLLE."""
+    deck = write_deck(tmp_path / "p.in", text=DECK.replace("Execute", lines + "Execute"))
+    out = subprocess.run([driver, "parse", deck, str(tmp_path / "p.case")], capture_output=True, text=True,
+                         check=True).stdout.split()
+    assert tuple(int(x) for x in out[5:8]) == want
+
+
+@pytest.mark.parametrize("value", ["First_Order_Inviscid_Roe", "First_Order_Inviscid_AUSM_plus_up",
+                                   "Second_Order_Diamond_Path_with_HLLE"])
+def test_jacobian_orders_without_euler2d_specialization_are_rejected(driver, tmp_path, value):
+    deck = write_deck(tmp_path / "j.in", text=DECK.replace("Execute", "Jacobian_Order =\n%s\nExecute" % value))
+    r = subprocess.run([driver, "parse", deck, str(tmp_path / "j.case")], capture_output=True, text=True)
+    assert r.returncode == 3
