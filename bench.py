@@ -227,20 +227,21 @@ def nks_measure(precision, device, cpu, ilu_level=None):
     return out
 
 
-def nks_batch_measure(precision, device, n_cases=16):
+def nks_batch_measure(precision, device, n_cases=16, ilu_level=None):
     """A sweep of steady cases (cases.bump_family: Mach, bump height and
     block layout drawn per case, 8-48 blocks of 32x32 cells) solved to a
     1e-10 drop as one batched handle, and one after another on single-case
-    handles (the plain GPU path), from the freestream."""
+    handles (the plain GPU path), from the freestream; block Jacobi
+    (ilu_level None) or ILU(ilu_level)."""
     from cffc_b200 import capi, cases
     fam = cases.bump_family(n_cases, precision=precision)
-    p = capi.nks_params(**NKS_PARAMS)
+    p = capi.nks_params(**NKS_PARAMS, ilu_level=ilu_level)
     # handles (device allocation) are made before the clock starts; each
     # timed solve uploads the freestream state and runs to convergence
     hb = capi.BatchHandle(fam, device=device)
     solo = [capi.Handle(bs, device=device) for bs in fam]
     hb.set_state()
-    hb.nks(capi.nks_params(1, gmres_restart=30, max_gmres=5))  # warm-up: work arrays, first launches
+    hb.nks(capi.nks_params(1, gmres_restart=30, max_gmres=5, ilu_level=ilu_level))  # warm-up: work arrays
     t0 = time.perf_counter()
     hb.set_state()
     rc, hists = hb.nks(p)
@@ -248,7 +249,7 @@ def nks_batch_measure(precision, device, n_cases=16):
     hb.close()
     for h in solo:
         h.set_state()
-        h.nks(capi.nks_params(1, gmres_restart=30, max_gmres=5))
+        h.nks(capi.nks_params(1, gmres_restart=30, max_gmres=5, ilu_level=ilu_level))
     t0 = time.perf_counter()
     solo_ok = 0
     for h in solo:
@@ -260,7 +261,8 @@ def nks_batch_measure(precision, device, n_cases=16):
         h.close()
     conv = sum(int(x and x[-1]["ratio"] <= NKS_PARAMS["overall_tol"]) for x in hists)
     return {"workload": f"{n_cases} supersonic bump cases (cases.bump_family, 8-48 blocks of 32x32, "
-                        f"{sum(b.n_interior for b in fam)} cells in all), first order, to a 1e-10 drop",
+                        f"{sum(b.n_interior for b in fam)} cells in all), first order, to a 1e-10 drop, "
+                        + ("block-Jacobi" if ilu_level is None else "ILU(%d)" % ilu_level),
             "batched_seconds": round(t_batch, 3), "sequential_seconds": round(t_solo, 3),
             "speedup": round(t_solo / t_batch, 2), "converged": conv, "converged_sequential": solo_ok,
             "newton_steps": [len(x) - 1 for x in hists],
@@ -492,6 +494,7 @@ def main():
             line["nks"] = nks_measure(PRECISION[args.precision], local, not args.no_cpu_baseline)
             line["nks_iluk"] = nks_measure(PRECISION[args.precision], local, not args.no_cpu_baseline, ilu_level=2)
             line["nks_batch"] = nks_batch_measure(PRECISION[args.precision], local)
+            line["nks_batch_iluk"] = nks_batch_measure(PRECISION[args.precision], local, ilu_level=2)
             line["nks_learned"] = nks_learned_measure(local)
         print(json.dumps(line), flush=True)
     h.close()
