@@ -1192,3 +1192,22 @@ extern "C" int e2d_block_precon_apply(e2d_handle* h, const e2d_nks_params* p, do
   E2D_CK(cudaMemsetAsync(s->Z, 0, nb, h->stream));
   return check_status(h);
 }
+
+// The level-of-fill pattern the ILU(k) preconditioner uses for blocks of
+// nci x ncj cells (host work only, no device needed): interior rows in cell
+// order, columns ascending.  row_ptr gets nci*ncj + 1 offsets, col up to
+// cap column indices; *nnz the pattern's size (col untouched when it
+// exceeds cap); levels (may be NULL) the forward and backward level counts.
+extern "C" int e2d_ilu_pattern(int32_t nci, int32_t ncj, int32_t level, int32_t* row_ptr, int32_t* col,
+                               int32_t cap, int32_t* nnz, int32_t* levels) {
+  if (nci < 1 || ncj < 1 || level < 0 || level > 16 || !row_ptr || !nnz || cap < 0 ||
+      (long long)nci * ncj > (1 << 22))
+    return E2D_ERR_ARG;
+  IluPattern P;
+  if (!ilu_pattern(nci, ncj, level, P)) return E2D_ERR_NOMEM;
+  std::copy(P.row_ptr.begin(), P.row_ptr.end(), row_ptr);
+  *nnz = P.nnz;
+  if (col && P.nnz <= cap) std::copy(P.col.begin(), P.col.end(), col);
+  if (levels) { levels[0] = P.nflev; levels[1] = P.nblev; }
+  return 0;
+}

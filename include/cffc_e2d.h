@@ -300,6 +300,16 @@ int e2d_nks(e2d_handle *h, const e2d_nks_params *p, e2d_nks_step *hist, int *n_s
  * is left as it was; dt is overwritten.  Returns 0 or a library error. */
 int e2d_block_precon_apply(e2d_handle *h, const e2d_nks_params *p, double cfl, const double *v, double *z);
 
+/* The level-of-fill pattern of the ILU(k) preconditioner for blocks of
+ * nci x ncj cells, as BPKIT's symbolic_ilu (bpkit/src/SparseUtil.cc:198)
+ * builds it on the reference's block matrix (ghost rows included), then
+ * restricted to interior cells: row_ptr[nci*ncj + 1], col[*nnz] (interior
+ * cell index y*nci + x, ascending per row; written only when *nnz <= cap),
+ * levels[2] (may be NULL) the forward and backward dependency-level counts.
+ * Host work only.  Returns 0 or a library error. */
+int e2d_ilu_pattern(int32_t nci, int32_t ncj, int32_t level, int32_t *row_ptr, int32_t *col, int32_t cap,
+                    int32_t *nnz, int32_t *levels);
+
 /* Device status word: 0 or the first error a kernel recorded. */
 int e2d_status(e2d_handle *h);
 
