@@ -618,9 +618,9 @@ int nks_setup(e2d_handle* h, int m) {
   E2D_CK(cudaMemsetAsync(s->bvec, 0, sizeof(double) * n, h->stream));
   E2D_CK(cudaMemsetAsync(s->step0, 0, sizeof(int), h->stream));
   E2D_CK(cudaMemsetAsync(s->counter, 0, sizeof(unsigned) * C, h->stream));
-  // enough CTAs per block for small block counts (about 2048 double2 / 512
+  // enough CTAs per block for small block counts (about 512 double2 / 512
   // cells per CTA), at most 16
-  s->ch_vec = std::max(1, std::min(16, s->nper4 / 2 / 2048));
+  s->ch_vec = std::max(1, std::min(16, s->nper4 / 2 / 512));
   s->graphs.assign(m, nullptr);
   s->graph_uses.assign(m, 0);
   s->ch_cell = std::max(1, std::min(16, h->B.NCi * h->B.NCj / 512));
