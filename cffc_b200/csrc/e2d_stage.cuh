@@ -62,7 +62,13 @@ using RT = float;   // reconstruction and flux arithmetic
 using RT = double;
 #endif
 
-constexpr int TI = 32, TJ = 8;          // interior cells per tile
+#ifndef E2D_TI
+#define E2D_TI 32
+#endif
+#ifndef E2D_TJ
+#define E2D_TJ 8
+#endif
+constexpr int TI = E2D_TI, TJ = E2D_TJ;  // interior cells per tile
 constexpr int HI = TI + 4, HJ = TJ + 4; // W tile with 2-cell halo
 constexpr int NI = TI + 5, NJ = TJ + 5; // nodes of the halo tile
 constexpr int RI = TI + 2, RJ = TJ + 2; // cells reconstructed (tile + 1 ring)
