@@ -277,6 +277,20 @@ def restart_deck(restart, extra="", grid=BUMP_GRID):
                                grid=grid)
 
 
+# deck D: Newton-Krylov with the ILU(2) preconditioner, first order, from the
+# freestream on the grid data file (no explicit steps)
+NKS_ILU_EXTRA = ("Maximum_Number_of_NKS_Iterations =\n12\nNKS_Overall_Tolerance =\n1e-10\n"
+                 "NKS_Finite_Time_Step_Initial_CFL =\n10.0\nGMRES_Tolerance =\n0.1\nGMRES_Restart =\n30\n"
+                 "Maximum_Number_of_GMRES_Iterations =\n100\nGMRES_Block_Preconditioner =\nILUK\n"
+                 "GMRES_ILUK_Level_of_Fill =\n2\nJacobian_Order =\nFirst_Order_Inviscid_HLLE\n")
+
+
+def nks_deck():
+    text = restart_deck(False, extra=DATA_GRID_FILE + NKS_ILU_EXTRA, grid=DATA_GRID)
+    text = text.replace("Limiter_Type =\nVenkatakrishnan", "Limiter_Type =\nZero")
+    return text.replace("Maximum_Number_of_Time_Steps =\n20", "Maximum_Number_of_Time_Steps =\n0")
+
+
 def make_restart_fixture():
     """tests/golden/restart.tar.gz: restart files the reference wrote and what
     its own reader (Read_QuadTree + Read_Restart_Solution) makes of them
@@ -288,15 +302,17 @@ def make_restart_fixture():
       bump2/  deck C's: deck A on the grid data file bumpgrid.grid (bump0's
               grids as Write_Quad_Block writes them) read back by the
               reference (Grid_Type Read_From_Data_File)
+      bump3/  deck D's: Newton-Krylov with ILU(2), first order, on the same
+              grid data file, from the freestream
       grid/   grid data files of the channel case and of a periodic box
-    and the three decks."""
+    and the four decks."""
     import shutil
     import tarfile
     ch_char = cases.channel(bc=dict(W=cases.BC_CHARACTERISTIC, E=cases.BC_CHARACTERISTIC,
                                     S=cases.BC_REFLECTION, N=cases.BC_CONSTANT_EXTRAPOLATION), seed=8)
     with tempfile.TemporaryDirectory() as td:
         root = os.path.join(td, "restart")
-        for d in ("chan", "bump0", "bump1", "bump2", "grid"):
+        for d in ("chan", "bump0", "bump1", "bump2", "bump3", "grid"):
             os.makedirs(os.path.join(root, d))
         grid = os.path.join(root, "grid")
         for name, bs in (("chan", ch_char), ("box", cases.periodic_box_bumps(nb=2, nc=8, seed=11))):
@@ -309,14 +325,16 @@ def make_restart_fixture():
         subprocess.run([HARNESS, "restart_write", cp, "chan", "17", "0.25"], cwd=chan, check=True)
         subprocess.run([HARNESS, "restart_read", cp, "chan", "read.bin"], cwd=chan, check=True)
         for name, text in (("deck_a.in", restart_deck(False)), ("deck_b.in", restart_deck(True)),
-                           ("deck_c.in", restart_deck(False, extra=DATA_GRID_FILE, grid=DATA_GRID))):
+                           ("deck_c.in", restart_deck(False, extra=DATA_GRID_FILE, grid=DATA_GRID)),
+                           ("deck_d.in", nks_deck())):
             with open(os.path.join(root, name), "w") as f:
                 f.write(text)
         dummy = os.path.join(td, "bump.case")  # block count and wiring for restart_read
         cases.write_case(dummy, cases.channel(nbi=4, nbj=2))
         run = os.path.join(td, "run")
         os.makedirs(run)
-        for stage, deck in (("bump0", "deck_a.in"), ("bump1", "deck_b.in"), ("bump2", "deck_c.in")):
+        for stage, deck in (("bump0", "deck_a.in"), ("bump1", "deck_b.in"), ("bump2", "deck_c.in"),
+                            ("bump3", "deck_d.in")):
             subprocess.run([HARNESS, "solve", os.path.join(root, deck)], cwd=run, check=True,
                            capture_output=True)
             dst = os.path.join(root, stage)
