@@ -37,7 +37,8 @@ struct IluPattern {
   int nrow = 0, nnz = 0, nflev = 0, nblev = 0, maxrow = 0, maxops = 0, level = -1, nci = 0, ncj = 0;
   std::vector<int> row_ptr, nlow, col, fop_ptr, flev_ptr, flev_rows, blev_ptr, blev_rows, apos;
   std::vector<int2> fop;
-  std::vector<int4> fdesc, bdesc;
+  std::vector<int4> fdesc, bdesc, xdesc;
+  std::vector<int2> xops;
 };
 
 struct IluDev {
@@ -46,6 +47,8 @@ struct IluDev {
   const int2* fop;
   const int *flev_ptr, *flev_rows, *blev_ptr, *blev_rows, *apos;
   const int4 *fdesc, *bdesc;  // per level-ordered row: (row, first entry, end entry, 0)
+  const int4* xdesc;          // factorization, level order: (row, first entry, L entries, entries)
+  const int2* xops;           // factorization, level order: the row's elimination list range
   double* vals;
   double* dinv;
   double* work;  // [nblk][nrow][4] when a block's vector does not fit shared memory
@@ -170,10 +173,14 @@ inline bool ilu_pattern(int nci, int ncj, int k_fill, IluPattern& P) {
   // the diagonal (backward)
   P.fdesc.resize(nr);
   P.bdesc.resize(nr);
+  P.xdesc.resize(nr);
+  P.xops.resize(nr);
   for (int q = 0; q < nr; ++q) {
     const int i = P.flev_rows[q], k = P.blev_rows[q];
     P.fdesc[q] = make_int4(i, P.row_ptr[i], P.row_ptr[i] + P.nlow[i], 0);
     P.bdesc[q] = make_int4(k, P.row_ptr[k] + P.nlow[k] + 1, P.row_ptr[k + 1], 0);
+    P.xdesc[q] = make_int4(i, P.row_ptr[i], P.nlow[i], P.row_ptr[i + 1] - P.row_ptr[i]);
+    P.xops[q] = make_int2(P.fop_ptr[P.row_ptr[i]], P.fop_ptr[P.row_ptr[i] + P.nlow[i]]);
   }
   // where cell c's column blocks go: its diagonal, then the rows of the
   // cells below (j-1), above (j+1), left (i-1), right (i+1) — the reference's
@@ -309,11 +316,16 @@ __global__ void __launch_bounds__(ILU_THREADS) ilu_factor_kernel(Blocks B, IluDe
   int* gcol = reinterpret_cast<int*>(row + 16 * D.maxrow);
   int* gfp = gcol + D.maxrow;
   int2* gops = reinterpret_cast<int2*>(gfp + D.maxrow + 2);
+  __shared__ int lev_ptr[2];
   for (int L = 0; L < D.nflev; ++L) {
-    for (int q = D.flev_ptr[L] + grp; q < D.flev_ptr[L + 1]; q += ILU_THREADS / 16) {
-      const int i = D.flev_rows[q];
-      const int e0 = D.row_ptr[i], nL = D.nlow[i], nE = D.row_ptr[i + 1] - e0;
-      const int ob = D.fop_ptr[e0], oe = D.fop_ptr[e0 + nL];
+    if (threadIdx.x < 2) lev_ptr[threadIdx.x] = D.flev_ptr[L + threadIdx.x];
+    __syncthreads();
+    const int q0 = lev_ptr[0], q1 = lev_ptr[1];
+    for (int q = q0 + grp; q < q1; q += ILU_THREADS / 16) {
+      const int4 xd = D.xdesc[q];
+      const int2 xo = D.xops[q];
+      const int i = xd.x, e0 = xd.y, nL = xd.z, nE = xd.w;
+      const int ob = xo.x, oe = xo.y;
       for (int e = 0; e < nE; ++e) row[16 * e + lane] = V[16 * size_t(e0 + e) + lane];
       for (int t = lane; t < nE; t += 16) gcol[t] = D.col[e0 + t];
       for (int t = lane; t <= nL; t += 16) gfp[t] = D.fop_ptr[e0 + t] - ob;

@@ -394,10 +394,13 @@ __device__ bool invert4(double a[4][4]) {
       if (fabs(a[r][k]) > best) { best = fabs(a[r][k]); p = r; }
     piv[k] = p;
     if (best == 0.0) return false;
-    if (p != k) {
+    // row interchange written with static indices only (keeps a[][] in registers)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) { const double t = a[k][c]; a[k][c] = a[p][c]; a[p][c] = t; }
-    }
+    for (int r = k + 1; r < 4; ++r)
+      if (r == p) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) { const double t = a[k][c]; a[k][c] = a[r][c]; a[r][c] = t; }
+      }
     const double rp = 1.0 / a[k][k];
 #pragma unroll
     for (int r = k + 1; r < 4; ++r) {
@@ -439,10 +442,12 @@ __device__ bool invert4(double a[4][4]) {
 #pragma unroll
   for (int j = 2; j >= 0; --j) {
     const int p = piv[j];
-    if (p != j) {
 #pragma unroll
-      for (int r = 0; r < 4; ++r) { const double t = a[r][j]; a[r][j] = a[r][p]; a[r][p] = t; }
-    }
+    for (int c = j + 1; c < 4; ++c)
+      if (c == p) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) { const double t = a[r][j]; a[r][j] = a[r][c]; a[r][c] = t; }
+      }
   }
   return true;
 }
@@ -659,7 +664,7 @@ int ilu_setup(e2d_handle* h, int level) {
   };
   const int nblk = h->B.nblk;
   int rc;
-  void *a0, *a1, *a2, *a3, *a4, *a5, *a6, *a7, *a8, *a9, *d0, *d1, *v0, *v1;
+  void *a0, *a1, *a2, *a3, *a4, *a5, *a6, *a7, *a8, *a9, *d0, *d1, *x0, *x1, *v0, *v1;
   if ((rc = up(P.row_ptr.data(), sizeof(int) * P.row_ptr.size(), &a0)) ||
       (rc = up(P.nlow.data(), sizeof(int) * P.nlow.size(), &a1)) ||
       (rc = up(P.col.data(), sizeof(int) * P.col.size(), &a2)) ||
@@ -672,6 +677,8 @@ int ilu_setup(e2d_handle* h, int level) {
       (rc = up(P.apos.data(), sizeof(int) * P.apos.size(), &a9)) ||
       (rc = up(P.fdesc.data(), sizeof(int4) * P.fdesc.size(), &d0)) ||
       (rc = up(P.bdesc.data(), sizeof(int4) * P.bdesc.size(), &d1)) ||
+      (rc = up(P.xdesc.data(), sizeof(int4) * P.xdesc.size(), &x0)) ||
+      (rc = up(P.xops.data(), sizeof(int2) * P.xops.size(), &x1)) ||
       (rc = up(nullptr, sizeof(double) * 16 * size_t(P.nnz) * nblk, &v0)) ||
       (rc = up(nullptr, sizeof(double) * 16 * size_t(P.nrow) * nblk, &v1)))
     return rc;
@@ -680,6 +687,7 @@ int ilu_setup(e2d_handle* h, int level) {
   D.flev_ptr = static_cast<int*>(a5); D.flev_rows = static_cast<int*>(a6);
   D.blev_ptr = static_cast<int*>(a7); D.blev_rows = static_cast<int*>(a8); D.apos = static_cast<int*>(a9);
   D.fdesc = static_cast<int4*>(d0); D.bdesc = static_cast<int4*>(d1);
+  D.xdesc = static_cast<int4*>(x0); D.xops = static_cast<int2*>(x1);
   D.vals = static_cast<double*>(v0); D.dinv = static_cast<double*>(v1);
   // a block's vector in shared memory when it fits, else a global work array
   const size_t smem = sizeof(double) * 4 * size_t(P.nrow) + sizeof(int4) * 2 * size_t(P.nrow) +

@@ -327,6 +327,17 @@ int Parse_Next_Input_Control_Parameter(Euler2D_Input_Parameters& IP, std::istrea
     N.block_preconditioner = v == "Diagonal" ? E2D_PRECON_BLOCK_JACOBI : E2D_PRECON_BLOCK_ILUK;
     return 0;
   }
+  if (code == "GMRES_Overlap") {
+    // Schwarz overlap: only 0 (no overlap, the reference's default) is built
+    int ov = 0;
+    return (num_i(ov, 0) || ov != 0) ? INVALID_INPUT_CODE : 0;
+  }
+  if (code == "NKS_Finite_Time_Step" || code == "GMRES_Normalization") {
+    // both on by default in the reference; OFF (or 0) runs are not built
+    std::string v;
+    if (str(v)) return INVALID_INPUT_CODE;
+    return (v == "OFF" || v == "0") ? INVALID_INPUT_CODE : 0;
+  }
   if (code == "GMRES_ILUK_Level_of_Fill") {
     int rc = num_i(N.ilu_level_of_fill, 0);
     return (rc || N.ilu_level_of_fill > 16) ? INVALID_INPUT_CODE : 0;

@@ -213,3 +213,17 @@ def test_jacobian_orders_without_euler2d_specialization_are_rejected(driver, tmp
     deck = write_deck(tmp_path / "j.in", text=DECK.replace("Execute", "Jacobian_Order =\n%s\nExecute" % value))
     r = subprocess.run([driver, "parse", deck, str(tmp_path / "j.case")], capture_output=True, text=True)
     assert r.returncode == 3
+
+
+@pytest.mark.parametrize("lines,ok", [
+    ("GMRES_Overlap =\n0\n", True), ("GMRES_Overlap =\n1\n", False),
+    ("NKS_Finite_Time_Step =\nON\n", True), ("NKS_Finite_Time_Step =\nOFF\n", False),
+    ("GMRES_Normalization =\nON\n", True), ("GMRES_Normalization =\n0\n", False),
+])
+def test_nks_options_outside_the_built_solver_are_rejected(driver, tmp_path, lines, ok):
+    """Schwarz overlap, fixed-CFL Newton steps and unnormalized GMRES are not
+    built: a deck asking for them is rejected instead of silently run with the
+    reference's defaults."""
+    deck = write_deck(tmp_path / "o.in", text=DECK.replace("Execute", lines + "Execute"))
+    r = subprocess.run([driver, "parse", deck, str(tmp_path / "o.case")], capture_output=True, text=True)
+    assert (r.returncode == 0) == ok
