@@ -281,44 +281,52 @@ def nks_learned_measure(device):
     p = capi.nks_params(**NKS_PARAMS)
     net, info = warmstart.train_network(cases.bump_family(48, seed=101), p, device=device)
     test = cases.bump_family(16, seed=202)
-    hb = capi.BatchHandle(test, device=device)
-    solo = [capi.Handle(bs, device=device) for bs in test]
-    hb.set_state()
-    hb.nks(capi.nks_params(1, gmres_restart=30, max_gmres=5))  # warm-up
-    for h in solo:
-        h.set_state()
-        h.nks(capi.nks_params(1, gmres_restart=30, max_gmres=5))
-    t0 = time.perf_counter()
-    rc_c, cold, cold_states = warmstart.solve_family(test, p, handle=hb)
-    t_cold = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    rc_w, warm, warm_states, fallback = warmstart.warm_solve(net, test, p, handle=hb)
-    t_warm = time.perf_counter() - t0
-    hb.close()
-    t0 = time.perf_counter()
-    for h in solo:
-        h.set_state()
-        h.nks(p)
-    t_seq = time.perf_counter() - t0
-    for h in solo:
-        h.close()
-    err = max(warmstart.l2_cells(bs.interior(a[1]), bs.interior(b[1]))
-              for bs, a, b in zip(test, warm_states, cold_states))
     tol = NKS_PARAMS["overall_tol"]
-    return {"workload": "16 held-out cases of cases.bump_family (seed 202), network trained on 48 (seed 101)",
-            "training": info,
-            "warm_batched_seconds": round(t_warm, 3), "cold_batched_seconds": round(t_cold, 3),
-            "cold_sequential_seconds": round(t_seq, 3),
-            "speedup_vs_plain_sequential": round(t_seq / t_warm, 2),
-            "speedup_vs_cold_batched": round(t_cold / t_warm, 2),
-            "newton_steps_warm": int(sum(len(x) - 1 for x in warm)),
-            "newton_steps_cold": int(sum(len(x) - 1 for x in cold)),
-            "gmres_iterations_warm": int(sum(st["gmres_iters"] for x in warm for st in x)),
-            "gmres_iterations_cold": int(sum(st["gmres_iters"] for x in cold for st in x)),
-            "converged_warm": int(sum(x[-1]["ratio"] <= tol for x in warm)),
-            "converged_cold": int(sum(x[-1]["ratio"] <= tol for x in cold)),
-            "fallback_cases": len(fallback),
-            "max_l2_error_warm_vs_cold": float(err), "rc": [rc_w, rc_c]}
+
+    def timings(p):
+        ilu = None if p.block_preconditioner == capi.PRECON_BLOCK_JACOBI else p.ilu_level_of_fill
+        warm_p = capi.nks_params(1, gmres_restart=30, max_gmres=5, ilu_level=ilu)
+        hb = capi.BatchHandle(test, device=device)
+        solo = [capi.Handle(bs, device=device) for bs in test]
+        hb.set_state()
+        hb.nks(warm_p)  # warm-up
+        for h in solo:
+            h.set_state()
+            h.nks(warm_p)
+        t0 = time.perf_counter()
+        rc_c, cold, cold_states = warmstart.solve_family(test, p, handle=hb)
+        t_cold = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        rc_w, warm, warm_states, fallback = warmstart.warm_solve(net, test, p, handle=hb)
+        t_warm = time.perf_counter() - t0
+        hb.close()
+        t0 = time.perf_counter()
+        for h in solo:
+            h.set_state()
+            h.nks(p)
+        t_seq = time.perf_counter() - t0
+        for h in solo:
+            h.close()
+        err = max(warmstart.l2_cells(bs.interior(a[1]), bs.interior(b[1]))
+                  for bs, a, b in zip(test, warm_states, cold_states))
+        return {"warm_batched_seconds": round(t_warm, 3), "cold_batched_seconds": round(t_cold, 3),
+                "cold_sequential_seconds": round(t_seq, 3),
+                "speedup_vs_plain_sequential": round(t_seq / t_warm, 2),
+                "speedup_vs_cold_batched": round(t_cold / t_warm, 2),
+                "newton_steps_warm": int(sum(len(x) - 1 for x in warm)),
+                "newton_steps_cold": int(sum(len(x) - 1 for x in cold)),
+                "gmres_iterations_warm": int(sum(st["gmres_iters"] for x in warm for st in x)),
+                "gmres_iterations_cold": int(sum(st["gmres_iters"] for x in cold for st in x)),
+                "converged_warm": int(sum(x[-1]["ratio"] <= tol for x in warm)),
+                "converged_cold": int(sum(x[-1]["ratio"] <= tol for x in cold)),
+                "fallback_cases": len(fallback),
+                "max_l2_error_warm_vs_cold": float(err), "rc": [rc_w, rc_c]}
+
+    out = {"workload": "16 held-out cases of cases.bump_family (seed 202), network trained on 48 (seed 101)",
+           "training": info}
+    out.update(timings(p))                     # block Jacobi, as the plain reference solver
+    out["iluk2"] = timings(capi.nks_params(**NKS_PARAMS, ilu_level=2))  # the same, with ILU(2)
+    return out
 
 
 def workload():
