@@ -182,6 +182,9 @@ def golden_cases():
         ("precon_bump_iluk4", bump, "precon", (100.0, 4, 4)),
         ("precon_bump_bj_global_iluk1", bump_bj, "precon", (5.0, 1, 5)),
         ("precon_curv_iluk3", curv, "precon", (3.0, 3, 6)),
+        # one 64x60 channel block: the solve's vector and descriptors exceed
+        # shared memory, so the device works them in global memory
+        ("precon_channel64_iluk1", cases.channel(nbi=1, nbj=1, nci=64, ncj=60, seed=7), "precon", (2.0, 1, 7)),
     ] + [
         # the other explicit schemes (optimally smoothing multistage, RK4, RK5),
         # implicit residual smoothing and limiter freezing
