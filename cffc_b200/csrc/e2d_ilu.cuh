@@ -286,6 +286,9 @@ __global__ void __launch_bounds__(128) ilu_assemble_kernel(Blocks B, IluDev D, d
 }
 
 constexpr int ILU_THREADS = 256;
+// the solves: 32 rows of a level at a time (4 threads per row); fewer idle
+// warps share the schedulers with the ones on the critical path
+constexpr int ILU_APPLY_THREADS = 128;
 
 // BILUK::setup's numeric factorization (BILUK.cc:85-150), one CTA per
 // block, rows level by level; a row is worked by 16 threads, one per element
@@ -494,7 +497,7 @@ __device__ __forceinline__ double row_finish(const RowPre& p, const double* __re
 // variable), rows level by level; the block's vector is worked in shared
 // memory (SHARED) or in D.work.
 template <bool SHARED>
-__global__ void __launch_bounds__(ILU_THREADS) ilu_apply_kernel(Blocks B, IluDev D, const double* __restrict__ v,
+__global__ void __launch_bounds__(ILU_APPLY_THREADS) ilu_apply_kernel(Blocks B, IluDev D, const double* __restrict__ v,
                                                                 double* __restrict__ z) {
   extern __shared__ double ysh[];
   const int b = blockIdx.x;
@@ -513,13 +516,13 @@ __global__ void __launch_bounds__(ILU_THREADS) ilu_apply_kernel(Blocks B, IluDev
     int4* bd = fd + D.nrow;
     int* fl = reinterpret_cast<int*>(bd + D.nrow);
     int* bl = fl + D.nflev + 1;
-    for (int t = threadIdx.x; t < D.nrow; t += ILU_THREADS) { fd[t] = D.fdesc[t]; bd[t] = D.bdesc[t]; }
-    for (int t = threadIdx.x; t <= D.nflev; t += ILU_THREADS) fl[t] = D.flev_ptr[t];
-    for (int t = threadIdx.x; t <= D.nblev; t += ILU_THREADS) bl[t] = D.blev_ptr[t];
+    for (int t = threadIdx.x; t < D.nrow; t += ILU_APPLY_THREADS) { fd[t] = D.fdesc[t]; bd[t] = D.bdesc[t]; }
+    for (int t = threadIdx.x; t <= D.nflev; t += ILU_APPLY_THREADS) fl[t] = D.flev_ptr[t];
+    for (int t = threadIdx.x; t <= D.nblev; t += ILU_APPLY_THREADS) bl[t] = D.blev_ptr[t];
     fdesc = fd; bdesc = bd; flp = fl; blp = bl;
   }
   const size_t base = size_t(b) * B.NCj * B.NCi;
-  for (int t = threadIdx.x; t < 4 * D.nrow; t += ILU_THREADS) {
+  for (int t = threadIdx.x; t < 4 * D.nrow; t += ILU_APPLY_THREADS) {
     const int r = t >> 2;
     y[t] = v[4 * (base + size_t(NG + r / B.nci) * B.NCi + NG + r % B.nci) + (t & 3)];
   }
@@ -533,7 +536,7 @@ __global__ void __launch_bounds__(ILU_THREADS) ilu_apply_kernel(Blocks B, IluDev
   for (int L = 1; L < D.nflev; ++L) {
     row_prefetch<false>(fdesc, flp, L + 1, D.nflev, grp, k, V, Di, D.col, nxt);
     if (cur.i >= 0) y[4 * cur.i + k] = row_finish(cur, V, y, D.col, k, y[4 * cur.i + k]);
-    for (int q = flp[L] + grp + ILU_THREADS / 4; q < flp[L + 1]; q += ILU_THREADS / 4) {
+    for (int q = flp[L] + grp + ILU_APPLY_THREADS / 4; q < flp[L + 1]; q += ILU_APPLY_THREADS / 4) {
       const int4 d = fdesc[q];
       y[4 * d.x + k] = row_solve(V, y, D.col, d.y, d.z, k, y[4 * d.x + k]);
     }
@@ -556,7 +559,7 @@ __global__ void __launch_bounds__(ILU_THREADS) ilu_apply_kernel(Blocks B, IluDev
       __syncwarp(qmask);
       y[4 * i + k] = x;
     }
-    for (int q = blp[L] + grp + ILU_THREADS / 4; q < blp[L + 1]; q += ILU_THREADS / 4) {
+    for (int q = blp[L] + grp + ILU_APPLY_THREADS / 4; q < blp[L + 1]; q += ILU_APPLY_THREADS / 4) {
       const int4 d = bdesc[q];
       const double* Dd = Di + 16 * size_t(d.x) + 4 * k;
       const double d0 = Dd[0], d1 = Dd[1], d2 = Dd[2], d3 = Dd[3];
@@ -573,7 +576,7 @@ __global__ void __launch_bounds__(ILU_THREADS) ilu_apply_kernel(Blocks B, IluDev
     __syncthreads();
     cur = nxt;
   }
-  for (int t = threadIdx.x; t < 4 * D.nrow; t += ILU_THREADS) {
+  for (int t = threadIdx.x; t < 4 * D.nrow; t += ILU_APPLY_THREADS) {
     const int r = t >> 2;
     z[4 * (base + size_t(NG + r / B.nci) * B.NCi + NG + r % B.nci) + (t & 3)] = y[t];
   }

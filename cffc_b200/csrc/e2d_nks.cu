@@ -842,9 +842,9 @@ void apply_rotation(double& dx, double& dy, double cs, double sn) {
 int ilu_apply(e2d_handle* h, const double* v, double* z) {
   e2d_nks_state* s = h->nks;
   if (s->ilu_smem)
-    ilu_apply_kernel<true><<<h->B.nblk, ILU_THREADS, s->ilu_smem, h->stream>>>(act(h), s->ilu, v, z);
+    ilu_apply_kernel<true><<<h->B.nblk, ILU_APPLY_THREADS, s->ilu_smem, h->stream>>>(act(h), s->ilu, v, z);
   else
-    ilu_apply_kernel<false><<<h->B.nblk, ILU_THREADS, 0, h->stream>>>(act(h), s->ilu, v, z);
+    ilu_apply_kernel<false><<<h->B.nblk, ILU_APPLY_THREADS, 0, h->stream>>>(act(h), s->ilu, v, z);
   E2D_CK(cudaGetLastError());
   return 0;
 }
