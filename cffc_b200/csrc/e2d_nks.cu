@@ -549,7 +549,8 @@ struct e2d_nks_state {
   std::vector<cudaGraphExec_t> graphs;  // Arnoldi step j, captured on its second use
   std::vector<int> graph_uses;
   double graph_eps0 = -1.0;
-  int graph_ilu = -1;        // preconditioner kind the graphs were captured with
+  int graph_ilu = -2;        // preconditioner the graphs were captured with:
+                             // the ILU level of fill, -1 block Jacobi
   double* eps = nullptr;     // [ncase]
   double* nrm = nullptr;     // [ncase]
   double* hcol = nullptr;    // [m + 2][ncase]
@@ -582,6 +583,16 @@ void nks_free(e2d_handle* h) {
 namespace {
 
 using namespace e2d_host;
+
+// Destroys the captured Arnoldi-step graphs: they hold the preconditioner's
+// device pointers and launch shapes by value, so they must go before any of
+// those arrays is freed or resized.
+void drop_graphs(e2d_nks_state* s) {
+  for (auto& g : s->graphs)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  std::fill(s->graph_uses.begin(), s->graph_uses.end(), 0);
+  s->graph_ilu = -2;
+}
 
 template <class T> int nalloc(e2d_nks_state* s, T** p, size_t n) {
   void* q = nullptr;
@@ -645,6 +656,7 @@ int grid_for(long long n) {
 int ilu_setup(e2d_handle* h, int level) {
   e2d_nks_state* s = h->nks;
   if (s->ilu_level == level) return 0;
+  drop_graphs(s);  // they reference the arrays freed next
   for (void* p : s->ilu_allocs) cudaFree(p);
   s->ilu_allocs.clear();
   s->ilu_level = -1;
@@ -706,7 +718,9 @@ int ilu_setup(e2d_handle* h, int level) {
   }
   // one row (blocks, columns, work list) per 16-thread group
   s->ilu_factor_smem = ilu_factor_smem_bytes(P);
-  if (s->ilu_factor_smem > size_t(optin)) return E2D_ERR_ARG;
+  cudaFuncAttributes fa{};
+  E2D_CK(cudaFuncGetAttributes(&fa, ilu_factor_kernel));  // its static shared memory counts too
+  if (s->ilu_factor_smem + fa.sharedSizeBytes > size_t(optin)) return E2D_ERR_ARG;
   E2D_CK(cudaFuncSetAttribute(ilu_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               int(s->ilu_factor_smem)));
   s->ilu_level = level;
@@ -770,11 +784,7 @@ cudaError_t launch_frechet(e2d_handle* h, const double* z, double* v, const Norm
   a.nks_v = v;
   a.nks_eps = h->nks->eps;
   for (int k = 0; k < 4; ++k) { a.normU[k] = nm.u[k]; a.normR[k] = nm.r[k]; }
-  int ti, tj;
-  stage_tile(h->sc.precision, &ti, &tj);
-  a.tiles_i = (h->B.nci + ti - 1) / ti;
-  a.tiles_j = (h->B.ncj + tj - 1) / tj;
-  return launch_stage_prec(h->sc.precision, a, h->stream);
+  return launch_stage_args(h, a);
 }
 
 // Perturbed residual + Frechet product: U = Uo + eps*dir (all cells), ghost
@@ -888,12 +898,11 @@ int arnoldi_step(e2d_handle* h, int j, double eps0, const Norm4& nm, bool ilu) {
 // memory at run time.
 int run_arnoldi(e2d_handle* h, int j, double eps0, const Norm4& nm, bool ilu) {
   e2d_nks_state* s = h->nks;
-  if (s->graph_eps0 != eps0 || s->graph_ilu != int(ilu)) {
-    for (auto& g : s->graphs)
-      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-    std::fill(s->graph_uses.begin(), s->graph_uses.end(), 0);
+  const int key = ilu ? s->ilu_level : -1;
+  if (s->graph_eps0 != eps0 || s->graph_ilu != key) {
+    drop_graphs(s);
     s->graph_eps0 = eps0;
-    s->graph_ilu = int(ilu);
+    s->graph_ilu = key;
   }
   if (s->graphs[j]) {
     E2D_CK(cudaGraphLaunch(s->graphs[j], h->stream));

@@ -353,8 +353,10 @@ int e2d_fastmath_check(const double *x, int n, double *out);
  * doubles (96 KiB), held on every GPU that loads the library until exit;
  * nblk above E2D_NORMS_STATIC_MAX_BLOCKS is rejected with E2D_ERR_ARG.
  * The first call on a device looks up the array's device address (with that
- * device current); make that first call before any stream capture.  All
- * calls share the array: calls that overlap on the GPU race. */
+ * device current); that lookup may load the library's device code, which
+ * can allocate device memory, so make the first call at start-up, before
+ * any stream capture.  Later calls allocate nothing.  All calls share the
+ * array: calls that overlap on the GPU race. */
 int e2d_residual_norms_static(const double *dUdt, int32_t nblk, int32_t nci, int32_t ncj,
                               double *out, void *stream);
 

@@ -4,10 +4,14 @@ library).  It serves callers that cannot allocate device memory when they
 need the norms — e.g. a solver loop where cudaMalloc could stall the device,
 or a plugin whose host process owns the whole device-memory budget.
 
-The test calls it through the C ABI on two block sets in a row (the second
-smaller than the first, so stale scratch from the first call would show) and
-checks each result against the allocating entry point e2d_norms.  It runs
-alone in a fresh process as well as after the rest of the suite.
+The test calls it through the C ABI on two block sets of different sizes in
+a row, and checks each result against the allocating entry point e2d_norms:
+each call's result must depend on its own input only, whatever the shared
+scratch held before.  It also checks the property the entry point exists
+for: once the first call on the device has been made (that call may load the
+library's device code, which can allocate), a further call leaves the free
+device memory unchanged.  It runs alone in a fresh process as well as after
+the rest of the suite.
 """
 import ctypes as C
 
@@ -58,6 +62,14 @@ def test_static_norms_match_allocating_norms_twice():
         got = out.cpu().numpy()
         assert np.all(expected > 0)
         np.testing.assert_allclose(got, expected, rtol=RTOL, atol=0)
+        # after the first call: no device allocation by a further call
+        free_before, _ = torch.cuda.mem_get_info()
+        rc = norms_static(_device_dudt(h), bs.nblk, bs.nci, bs.ncj,
+                          C.c_void_p(out.data_ptr()), C.c_void_p(stream.cuda_stream))
+        torch.cuda.synchronize()
+        free_after, _ = torch.cuda.mem_get_info()
+        assert rc == 0 and free_after == free_before
+        np.testing.assert_allclose(out.cpu().numpy(), expected, rtol=RTOL, atol=0)
         h.close()
 
 
