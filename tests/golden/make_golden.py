@@ -37,6 +37,7 @@ from cffc_b200 import cases  # noqa: E402
 
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "e2d_ref_harness")
 OUT = os.path.dirname(os.path.abspath(__file__))
+NKS_SUB = 4  # large NKS fixtures keep the final state on every 4th cell in i and j
 
 
 def run_residual(bs):
@@ -149,6 +150,9 @@ def golden_cases():
                                  scheme=cases.Scheme(limiter=cases.LIMITER_BARTH_JESPERSEN, local_dt=0))
     bump_m14 = cases.bump_channel(nbi=6, nbj=2, nci=16, ncj=16, mach=1.4, h=0.04,
                                   scheme=cases.Scheme(limiter=cases.LIMITER_ZERO, local_dt=1))
+    c2 = cases.bump_channel()  # 12 x 4 blocks of 64 x 32, h 0.1, Mach 0.5
+    box21 = cases.periodic_box_bumps(nb=2, nbj=1, nc=16, seed=31)
+    box11 = cases.periodic_box_bumps(nb=1, nc=16, seed=32)
     ch_ms = cases.channel(nbi=2, nbj=2, nci=12, ncj=10, seed=9,
                           scheme=cases.Scheme(limiter=cases.LIMITER_VENKATAKRISHNAN, cfl=0.8, n_stage=4, local_dt=1))
     return [
@@ -161,6 +165,12 @@ def golden_cases():
         ("explicit_channel_local_bj_40", ch_bj, "explicit", 40),
         ("explicit_channel_char_40", ch_char, "explicit", 40),
         ("explicit_curv_4x2x16_30", curv, "explicit", 30),
+        # periodic boxes with a single block across a direction: BC_PERIODIC
+        # edges, and for 2 x 1 no wrap in i (the reference's periodic-box
+        # wiring needs several blocks in both directions)
+        ("residual_box_2x1x16", box21, "residual", 0),
+        ("explicit_box_2x1x16_20", box21, "explicit", 20),
+        ("explicit_box_1x1x16_20", box11, "explicit", 20),
         # Newton steps, GMRES restart, GMRES iteration cap, initial CFL, tolerance
         ("nks_bump_6x2x16_6", bump, "nks", (6, 30, 60, 1.0, 1e-10)),
         # global time step, Barth-Jespersen, GMRES restarts and its iteration cap
@@ -174,6 +184,12 @@ def golden_cases():
         ("nks_bump_iluk4", bump, "nks", (12, 30, 120, 10.0, 1e-10, 0.1, 4)),
         # global time step, Barth-Jespersen, restarts, with ILU(0)
         ("nks_bump_bj_global_iluk0", bump_bj, "nks", (4, 10, 25, 5.0, 1e-10, 1e-5, 0)),
+        # the 98,304-cell subsonic bump channel (12 x 4 blocks of 64 x 32,
+        # h 0.1, Mach 0.5) from the freestream: GMRES(30) with block Jacobi,
+        # 40 Newton steps of the reference's stalling history, and the ILU(4)
+        # preconditioner of the reference's example decks
+        ("nks_c2_bump_12x4x64x32_bj", c2, "nks", (40, 30, 60, 1.0, 1e-10)),
+        ("nks_c2_bump_12x4x64x32_iluk4", c2, "nks", (12, 30, 120, 10.0, 1e-10, 0.1, 4)),
         # the Newton step's preconditioner alone: (CFL, ILU level or -1 for
         # block Jacobi, vector seed)
         ("precon_bump_jacobi", bump, "precon", (10.0, -1, 1)),
@@ -371,7 +387,13 @@ def main():
             steps = 0
         else:
             res = run_residual(bs) if kind == "residual" else run_explicit(bs, steps)
-        if bs.nblk * bs.nci * bs.ncj > 8192:
+        if kind == "nks" and bs.nblk * bs.nci * bs.ncj > 8192:
+            # large Newton-Krylov fixtures: the whole history, and the final
+            # states on every NKS_SUB-th interior cell in i and j
+            for k in ("U", "pert_U"):
+                res[k + "_sub"] = np.ascontiguousarray(bs.interior(res.pop(k))[..., ::NKS_SUB, ::NKS_SUB])
+            out["lean"] = np.int32(1)
+        elif bs.nblk * bs.nci * bs.ncj > 8192:
             # keep the large fixtures small: the interior of the main output only
             keep = "dUdt" if kind == "residual" else "U"
             res = {k: (bs.interior(v) if k == keep else v) for k, v in res.items()
