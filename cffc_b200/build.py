@@ -36,7 +36,8 @@ SOURCES = {
     "e2d_mlp.cu": ["-fmad=true"],
 }
 HEADERS = ["e2d_device.cuh", "e2d_stage.cuh", "e2d_aux.cuh", "e2d_geom.cuh", "e2d_launch.h",
-           "e2d_fastmath.cuh", "e2d_handle.h", "e2d_tc.cuh", "e2d_smooth.cuh", "e2d_ilu.cuh", os.path.join("..", "..", "include", "cffc_e2d.h")]
+           "e2d_fastmath.cuh", "e2d_handle.h", "e2d_tc.cuh", "e2d_smooth.cuh", "e2d_ilu.cuh",
+           "e2d_march.cuh", "e2d_march_args.h", os.path.join("..", "..", "include", "cffc_e2d.h")]
 
 
 def _newer(target, deps):

@@ -138,12 +138,114 @@ void stage_buffers(e2d_handle* h, int k, double*& W, double*& U) {
   U = k == 0 ? h->B.U : (k == 1 ? h->B.U2 : h->U3);
 }
 
+// The stage kernel for a stage: the column-marching kernel where the handle
+// allows it (fast and FP32 paths, Roe flux, even block width, no degenerate
+// edges), else the tiled stage kernel.
 cudaError_t launch_stage_args(e2d_handle* h, StageArgs& a) {
+  if (h->march && a.B.flux == E2D_FLUX_ROE) {
+    const CUtensorMap* tw = nullptr;
+    if (a.Win == h->B.W) tw = &h->tmW[0];
+    else if (a.Win == h->B.W2) tw = &h->tmW[1];
+    else if (a.Win == h->W3 && h->W3) tw = &h->tmW[2];
+    if (tw) {
+      MarchArgs m;
+      memset(&m, 0, sizeof(m));
+      m.a = a;
+      m.tmW = *tw;
+      m.tmG = h->tmG;
+      m.tmN = h->tmN;
+      m.geom = h->geom;
+      m.mask = h->gmask;
+      const int mi = fast::march_strip_cols();
+      m.strips = (h->B.nci + mi - 1) / mi;
+      m.cps = fast::march_chunks(h->B.ncj);
+      m.nchunk = (long long)m.strips * m.cps * h->B.nblk;
+      const int grid = int(std::min<long long>(m.nchunk, h->march_grid));
+      return h->sc.precision == E2D_PREC_FP32 ? f32::launch_march(m, grid, h->stream)
+                                              : fast::launch_march(m, grid, h->stream);
+    }
+  }
   int ti, tj;
   stage_tile(h->sc.precision, &ti, &tj);
   a.tiles_i = (h->B.nci + ti - 1) / ti;
   a.tiles_j = (h->B.ncj + tj - 1) / tj;
   return launch_stage_prec(h->sc.precision, a, h->stream);
+}
+
+// ---- column-marching kernel set-up -------------------------------------------
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  }
+  return fn;
+}
+
+// 3D tensor map of doubles [d2][d1][d0] (rows of d0), box b0 x b1 x b2,
+// zero fill outside.
+bool encode3(CUtensorMap* map, void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint32_t b0, uint32_t b1,
+             uint32_t b2) {
+  const EncodeTiled fn = encode_fn();
+  if (!fn || !base) return false;
+  const cuuint64_t dims[3] = {d0, d1, d2};
+  const cuuint64_t strides[2] = {d0 * sizeof(double), d0 * d1 * sizeof(double)};
+  const cuuint32_t box[3] = {b0, b1, b2};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Geometry, padded nodes and tensor maps of the marching kernel.  The handle
+// keeps the tiled stage kernel when the marching kernel does not apply: the
+// exact path, another flux function, an odd block width (row strides of the
+// tensor maps must be multiples of 16 bytes) or a degenerate edge.
+int setup_march(e2d_handle* h) {
+  h->march = false;
+  if (h->sc.precision == E2D_PREC_FP64_EXACT || h->sc.flux != E2D_FLUX_ROE) return 0;
+  const Blocks& B = h->B;
+  if (B.NCi % 2 || !encode_fn()) return 0;
+  const int mi = fast::march_strip_cols(), wj = fast::march_window_rows();
+  const int NNp = B.NNi + 1;  // NNi is odd for an even NCi
+  int rc;
+  int* degenerate = nullptr;
+  if ((rc = dalloc(h, &h->geom, size_t(GEOM_NF) * h->ncell)) || (rc = dalloc(h, &h->gmask, h->ncell)) ||
+      (rc = dalloc(h, &h->nodes_pad, size_t(B.nblk) * 2 * B.NNj * NNp)) || (rc = dalloc(h, &degenerate, 1)))
+    return rc;
+  CK(cudaMemsetAsync(degenerate, 0, sizeof(int), h->stream));
+  CK(cudaMemsetAsync(h->nodes_pad, 0, sizeof(double) * size_t(B.nblk) * 2 * B.NNj * NNp, h->stream));
+  CK(fast::launch_geometry(B, h->geom, h->gmask, degenerate, NNp, h->nodes_pad, h->stream));
+  int deg = 0;
+  CK(cudaMemcpyAsync(&deg, degenerate, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (deg) return 0;
+  const uint32_t wi = mi + 4, nwi = mi + 6;
+  bool ok = encode3(&h->tmW[0], B.W, B.NCi, B.NCj, 4ull * B.nblk, wi, wj, 4) &&
+            encode3(&h->tmW[1], B.W2, B.NCi, B.NCj, 4ull * B.nblk, wi, wj, 4) &&
+            encode3(&h->tmG, h->geom, B.NCi, B.NCj, uint64_t(GEOM_NF) * B.nblk, wi, wj, 2) &&
+            encode3(&h->tmN, h->nodes_pad, NNp, B.NNj, 2ull * B.nblk, nwi, wj, 2);
+  if (ok && h->W3) ok = encode3(&h->tmW[2], h->W3, B.NCi, B.NCj, 4ull * B.nblk, wi, wj, 4);
+  if (!ok) return 0;
+  const int per_sm = h->sc.precision == E2D_PREC_FP32 ? f32::march_ctas_per_sm() : fast::march_ctas_per_sm();
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+  if (per_sm < 1 || sms < 1) return 0;
+  h->march_grid = per_sm * sms;
+  // CFFC_E2D_STAGE_KERNEL=tiled keeps the tiled kernel (comparisons of the two)
+  const char* kind = getenv("CFFC_E2D_STAGE_KERNEL");
+  h->march = !(kind && strcmp(kind, "tiled") == 0);
+  return 0;
 }
 
 // Residual (mode 0) or Frechet product (mode 3) of the state (W, U).
@@ -436,6 +538,7 @@ e2d_handle* e2d_create(const e2d_blocks_desc* d, const e2d_scheme* sc, int devic
   if ((rc = alloc_freeze(h))) return fail(rc, h);
   if ((rc = ensure_hist(h, 64))) return fail(rc, h);
   B.dWdx = B.dWdy = B.phi = nullptr;
+  if ((rc = setup_march(h))) return fail(rc, h);
   return h;
 }
 
@@ -533,6 +636,21 @@ __global__ void u_of_w_kernel(Blocks B, long long ncell) {
   }
 }
 
+// The stage buffers (W2, U2) and (W3, U3) take the whole state, ghost cells
+// included: a ghost cell that neither an exchange nor a BC fills (an edge
+// with BC_NONE and no neighbour) keeps its value in the reference's single
+// state array, so it must hold it in every buffer a stage reads.
+static int mirror_stage_buffers(e2d_handle* h) {
+  const size_t n = sizeof(double) * 4 * h->ncell;
+  CK(cudaMemcpyAsync(h->B.W2, h->B.W, n, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->B.U2, h->B.U, n, cudaMemcpyDeviceToDevice, h->stream));
+  if (h->W3) {
+    CK(cudaMemcpyAsync(h->W3, h->B.W, n, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->U3, h->B.U, n, cudaMemcpyDeviceToDevice, h->stream));
+  }
+  return 0;
+}
+
 int e2d_set_state(e2d_handle* h, const double* W) {
   if (!h || !W) return E2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
@@ -541,6 +659,7 @@ int e2d_set_state(e2d_handle* h, const double* W) {
   if (grid > 4096) grid = 4096;
   u_of_w_kernel<<<grid, 256, 0, h->stream>>>(h->B, (long long)h->ncell);
   CK(cudaGetLastError());
+  if (int rc = mirror_stage_buffers(h)) return rc;
   CK(cudaMemsetAsync(h->B.status, 0, sizeof(int) * 2, h->stream));
   if (int rc = reset_run(h)) return rc;
   CK(cudaStreamSynchronize(h->stream));
@@ -568,6 +687,7 @@ int e2d_set_conserved(e2d_handle* h, const double* U) {
   if (grid > 4096) grid = 4096;
   w_of_u_kernel<<<grid, 256, 0, h->stream>>>(h->B, (long long)h->ncell);
   CK(cudaGetLastError());
+  if (int rc = mirror_stage_buffers(h)) return rc;
   CK(cudaMemsetAsync(h->B.status, 0, sizeof(int) * 2, h->stream));
   if (int rc = reset_run(h)) return rc;
   CK(cudaStreamSynchronize(h->stream));

@@ -7,3 +7,4 @@
 #define E2D_FAST 1
 #define E2D_FP32 1
 #include "e2d_stage.cuh"
+#include "e2d_march.cuh"

@@ -4,6 +4,7 @@
 #define E2D_NS fast
 #define E2D_FAST 1
 #include "e2d_stage.cuh"
+#include "e2d_march.cuh"
 
 #include <cstring>
 

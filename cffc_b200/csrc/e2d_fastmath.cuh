@@ -15,10 +15,10 @@
 //   lp_x(1|4) = (0, -+d_a/(2 a_a), 0, 1/(2 a_a^2)),  lp_x(2) = (1, 0, 0, -1/a_a^2),
 //   rc_x(1|4) = (1, u_a -+ a_a, v_a, h_a -+ u_a a_a)  (h of the Roe state is h_a);
 //   least-squares: the 1/n averaging cancels in the gradient;
-//   limiters: phi(y) with y = a/b is compared as the fraction
-//   (a^2 + 2ab)/(a^2 + ab + 2b^2) (Venkatakrishnan) or min(|a|,|b|)/|b|
-//   (Barth–Jespersen), the minimum over the face points taken by
-//   cross-multiplication, and one division at the end.
+//   limiters: phi increases with y, so the smallest y = |a|/|b| over the
+//   face points is found by cross-multiplication and phi is evaluated once,
+//   (a^2 + 2ab)/(a^2 + ab + 2b^2) (Venkatakrishnan) or a/b (Barth–Jespersen),
+//   capped at 1, with one reciprocal.
 #pragma once
 #include "e2d_device.cuh"
 
@@ -136,30 +136,35 @@ __device__ __forceinline__ CState<double> flux_roe_n(const PState<double>& wl0, 
   return R;
 }
 
-// Limiter over the 4 face points, one division.
-__device__ __forceinline__ double limiter(int kind, const double* uq, double u0, double umin, double umax) {
-  if (kind == E2D_LIMITER_ONE) return 1.0;
-  if (kind == E2D_LIMITER_ZERO) return 0.0;
-  double bn = 1.0, bd = 1.0;  // best fraction bn/bd, starts at phi = 1
-  const bool venk = kind == E2D_LIMITER_VENKATAKRISHNAN;
+// Limiter over the 4 face points with one reciprocal.  The reference takes
+// the smallest of phi(y_q) over the face points q, y_q = (u_max or u_min -
+// u0) / (u_q - u0) >= 0, skipping points within TOLER of u0
+// (CFD.cc:696-751).  Both phi here -- Venkatakrishnan's (y^2 + 2y) /
+// (y^2 + y + 2) and Barth-Jespersen's min(1, y) -- increase with y, so that
+// minimum is phi at the smallest y_q, capped at 1: the smallest ratio is found
+// by cross-multiplying |a| / |b| pairs and phi is evaluated once.
+__device__ __forceinline__ double rcp_t(double x) { return rcp(x); }
+__device__ __forceinline__ float rcp_t(float x) { return 1.0f / x; }
+template <class T>
+__device__ __forceinline__ T limiter(int kind, const T* uq, T u0, T umin, T umax) {
+  if (kind == E2D_LIMITER_ONE) return T(1);
+  if (kind == E2D_LIMITER_ZERO) return T(0);
+  T A = T(1), Bm = T(0);  // smallest ratio A / Bm so far; 1/0 stands for "none"
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const double b = uq[q] - u0;
-    if (b > TOLER || b < -TOLER) {
-      const double a = (b > 0.0 ? umax : umin) - u0;  // y = a / b >= 0
-      double n, dd;
-      if (venk) {
-        n = a * a + 2.0 * a * b;
-        dd = a * a + a * b + 2.0 * b * b;
-      } else {
-        const double aa = fabs(a), ab = fabs(b);
-        n = aa < ab ? aa : ab;  // min(1, y) = min(|a|, |b|) / |b|
-        dd = ab;
-      }
-      if (n * bd < bn * dd) { bn = n; bd = dd; }
+    const T b = uq[q] - u0;
+    const T ab = fabs(b);
+    if (ab > T(TOLER)) {
+      const T a = fabs((b > T(0) ? umax : umin) - u0);
+      if (a * Bm < A * ab) { A = a; Bm = ab; }
     }
   }
-  return bn == bd ? 1.0 : bn * rcp(bd);
+  if (kind == E2D_LIMITER_VENKATAKRISHNAN) {
+    const T n = A * A + T(2) * A * Bm;         // y^2 + 2y, times Bm^2
+    const T d = A * A + A * Bm + T(2) * Bm * Bm;  // y^2 + y + 2, times Bm^2
+    return n < d ? n * rcp_t(d) : T(1);
+  }
+  return A < Bm ? A * rcp_t(Bm) : T(1);  // Barth-Jespersen
 }
 
 // quadCentroid with the reference-rounded moments and one reciprocal.

@@ -34,6 +34,15 @@ struct e2d_handle {
   int *freeze = nullptr, *first = nullptr;
   double* smooth_scratch = nullptr;
   size_t smooth_smem = 0;
+  // column-marching stage kernel of the fast and FP32 paths: per-cell
+  // geometry, padded nodes, tensor maps of the stage inputs (W, W2, W3), the
+  // geometry and the nodes, and the persistent grid size
+  bool march = false;
+  double* geom = nullptr;
+  unsigned char* gmask = nullptr;
+  double* nodes_pad = nullptr;
+  CUtensorMap tmW[3], tmG, tmN;
+  int march_grid = 0;
   // captured explicit step
   cudaGraphExec_t step_graph = nullptr;
   e2d_nks_state* nks = nullptr;
@@ -60,6 +69,7 @@ template <class T> int dalloc(e2d_handle* h, T** p, size_t n) {
 
 int check_status(e2d_handle* h);
 cudaError_t launch_stage_any(e2d_handle* h, int mode, int fuse_next);
+cudaError_t launch_stage_args(e2d_handle* h, e2d::StageArgs& a);
 cudaError_t ghost_fill_for(e2d_handle* h, int mode);
 int ensure_hist(e2d_handle* h, int n);
 void nks_free(e2d_handle* h);

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "e2d_device.cuh"
+#include "e2d_march_args.h"
 
 namespace e2d {
 namespace exact {
@@ -16,12 +17,23 @@ cudaError_t launch_stage(const StageArgs& a, cudaStream_t st);
 size_t stage_smem_bytes();
 int tile_i();
 int tile_j();
+// column-marching stage kernel (e2d_march.cuh) and its per-handle geometry
+cudaError_t launch_march(const MarchArgs& m, int grid, cudaStream_t st);
+int march_ctas_per_sm();
+int march_strip_cols();
+int march_chunk_rows();
+int march_window_rows();
+int march_chunks(int ncj);
+cudaError_t launch_geometry(const Blocks& B, double* geom, unsigned char* mask, int* degenerate, int NNp,
+                            double* nodes_pad, cudaStream_t st);
 }  // namespace fast
 namespace f32 {
 cudaError_t launch_stage(const StageArgs& a, cudaStream_t st);
 size_t stage_smem_bytes();
 int tile_i();
 int tile_j();
+cudaError_t launch_march(const MarchArgs& m, int grid, cudaStream_t st);
+int march_ctas_per_sm();
 }  // namespace f32
 
 // The stage kernel of a precision (E2D_PREC_*): launch and tile shape.

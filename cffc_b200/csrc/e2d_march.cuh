@@ -1,0 +1,726 @@
+// e2d_march.cuh — the column-marching stage kernel of the fast FP64 and FP32
+// paths: the same residual / explicit stage / Frechet product as
+// stage_kernel (e2d_stage.cuh), restating the same reference routines
+//   Linear_Reconstruction_LeastSquares   src_2D/Euler2D/Euler2DQuadSingleBlock.cc:3678-4087
+//   Euler2D_Quad_Block::dUdt_Residual_Evaluation   src_2D/Euler2D/Euler2DQuad.cc:814-1227
+//   Euler2D_Quad_Block::dUdt_Multistage_Explicit   src_2D/Euler2D/Euler2DQuad.cc:1235-1727
+//   Update_Solution_Multistage_Explicit   src_2D/Euler2D/Euler2DQuadSingleBlock.cc:5300-5507
+// but organised for the hardware:
+//
+// * Work: a block is cut into column strips of MI = 32 interior cells, a
+//   strip into chunks of CH = 7 rows (the last one of a strip 1 to 8 rows:
+//   a remainder of one row joins the chunk below it).  With 8 warps a chunk
+//   of 7 rows reconstructs its 7 rows and their 2 edge columns in one round,
+//   its 15 face rows in two and updates in one.  The launch is persistent: CTA k takes
+//   a contiguous range of the (block, strip, chunk) list, so every SM gets the
+//   same number of chunks to within one, and marches up its strips.
+// * Reuse along j: the one-cell reconstruction ring and the bottom j-face row
+//   a chunk needs were computed by the chunk below; they are carried in
+//   shared memory, so each cell is reconstructed once (plus the 2 ring columns
+//   of its strip) and each face evaluated once.
+// * Staging: the chunk's window of primitive state (36 x 12 cells, 4
+//   variables), centroids and nodes arrives through three TMA tensor copies
+//   issued by one thread and completing on an mbarrier; the next chunk's
+//   copies are issued before the current chunk is computed (double buffer).
+// * Geometry is not recomputed per stage: centroids, the least-squares
+//   inverse of each cell's stencil, 1/area and the CFL lengths were computed
+//   once per handle (e2d_march_args.h); face normals and lengths come from
+//   the staged nodes with one reciprocal square root per face.
+//
+// Used when the block set allows it (even nci, no degenerate edges, the Roe
+// flux); stage_kernel covers every other case and the exact path.
+#pragma once
+#include "e2d_march_args.h"
+#include "e2d_tc.cuh"
+
+namespace e2d {
+namespace E2D_NS {
+namespace mk {
+
+#ifndef E2D_MARCH_ROWS
+#define E2D_MARCH_ROWS 7
+#endif
+constexpr int MI = 32, MJ = 8, CH = E2D_MARCH_ROWS;  // interior columns; rows of a chunk (at most, nominal)
+constexpr int WI = MI + 4, WJ = MJ + 4, NWI = MI + 6;  // staged window (cells, node columns)
+constexpr int RCI = MI + 2, RCJ = MJ + 2;          // reconstruction slots (cols, rows j0+1..j0+10)
+constexpr int FJ = MJ + 1;                         // j-face slots (faces j0+2-1/2 .. j0+10-1/2)
+constexpr int THREADS = 256, NWARP = THREADS / 32;  // 8 warps: 128 registers at 2 CTAs per SM
+constexpr uint32_t WAIT_ITERS = 1u << 24;          // bounded mbarrier wait (about a second)
+constexpr int ST_TIMEOUT = 2;                      // status code: a staging wait ran out
+
+struct Tile {
+  double W[4][WJ][WI];   // primitive state, rows j0 .. j0+11, cols i0 .. i0+35
+  double G[2][WJ][WI];   // centroids
+  double N[2][WJ][NWI];  // nodes, cols i0 .. i0+37
+};
+constexpr uint32_t TILE_BYTES = sizeof(double) * (6 * WJ * WI + 2 * WJ * NWI);
+static_assert(sizeof(Tile) == TILE_BYTES && TILE_BYTES % 128 == 0, "tile packing");
+static_assert((4 * WJ * WI * 8) % 128 == 0 && (6 * WJ * WI * 8) % 128 == 0, "TMA destinations 128-byte aligned");
+static_assert(NWARP >= MJ, "one warp per update row");
+static_assert(2 * (MJ + 2) <= 32, "one warp covers the edge columns of every reconstructed row");
+
+struct Smem {
+  Tile in[2];
+  RT px[RCJ][4][RCI], py[RCJ][4][RCI];  // phi * gradient of the reconstructed cells
+  double Fi[MJ][4][MI + 1];             // i-face flux x length, faces I-1/2, I = i0+2 .. i0+34
+  double Fj[FJ][4][MI];                 // j-face flux x length
+  double red[4][NWARP];
+  uint64_t full[2];
+  int failed;
+};
+
+// neighbour k of the canonical stencil order
+__device__ constexpr int KDI[8] = {-1, 0, 1, -1, 1, -1, 0, 1};
+__device__ constexpr int KDJ[8] = {-1, -1, -1, 0, 0, 1, 1, 1};
+
+__device__ __forceinline__ void expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+// 3D tiled tensor copy global -> this CTA's shared memory (no multicast).
+__device__ __forceinline__ void tma3(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+      "[%2];" ::"r"(tc::smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(tc::smem_addr(bar)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+struct Chunk {
+  int b, i0, j0, c, h;  // block, strip origin (interior column), chunk origin (interior row), chunk index, rows
+};
+__device__ __forceinline__ Chunk decode(const MarchArgs& m, long long g) {
+  Chunk k;
+  const long long strip = g / m.cps;
+  k.c = int(g - strip * m.cps);
+  k.b = int(strip / m.strips);
+  k.i0 = int(strip - (long long)k.b * m.strips) * MI;
+  k.j0 = k.c * CH;
+  k.h = k.c == m.cps - 1 ? min(MJ, m.a.B.ncj - k.j0) : CH;
+  return k;
+}
+
+__device__ __forceinline__ PState<RT> wwin(const Tile& T, int wj, int wi) {
+  PState<RT> w;
+  w.d = RT(T.W[0][wj][wi]); w.u = RT(T.W[1][wj][wi]); w.v = RT(T.W[2][wj][wi]); w.p = RT(T.W[3][wj][wi]);
+  return w;
+}
+
+// Limited linear state of reconstructed cell (slot sl, column c; window
+// (c+1, sl+1)) at the face point (fx, fy).
+__device__ __forceinline__ PState<RT> fstate(const Smem& s, const Tile& T, int sl, int c, double fx, double fy) {
+  const RT dx = RT(fx - T.G[0][sl + 1][c + 1]), dy = RT(fy - T.G[1][sl + 1][c + 1]);
+  PState<RT> w = wwin(T, sl + 1, c + 1);
+  w.d = w.d + s.px[sl][0][c] * dx + s.py[sl][0][c] * dy;
+  w.u = w.u + s.px[sl][1][c] * dx + s.py[sl][1][c] * dy;
+  w.v = w.v + s.px[sl][2][c] * dx + s.py[sl][2][c] * dy;
+  w.p = w.p + s.px[sl][3][c] * dx + s.py[sl][3][c] * dy;
+  return w;
+}
+
+// The per-cell inputs of a reconstruction: stencil mask and least-squares
+// inverse (loaded before the staging wait, so their latency overlaps it).
+struct ReconIn {
+  unsigned msk;
+  double K0, K1, K2;
+};
+__device__ __forceinline__ ReconIn recon_in(const MarchArgs& m, const Chunk& k, int sl, int c, size_t plane) {
+  const Blocks& B = m.a.B;
+  ReconIn r{0u, 0.0, 0.0, 0.0};
+  const int I = k.i0 + 1 + c, J = k.j0 + 1 + sl;
+  if (I > B.nci + 2 || J > B.ncj + 2) return r;
+  const size_t off = size_t(J) * B.NCi + I;
+  r.msk = m.mask[size_t(k.b) * plane + off];
+  const double* gp = m.geom + size_t(k.b) * GEOM_NF * plane + off;
+  r.K0 = gp[G_K0 * plane];
+  r.K1 = gp[G_K1 * plane];
+  r.K2 = gp[G_K2 * plane];
+  return r;
+}
+
+// Least-squares gradients and limiter of the cell in slot sl, column c.
+// frozen: the case's limiters are frozen (Freeze_Limiter): phi is the stored
+// one.  With B.dWdx set the gradients and limiter are exported as well.
+__device__ __forceinline__ void recon_cell(const MarchArgs& m, Smem& s, const Tile& T, const Chunk& k, int sl, int c,
+                                           const ReconIn& in, bool frozen) {
+  const Blocks& B = m.a.B;
+  const int I = k.i0 + 1 + c, J = k.j0 + 1 + sl;
+  if (I > B.nci + 2 || J > B.ncj + 2) return;  // beyond the block's ring: never read
+  const unsigned msk = in.msk;
+  if (msk == 0) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) { s.px[sl][v][c] = RT(0); s.py[sl][v][c] = RT(0); }
+    if (B.dWdx)
+      for (int v = 0; v < 4; ++v) {
+        const size_t o = cell_var(B, k.b, v, J, I);
+        B.dWdx[o] = 0.0; B.dWdy[o] = 0.0; B.phi[o] = 0.0;
+      }
+    return;
+  }
+  const RT K0 = RT(in.K0), K1 = RT(in.K1), K2 = RT(in.K2);
+  const int wi = c + 1, wj = sl + 1;
+  const double xc0 = T.G[0][wj][wi], yc0 = T.G[1][wj][wi];
+  RT w0[4], Sx[4], Sy[4], mn[4], mx[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    w0[v] = RT(T.W[v][wj][wi]);
+    Sx[v] = RT(0); Sy[v] = RT(0); mn[v] = w0[v]; mx[v] = w0[v];
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    if (msk & (1u << q)) {
+      const int ni = wi + KDI[q], nj = wj + KDJ[q];
+      const RT dx = RT(T.G[0][nj][ni] - xc0), dy = RT(T.G[1][nj][ni] - yc0);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const RT w = RT(T.W[v][nj][ni]);
+        const RT du = w - w0[v];
+        Sx[v] += du * dx;
+        Sy[v] += du * dy;
+        mn[v] = dmin(mn[v], w);
+        mx[v] = dmax(mx[v], w);
+      }
+    }
+  }
+  // face midpoints E, W, N, S of the cell, relative to its centroid
+  const double x00 = T.N[0][wj][wi], y00 = T.N[1][wj][wi], x10 = T.N[0][wj][wi + 1], y10 = T.N[1][wj][wi + 1];
+  const double x01 = T.N[0][wj + 1][wi], y01 = T.N[1][wj + 1][wi];
+  const double x11 = T.N[0][wj + 1][wi + 1], y11 = T.N[1][wj + 1][wi + 1];
+  const RT ofx[4] = {RT(HALF * (x10 + x11) - xc0), RT(HALF * (x00 + x01) - xc0), RT(HALF * (x01 + x11) - xc0),
+                     RT(HALF * (x00 + x10) - xc0)};
+  const RT ofy[4] = {RT(HALF * (y10 + y11) - yc0), RT(HALF * (y00 + y01) - yc0), RT(HALF * (y01 + y11) - yc0),
+                     RT(HALF * (y00 + y10) - yc0)};
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const RT gx = Sx[v] * K0 + Sy[v] * K1;
+    const RT gy = Sx[v] * K1 + Sy[v] * K2;
+    RT uq[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) uq[q] = w0[v] + gx * ofx[q] + gy * ofy[q];
+    RT phi;
+    if (frozen) {
+      phi = RT(B.phi_keep[cell_var(B, k.b, v, J, I)]);
+    } else {
+      phi = cell_limiter(B.limiter, uq, w0[v], mn[v], mx[v]);
+      if (B.freeze) B.phi_keep[cell_var(B, k.b, v, J, I)] = double(phi);
+    }
+    s.px[sl][v][c] = phi * gx;
+    s.py[sl][v][c] = phi * gy;
+    if (B.dWdx) {
+      const size_t o = cell_var(B, k.b, v, J, I);
+      B.dWdx[o] = gx; B.dWdy[o] = gy; B.phi[o] = phi;
+    }
+  }
+}
+
+// Face normal, length and midpoint of the edge a -> c (outward normal of the
+// cell on the left of a -> c: (dy, -dx) / |d|, d = a - c).
+struct FaceGeo {
+  double nx, ny, l, mx, my;
+};
+__device__ __forceinline__ FaceGeo face_geo(double ax, double ay, double cx, double cy) {
+  FaceGeo f;
+  const double dx = ax - cx, dy = ay - cy;
+  const double q = dx * dx + dy * dy;
+  const double rn = fm::rsqrt(q);
+  f.l = fm::sqrt_from_rsqrt(q, rn);
+  f.nx = dy * rn;
+  f.ny = -dx * rn;
+  f.mx = HALF * (cx + ax);
+  f.my = HALF * (cy + ay);
+  return f;
+}
+
+// i-face I-1/2, I = i0+2+q, of row r (J = j0+2+r).
+__device__ __forceinline__ void iface(const MarchArgs& m, Smem& s, const Tile& T, const Chunk& k, int r, int q) {
+  const Blocks& B = m.a.B;
+  const int I = k.i0 + 2 + q, J = k.j0 + 2 + r;
+  if (I > B.nci + 2 || J > B.ncj + 1) return;
+  // nodes (I, J+1) -> (I, J): window (q+2, r+3), (q+2, r+2)
+  const FaceGeo f = face_geo(T.N[0][r + 3][q + 2], T.N[1][r + 3][q + 2], T.N[0][r + 2][q + 2], T.N[1][r + 2][q + 2]);
+  // BC codes matter at the block's west and east faces only
+  const int bw = I == NG ? B.bcw[size_t(k.b) * B.NCj + J] : E2D_BC_NONE;
+  const int be = I == B.nci + NG ? B.bce[size_t(k.b) * B.NCj + J] : E2D_BC_NONE;
+  const RT g = RT(B.g), gm1 = RT(B.gm1), gm1i = RT(B.gm1i);
+  PState<RT> wl, wr;
+  // left cell (I-1, J): slot r+1, column q; right cell (I, J): slot r+1, column q+1
+  if (I == NG && face_bc(bw)) {
+    wr = fstate(s, T, r + 1, q + 1, f.mx, f.my);
+    wl = (bw == E2D_BC_REFLECTION) ? reflect(wr, RT(-f.nx), RT(-f.ny))
+                                   : bc_char_pressure(wr, load_wo(B.wow, k.b, B.NCj, J), RT(-f.nx), RT(-f.ny), g, gm1i);
+  } else if (I == B.nci + NG && face_bc(be)) {
+    wl = fstate(s, T, r + 1, q, f.mx, f.my);
+    wr = (be == E2D_BC_REFLECTION) ? reflect(wl, RT(f.nx), RT(f.ny))
+                                   : bc_char_pressure(wl, load_wo(B.woe, k.b, B.NCj, J), RT(f.nx), RT(f.ny), g, gm1i);
+  } else {
+    wl = fstate(s, T, r + 1, q, f.mx, f.my);
+    wr = fstate(s, T, r + 1, q + 1, f.mx, f.my);
+  }
+  const CState<RT> F = face_flux<true>(B.flux, wl, wr, RT(f.nx), RT(f.ny), g, gm1, gm1i);
+  s.Fi[r][0][q] = double(F.d) * f.l;
+  s.Fi[r][1][q] = double(F.mx) * f.l;
+  s.Fi[r][2][q] = double(F.my) * f.l;
+  s.Fi[r][3][q] = double(F.E) * f.l;
+}
+
+// j-face J-1/2 (J = j0+2+sl) of column I = i0+2+q.
+__device__ __forceinline__ void jface(const MarchArgs& m, Smem& s, const Tile& T, const Chunk& k, int sl, int q) {
+  const Blocks& B = m.a.B;
+  const int I = k.i0 + 2 + q, J = k.j0 + 2 + sl;
+  if (I > B.nci + 1 || J > B.ncj + 2) return;
+  // nodes (I, J) -> (I+1, J): window (q+2, sl+2), (q+3, sl+2)
+  const FaceGeo f = face_geo(T.N[0][sl + 2][q + 2], T.N[1][sl + 2][q + 2], T.N[0][sl + 2][q + 3], T.N[1][sl + 2][q + 3]);
+  const int bs = J == NG ? B.bcs[size_t(k.b) * B.NCi + I] : E2D_BC_NONE;
+  const int bn = J == B.ncj + NG ? B.bcn[size_t(k.b) * B.NCi + I] : E2D_BC_NONE;
+  const RT g = RT(B.g), gm1 = RT(B.gm1), gm1i = RT(B.gm1i);
+  PState<RT> wl, wr;
+  // lower cell (I, J-1): slot sl, column q+1; upper cell (I, J): slot sl+1
+  if (J == NG && face_bc(bs)) {
+    wr = fstate(s, T, sl + 1, q + 1, f.mx, f.my);
+    wl = (bs == E2D_BC_REFLECTION) ? reflect(wr, RT(-f.nx), RT(-f.ny))
+                                   : bc_char_pressure(wr, load_wo(B.wos, k.b, B.NCi, I), RT(-f.nx), RT(-f.ny), g, gm1i);
+  } else if (J == B.ncj + NG && face_bc(bn)) {
+    wl = fstate(s, T, sl, q + 1, f.mx, f.my);
+    wr = (bn == E2D_BC_REFLECTION) ? reflect(wl, RT(f.nx), RT(f.ny))
+                                   : bc_char_pressure(wl, load_wo(B.won, k.b, B.NCi, I), RT(f.nx), RT(f.ny), g, gm1i);
+  } else {
+    wl = fstate(s, T, sl, q + 1, f.mx, f.my);
+    wr = fstate(s, T, sl + 1, q + 1, f.mx, f.my);
+  }
+  const CState<RT> F = face_flux<true>(B.flux, wl, wr, RT(f.nx), RT(f.ny), g, gm1, gm1i);
+  s.Fj[sl][0][q] = double(F.d) * f.l;
+  s.Fj[sl][1][q] = double(F.mx) * f.l;
+  s.Fj[sl][2][q] = double(F.my) * f.l;
+  s.Fj[sl][3][q] = double(F.E) * f.l;
+}
+
+// Contributions of the CTA's cells to the next step's CFL minimum and
+// residual norms of case cs, added into the step history.
+__device__ __forceinline__ void flush_next(const StageArgs& a, Smem& s, int cs, double dt_next, double n1, double n2,
+                                           double nmax) {
+  const int tid = threadIdx.x;
+  for (int o = 16; o > 0; o >>= 1) {
+    dt_next = dmin(dt_next, __shfl_xor_sync(0xffffffffu, dt_next, o));
+    n1 += __shfl_xor_sync(0xffffffffu, n1, o);
+    n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+    nmax = dmax(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+  }
+  if ((tid & 31) == 0) {
+    s.red[0][tid >> 5] = dt_next; s.red[1][tid >> 5] = n1; s.red[2][tid >> 5] = n2; s.red[3][tid >> 5] = nmax;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < NWARP; ++w) {
+      dt_next = dmin(dt_next, s.red[0][w]); n1 += s.red[1][w]; n2 += s.red[2][w]; nmax = dmax(nmax, s.red[3][w]);
+    }
+    double* next = const_cast<double*>(a.hist) + 4 * ((*a.step + 1) * a.B.ncase + cs);
+    atomicMin(reinterpret_cast<unsigned long long*>(next), (unsigned long long)__double_as_longlong(dt_next));
+    atomicAdd(next + 1, n1);
+    atomicAdd(next + 2, n2);
+    atomicMax(reinterpret_cast<unsigned long long*>(next + 3), (unsigned long long)__double_as_longlong(nmax));
+  }
+  __syncthreads();
+}
+
+template <int MODE, bool FUSE>
+__global__ void __launch_bounds__(THREADS, 2) march_kernel(const __grid_constant__ MarchArgs m) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // TMA destinations want 128-byte alignment: align the base by hand
+  const uint32_t base = tc::smem_addr(smem_raw);
+  Smem& s = *reinterpret_cast<Smem*>(smem_raw + ((128u - (base & 127u)) & 127u));
+  const StageArgs& a = m.a;
+  const Blocks& B = a.B;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long g0 = m.nchunk * blockIdx.x / gridDim.x, g1 = m.nchunk * (blockIdx.x + 1) / gridDim.x;
+  if (tid == 0) {
+    s.failed = *(volatile int*)B.status;
+    tc::mbar_init(&s.full[0], 1);
+    tc::mbar_init(&s.full[1], 1);
+  }
+  __syncthreads();
+  if (s.failed || g0 >= g1) return;  // an earlier kernel failed: stop marching (uniform)
+  const size_t plane = size_t(B.NCi) * B.NCj;
+  const double g = B.g, gm1 = B.gm1;
+
+  auto issue = [&](long long gg, int buf) {
+    const Chunk k = decode(m, gg);
+    uint64_t* bar = &s.full[buf];
+    expect_tx(bar, TILE_BYTES);
+    tma3(&s.in[buf].W[0][0][0], &m.tmW, bar, k.i0, k.j0, 4 * k.b);
+    tma3(&s.in[buf].G[0][0][0], &m.tmG, bar, k.i0, k.j0, GEOM_NF * k.b);
+    tma3(&s.in[buf].N[0][0][0], &m.tmN, bar, k.i0, k.j0, 2 * k.b);
+  };
+  if (tid == 0) issue(g0, 0);
+
+  double dt_next = 1000000.0, n1 = 0.0, n2 = 0.0, nmax = 0.0;  // fused next-step CFL / norms
+  int cur_case = -1;
+  int it = 0;
+  for (long long gg = g0; gg < g1; ++gg, ++it) {
+    const int buf = it & 1;
+    const Chunk k = decode(m, gg);
+    if (tid == 0 && gg + 1 < g1) {
+      tc::fence_async_smem();  // the other buffer's generic reads come before its overwrite
+      issue(gg + 1, buf ^ 1);
+    }
+    // the update cells' own inputs: into L2 ahead of the update phase (lane
+    // pairs cover the two halves of the warp's row: state variables, 1/A, the
+    // CFL geometry)
+    if (MODE != 0 && MODE != 3 && warp < k.h) {
+      const int J = k.j0 + NG + warp, I = k.i0 + NG + 16 * (lane & 1), f = lane >> 1;
+      if (J <= B.ncj + 1 && I <= B.nci + 1) {
+        const double* gq = m.geom + size_t(k.b) * GEOM_NF * plane + size_t(J) * B.NCi + I;
+        if (f < 4) {
+          const size_t q = cell_var(B, k.b, f, J, I);
+          prefetch_l2(a.Ubase + q);
+          if (MODE == 2) prefetch_l2(a.res_out + q);
+        } else if (f == 4) {
+          prefetch_l2(gq + G_RA * plane);
+        } else if (FUSE && f < 11) {
+          prefetch_l2(gq + (G_DI + f - 5) * plane);
+        }
+      }
+    }
+    // this warp's first reconstruction row: its inputs, ahead of the wait
+    const bool pro = (gg == g0) || (k.c == 0);  // start of a strip: no carried rows
+    const int s_lo = pro ? 0 : 2, nrow = k.h + 2 - s_lo;  // reconstruction slots [s_lo, h+2)
+    ReconIn rin{0u, 0.0, 0.0, 0.0};
+    if (warp < nrow) rin = recon_in(m, k, s_lo + warp, lane + 1, plane);
+    const bool ok = tc::mbar_wait(&s.full[buf], uint32_t(it >> 1) & 1u, WAIT_ITERS);
+    if (__syncthreads_or(!ok)) {
+      // a staging copy did not complete in time: record it, let the copies
+      // in flight land (bounded), and stop
+      if (tid == 0) {
+        set_status(B.status, ST_TIMEOUT, int(gg));
+        tc::mbar_wait(&s.full[buf], uint32_t(it >> 1) & 1u, WAIT_ITERS);
+        if (gg + 1 < g1) tc::mbar_wait(&s.full[buf ^ 1], uint32_t((it + 1) >> 1) & 1u, WAIT_ITERS);
+      }
+      return;
+    }
+    const int cs = case_id(B, k.b);
+    if (B.case_active && !B.case_active[cs]) {  // a finished case of a batch (uniform)
+      __syncthreads();
+      continue;
+    }
+    if (FUSE && cs != cur_case) {
+      if (cur_case >= 0) flush_next(a, s, cur_case, dt_next, n1, n2, nmax);
+      cur_case = cs;
+      dt_next = 1000000.0; n1 = 0.0; n2 = 0.0; nmax = 0.0;
+    }
+    const Tile& T = s.in[buf];
+    const bool frozen = B.freeze && B.freeze[cs];
+
+    // ---- reconstruction of slots [s_lo, RCJ) ---------------------------------
+    // row tasks 0 .. nrow-1 (32 interior-facing columns), task nrow: the two
+    // edge columns of every row
+    for (int task = warp; task <= nrow; task += NWARP) {
+      const bool row = task < nrow;
+      const int sl = row ? s_lo + task : s_lo + (lane >> 1);
+      const int c = row ? lane + 1 : ((lane & 1) ? RCI - 1 : 0);
+      if (row || lane < 2 * nrow)
+        recon_cell(m, s, T, k, sl, c, (row && task == warp) ? rin : recon_in(m, k, sl, c, plane), frozen);
+    }
+    __syncthreads();
+
+    // ---- faces: i-face rows, their last column, j-face rows ----------------------
+    {
+      const int h = k.h, sf_lo = pro ? 0 : 1, nfj = h + 1 - sf_lo;  // j-face slots [sf_lo, h]
+      for (int task = warp; task < h + 1 + nfj; task += NWARP) {
+        if (task <= h) {
+          if (task < h || lane < h) iface(m, s, T, k, task < h ? task : lane, task < h ? lane : MI);
+        } else {
+          jface(m, s, T, k, sf_lo + task - h - 1, lane);
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- flux divergence and update, one interior cell per thread ---------------
+    if (warp < k.h) {
+      const int r = warp, q = lane;
+      const int I = k.i0 + NG + q, J = k.j0 + NG + r;
+      if (I <= B.nci + 1 && J <= B.ncj + 1) {
+        const size_t c = cell_sc(B, k.b, J, I);
+        const double* gp = m.geom + size_t(k.b) * GEOM_NF * plane + (c - size_t(k.b) * plane);
+        const double rA = gp[G_RA * plane];
+        double kk = 1.0;
+        if (MODE == 1 || MODE == 2) {
+          const double* dtmin_p = a.hist + 4 * ((*a.step) * B.ncase + cs);
+          kk = B.cfl * (B.local_dt ? B.dt[c] : *dtmin_p);
+        }
+        const double kA = kk * rA;
+        double res[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          double d = 0.0;
+          if (MODE == 2) {
+            const size_t qv = cell_var(B, k.b, v, J, I);
+            d = a.res_out[qv];
+            if (a.acc1) d = d + 2.0 * a.acc1[qv] + 2.0 * a.acc2[qv];
+          }
+          d += s.Fi[r][v][q] * kA;
+          d -= s.Fi[r][v][q + 1] * kA;
+          d += s.Fj[r][v][q] * kA;
+          d -= s.Fj[r + 1][v][q] * kA;
+          res[v] = d;
+        }
+        if (MODE == 0) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, k.b, v, J, I)] = res[v];
+        } else if (MODE == 3) {
+          // Frechet derivative (GMRES2D.h:445-488):
+          // V = (normalizeR(R) - b)/eps - normalizeUtoR(z * (1/dt))
+          const double eps = a.nks_eps[cs];
+          const double rdt = 1.0 / B.dt[c];
+          const size_t qv = c * 4;
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            double val = (res[v] / a.normR[v] - a.nks_b[qv + v]) / eps;
+            val -= (a.nks_z[qv + v] * rdt) * a.normU[v] / a.normR[v];
+            a.nks_v[qv + v] = val;
+          }
+        } else if (a.no_update) {
+#pragma unroll
+          for (int v = 0; v < 4; ++v) a.res_out[cell_var(B, k.b, v, J, I)] = res[v];
+        } else {
+          // Update_Solution_Multistage_Explicit: U = Uo + omega*dUdt
+          CState<double> uo;
+          uo.d = a.Ubase[cell_var(B, k.b, 0, J, I)]; uo.mx = a.Ubase[cell_var(B, k.b, 1, J, I)];
+          uo.my = a.Ubase[cell_var(B, k.b, 2, J, I)]; uo.E = a.Ubase[cell_var(B, k.b, 3, J, I)];
+          const double omega = a.omega;
+          CState<double> u;
+          u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
+          u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
+          if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) {
+            if (!B.local_dt) {
+              set_status(B.status, ST_NEGATIVE, int(c));
+            } else {
+              double rrf = 1.0, dtc = B.dt[c];
+              for (int nr = 1; nr <= 10; ++nr) {
+                rrf = HALF * rrf;
+                dtc = rrf * dtc;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) res[v] = rrf * res[v];
+                u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
+                u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
+                if (u.d > 0.0 && u.E > 0.0 && e_of_U(u) > 0.0) break;
+              }
+              B.dt[c] = dtc;
+              if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) set_status(B.status, ST_NEGATIVE, int(c));
+            }
+          }
+#pragma unroll
+          for (int v = 0; v < 4; ++v) a.res_out[cell_var(B, k.b, v, J, I)] = res[v];
+          const PState<double> w = fm::W_of_U(u, gm1);
+          a.Uout[cell_var(B, k.b, 0, J, I)] = u.d; a.Uout[cell_var(B, k.b, 1, J, I)] = u.mx;
+          a.Uout[cell_var(B, k.b, 2, J, I)] = u.my; a.Uout[cell_var(B, k.b, 3, J, I)] = u.E;
+          a.Wout[cell_var(B, k.b, 0, J, I)] = w.d; a.Wout[cell_var(B, k.b, 1, J, I)] = w.u;
+          a.Wout[cell_var(B, k.b, 2, J, I)] = w.v; a.Wout[cell_var(B, k.b, 3, J, I)] = w.p;
+          if (FUSE) {
+            // CFL of the updated cell (Euler2DQuadSingleBlock.cc:3019-3080)
+            const double v_i = w.u * gp[G_VIX * plane] + w.v * gp[G_VIY * plane];
+            const double v_j = w.u * gp[G_VJX * plane] + w.v * gp[G_VJY * plane];
+            const double c2 = g * w.p * fm::rcp(w.d);
+            const double snd = fm::sqrt_from_rsqrt(c2, fm::rsqrt(c2));
+            const double ti = gp[G_DI * plane] * fm::rcp(snd + fabs(v_i));
+            const double tj = gp[G_DJ * plane] * fm::rcp(snd + fabs(v_j));
+            const double dtc = dmin(ti, tj);
+            if (B.local_dt) B.dt[c] = dtc;
+            dt_next = dmin(dt_next, dtc);
+            n1 += fabs(res[0]);
+            n2 += res[0] * res[0];
+            nmax = dmax(nmax, fabs(res[0]));
+          }
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- carry the top reconstruction row and j-face row to the next chunk -----
+    for (int q = tid; q < 4 * RCI; q += THREADS) {
+      const int v = q / RCI, c = q % RCI;
+      s.px[1][v][c] = s.px[k.h + 1][v][c];
+      s.py[1][v][c] = s.py[k.h + 1][v][c];
+    }
+    for (int q = tid; q < 4 * MI; q += THREADS) {
+      const int v = q / MI, c = q % MI;
+      s.Fj[0][v][c] = s.Fj[k.h][v][c];
+    }
+    __syncthreads();
+  }
+  if (FUSE && cur_case >= 0) flush_next(a, s, cur_case, dt_next, n1, n2, nmax);
+}
+
+}  // namespace mk
+
+size_t march_smem_bytes() { return sizeof(mk::Smem) + 128; }
+
+template <int MODE, bool FUSE>
+cudaError_t march_one(const MarchArgs& m, int grid, cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(mk::march_kernel<MODE, FUSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(march_smem_bytes()));
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  mk::march_kernel<MODE, FUSE><<<grid, mk::THREADS, march_smem_bytes(), st>>>(m);
+  return cudaGetLastError();
+}
+// grid: CTAs of the persistent launch (the caller sizes it to the SMs)
+cudaError_t launch_march(const MarchArgs& m, int grid, cudaStream_t st) {
+  switch (m.a.mode * 2 + (m.a.fuse_next ? 1 : 0)) {
+    case 0: return march_one<0, false>(m, grid, st);
+    case 2: return march_one<1, false>(m, grid, st);
+    case 3: return march_one<1, true>(m, grid, st);
+    case 4: return march_one<2, false>(m, grid, st);
+    case 5: return march_one<2, true>(m, grid, st);
+    case 6: return march_one<3, false>(m, grid, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+int march_ctas_per_sm() {
+  int n = 0;
+  if (cudaFuncSetAttribute(mk::march_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(march_smem_bytes())) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mk::march_kernel<1, false>, mk::THREADS,
+                                                    march_smem_bytes()) != cudaSuccess)
+    return 0;
+  return n;
+}
+int march_strip_cols() { return mk::MI; }
+int march_chunk_rows() { return mk::CH; }
+int march_window_rows() { return mk::WJ; }
+// chunks per strip of ncj rows: CH rows each, a remainder of one row joining
+// the last full chunk (at most MJ rows)
+int march_chunks(int ncj) {
+  const int n = ncj / mk::CH, r = ncj % mk::CH;
+  if (r == 0 || (r == 1 && n > 0 && mk::CH + 1 <= mk::MJ)) return n;
+  return n + 1;
+}
+
+}  // namespace E2D_NS
+}  // namespace e2d
+
+#if defined(E2D_FAST) && !defined(E2D_FP32)
+// ---- per-handle geometry of the marching kernel (fast-path arithmetic) ------
+namespace e2d {
+namespace E2D_NS {
+namespace mk {
+
+__device__ __forceinline__ void cell_geo(const Blocks& B, int b, int I, int J, double& xc, double& yc, double& A) {
+  fm::quad_centroid(B.X[node_ix(B, b, J, I)], B.Y[node_ix(B, b, J, I)], B.X[node_ix(B, b, J, I + 1)],
+                    B.Y[node_ix(B, b, J, I + 1)], B.X[node_ix(B, b, J + 1, I + 1)], B.Y[node_ix(B, b, J + 1, I + 1)],
+                    B.X[node_ix(B, b, J + 1, I)], B.Y[node_ix(B, b, J + 1, I)], xc, yc, A);
+}
+__device__ __forceinline__ double node_len(const Blocks& B, int b, int ai, int aj, int ci, int cj) {
+  const double dx = B.X[node_ix(B, b, aj, ai)] - B.X[node_ix(B, b, cj, ci)];
+  const double dy = B.Y[node_ix(B, b, aj, ai)] - B.Y[node_ix(B, b, cj, ci)];
+  const double q = dx * dx + dy * dy;
+  return fm::sqrt_from_rsqrt(q, fm::rsqrt(q));
+}
+
+// One thread per cell (ghosts included): centroid; for ring cells the
+// stencil mask and least-squares inverse; for interior cells 1/A and the CFL
+// lengths; and the degenerate-edge test (an edge no longer than 1e-9 of its
+// cell's perimeter takes the reference's ihat normal, which the marching
+// kernel does not restate: *degenerate is set and the stage kernel is used).
+__global__ void geometry_kernel(Blocks B, double* geom, unsigned char* mask, int* degenerate) {
+  const long long plane = (long long)B.NCi * B.NCj;
+  const long long n = plane * B.nblk;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int b = int(t / plane);
+    const long long r = t - b * plane;
+    const int J = int(r / B.NCi), I = int(r - (long long)J * B.NCi);
+    double* gp = geom + size_t(b) * GEOM_NF * plane + r;
+    double xc, yc, A;
+    cell_geo(B, b, I, J, xc, yc, A);
+    gp[G_XC * plane] = xc;
+    gp[G_YC * plane] = yc;
+    for (int f = G_K0; f < GEOM_NF; ++f) gp[f * plane] = 0.0;
+    mask[t] = 0;
+    const bool ring = I >= 1 && I <= B.nci + 2 && J >= 1 && J <= B.ncj + 2;
+    if (!ring) continue;
+    const double lE = node_len(B, b, I + 1, J, I + 1, J + 1), lN = node_len(B, b, I, J + 1, I + 1, J + 1);
+    const double lW = node_len(B, b, I, J, I, J + 1), lS = node_len(B, b, I, J, I + 1, J);
+    const double per = lE + lN + lW + lS;
+    if (!(lE > NANO * per && lN > NANO * per && lW > NANO * per && lS > NANO * per)) atomicOr(degenerate, 1);
+    int di[8], dj[8];
+    const int np = lsq_stencil(B, b, I, J, di, dj);
+    unsigned m = 0;
+    double DxDx = 0, DxDy = 0, DyDy = 0;
+    for (int k = 0; k < np; ++k) {
+      int q = (dj[k] + 1) * 3 + (di[k] + 1);
+      if (q > 4) --q;
+      m |= 1u << q;
+    }
+    for (int q = 0; q < 8; ++q) {
+      if (!(m & (1u << q))) continue;
+      double xn, yn, An;
+      cell_geo(B, b, I + KDI[q], J + KDJ[q], xn, yn, An);
+      const double dx = xn - xc, dy = yn - yc;
+      DxDx += dx * dx; DxDy += dx * dy; DyDy += dy * dy;
+    }
+    mask[t] = (unsigned char)m;
+    if (m) {
+      const double rdet = fm::rcp(DxDx * DyDy - DxDy * DxDy);
+      gp[G_K0 * plane] = DyDy * rdet;
+      gp[G_K1 * plane] = -DxDy * rdet;
+      gp[G_K2 * plane] = DxDx * rdet;
+    }
+    if (I >= NG && I <= B.nci + 1 && J >= NG && J <= B.ncj + 1) {
+      gp[G_RA * plane] = fm::rcp(A);
+      gp[G_DI * plane] = 2.0 * A * fm::rcp(lE + lW);
+      gp[G_DJ * plane] = 2.0 * A * fm::rcp(lN + lS);
+      // outward unit normals nfaceE/W/N/S of the cell (edges a -> c:
+      // (dy, -dx) / |d|, d = a - c)
+      auto nrm = [&](int ai, int aj, int ci, int cj, double& nx, double& ny) {
+        const double dx = B.X[node_ix(B, b, aj, ai)] - B.X[node_ix(B, b, cj, ci)];
+        const double dy = B.Y[node_ix(B, b, aj, ai)] - B.Y[node_ix(B, b, cj, ci)];
+        const double rn = fm::rsqrt(dx * dx + dy * dy);
+        nx = dy * rn;
+        ny = -dx * rn;
+      };
+      double eX, eY, wX, wY, nX, nY, sX, sY;
+      nrm(I + 1, J + 1, I + 1, J, eX, eY);
+      nrm(I, J, I, J + 1, wX, wY);
+      nrm(I, J + 1, I + 1, J + 1, nX, nY);
+      nrm(I + 1, J, I, J, sX, sY);
+      gp[G_VIX * plane] = HALF * (eX - wX);
+      gp[G_VIY * plane] = HALF * (eY - wY);
+      gp[G_VJX * plane] = HALF * (nX - sX);
+      gp[G_VJY * plane] = HALF * (nY - sY);
+    }
+  }
+}
+
+// Nodes [nblk][NNj][NNi] -> [nblk][2][NNj][NNp] (X, Y; rows padded to NNp).
+__global__ void pad_nodes_kernel(Blocks B, int NNp, double* out) {
+  const long long plane = (long long)B.NNi * B.NNj;
+  const long long n = plane * B.nblk;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int b = int(t / plane);
+    const long long r = t - b * plane;
+    const int j = int(r / B.NNi), i = int(r - (long long)j * B.NNi);
+    double* o = out + size_t(b) * 2 * B.NNj * NNp + size_t(j) * NNp + i;
+    o[0] = B.X[t];
+    o[size_t(B.NNj) * NNp] = B.Y[t];
+  }
+}
+
+}  // namespace mk
+
+cudaError_t launch_geometry(const Blocks& B, double* geom, unsigned char* mask, int* degenerate, int NNp,
+                            double* nodes_pad, cudaStream_t st) {
+  mk::geometry_kernel<<<1024, 256, 0, st>>>(B, geom, mask, degenerate);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  mk::pad_nodes_kernel<<<1024, 256, 0, st>>>(B, NNp, nodes_pad);
+  return cudaGetLastError();
+}
+
+}  // namespace E2D_NS
+}  // namespace e2d
+#endif

@@ -1,0 +1,44 @@
+// e2d_march_args.h — arguments of the column-marching stage kernel
+// (e2d_march.cuh) and the layout of the per-cell geometry it streams.
+//
+// Geometry (computed once per handle from the nodes, fast-path arithmetic):
+// an array [nblk][GEOM_NF][NCj][NCi] of doubles holding, per cell,
+//   0, 1  centroid xc, yc                         (every cell, ghosts included)
+//   2..4  least-squares inverse K0, K1, K2         (ring cells: the interior and
+//         one ghost layer); the gradient of a variable is
+//         (Sx K0 + Sy K1, Sx K1 + Sy K2) with Sx, Sy the sums of dW dx, dW dy
+//         over the cell's stencil
+//   5     1 / area                                 (interior cells)
+//   6, 7  2 A / (lE + lW), 2 A / (lN + lS)          (interior cells, CFL step)
+//   8..11 (n_E - n_W) / 2 and (n_N - n_S) / 2, x then y, with the cell's own
+//         outward unit normals                      (interior cells, CFL step)
+// and a byte per cell naming the stencil's neighbours: bit k set when
+// neighbour k of (-1,-1) (0,-1) (1,-1) (-1,0) (1,0) (-1,1) (0,1) (1,1)
+// belongs to the least-squares stencil (the reference's stencils are all
+// subsets of these eight, listed in this order).  The nodes are kept a second
+// time with rows padded to an even length, [nblk][2][NNj][NNp] (X then Y),
+// so that a tensor map can describe them (row strides must be multiples of
+// 16 bytes).
+#pragma once
+#include <cuda.h>
+
+#include "e2d_device.cuh"
+
+namespace e2d {
+
+constexpr int GEOM_NF = 12;
+enum GeomField { G_XC = 0, G_YC, G_K0, G_K1, G_K2, G_RA, G_DI, G_DJ, G_VIX, G_VIY, G_VJX, G_VJY };
+
+struct MarchArgs {
+  StageArgs a;
+  CUtensorMap tmW;   // the stage's input primitive state, as [4 nblk][NCj][NCi]
+  CUtensorMap tmG;   // the geometry, as [GEOM_NF nblk][NCj][NCi]
+  CUtensorMap tmN;   // padded nodes, as [2 nblk][NNj][NNp]
+  const double* geom;
+  const unsigned char* mask;
+  int strips;        // column strips per block
+  int cps;           // chunks per strip
+  long long nchunk;  // strips * cps * nblk
+};
+
+}  // namespace e2d

@@ -270,8 +270,8 @@ __device__ __forceinline__ CState<RT> face_flux(int kind, const PState<RT>& wl, 
 #endif
 }
 __device__ __forceinline__ RT cell_limiter(int kind, const RT* uq, RT u0, RT umin, RT umax) {
-#if defined(E2D_FAST) && !defined(E2D_FP32)
-  return fm::limiter(kind, uq, u0, umin, umax);
+#if defined(E2D_FAST)
+  return fm::limiter<RT>(kind, uq, u0, umin, umax);
 #else
   return limiter(kind, uq, u0, umin, umax);
 #endif
