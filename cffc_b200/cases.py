@@ -158,6 +158,19 @@ def structured(nbi, nbj, nci, ncj, node_fn, periodic_i=False, periodic_j=False,
     """
     bc = dict(bc or {})
     wo = dict(wo or {})
+    # Periodic in both directions is the reference's GRID_PERIODIC_BOX: its
+    # root blocks are wired across the box edges only when there are several
+    # blocks in both directions (Find_Neighbours_of_Root_Solution_Blocks,
+    # src_2D/AMR/QuadTree.cc:363), and a direction with a single block gets
+    # BC_PERIODIC on its two edges instead, BC_NONE otherwise
+    # (src_2D/Grid/HO_Grid2DQuadMultiBlock.h:1299-1330).  A box of 2 x 1
+    # blocks is therefore not wrapped in i at all, as in the reference.
+    box = periodic_i and periodic_j
+    if box:
+        per_i = BC_PERIODIC if nbi == 1 else BC_NONE
+        per_j = BC_PERIODIC if nbj == 1 else BC_NONE
+        bc = dict(W=per_i, E=per_i, S=per_j, N=per_j)
+        periodic_i = periodic_j = nbi > 1 and nbj > 1
     nblk = nbi * nbj
     NCi, NCj = nci + 2 * NG, ncj + 2 * NG
     NNi, NNj = NCi + 1, NCj + 1
@@ -207,11 +220,11 @@ def structured(nbi, nbj, nci, ncj, node_fn, periodic_i=False, periodic_j=False,
                 W[b] = W_fn(xc, yc, b)
     return BlockSet(nci, ncj, neighbour, bc_w, bc_e, bc_s, bc_n, node_x, node_y,
                     wo_w, wo_e, wo_s, wo_n, W, scheme or Scheme(), name, NG, nbi, nbj,
-                    int(periodic_i and periodic_j)).contiguous()
+                    int(box)).contiguous()
 
 
-def periodic_box_bumps(nb=4, nc=32, n_bumps=8, seed=20261203, scheme=None) -> BlockSet:
-    """Unit square, nb x nb blocks of nc x nc cells, periodic; rho = p = 1,
+def periodic_box_bumps(nb=4, nc=32, n_bumps=8, seed=20261203, scheme=None, nbj=None) -> BlockSet:
+    """Unit square, nb x nbj blocks (nbj defaults to nb) of nc x nc cells, periodic; rho = p = 1,
     u = 0.5, v = 0 plus n_bumps Gaussian bumps added to rho and p.
     Draw order (PCG64(seed)): for each bump, amplitude U(0, 0.1), width
     U(0.03, 0.1), centre x U(0, 1), centre y U(0, 1).  Distances are taken to
@@ -219,10 +232,11 @@ def periodic_box_bumps(nb=4, nc=32, n_bumps=8, seed=20261203, scheme=None) -> Bl
     rng = np.random.Generator(np.random.PCG64(seed))
     bumps = [(rng.uniform(0, 0.1), rng.uniform(0.03, 0.1), rng.uniform(0, 1), rng.uniform(0, 1))
              for _ in range(n_bumps)]
-    h = 1.0 / (nb * nc)
+    nbj = nb if nbj is None else nbj
+    hx, hy = 1.0 / (nb * nc), 1.0 / (nbj * nc)
 
     def nodes(I, J):
-        return I * h, J * h
+        return I * hx, J * hy
 
     def W_fn(x, y, b):
         g = np.zeros_like(x)
@@ -232,9 +246,9 @@ def periodic_box_bumps(nb=4, nc=32, n_bumps=8, seed=20261203, scheme=None) -> Bl
             g += amp * np.exp(-(dx * dx + dy * dy) / (w * w))
         return np.stack([1.0 + g, np.full_like(x, 0.5), np.zeros_like(x), 1.0 + g])
 
-    return structured(nb, nb, nc, nc, nodes, True, True, W_fn=W_fn,
+    return structured(nb, nbj, nc, nc, nodes, True, True, W_fn=W_fn,
                       scheme=scheme or Scheme(cfl=0.5, n_stage=2),
-                      name=f"periodic_box_{nb}x{nb}x{nc}^2")
+                      name=f"periodic_box_{nb}x{nbj}x{nc}^2")
 
 
 def curvilinear_mach2(nbi=32, nbj=8, nc=64, seed=20261204, scheme=None,

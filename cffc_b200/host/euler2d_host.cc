@@ -409,7 +409,15 @@ int Create_Initial_Solution_Blocks(const Euler2D_Input_Parameters& IP, std::vect
   const bool periodic = IP.Grid_Type == "Periodic_Box";
   const bool bump = IP.Grid_Type == "Sine_Squared_Bump_Channel";
   int bcW = E2D_BC_REFLECTION, bcE = E2D_BC_REFLECTION, bcS = E2D_BC_REFLECTION, bcN = E2D_BC_REFLECTION;
-  if (periodic) bcW = bcE = bcS = bcN = E2D_BC_NONE;
+  // Periodic_Box: BC_PERIODIC on the edges of a direction with one block,
+  // BC_NONE otherwise (Grid/HO_Grid2DQuadMultiBlock.h:1299-1330); the blocks
+  // are wired across the box edges only with several blocks in both
+  // directions (AMR/QuadTree.cc:363)
+  if (periodic) {
+    bcW = bcE = nbi == 1 ? E2D_BC_PERIODIC : E2D_BC_NONE;
+    bcS = bcN = nbj == 1 ? E2D_BC_PERIODIC : E2D_BC_NONE;
+  }
+  const bool wrap = periodic && nbi > 1 && nbj > 1;
   if (bump) bcW = bcE = E2D_BC_CHARACTERISTIC;
   // node map of global node indices (ghost nodes continue the same map)
   auto node = [&](int I, int J) -> Vector2D {
@@ -431,7 +439,7 @@ int Create_Initial_Solution_Blocks(const Euler2D_Input_Parameters& IP, std::vect
       B.allocate(nci, ncj, ng);
       for (int k = 0; k < 8; ++k) {
         int ni = bi + off[k][0], nj = bj + off[k][1];
-        if (periodic) { ni = (ni + nbi) % nbi; nj = (nj + nbj) % nbj; }
+        if (wrap) { ni = (ni + nbi) % nbi; nj = (nj + nbj) % nbj; }
         if (ni >= 0 && ni < nbi && nj >= 0 && nj < nbj) neighbour[8 * b + k] = nj * nbi + ni;
       }
       for (int i = 0; i < B.Grid.NNi; ++i)
@@ -1020,7 +1028,8 @@ int Read_Multi_Block_Grid(const std::string& path, std::vector<Euler2D_Quad_Bloc
     if (B.NCi != blocks[0].NCi || B.NCj != blocks[0].NCj) return 1;
   // root blocks of the layout (Find_Neighbours_of_Root_Solution_Blocks,
   // AMR/QuadTree.cc:363, with the periodic-box wiring of GRID_PERIODIC_BOX)
-  const bool periodic = code == 55;
+  // (several blocks in both directions)
+  const bool periodic = code == 55 && nbi > 1 && nbj > 1;
   static const int off[8][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}, {-1, -1}, {1, -1}, {-1, 1}, {1, 1}};
   neighbour.assign(size_t(8) * nbi * nbj, -1);
   for (int bj = 0; bj < nbj; ++bj)
