@@ -63,6 +63,126 @@ def fp32_error(bs, nsteps, device):
     return err
 
 
+def fp32_leg(bs, rk_steps, device, steps=3):
+    """The FP32 reconstruction/flux path on the bench workload: its
+    throughput (device time over `steps` calls of rk_steps RK2 steps) and the
+    density / total-energy L2 error against the FP64 path after rk_steps."""
+    import dataclasses
+
+    import torch
+
+    from cffc_b200 import capi
+    b32 = dataclasses.replace(bs, scheme=dataclasses.replace(bs.scheme, precision=PRECISION["fp32"]))
+    h = capi.Handle(b32, device=device)
+    h.set_state()
+    rc, _ = h.rk_steps(rk_steps, history=False)
+    assert rc == 0, rc
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        rc, _ = h.rk_steps(rk_steps, history=False)
+        assert rc == 0, rc
+    secs = (time.perf_counter() - t0) / steps
+    h.close()
+    return {"value": round(bs.n_interior * rk_steps / secs * 1e-6, 3), "unit": "Mcell-updates/s",
+            "timing": "host clock around e2d_rk_steps (returns after the device finished)",
+            "l2_error_vs_fp64": dict(fp32_error(bs, rk_steps, device), steps=rk_steps)}
+
+
+def parity_leg(bs, device):
+    """Per-cell relative error of the fast FP64 residual (the benchmarked
+    kernels) against the exact FP64 path, which reproduces the reference's
+    residual bit for bit (tests/test_gpu_parity.py), on the bench workload."""
+    import dataclasses
+
+    import numpy as np
+
+    from cffc_b200 import capi
+    out = {}
+    for prec in (PRECISION["exact"], PRECISION["fp64"]):
+        h = capi.Handle(dataclasses.replace(bs, scheme=dataclasses.replace(bs.scheme, precision=prec)), device=device)
+        h.set_state()
+        out[prec] = bs.interior(h.residual())
+        h.close()
+    ref, got = out[PRECISION["exact"]], out[PRECISION["fp64"]]
+    nz = ref != 0
+    rel = np.abs(got[nz] - ref[nz]) / np.abs(ref[nz])
+    return {"quantity": "dUdt per cell and variable, fast FP64 vs exact FP64 (= the reference)",
+            "values": int(ref.size), "zero_in_reference": int(ref.size - nz.sum()),
+            "max_rel_err": float(rel.max()), "p99_rel_err": float(np.quantile(rel, 0.99)),
+            "median_rel_err": float(np.median(rel)),
+            "above_1e-12": int((rel > 1e-12).sum()), "above_1e-10": int((rel > 1e-10).sum())}
+
+
+C2_FIXTURES = {None: "nks_c2_bump_12x4x64x32_bj", 4: "nks_c2_bump_12x4x64x32_iluk4"}
+
+
+def nks_c2_measure(precision, device, cpu):
+    """The 98,304-cell subsonic bump channel (12 x 4 blocks of 64 x 32, bump
+    height 0.1, Mach 0.5) from the freestream, as the reference's fixtures
+    run it: block Jacobi for 40 Newton steps (GMRES(30), at most 60
+    iterations) and ILU(4) for 12.  Seconds per Newton step on the device,
+    the history next to the reference's (from the committed fixtures), and
+    the compiled reference's seconds per Newton step on one host core (two
+    steps)."""
+    import numpy as np
+
+    from cffc_b200 import capi, cases
+    out = {"workload": "subsonic bump channel, 12 x 4 blocks x 64x32 (98,304 cells), h 0.1, Mach 0.5, "
+                       "freestream start, tolerance 1e-10"}
+    for level, fx in C2_FIXTURES.items():
+        path = os.path.join(ROOT, "tests", "golden", fx + ".npz")
+        if not os.path.exists(path):
+            continue
+        z = np.load(path)
+        par = z["ref_params"]
+        max_newton, restart, max_gmres, cfl0, tol = par[:5]
+        gtol = float(par[5]) if len(par) > 5 else 1e-5
+        bs = cases.bump_channel()
+        bs.scheme.precision = precision
+        p = capi.nks_params(int(max_newton), gmres_restart=int(restart), max_gmres=int(max_gmres),
+                            overall_tol=float(tol), cfl0=float(cfl0), gmres_tol=gtol, ilu_level=level)
+        h = capi.Handle(bs, device=device)
+        h.set_state()
+        h.nks(capi.nks_params(1, gmres_restart=int(restart), max_gmres=5, ilu_level=level))  # warm-up
+        t0 = time.perf_counter()
+        h.set_state()
+        rc, hist = h.nks(p)
+        secs = time.perf_counter() - t0
+        h.close()
+        ref_ratio = z["ref_newton"][:, 1]
+        n = min(len(hist), len(ref_ratio))
+        dev = [abs(hist[k]["ratio"] - ref_ratio[k]) / ref_ratio[k] for k in range(n)]
+        leg = {"preconditioner": "block Jacobi" if level is None else f"ILU({level})",
+               "newton_steps": len(hist), "seconds": round(secs, 4),
+               "seconds_per_newton_step": round(secs / max(1, len(hist)), 5),
+               "gmres_iterations": int(sum(st["gmres_iters"] for st in hist)),
+               "converged": bool(rc == 0 and hist and hist[-1]["ratio"] <= float(tol)),
+               "final_ratio": hist[-1]["ratio"] if hist else None,
+               "reference_final_ratio": float(z["ref_final"][2]),
+               "ratio_history": [round(st["ratio"], 6) for st in hist],
+               "max_rel_dev_ratio_vs_reference": float(max(dev)) if dev else None,
+               "gmres_counts_equal_to_reference": int(sum(hist[k]["gmres_iters"] == int(z["ref_gmres"][k, 0])
+                                                          for k in range(n)))}
+        harness = os.path.join(ROOT, "oracle", "_ref", "e2d_ref_harness")
+        if cpu and os.path.exists(harness):
+            with tempfile.TemporaryDirectory() as td:
+                cp, op = os.path.join(td, "c.bin"), os.path.join(td, "o.bin")
+                cases.write_case(cp, bs)
+                extra = [] if level is None else ["ILUK", str(level)]
+                r = subprocess.run([harness, "nks", cp, op, "2", str(int(restart)), str(int(max_gmres)),
+                                    str(float(cfl0)), str(float(tol)), str(gtol)] + extra,
+                                   capture_output=True, text=True)
+                try:
+                    ref_s = float(r.stderr.strip().split(",")[-1].split()[0])
+                    leg["cpu_reference"] = {"seconds_per_newton_step": round(ref_s / 2, 3), "cores": 1,
+                                            "kind": "reference", "sample": "2 Newton steps"}
+                except (ValueError, IndexError):
+                    pass
+        out["iluk4" if level else "block_jacobi"] = leg
+    return out
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -156,6 +276,14 @@ def cpu_port_run(bs, nsteps):
             "mcell_updates_per_s": bs.n_interior * nsteps / s * 1e-6, "error": rc}
 
 
+CPU_DETAIL = {
+    "reference": "the compiled reference's own per-block routines (BCs, dUdt_Multistage_Explicit, "
+                 "Update_Solution_Multistage_Explicit, CFL, norms) on {n} pthreads over blocks, with a "
+                 "restated same-resolution exchange; the reference itself runs one thread per process",
+    "port": "the C restatement of the path (oracle/e2d_oracle.c) on one thread",
+}
+
+
 def cpu_baseline(bs, nsteps=12):
     threads = os.cpu_count() or 1
     r = cpu_reference_run(bs, nsteps, threads)
@@ -166,7 +294,8 @@ def cpu_baseline(bs, nsteps=12):
     sample = (f"{r['steps']} RK2 steps of the same 1,048,576-cell block set "
               f"({r['cells'] * r['steps'] / 1e6:.1f} M cell-updates, {r['seconds']:.1f} s)")
     return {"value": round(r["mcell_updates_per_s"], 4), "unit": "Mcell-updates/s",
-            "cores": r["threads"], "kind": kind, "sample": sample}
+            "cores": r["threads"], "kind": kind, "detail": CPU_DETAIL[kind].format(n=r["threads"]),
+            "sample": sample}
 
 
 NKS_PARAMS = dict(max_newton=40, gmres_restart=30, max_gmres=200, overall_tol=1e-10, cfl0=10.0,
@@ -359,7 +488,9 @@ def run_reference(args):
         if k >= args.warmup:
             vals.append(r)
     v = statistics.median(x["mcell_updates_per_s"] for x in vals)
-    ms = statistics.median(x["seconds"] / x["steps"] * args.rk_steps * 1e3 for x in vals)
+    # one step of this arm is one sample of sample_steps RK2 steps: its
+    # measured time, not a projection to the GPU arm's step length
+    ms = statistics.median(x["seconds"] * 1e3 for x in vals)
     line = {"impl": "reference", "metric": "Mcell-updates/s (Roe+limiter residual, explicit RK2)",
             "value": round(v, 4), "unit": "Mcell-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
@@ -368,7 +499,9 @@ def run_reference(args):
             "data": "synthetic (seeded)", "config": config(bs, 1, args),
             "cpu_baseline": {"value": round(v, 4), "unit": "Mcell-updates/s",
                              "cores": vals[0]["threads"], "kind": kind,
-                             "sample": f"{sample_steps} RK2 steps of the 1,048,576-cell block set per bench step"},
+                             "detail": CPU_DETAIL[kind].format(n=vals[0]["threads"]),
+                             "sample": f"{sample_steps} RK2 steps of the 1,048,576-cell block set per bench step",
+                             "sample_rk_steps": sample_steps},
             "e2e": {"value": round(v, 4), "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -496,9 +629,14 @@ def main():
         }
         if args.precision == "fp32":
             line["l2_error_vs_fp64"] = dict(fp32_error(bs, args.rk_steps, local), steps=args.rk_steps)
+        elif world == 1:
+            line["fp32"] = fp32_leg(bs, args.rk_steps, local)
+        if world == 1:
+            line["parity"] = parity_leg(bs, local)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(bs)
         if world == 1 and not args.no_nks:
+            line["nks_c2"] = nks_c2_measure(PRECISION[args.precision], local, not args.no_cpu_baseline)
             line["nks"] = nks_measure(PRECISION[args.precision], local, not args.no_cpu_baseline)
             line["nks_iluk"] = nks_measure(PRECISION[args.precision], local, not args.no_cpu_baseline, ilu_level=2)
             line["nks_batch"] = nks_batch_measure(PRECISION[args.precision], local)
