@@ -223,6 +223,22 @@ class Handle:
         self._call("norms", ptr(out))
         return out
 
+    def set_precision(self, precision: int) -> None:
+        """e2d_set_precision: E2D_PREC_FP64 (0), _FP32 (1) or _FP64_EXACT (2)
+        for the calls that follow."""
+        self.lib.e2d_set_precision.argtypes = [C.c_void_p, C.c_int]
+        self._call("set_precision", precision)
+
+    def stage_config(self):
+        """e2d_stage_config: (kernel, rows per chunk, tuned microseconds per
+        explicit stage) the autotuner chose for the current precision;
+        kernel 0 = tiled, 1 = column-marching."""
+        k, r, us = C.c_int(0), C.c_int(0), C.c_double(0.0)
+        self.lib.e2d_stage_config.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                              C.POINTER(C.c_double)]
+        self._call("stage_config", C.byref(k), C.byref(r), C.byref(us))
+        return k.value, r.value, us.value
+
     def nks(self, params: NksParams):
         """Newton-Krylov steady solve from the resident state.  Returns
         (rc, history) with one dict per Newton step evaluated."""

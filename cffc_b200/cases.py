@@ -425,6 +425,10 @@ def read_case(path: str) -> BlockSet:
                     os.path.basename(path), ng, nbi, nbj, periodic).contiguous()
 
 
+# block layouts of the batched sweep: 8 to 96 blocks of 32 x 32 cells
+LAYOUTS_8_96 = ((4, 2), (6, 2), (8, 2), (6, 3), (8, 3), (12, 2), (8, 4), (12, 4), (16, 4), (12, 6), (16, 6))
+
+
 def bump_family(n_cases: int, seed: int = 20261205, mach=(1.35, 1.6), height=(0.02, 0.045),
                 layouts=((4, 2), (6, 2), (8, 2), (6, 3), (8, 3), (12, 2), (8, 4), (12, 4)), nc: int = 32,
                 precision: int = 0) -> list:

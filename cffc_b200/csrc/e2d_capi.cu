@@ -6,6 +6,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "../../include/cffc_e2d.h"
@@ -142,7 +145,7 @@ void stage_buffers(e2d_handle* h, int k, double*& W, double*& U) {
 // allows it (fast and FP32 paths, Roe flux, even block width, no degenerate
 // edges), else the tiled stage kernel.
 cudaError_t launch_stage_args(e2d_handle* h, StageArgs& a) {
-  if (h->march && a.B.flux == E2D_FLUX_ROE) {
+  if (h->march && h->sc.precision != E2D_PREC_FP64_EXACT && a.B.flux == E2D_FLUX_ROE) {
     const CUtensorMap* tw = nullptr;
     if (a.Win == h->B.W) tw = &h->tmW[0];
     else if (a.Win == h->B.W2) tw = &h->tmW[1];
@@ -158,7 +161,8 @@ cudaError_t launch_stage_args(e2d_handle* h, StageArgs& a) {
       m.mask = h->gmask;
       const int mi = fast::march_strip_cols();
       m.strips = (h->B.nci + mi - 1) / mi;
-      m.cps = fast::march_chunks(h->B.ncj);
+      m.ch = h->march_rows;
+      m.cps = fast::march_chunks(h->B.ncj, m.ch);
       m.nchunk = (long long)m.strips * m.cps * h->B.nblk;
       const int grid = int(std::min<long long>(m.nchunk, h->march_grid));
       return h->sc.precision == E2D_PREC_FP32 ? f32::launch_march(m, grid, h->stream)
@@ -208,12 +212,13 @@ bool encode3(CUtensorMap* map, void* base, uint64_t d0, uint64_t d1, uint64_t d2
 }
 
 // Geometry, padded nodes and tensor maps of the marching kernel.  The handle
-// keeps the tiled stage kernel when the marching kernel does not apply: the
-// exact path, another flux function, an odd block width (row strides of the
-// tensor maps must be multiples of 16 bytes) or a degenerate edge.
+// keeps the tiled stage kernel when the marching kernel does not apply:
+// another flux function, an odd block width (row strides of the tensor maps
+// must be multiples of 16 bytes) or a degenerate edge (and the exact path
+// always uses the tiled kernel).
 int setup_march(e2d_handle* h) {
-  h->march = false;
-  if (h->sc.precision == E2D_PREC_FP64_EXACT || h->sc.flux != E2D_FLUX_ROE) return 0;
+  h->march = h->march_ok = false;
+  if (h->sc.flux != E2D_FLUX_ROE) return 0;
   const Blocks& B = h->B;
   if (B.NCi % 2 || !encode_fn()) return 0;
   const int mi = fast::march_strip_cols(), wj = fast::march_window_rows();
@@ -237,14 +242,151 @@ int setup_march(e2d_handle* h) {
             encode3(&h->tmN, h->nodes_pad, NNp, B.NNj, 2ull * B.nblk, nwi, wj, 2);
   if (ok && h->W3) ok = encode3(&h->tmW[2], h->W3, B.NCi, B.NCj, 4ull * B.nblk, wi, wj, 4);
   if (!ok) return 0;
-  const int per_sm = h->sc.precision == E2D_PREC_FP32 ? f32::march_ctas_per_sm() : fast::march_ctas_per_sm();
+  const int per_sm = std::min(f32::march_ctas_per_sm(), fast::march_ctas_per_sm());
   int sms = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
   if (per_sm < 1 || sms < 1) return 0;
   h->march_grid = per_sm * sms;
-  // CFFC_E2D_STAGE_KERNEL=tiled keeps the tiled kernel (comparisons of the two)
-  const char* kind = getenv("CFFC_E2D_STAGE_KERNEL");
-  h->march = !(kind && strcmp(kind, "tiled") == 0);
+  h->march_ok = true;
+  return 0;
+}
+
+// ---- stage-kernel autotuner --------------------------------------------------
+// The candidates -- the tiled kernel and the marching kernel with 4 to 8
+// rows per chunk -- are timed on the handle's own block set (a uniform
+// state, an explicit stage 1 per launch, one warm-up and three timed
+// launches each) when the handle is created; the fastest is kept.  Choices
+// are cached per (block shape, block count, precision) for the process.
+struct TuneKey {
+  int nci, ncj, nblk, prec;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(nci, ncj, nblk, prec) < std::tie(o.nci, o.ncj, o.nblk, o.prec);
+  }
+};
+struct TuneChoice {
+  bool march;
+  int rows;
+  float us;
+};
+std::map<TuneKey, TuneChoice> g_tune;
+std::mutex g_tune_mutex;
+
+__global__ void uniform_state_kernel(Blocks B, long long ncell) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    const long long b = q / ((long long)B.NCi * B.NCj), r = q % ((long long)B.NCi * B.NCj);
+    const size_t s = size_t(B.NCi) * B.NCj;
+    const size_t base = size_t(b) * 4 * s + size_t(r);
+    const PState<double> w{1.0, 0.5, 0.1, 1.0};
+    const CState<double> u = U_of_W(w, B.gm1i);
+    B.W[base] = w.d; B.W[base + s] = w.u; B.W[base + 2 * s] = w.v; B.W[base + 3 * s] = w.p;
+    B.U[base] = u.d; B.U[base + s] = u.mx; B.U[base + 2 * s] = u.my; B.U[base + 3 * s] = u.E;
+  }
+}
+
+// Tunes one precision of the fast family (FP64 or FP32) into sel_*[prec].
+int autotune_precision(e2d_handle* h, int prec) {
+  const TuneKey key{h->B.nci, h->B.ncj, h->B.nblk, prec};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      h->sel_march[prec] = it->second.march;
+      h->sel_rows[prec] = it->second.rows;
+      h->sel_us[prec] = it->second.us;
+      return 0;
+    }
+  }
+  const int saved = h->sc.precision;
+  h->sc.precision = prec;
+  StageArgs a{};
+  a.B = h->B;
+  a.B.dWdx = a.B.dWdy = a.B.phi = nullptr;
+  a.mode = 1;
+  a.hist = h->hist;
+  a.step = h->step;
+  a.Win = h->B.W2;
+  a.Ubase = h->B.U2;
+  a.Wout = h->B.W;
+  a.Uout = h->B.U;
+  a.res_out = h->B.dUdt;
+  a.omega = 1.0;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  TuneChoice best{true, h->march_rows, 1e30f};
+  for (int cand = 0; cand <= 5; ++cand) {  // 0: tiled; 1..5: marching, 4..8 rows
+    h->march = cand > 0;
+    h->march_rows = cand > 0 ? 3 + cand : h->march_rows;
+    if (cand > 0 && h->march_rows > fast::march_max_rows()) continue;
+    StageArgs t = a;
+    CK(launch_stage_args(h, t));
+    CK(cudaEventRecord(e0, h->stream));
+    for (int r = 0; r < 3; ++r) {
+      t = a;
+      CK(launch_stage_args(h, t));
+    }
+    CK(cudaEventRecord(e1, h->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    const float us = 1000.f * ms / 3.f;
+    if (us < best.us) best = TuneChoice{h->march, h->march_rows, us};
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->sc.precision = saved;
+  h->sel_march[prec] = best.march;
+  h->sel_rows[prec] = best.rows;
+  h->sel_us[prec] = best.us;
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tune[key] = best;
+  return 0;
+}
+
+// The kernel of the handle's current precision.
+void apply_selection(e2d_handle* h) {
+  const int p = h->sc.precision;
+  if (!h->march_ok || p == E2D_PREC_FP64_EXACT) {
+    h->march = false;
+    return;
+  }
+  h->march = h->sel_march[p];
+  h->march_rows = h->sel_rows[p];
+  h->tune_us = h->sel_us[p];
+}
+
+// Both fast precisions are tuned when the handle is created (a handle may
+// switch between them, e2d_set_precision) on a uniform state in (W2, U2); the
+// state arrays are cleared afterwards.
+int autotune_stage(e2d_handle* h) {
+  if (!h->march_ok) return 0;
+  const char* kind = getenv("CFFC_E2D_STAGE_KERNEL");  // "tiled": comparisons of the two kernels
+  if (kind && strcmp(kind, "tiled") == 0) {
+    h->sel_march[0] = h->sel_march[1] = false;
+    apply_selection(h);
+    return 0;
+  }
+  Blocks Bs = h->B;
+  Bs.W = h->B.W2;
+  Bs.U = h->B.U2;
+  const int grid = int(std::min<size_t>((h->ncell + 255) / 256, 4096));
+  uniform_state_kernel<<<grid, 256, 0, h->stream>>>(Bs, (long long)h->ncell);
+  CK(cudaGetLastError());
+  CK(cudaMemsetAsync(h->hist, 0, sizeof(double) * 4 * size_t(h->hist_cap) * h->B.ncase, h->stream));
+  int rc;
+  if ((rc = autotune_precision(h, E2D_PREC_FP64)) || (rc = autotune_precision(h, E2D_PREC_FP32))) return rc;
+  apply_selection(h);
+  // the handle starts from a clean slate
+  const size_t nb = sizeof(double) * 4 * h->ncell;
+  CK(cudaMemsetAsync(h->B.W, 0, nb, h->stream));
+  CK(cudaMemsetAsync(h->B.U, 0, nb, h->stream));
+  CK(cudaMemsetAsync(h->B.W2, 0, nb, h->stream));
+  CK(cudaMemsetAsync(h->B.U2, 0, nb, h->stream));
+  CK(cudaMemsetAsync(h->B.dUdt, 0, nb, h->stream));
+  CK(cudaMemsetAsync(h->B.dt, 0, sizeof(double) * h->ncell, h->stream));
+  CK(cudaMemsetAsync(h->B.status, 0, sizeof(int) * 2, h->stream));
+  if (h->B.phi_keep) CK(cudaMemsetAsync(h->B.phi_keep, 0, nb, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
   return 0;
 }
 
@@ -538,7 +680,7 @@ e2d_handle* e2d_create(const e2d_blocks_desc* d, const e2d_scheme* sc, int devic
   if ((rc = alloc_freeze(h))) return fail(rc, h);
   if ((rc = ensure_hist(h, 64))) return fail(rc, h);
   B.dWdx = B.dWdy = B.phi = nullptr;
-  if ((rc = setup_march(h))) return fail(rc, h);
+  if ((rc = setup_march(h)) || (rc = autotune_stage(h))) return fail(rc, h);
   return h;
 }
 
@@ -804,6 +946,31 @@ int e2d_cfl(e2d_handle* h, double* dt, double* dtmin) {
   CK(cudaStreamSynchronize(h->stream));
   if (dtmin)
     for (int c = 0; c < h->B.ncase; ++c) dtmin[c] = tmp[4 * c];
+  return 0;
+}
+
+int e2d_set_precision(e2d_handle* h, int precision) {
+  if (!h || (precision != E2D_PREC_FP64 && precision != E2D_PREC_FP32 && precision != E2D_PREC_FP64_EXACT))
+    return E2D_ERR_ARG;
+  if (precision == h->sc.precision) return 0;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  h->sc.precision = precision;
+  apply_selection(h);
+  // captured launches hold the previous precision's kernels
+  if (h->step_graph) {
+    cudaGraphExecDestroy(h->step_graph);
+    h->step_graph = nullptr;
+  }
+  nks_drop_graphs(h);
+  return 0;
+}
+
+int e2d_stage_config(e2d_handle* h, int* kernel, int* rows, double* us) {
+  if (!h) return E2D_ERR_ARG;
+  if (kernel) *kernel = h->march ? 1 : 0;
+  if (rows) *rows = h->march ? h->march_rows : 0;
+  if (us) *us = h->tune_us;
   return 0;
 }
 

@@ -75,7 +75,6 @@ __device__ __forceinline__ CState<double> flux_roe_n(const PState<double>& wl0, 
   const double rsdl = rsqrt(dl), rsdr = rsqrt(dr);
   const double sdl = sqrt_from_rsqrt(dl, rsdl), sdr = sqrt_from_rsqrt(dr, rsdr);
   const double cl2 = g * pl * (rsdl * rsdl), cr2 = g * pr * (rsdr * rsdr);
-  const double cl = sqrt_from_rsqrt(cl2, rsqrt(cl2)), cr = sqrt_from_rsqrt(cr2, rsqrt(cr2));
   const double hl = cl2 * gm1i + 0.5 * (ul * ul + vl * vl);
   const double hr = cr2 * gm1i + 0.5 * (ur * ur + vr * vr);
   const double inv = rcp(sdl + sdr);
@@ -94,8 +93,18 @@ __device__ __forceinline__ CState<double> flux_roe_n(const PState<double>& wl0, 
   const double du = d * u;
   double F0 = du, F1 = du * u + p, F2 = du * v, F3 = du * h;
   const double la0 = ua - ca, la3 = ua + ca;
-  const double d0 = harten_delta(la0, ul - cl, ur - cr);
-  const double d3 = harten_delta(la3, ul + cl, ur + cr);
+  // Harten's fix acts on a wave only where |la| <= delta = max(0, 2 (lr - ll)),
+  // lr - ll = (ur - ul) -+ (cr - cl).  Since |cr - cl| <= sqrt|cr^2 - cl^2|,
+  // delta <= 2 (|ur - ul| + sqrt|cr^2 - cl^2|): faces whose wave speeds
+  // exceed that bound (computed in single precision with a wide margin)
+  // skip the exact sound speeds.
+  const float dbound = 2.0f * (float(fabs(ur - ul)) + sqrtf(float(fabs(cr2 - cl2)))) * 1.001f + 1e-30f;
+  double d0 = 0.0, d3 = 0.0;
+  if (!(float(fabs(la0)) > dbound) || !(float(fabs(la3)) > dbound)) {
+    const double cl = sqrt_from_rsqrt(cl2, rsqrt(cl2)), cr = sqrt_from_rsqrt(cr2, rsqrt(cr2));
+    d0 = harten_delta(la0, ul - cl, ur - cr);
+    d3 = harten_delta(la3, ul + cl, ur + cr);
+  }
   double ws0, ws1, ws3;
   if (up) {
     ws0 = 0.5 * (la0 - fabs(la0) - d0);

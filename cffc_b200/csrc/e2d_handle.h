@@ -43,6 +43,13 @@ struct e2d_handle {
   double* nodes_pad = nullptr;
   CUtensorMap tmW[3], tmG, tmN;
   int march_grid = 0;
+  int march_rows = 7;  // rows of a chunk
+  double tune_us = 0.0;  // the autotuner's time of one explicit stage with the chosen kernel
+  bool march_ok = false;  // geometry and tensor maps set up
+  // the autotuner's choice per fast precision (E2D_PREC_FP64, E2D_PREC_FP32)
+  bool sel_march[2] = {false, false};
+  int sel_rows[2] = {7, 7};
+  double sel_us[2] = {0.0, 0.0};
   // captured explicit step
   cudaGraphExec_t step_graph = nullptr;
   e2d_nks_state* nks = nullptr;
@@ -73,5 +80,6 @@ cudaError_t launch_stage_args(e2d_handle* h, e2d::StageArgs& a);
 cudaError_t ghost_fill_for(e2d_handle* h, int mode);
 int ensure_hist(e2d_handle* h, int n);
 void nks_free(e2d_handle* h);
+void nks_drop_graphs(e2d_handle* h);
 
 }  // namespace e2d_host

@@ -22,8 +22,9 @@ cudaError_t launch_march(const MarchArgs& m, int grid, cudaStream_t st);
 int march_ctas_per_sm();
 int march_strip_cols();
 int march_chunk_rows();
+int march_max_rows();
 int march_window_rows();
-int march_chunks(int ncj);
+int march_chunks(int ncj, int ch);
 cudaError_t launch_geometry(const Blocks& B, double* geom, unsigned char* mask, int* degenerate, int NNp,
                             double* nodes_pad, cudaStream_t st);
 }  // namespace fast

@@ -8,10 +8,11 @@
 // but organised for the hardware:
 //
 // * Work: a block is cut into column strips of MI = 32 interior cells, a
-//   strip into chunks of CH = 7 rows (the last one of a strip 1 to 8 rows:
-//   a remainder of one row joins the chunk below it).  With 8 warps a chunk
-//   of 7 rows reconstructs its 7 rows and their 2 edge columns in one round,
-//   its 15 face rows in two and updates in one.  The launch is persistent: CTA k takes
+//   strip into chunks of ch rows (ch <= 8, chosen per block shape by the
+//   handle's autotuner; the last chunk of a strip takes a remainder that fits
+//   in 8 rows).  With 8 warps a chunk of 7 rows reconstructs its 7 rows and
+//   their 2 edge columns in one round, its 15 face rows in two and updates in
+//   one.  The launch is persistent: CTA k takes
 //   a contiguous range of the (block, strip, chunk) list, so every SM gets the
 //   same number of chunks to within one, and marches up its strips.
 // * Reuse along j: the one-cell reconstruction ring and the bottom j-face row
@@ -37,14 +38,18 @@ namespace e2d {
 namespace E2D_NS {
 namespace mk {
 
-#ifndef E2D_MARCH_ROWS
-#define E2D_MARCH_ROWS 7
+#ifndef E2D_MARCH_COLS
+#define E2D_MARCH_COLS 32
 #endif
-constexpr int MI = 32, MJ = 8, CH = E2D_MARCH_ROWS;  // interior columns; rows of a chunk (at most, nominal)
+#ifndef E2D_MARCH_THREADS
+#define E2D_MARCH_THREADS 256
+#endif
+constexpr int MI = E2D_MARCH_COLS, MJ = 8, CH = 7;  // interior columns; rows of a chunk (at most; default)
 constexpr int WI = MI + 4, WJ = MJ + 4, NWI = MI + 6;  // staged window (cells, node columns)
 constexpr int RCI = MI + 2, RCJ = MJ + 2;          // reconstruction slots (cols, rows j0+1..j0+10)
 constexpr int FJ = MJ + 1;                         // j-face slots (faces j0+2-1/2 .. j0+10-1/2)
-constexpr int THREADS = 256, NWARP = THREADS / 32;  // 8 warps: 128 registers at 2 CTAs per SM
+constexpr int THREADS = E2D_MARCH_THREADS, NWARP = THREADS / 32;
+constexpr int MIN_CTAS = 65536 / (128 * THREADS);                     // CTAs per SM at 128 registers
 constexpr uint32_t WAIT_ITERS = 1u << 24;          // bounded mbarrier wait (about a second)
 constexpr int ST_TIMEOUT = 2;                      // status code: a staging wait ran out
 
@@ -56,8 +61,8 @@ struct Tile {
 constexpr uint32_t TILE_BYTES = sizeof(double) * (6 * WJ * WI + 2 * WJ * NWI);
 static_assert(sizeof(Tile) == TILE_BYTES && TILE_BYTES % 128 == 0, "tile packing");
 static_assert((4 * WJ * WI * 8) % 128 == 0 && (6 * WJ * WI * 8) % 128 == 0, "TMA destinations 128-byte aligned");
-static_assert(NWARP >= MJ, "one warp per update row");
-static_assert(2 * (MJ + 2) <= 32, "one warp covers the edge columns of every reconstructed row");
+static_assert(THREADS >= MJ * MI, "one thread per update cell");
+static_assert(MI % 2 == 0 && (MI * 8) % 16 == 0, "strip origins on 16-byte boundaries");
 
 struct Smem {
   Tile in[2];
@@ -98,8 +103,8 @@ __device__ __forceinline__ Chunk decode(const MarchArgs& m, long long g) {
   k.c = int(g - strip * m.cps);
   k.b = int(strip / m.strips);
   k.i0 = int(strip - (long long)k.b * m.strips) * MI;
-  k.j0 = k.c * CH;
-  k.h = k.c == m.cps - 1 ? min(MJ, m.a.B.ncj - k.j0) : CH;
+  k.j0 = k.c * m.ch;
+  k.h = k.c == m.cps - 1 ? min(MJ, m.a.B.ncj - k.j0) : m.ch;
   return k;
 }
 
@@ -326,14 +331,14 @@ __device__ __forceinline__ void flush_next(const StageArgs& a, Smem& s, int cs, 
 }
 
 template <int MODE, bool FUSE>
-__global__ void __launch_bounds__(THREADS, 2) march_kernel(const __grid_constant__ MarchArgs m) {
+__global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_constant__ MarchArgs m) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // TMA destinations want 128-byte alignment: align the base by hand
   const uint32_t base = tc::smem_addr(smem_raw);
   Smem& s = *reinterpret_cast<Smem*>(smem_raw + ((128u - (base & 127u)) & 127u));
   const StageArgs& a = m.a;
   const Blocks& B = a.B;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   const long long g0 = m.nchunk * blockIdx.x / gridDim.x, g1 = m.nchunk * (blockIdx.x + 1) / gridDim.x;
   if (tid == 0) {
     s.failed = *(volatile int*)B.status;
@@ -365,12 +370,16 @@ __global__ void __launch_bounds__(THREADS, 2) march_kernel(const __grid_constant
       tc::fence_async_smem();  // the other buffer's generic reads come before its overwrite
       issue(gg + 1, buf ^ 1);
     }
-    // the update cells' own inputs: into L2 ahead of the update phase (lane
-    // pairs cover the two halves of the warp's row: state variables, 1/A, the
-    // CFL geometry)
-    if (MODE != 0 && MODE != 3 && warp < k.h) {
-      const int J = k.j0 + NG + warp, I = k.i0 + NG + 16 * (lane & 1), f = lane >> 1;
-      if (J <= B.ncj + 1 && I <= B.nci + 1) {
+    // phase item counts of this chunk (flat item -> (row, column) maps)
+    const bool pro = (gg == g0) || (k.c == 0);  // start of a strip: no carried rows
+    const int s_lo = pro ? 0 : 2, nrow = k.h + 2 - s_lo;  // reconstruction slots [s_lo, h+2)
+    // the update cells' own inputs: into L2 ahead of the update phase (every
+    // 16th cell of a row per field: the state variables, 1/A, the CFL geometry)
+    if (MODE != 0 && MODE != 3) {
+      constexpr int PER_ROW = MI / 16;
+      const int r = tid / (11 * PER_ROW), rem = tid % (11 * PER_ROW), f = rem / PER_ROW;
+      const int J = k.j0 + NG + r, I = k.i0 + NG + 16 * (rem % PER_ROW);
+      if (r < k.h && J <= B.ncj + 1 && I <= B.nci + 1) {
         const double* gq = m.geom + size_t(k.b) * GEOM_NF * plane + size_t(J) * B.NCi + I;
         if (f < 4) {
           const size_t q = cell_var(B, k.b, f, J, I);
@@ -378,16 +387,14 @@ __global__ void __launch_bounds__(THREADS, 2) march_kernel(const __grid_constant
           if (MODE == 2) prefetch_l2(a.res_out + q);
         } else if (f == 4) {
           prefetch_l2(gq + G_RA * plane);
-        } else if (FUSE && f < 11) {
+        } else if (FUSE) {
           prefetch_l2(gq + (G_DI + f - 5) * plane);
         }
       }
     }
-    // this warp's first reconstruction row: its inputs, ahead of the wait
-    const bool pro = (gg == g0) || (k.c == 0);  // start of a strip: no carried rows
-    const int s_lo = pro ? 0 : 2, nrow = k.h + 2 - s_lo;  // reconstruction slots [s_lo, h+2)
+    // this thread's first reconstruction cell: its inputs, ahead of the wait
     ReconIn rin{0u, 0.0, 0.0, 0.0};
-    if (warp < nrow) rin = recon_in(m, k, s_lo + warp, lane + 1, plane);
+    if (tid < nrow * RCI) rin = recon_in(m, k, s_lo + tid / RCI, tid % RCI, plane);
     const bool ok = tc::mbar_wait(&s.full[buf], uint32_t(it >> 1) & 1u, WAIT_ITERS);
     if (__syncthreads_or(!ok)) {
       // a staging copy did not complete in time: record it, let the copies
@@ -412,34 +419,27 @@ __global__ void __launch_bounds__(THREADS, 2) march_kernel(const __grid_constant
     const Tile& T = s.in[buf];
     const bool frozen = B.freeze && B.freeze[cs];
 
-    // ---- reconstruction of slots [s_lo, RCJ) ---------------------------------
-    // row tasks 0 .. nrow-1 (32 interior-facing columns), task nrow: the two
-    // edge columns of every row
-    for (int task = warp; task <= nrow; task += NWARP) {
-      const bool row = task < nrow;
-      const int sl = row ? s_lo + task : s_lo + (lane >> 1);
-      const int c = row ? lane + 1 : ((lane & 1) ? RCI - 1 : 0);
-      if (row || lane < 2 * nrow)
-        recon_cell(m, s, T, k, sl, c, (row && task == warp) ? rin : recon_in(m, k, sl, c, plane), frozen);
+    // ---- reconstruction of slots [s_lo, h+2), all RCI columns -------------------
+    for (int t = tid; t < nrow * RCI; t += THREADS) {
+      const int sl = s_lo + t / RCI, c = t % RCI;
+      recon_cell(m, s, T, k, sl, c, t == tid ? rin : recon_in(m, k, sl, c, plane), frozen);
     }
     __syncthreads();
 
     // ---- faces: i-face rows, their last column, j-face rows ----------------------
     {
-      const int h = k.h, sf_lo = pro ? 0 : 1, nfj = h + 1 - sf_lo;  // j-face slots [sf_lo, h]
-      for (int task = warp; task < h + 1 + nfj; task += NWARP) {
-        if (task <= h) {
-          if (task < h || lane < h) iface(m, s, T, k, task < h ? task : lane, task < h ? lane : MI);
-        } else {
-          jface(m, s, T, k, sf_lo + task - h - 1, lane);
-        }
+      // i-faces: h rows of MI+1; j-faces: slots [sf_lo, h] of MI
+      const int h = k.h, sf_lo = pro ? 0 : 1, ni = h * (MI + 1), nj = (h + 1 - sf_lo) * MI;
+      for (int t = tid; t < ni + nj; t += THREADS) {
+        if (t < ni) iface(m, s, T, k, t / (MI + 1), t % (MI + 1));
+        else jface(m, s, T, k, sf_lo + (t - ni) / MI, (t - ni) % MI);
       }
     }
     __syncthreads();
 
     // ---- flux divergence and update, one interior cell per thread ---------------
-    if (warp < k.h) {
-      const int r = warp, q = lane;
+    if (tid < k.h * MI) {
+      const int r = tid / MI, q = tid % MI;
       const int I = k.i0 + NG + q, J = k.j0 + NG + r;
       if (I <= B.nci + 1 && J <= B.ncj + 1) {
         const size_t c = cell_sc(B, k.b, J, I);
@@ -592,12 +592,13 @@ int march_ctas_per_sm() {
 }
 int march_strip_cols() { return mk::MI; }
 int march_chunk_rows() { return mk::CH; }
+int march_max_rows() { return mk::MJ; }
 int march_window_rows() { return mk::WJ; }
-// chunks per strip of ncj rows: CH rows each, a remainder of one row joining
+// chunks per strip of ncj rows: ch rows each, a remainder that fits joining
 // the last full chunk (at most MJ rows)
-int march_chunks(int ncj) {
-  const int n = ncj / mk::CH, r = ncj % mk::CH;
-  if (r == 0 || (r == 1 && n > 0 && mk::CH + 1 <= mk::MJ)) return n;
+int march_chunks(int ncj, int ch) {
+  const int n = ncj / ch, r = ncj % ch;
+  if (r == 0 || (n > 0 && ch + r <= mk::MJ)) return n;
   return n + 1;
 }
 

@@ -37,6 +37,7 @@ struct MarchArgs {
   const double* geom;
   const unsigned char* mask;
   int strips;        // column strips per block
+  int ch;            // rows of a chunk (the last chunk of a strip may hold up to 8)
   int cps;           // chunks per strip
   long long nchunk;  // strips * cps * nblk
 };

@@ -524,6 +524,142 @@ __global__ void identity_blocks_kernel(double* Minv, long long ncell) {
 
 #include "e2d_ilu.cuh"
 
+// ---- GMRES bookkeeping on the device ----------------------------------------
+// Per case: the rotated Hessenberg columns, Givens rotations and right-hand
+// side of the least-squares problem (GMRES2D.h:761-783, 1250-1304), the
+// residual at the cycle's start and the current relative residual, the
+// iteration count and the stop state.  The host only launches the Arnoldi
+// steps; it reads the number of cases still iterating a few steps behind and
+// the per-case results once per restart cycle.
+enum GmresFlag { GF_MET = 1, GF_FAILED = 2, GF_RESTARTED = 4, GF_DONE = 8 };
+
+struct GmresDev {
+  int m, ncase;                    // m: the buffers' cycle length (array strides)
+  const int* cfg;                  // device: [0] cycle length of this solve (<= m), [1] iteration cap
+  double *H, *cs, *sn, *sv;        // [C][m][m+1], [C][m], [C][m], [C][m+1]
+  double *resid0, *relres, *tol;   // [C]
+  int *iters, *flags, *jstop;      // [C]
+  int* its;                        // iterations of this GMRES solve (all cases in lockstep)
+  int* err;                        // first error (E2D_ERR_*), 0 = none
+  int* progress;                   // host-mapped [m]: cases still iterating after step j
+};
+
+__device__ void gm_error(const GmresDev& G, int code) { atomicCAS(G.err, 0, code); }
+
+// Start of a restart cycle: the cases not yet done iterate (active mask),
+// their right-hand side is (beta, 0, ..., 0) with beta = ||V0|| (nrm), and
+// the first cycle records beta as the solve's initial residual.
+__global__ void gmres_cycle_start_kernel(GmresDev G, const double* nrm, int* active, int first) {
+  for (int c = threadIdx.x; c < G.ncase; c += blockDim.x) {
+    const bool on = !(G.flags[c] & GF_DONE);
+    active[c] = on ? 1 : 0;
+    if (!on) continue;
+    const double beta = nrm[c];
+    if (!(beta > 0.0) || !isfinite(beta)) gm_error(G, E2D_ERR_GMRES);
+    double* sv = G.sv + size_t(c) * (G.m + 1);
+    sv[0] = beta;
+    for (int q = 1; q <= G.cfg[0]; ++q) sv[q] = 0.0;
+    if (first) G.resid0[c] = beta;
+    G.flags[c] = 0;
+    G.jstop[c] = -1;
+  }
+}
+
+// The multi-block cycle activity: cases not yet done (before the restart's
+// J x + b product).
+__global__ void gmres_cycle_active_kernel(GmresDev G, int* active) {
+  for (int c = threadIdx.x; c < G.ncase; c += blockDim.x) active[c] = (G.flags[c] & GF_DONE) ? 0 : 1;
+}
+
+__device__ __forceinline__ void apply_rot(double& dx, double& dy, double cs, double sn) {
+  const double t = cs * dx + sn * dy;
+  dy = -sn * dx + cs * dy;
+  dx = t;
+}
+
+// End of Arnoldi step j: per iterating case, the Hessenberg column (hcol,
+// [j+2][ncase]) takes the previous rotations, a new rotation zeroes its
+// subdiagonal, the right-hand side rotates with it, and the stop test
+// (tolerance met, iteration cap, end of the cycle) runs.  One CTA.
+__global__ void gmres_givens_kernel(GmresDev G, const double* hcol, int* active, int j) {
+  __shared__ int its, count;
+  if (threadIdx.x == 0) {
+    its = ++*G.its;
+    count = 0;
+  }
+  __syncthreads();
+  const int m = G.m, C = G.ncase, mc = G.cfg[0], cap = G.cfg[1];
+  for (int c = threadIdx.x; c < C; c += blockDim.x) {
+    if (!active[c]) continue;
+    double* Hj = G.H + (size_t(c) * m + j) * (m + 1);
+    for (int k = 0; k <= j + 1; ++k) Hj[k] = hcol[size_t(k) * C + c];
+    if (!isfinite(Hj[j + 1])) gm_error(G, E2D_ERR_NAN);
+    double* cs = G.cs + size_t(c) * m;
+    double* sn = G.sn + size_t(c) * m;
+    double* sv = G.sv + size_t(c) * (m + 1);
+    for (int k = 0; k < j; ++k) apply_rot(Hj[k], Hj[k + 1], cs[k], sn[k]);
+    // generate_rotation (GMRES2D.h:761-775)
+    const double dx = Hj[j], dy = Hj[j + 1];
+    double cj, sj;
+    if (dy == 0.0) {
+      cj = 1.0; sj = 0.0;
+    } else if (fabs(dy) > fabs(dx)) {
+      const double t = dx / dy;
+      sj = 1.0 / sqrt(1.0 + t * t);
+      cj = t * sj;
+    } else {
+      const double t = dy / dx;
+      cj = 1.0 / sqrt(1.0 + t * t);
+      sj = t * cj;
+    }
+    cs[j] = cj; sn[j] = sj;
+    apply_rot(Hj[j], Hj[j + 1], cj, sj);
+    apply_rot(sv[j], sv[j + 1], cj, sj);
+    const double rr = fabs(sv[j + 1]) / G.resid0[c];
+    G.relres[c] = rr;
+    int f = 0;
+    if (rr <= G.tol[c]) f = GF_MET;
+    else if (its >= cap) f = GF_FAILED;
+    else if (j >= mc - 1) f = GF_RESTARTED;
+    if (f) {
+      G.flags[c] = f;
+      G.jstop[c] = j;
+      G.iters[c] = its;
+      active[c] = 0;
+    } else {
+      atomicAdd(&count, 1);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *(volatile int*)(G.progress + j) = count;
+    __threadfence_system();
+  }
+}
+
+// End of a cycle: back substitution of the triangular system of every case
+// that iterated in it (GMRES2D.h:1290-1299), its coefficients for the
+// x update, and the cases that met the tolerance or the cap are done.
+__global__ void gmres_backsub_kernel(GmresDev G, double* svals, int* kcount) {
+  const int m = G.m;
+  for (int c = threadIdx.x; c < G.ncase; c += blockDim.x) {
+    kcount[c] = 0;
+    const int f = G.flags[c];
+    if (f & GF_DONE) continue;
+    const int jj0 = G.jstop[c];
+    if (jj0 < 0) continue;
+    double* sv = G.sv + size_t(c) * (m + 1);
+    const double* H = G.H + size_t(c) * m * (m + 1);
+    for (int jj = jj0; jj >= 0; --jj) {
+      sv[jj] /= H[size_t(jj) * (m + 1) + jj];
+      for (int k = jj - 1; k >= 0; --k) sv[k] -= H[size_t(jj) * (m + 1) + k] * sv[jj];
+    }
+    for (int q = 0; q <= jj0; ++q) svals[size_t(c) * m + q] = sv[q];
+    kcount[c] = jj0 + 1;
+    if (f & (GF_MET | GF_FAILED)) G.flags[c] = f | GF_DONE;
+  }
+}
+
 }  // namespace
 
 struct e2d_nks_state {
@@ -562,6 +698,12 @@ struct e2d_nks_state {
   int* step0 = nullptr;
   double* host = nullptr;    // pinned staging
   size_t host_n = 0;
+  // device-side GMRES bookkeeping; progress is host memory mapped into the
+  // device, step_done the events of the Arnoldi steps in flight
+  GmresDev gd{};
+  int* progress_host = nullptr;
+  int* gcfg = nullptr;       // GmresDev::cfg
+  std::vector<cudaEvent_t> step_done;
   std::vector<void*> allocs;
 };
 
@@ -571,6 +713,9 @@ void nks_free(e2d_handle* h) {
   if (!h->nks) return;
   for (auto g : h->nks->graphs)
     if (g) cudaGraphExecDestroy(g);
+  for (auto ev : h->nks->step_done)
+    if (ev) cudaEventDestroy(ev);
+  if (h->nks->progress_host) cudaFreeHost(h->nks->progress_host);
   for (void* p : h->nks->allocs) cudaFree(p);
   for (void* p : h->nks->ilu_allocs) cudaFree(p);
   if (h->nks->host) cudaFreeHost(h->nks->host);
@@ -583,6 +728,16 @@ void nks_free(e2d_handle* h) {
 namespace {
 
 using namespace e2d_host;
+
+void drop_graphs(e2d_nks_state* s);
+
+}  // namespace
+
+void e2d_host::nks_drop_graphs(e2d_handle* h) {
+  if (h->nks) drop_graphs(h->nks);
+}
+
+namespace {
 
 // Destroys the captured Arnoldi-step graphs: they hold the preconditioner's
 // device pointers and launch shapes by value, so they must go before any of
@@ -624,11 +779,34 @@ int nks_setup(e2d_handle* h, int m) {
     nks_free(h);
     return rc;
   }
-  s->host_n = std::max(size_t(m + 2) * C, size_t(m + 1) * C + C) + 8;
+  s->host_n = std::max(std::max(size_t(m + 2) * C, size_t(m + 1) * C + C), 5 * size_t(C)) + 8;
   if (cudaMallocHost(&s->host, sizeof(double) * s->host_n) != cudaSuccess) {
     nks_free(h);
     return E2D_ERR_NOMEM;
   }
+  GmresDev& G = s->gd;
+  G.m = m;
+  G.ncase = C;
+  if ((rc = nalloc(s, &G.H, size_t(C) * m * (m + 1))) || (rc = nalloc(s, &G.cs, size_t(C) * m)) ||
+      (rc = nalloc(s, &G.sn, size_t(C) * m)) || (rc = nalloc(s, &G.sv, size_t(C) * (m + 1))) ||
+      (rc = nalloc(s, &G.resid0, C)) || (rc = nalloc(s, &G.relres, C)) || (rc = nalloc(s, &G.tol, C)) ||
+      (rc = nalloc(s, &G.iters, C)) || (rc = nalloc(s, &G.flags, C)) || (rc = nalloc(s, &G.jstop, C)) ||
+      (rc = nalloc(s, &G.its, 1)) || (rc = nalloc(s, &G.err, 1)) || (rc = nalloc(s, &s->gcfg, 2))) {
+    nks_free(h);
+    return rc;
+  }
+  if (cudaHostAlloc(&s->progress_host, sizeof(int) * m, cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(reinterpret_cast<void**>(&G.progress), s->progress_host, 0) != cudaSuccess) {
+    nks_free(h);
+    return E2D_ERR_NOMEM;
+  }
+  G.cfg = s->gcfg;
+  s->step_done.assign(m, nullptr);
+  for (auto& ev : s->step_done)
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+      nks_free(h);
+      return E2D_ERR_CUDA;
+    }
   E2D_CK(cudaMemsetAsync(s->V, 0, sizeof(double) * (m + 1) * n, h->stream));
   E2D_CK(cudaMemsetAsync(s->Z, 0, sizeof(double) * m * n, h->stream));
   E2D_CK(cudaMemsetAsync(s->bvec, 0, sizeof(double) * n, h->stream));
@@ -829,25 +1007,6 @@ int fetch(e2d_handle* h, const double* dev, size_t count, double* out) {
   return 0;
 }
 
-void generate_rotation(double dx, double dy, double& cs, double& sn) {
-  if (dy == 0.0) {
-    cs = 1.0; sn = 0.0;
-  } else if (fabs(dy) > fabs(dx)) {
-    const double t = dx / dy;
-    sn = 1.0 / sqrt(1.0 + t * t);
-    cs = t * sn;
-  } else {
-    const double t = dy / dx;
-    cs = 1.0 / sqrt(1.0 + t * t);
-    sn = t * cs;
-  }
-}
-void apply_rotation(double& dx, double& dy, double cs, double sn) {
-  const double t = cs * dx + sn * dy;
-  dy = -sn * dx + cs * dy;
-  dx = t;
-}
-
 // z = M^-1 v with the ILU factors, every active block.
 int ilu_apply(e2d_handle* h, const double* v, double* z) {
   e2d_nks_state* s = h->nks;
@@ -888,7 +1047,10 @@ int arnoldi_step(e2d_handle* h, int j, double eps0, const Norm4& nm, bool ilu) {
   }
   double* hn = s->hcol + size_t(j + 1) * C;
   if ((rc = dot(h, Vn, Vn, hn, FIN_SQRT))) return rc;
-  return scale(h, Vn, hn, 1.0);
+  if ((rc = scale(h, Vn, hn, 1.0))) return rc;
+  gmres_givens_kernel<<<1, VT, 0, h->stream>>>(s->gd, s->hcol, s->active, j);
+  E2D_CK(cudaGetLastError());
+  return 0;
 }
 
 // Arnoldi step j through a CUDA graph: the first use of a j runs eagerly,
@@ -927,14 +1089,20 @@ int run_arnoldi(e2d_handle* h, int j, double eps0, const Norm4& nm, bool ilu) {
 struct GmresCase {
   double resid0 = 0, relres = 0;
   int iters = 0;
-  bool restarted = false, failed = false, met = false, done = false;
-  int jstop = -1;                        // j at which the case left this cycle
-  std::vector<double> H, cs, sn, sv;     // Hessenberg columns [m][m+1], rotations, rhs
+  bool restarted = false, failed = false, met = false;
 };
+
+// Steps launched ahead of the one whose progress the host reads.
+constexpr int GMRES_LOOKAHEAD = 2;
 
 // GMRES_RightPrecon_MatrixFree::solve (GMRES2D.h:790-1544) with the default
 // options (first-order Frechet derivative, no GMRES check), for every case
-// with on[c] set, in lockstep.
+// with on[c] set, in lockstep.  The rotations, the stop test and the back
+// substitution run on the device (gmres_*_kernel); the host launches the
+// Arnoldi steps of a cycle one after another and stops launching when the
+// step GMRES_LOOKAHEAD behind reports no case still iterating (the steps
+// already launched run with every case masked off).  One synchronisation per
+// cycle reads the cases' results.
 int gmres(e2d_handle* h, const e2d_nks_params& p, const std::vector<double>& tol, const std::vector<int>& on,
           const Norm4& nm, std::vector<GmresCase>& G) {
   e2d_nks_state* s = h->nks;
@@ -942,22 +1110,32 @@ int gmres(e2d_handle* h, const e2d_nks_params& p, const std::vector<double>& tol
   const long long n = s->n;
   const size_t nb = sizeof(double) * size_t(n);
   int rc;
+  const GmresDev D = s->gd;
   G.assign(C, GmresCase());
+  // per-case tolerance and start state: the cases not iterating are done
+  double* ht = s->host;
+  int* hf = reinterpret_cast<int*>(s->host + C);
+  E2D_CK(cudaStreamSynchronize(h->stream));  // the staging buffer is free
   for (int c = 0; c < C; ++c) {
-    G[c].H.assign(size_t(m) * (m + 1), 0.0);
-    G[c].cs.assign(m, 0.0); G[c].sn.assign(m, 0.0); G[c].sv.assign(m + 1, 0.0);
-    G[c].done = !on[c];
+    ht[c] = tol[c];
+    hf[c] = on[c] ? 0 : GF_DONE;
   }
+  hf[C] = m;  // cycle length and iteration cap of this solve
+  hf[C + 1] = p.max_gmres;
+  E2D_CK(cudaMemcpyAsync(s->gcfg, hf + C, sizeof(int) * 2, cudaMemcpyHostToDevice, h->stream));
+  E2D_CK(cudaMemcpyAsync(D.tol, ht, sizeof(double) * C, cudaMemcpyHostToDevice, h->stream));
+  E2D_CK(cudaMemcpyAsync(D.flags, hf, sizeof(int) * C, cudaMemcpyHostToDevice, h->stream));
+  E2D_CK(cudaMemsetAsync(D.its, 0, sizeof(int), h->stream));
+  E2D_CK(cudaMemsetAsync(D.err, 0, sizeof(int), h->stream));
   E2D_CK(cudaMemsetAsync(s->x, 0, nb, h->stream));
   // V(0) = b (the Initialize'd V(0) is zero; daxpy adds b)
   E2D_CK(cudaMemcpyAsync(s->V, s->bvec, nb, cudaMemcpyDeviceToDevice, h->stream));
-  std::vector<double> col(size_t(m + 2) * C), beta(C);
-  std::vector<int> cyc(C), kc(C);
-  int iters = 0;
+  std::vector<double> res(3 * size_t(C));
+  std::vector<int> ires(3 * size_t(C) + 1);
   bool first = true;
   for (;;) {
-    for (int c = 0; c < C; ++c) { cyc[c] = !G[c].done; G[c].jstop = -1; }
-    if ((rc = set_active(h, cyc))) return rc;
+    gmres_cycle_active_kernel<<<1, VT, 0, h->stream>>>(D, s->active);
+    E2D_CK(cudaGetLastError());
     if (!first) {
       // V(0) = J x + b with eps = eps0 / ||x|| (GMRES2D.h:838-1000)
       if ((rc = dot(h, s->x, s->x, s->eps, FIN_EPS, p.epsilon0))) return rc;
@@ -965,72 +1143,44 @@ int gmres(e2d_handle* h, const e2d_nks_params& p, const std::vector<double>& tol
       if ((rc = axpy(h, s->V, s->bvec, nullptr, 0.0, 1.0))) return rc;
     }
     if ((rc = dot(h, s->V, s->V, s->nrm, FIN_SQRT))) return rc;
-    if ((rc = fetch(h, s->nrm, C, beta.data()))) return rc;
-    for (int c = 0; c < C; ++c)
-      if (cyc[c] && (!(beta[c] > 0.0) || !std::isfinite(beta[c]))) return E2D_ERR_GMRES;
     if ((rc = scale(h, s->V, s->nrm, -1.0))) return rc;
-    for (int c = 0; c < C; ++c) {
-      if (!cyc[c]) continue;
-      for (int q = 1; q < m + 1; ++q) G[c].sv[q] = 0.0;
-      G[c].sv[0] = beta[c];
-      if (iters == 0) G[c].resid0 = beta[c];
-    }
-    int j = -1;
-    std::vector<int> inner = cyc;
-    for (;;) {
-      ++j;
-      ++iters;
+    gmres_cycle_start_kernel<<<1, VT, 0, h->stream>>>(D, s->nrm, s->active, first ? 1 : 0);
+    E2D_CK(cudaGetLastError());
+    for (int q = 0; q < m; ++q) s->progress_host[q] = -1;
+    for (int j = 0; j < m; ++j) {
       if ((rc = run_arnoldi(h, j, p.epsilon0, nm, use_ilu(p)))) return rc;
-      if ((rc = fetch(h, s->hcol, size_t(j + 2) * C, col.data()))) return rc;
-      bool any = false, changed = false;
-      for (int c = 0; c < C; ++c) {
-        if (!inner[c]) continue;
-        GmresCase& g = G[c];
-        double* Hj = &g.H[size_t(j) * (m + 1)];
-        for (int k = 0; k <= j + 1; ++k) Hj[k] = col[size_t(k) * C + c];
-        if (!std::isfinite(Hj[j + 1])) return E2D_ERR_NAN;
-        for (int k = 0; k < j; ++k) apply_rotation(Hj[k], Hj[k + 1], g.cs[k], g.sn[k]);
-        generate_rotation(Hj[j], Hj[j + 1], g.cs[j], g.sn[j]);
-        apply_rotation(Hj[j], Hj[j + 1], g.cs[j], g.sn[j]);
-        apply_rotation(g.sv[j], g.sv[j + 1], g.cs[j], g.sn[j]);
-        g.relres = fabs(g.sv[j + 1]) / g.resid0;
-        bool stop = false;
-        if (g.relres <= tol[c]) { g.met = true; stop = true; }
-        else if (iters >= p.max_gmres) { g.failed = true; stop = true; }
-        else if (j >= m - 1) { g.restarted = true; stop = true; }
-        if (stop) { g.jstop = j; g.iters = iters; inner[c] = 0; changed = true; }
-        else any = true;
-      }
-      if (!any) break;
-      if (changed && (rc = set_active(h, inner))) return rc;
+      E2D_CK(cudaEventRecord(s->step_done[j], h->stream));
+      const int k = j - GMRES_LOOKAHEAD;
+      if (k < 0) continue;
+      E2D_CK(cudaEventSynchronize(s->step_done[k]));
+      if (*(volatile int*)(s->progress_host + k) == 0) break;  // no case iterates after step k
     }
     // back substitution and x += sum s_k Z_k per case (GMRES2D.h:1290-1304)
-    double* hs = s->host;
-    int* hk = reinterpret_cast<int*>(s->host + size_t(m) * C);
-    E2D_CK(cudaStreamSynchronize(h->stream));
-    for (int c = 0; c < C; ++c) {
-      kc[c] = 0;
-      if (!cyc[c]) continue;
-      GmresCase& g = G[c];
-      const int jj0 = g.jstop;
-      for (int jj = jj0; jj >= 0; --jj) {
-        g.sv[jj] /= g.H[size_t(jj) * (m + 1) + jj];
-        for (int k = jj - 1; k >= 0; --k) g.sv[k] -= g.H[size_t(jj) * (m + 1) + k] * g.sv[jj];
-      }
-      kc[c] = jj0 + 1;
-      for (int q = 0; q < jj0 + 1; ++q) hs[size_t(c) * m + q] = g.sv[q];
-    }
-    for (int c = 0; c < C; ++c) hk[c] = kc[c];
-    E2D_CK(cudaMemcpyAsync(s->svals, hs, sizeof(double) * size_t(m) * C, cudaMemcpyHostToDevice, h->stream));
-    E2D_CK(cudaMemcpyAsync(s->kcount, hk, sizeof(int) * C, cudaMemcpyHostToDevice, h->stream));
+    gmres_backsub_kernel<<<1, VT, 0, h->stream>>>(D, s->svals, s->kcount);
+    E2D_CK(cudaGetLastError());
     update_x_kernel<<<VGRID, VT, 0, h->stream>>>(s->x, s->Z, n, s->nper4, s->svals, s->kcount, m, h->B);
     E2D_CK(cudaGetLastError());
+    double* hr = s->host;
+    int* hi = reinterpret_cast<int*>(s->host + 3 * size_t(C));
+    E2D_CK(cudaMemcpyAsync(hr, D.resid0, sizeof(double) * C, cudaMemcpyDeviceToHost, h->stream));
+    E2D_CK(cudaMemcpyAsync(hr + C, D.relres, sizeof(double) * C, cudaMemcpyDeviceToHost, h->stream));
+    E2D_CK(cudaMemcpyAsync(hi, D.iters, sizeof(int) * C, cudaMemcpyDeviceToHost, h->stream));
+    E2D_CK(cudaMemcpyAsync(hi + C, D.flags, sizeof(int) * C, cudaMemcpyDeviceToHost, h->stream));
+    E2D_CK(cudaMemcpyAsync(hi + 2 * C, D.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     E2D_CK(cudaStreamSynchronize(h->stream));
+    if (hi[2 * C]) return hi[2 * C];
     bool more = false;
     for (int c = 0; c < C; ++c) {
-      if (!cyc[c]) continue;
-      if (G[c].met || G[c].failed) G[c].done = true;
-      else more = true;
+      if (!on[c]) continue;
+      GmresCase& g = G[c];
+      const int f = hi[C + c];
+      g.resid0 = hr[c];
+      g.relres = hr[C + c];
+      g.iters = hi[c];
+      if (f & GF_RESTARTED) g.restarted = true;
+      if (f & GF_MET) g.met = true;
+      if (f & GF_FAILED) g.failed = true;
+      if (!(f & GF_DONE)) more = true;
     }
     if (!more) break;
     first = false;

@@ -335,6 +335,19 @@ int e2d_kernel_times(e2d_handle *h, int n_steps, double out[6]);
  * No reference counterpart. */
 int e2d_fastmath_check(const double *x, int n, double *out);
 
+/* Switches the precision of the handle's reconstruction and flux
+ * (E2D_PREC_*) for the calls that follow -- e.g. an FP32 Newton-Krylov
+ * phase down to the single-precision residual floor, then FP64 to the final
+ * tolerance on the same state.  No reference counterpart. */
+int e2d_set_precision(e2d_handle *h, int precision);
+
+/* The stage kernel the handle's autotuner chose when the handle was created:
+ * *kernel 0 = the tiled kernel, 1 = the column-marching kernel with *rows
+ * rows per chunk; *us the tuner's time of one explicit stage with it (0 when
+ * no tuning ran: the exact path, a flux function other than Roe's, an odd
+ * block width).  Any pointer may be NULL.  No reference counterpart. */
+int e2d_stage_config(e2d_handle *h, int *kernel, int *rows, double *us);
+
 /* Largest block count e2d_residual_norms_static serves. */
 #define E2D_NORMS_STATIC_MAX_BLOCKS 4096
 
