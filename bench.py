@@ -407,7 +407,7 @@ def nks_batch_measure(precision, device, n_cases=16, ilu_level=None):
             "gmres_iterations": sum(st["gmres_iters"] for x in hists for st in x)}
 
 
-def nks_sweep_measure(device, n_cases=512, ilu_level=2, fp32_tol=1e-4):
+def nks_sweep_measure(device, n_cases=512, ilu_level=2, fp32_tol=1e-4, fp32_eps0=1e-2):
     """The batched sweep: n_cases supersonic bump-channel cases
     (cases.bump_family, 8 to 96 blocks of 32 x 32 cells, Mach and bump height
     drawn per case) solved to a 1e-10 drop as ONE batch on one handle, with
@@ -415,9 +415,12 @@ def nks_sweep_measure(device, n_cases=512, ilu_level=2, fp32_tol=1e-4):
     reconstruction and flux down to a fp32_tol drop (near the single-precision
     floor of the residual), then FP64 on the same state to 1e-10
     (e2d_set_precision), the ratio still taken against the freestream
-    residual.  Compared with the same batch solved in FP64 throughout: time,
-    and the per-case relative L2 difference of density and total energy
-    between the two converged states."""
+    residual.  The FP32 phase's Frechet derivatives use a larger perturbation
+    (epsilon0 = fp32_eps0): single-precision round-off in the residual
+    difference divided by the default 1e-6 would swamp the product.
+    Compared with the same batch solved in FP64 throughout: time, and the
+    per-case relative L2 difference of density and total energy between the
+    two converged states."""
     import numpy as np
 
     from cffc_b200 import capi, cases
@@ -425,7 +428,7 @@ def nks_sweep_measure(device, n_cases=512, ilu_level=2, fp32_tol=1e-4):
     cells = sum(b.n_interior for b in fam)
     tol = NKS_PARAMS["overall_tol"]
     p64 = capi.nks_params(**NKS_PARAMS, ilu_level=ilu_level)
-    p32 = capi.nks_params(**dict(NKS_PARAMS, overall_tol=fp32_tol), ilu_level=ilu_level)
+    p32 = capi.nks_params(**dict(NKS_PARAMS, overall_tol=fp32_tol), epsilon0=fp32_eps0, ilu_level=ilu_level)
     hb = capi.BatchHandle(fam, device=device)
     tiles = {}
     for prec, name in ((PRECISION["fp64"], "fp64"), (PRECISION["fp32"], "fp32")):

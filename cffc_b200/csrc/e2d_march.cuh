@@ -48,8 +48,16 @@ constexpr int MI = E2D_MARCH_COLS, MJ = 8, CH = 7;  // interior columns; rows of
 constexpr int WI = MI + 4, WJ = MJ + 4, NWI = MI + 6;  // staged window (cells, node columns)
 constexpr int RCI = MI + 2, RCJ = MJ + 2;          // reconstruction slots (cols, rows j0+1..j0+10)
 constexpr int FJ = MJ + 1;                         // j-face slots (faces j0+2-1/2 .. j0+10-1/2)
+#ifndef E2D_MARCH_NBUF
+#define E2D_MARCH_NBUF 2
+#endif
 constexpr int THREADS = E2D_MARCH_THREADS, NWARP = THREADS / 32;
+#ifdef E2D_MARCH_MINCTAS
+constexpr int MIN_CTAS = E2D_MARCH_MINCTAS;
+#else
 constexpr int MIN_CTAS = 65536 / (128 * THREADS);                     // CTAs per SM at 128 registers
+#endif
+constexpr int NBUF = E2D_MARCH_NBUF;  // staging buffers: 2 = the next chunk's copies overlap this chunk
 constexpr uint32_t WAIT_ITERS = 1u << 24;          // bounded mbarrier wait (about a second)
 constexpr int ST_TIMEOUT = 2;                      // status code: a staging wait ran out
 
@@ -64,11 +72,18 @@ static_assert((4 * WJ * WI * 8) % 128 == 0 && (6 * WJ * WI * 8) % 128 == 0, "TMA
 static_assert(THREADS >= MJ * MI, "one thread per update cell");
 static_assert(MI % 2 == 0 && (MI * 8) % 16 == 0, "strip origins on 16-byte boundaries");
 
+// Reconstructions and j-face fluxes live in rings indexed by the array row
+// (row mod RR): a chunk reads the top reconstruction row and the bottom j-face
+// row the chunk below it left there, and the next chunk's reconstruction
+// overwrites nothing the pending update still reads.
+constexpr int RR = 12;
+static_assert(RR >= RCJ + 2, "ring holds a chunk's rows and the next chunk's first");
+
 struct Smem {
-  Tile in[2];
-  RT px[RCJ][4][RCI], py[RCJ][4][RCI];  // phi * gradient of the reconstructed cells
+  Tile in[NBUF];
+  RT px[RR][4][RCI], py[RR][4][RCI];    // phi * gradient of the reconstructed cells
   double Fi[MJ][4][MI + 1];             // i-face flux x length, faces I-1/2, I = i0+2 .. i0+34
-  double Fj[FJ][4][MI];                 // j-face flux x length
+  double Fj[RR][4][MI];                 // j-face flux x length, face row J (face J-1/2)
   double red[4][NWARP];
   uint64_t full[2];
   int failed;
@@ -114,15 +129,22 @@ __device__ __forceinline__ PState<RT> wwin(const Tile& T, int wj, int wi) {
   return w;
 }
 
+// Ring slot of the reconstruction of chunk slot sl (array row j0+1+sl) and
+// of j-face slot sl (face row j0+2+sl).
+__device__ __forceinline__ int rslot(const Chunk& k, int sl) { return (k.j0 + 1 + sl) % RR; }
+__device__ __forceinline__ int fslot(const Chunk& k, int sl) { return (k.j0 + 2 + sl) % RR; }
+
 // Limited linear state of reconstructed cell (slot sl, column c; window
 // (c+1, sl+1)) at the face point (fx, fy).
-__device__ __forceinline__ PState<RT> fstate(const Smem& s, const Tile& T, int sl, int c, double fx, double fy) {
+__device__ __forceinline__ PState<RT> fstate(const Smem& s, const Tile& T, const Chunk& k, int sl, int c, double fx,
+                                             double fy) {
   const RT dx = RT(fx - T.G[0][sl + 1][c + 1]), dy = RT(fy - T.G[1][sl + 1][c + 1]);
   PState<RT> w = wwin(T, sl + 1, c + 1);
-  w.d = w.d + s.px[sl][0][c] * dx + s.py[sl][0][c] * dy;
-  w.u = w.u + s.px[sl][1][c] * dx + s.py[sl][1][c] * dy;
-  w.v = w.v + s.px[sl][2][c] * dx + s.py[sl][2][c] * dy;
-  w.p = w.p + s.px[sl][3][c] * dx + s.py[sl][3][c] * dy;
+  const int rs = rslot(k, sl);
+  w.d = w.d + s.px[rs][0][c] * dx + s.py[rs][0][c] * dy;
+  w.u = w.u + s.px[rs][1][c] * dx + s.py[rs][1][c] * dy;
+  w.v = w.v + s.px[rs][2][c] * dx + s.py[rs][2][c] * dy;
+  w.p = w.p + s.px[rs][3][c] * dx + s.py[rs][3][c] * dy;
   return w;
 }
 
@@ -157,7 +179,7 @@ __device__ __forceinline__ void recon_cell(const MarchArgs& m, Smem& s, const Ti
   const unsigned msk = in.msk;
   if (msk == 0) {
 #pragma unroll
-    for (int v = 0; v < 4; ++v) { s.px[sl][v][c] = RT(0); s.py[sl][v][c] = RT(0); }
+    for (int v = 0; v < 4; ++v) { s.px[rslot(k, sl)][v][c] = RT(0); s.py[rslot(k, sl)][v][c] = RT(0); }
     if (B.dWdx)
       for (int v = 0; v < 4; ++v) {
         const size_t o = cell_var(B, k.b, v, J, I);
@@ -174,21 +196,29 @@ __device__ __forceinline__ void recon_cell(const MarchArgs& m, Smem& s, const Ti
     w0[v] = RT(T.W[v][wj][wi]);
     Sx[v] = RT(0); Sy[v] = RT(0); mn[v] = w0[v]; mx[v] = w0[v];
   }
+  // the full eight-point stencil (every cell away from a boundary condition)
+  // as straight-line code, so its shared-memory loads can be issued together;
+  // reduced stencils through the mask
+  auto add = [&](int q) {
+    const int ni = wi + KDI[q], nj = wj + KDJ[q];
+    const RT dx = RT(T.G[0][nj][ni] - xc0), dy = RT(T.G[1][nj][ni] - yc0);
 #pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    if (msk & (1u << q)) {
-      const int ni = wi + KDI[q], nj = wj + KDJ[q];
-      const RT dx = RT(T.G[0][nj][ni] - xc0), dy = RT(T.G[1][nj][ni] - yc0);
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const RT w = RT(T.W[v][nj][ni]);
-        const RT du = w - w0[v];
-        Sx[v] += du * dx;
-        Sy[v] += du * dy;
-        mn[v] = dmin(mn[v], w);
-        mx[v] = dmax(mx[v], w);
-      }
+    for (int v = 0; v < 4; ++v) {
+      const RT w = RT(T.W[v][nj][ni]);
+      const RT du = w - w0[v];
+      Sx[v] += du * dx;
+      Sy[v] += du * dy;
+      mn[v] = dmin(mn[v], w);
+      mx[v] = dmax(mx[v], w);
     }
+  };
+  if (msk == 0xFFu) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) add(q);
+  } else {
+#pragma unroll 1
+    for (int q = 0; q < 8; ++q)
+      if (msk & (1u << q)) add(q);
   }
   // face midpoints E, W, N, S of the cell, relative to its centroid
   const double x00 = T.N[0][wj][wi], y00 = T.N[1][wj][wi], x10 = T.N[0][wj][wi + 1], y10 = T.N[1][wj][wi + 1];
@@ -212,8 +242,8 @@ __device__ __forceinline__ void recon_cell(const MarchArgs& m, Smem& s, const Ti
       phi = cell_limiter(B.limiter, uq, w0[v], mn[v], mx[v]);
       if (B.freeze) B.phi_keep[cell_var(B, k.b, v, J, I)] = double(phi);
     }
-    s.px[sl][v][c] = phi * gx;
-    s.py[sl][v][c] = phi * gy;
+    s.px[rslot(k, sl)][v][c] = phi * gx;
+    s.py[rslot(k, sl)][v][c] = phi * gy;
     if (B.dWdx) {
       const size_t o = cell_var(B, k.b, v, J, I);
       B.dWdx[o] = gx; B.dWdy[o] = gy; B.phi[o] = phi;
@@ -253,16 +283,16 @@ __device__ __forceinline__ void iface(const MarchArgs& m, Smem& s, const Tile& T
   PState<RT> wl, wr;
   // left cell (I-1, J): slot r+1, column q; right cell (I, J): slot r+1, column q+1
   if (I == NG && face_bc(bw)) {
-    wr = fstate(s, T, r + 1, q + 1, f.mx, f.my);
+    wr = fstate(s, T, k, r + 1, q + 1, f.mx, f.my);
     wl = (bw == E2D_BC_REFLECTION) ? reflect(wr, RT(-f.nx), RT(-f.ny))
                                    : bc_char_pressure(wr, load_wo(B.wow, k.b, B.NCj, J), RT(-f.nx), RT(-f.ny), g, gm1i);
   } else if (I == B.nci + NG && face_bc(be)) {
-    wl = fstate(s, T, r + 1, q, f.mx, f.my);
+    wl = fstate(s, T, k, r + 1, q, f.mx, f.my);
     wr = (be == E2D_BC_REFLECTION) ? reflect(wl, RT(f.nx), RT(f.ny))
                                    : bc_char_pressure(wl, load_wo(B.woe, k.b, B.NCj, J), RT(f.nx), RT(f.ny), g, gm1i);
   } else {
-    wl = fstate(s, T, r + 1, q, f.mx, f.my);
-    wr = fstate(s, T, r + 1, q + 1, f.mx, f.my);
+    wl = fstate(s, T, k, r + 1, q, f.mx, f.my);
+    wr = fstate(s, T, k, r + 1, q + 1, f.mx, f.my);
   }
   const CState<RT> F = face_flux<true>(B.flux, wl, wr, RT(f.nx), RT(f.ny), g, gm1, gm1i);
   s.Fi[r][0][q] = double(F.d) * f.l;
@@ -284,22 +314,23 @@ __device__ __forceinline__ void jface(const MarchArgs& m, Smem& s, const Tile& T
   PState<RT> wl, wr;
   // lower cell (I, J-1): slot sl, column q+1; upper cell (I, J): slot sl+1
   if (J == NG && face_bc(bs)) {
-    wr = fstate(s, T, sl + 1, q + 1, f.mx, f.my);
+    wr = fstate(s, T, k, sl + 1, q + 1, f.mx, f.my);
     wl = (bs == E2D_BC_REFLECTION) ? reflect(wr, RT(-f.nx), RT(-f.ny))
                                    : bc_char_pressure(wr, load_wo(B.wos, k.b, B.NCi, I), RT(-f.nx), RT(-f.ny), g, gm1i);
   } else if (J == B.ncj + NG && face_bc(bn)) {
-    wl = fstate(s, T, sl, q + 1, f.mx, f.my);
+    wl = fstate(s, T, k, sl, q + 1, f.mx, f.my);
     wr = (bn == E2D_BC_REFLECTION) ? reflect(wl, RT(f.nx), RT(f.ny))
                                    : bc_char_pressure(wl, load_wo(B.won, k.b, B.NCi, I), RT(f.nx), RT(f.ny), g, gm1i);
   } else {
-    wl = fstate(s, T, sl, q + 1, f.mx, f.my);
-    wr = fstate(s, T, sl + 1, q + 1, f.mx, f.my);
+    wl = fstate(s, T, k, sl, q + 1, f.mx, f.my);
+    wr = fstate(s, T, k, sl + 1, q + 1, f.mx, f.my);
   }
   const CState<RT> F = face_flux<true>(B.flux, wl, wr, RT(f.nx), RT(f.ny), g, gm1, gm1i);
-  s.Fj[sl][0][q] = double(F.d) * f.l;
-  s.Fj[sl][1][q] = double(F.mx) * f.l;
-  s.Fj[sl][2][q] = double(F.my) * f.l;
-  s.Fj[sl][3][q] = double(F.E) * f.l;
+  const int fs = fslot(k, sl);
+  s.Fj[fs][0][q] = double(F.d) * f.l;
+  s.Fj[fs][1][q] = double(F.mx) * f.l;
+  s.Fj[fs][2][q] = double(F.my) * f.l;
+  s.Fj[fs][3][q] = double(F.E) * f.l;
 }
 
 // Contributions of the CTA's cells to the next step's CFL minimum and
@@ -330,6 +361,117 @@ __device__ __forceinline__ void flush_next(const StageArgs& a, Smem& s, int cs, 
   __syncthreads();
 }
 
+// Flux divergence and update of cell (row r, column q) of chunk k (case cs):
+// dUdt from the chunk's face fluxes, then per MODE the residual, the Frechet
+// product or the explicit update with its positivity back-off and, fused, the
+// cell's CFL step and density-residual contributions to the next step.
+template <int MODE, bool FUSE>
+__device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, const Chunk& k, int cs, int r, int q,
+                                            size_t plane, double& dt_next, double& n1, double& n2, double& nmax) {
+  const StageArgs& a = m.a;
+  const Blocks& B = a.B;
+  const int I = k.i0 + NG + q, J = k.j0 + NG + r;
+  if (I > B.nci + 1 || J > B.ncj + 1) return;
+  const double g = B.g, gm1 = B.gm1;
+  const size_t c = cell_sc(B, k.b, J, I);
+  const double* gp = m.geom + size_t(k.b) * GEOM_NF * plane + (c - size_t(k.b) * plane);
+  const double rA = gp[G_RA * plane];
+  double kk = 1.0;
+  if (MODE == 1 || MODE == 2) {
+    const double* dtmin_p = a.hist + 4 * ((*a.step) * B.ncase + cs);
+    kk = B.cfl * (B.local_dt ? B.dt[c] : *dtmin_p);
+  }
+  const double kA = kk * rA;
+  const int fs = fslot(k, r), fn = fslot(k, r + 1);
+  double res[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    double d = 0.0;
+    if (MODE == 2) {
+      const size_t qv = cell_var(B, k.b, v, J, I);
+      d = a.res_out[qv];
+      if (a.acc1) d = d + 2.0 * a.acc1[qv] + 2.0 * a.acc2[qv];
+    }
+    d += s.Fi[r][v][q] * kA;
+    d -= s.Fi[r][v][q + 1] * kA;
+    d += s.Fj[fs][v][q] * kA;
+    d -= s.Fj[fn][v][q] * kA;
+    res[v] = d;
+  }
+  if (MODE == 0) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, k.b, v, J, I)] = res[v];
+  } else if (MODE == 3) {
+    // Frechet derivative (GMRES2D.h:445-488):
+    // V = (normalizeR(R) - b)/eps - normalizeUtoR(z * (1/dt))
+    const double eps = a.nks_eps[cs];
+    const double rdt = 1.0 / B.dt[c];
+    const size_t qv = c * 4;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      double val = (res[v] / a.normR[v] - a.nks_b[qv + v]) / eps;
+      val -= (a.nks_z[qv + v] * rdt) * a.normU[v] / a.normR[v];
+      a.nks_v[qv + v] = val;
+    }
+  } else if (a.no_update) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) a.res_out[cell_var(B, k.b, v, J, I)] = res[v];
+  } else {
+    // Update_Solution_Multistage_Explicit: U = Uo + omega*dUdt
+    CState<double> uo;
+    uo.d = a.Ubase[cell_var(B, k.b, 0, J, I)]; uo.mx = a.Ubase[cell_var(B, k.b, 1, J, I)];
+    uo.my = a.Ubase[cell_var(B, k.b, 2, J, I)]; uo.E = a.Ubase[cell_var(B, k.b, 3, J, I)];
+    const double omega = a.omega;
+    CState<double> u;
+    u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
+    u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
+    if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) {
+      if (!B.local_dt) {
+        set_status(B.status, ST_NEGATIVE, int(c));
+      } else {
+        double rrf = 1.0, dtc = B.dt[c];
+        for (int nr = 1; nr <= 10; ++nr) {
+          rrf = HALF * rrf;
+          dtc = rrf * dtc;
+#pragma unroll
+          for (int v = 0; v < 4; ++v) res[v] = rrf * res[v];
+          u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
+          u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
+          if (u.d > 0.0 && u.E > 0.0 && e_of_U(u) > 0.0) break;
+        }
+        B.dt[c] = dtc;
+        if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) set_status(B.status, ST_NEGATIVE, int(c));
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) a.res_out[cell_var(B, k.b, v, J, I)] = res[v];
+    const PState<double> w = fm::W_of_U(u, gm1);
+    a.Uout[cell_var(B, k.b, 0, J, I)] = u.d; a.Uout[cell_var(B, k.b, 1, J, I)] = u.mx;
+    a.Uout[cell_var(B, k.b, 2, J, I)] = u.my; a.Uout[cell_var(B, k.b, 3, J, I)] = u.E;
+    a.Wout[cell_var(B, k.b, 0, J, I)] = w.d; a.Wout[cell_var(B, k.b, 1, J, I)] = w.u;
+    a.Wout[cell_var(B, k.b, 2, J, I)] = w.v; a.Wout[cell_var(B, k.b, 3, J, I)] = w.p;
+    if (FUSE) {
+      // CFL of the updated cell (Euler2DQuadSingleBlock.cc:3019-3080)
+      const double v_i = w.u * gp[G_VIX * plane] + w.v * gp[G_VIY * plane];
+      const double v_j = w.u * gp[G_VJX * plane] + w.v * gp[G_VJY * plane];
+      const double c2 = g * w.p * fm::rcp(w.d);
+      const double snd = fm::sqrt_from_rsqrt(c2, fm::rsqrt(c2));
+      const double ti = gp[G_DI * plane] * fm::rcp(snd + fabs(v_i));
+      const double tj = gp[G_DJ * plane] * fm::rcp(snd + fabs(v_j));
+      const double dtc = dmin(ti, tj);
+      if (B.local_dt) B.dt[c] = dtc;
+      dt_next = dmin(dt_next, dtc);
+      n1 += fabs(res[0]);
+      n2 += res[0] * res[0];
+      nmax = dmax(nmax, fabs(res[0]));
+    }
+  }
+}
+
+// Schedule of a CTA over its chunks c = g0 .. g1-1: per chunk one phase that
+// reconstructs chunk c and updates chunk c-1 (whose face fluxes are complete),
+// then one phase that evaluates chunk c's faces; the last chunk's update runs
+// after the loop.  Two CTA barriers a chunk (and the staging wait).
 template <int MODE, bool FUSE>
 __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_constant__ MarchArgs m) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -348,7 +490,6 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
   __syncthreads();
   if (s.failed || g0 >= g1) return;  // an earlier kernel failed: stop marching (uniform)
   const size_t plane = size_t(B.NCi) * B.NCj;
-  const double g = B.g, gm1 = B.gm1;
 
   auto issue = [&](long long gg, int buf) {
     const Chunk k = decode(m, gg);
@@ -361,20 +502,22 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
   if (tid == 0) issue(g0, 0);
 
   double dt_next = 1000000.0, n1 = 0.0, n2 = 0.0, nmax = 0.0;  // fused next-step CFL / norms
-  int cur_case = -1;
+  int cur_case = -1;  // case the fused contributions belong to
+  Chunk pk{};         // chunk whose update is pending (faces done)
+  int pcase = -1;     // its case, -1: none pending
   int it = 0;
   for (long long gg = g0; gg < g1; ++gg, ++it) {
-    const int buf = it & 1;
+    const int buf = NBUF == 2 ? (it & 1) : 0;
+    const uint32_t par = NBUF == 2 ? (uint32_t(it >> 1) & 1u) : (uint32_t(it) & 1u);
     const Chunk k = decode(m, gg);
-    if (tid == 0 && gg + 1 < g1) {
+    if (NBUF == 2 && tid == 0 && gg + 1 < g1) {
       tc::fence_async_smem();  // the other buffer's generic reads come before its overwrite
       issue(gg + 1, buf ^ 1);
     }
-    // phase item counts of this chunk (flat item -> (row, column) maps)
-    const bool pro = (gg == g0) || (k.c == 0);  // start of a strip: no carried rows
+    const bool pro = (gg == g0) || (k.c == 0);  // start of a strip: no rows below in the rings
     const int s_lo = pro ? 0 : 2, nrow = k.h + 2 - s_lo;  // reconstruction slots [s_lo, h+2)
-    // the update cells' own inputs: into L2 ahead of the update phase (every
-    // 16th cell of a row per field: the state variables, 1/A, the CFL geometry)
+    // this chunk's update cells' own inputs into L2 (its update runs one
+    // chunk later): every 16th cell of a row per field
     if (MODE != 0 && MODE != 3) {
       constexpr int PER_ROW = MI / 16;
       const int r = tid / (11 * PER_ROW), rem = tid % (11 * PER_ROW), f = rem / PER_ROW;
@@ -395,160 +538,68 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
     // this thread's first reconstruction cell: its inputs, ahead of the wait
     ReconIn rin{0u, 0.0, 0.0, 0.0};
     if (tid < nrow * RCI) rin = recon_in(m, k, s_lo + tid / RCI, tid % RCI, plane);
-    const bool ok = tc::mbar_wait(&s.full[buf], uint32_t(it >> 1) & 1u, WAIT_ITERS);
+    const bool ok = tc::mbar_wait(&s.full[buf], par, WAIT_ITERS);
     if (__syncthreads_or(!ok)) {
       // a staging copy did not complete in time: record it, let the copies
       // in flight land (bounded), and stop
       if (tid == 0) {
         set_status(B.status, ST_TIMEOUT, int(gg));
-        tc::mbar_wait(&s.full[buf], uint32_t(it >> 1) & 1u, WAIT_ITERS);
-        if (gg + 1 < g1) tc::mbar_wait(&s.full[buf ^ 1], uint32_t((it + 1) >> 1) & 1u, WAIT_ITERS);
+        tc::mbar_wait(&s.full[buf], par, WAIT_ITERS);
+        if (NBUF == 2 && gg + 1 < g1) tc::mbar_wait(&s.full[buf ^ 1], uint32_t((it + 1) >> 1) & 1u, WAIT_ITERS);
       }
       return;
     }
     const int cs = case_id(B, k.b);
-    if (B.case_active && !B.case_active[cs]) {  // a finished case of a batch (uniform)
-      __syncthreads();
-      continue;
-    }
-    if (FUSE && cs != cur_case) {
+    const bool on = !B.case_active || B.case_active[cs];  // a finished case of a batch: skipped (uniform)
+    if (FUSE && pcase >= 0 && pcase != cur_case) {
       if (cur_case >= 0) flush_next(a, s, cur_case, dt_next, n1, n2, nmax);
-      cur_case = cs;
+      cur_case = pcase;
       dt_next = 1000000.0; n1 = 0.0; n2 = 0.0; nmax = 0.0;
     }
     const Tile& T = s.in[buf];
     const bool frozen = B.freeze && B.freeze[cs];
 
-    // ---- reconstruction of slots [s_lo, h+2), all RCI columns -------------------
-    for (int t = tid; t < nrow * RCI; t += THREADS) {
-      const int sl = s_lo + t / RCI, c = t % RCI;
-      recon_cell(m, s, T, k, sl, c, t == tid ? rin : recon_in(m, k, sl, c, plane), frozen);
+    // ---- reconstruction of chunk gg, update of the pending chunk -------------
+    {
+      const int nrec = on ? nrow * RCI : 0, nupd = pcase >= 0 ? pk.h * MI : 0;
+      for (int t = tid; t < nrec + nupd; t += THREADS) {
+        if (t < nrec) {
+          const int sl = s_lo + t / RCI, c = t % RCI;
+          recon_cell(m, s, T, k, sl, c, t == tid ? rin : recon_in(m, k, sl, c, plane), frozen);
+        } else {
+          const int u = t - nrec;
+          update_cell<MODE, FUSE>(m, s, pk, pcase, u / MI, u % MI, plane, dt_next, n1, n2, nmax);
+        }
+      }
     }
     __syncthreads();
+    pcase = -1;
 
-    // ---- faces: i-face rows, their last column, j-face rows ----------------------
-    {
-      // i-faces: h rows of MI+1; j-faces: slots [sf_lo, h] of MI
+    // ---- faces of chunk gg: i-faces (h rows of MI+1), j-faces (slots [sf_lo, h]) ---
+    if (on) {
       const int h = k.h, sf_lo = pro ? 0 : 1, ni = h * (MI + 1), nj = (h + 1 - sf_lo) * MI;
       for (int t = tid; t < ni + nj; t += THREADS) {
         if (t < ni) iface(m, s, T, k, t / (MI + 1), t % (MI + 1));
         else jface(m, s, T, k, sf_lo + (t - ni) / MI, (t - ni) % MI);
       }
+      pk = k;
+      pcase = cs;
     }
     __syncthreads();
-
-    // ---- flux divergence and update, one interior cell per thread ---------------
-    if (tid < k.h * MI) {
-      const int r = tid / MI, q = tid % MI;
-      const int I = k.i0 + NG + q, J = k.j0 + NG + r;
-      if (I <= B.nci + 1 && J <= B.ncj + 1) {
-        const size_t c = cell_sc(B, k.b, J, I);
-        const double* gp = m.geom + size_t(k.b) * GEOM_NF * plane + (c - size_t(k.b) * plane);
-        const double rA = gp[G_RA * plane];
-        double kk = 1.0;
-        if (MODE == 1 || MODE == 2) {
-          const double* dtmin_p = a.hist + 4 * ((*a.step) * B.ncase + cs);
-          kk = B.cfl * (B.local_dt ? B.dt[c] : *dtmin_p);
-        }
-        const double kA = kk * rA;
-        double res[4];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-          double d = 0.0;
-          if (MODE == 2) {
-            const size_t qv = cell_var(B, k.b, v, J, I);
-            d = a.res_out[qv];
-            if (a.acc1) d = d + 2.0 * a.acc1[qv] + 2.0 * a.acc2[qv];
-          }
-          d += s.Fi[r][v][q] * kA;
-          d -= s.Fi[r][v][q + 1] * kA;
-          d += s.Fj[r][v][q] * kA;
-          d -= s.Fj[r + 1][v][q] * kA;
-          res[v] = d;
-        }
-        if (MODE == 0) {
-#pragma unroll
-          for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, k.b, v, J, I)] = res[v];
-        } else if (MODE == 3) {
-          // Frechet derivative (GMRES2D.h:445-488):
-          // V = (normalizeR(R) - b)/eps - normalizeUtoR(z * (1/dt))
-          const double eps = a.nks_eps[cs];
-          const double rdt = 1.0 / B.dt[c];
-          const size_t qv = c * 4;
-#pragma unroll
-          for (int v = 0; v < 4; ++v) {
-            double val = (res[v] / a.normR[v] - a.nks_b[qv + v]) / eps;
-            val -= (a.nks_z[qv + v] * rdt) * a.normU[v] / a.normR[v];
-            a.nks_v[qv + v] = val;
-          }
-        } else if (a.no_update) {
-#pragma unroll
-          for (int v = 0; v < 4; ++v) a.res_out[cell_var(B, k.b, v, J, I)] = res[v];
-        } else {
-          // Update_Solution_Multistage_Explicit: U = Uo + omega*dUdt
-          CState<double> uo;
-          uo.d = a.Ubase[cell_var(B, k.b, 0, J, I)]; uo.mx = a.Ubase[cell_var(B, k.b, 1, J, I)];
-          uo.my = a.Ubase[cell_var(B, k.b, 2, J, I)]; uo.E = a.Ubase[cell_var(B, k.b, 3, J, I)];
-          const double omega = a.omega;
-          CState<double> u;
-          u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
-          u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
-          if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) {
-            if (!B.local_dt) {
-              set_status(B.status, ST_NEGATIVE, int(c));
-            } else {
-              double rrf = 1.0, dtc = B.dt[c];
-              for (int nr = 1; nr <= 10; ++nr) {
-                rrf = HALF * rrf;
-                dtc = rrf * dtc;
-#pragma unroll
-                for (int v = 0; v < 4; ++v) res[v] = rrf * res[v];
-                u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
-                u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
-                if (u.d > 0.0 && u.E > 0.0 && e_of_U(u) > 0.0) break;
-              }
-              B.dt[c] = dtc;
-              if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) set_status(B.status, ST_NEGATIVE, int(c));
-            }
-          }
-#pragma unroll
-          for (int v = 0; v < 4; ++v) a.res_out[cell_var(B, k.b, v, J, I)] = res[v];
-          const PState<double> w = fm::W_of_U(u, gm1);
-          a.Uout[cell_var(B, k.b, 0, J, I)] = u.d; a.Uout[cell_var(B, k.b, 1, J, I)] = u.mx;
-          a.Uout[cell_var(B, k.b, 2, J, I)] = u.my; a.Uout[cell_var(B, k.b, 3, J, I)] = u.E;
-          a.Wout[cell_var(B, k.b, 0, J, I)] = w.d; a.Wout[cell_var(B, k.b, 1, J, I)] = w.u;
-          a.Wout[cell_var(B, k.b, 2, J, I)] = w.v; a.Wout[cell_var(B, k.b, 3, J, I)] = w.p;
-          if (FUSE) {
-            // CFL of the updated cell (Euler2DQuadSingleBlock.cc:3019-3080)
-            const double v_i = w.u * gp[G_VIX * plane] + w.v * gp[G_VIY * plane];
-            const double v_j = w.u * gp[G_VJX * plane] + w.v * gp[G_VJY * plane];
-            const double c2 = g * w.p * fm::rcp(w.d);
-            const double snd = fm::sqrt_from_rsqrt(c2, fm::rsqrt(c2));
-            const double ti = gp[G_DI * plane] * fm::rcp(snd + fabs(v_i));
-            const double tj = gp[G_DJ * plane] * fm::rcp(snd + fabs(v_j));
-            const double dtc = dmin(ti, tj);
-            if (B.local_dt) B.dt[c] = dtc;
-            dt_next = dmin(dt_next, dtc);
-            n1 += fabs(res[0]);
-            n2 += res[0] * res[0];
-            nmax = dmax(nmax, fabs(res[0]));
-          }
-        }
-      }
+    if (NBUF == 1 && tid == 0 && gg + 1 < g1) {
+      tc::fence_async_smem();  // this chunk's generic reads come before the overwrite
+      issue(gg + 1, 0);
     }
-    __syncthreads();
-
-    // ---- carry the top reconstruction row and j-face row to the next chunk -----
-    for (int q = tid; q < 4 * RCI; q += THREADS) {
-      const int v = q / RCI, c = q % RCI;
-      s.px[1][v][c] = s.px[k.h + 1][v][c];
-      s.py[1][v][c] = s.py[k.h + 1][v][c];
+  }
+  // the last chunk's update
+  if (pcase >= 0) {
+    if (FUSE && pcase != cur_case) {
+      if (cur_case >= 0) flush_next(a, s, cur_case, dt_next, n1, n2, nmax);
+      cur_case = pcase;
+      dt_next = 1000000.0; n1 = 0.0; n2 = 0.0; nmax = 0.0;
     }
-    for (int q = tid; q < 4 * MI; q += THREADS) {
-      const int v = q / MI, c = q % MI;
-      s.Fj[0][v][c] = s.Fj[k.h][v][c];
-    }
-    __syncthreads();
+    for (int t = tid; t < pk.h * MI; t += THREADS)
+      update_cell<MODE, FUSE>(m, s, pk, pcase, t / MI, t % MI, plane, dt_next, n1, n2, nmax);
   }
   if (FUSE && cur_case >= 0) flush_next(a, s, cur_case, dt_next, n1, n2, nmax);
 }
