@@ -34,6 +34,7 @@ SOURCES = {
     "e2d_noalloc.cu": ["-fmad=false"],
     "e2d_nks.cu": ["-fmad=false"],
     "e2d_mlp.cu": ["-fmad=true"],
+    "e2d_mlp_deep.cu": ["-fmad=true"],
 }
 HEADERS = ["e2d_device.cuh", "e2d_stage.cuh", "e2d_aux.cuh", "e2d_geom.cuh", "e2d_launch.h",
            "e2d_fastmath.cuh", "e2d_handle.h", "e2d_tc.cuh", "e2d_smooth.cuh", "e2d_ilu.cuh",

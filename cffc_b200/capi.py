@@ -77,7 +77,7 @@ class NksParams(C.Structure):
                 ("gmres_tol_initial", C.c_double), ("gmres_tol_final", C.c_double),
                 ("epsilon0", C.c_double), ("min_ratio", C.c_double),
                 ("l2_reference", C.POINTER(C.c_double)), ("ilu_level_of_fill", C.c_int32),
-                ("jacobian_order", C.c_int32)]
+                ("jacobian_order", C.c_int32), ("cfl_reference", C.POINTER(C.c_double))]
 
 
 PRECON_BLOCK_JACOBI = 0    # GMRES_Block_Preconditioner Diagonal
@@ -319,12 +319,15 @@ class BatchHandle(Handle):
         rc = self._call("rk_steps", n, ptr(hist))
         return rc, hist
 
-    def nks(self, params: NksParams, l2_reference=None):
+    def nks(self, params: NksParams, l2_reference=None, cfl_reference=None):
         C_ = len(self.cases)
-        ref = None
+        ref = cref = None
         if l2_reference is not None:
             ref = np.ascontiguousarray(l2_reference, dtype=np.float64)
             params.l2_reference = ref.ctypes.data_as(C.POINTER(C.c_double))
+        if cfl_reference is not None:
+            cref = np.ascontiguousarray(cfl_reference, dtype=np.float64)
+            params.cfl_reference = cref.ctypes.data_as(C.POINTER(C.c_double))
         m = max(params.max_newton, 1)
         steps = (NksStep * (m * C_))()
         counts = (C.c_int * C_)()
@@ -333,4 +336,5 @@ class BatchHandle(Handle):
         hists = [[{f: getattr(steps[c * m + k], f) for f, _ in NksStep._fields_ if f != "pad"}
                   for k in range(counts[c])] for c in range(C_)]
         params.l2_reference = None
+        params.cfl_reference = None
         return rc, hists

@@ -1281,7 +1281,8 @@ static int nks_run(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, i
       }
       any = true;
       // SER finite time step (Finite_Time_Step, NKS2D.h:1316-1340)
-      cfl[c] = ratio[c] > p->min_ratio ? p->cfl0 * pow(std::max(1.0, 1.0 / ratio[c]), 1.0) : p->cfl0 / p->min_ratio;
+      const double cr = (p->cfl_reference && p->cfl_reference[c] > 0.0) ? l2 / p->cfl_reference[c] : ratio[c];
+      cfl[c] = cr > p->min_ratio ? p->cfl0 * pow(std::max(1.0, 1.0 / cr), 1.0) : p->cfl0 / p->min_ratio;
       cur[c].cfl = cfl[c];
       tol[c] = std::min(0.9, p->gmres_tol_initial * pow(ratio[c], forcing));
     }

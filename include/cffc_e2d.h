@@ -268,6 +268,11 @@ typedef struct e2d_nks_params {
   const double *l2_reference;
   int32_t ilu_level_of_fill; /* GMRES_ILUK_Level_of_Fill, 0-16         [0]     */
   int32_t jacobian_order;    /* Jacobian_Order: E2D_JACOBIAN_*   [HLLE]    */
+  /* Per case (host, may be NULL): the L2 the SER CFL ratio is measured
+   * against, while the tolerance keeps l2_reference (library extension; a
+   * warm-started case passes its own first residual, so its pseudo-time
+   * step grows from the initial CFL as a cold start's does). */
+  const double *cfl_reference;
 } e2d_nks_params;
 
 /* One Newton step of the history (the values the reference prints). */
@@ -347,6 +352,25 @@ int e2d_set_precision(e2d_handle *h, int precision);
  * no tuning ran: the exact path, a flux function other than Roe's, an odd
  * block width).  Any pointer may be NULL.  No reference counterpart. */
 int e2d_stage_config(e2d_handle *h, int *kernel, int *rows, double *us);
+
+/* The deep warm-start network (library extension, no reference
+ * counterpart): 5 input features padded to 16, four hidden layers of 256
+ * units with GELU (tanh form), 4 outputs; BF16 tcgen05 products with FP32
+ * accumulation, layer by layer over batches of rows.  X: device [n][16]
+ * FP32 (features 5..15 zero), T: device [n][4], Y: device [n][4].  Training
+ * takes `steps` Adam steps on minibatches of `batch` rows drawn without
+ * replacement per epoch (seeded); loss_hist (host, may be NULL) receives the
+ * minibatch losses. */
+typedef struct e2d_mlp_deep e2d_mlp_deep;
+e2d_mlp_deep *e2d_mlp_deep_create(uint64_t seed, int *err);
+void e2d_mlp_deep_destroy(e2d_mlp_deep *d);
+int e2d_mlp_deep_nparams(void);
+int e2d_mlp_deep_params(e2d_mlp_deep *d, float *out, const float *in);
+int e2d_mlp_deep_forward(e2d_mlp_deep *d, const float *X, int n, float *Y, void *stream);
+int e2d_mlp_deep_gradient(e2d_mlp_deep *d, const float *X, const float *T, int n, float *grad, double *loss,
+                          void *stream);
+int e2d_mlp_deep_train(e2d_mlp_deep *d, const float *X, const float *T, int n, int steps, int batch, float lr,
+                       uint64_t seed, float *loss_hist, void *stream);
 
 /* Largest block count e2d_residual_norms_static serves. */
 #define E2D_NORMS_STATIC_MAX_BLOCKS 4096

@@ -61,6 +61,38 @@ def test_residual_fast_within_tolerance(name):
     assert err <= rtol_fast(bs), err
 
 
+def per_value_relative(got, ref):
+    """Pure relative error |x - ref| / |ref| of every value that is not
+    round-off (|ref| >= 1e-8 of its variable's largest |ref|, floored at 1e-3
+    of the largest over all variables, as helpers.rel_err), and the ratio
+    scale / |ref| of each such value."""
+    scale = np.max(np.abs(ref), axis=tuple(a for a in range(ref.ndim) if a != 1), keepdims=True)
+    scale = np.maximum(scale, 1e-3 * np.max(np.abs(ref)))
+    scale = np.broadcast_to(scale, ref.shape)
+    sig = np.abs(ref) >= 1e-8 * scale
+    return np.abs(got[sig] - ref[sig]) / np.abs(ref[sig]), scale[sig] / np.abs(ref[sig])
+
+
+@pytest.mark.parametrize("name", fixtures("residual"))
+def test_residual_fast_relative_per_value(name):
+    """The fast path's residual read value by value: the pure relative error
+    against the reference.  The median is at most 1e-12; a value whose cell's
+    fluxes cancel (|ref| small against its variable's scale) carries the
+    cancellation, so each value's relative error is at most
+    1e-12 (1 + scale / |ref|) (the flux functions other than Roe: 1e-11).
+    The statistics (median, largest, count above 1e-12) are printed."""
+    bs, ref, _, lean = load(name)
+    h = capi.Handle(with_precision(bs, FAST))
+    h.set_state()
+    dUdt = bs.interior(h.residual())
+    r = ref["dUdt"] if lean else bs.interior(ref["dUdt"])
+    rel, amp = per_value_relative(dUdt, r)
+    print(f"{name}: {rel.size} values, median {np.median(rel):.2e}, max {rel.max():.2e}, "
+          f"above 1e-12: {int((rel > 1e-12).sum())}")
+    assert np.median(rel) <= 1e-12
+    assert np.all(rel <= rtol_fast(bs) * (1.0 + amp))
+
+
 @pytest.mark.parametrize("name", fixtures("explicit"))
 def test_explicit_exact_is_bitwise(name):
     bs, ref, steps, lean = load(name)

@@ -12,10 +12,12 @@ from helpers import fixtures, load
 
 
 def test_struct_layouts_match_header():
-    # e2d_nks_params: 4 int32 + 6 double + 1 pointer + 2 int32; e2d_nks_step: 7 double + 4 int32
-    assert ctypes.sizeof(capi.NksParams) == 80
+    # e2d_nks_params: 4 int32 + 6 double + 1 pointer + 2 int32 + 1 pointer;
+    # e2d_nks_step: 7 double + 4 int32
+    assert ctypes.sizeof(capi.NksParams) == 88
     assert capi.NksParams.l2_reference.offset == 64
     assert capi.NksParams.ilu_level_of_fill.offset == 72
+    assert capi.NksParams.cfl_reference.offset == 80
     assert ctypes.sizeof(capi.NksStep) == 72
     assert capi.NksStep.gmres_iters.offset == 56
 
