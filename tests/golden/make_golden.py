@@ -38,6 +38,7 @@ from cffc_b200 import cases  # noqa: E402
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "e2d_ref_harness")
 OUT = os.path.dirname(os.path.abspath(__file__))
 NKS_SUB = 4  # large NKS fixtures keep the final state on every 4th cell in i and j
+SWEEP_SIZE, SWEEP_CASES = 512, (3, 11, 5)  # sweep cases with a reference fixture (8, 12, 16 blocks)
 
 
 def run_residual(bs):
@@ -153,6 +154,7 @@ def golden_cases():
     c2 = cases.bump_channel()  # 12 x 4 blocks of 64 x 32, h 0.1, Mach 0.5
     box21 = cases.periodic_box_bumps(nb=2, nbj=1, nc=16, seed=31)
     box11 = cases.periodic_box_bumps(nb=1, nc=16, seed=32)
+    sweep = cases.bump_family(SWEEP_SIZE, layouts=cases.LAYOUTS_8_96)
     ch_ms = cases.channel(nbi=2, nbj=2, nci=12, ncj=10, seed=9,
                           scheme=cases.Scheme(limiter=cases.LIMITER_VENKATAKRISHNAN, cfl=0.8, n_stage=4, local_dt=1))
     return [
@@ -190,6 +192,14 @@ def golden_cases():
         # preconditioner of the reference's example decks
         ("nks_c2_bump_12x4x64x32_bj", c2, "nks", (40, 30, 60, 1.0, 1e-10)),
         ("nks_c2_bump_12x4x64x32_iluk4", c2, "nks", (12, 30, 120, 10.0, 1e-10, 0.1, 4)),
+    ] + [
+        # three cases of the 512-case supersonic sweep (cases.bump_family with
+        # the 8-96 block layouts), solved to 1e-10 with ILU(2) as the batched
+        # sweep runs them: the FP64 reference answer each case of a batch is
+        # compared with ("sweep_index" in the fixture)
+        (f"nks_sweep{k:03d}_{sweep[k].name.rsplit('_', 1)[1]}", sweep[k], "nks",
+         (40, 30, 200, 10.0, 1e-10, 0.1, 2)) for k in SWEEP_CASES
+    ] + [
         # the Newton step's preconditioner alone: (CFL, ILU level or -1 for
         # block Jacobi, vector seed)
         ("precon_bump_jacobi", bump, "precon", (10.0, -1, 1)),
@@ -400,6 +410,8 @@ def main():
                    if k in (keep, "hist", "err")}
             out["lean"] = np.int32(1)
         out.update({"ref_" + k: v for k, v in res.items()})
+        if name.startswith("nks_sweep"):
+            out["sweep_index"] = np.int32(int(name[len("nks_sweep"):len("nks_sweep") + 3]))
         out["steps"] = np.int32(steps)
         np.savez_compressed(os.path.join(OUT, name + ".npz"), **out)
         print(name, {k: v.shape for k, v in res.items()})

@@ -83,3 +83,53 @@ def test_batch_rejects_mismatched_blocks():
     b = cases.periodic_box_bumps(nb=2, nc=8, seed=1)
     with pytest.raises(RuntimeError):
         capi.BatchHandle([a, b])
+
+
+def _sweep_l2(bs, ref, U):
+    """Relative L2 difference of density and total energy between a solved
+    state and the reference's (every cell, or the fixture's subsample)."""
+    got = bs.interior(U)
+    if "U_sub" in ref:
+        got, want = got[..., ::4, ::4], ref["U_sub"]
+    else:
+        want = bs.interior(ref["U"])
+    return [float(np.sqrt(np.sum((got[:, v] - want[:, v]) ** 2) / np.sum(want[:, v] ** 2))) for v in (0, 3)]
+
+
+def test_sweep_cases_match_reference_fp64_and_mixed():
+    """Three cases of the 512-case supersonic sweep (reference fixtures
+    nks_sweep*: the compiled reference's Newton-Krylov with ILU(2) to a 1e-10
+    drop) solved together in one batch, first in FP64 throughout, then with
+    the FP32 reconstruction and flux down to a 1e-4 drop followed by FP64 to
+    1e-10 (the sweep's mixed-precision solve).  Each case's converged state
+    must agree with the reference's FP64 answer to 1e-9 (relative L2 of
+    density and energy) either way."""
+    from helpers import fixtures, load
+    names = fixtures("nks_sweep")
+    assert len(names) >= 3
+    loaded = [load(n) for n in names]
+    cs = [with_scheme(bs, precision=0) for bs, _, _, _ in loaded]
+    refs = [r for _, r, _, _ in loaded]
+    p64 = capi.nks_params(40, gmres_restart=30, max_gmres=200, overall_tol=1e-10, cfl0=10.0, gmres_tol=0.1,
+                          ilu_level=2)
+    p32 = capi.nks_params(40, gmres_restart=30, max_gmres=200, overall_tol=1e-4, cfl0=10.0, gmres_tol=0.1,
+                          ilu_level=2, epsilon0=1e-2)
+    hb = capi.BatchHandle(cs)
+    hb.set_state()
+    rc, h64 = hb.nks(p64)
+    assert rc == 0
+    s64 = hb.get_state()
+    hb.set_state()
+    hb.set_precision(1)
+    rcA, hA = hb.nks(p32)
+    assert rcA == 0
+    hb.set_precision(0)
+    rcB, hB = hb.nks(p64, [h[0]["l2"] for h in hA])
+    assert rcB == 0
+    smix = hb.get_state()
+    hb.close()
+    for c, (bs, ref) in enumerate(zip(cs, refs)):
+        assert h64[c][-1]["ratio"] <= 1e-10 and hB[c][-1]["ratio"] <= 1e-10, c
+        e64, emix = _sweep_l2(bs, ref, s64[c][1]), _sweep_l2(bs, ref, smix[c][1])
+        print(f"{names[c]}: L2 vs reference fp64 {e64[0]:.1e} {e64[1]:.1e}, mixed {emix[0]:.1e} {emix[1]:.1e}")
+        assert max(e64) <= 1e-9 and max(emix) <= 1e-9, (names[c], e64, emix)
