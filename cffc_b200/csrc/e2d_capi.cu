@@ -159,6 +159,7 @@ cudaError_t launch_stage_args(e2d_handle* h, StageArgs& a) {
       m.tmN = h->tmN;
       m.geom = h->geom;
       m.mask = h->gmask;
+      m.bcside = h->bcside;
       const int mi = fast::march_strip_cols();
       m.strips = (h->B.nci + mi - 1) / mi;
       m.ch = h->march_rows;
@@ -226,11 +227,12 @@ int setup_march(e2d_handle* h) {
   int rc;
   int* degenerate = nullptr;
   if ((rc = dalloc(h, &h->geom, size_t(GEOM_NF) * h->ncell)) || (rc = dalloc(h, &h->gmask, h->ncell)) ||
-      (rc = dalloc(h, &h->nodes_pad, size_t(B.nblk) * 2 * B.NNj * NNp)) || (rc = dalloc(h, &degenerate, 1)))
+      (rc = dalloc(h, &h->bcside, B.nblk)) || (rc = dalloc(h, &h->nodes_pad, size_t(B.nblk) * 2 * B.NNj * NNp)) ||
+      (rc = dalloc(h, &degenerate, 1)))
     return rc;
   CK(cudaMemsetAsync(degenerate, 0, sizeof(int), h->stream));
   CK(cudaMemsetAsync(h->nodes_pad, 0, sizeof(double) * size_t(B.nblk) * 2 * B.NNj * NNp, h->stream));
-  CK(fast::launch_geometry(B, h->geom, h->gmask, degenerate, NNp, h->nodes_pad, h->stream));
+  CK(fast::launch_geometry(B, h->geom, h->gmask, h->bcside, degenerate, NNp, h->nodes_pad, h->stream));
   int deg = 0;
   CK(cudaMemcpyAsync(&deg, degenerate, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));

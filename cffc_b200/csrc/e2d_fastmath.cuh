@@ -176,6 +176,31 @@ __device__ __forceinline__ T limiter(int kind, const T* uq, T u0, T umin, T umax
   return A < Bm ? A * rcp_t(Bm) : T(1);  // Barth-Jespersen
 }
 
+// The same limiter from the face-point differences dq[q] = u_q - u0 and the
+// neighbour extremes as differences dmax = u_max - u0 >= 0, dmin = u_min - u0
+// <= 0 (the marching kernel forms dq directly from the gradient, without
+// the round trip through u_q).
+template <class T>
+__device__ __forceinline__ T limiter_diff(int kind, const T* dq, T dmin, T dmax) {
+  if (kind == E2D_LIMITER_ONE) return T(1);
+  if (kind == E2D_LIMITER_ZERO) return T(0);
+  T A = T(1), Bm = T(0);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const T ab = fabs(dq[q]);
+    if (ab > T(TOLER)) {
+      const T a = fabs(dq[q] > T(0) ? dmax : dmin);
+      if (a * Bm < A * ab) { A = a; Bm = ab; }
+    }
+  }
+  if (kind == E2D_LIMITER_VENKATAKRISHNAN) {
+    const T n = A * A + T(2) * A * Bm;
+    const T d = A * A + A * Bm + T(2) * Bm * Bm;
+    return n < d ? n * rcp_t(d) : T(1);
+  }
+  return A < Bm ? A * rcp_t(Bm) : T(1);
+}
+
 // quadCentroid with the reference-rounded moments and one reciprocal.
 __device__ __forceinline__ void quad_centroid(double x0, double y0, double x1, double y1,
                                               double x2, double y2, double x3, double y3,

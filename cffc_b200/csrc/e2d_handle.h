@@ -40,6 +40,7 @@ struct e2d_handle {
   bool march = false;
   double* geom = nullptr;
   unsigned char* gmask = nullptr;
+  unsigned char* bcside = nullptr;  // per block: sides with face-setting BCs (marching kernel)
   double* nodes_pad = nullptr;
   CUtensorMap tmW[3], tmG, tmN;
   int march_grid = 0;

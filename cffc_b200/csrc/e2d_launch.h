@@ -25,8 +25,8 @@ int march_chunk_rows();
 int march_max_rows();
 int march_window_rows();
 int march_chunks(int ncj, int ch);
-cudaError_t launch_geometry(const Blocks& B, double* geom, unsigned char* mask, int* degenerate, int NNp,
-                            double* nodes_pad, cudaStream_t st);
+cudaError_t launch_geometry(const Blocks& B, double* geom, unsigned char* mask, unsigned char* bcside, int* degenerate,
+                            int NNp, double* nodes_pad, cudaStream_t st);
 }  // namespace fast
 namespace f32 {
 cudaError_t launch_stage(const StageArgs& a, cudaStream_t st);

@@ -21,8 +21,14 @@
 //   of its strip) and each face evaluated once.
 // * Staging: the chunk's window of primitive state (36 x 12 cells, 4
 //   variables), centroids and nodes arrives through three TMA tensor copies
-//   issued by one thread and completing on an mbarrier; the next chunk's
-//   copies are issued before the current chunk is computed (double buffer).
+//   issued by one thread and completing on an mbarrier.  With two staging
+//   buffers (E2D_MARCH_NBUF 2) the next chunk's copies are issued before the
+//   current chunk is computed; with one, after the chunk's faces, and the
+//   other CTA on the SM covers the copy latency.
+// * Faces: an i-face and a j-face item differ only in their cells, edge and
+//   destination and share one flux evaluation; a chunk that reaches no block
+//   edge with a face-setting boundary condition (reflection, characteristic:
+//   a mask of sides per block) evaluates its faces without the BC codes.
 // * Geometry is not recomputed per stage: centroids, the least-squares
 //   inverse of each cell's stencil, 1/area and the CFL lengths were computed
 //   once per handle (e2d_march_args.h); face normals and lengths come from
@@ -111,6 +117,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 
 struct Chunk {
   int b, i0, j0, c, h;  // block, strip origin (interior column), chunk origin (interior row), chunk index, rows
+  int r0;               // ring slot of the chunk's first reconstruction row (array row j0+1)
 };
 __device__ __forceinline__ Chunk decode(const MarchArgs& m, long long g) {
   Chunk k;
@@ -120,6 +127,7 @@ __device__ __forceinline__ Chunk decode(const MarchArgs& m, long long g) {
   k.i0 = int(strip - (long long)k.b * m.strips) * MI;
   k.j0 = k.c * m.ch;
   k.h = k.c == m.cps - 1 ? min(MJ, m.a.B.ncj - k.j0) : m.ch;
+  k.r0 = (k.j0 + 1) % RR;
   return k;
 }
 
@@ -130,9 +138,12 @@ __device__ __forceinline__ PState<RT> wwin(const Tile& T, int wj, int wi) {
 }
 
 // Ring slot of the reconstruction of chunk slot sl (array row j0+1+sl) and
-// of j-face slot sl (face row j0+2+sl).
-__device__ __forceinline__ int rslot(const Chunk& k, int sl) { return (k.j0 + 1 + sl) % RR; }
-__device__ __forceinline__ int fslot(const Chunk& k, int sl) { return (k.j0 + 2 + sl) % RR; }
+// of j-face slot sl (face row j0+2+sl); sl + 1 < RR.
+__device__ __forceinline__ int rslot(const Chunk& k, int sl) {
+  const int r = k.r0 + sl;
+  return r >= RR ? r - RR : r;
+}
+__device__ __forceinline__ int fslot(const Chunk& k, int sl) { return rslot(k, sl + 1); }
 
 // Limited linear state of reconstructed cell (slot sl, column c; window
 // (c+1, sl+1)) at the face point (fx, fy).
@@ -232,14 +243,14 @@ __device__ __forceinline__ void recon_cell(const MarchArgs& m, Smem& s, const Ti
   for (int v = 0; v < 4; ++v) {
     const RT gx = Sx[v] * K0 + Sy[v] * K1;
     const RT gy = Sx[v] * K1 + Sy[v] * K2;
-    RT uq[4];
+    RT dq[4];  // unlimited change from the centroid to each face point
 #pragma unroll
-    for (int q = 0; q < 4; ++q) uq[q] = w0[v] + gx * ofx[q] + gy * ofy[q];
+    for (int q = 0; q < 4; ++q) dq[q] = gx * ofx[q] + gy * ofy[q];
     RT phi;
     if (frozen) {
       phi = RT(B.phi_keep[cell_var(B, k.b, v, J, I)]);
     } else {
-      phi = cell_limiter(B.limiter, uq, w0[v], mn[v], mx[v]);
+      phi = fm::limiter_diff<RT>(B.limiter, dq, mn[v] - w0[v], mx[v] - w0[v]);
       if (B.freeze) B.phi_keep[cell_var(B, k.b, v, J, I)] = double(phi);
     }
     s.px[rslot(k, sl)][v][c] = phi * gx;
@@ -269,68 +280,74 @@ __device__ __forceinline__ FaceGeo face_geo(double ax, double ay, double cx, dou
   return f;
 }
 
-// i-face I-1/2, I = i0+2+q, of row r (J = j0+2+r).
-__device__ __forceinline__ void iface(const MarchArgs& m, Smem& s, const Tile& T, const Chunk& k, int r, int q) {
+// Face item t of chunk k.  Items [0, ni) are the i-faces I-1/2 of rows
+// r = t / (MI+1) (I = i0+2+q, J = j0+2+r), the rest the j-faces J-1/2 of
+// slots sl in [sf_lo, h] (J = j0+2+sl, I = i0+2+q).  Both kinds share one
+// flux evaluation; only the cells, the edge and the destination differ.  BC:
+// the chunk has faces on a block edge whose boundary condition sets the face
+// state (otherwise the BC codes are not read).
+template <bool BC>
+__device__ __forceinline__ void face(const MarchArgs& m, Smem& s, const Tile& T, const Chunk& k, int t, int ni,
+                                     int sf_lo) {
   const Blocks& B = m.a.B;
-  const int I = k.i0 + 2 + q, J = k.j0 + 2 + r;
-  if (I > B.nci + 2 || J > B.ncj + 1) return;
-  // nodes (I, J+1) -> (I, J): window (q+2, r+3), (q+2, r+2)
-  const FaceGeo f = face_geo(T.N[0][r + 3][q + 2], T.N[1][r + 3][q + 2], T.N[0][r + 2][q + 2], T.N[1][r + 2][q + 2]);
-  // BC codes matter at the block's west and east faces only
-  const int bw = I == NG ? B.bcw[size_t(k.b) * B.NCj + J] : E2D_BC_NONE;
-  const int be = I == B.nci + NG ? B.bce[size_t(k.b) * B.NCj + J] : E2D_BC_NONE;
+  int ls, lc, rs, rc;  // reconstructed cells on the left / right: slot, column
+  int aj, ai, cj, ci;  // window row and node column of the edge's ends a -> c
+  double* out;         // flux x length, variable v at out[v * vs]
+  int vs;
+  int bcl = E2D_BC_NONE, bcr = E2D_BC_NONE;  // face-setting BC on the left (W, S) / right (E, N) edge
+  const double *wol = nullptr, *wor = nullptr;
+  int wlen = 0, widx = 0;
+  if (t < ni) {
+    const int r = t / (MI + 1), q = t - r * (MI + 1);
+    const int I = k.i0 + 2 + q, J = k.j0 + 2 + r;
+    if (I > B.nci + 2 || J > B.ncj + 1) return;
+    // left cell (I-1, J): slot r+1, column q; right cell (I, J): column q+1;
+    // nodes (I, J+1) -> (I, J)
+    ls = r + 1; lc = q; rs = r + 1; rc = q + 1;
+    aj = r + 3; ai = q + 2; cj = r + 2; ci = q + 2;
+    out = &s.Fi[r][0][q];
+    vs = MI + 1;
+    if (BC) {  // BC codes matter at the block's west and east faces only
+      if (I == NG) bcl = B.bcw[size_t(k.b) * B.NCj + J];
+      if (I == B.nci + NG) bcr = B.bce[size_t(k.b) * B.NCj + J];
+      wol = B.wow; wor = B.woe; wlen = B.NCj; widx = J;
+    }
+  } else {
+    const int u = t - ni, sl = sf_lo + u / MI, q = u % MI;
+    const int I = k.i0 + 2 + q, J = k.j0 + 2 + sl;
+    if (I > B.nci + 1 || J > B.ncj + 2) return;
+    // lower cell (I, J-1): slot sl, column q+1; upper cell (I, J): slot
+    // sl+1; nodes (I, J) -> (I+1, J)
+    ls = sl; lc = q + 1; rs = sl + 1; rc = q + 1;
+    aj = sl + 2; ai = q + 2; cj = sl + 2; ci = q + 3;
+    out = &s.Fj[fslot(k, sl)][0][q];
+    vs = MI;
+    if (BC) {
+      if (J == NG) bcl = B.bcs[size_t(k.b) * B.NCi + I];
+      if (J == B.ncj + NG) bcr = B.bcn[size_t(k.b) * B.NCi + I];
+      wol = B.wos; wor = B.won; wlen = B.NCi; widx = I;
+    }
+  }
+  const FaceGeo f = face_geo(T.N[0][aj][ai], T.N[1][aj][ai], T.N[0][cj][ci], T.N[1][cj][ci]);
   const RT g = RT(B.g), gm1 = RT(B.gm1), gm1i = RT(B.gm1i);
   PState<RT> wl, wr;
-  // left cell (I-1, J): slot r+1, column q; right cell (I, J): slot r+1, column q+1
-  if (I == NG && face_bc(bw)) {
-    wr = fstate(s, T, k, r + 1, q + 1, f.mx, f.my);
-    wl = (bw == E2D_BC_REFLECTION) ? reflect(wr, RT(-f.nx), RT(-f.ny))
-                                   : bc_char_pressure(wr, load_wo(B.wow, k.b, B.NCj, J), RT(-f.nx), RT(-f.ny), g, gm1i);
-  } else if (I == B.nci + NG && face_bc(be)) {
-    wl = fstate(s, T, k, r + 1, q, f.mx, f.my);
-    wr = (be == E2D_BC_REFLECTION) ? reflect(wl, RT(f.nx), RT(f.ny))
-                                   : bc_char_pressure(wl, load_wo(B.woe, k.b, B.NCj, J), RT(f.nx), RT(f.ny), g, gm1i);
+  if (BC && face_bc(bcl)) {
+    wr = fstate(s, T, k, rs, rc, f.mx, f.my);
+    wl = (bcl == E2D_BC_REFLECTION) ? reflect(wr, RT(-f.nx), RT(-f.ny))
+                                    : bc_char_pressure(wr, load_wo(wol, k.b, wlen, widx), RT(-f.nx), RT(-f.ny), g, gm1i);
+  } else if (BC && face_bc(bcr)) {
+    wl = fstate(s, T, k, ls, lc, f.mx, f.my);
+    wr = (bcr == E2D_BC_REFLECTION) ? reflect(wl, RT(f.nx), RT(f.ny))
+                                    : bc_char_pressure(wl, load_wo(wor, k.b, wlen, widx), RT(f.nx), RT(f.ny), g, gm1i);
   } else {
-    wl = fstate(s, T, k, r + 1, q, f.mx, f.my);
-    wr = fstate(s, T, k, r + 1, q + 1, f.mx, f.my);
+    wl = fstate(s, T, k, ls, lc, f.mx, f.my);
+    wr = fstate(s, T, k, rs, rc, f.mx, f.my);
   }
   const CState<RT> F = face_flux<true>(B.flux, wl, wr, RT(f.nx), RT(f.ny), g, gm1, gm1i);
-  s.Fi[r][0][q] = double(F.d) * f.l;
-  s.Fi[r][1][q] = double(F.mx) * f.l;
-  s.Fi[r][2][q] = double(F.my) * f.l;
-  s.Fi[r][3][q] = double(F.E) * f.l;
-}
-
-// j-face J-1/2 (J = j0+2+sl) of column I = i0+2+q.
-__device__ __forceinline__ void jface(const MarchArgs& m, Smem& s, const Tile& T, const Chunk& k, int sl, int q) {
-  const Blocks& B = m.a.B;
-  const int I = k.i0 + 2 + q, J = k.j0 + 2 + sl;
-  if (I > B.nci + 1 || J > B.ncj + 2) return;
-  // nodes (I, J) -> (I+1, J): window (q+2, sl+2), (q+3, sl+2)
-  const FaceGeo f = face_geo(T.N[0][sl + 2][q + 2], T.N[1][sl + 2][q + 2], T.N[0][sl + 2][q + 3], T.N[1][sl + 2][q + 3]);
-  const int bs = J == NG ? B.bcs[size_t(k.b) * B.NCi + I] : E2D_BC_NONE;
-  const int bn = J == B.ncj + NG ? B.bcn[size_t(k.b) * B.NCi + I] : E2D_BC_NONE;
-  const RT g = RT(B.g), gm1 = RT(B.gm1), gm1i = RT(B.gm1i);
-  PState<RT> wl, wr;
-  // lower cell (I, J-1): slot sl, column q+1; upper cell (I, J): slot sl+1
-  if (J == NG && face_bc(bs)) {
-    wr = fstate(s, T, k, sl + 1, q + 1, f.mx, f.my);
-    wl = (bs == E2D_BC_REFLECTION) ? reflect(wr, RT(-f.nx), RT(-f.ny))
-                                   : bc_char_pressure(wr, load_wo(B.wos, k.b, B.NCi, I), RT(-f.nx), RT(-f.ny), g, gm1i);
-  } else if (J == B.ncj + NG && face_bc(bn)) {
-    wl = fstate(s, T, k, sl, q + 1, f.mx, f.my);
-    wr = (bn == E2D_BC_REFLECTION) ? reflect(wl, RT(f.nx), RT(f.ny))
-                                   : bc_char_pressure(wl, load_wo(B.won, k.b, B.NCi, I), RT(f.nx), RT(f.ny), g, gm1i);
-  } else {
-    wl = fstate(s, T, k, sl, q + 1, f.mx, f.my);
-    wr = fstate(s, T, k, sl + 1, q + 1, f.mx, f.my);
-  }
-  const CState<RT> F = face_flux<true>(B.flux, wl, wr, RT(f.nx), RT(f.ny), g, gm1, gm1i);
-  const int fs = fslot(k, sl);
-  s.Fj[fs][0][q] = double(F.d) * f.l;
-  s.Fj[fs][1][q] = double(F.mx) * f.l;
-  s.Fj[fs][2][q] = double(F.my) * f.l;
-  s.Fj[fs][3][q] = double(F.E) * f.l;
+  out[0] = double(F.d) * f.l;
+  out[vs] = double(F.mx) * f.l;
+  out[2 * vs] = double(F.my) * f.l;
+  out[3 * vs] = double(F.E) * f.l;
 }
 
 // Contributions of the CTA's cells to the next step's CFL minimum and
@@ -365,22 +382,36 @@ __device__ __forceinline__ void flush_next(const StageArgs& a, Smem& s, int cs, 
 // dUdt from the chunk's face fluxes, then per MODE the residual, the Frechet
 // product or the explicit update with its positivity back-off and, fused, the
 // cell's CFL step and density-residual contributions to the next step.
+// Non-positive density, total energy or specific internal energy (the
+// reference's test U.d <= 0 || U.E <= 0 || U.e() <= 0, with e <= 0 taken as
+// E d - (mx^2 + my^2) / 2 <= 0 for d > 0: no division).
+__device__ __forceinline__ double e_times_d2(const CState<double>& u) {
+  return u.E * u.d - 0.5 * (u.mx * u.mx + u.my * u.my);
+}
+__device__ __forceinline__ bool not_positive(const CState<double>& u) {
+  return u.d <= 0.0 || u.E <= 0.0 || e_times_d2(u) <= 0.0;
+}
+
+// dtg: the case's global time step of this explicit step (modes 1, 2 with
+// global time stepping).
 template <int MODE, bool FUSE>
 __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, const Chunk& k, int cs, int r, int q,
-                                            size_t plane, double& dt_next, double& n1, double& n2, double& nmax) {
+                                            size_t plane, double dtg, double& dt_next, double& n1, double& n2,
+                                            double& nmax) {
   const StageArgs& a = m.a;
   const Blocks& B = a.B;
   const int I = k.i0 + NG + q, J = k.j0 + NG + r;
   if (I > B.nci + 1 || J > B.ncj + 1) return;
   const double g = B.g, gm1 = B.gm1;
-  const size_t c = cell_sc(B, k.b, J, I);
-  const double* gp = m.geom + size_t(k.b) * GEOM_NF * plane + (c - size_t(k.b) * plane);
+  // offsets of the cell: in its block's plane, in the scalar arrays, and of
+  // variable 0 in the [nblk][4][NCj][NCi] arrays (variable v: + v * plane)
+  const size_t off = size_t(J) * B.NCi + I;
+  const size_t c = size_t(k.b) * plane + off;
+  const size_t c0 = size_t(k.b) * 4 * plane + off;
+  const double* gp = m.geom + size_t(k.b) * GEOM_NF * plane + off;
   const double rA = gp[G_RA * plane];
   double kk = 1.0;
-  if (MODE == 1 || MODE == 2) {
-    const double* dtmin_p = a.hist + 4 * ((*a.step) * B.ncase + cs);
-    kk = B.cfl * (B.local_dt ? B.dt[c] : *dtmin_p);
-  }
+  if (MODE == 1 || MODE == 2) kk = B.cfl * (B.local_dt ? B.dt[c] : dtg);
   const double kA = kk * rA;
   const int fs = fslot(k, r), fn = fslot(k, r + 1);
   double res[4];
@@ -388,7 +419,7 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
   for (int v = 0; v < 4; ++v) {
     double d = 0.0;
     if (MODE == 2) {
-      const size_t qv = cell_var(B, k.b, v, J, I);
+      const size_t qv = c0 + v * plane;
       d = a.res_out[qv];
       if (a.acc1) d = d + 2.0 * a.acc1[qv] + 2.0 * a.acc2[qv];
     }
@@ -400,7 +431,7 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
   }
   if (MODE == 0) {
 #pragma unroll
-    for (int v = 0; v < 4; ++v) B.dUdt[cell_var(B, k.b, v, J, I)] = res[v];
+    for (int v = 0; v < 4; ++v) B.dUdt[c0 + v * plane] = res[v];
   } else if (MODE == 3) {
     // Frechet derivative (GMRES2D.h:445-488):
     // V = (normalizeR(R) - b)/eps - normalizeUtoR(z * (1/dt))
@@ -415,17 +446,17 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
     }
   } else if (a.no_update) {
 #pragma unroll
-    for (int v = 0; v < 4; ++v) a.res_out[cell_var(B, k.b, v, J, I)] = res[v];
+    for (int v = 0; v < 4; ++v) a.res_out[c0 + v * plane] = res[v];
   } else {
     // Update_Solution_Multistage_Explicit: U = Uo + omega*dUdt
     CState<double> uo;
-    uo.d = a.Ubase[cell_var(B, k.b, 0, J, I)]; uo.mx = a.Ubase[cell_var(B, k.b, 1, J, I)];
-    uo.my = a.Ubase[cell_var(B, k.b, 2, J, I)]; uo.E = a.Ubase[cell_var(B, k.b, 3, J, I)];
+    uo.d = a.Ubase[c0]; uo.mx = a.Ubase[c0 + plane];
+    uo.my = a.Ubase[c0 + 2 * plane]; uo.E = a.Ubase[c0 + 3 * plane];
     const double omega = a.omega;
     CState<double> u;
     u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
     u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
-    if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) {
+    if (not_positive(u)) {
       if (!B.local_dt) {
         set_status(B.status, ST_NEGATIVE, int(c));
       } else {
@@ -437,19 +468,17 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
           for (int v = 0; v < 4; ++v) res[v] = rrf * res[v];
           u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
           u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
-          if (u.d > 0.0 && u.E > 0.0 && e_of_U(u) > 0.0) break;
+          if (u.d > 0.0 && u.E > 0.0 && e_times_d2(u) > 0.0) break;
         }
         B.dt[c] = dtc;
-        if (u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0) set_status(B.status, ST_NEGATIVE, int(c));
+        if (not_positive(u)) set_status(B.status, ST_NEGATIVE, int(c));
       }
     }
 #pragma unroll
-    for (int v = 0; v < 4; ++v) a.res_out[cell_var(B, k.b, v, J, I)] = res[v];
+    for (int v = 0; v < 4; ++v) a.res_out[c0 + v * plane] = res[v];
     const PState<double> w = fm::W_of_U(u, gm1);
-    a.Uout[cell_var(B, k.b, 0, J, I)] = u.d; a.Uout[cell_var(B, k.b, 1, J, I)] = u.mx;
-    a.Uout[cell_var(B, k.b, 2, J, I)] = u.my; a.Uout[cell_var(B, k.b, 3, J, I)] = u.E;
-    a.Wout[cell_var(B, k.b, 0, J, I)] = w.d; a.Wout[cell_var(B, k.b, 1, J, I)] = w.u;
-    a.Wout[cell_var(B, k.b, 2, J, I)] = w.v; a.Wout[cell_var(B, k.b, 3, J, I)] = w.p;
+    a.Uout[c0] = u.d; a.Uout[c0 + plane] = u.mx; a.Uout[c0 + 2 * plane] = u.my; a.Uout[c0 + 3 * plane] = u.E;
+    a.Wout[c0] = w.d; a.Wout[c0 + plane] = w.u; a.Wout[c0 + 2 * plane] = w.v; a.Wout[c0 + 3 * plane] = w.p;
     if (FUSE) {
       // CFL of the updated cell (Euler2DQuadSingleBlock.cc:3019-3080)
       const double v_i = w.u * gp[G_VIX * plane] + w.v * gp[G_VIY * plane];
@@ -501,6 +530,16 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
   };
   if (tid == 0) issue(g0, 0);
 
+  // the L2 prefetch share of this thread (fixed over the chunks): row pf_r
+  // of the chunk, field pf_f (0-3 U, 4 1/A, 5-6 CFL lengths), column pf_c
+  constexpr int PER_ROW = MI / 16;
+  const int pf_r = tid / (11 * PER_ROW), pf_f = (tid % (11 * PER_ROW)) / PER_ROW;
+  const int pf_c = 16 * (tid % PER_ROW);
+  // the global time step of case cs for this explicit step
+  auto step_dt = [&](int cs) {
+    return (MODE == 1 || MODE == 2) && !B.local_dt ? a.hist[4 * ((*a.step) * B.ncase + cs)] : 0.0;
+  };
+
   double dt_next = 1000000.0, n1 = 0.0, n2 = 0.0, nmax = 0.0;  // fused next-step CFL / norms
   int cur_case = -1;  // case the fused contributions belong to
   Chunk pk{};         // chunk whose update is pending (faces done)
@@ -514,24 +553,25 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
       tc::fence_async_smem();  // the other buffer's generic reads come before its overwrite
       issue(gg + 1, buf ^ 1);
     }
+    // per-block facts of the chunk (uniform), loaded ahead of the staging wait
+    const int cs = case_id(B, k.b);
+    const bool on = !B.case_active || B.case_active[cs];  // a finished case of a batch: skipped (uniform)
+    const bool frozen = B.freeze && B.freeze[cs];
+    const unsigned sides = m.bcside[k.b];
     const bool pro = (gg == g0) || (k.c == 0);  // start of a strip: no rows below in the rings
     const int s_lo = pro ? 0 : 2, nrow = k.h + 2 - s_lo;  // reconstruction slots [s_lo, h+2)
     // this chunk's update cells' own inputs into L2 (its update runs one
     // chunk later): every 16th cell of a row per field
     if (MODE != 0 && MODE != 3) {
-      constexpr int PER_ROW = MI / 16;
-      const int r = tid / (11 * PER_ROW), rem = tid % (11 * PER_ROW), f = rem / PER_ROW;
-      const int J = k.j0 + NG + r, I = k.i0 + NG + 16 * (rem % PER_ROW);
-      if (r < k.h && J <= B.ncj + 1 && I <= B.nci + 1) {
-        const double* gq = m.geom + size_t(k.b) * GEOM_NF * plane + size_t(J) * B.NCi + I;
-        if (f < 4) {
-          const size_t q = cell_var(B, k.b, f, J, I);
+      const int J = k.j0 + NG + pf_r, I = k.i0 + NG + pf_c;
+      if (pf_r < k.h && J <= B.ncj + 1 && I <= B.nci + 1) {
+        const size_t off = size_t(J) * B.NCi + I;
+        if (pf_f < 4) {
+          const size_t q = (size_t(k.b) * 4 + pf_f) * plane + off;
           prefetch_l2(a.Ubase + q);
           if (MODE == 2) prefetch_l2(a.res_out + q);
-        } else if (f == 4) {
-          prefetch_l2(gq + G_RA * plane);
-        } else if (FUSE) {
-          prefetch_l2(gq + (G_DI + f - 5) * plane);
+        } else if (pf_f == 4 || FUSE) {
+          prefetch_l2(m.geom + (size_t(k.b) * GEOM_NF + (pf_f == 4 ? G_RA : G_DI + pf_f - 5)) * plane + off);
         }
       }
     }
@@ -549,26 +589,26 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
       }
       return;
     }
-    const int cs = case_id(B, k.b);
-    const bool on = !B.case_active || B.case_active[cs];  // a finished case of a batch: skipped (uniform)
     if (FUSE && pcase >= 0 && pcase != cur_case) {
       if (cur_case >= 0) flush_next(a, s, cur_case, dt_next, n1, n2, nmax);
       cur_case = pcase;
       dt_next = 1000000.0; n1 = 0.0; n2 = 0.0; nmax = 0.0;
     }
     const Tile& T = s.in[buf];
-    const bool frozen = B.freeze && B.freeze[cs];
 
     // ---- reconstruction of chunk gg, update of the pending chunk -------------
     {
+      // the update items start on a warp boundary: no warp runs both kinds
       const int nrec = on ? nrow * RCI : 0, nupd = pcase >= 0 ? pk.h * MI : 0;
-      for (int t = tid; t < nrec + nupd; t += THREADS) {
+      const int nrec_w = (nrec + 31) & ~31;
+      const double dtg = pcase >= 0 ? step_dt(pcase) : 0.0;
+      for (int t = tid; t < nrec_w + nupd; t += THREADS) {
         if (t < nrec) {
           const int sl = s_lo + t / RCI, c = t % RCI;
           recon_cell(m, s, T, k, sl, c, t == tid ? rin : recon_in(m, k, sl, c, plane), frozen);
-        } else {
-          const int u = t - nrec;
-          update_cell<MODE, FUSE>(m, s, pk, pcase, u / MI, u % MI, plane, dt_next, n1, n2, nmax);
+        } else if (t >= nrec_w) {
+          const int u = t - nrec_w;
+          update_cell<MODE, FUSE>(m, s, pk, pcase, u / MI, u % MI, plane, dtg, dt_next, n1, n2, nmax);
         }
       }
     }
@@ -578,9 +618,14 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
     // ---- faces of chunk gg: i-faces (h rows of MI+1), j-faces (slots [sf_lo, h]) ---
     if (on) {
       const int h = k.h, sf_lo = pro ? 0 : 1, ni = h * (MI + 1), nj = (h + 1 - sf_lo) * MI;
-      for (int t = tid; t < ni + nj; t += THREADS) {
-        if (t < ni) iface(m, s, T, k, t / (MI + 1), t % (MI + 1));
-        else jface(m, s, T, k, sf_lo + (t - ni) / MI, (t - ni) % MI);
+      // does the chunk reach a block edge whose boundary condition sets the
+      // face state?  (uniform; most chunks do not, and skip the BC codes)
+      const bool bc = ((sides & 1u) && k.i0 == 0) || ((sides & 2u) && k.i0 + MI >= B.nci) ||
+                      ((sides & 4u) && k.c == 0) || ((sides & 8u) && k.c == m.cps - 1);
+      if (bc) {
+        for (int t = tid; t < ni + nj; t += THREADS) face<true>(m, s, T, k, t, ni, sf_lo);
+      } else {
+        for (int t = tid; t < ni + nj; t += THREADS) face<false>(m, s, T, k, t, ni, sf_lo);
       }
       pk = k;
       pcase = cs;
@@ -598,8 +643,9 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
       cur_case = pcase;
       dt_next = 1000000.0; n1 = 0.0; n2 = 0.0; nmax = 0.0;
     }
+    const double dtg = step_dt(pcase);
     for (int t = tid; t < pk.h * MI; t += THREADS)
-      update_cell<MODE, FUSE>(m, s, pk, pcase, t / MI, t % MI, plane, dt_next, n1, n2, nmax);
+      update_cell<MODE, FUSE>(m, s, pk, pcase, t / MI, t % MI, plane, dtg, dt_next, n1, n2, nmax);
   }
   if (FUSE && cur_case >= 0) flush_next(a, s, cur_case, dt_next, n1, n2, nmax);
 }
@@ -748,6 +794,24 @@ __global__ void geometry_kernel(Blocks B, double* geom, unsigned char* mask, int
   }
 }
 
+// Per block a bit per side (1 W, 2 E, 4 S, 8 N): at least one of the
+// side's edge cells has a boundary condition that sets the face state
+// (reflection, characteristic).  One warp per block.
+__global__ void bc_side_kernel(Blocks B, unsigned char* side) {
+  const int b = blockIdx.x;
+  unsigned m = 0;
+  for (int J = threadIdx.x; J < B.NCj; J += 32) {
+    if (face_bc(B.bcw[size_t(b) * B.NCj + J])) m |= 1u;
+    if (face_bc(B.bce[size_t(b) * B.NCj + J])) m |= 2u;
+  }
+  for (int I = threadIdx.x; I < B.NCi; I += 32) {
+    if (face_bc(B.bcs[size_t(b) * B.NCi + I])) m |= 4u;
+    if (face_bc(B.bcn[size_t(b) * B.NCi + I])) m |= 8u;
+  }
+  m = __reduce_or_sync(0xffffffffu, m);
+  if (threadIdx.x == 0) side[b] = (unsigned char)m;
+}
+
 // Nodes [nblk][NNj][NNi] -> [nblk][2][NNj][NNp] (X, Y; rows padded to NNp).
 __global__ void pad_nodes_kernel(Blocks B, int NNp, double* out) {
   const long long plane = (long long)B.NNi * B.NNj;
@@ -764,11 +828,13 @@ __global__ void pad_nodes_kernel(Blocks B, int NNp, double* out) {
 
 }  // namespace mk
 
-cudaError_t launch_geometry(const Blocks& B, double* geom, unsigned char* mask, int* degenerate, int NNp,
-                            double* nodes_pad, cudaStream_t st) {
+cudaError_t launch_geometry(const Blocks& B, double* geom, unsigned char* mask, unsigned char* bcside, int* degenerate,
+                            int NNp, double* nodes_pad, cudaStream_t st) {
   mk::geometry_kernel<<<1024, 256, 0, st>>>(B, geom, mask, degenerate);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  mk::bc_side_kernel<<<B.nblk, 32, 0, st>>>(B, bcside);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   mk::pad_nodes_kernel<<<1024, 256, 0, st>>>(B, NNp, nodes_pad);
   return cudaGetLastError();
 }

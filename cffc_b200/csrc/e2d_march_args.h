@@ -36,6 +36,7 @@ struct MarchArgs {
   CUtensorMap tmN;   // padded nodes, as [2 nblk][NNj][NNp]
   const double* geom;
   const unsigned char* mask;
+  const unsigned char* bcside;  // per block: sides with face-setting boundary conditions (bits W E S N)
   int strips;        // column strips per block
   int ch;            // rows of a chunk (the last chunk of a strip may hold up to 8)
   int cps;           // chunks per strip

@@ -16,15 +16,26 @@ within ENVELOPE times that envelope, with a floor:
 * per Newton step: L2 norm, ratio, CFL and GMRES resid0, floor 1e-8
   relative (the reference prints 10 significant digits);
 * GMRES inner iterations: equal, up to the first step at which the
-  perturbed reference run's count differs (after it, the counts are
-  round-off-sensitive for the reference itself);
+  perturbed reference run's count differs or its L2 norm has moved by more
+  than CHAOS (after it, the counts are round-off-sensitive for the
+  reference itself: its Newton iterates differ at that level, and whether a
+  linear solve stops at its iteration cap or just below it is not
+  determined by the method);
 * GMRES final relative residual: floor 1e-6 relative and 10x the envelope
   (RELRES_ENVELOPE): it is the end value of a GMRES recurrence that, on the
   later steps, stops at its iteration cap unconverged, and one perturbed run
   underestimates its spread (the device has been seen at up to 17x);
 * converged runs: the same number of Newton steps, and the final L2 within
   the envelope of the whole run;
-* final conserved state: helpers.rel_err, floor 1e-10.
+* final conserved state: helpers.rel_err, floor 1e-10;
+* fast precision (contraction, refined reciprocals): its arithmetic differs
+  from the reference's at every residual evaluation, by up to about 1e-12
+  of the flux scale per cell -- some 100 times the twin's 2^-46 change of the
+  input -- so its L2, ratio, CFL and resid0 are held to FAST_ENVELOPE times
+  the twin's divergence, with a further floor of FAST_FLOOR times the first
+  step's L2 (absolute: near convergence the residual norm itself falls to
+  the order of that difference); its GMRES counts are compared only while
+  that floor is below CHAOS relative.
 """
 import dataclasses
 
@@ -40,6 +51,9 @@ EXACT = 2
 FAST = 0
 ENVELOPE = 10.0
 RELRES_ENVELOPE = 100.0
+CHAOS = 1e-3
+FAST_FLOOR = 1e-11
+FAST_ENVELOPE = 100.0
 NKS_SUB = 4  # subsampling of the final state in the large fixtures (make_golden.py)
 
 
@@ -78,25 +92,30 @@ def test_nks_matches_reference(name, precision):
     assert len(hist) == len(newton) + (1 if converged else 0)
     rows, bad = [], []
     floor = [1e-8, 1e-8, 1e-8, 1e-8, 1e-6]
-    env = [ENVELOPE] * 4 + [RELRES_ENVELOPE]
+    env = [ENVELOPE if precision != FAST else FAST_ENVELOPE] * 4 + [RELRES_ENVELOPE]
     span = [0.0] * 5           # running max of the reference's self-divergence
-    chaotic = False            # the perturbed reference's GMRES count has differed
+    chaotic = False            # the perturbed reference has departed (GMRES count or L2)
+    l2_0 = newton[0, 0]
     for k, st in enumerate(hist[:len(newton)]):
+        fast = FAST_FLOOR * l2_0 / newton[k, 0] if precision == FAST else 0.0
         got = [st["l2"], st["ratio"], st["cfl"], st["gmres_resid0"], st["gmres_relres"]]
         want = [newton[k, 0], newton[k, 1], newton[k, 2], gmres[k, 1], gmres[k, 3]]
         pert = [pn[k, 0], pn[k, 1], pn[k, 2], pg[k, 1], pg[k, 3]]
         span = [max(sp, rel(p, w)) for sp, p, w in zip(span, pert, want)]
         devs = [rel(g, w) for g, w in zip(got, want)]
         lims = [max(f, e * sp) for f, e, sp in zip(floor, env, span)]
+        lims[:4] = [max(x, fast) for x in lims[:4]]
         rows.append((k, st["gmres_iters"] - int(gmres[k, 0])) + tuple(devs))
         bad += [(k, q) for q in range(5) if not devs[q] <= lims[q]]
-        chaotic = chaotic or int(pg[k, 0]) != int(gmres[k, 0])
+        chaotic = chaotic or int(pg[k, 0]) != int(gmres[k, 0]) or span[0] > CHAOS or fast > CHAOS
         if st["gmres_iters"] != int(gmres[k, 0]) and not chaotic:
             bad.append((k, "iters"))
     if converged:
         last = hist[-1]
         assert last["ratio"] <= tol and last["gmres_iters"] == 0
         lim = max(1e-8, ENVELOPE * max(span[0], rel(ref["pert_final"][1], ref["final"][1])))
+        if precision == FAST:
+            lim = max(lim, FAST_ENVELOPE / ENVELOPE * lim, FAST_FLOOR * l2_0 / ref["final"][1])
         if not rel(last["l2"], ref["final"][1]) <= lim:
             bad.append(("final", last["l2"], ref["final"][1], lim))
     if "U_sub" in ref:  # large fixtures keep every NKS_SUB-th interior cell
@@ -108,6 +127,8 @@ def test_nks_matches_reference(name, precision):
     u_lim = max(1e-10, ENVELOPE * rel_err(pert_u, ref_u))
     table = "\n".join("step %d: iters %+d l2 %.1e ratio %.1e cfl %.1e resid0 %.1e relres %.1e" % r for r in rows)
     table += "\nfinal U rel_err %.2e (limit %.2e)" % (u_err, u_lim)
+    if bad:
+        print(table)
     assert not bad, (bad, table)
     assert u_err <= u_lim, table
 
