@@ -13,9 +13,12 @@
 #include "e2d_device.cuh"
 #include "e2d_geom.cuh"
 
+#include <algorithm>
+
 namespace e2d {
 
 constexpr int AUX_THREADS = 256;
+constexpr int GHOST_THREADS = 1024;  // most threads of a ghost-fill CTA
 constexpr double MILLION = 1000000.0;
 
 // One edge-cell of the W or E (vertical) boundary: side 0 = W, 1 = E.
@@ -91,13 +94,25 @@ __device__ void bc_horizontal(const Blocks& B, int b, int i, int side) {
 }
 
 // One CTA per block: exchange, then W/E BCs, then S/N BCs (the reference's
-// order; the S/N pass also fills the corner ghosts).
-__global__ void __launch_bounds__(AUX_THREADS) ghost_fill_kernel(Blocks B) {
+// order; the S/N pass also fills the corner ghosts).  The status word, the
+// 8 neighbours and the block's BC codes are read together up front; a block
+// whose edges all have code BC_NONE (every edge exchanged) stops after the
+// exchange.
+__global__ void __launch_bounds__(GHOST_THREADS) ghost_fill_kernel(Blocks B) {
   const int b = blockIdx.x;
   const int ICl = NG, ICu = B.nci + NG - 1, JCl = NG, JCu = B.ncj + NG - 1;
-  __shared__ int failed;
+  __shared__ int failed, nb[8];
   if (threadIdx.x == 0) failed = *(volatile int*)B.status;
-  __syncthreads();
+  if (threadIdx.x < 8) nb[threadIdx.x] = B.neigh[b * 8 + threadIdx.x];
+  int bc_here = 0;
+  for (int q = threadIdx.x; q < 2 * (B.NCj + B.NCi); q += blockDim.x) {
+    const int code = q < B.NCj           ? B.bcw[size_t(b) * B.NCj + q]
+                     : q < 2 * B.NCj     ? B.bce[size_t(b) * B.NCj + q - B.NCj]
+                     : q < 2 * B.NCj + B.NCi ? B.bcs[size_t(b) * B.NCi + q - 2 * B.NCj]
+                                         : B.bcn[size_t(b) * B.NCi + q - 2 * B.NCj - B.NCi];
+    bc_here |= code != E2D_BC_NONE;
+  }
+  const bool any_bc = __syncthreads_or(bc_here);
   if (failed) return;  // uniform per CTA
   // exchange: edges (2 layers) and corners (2x2) from the 8 neighbours
   const int ne = NG * B.ncj, nn = NG * B.nci, nc = NG * NG;
@@ -107,7 +122,7 @@ __global__ void __launch_bounds__(AUX_THREADS) ghost_fill_kernel(Blocks B) {
     if (r < 2 * ne) { k = r / ne; r %= ne; }
     else if ((r -= 2 * ne) < 2 * nn) { k = 2 + r / nn; r %= nn; }
     else { r -= 2 * nn; k = 4 + r / nc; r %= nc; }
-    const int s = B.neigh[b * 8 + k];
+    const int s = nb[k];
     if (s < 0) continue;
     int i, j, di, dj;
     const bool wi = (k == 0 || k == 4 || k == 6), ei = (k == 1 || k == 5 || k == 7);
@@ -126,6 +141,7 @@ __global__ void __launch_bounds__(AUX_THREADS) ghost_fill_kernel(Blocks B) {
     stU(B, b, i, j, u);
     stW(B, b, i, j, W_of_U(u, B.gm1));
   }
+  if (!any_bc) return;  // uniform: no boundary condition to apply
   __syncthreads();
   const bool s_none_w = B.bcs[size_t(b) * B.NCi + ICl - 1] == E2D_BC_NONE;
   const bool n_none_w = B.bcn[size_t(b) * B.NCi + ICl - 1] == E2D_BC_NONE;
@@ -274,7 +290,11 @@ __global__ void step_end_kernel(double* hist, int* step, int fused, int ncase) {
 }
 
 cudaError_t launch_ghost_fill(const Blocks& B, cudaStream_t st) {
-  ghost_fill_kernel<<<B.nblk, AUX_THREADS, 0, st>>>(B);
+  // one thread per exchanged ghost cell where the block allows (the exchange
+  // is a single round of independent loads), at least one CTA of AUX_THREADS
+  const int cells = 2 * NG * (B.nci + B.ncj) + 4 * NG * NG;
+  const int threads = std::min(GHOST_THREADS, std::max(AUX_THREADS, (cells + 31) / 32 * 32));
+  ghost_fill_kernel<<<B.nblk, threads, 0, st>>>(B);
   return cudaGetLastError();
 }
 

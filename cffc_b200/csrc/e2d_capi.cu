@@ -160,6 +160,17 @@ cudaError_t launch_stage_args(e2d_handle* h, StageArgs& a) {
       m.geom = h->geom;
       m.mask = h->gmask;
       m.bcside = h->bcside;
+      // update inputs by TMA: explicit stages over U or U2 whose second
+      // stage adds to dUdt (RK4's slot combination reads global memory)
+      const bool ubase = a.Ubase == h->B.U || a.Ubase == h->B.U2;
+      if (h->upd_ok && (a.mode == 1 || a.mode == 2) && !a.no_update && ubase &&
+          (a.mode == 1 || (a.res_out == h->B.dUdt && !a.acc1))) {
+        m.upd = 1;
+        m.tmU = a.Ubase == h->B.U ? h->tmU[0] : h->tmU[1];
+        m.tmR = h->tmR;
+        m.tmGA = h->tmGA;
+        m.tmGF = h->tmGF;
+      }
       const int mi = fast::march_strip_cols();
       m.strips = (h->B.nci + mi - 1) / mi;
       m.ch = h->march_rows;
@@ -244,6 +255,14 @@ int setup_march(e2d_handle* h) {
             encode3(&h->tmN, h->nodes_pad, NNp, B.NNj, 2ull * B.nblk, nwi, wj, 2);
   if (ok && h->W3) ok = encode3(&h->tmW[2], h->W3, B.NCi, B.NCj, 4ull * B.nblk, wi, wj, 4);
   if (!ok) return 0;
+  // update inputs of the explicit stages: boxes of the strip's columns x the
+  // most rows of a chunk
+  const uint32_t mj = fast::march_max_rows();
+  h->upd_ok = encode3(&h->tmU[0], B.U, B.NCi, B.NCj, 4ull * B.nblk, mi, mj, 4) &&
+              encode3(&h->tmU[1], B.U2, B.NCi, B.NCj, 4ull * B.nblk, mi, mj, 4) &&
+              encode3(&h->tmR, B.dUdt, B.NCi, B.NCj, 4ull * B.nblk, mi, mj, 4) &&
+              encode3(&h->tmGA, h->geom, B.NCi, B.NCj, uint64_t(GEOM_NF) * B.nblk, mi, mj, 1) &&
+              encode3(&h->tmGF, h->geom, B.NCi, B.NCj, uint64_t(GEOM_NF) * B.nblk, mi, mj, GEOM_NF - G_RA);
   const int per_sm = std::min(f32::march_ctas_per_sm(), fast::march_ctas_per_sm());
   int sms = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));

@@ -8,6 +8,8 @@
 // on the 1M-cell set: stage 2 at 192 against 205 us with two buffers; the
 // FP32 path, with half the register footprint per value, keeps two)
 #define E2D_MARCH_NBUF 1
+// the explicit stages' update inputs staged by TMA (fits beside one buffer)
+#define E2D_MARCH_UPD 1
 #include "e2d_stage.cuh"
 #include "e2d_march.cuh"
 

@@ -41,6 +41,8 @@ struct e2d_handle {
   double* geom = nullptr;
   unsigned char* gmask = nullptr;
   unsigned char* bcside = nullptr;  // per block: sides with face-setting BCs (marching kernel)
+  CUtensorMap tmU[2], tmR, tmGA, tmGF;  // marching kernel update inputs: U and U2, dUdt, geometry
+  bool upd_ok = false;
   double* nodes_pad = nullptr;
   CUtensorMap tmW[3], tmG, tmN;
   int march_grid = 0;

@@ -64,6 +64,14 @@ constexpr int MIN_CTAS = E2D_MARCH_MINCTAS;
 constexpr int MIN_CTAS = 65536 / (128 * THREADS);                     // CTAs per SM at 128 registers
 #endif
 constexpr int NBUF = E2D_MARCH_NBUF;  // staging buffers: 2 = the next chunk's copies overlap this chunk
+#ifndef E2D_MARCH_UPD
+#define E2D_MARCH_UPD 0
+#endif
+// E2D_MARCH_UPD 1: the explicit stages' update inputs of a chunk (base state,
+// stage-1 residual, 1/A and the CFL geometry) arrive in shared memory by TMA
+// while the chunk's faces are evaluated, instead of as global loads in the
+// update (whose latency every warp meets at once after the phase barrier)
+constexpr bool UPD = E2D_MARCH_UPD;
 constexpr uint32_t WAIT_ITERS = 1u << 24;          // bounded mbarrier wait (about a second)
 constexpr int ST_TIMEOUT = 2;                      // status code: a staging wait ran out
 
@@ -85,13 +93,27 @@ static_assert(MI % 2 == 0 && (MI * 8) % 16 == 0, "strip origins on 16-byte bound
 constexpr int RR = 12;
 static_assert(RR >= RCJ + 2, "ring holds a chunk's rows and the next chunk's first");
 
+// Update inputs of a chunk's cells (rows j0+2 .., columns i0+2 ..): the base
+// conserved state, the residual RK stage 2 adds to, and geometry planes
+// G_RA .. G_VJY (1/A alone without the fused CFL step).
+struct UpdIn {
+  double U[4][MJ][MI];
+  double R[4][MJ][MI];
+  double G[GEOM_NF - G_RA][MJ][MI];
+};
+static_assert(sizeof(double) * 4 * MJ * MI % 128 == 0, "update buffers 128-byte aligned");
+
 struct Smem {
   Tile in[NBUF];
+#if E2D_MARCH_UPD
+  UpdIn up;
+#endif
   RT px[RR][4][RCI], py[RR][4][RCI];    // phi * gradient of the reconstructed cells
   double Fi[MJ][4][MI + 1];             // i-face flux x length, faces I-1/2, I = i0+2 .. i0+34
   double Fj[RR][4][MI];                 // j-face flux x length, face row J (face J-1/2)
   double red[4][NWARP];
   uint64_t full[2];
+  uint64_t fullu;  // the update inputs
   int failed;
 };
 
@@ -394,10 +416,11 @@ __device__ __forceinline__ bool not_positive(const CState<double>& u) {
 
 // dtg: the case's global time step of this explicit step (modes 1, 2 with
 // global time stepping).
+// up: the chunk's update inputs in shared memory (null: global loads).
 template <int MODE, bool FUSE>
 __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, const Chunk& k, int cs, int r, int q,
-                                            size_t plane, double dtg, double& dt_next, double& n1, double& n2,
-                                            double& nmax) {
+                                            size_t plane, double dtg, const UpdIn* up, double& dt_next, double& n1,
+                                            double& n2, double& nmax) {
   const StageArgs& a = m.a;
   const Blocks& B = a.B;
   const int I = k.i0 + NG + q, J = k.j0 + NG + r;
@@ -409,7 +432,7 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
   const size_t c = size_t(k.b) * plane + off;
   const size_t c0 = size_t(k.b) * 4 * plane + off;
   const double* gp = m.geom + size_t(k.b) * GEOM_NF * plane + off;
-  const double rA = gp[G_RA * plane];
+  const double rA = up ? up->G[0][r][q] : gp[G_RA * plane];
   double kk = 1.0;
   if (MODE == 1 || MODE == 2) kk = B.cfl * (B.local_dt ? B.dt[c] : dtg);
   const double kA = kk * rA;
@@ -420,7 +443,7 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
     double d = 0.0;
     if (MODE == 2) {
       const size_t qv = c0 + v * plane;
-      d = a.res_out[qv];
+      d = up ? up->R[v][r][q] : a.res_out[qv];
       if (a.acc1) d = d + 2.0 * a.acc1[qv] + 2.0 * a.acc2[qv];
     }
     d += s.Fi[r][v][q] * kA;
@@ -450,8 +473,12 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
   } else {
     // Update_Solution_Multistage_Explicit: U = Uo + omega*dUdt
     CState<double> uo;
-    uo.d = a.Ubase[c0]; uo.mx = a.Ubase[c0 + plane];
-    uo.my = a.Ubase[c0 + 2 * plane]; uo.E = a.Ubase[c0 + 3 * plane];
+    if (up) {
+      uo.d = up->U[0][r][q]; uo.mx = up->U[1][r][q]; uo.my = up->U[2][r][q]; uo.E = up->U[3][r][q];
+    } else {
+      uo.d = a.Ubase[c0]; uo.mx = a.Ubase[c0 + plane];
+      uo.my = a.Ubase[c0 + 2 * plane]; uo.E = a.Ubase[c0 + 3 * plane];
+    }
     const double omega = a.omega;
     CState<double> u;
     u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
@@ -476,17 +503,22 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
     }
 #pragma unroll
     for (int v = 0; v < 4; ++v) a.res_out[c0 + v * plane] = res[v];
-    const PState<double> w = fm::W_of_U(u, gm1);
+    // W(U) (fm::W_of_U) with its reciprocal density kept for the CFL step
+    const double rd = fm::rcp(u.d);
+    PState<double> w;
+    w.d = u.d; w.u = u.mx * rd; w.v = u.my * rd;
+    w.p = gm1 * (u.E - 0.5 * (u.mx * u.mx + u.my * u.my) * rd);
     a.Uout[c0] = u.d; a.Uout[c0 + plane] = u.mx; a.Uout[c0 + 2 * plane] = u.my; a.Uout[c0 + 3 * plane] = u.E;
     a.Wout[c0] = w.d; a.Wout[c0 + plane] = w.u; a.Wout[c0 + 2 * plane] = w.v; a.Wout[c0 + 3 * plane] = w.p;
     if (FUSE) {
       // CFL of the updated cell (Euler2DQuadSingleBlock.cc:3019-3080)
-      const double v_i = w.u * gp[G_VIX * plane] + w.v * gp[G_VIY * plane];
-      const double v_j = w.u * gp[G_VJX * plane] + w.v * gp[G_VJY * plane];
-      const double c2 = g * w.p * fm::rcp(w.d);
+      auto geo = [&](int f) { return up ? up->G[f - G_RA][r][q] : gp[f * plane]; };
+      const double v_i = w.u * geo(G_VIX) + w.v * geo(G_VIY);
+      const double v_j = w.u * geo(G_VJX) + w.v * geo(G_VJY);
+      const double c2 = g * w.p * rd;
       const double snd = fm::sqrt_from_rsqrt(c2, fm::rsqrt(c2));
-      const double ti = gp[G_DI * plane] * fm::rcp(snd + fabs(v_i));
-      const double tj = gp[G_DJ * plane] * fm::rcp(snd + fabs(v_j));
+      const double ti = geo(G_DI) * fm::rcp(snd + fabs(v_i));
+      const double tj = geo(G_DJ) * fm::rcp(snd + fabs(v_j));
       const double dtc = dmin(ti, tj);
       if (B.local_dt) B.dt[c] = dtc;
       dt_next = dmin(dt_next, dtc);
@@ -515,6 +547,7 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
     s.failed = *(volatile int*)B.status;
     tc::mbar_init(&s.full[0], 1);
     tc::mbar_init(&s.full[1], 1);
+    tc::mbar_init(&s.fullu, 1);
   }
   __syncthreads();
   if (s.failed || g0 >= g1) return;  // an earlier kernel failed: stop marching (uniform)
@@ -529,6 +562,24 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
     tma3(&s.in[buf].N[0][0][0], &m.tmN, bar, k.i0, k.j0, 2 * k.b);
   };
   if (tid == 0) issue(g0, 0);
+  // update inputs by TMA (explicit stages whose arrays have tensor maps)
+  const bool upd = UPD && (MODE == 1 || MODE == 2) && m.upd;
+#if E2D_MARCH_UPD
+  const UpdIn* upp = upd ? &s.up : nullptr;
+#else
+  const UpdIn* upp = nullptr;
+#endif
+  auto issue_upd = [&](const Chunk& k) {
+#if E2D_MARCH_UPD
+    constexpr uint32_t PLANE_BYTES = sizeof(double) * MJ * MI;
+    const uint32_t bytes = PLANE_BYTES * (4 + (MODE == 2 ? 4 : 0) + (FUSE ? GEOM_NF - G_RA : 1));
+    expect_tx(&s.fullu, bytes);
+    tma3(&s.up.U[0][0][0], &m.tmU, &s.fullu, k.i0 + NG, k.j0 + NG, 4 * k.b);
+    if (MODE == 2) tma3(&s.up.R[0][0][0], &m.tmR, &s.fullu, k.i0 + NG, k.j0 + NG, 4 * k.b);
+    tma3(&s.up.G[0][0][0], FUSE ? &m.tmGF : &m.tmGA, &s.fullu, k.i0 + NG, k.j0 + NG, GEOM_NF * k.b + G_RA);
+#endif
+  };
+  int upd_issued = 0, upd_waited = 0;  // update-input copies issued / consumed
 
   // the L2 prefetch share of this thread (fixed over the chunks): row pf_r
   // of the chunk, field pf_f (0-3 U, 4 1/A, 5-6 CFL lengths), column pf_c
@@ -562,7 +613,7 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
     const int s_lo = pro ? 0 : 2, nrow = k.h + 2 - s_lo;  // reconstruction slots [s_lo, h+2)
     // this chunk's update cells' own inputs into L2 (its update runs one
     // chunk later): every 16th cell of a row per field
-    if (MODE != 0 && MODE != 3) {
+    if (MODE != 0 && MODE != 3 && !upd) {
       const int J = k.j0 + NG + pf_r, I = k.i0 + NG + pf_c;
       if (pf_r < k.h && J <= B.ncj + 1 && I <= B.nci + 1) {
         const size_t off = size_t(J) * B.NCi + I;
@@ -578,7 +629,8 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
     // this thread's first reconstruction cell: its inputs, ahead of the wait
     ReconIn rin{0u, 0.0, 0.0, 0.0};
     if (tid < nrow * RCI) rin = recon_in(m, k, s_lo + tid / RCI, tid % RCI, plane);
-    const bool ok = tc::mbar_wait(&s.full[buf], par, WAIT_ITERS);
+    bool ok = tc::mbar_wait(&s.full[buf], par, WAIT_ITERS);
+    if (upd && pcase >= 0) ok = tc::mbar_wait(&s.fullu, uint32_t(upd_waited) & 1u, WAIT_ITERS) && ok;
     if (__syncthreads_or(!ok)) {
       // a staging copy did not complete in time: record it, let the copies
       // in flight land (bounded), and stop
@@ -586,9 +638,11 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
         set_status(B.status, ST_TIMEOUT, int(gg));
         tc::mbar_wait(&s.full[buf], par, WAIT_ITERS);
         if (NBUF == 2 && gg + 1 < g1) tc::mbar_wait(&s.full[buf ^ 1], uint32_t((it + 1) >> 1) & 1u, WAIT_ITERS);
+        if (upd_issued > upd_waited) tc::mbar_wait(&s.fullu, uint32_t(upd_waited) & 1u, WAIT_ITERS);
       }
       return;
     }
+    if (upd && pcase >= 0) ++upd_waited;
     if (FUSE && pcase >= 0 && pcase != cur_case) {
       if (cur_case >= 0) flush_next(a, s, cur_case, dt_next, n1, n2, nmax);
       cur_case = pcase;
@@ -608,12 +662,19 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
           recon_cell(m, s, T, k, sl, c, t == tid ? rin : recon_in(m, k, sl, c, plane), frozen);
         } else if (t >= nrec_w) {
           const int u = t - nrec_w;
-          update_cell<MODE, FUSE>(m, s, pk, pcase, u / MI, u % MI, plane, dtg, dt_next, n1, n2, nmax);
+          update_cell<MODE, FUSE>(m, s, pk, pcase, u / MI, u % MI, plane, dtg, upp, dt_next, n1, n2, nmax);
         }
       }
     }
     __syncthreads();
     pcase = -1;
+    // this chunk's update inputs, now that the pending update has read the
+    // buffer; they land while the faces are evaluated
+    if (upd && on && tid == 0) {
+      tc::fence_async_smem();
+      issue_upd(k);
+    }
+    if (upd && on) ++upd_issued;
 
     // ---- faces of chunk gg: i-faces (h rows of MI+1), j-faces (slots [sf_lo, h]) ---
     if (on) {
@@ -643,9 +704,20 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
       cur_case = pcase;
       dt_next = 1000000.0; n1 = 0.0; n2 = 0.0; nmax = 0.0;
     }
+    if (upd) {
+      const bool ok = tc::mbar_wait(&s.fullu, uint32_t(upd_waited) & 1u, WAIT_ITERS);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          set_status(B.status, ST_TIMEOUT, int(g1));
+          tc::mbar_wait(&s.fullu, uint32_t(upd_waited) & 1u, WAIT_ITERS);
+        }
+        return;
+      }
+      ++upd_waited;
+    }
     const double dtg = step_dt(pcase);
     for (int t = tid; t < pk.h * MI; t += THREADS)
-      update_cell<MODE, FUSE>(m, s, pk, pcase, t / MI, t % MI, plane, dtg, dt_next, n1, n2, nmax);
+      update_cell<MODE, FUSE>(m, s, pk, pcase, t / MI, t % MI, plane, dtg, upp, dt_next, n1, n2, nmax);
   }
   if (FUSE && cur_case >= 0) flush_next(a, s, cur_case, dt_next, n1, n2, nmax);
 }

@@ -34,6 +34,12 @@ struct MarchArgs {
   CUtensorMap tmW;   // the stage's input primitive state, as [4 nblk][NCj][NCi]
   CUtensorMap tmG;   // the geometry, as [GEOM_NF nblk][NCj][NCi]
   CUtensorMap tmN;   // padded nodes, as [2 nblk][NNj][NNp]
+  // update inputs of the explicit stages (builds with E2D_MARCH_UPD), boxes
+  // of 32 columns x 8 rows: the base conserved state and the residual of
+  // RK stage 1 as [4 nblk][NCj][NCi], geometry plane G_RA alone and planes
+  // G_RA .. G_VJY, as [GEOM_NF nblk][NCj][NCi]
+  CUtensorMap tmU, tmR, tmGA, tmGF;
+  int upd;           // 1: the update inputs of this launch arrive through these maps
   const double* geom;
   const unsigned char* mask;
   const unsigned char* bcside;  // per block: sides with face-setting boundary conditions (bits W E S N)
