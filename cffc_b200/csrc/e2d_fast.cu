@@ -3,12 +3,11 @@
 // algebra of e2d_fastmath.cuh; within 1e-12 of the reference (see tests).
 #define E2D_NS fast
 #define E2D_FAST 1
-// one staging buffer for the marching kernel: the shared memory it frees
-// goes to L1, which holds the second RK stage's extra global inputs (measured
-// on the 1M-cell set: stage 2 at 192 against 205 us with two buffers; the
-// FP32 path, with half the register footprint per value, keeps two)
+// one staging buffer for the marching kernel (measured on the 1M-cell set:
+// stage 2 at 192 against 205 us with two, the freed shared memory serving
+// L1), and the explicit stages' update inputs staged by TMA in the space it
+// leaves (152 / 177 against 163 / 191 us)
 #define E2D_MARCH_NBUF 1
-// the explicit stages' update inputs staged by TMA (fits beside one buffer)
 #define E2D_MARCH_UPD 1
 #include "e2d_stage.cuh"
 #include "e2d_march.cuh"

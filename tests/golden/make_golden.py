@@ -379,12 +379,44 @@ def make_restart_fixture():
     print("restart.tar.gz")
 
 
+BIG_SUB = 8  # the 1M-cell residual digest keeps dUdt on every 8th interior cell in i and j
+
+
+def block_digests(bs, dUdt):
+    """SHA-256 of each block's interior dUdt bytes ([nblk][32] uint8)."""
+    import hashlib
+    inner = np.ascontiguousarray(bs.interior(dUdt))
+    return np.array([np.frombuffer(hashlib.sha256(inner[b].tobytes()).digest(), np.uint8)
+                     for b in range(bs.nblk)])
+
+
+def make_big_residual():
+    """The reference's residual of the full 1,048,576-cell curvilinear Mach-2
+    block set (cases.curvilinear_mach2()), kept as digests: SHA-256 of each
+    block's interior dUdt (a bit-exact comparison without storing 34 MB),
+    dUdt on every BIG_SUB-th interior cell, and SHA-256 of the inputs the
+    reference saw (W and the nodes), so a test can check that it rebuilt the
+    same case."""
+    import hashlib
+    bs = cases.curvilinear_mach2()
+    res = run_residual(bs)
+    inputs = hashlib.sha256(np.ascontiguousarray(bs.W).tobytes() + np.ascontiguousarray(bs.node_x).tobytes() +
+                            np.ascontiguousarray(bs.node_y).tobytes()).digest()
+    np.savez_compressed(os.path.join(OUT, "digest_residual_curv_256x64.npz"),
+                        dUdt_block_sha256=block_digests(bs, res["dUdt"]),
+                        dUdt_sub=np.ascontiguousarray(bs.interior(res["dUdt"])[..., ::BIG_SUB, ::BIG_SUB]),
+                        inputs_sha256=np.frombuffer(inputs, np.uint8), sub=np.int32(BIG_SUB))
+    print("digest_residual_curv_256x64", bs.nblk, "blocks")
+
+
 def main():
     if not os.path.exists(HARNESS):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "reference"], check=True)
     only = set(sys.argv[1:])
     if not only or "restart" in only:
         make_restart_fixture()
+    if not only or "digest_residual_curv_256x64" in only:
+        make_big_residual()
     for name, bs, kind, steps in golden_cases():
         if only and name not in only:
             continue

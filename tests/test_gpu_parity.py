@@ -194,3 +194,36 @@ def test_curvilinear_full_size_steps_match_oracle(prec):
     else:
         err = rel_err(bs.interior(Ug), bs.interior(Uo))
         assert err <= 1e-12, err
+
+
+def test_full_size_residual_against_reference_digest():
+    """The full 1,048,576-cell bench set (cases.curvilinear_mach2()) against
+    the compiled reference's own residual, kept as digests
+    (tests/golden/digest_residual_curv_256x64.npz): the exact path's interior
+    dUdt must hash to the reference's per block (bit-identical), and the fast
+    path must meet the per-value bound of the fast residual on the stored
+    subsample (every 8th interior cell in i and j)."""
+    import hashlib
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "digest_residual_curv_256x64.npz"))
+    bs = cases.curvilinear_mach2()
+    inputs = hashlib.sha256(np.ascontiguousarray(bs.W).tobytes() + np.ascontiguousarray(bs.node_x).tobytes() +
+                            np.ascontiguousarray(bs.node_y).tobytes()).digest()
+    assert inputs == z["inputs_sha256"].tobytes(), "the case differs from the one the reference saw"
+    sub = int(z["sub"])
+    h = capi.Handle(with_precision(bs, EXACT))
+    h.set_state()
+    inner = np.ascontiguousarray(bs.interior(h.residual()))
+    h.close()
+    got = np.array([np.frombuffer(hashlib.sha256(inner[b].tobytes()).digest(), np.uint8) for b in range(bs.nblk)])
+    bad = [b for b in range(bs.nblk) if not np.array_equal(got[b], z["dUdt_block_sha256"][b])]
+    assert not bad, f"{len(bad)} blocks differ from the reference, first {bad[:5]}"
+    assert np.array_equal(inner[..., ::sub, ::sub], z["dUdt_sub"])
+    h = capi.Handle(with_precision(bs, FAST))
+    h.set_state()
+    fast = bs.interior(h.residual())[..., ::sub, ::sub]
+    h.close()
+    rel, amp = per_value_relative(fast, z["dUdt_sub"])
+    print(f"1M-cell fast residual on {rel.size} values: median {np.median(rel):.2e}, max {rel.max():.2e}")
+    assert np.median(rel) <= 1e-12
+    assert np.all(rel <= rtol_fast(bs) * (1.0 + amp))
