@@ -108,6 +108,40 @@ __global__ void __launch_bounds__(VT) blk_dot_kernel(const double* __restrict__ 
   partial_done(s, partial, blockIdx.x, B, c, ch, counter, out, fin, eps0);
 }
 
+// One modified Gram-Schmidt update fused with the next reduction: y -=
+// coef[case] * x (the axpy of axpy_kernel, element for element), then
+// out[case] = f(sum of y * b) with b the next Krylov vector, or y itself
+// when b is null (the norm that closes the step) -- the same products in
+// the same order as blk_dot_kernel over the updated y, so the results are
+// those of the separate axpy and dot kernels, with one pass over y instead
+// of two.  Grid as blk_dot_kernel.
+__global__ void __launch_bounds__(VT) axpy_dot_kernel(double* __restrict__ y, const double* __restrict__ x,
+                                                      const double* coef, const double* bv, int nper2, int ch,
+                                                      double* partial, unsigned* counter, double* out, int fin,
+                                                      Blocks B) {
+  const int blk = blockIdx.x / ch, part = blockIdx.x % ch;
+  const int c = case_id(B, blk);
+  if (!case_on(B, c)) return;  // uniform per CTA
+  const int len = (nper2 + ch - 1) / ch, q0 = part * len, q1 = min(nper2, q0 + len);
+  double2* y2 = reinterpret_cast<double2*>(y) + size_t(blk) * nper2;
+  const double2* x2 = reinterpret_cast<const double2*>(x) + size_t(blk) * nper2;
+  const double2* b2 = bv ? reinterpret_cast<const double2*>(bv) + size_t(blk) * nper2 : nullptr;
+  const double alpha = -1.0 * coef[c];
+  double s = 0.0;
+  for (int q = q0 + threadIdx.x; q < q1; q += VT) {
+    double2 v = y2[q];
+    const double2 u = x2[q];
+    v.x = v.x + alpha * u.x;
+    v.y = v.y + alpha * u.y;
+    y2[q] = v;
+    const double2 w = b2 ? b2[q] : v;
+    s += v.x * w.x;
+    s += v.y * w.y;
+  }
+  s = cta_sum(s);
+  partial_done(s, partial, blockIdx.x, B, c, ch, counter, out, fin, 0.0);
+}
+
 // y += alpha * x, alpha = sign * coef[case] (device, per case) or alpha_h.
 __global__ void __launch_bounds__(VT) axpy_kernel(double* __restrict__ y, const double* __restrict__ x, long long n2,
                                                   int nper2, const double* coef, double sign, double alpha_h, Blocks B) {
@@ -986,6 +1020,15 @@ int dot(e2d_handle* h, const double* a, const double* b, double* out, int fin, d
   return 0;
 }
 
+// y -= coef[case] * x, then out[case] = f(dot(y, b)) (b null: dot(y, y)).
+int axpy_dot(e2d_handle* h, double* y, const double* x, const double* coef, const double* b, double* out, int fin) {
+  e2d_nks_state* s = h->nks;
+  axpy_dot_kernel<<<h->B.nblk * s->ch_vec, VT, 0, h->stream>>>(y, x, coef, b, s->nper4 / 2, s->ch_vec, s->partial,
+                                                               s->counter, out, fin, act(h));
+  E2D_CK(cudaGetLastError());
+  return 0;
+}
+
 int axpy(e2d_handle* h, double* y, const double* x, const double* coef, double sign, double alpha) {
   e2d_nks_state* s = h->nks;
   axpy_kernel<<<VGRID, VT, 0, h->stream>>>(y, x, s->n / 2, s->nper4 / 2, coef, sign, alpha, act(h));
@@ -1039,14 +1082,17 @@ int arnoldi_step(e2d_handle* h, int j, double eps0, const Norm4& nm, bool ilu) {
     E2D_CK(cudaGetLastError());
   }
   if ((rc = matvec(h, Zj, Vn, nm))) return rc;
-  // modified Gram-Schmidt (GMRES2D.h:1224-1240)
-  for (int k = 0; k <= j; ++k) {
-    double* hk = s->hcol + size_t(k) * C;
-    if ((rc = dot(h, Vn, s->V + size_t(k) * n, hk, FIN_SUM))) return rc;
-    if ((rc = axpy(h, Vn, s->V + size_t(k) * n, hk, -1.0, 0.0))) return rc;
-  }
+  // modified Gram-Schmidt (GMRES2D.h:1224-1240): h_k = (w, v_k), w -= h_k
+  // v_k for k = 0..j, then ||w||; each update runs fused with the next dot
   double* hn = s->hcol + size_t(j + 1) * C;
-  if ((rc = dot(h, Vn, Vn, hn, FIN_SQRT))) return rc;
+  if ((rc = dot(h, Vn, s->V, s->hcol, FIN_SUM))) return rc;
+  for (int k = 0; k <= j; ++k) {
+    const double* hk = s->hcol + size_t(k) * C;
+    const bool last = k == j;
+    if ((rc = axpy_dot(h, Vn, s->V + size_t(k) * n, hk, last ? nullptr : s->V + size_t(k + 1) * n,
+                       last ? hn : s->hcol + size_t(k + 1) * C, last ? FIN_SQRT : FIN_SUM)))
+      return rc;
+  }
   if ((rc = scale(h, Vn, hn, 1.0))) return rc;
   gmres_givens_kernel<<<1, VT, 0, h->stream>>>(s->gd, s->hcol, s->active, j);
   E2D_CK(cudaGetLastError());
