@@ -626,12 +626,24 @@ __global__ void gmres_givens_kernel(GmresDev G, const double* hcol, int* active,
   for (int c = threadIdx.x; c < C; c += blockDim.x) {
     if (!active[c]) continue;
     double* Hj = G.H + (size_t(c) * m + j) * (m + 1);
-    for (int k = 0; k <= j + 1; ++k) Hj[k] = hcol[size_t(k) * C + c];
-    if (!isfinite(Hj[j + 1])) gm_error(G, E2D_ERR_NAN);
     double* cs = G.cs + size_t(c) * m;
     double* sn = G.sn + size_t(c) * m;
     double* sv = G.sv + size_t(c) * (m + 1);
-    for (int k = 0; k < j; ++k) apply_rot(Hj[k], Hj[k + 1], cs[k], sn[k]);
+    // the previous rotations, entry k with entry k+1 in order; the entry
+    // being rotated is carried in a register and the column, cosines and
+    // sines (read-only here) are loaded independently of that chain
+    double a = __ldg(hcol + c);
+#pragma unroll 4
+    for (int k = 0; k < j; ++k) {
+      double b = __ldg(hcol + size_t(k + 1) * C + c);
+      apply_rot(a, b, __ldg(cs + k), __ldg(sn + k));
+      Hj[k] = a;
+      a = b;
+    }
+    const double hlast = __ldg(hcol + size_t(j + 1) * C + c);
+    if (!isfinite(hlast)) gm_error(G, E2D_ERR_NAN);
+    Hj[j] = a;
+    Hj[j + 1] = hlast;
     // generate_rotation (GMRES2D.h:761-775)
     const double dx = Hj[j], dy = Hj[j + 1];
     double cj, sj;
