@@ -706,6 +706,9 @@ def main():
     rc = h.lib.e2d_kernel_times(h.h, 20, capi.ptr(kt))
     assert rc == 0, rc
     hbm, peak_kind = peaks()
+    kind, rows, _ = h.stage_config()
+    stage_name = (f"march_kernel (column-marching LSQ+limiter+Roe+update, {rows} rows per chunk)" if kind == 1
+                  else "stage_kernel (tiled LSQ+limiter+Roe+update)")
     stage_ms = 0.5 * (kt[1] + kt[2])
     stage_bytes = bs.n_interior * 0.5 * (80 + 112)  # per launch, mean of the two stages
     achieved = stage_bytes / (stage_ms * 1e-3) / 1e9
@@ -754,7 +757,7 @@ def main():
             "config": config(bs, world, args),
             "e2e": {"value": round(e2e, 3), "unit": "Mcell-updates/s",
                     "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
-            "roofline": {"bound": "hbm", "kernel": "stage_kernel (fused LSQ+limiter+Roe+update)",
+            "roofline": {"bound": "hbm", "kernel": stage_name,
                          "achieved": round(achieved, 2), "peak": hbm, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": traffic,
                          "algorithmic_bytes_per_launch": stage_bytes,

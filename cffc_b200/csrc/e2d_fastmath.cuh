@@ -179,20 +179,20 @@ __device__ __forceinline__ T limiter(int kind, const T* uq, T u0, T umin, T umax
 // The same limiter from the face-point differences dq[q] = u_q - u0 and the
 // neighbour extremes as differences dmax = u_max - u0 >= 0, dmin = u_min - u0
 // <= 0 (the marching kernel forms dq directly from the gradient, without
-// the round trip through u_q).
+// the round trip through u_q).  Among the points that rise (dq > TOLER) the
+// smallest ratio dmax / dq is at the largest rise, among those that fall
+// (dq < -TOLER) the smallest dmin / dq at the largest fall, so the smallest
+// ratio over all points is the smaller of those two: two extremes of the
+// four differences and one comparison instead of a test per point.
 template <class T>
 __device__ __forceinline__ T limiter_diff(int kind, const T* dq, T dmin, T dmax) {
   if (kind == E2D_LIMITER_ONE) return T(1);
   if (kind == E2D_LIMITER_ZERO) return T(0);
-  T A = T(1), Bm = T(0);
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const T ab = fabs(dq[q]);
-    if (ab > T(TOLER)) {
-      const T a = fabs(dq[q] > T(0) ? dmax : dmin);
-      if (a * Bm < A * ab) { A = a; Bm = ab; }
-    }
-  }
+  const T rise = e2d::dmax(e2d::dmax(dq[0], dq[1]), e2d::dmax(dq[2], dq[3]));
+  const T fall = e2d::dmin(e2d::dmin(dq[0], dq[1]), e2d::dmin(dq[2], dq[3]));
+  T A = T(1), Bm = T(0);  // smallest ratio A / Bm; 1/0 stands for "none"
+  if (rise > T(TOLER)) { A = dmax; Bm = rise; }
+  if (fall < -T(TOLER) && -dmin * Bm < A * -fall) { A = -dmin; Bm = -fall; }
   if (kind == E2D_LIMITER_VENKATAKRISHNAN) {
     const T n = A * A + T(2) * A * Bm;
     const T d = A * A + A * Bm + T(2) * Bm * Bm;
