@@ -184,21 +184,30 @@ __device__ __forceinline__ T limiter(int kind, const T* uq, T u0, T umin, T umax
 // (dq < -TOLER) the smallest dmin / dq at the largest fall, so the smallest
 // ratio over all points is the smaller of those two: two extremes of the
 // four differences and one comparison instead of a test per point.
-template <class T>
-__device__ __forceinline__ T limiter_diff(int kind, const T* dq, T dmin, T dmax) {
-  if (kind == E2D_LIMITER_ONE) return T(1);
-  if (kind == E2D_LIMITER_ZERO) return T(0);
+template <int KIND, class T>
+__device__ __forceinline__ T limiter_diff_k(const T* dq, T dmin, T dmax) {
+  if (KIND == E2D_LIMITER_ONE) return T(1);
+  if (KIND == E2D_LIMITER_ZERO) return T(0);
   const T rise = e2d::dmax(e2d::dmax(dq[0], dq[1]), e2d::dmax(dq[2], dq[3]));
   const T fall = e2d::dmin(e2d::dmin(dq[0], dq[1]), e2d::dmin(dq[2], dq[3]));
   T A = T(1), Bm = T(0);  // smallest ratio A / Bm; 1/0 stands for "none"
   if (rise > T(TOLER)) { A = dmax; Bm = rise; }
   if (fall < -T(TOLER) && -dmin * Bm < A * -fall) { A = -dmin; Bm = -fall; }
-  if (kind == E2D_LIMITER_VENKATAKRISHNAN) {
+  if (KIND == E2D_LIMITER_VENKATAKRISHNAN) {
     const T n = A * A + T(2) * A * Bm;
     const T d = A * A + A * Bm + T(2) * Bm * Bm;
     return n < d ? n * rcp_t(d) : T(1);
   }
   return A < Bm ? A * rcp_t(Bm) : T(1);
+}
+template <class T>
+__device__ __forceinline__ T limiter_diff(int kind, const T* dq, T dmin, T dmax) {
+  switch (kind) {
+    case E2D_LIMITER_ONE: return T(1);
+    case E2D_LIMITER_ZERO: return T(0);
+    case E2D_LIMITER_VENKATAKRISHNAN: return limiter_diff_k<E2D_LIMITER_VENKATAKRISHNAN>(dq, dmin, dmax);
+    default: return limiter_diff_k<E2D_LIMITER_BARTH_JESPERSEN>(dq, dmin, dmax);
+  }
 }
 
 // quadCentroid with the reference-rounded moments and one reciprocal.

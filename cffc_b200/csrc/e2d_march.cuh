@@ -261,6 +261,22 @@ __device__ __forceinline__ void recon_cell(const MarchArgs& m, Smem& s, const Ti
                      RT(HALF * (x00 + x10) - xc0)};
   const RT ofy[4] = {RT(HALF * (y10 + y11) - yc0), RT(HALF * (y00 + y01) - yc0), RT(HALF * (y01 + y11) - yc0),
                      RT(HALF * (y00 + y10) - yc0)};
+  const int rs = rslot(k, sl);
+  if (!frozen && !B.freeze && !B.dWdx && B.limiter == E2D_LIMITER_VENKATAKRISHNAN) {
+    // the common case (uniform): Venkatakrishnan, no freezing, no export
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const RT gx = Sx[v] * K0 + Sy[v] * K1;
+      const RT gy = Sx[v] * K1 + Sy[v] * K2;
+      RT dq[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) dq[q] = gx * ofx[q] + gy * ofy[q];
+      const RT phi = fm::limiter_diff_k<E2D_LIMITER_VENKATAKRISHNAN>(dq, mn[v] - w0[v], mx[v] - w0[v]);
+      s.px[rs][v][c] = phi * gx;
+      s.py[rs][v][c] = phi * gy;
+    }
+    return;
+  }
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
     const RT gx = Sx[v] * K0 + Sy[v] * K1;
@@ -275,8 +291,8 @@ __device__ __forceinline__ void recon_cell(const MarchArgs& m, Smem& s, const Ti
       phi = fm::limiter_diff<RT>(B.limiter, dq, mn[v] - w0[v], mx[v] - w0[v]);
       if (B.freeze) B.phi_keep[cell_var(B, k.b, v, J, I)] = double(phi);
     }
-    s.px[rslot(k, sl)][v][c] = phi * gx;
-    s.py[rslot(k, sl)][v][c] = phi * gy;
+    s.px[rs][v][c] = phi * gx;
+    s.py[rs][v][c] = phi * gy;
     if (B.dWdx) {
       const size_t o = cell_var(B, k.b, v, J, I);
       B.dWdx[o] = gx; B.dWdy[o] = gy; B.phi[o] = phi;
