@@ -433,7 +433,9 @@ __device__ __forceinline__ bool not_positive(const CState<double>& u) {
 // dtg: the case's global time step of this explicit step (modes 1, 2 with
 // global time stepping).
 // up: the chunk's update inputs in shared memory (null: global loads).
-template <int MODE, bool FUSE>
+// PLAIN: the common explicit stage (up set, global time step, no RK4 slot
+// combination, no residual-only stage), with those tests compiled out.
+template <int MODE, bool FUSE, bool PLAIN>
 __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, const Chunk& k, int cs, int r, int q,
                                             size_t plane, double dtg, const UpdIn* up, double& dt_next, double& n1,
                                             double& n2, double& nmax) {
@@ -448,9 +450,11 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
   const size_t c = size_t(k.b) * plane + off;
   const size_t c0 = size_t(k.b) * 4 * plane + off;
   const double* gp = m.geom + size_t(k.b) * GEOM_NF * plane + off;
-  const double rA = up ? up->G[0][r][q] : gp[G_RA * plane];
+  const bool su = PLAIN || up != nullptr;  // update inputs in shared memory
+  const bool ldt = !PLAIN && B.local_dt;
+  const double rA = su ? up->G[0][r][q] : gp[G_RA * plane];
   double kk = 1.0;
-  if (MODE == 1 || MODE == 2) kk = B.cfl * (B.local_dt ? B.dt[c] : dtg);
+  if (MODE == 1 || MODE == 2) kk = B.cfl * (ldt ? B.dt[c] : dtg);
   const double kA = kk * rA;
   const int fs = fslot(k, r), fn = fslot(k, r + 1);
   double res[4];
@@ -459,8 +463,8 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
     double d = 0.0;
     if (MODE == 2) {
       const size_t qv = c0 + v * plane;
-      d = up ? up->R[v][r][q] : a.res_out[qv];
-      if (a.acc1) d = d + 2.0 * a.acc1[qv] + 2.0 * a.acc2[qv];
+      d = su ? up->R[v][r][q] : a.res_out[qv];
+      if (!PLAIN && a.acc1) d = d + 2.0 * a.acc1[qv] + 2.0 * a.acc2[qv];
     }
     d += s.Fi[r][v][q] * kA;
     d -= s.Fi[r][v][q + 1] * kA;
@@ -483,13 +487,13 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
       val -= (a.nks_z[qv + v] * rdt) * a.normU[v] / a.normR[v];
       a.nks_v[qv + v] = val;
     }
-  } else if (a.no_update) {
+  } else if (!PLAIN && a.no_update) {
 #pragma unroll
     for (int v = 0; v < 4; ++v) a.res_out[c0 + v * plane] = res[v];
   } else {
     // Update_Solution_Multistage_Explicit: U = Uo + omega*dUdt
     CState<double> uo;
-    if (up) {
+    if (su) {
       uo.d = up->U[0][r][q]; uo.mx = up->U[1][r][q]; uo.my = up->U[2][r][q]; uo.E = up->U[3][r][q];
     } else {
       uo.d = a.Ubase[c0]; uo.mx = a.Ubase[c0 + plane];
@@ -500,7 +504,7 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
     u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
     u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
     if (not_positive(u)) {
-      if (!B.local_dt) {
+      if (!ldt) {
         set_status(B.status, ST_NEGATIVE, int(c));
       } else {
         double rrf = 1.0, dtc = B.dt[c];
@@ -528,7 +532,7 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
     a.Wout[c0] = w.d; a.Wout[c0 + plane] = w.u; a.Wout[c0 + 2 * plane] = w.v; a.Wout[c0 + 3 * plane] = w.p;
     if (FUSE) {
       // CFL of the updated cell (Euler2DQuadSingleBlock.cc:3019-3080)
-      auto geo = [&](int f) { return up ? up->G[f - G_RA][r][q] : gp[f * plane]; };
+      auto geo = [&](int f) { return su ? up->G[f - G_RA][r][q] : gp[f * plane]; };
       const double v_i = w.u * geo(G_VIX) + w.v * geo(G_VIY);
       const double v_j = w.u * geo(G_VJX) + w.v * geo(G_VJY);
       const double c2 = g * w.p * rd;
@@ -536,7 +540,7 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
       const double ti = geo(G_DI) * fm::rcp(snd + fabs(v_i));
       const double tj = geo(G_DJ) * fm::rcp(snd + fabs(v_j));
       const double dtc = dmin(ti, tj);
-      if (B.local_dt) B.dt[c] = dtc;
+      if (ldt) B.dt[c] = dtc;
       dt_next = dmin(dt_next, dtc);
       n1 += fabs(res[0]);
       n2 += res[0] * res[0];
@@ -596,6 +600,9 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
 #endif
   };
   int upd_issued = 0, upd_waited = 0;  // update-input copies issued / consumed
+  // the common explicit stage: update inputs in shared memory, global time
+  // step, no RK4 slot combination, no residual-only stage (uniform)
+  const bool plain = upp != nullptr && !a.acc1 && !a.no_update && !B.local_dt;
 
   // the L2 prefetch share of this thread (fixed over the chunks): row pf_r
   // of the chunk, field pf_f (0-3 U, 4 1/A, 5-6 CFL lengths), column pf_c
@@ -678,7 +685,10 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
           recon_cell(m, s, T, k, sl, c, t == tid ? rin : recon_in(m, k, sl, c, plane), frozen);
         } else if (t >= nrec_w) {
           const int u = t - nrec_w;
-          update_cell<MODE, FUSE>(m, s, pk, pcase, u / MI, u % MI, plane, dtg, upp, dt_next, n1, n2, nmax);
+          if (plain)
+            update_cell<MODE, FUSE, true>(m, s, pk, pcase, u / MI, u % MI, plane, dtg, upp, dt_next, n1, n2, nmax);
+          else
+            update_cell<MODE, FUSE, false>(m, s, pk, pcase, u / MI, u % MI, plane, dtg, upp, dt_next, n1, n2, nmax);
         }
       }
     }
@@ -732,8 +742,12 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
       ++upd_waited;
     }
     const double dtg = step_dt(pcase);
-    for (int t = tid; t < pk.h * MI; t += THREADS)
-      update_cell<MODE, FUSE>(m, s, pk, pcase, t / MI, t % MI, plane, dtg, upp, dt_next, n1, n2, nmax);
+    for (int t = tid; t < pk.h * MI; t += THREADS) {
+      if (plain)
+        update_cell<MODE, FUSE, true>(m, s, pk, pcase, t / MI, t % MI, plane, dtg, upp, dt_next, n1, n2, nmax);
+      else
+        update_cell<MODE, FUSE, false>(m, s, pk, pcase, t / MI, t % MI, plane, dtg, upp, dt_next, n1, n2, nmax);
+    }
   }
   if (FUSE && cur_case >= 0) flush_next(a, s, cur_case, dt_next, n1, n2, nmax);
 }
