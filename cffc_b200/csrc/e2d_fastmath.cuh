@@ -86,7 +86,7 @@ __device__ __forceinline__ CState<double> flux_roe_n(const PState<double>& wl0, 
   const double rca = rsqrt(aa2);
   const double ca = sqrt_from_rsqrt(aa2, rca);
   const double da = sdl * sdr;
-  const double dW0 = dr - dl, dW1 = ur - ul, dW2 = vr - vl, dW3 = pr - pl;
+  const double dW1 = ur - ul, dW3 = pr - pl;
   const bool up = ua >= 0.0;
   const double d = up ? dl : dr, u = up ? ul : ur, v = up ? vl : vr, p = up ? pl : pr;
   const double h = up ? hl : hr;
@@ -105,14 +105,15 @@ __device__ __forceinline__ CState<double> flux_roe_n(const PState<double>& wl0, 
     d0 = harten_delta(la0, ul - cl, ur - cr);
     d3 = harten_delta(la3, ul + cl, ur + cr);
   }
-  double ws0, ws1, ws3;
+  // The entropy and shear waves travel at ua itself: with the upwind side
+  // taken from the sign of ua their strengths (ua -+ |ua|) / 2 are exactly
+  // zero, so only the two acoustic waves can contribute.
+  double ws0, ws3;
   if (up) {
     ws0 = 0.5 * (la0 - fabs(la0) - d0);
-    ws1 = 0.5 * (ua - fabs(ua));
     ws3 = 0.5 * (la3 - fabs(la3) - d3);
   } else {
     ws0 = 0.5 * (la0 + fabs(la0) + d0);
-    ws1 = 0.5 * (ua + fabs(ua));
     ws3 = 0.5 * (la3 + fabs(la3) + d3);
   }
   const double sg = up ? 1.0 : -1.0;
@@ -121,17 +122,10 @@ __device__ __forceinline__ CState<double> flux_roe_n(const PState<double>& wl0, 
   // Each wave contributes only where the reference's upwind test selects it;
   // a wave speed of exactly zero contributes nothing either way.
   const bool on0 = up ? (ws0 < 0.0) : (ws0 > 0.0);
-  const bool on1 = up ? (ws1 < 0.0) : (ws1 > 0.0);
   const bool on3 = up ? (ws3 < 0.0) : (ws3 > 0.0);
   if (on0) {
     const double k = sg * ws0 * (pdr - hdr);
     F0 += k; F1 += k * (ua - ca); F2 += k * va; F3 += k * (ha - ua * ca);
-  }
-  if (on1) {
-    const double k1 = sg * ws1 * (dW0 - rca2 * dW3);
-    F0 += k1; F1 += k1 * ua; F2 += k1 * va; F3 += k1 * (0.5 * qa2);
-    const double k2 = sg * ws1 * dW2;
-    F2 += k2 * da; F3 += k2 * (da * va);
   }
   if (on3) {
     const double k = sg * ws3 * (pdr + hdr);
