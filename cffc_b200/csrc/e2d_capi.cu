@@ -381,9 +381,12 @@ void apply_selection(e2d_handle* h) {
 // state arrays are cleared afterwards.
 int autotune_stage(e2d_handle* h) {
   if (!h->march_ok) return 0;
-  const char* kind = getenv("CFFC_E2D_STAGE_KERNEL");  // "tiled": comparisons of the two kernels
-  if (kind && strcmp(kind, "tiled") == 0) {
-    h->sel_march[0] = h->sel_march[1] = false;
+  // "tiled" / "march": one kernel without tuning (tests and comparisons of
+  // the two kernels; "march" with its default rows per chunk)
+  const char* kind = getenv("CFFC_E2D_STAGE_KERNEL");
+  if (kind && (strcmp(kind, "tiled") == 0 || strcmp(kind, "march") == 0)) {
+    h->sel_march[0] = h->sel_march[1] = strcmp(kind, "march") == 0;
+    h->sel_rows[0] = h->sel_rows[1] = fast::march_chunk_rows();
     apply_selection(h);
     return 0;
   }

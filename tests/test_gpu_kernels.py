@@ -1,0 +1,62 @@
+"""Both stage kernels of the fast FP64 precision against the reference's
+golden vectors, whichever one the handle's autotuner would choose:
+CFFC_E2D_STAGE_KERNEL=tiled / march fixes the kernel when a handle is
+created.  The column-marching kernel serves the Roe flux on blocks of even
+width; other cases keep the tiled kernel whatever the setting.  Tolerances
+as tests/test_gpu_parity.py: residual per cell within helpers.rtol_fast (and
+per value within 1e-12 (1 + scale / |ref|)), explicit runs within 1e-11 with
+the time-step history to 1e-12."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from cffc_b200 import capi, cases
+from helpers import fixtures, load, rel_err, rtol_fast
+
+pytestmark = pytest.mark.gpu
+
+FAST = 0
+KERNELS = {"tiled": 0, "march": 1}
+
+
+def fast_handle(bs, kernel, monkeypatch):
+    monkeypatch.setenv("CFFC_E2D_STAGE_KERNEL", kernel)
+    h = capi.Handle(dataclasses.replace(bs, scheme=dataclasses.replace(bs.scheme, precision=FAST)))
+    monkeypatch.delenv("CFFC_E2D_STAGE_KERNEL")
+    k, _, _ = h.stage_config()
+    marchable = bs.scheme.flux == cases.FLUX_ROE and bs.nci % 2 == 0
+    assert k == (KERNELS[kernel] if marchable else 0), (kernel, k)
+    return h
+
+
+@pytest.mark.parametrize("kernel", sorted(KERNELS))
+@pytest.mark.parametrize("name", fixtures("residual"))
+def test_residual_fast_each_kernel(name, kernel, monkeypatch):
+    bs, ref, _, lean = load(name)
+    h = fast_handle(bs, kernel, monkeypatch)
+    h.set_state()
+    dUdt = bs.interior(h.residual())
+    h.close()
+    r = ref["dUdt"] if lean else bs.interior(ref["dUdt"])
+    assert rel_err(dUdt, r) <= rtol_fast(bs)
+    scale = np.max(np.abs(r), axis=(0, 2, 3), keepdims=True)
+    scale = np.broadcast_to(np.maximum(scale, 1e-3 * np.max(np.abs(r))), r.shape)
+    sig = np.abs(r) >= 1e-8 * scale
+    rel = np.abs(dUdt[sig] - r[sig]) / np.abs(r[sig])
+    assert np.all(rel <= rtol_fast(bs) * (1.0 + scale[sig] / np.abs(r[sig])))
+
+
+@pytest.mark.parametrize("kernel", sorted(KERNELS))
+@pytest.mark.parametrize("name", fixtures("explicit"))
+def test_explicit_fast_each_kernel(name, kernel, monkeypatch):
+    bs, ref, steps, lean = load(name)
+    h = fast_handle(bs, kernel, monkeypatch)
+    h.set_state()
+    rc, hist = h.rk_steps(steps)
+    _, U = h.get_state()
+    h.close()
+    assert rc == 0
+    r = ref["U"] if lean else bs.interior(ref["U"])
+    assert rel_err(bs.interior(U), r) <= 1e-11
+    np.testing.assert_allclose(hist[:, 0], ref["hist"][:, 0], rtol=1e-12)
