@@ -208,7 +208,7 @@ def nks_c2_measure(precision, device, cpu):
     return out
 
 
-def parse():
+def parse_args(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
@@ -219,7 +219,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-nks", action="store_true", help="skip the Newton-Krylov s-to-steady measurement")
     p.add_argument("--sweep-cases", type=int, default=512, help="cases of the batched Newton-Krylov sweep")
-    return p.parse_args()
+    return p.parse_args(argv)
 
 
 def peaks():
@@ -647,8 +647,26 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(x, world, device):
+    """The largest x over the ranks (replicas: each rank times its own
+    device, the job takes as long as the slowest); every rank gets it."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, cell_updates, ms):
+    """Mcell-updates/s of the whole job: world replicas, each advancing
+    cell_updates per step, in ms per step (the slowest rank's)."""
+    return world * cell_updates / (ms * 1e-3) * 1e-6
+
+
 def main():
-    args = parse()
+    args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
 
@@ -692,13 +710,9 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
     barrier()
-    ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, "cuda")
     cell_updates = bs.n_interior * args.rk_steps
-    value = world * cell_updates / (ms * 1e-3) * 1e-6
+    value = job_throughput(world, cell_updates, ms)
 
     # per-kernel device times of the fused stage kernel (launch by launch)
     kt = np.zeros(6)
@@ -735,12 +749,8 @@ def main():
         assert rc == 0
         assert h.lib.e2d_get_state(h.h, capi.C.cast(None, capi._dp), Up) == 0
     torch.cuda.synchronize()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = world * cell_updates / (e2e_ms * 1e-3) * 1e-6
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, world, "cuda")
+    e2e = job_throughput(world, cell_updates, e2e_ms)
 
     line = None
     if rank == 0:
