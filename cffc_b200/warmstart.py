@@ -384,19 +384,31 @@ def solve_in_batches(fam, params, device=0, per_batch=256):
 
 
 def train_network_deep(train_fam, params, steps=((1e-3, 2000), (3e-4, 1500), (1e-4, 500)), batch=8192, seed=11,
-                       device=0):
-    """Solves the training cases (batched, from the freestream), builds the
-    per-cell training set of the deep network (features_deep) and trains it
-    on minibatches.  Returns (net, info)."""
+                       device=0, per_batch=256, row_stride=1):
+    """Solves the training cases (batched, per_batch cases a handle, from the
+    freestream), builds the per-cell training set of the deep network
+    (features_deep; every row_stride-th cell of each case, so that large
+    training families stay within host memory; each batch's states are
+    dropped once its rows are taken) and trains it on minibatches.  Returns
+    (net, info)."""
     import time
 
     import torch
     t0 = time.perf_counter()
-    rc, hists, states = solve_in_batches(train_fam, params, device=device)
+    Xs, Ts, hists = [], [], []
+    for k in range(0, len(train_fam), per_batch):
+        sub = train_fam[k:k + per_batch]
+        rc, h, states = solve_family(sub, params, device=device)
+        if rc:
+            raise RuntimeError(f"training-set solve failed: {rc}")
+        X, T = build_training_set(sub, states, features_deep)
+        Xs.append(X[::row_stride])
+        Ts.append(T[::row_stride])
+        hists += h
+        del states
     t_solve = time.perf_counter() - t0
-    if rc:
-        raise RuntimeError(f"training-set solve failed: {rc}")
-    X, T = build_training_set(train_fam, states, features_deep)
+    X, T = np.concatenate(Xs), np.concatenate(Ts)
+    del Xs, Ts
     Xd, Td = torch.from_numpy(X).cuda(device), torch.from_numpy(T).cuda(device)
     net = MlpDeep(seed=seed)
     t0 = time.perf_counter()
