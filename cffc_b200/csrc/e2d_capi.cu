@@ -251,7 +251,7 @@ int setup_march(e2d_handle* h) {
   const uint32_t wi = mi + 4, nwi = mi + 6;
   bool ok = encode3(&h->tmW[0], B.W, B.NCi, B.NCj, 4ull * B.nblk, wi, wj, 4) &&
             encode3(&h->tmW[1], B.W2, B.NCi, B.NCj, 4ull * B.nblk, wi, wj, 4) &&
-            encode3(&h->tmG, h->geom, B.NCi, B.NCj, uint64_t(GEOM_NF) * B.nblk, wi, wj, 2) &&
+            encode3(&h->tmG, h->geom, B.NCi, B.NCj, uint64_t(GEOM_NF) * B.nblk, wi, wj, G_K2 + 1) &&
             encode3(&h->tmN, h->nodes_pad, NNp, B.NNj, 2ull * B.nblk, nwi, wj, 2);
   if (ok && h->W3) ok = encode3(&h->tmW[2], h->W3, B.NCi, B.NCj, 4ull * B.nblk, wi, wj, 4);
   if (!ok) return 0;

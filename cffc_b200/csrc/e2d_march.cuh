@@ -75,23 +75,29 @@ constexpr bool UPD = E2D_MARCH_UPD;
 constexpr uint32_t WAIT_ITERS = 1u << 24;          // bounded mbarrier wait (about a second)
 constexpr int ST_TIMEOUT = 2;                      // status code: a staging wait ran out
 
+// geometry planes of the window: centroid x, y and the least-squares
+// inverse K0, K1, K2 (planes G_XC .. G_K2 of the per-handle geometry)
+constexpr int TG = G_K2 + 1;
 struct Tile {
   double W[4][WJ][WI];   // primitive state, rows j0 .. j0+11, cols i0 .. i0+35
-  double G[2][WJ][WI];   // centroids
+  double G[TG][WJ][WI];  // centroids, least-squares inverse
   double N[2][WJ][NWI];  // nodes, cols i0 .. i0+37
 };
-constexpr uint32_t TILE_BYTES = sizeof(double) * (6 * WJ * WI + 2 * WJ * NWI);
+constexpr uint32_t TILE_BYTES = sizeof(double) * ((4 + TG) * WJ * WI + 2 * WJ * NWI);
 static_assert(sizeof(Tile) == TILE_BYTES && TILE_BYTES % 128 == 0, "tile packing");
-static_assert((4 * WJ * WI * 8) % 128 == 0 && (6 * WJ * WI * 8) % 128 == 0, "TMA destinations 128-byte aligned");
+static_assert((4 * WJ * WI * 8) % 128 == 0 && ((4 + TG) * WJ * WI * 8) % 128 == 0, "TMA destinations 128-byte aligned");
 static_assert(THREADS >= MJ * MI, "one thread per update cell");
 static_assert(MI % 2 == 0 && (MI * 8) % 16 == 0, "strip origins on 16-byte boundaries");
 
 // Reconstructions and j-face fluxes live in rings indexed by the array row
 // (row mod RR): a chunk reads the top reconstruction row and the bottom j-face
-// row the chunk below it left there, and the next chunk's reconstruction
-// overwrites nothing the pending update still reads.
-constexpr int RR = 12;
-static_assert(RR >= RCJ + 2, "ring holds a chunk's rows and the next chunk's first");
+// row the chunk below it left there.  Live at once: the reconstruction rows
+// j0+1 .. j0+h+2 of the chunk being evaluated (its own and the two carried
+// up), at most RCJ; the j-face rows j0+2 .. j0+h+2 of a chunk between its
+// faces and its update, at most MJ + 1 (the update of chunk c-1 runs before
+// chunk c's faces overwrite any of its rows).
+constexpr int RR = RCJ;
+static_assert(RR >= RCJ && RR >= MJ + 1, "ring holds the live rows");
 
 // Update inputs of a chunk's cells (rows j0+2 .., columns i0+2 ..): the base
 // conserved state, the residual RK stage 2 adds to, and geometry planes
@@ -160,7 +166,7 @@ __device__ __forceinline__ PState<RT> wwin(const Tile& T, int wj, int wi) {
 }
 
 // Ring slot of the reconstruction of chunk slot sl (array row j0+1+sl) and
-// of j-face slot sl (face row j0+2+sl); sl + 1 < RR.
+// of j-face slot sl (face row j0+2+sl); r0 + sl < 2 RR (r0 < RR, sl <= RCJ - 1).
 __device__ __forceinline__ int rslot(const Chunk& k, int sl) {
   const int r = k.r0 + sl;
   return r >= RR ? r - RR : r;
@@ -181,23 +187,18 @@ __device__ __forceinline__ PState<RT> fstate(const Smem& s, const Tile& T, const
   return w;
 }
 
-// The per-cell inputs of a reconstruction: stencil mask and least-squares
-// inverse (loaded before the staging wait, so their latency overlaps it).
+// The per-cell input of a reconstruction from global memory: its stencil
+// mask (loaded before the staging wait, so its latency overlaps it; the
+// least-squares inverse arrives with the window).
 struct ReconIn {
   unsigned msk;
-  double K0, K1, K2;
 };
 __device__ __forceinline__ ReconIn recon_in(const MarchArgs& m, const Chunk& k, int sl, int c, size_t plane) {
   const Blocks& B = m.a.B;
-  ReconIn r{0u, 0.0, 0.0, 0.0};
+  ReconIn r{0u};
   const int I = k.i0 + 1 + c, J = k.j0 + 1 + sl;
   if (I > B.nci + 2 || J > B.ncj + 2) return r;
-  const size_t off = size_t(J) * B.NCi + I;
-  r.msk = m.mask[size_t(k.b) * plane + off];
-  const double* gp = m.geom + size_t(k.b) * GEOM_NF * plane + off;
-  r.K0 = gp[G_K0 * plane];
-  r.K1 = gp[G_K1 * plane];
-  r.K2 = gp[G_K2 * plane];
+  r.msk = m.mask[size_t(k.b) * plane + size_t(J) * B.NCi + I];
   return r;
 }
 
@@ -220,8 +221,8 @@ __device__ __forceinline__ void recon_cell(const MarchArgs& m, Smem& s, const Ti
       }
     return;
   }
-  const RT K0 = RT(in.K0), K1 = RT(in.K1), K2 = RT(in.K2);
   const int wi = c + 1, wj = sl + 1;
+  const RT K0 = RT(T.G[G_K0][wj][wi]), K1 = RT(T.G[G_K1][wj][wi]), K2 = RT(T.G[G_K2][wj][wi]);
   const double xc0 = T.G[0][wj][wi], yc0 = T.G[1][wj][wi];
   RT w0[4], Sx[4], Sy[4], mn[4], mx[4];
 #pragma unroll
@@ -650,7 +651,7 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
       }
     }
     // this thread's first reconstruction cell: its inputs, ahead of the wait
-    ReconIn rin{0u, 0.0, 0.0, 0.0};
+    ReconIn rin{0u};
     if (tid < nrow * RCI) rin = recon_in(m, k, s_lo + tid / RCI, tid % RCI, plane);
     bool ok = tc::mbar_wait(&s.full[buf], par, WAIT_ITERS);
     if (upd && pcase >= 0) ok = tc::mbar_wait(&s.fullu, uint32_t(upd_waited) & 1u, WAIT_ITERS) && ok;
