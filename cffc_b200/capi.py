@@ -268,7 +268,9 @@ class Handle:
 class BatchHandle(Handle):
     """Several independent cases on one handle (e2d_create_batch): their
     blocks end to end in case order; per-case histories and Newton-Krylov
-    solves.  Block dimensions and the scheme must agree across cases."""
+    solves.  The scheme must agree across cases; cases of different block
+    shapes run as one sub-batch per shape, and the host arrays are each
+    case's array in its own shape, concatenated in case order."""
 
     def __init__(self, cases: list[BlockSet], device: int = 0, lib=None):
         self.lib = lib or load_library()
@@ -292,25 +294,30 @@ class BatchHandle(Handle):
             raise RuntimeError(f"e2d_create_batch failed: {E2D_ERRORS.get(err.value, err.value)}")
         self.nblk = sum(bs.nblk for bs in cases)
         self.offsets = np.cumsum([0] + [bs.nblk for bs in cases])
-
-    def shape(self):
-        return (self.nblk, 4, self.bs.NCj, self.bs.NCi)
+        self._shapes = [(bs.nblk, 4, bs.NCj, bs.NCi) for bs in cases]
+        self._sizes = [int(np.prod(sh)) for sh in self._shapes]
+        self._flat_off = np.cumsum([0] + self._sizes)
 
     def split(self, a):
-        return [a[self.offsets[c]:self.offsets[c + 1]] for c in range(len(self.cases))]
+        """Per-case views of a concatenated host array."""
+        a = a.ravel()
+        return [a[self._flat_off[c]:self._flat_off[c + 1]].reshape(self._shapes[c]) for c in range(len(self.cases))]
+
+    def _flat(self):
+        return np.empty(int(self._flat_off[-1]))
 
     def set_state(self, Ws=None) -> None:
         Ws = [bs.W for bs in self.cases] if Ws is None else Ws
-        W = np.ascontiguousarray(np.concatenate(Ws, axis=0), dtype=np.float64)
+        W = np.ascontiguousarray(np.concatenate([np.asarray(w, dtype=np.float64).ravel() for w in Ws]))
         self._call("set_state", ptr(W))
 
     def get_state(self):
-        W, U = np.empty(self.shape()), np.empty(self.shape())
+        W, U = self._flat(), self._flat()
         self._call("get_state", ptr(W), ptr(U))
         return list(zip(self.split(W), self.split(U)))
 
     def residual(self):
-        out = np.empty(self.shape())
+        out = self._flat()
         self._call("residual", ptr(out))
         return self.split(out)
 

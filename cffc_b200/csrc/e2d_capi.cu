@@ -598,6 +598,126 @@ cudaError_t enqueue_step(e2d_handle* h) {
 
 using namespace e2d_host;
 
+// ---- batches of cases with different block shapes ---------------------------
+// One uniform sub-batch per shape (cases grouped in order of first
+// appearance); the handle dispatches every call to them and moves each
+// case's host arrays between the callers' concatenation (cases in the order
+// given, each in its own shape) and the sub-batches' own concatenations.
+
+static e2d_handle* create_mixed_batch(const e2d_blocks_desc* cases, int ncase, const e2d_scheme* sc, int device,
+                                      int* err) {
+  std::vector<std::vector<int>> groups;
+  std::vector<int> group_of(ncase, -1);
+  for (int c = 0; c < ncase; ++c) {
+    for (size_t g = 0; g < groups.size() && group_of[c] < 0; ++g) {
+      const e2d_blocks_desc& r = cases[groups[g][0]];
+      if (r.nci == cases[c].nci && r.ncj == cases[c].ncj && r.ng == cases[c].ng) group_of[c] = int(g);
+    }
+    if (group_of[c] < 0) {
+      group_of[c] = int(groups.size());
+      groups.emplace_back();
+    }
+    groups[group_of[c]].push_back(c);
+  }
+  e2d_handle* h = new e2d_handle;
+  h->device = device;
+  h->sc = *sc;
+  h->B.ncase = ncase;
+  h->sub_of.resize(ncase);
+  h->local_of.resize(ncase);
+  for (size_t g = 0; g < groups.size(); ++g) {
+    std::vector<e2d_blocks_desc> d;
+    for (size_t k = 0; k < groups[g].size(); ++k) {
+      d.push_back(cases[groups[g][k]]);
+      h->sub_of[groups[g][k]] = int(g);
+      h->local_of[groups[g][k]] = int(k);
+    }
+    e2d_handle* sub = e2d_create_batch(d.data(), int(d.size()), sc, device, err);
+    if (!sub) {
+      e2d_destroy(h);
+      return nullptr;
+    }
+    h->subs.push_back(sub);
+  }
+  size_t o4 = 0, o1 = 0;
+  for (int c = 0; c < ncase; ++c) {
+    const size_t plane = size_t(cases[c].nci + 2 * cases[c].ng) * (cases[c].ncj + 2 * cases[c].ng);
+    h->off4.push_back(o4);
+    h->size4.push_back(size_t(cases[c].nblk) * 4 * plane);
+    h->off1.push_back(o1);
+    h->size1.push_back(size_t(cases[c].nblk) * plane);
+    o4 += h->size4.back();
+    o1 += h->size1.back();
+  }
+  return h;
+}
+
+namespace e2d_host {
+
+// Cases of sub-batch s in its own order.
+static std::vector<int> sub_cases(const e2d_handle* h, int s) {
+  std::vector<int> out;
+  for (int c = 0; c < int(h->sub_of.size()); ++c)
+    if (h->sub_of[c] == s) out.push_back(c);
+  return out;
+}
+
+// Caller array (per case off/size) -> sub-batch s's concatenation, or back.
+static void gather_sub(const e2d_handle* h, int s, const double* all, const std::vector<size_t>& off,
+                       const std::vector<size_t>& size, std::vector<double>& out) {
+  out.clear();
+  for (int c : sub_cases(h, s)) out.insert(out.end(), all + off[c], all + off[c] + size[c]);
+}
+static void scatter_sub(const e2d_handle* h, int s, const std::vector<double>& in, const std::vector<size_t>& off,
+                        const std::vector<size_t>& size, double* all) {
+  size_t q = 0;
+  for (int c : sub_cases(h, s)) {
+    std::copy(in.begin() + q, in.begin() + q + size[c], all + off[c]);
+    q += size[c];
+  }
+}
+static size_t total(const std::vector<size_t>& size) {
+  size_t t = 0;
+  for (size_t v : size) t += v;
+  return t;
+}
+static size_t sub_total(const e2d_handle* h, int s, const std::vector<size_t>& size) {
+  size_t t = 0;
+  for (int c : sub_cases(h, s)) t += size[c];
+  return t;
+}
+
+// Newton-Krylov over the sub-batches, one after another: per-case reference
+// levels go to each sub-batch, histories ([case][max_newton]) and step
+// counts come back to the caller's case order.
+int composite_nks(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, int* n_steps) {
+  const int m = std::max(p->max_newton, 1);
+  int rc = 0;
+  for (int s = 0; s < int(h->subs.size()); ++s) {
+    const std::vector<int> cs = sub_cases(h, s);
+    e2d_nks_params q = *p;
+    std::vector<double> l2, cfl;
+    for (int c : cs) {
+      if (p->l2_reference) l2.push_back(p->l2_reference[c]);
+      if (p->cfl_reference) cfl.push_back(p->cfl_reference[c]);
+    }
+    q.l2_reference = p->l2_reference ? l2.data() : nullptr;
+    q.cfl_reference = p->cfl_reference ? cfl.data() : nullptr;
+    std::vector<e2d_nks_step> hs(size_t(m) * cs.size());
+    std::vector<int> ns(cs.size(), 0);
+    const int r = e2d_nks(h->subs[s], &q, hist ? hs.data() : nullptr, ns.data());
+    if (r < 0) return r;
+    if (r > 0 && rc == 0) rc = r;
+    for (size_t k = 0; k < cs.size(); ++k) {
+      if (n_steps) n_steps[cs[k]] = ns[k];
+      if (hist) std::copy(hs.begin() + k * m, hs.begin() + (k + 1) * m, hist + size_t(cs[k]) * m);
+    }
+  }
+  return rc;
+}
+
+}  // namespace e2d_host
+
 extern "C" {
 
 e2d_handle* e2d_create(const e2d_blocks_desc* d, const e2d_scheme* sc, int device, int* err) {
@@ -717,10 +837,12 @@ e2d_handle* e2d_create_batch(const e2d_blocks_desc* cases, int ncase, const e2d_
   const int nci = cases[0].nci, ncj = cases[0].ncj, ng = cases[0].ng;
   int nblk = 0;
   for (int c = 0; c < ncase; ++c) {
-    if (cases[c].nci != nci || cases[c].ncj != ncj || cases[c].ng != ng || cases[c].nblk < 1) {
+    if (cases[c].nblk < 1) {
       if (err) *err = E2D_ERR_ARG;
       return nullptr;
     }
+    if (cases[c].nci != nci || cases[c].ncj != ncj || cases[c].ng != ng)
+      return create_mixed_batch(cases, ncase, sc, device, err);
     nblk += cases[c].nblk;
   }
   const size_t NCi = nci + 2 * ng, NCj = ncj + 2 * ng, NN = (NCi + 1) * (NCj + 1);
@@ -781,6 +903,11 @@ int e2d_batch_cases(e2d_handle* h) { return h ? h->B.ncase : E2D_ERR_ARG; }
 
 void e2d_destroy(e2d_handle* h) {
   if (!h) return;
+  if (!h->subs.empty()) {
+    for (e2d_handle* s : h->subs) e2d_destroy(s);
+    delete h;
+    return;
+  }
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
@@ -819,6 +946,14 @@ static int mirror_stage_buffers(e2d_handle* h) {
 
 int e2d_set_state(e2d_handle* h, const double* W) {
   if (!h || !W) return E2D_ERR_ARG;
+  if (!h->subs.empty()) {
+    std::vector<double> t;
+    for (int s = 0; s < int(h->subs.size()); ++s) {
+      gather_sub(h, s, W, h->off4, h->size4, t);
+      if (int rc = e2d_set_state(h->subs[s], t.data())) return rc;
+    }
+    return 0;
+  }
   CK(cudaSetDevice(h->device));
   CK(cudaMemcpyAsync(h->B.W, W, sizeof(double) * 4 * h->ncell, cudaMemcpyHostToDevice, h->stream));
   int grid = int((h->ncell + 255) / 256);
@@ -847,6 +982,14 @@ __global__ void w_of_u_kernel(Blocks B, long long ncell) {
 
 int e2d_set_conserved(e2d_handle* h, const double* U) {
   if (!h || !U) return E2D_ERR_ARG;
+  if (!h->subs.empty()) {
+    std::vector<double> t;
+    for (int s = 0; s < int(h->subs.size()); ++s) {
+      gather_sub(h, s, U, h->off4, h->size4, t);
+      if (int rc = e2d_set_conserved(h->subs[s], t.data())) return rc;
+    }
+    return 0;
+  }
   CK(cudaSetDevice(h->device));
   CK(cudaMemcpyAsync(h->B.U, U, sizeof(double) * 4 * h->ncell, cudaMemcpyHostToDevice, h->stream));
   int grid = int((h->ncell + 255) / 256);
@@ -862,6 +1005,16 @@ int e2d_set_conserved(e2d_handle* h, const double* U) {
 
 int e2d_get_state(e2d_handle* h, double* W, double* U) {
   if (!h) return E2D_ERR_ARG;
+  if (!h->subs.empty()) {
+    for (int s = 0; s < int(h->subs.size()); ++s) {
+      const size_t n = sub_total(h, s, h->size4);
+      std::vector<double> w(W ? n : 0), u(U ? n : 0);
+      if (int rc = e2d_get_state(h->subs[s], W ? w.data() : nullptr, U ? u.data() : nullptr)) return rc;
+      if (W) scatter_sub(h, s, w, h->off4, h->size4, W);
+      if (U) scatter_sub(h, s, u, h->off4, h->size4, U);
+    }
+    return 0;
+  }
   CK(cudaSetDevice(h->device));
   if (W) CK(cudaMemcpyAsync(W, h->B.W, sizeof(double) * 4 * h->ncell, cudaMemcpyDeviceToHost, h->stream));
   if (U) CK(cudaMemcpyAsync(U, h->B.U, sizeof(double) * 4 * h->ncell, cudaMemcpyDeviceToHost, h->stream));
@@ -871,6 +1024,11 @@ int e2d_get_state(e2d_handle* h, double* W, double* U) {
 
 int e2d_fill_ghosts(e2d_handle* h) {
   if (!h) return E2D_ERR_ARG;
+  if (!h->subs.empty()) {
+    for (e2d_handle* s : h->subs)
+      if (int rc = e2d_fill_ghosts(s)) return rc;
+    return 0;
+  }
   CK(cudaSetDevice(h->device));
   CK(launch_ghost_fill(h->B, h->stream));
   return check_status(h);
@@ -878,6 +1036,17 @@ int e2d_fill_ghosts(e2d_handle* h) {
 
 int e2d_residual(e2d_handle* h, double* dUdt) {
   if (!h) return E2D_ERR_ARG;
+  if (!h->subs.empty()) {
+    int rc = 0;
+    for (int s = 0; s < int(h->subs.size()); ++s) {
+      std::vector<double> r(dUdt ? sub_total(h, s, h->size4) : 0);
+      const int q = e2d_residual(h->subs[s], dUdt ? r.data() : nullptr);
+      if (q < 0) return q;
+      if (q > 0 && rc == 0) rc = q;
+      if (dUdt) scatter_sub(h, s, r, h->off4, h->size4, dUdt);
+    }
+    return rc;
+  }
   CK(cudaSetDevice(h->device));
   int rc = ensure_recon(h);
   if (rc) return rc;
@@ -888,7 +1057,7 @@ int e2d_residual(e2d_handle* h, double* dUdt) {
 }
 
 int e2d_get_reconstruction(e2d_handle* h, double* dWdx, double* dWdy, double* phi) {
-  if (!h) return E2D_ERR_ARG;
+  if (!h || !h->subs.empty()) return E2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
   int rc = ensure_recon(h);
   if (rc) return rc;
@@ -902,6 +1071,23 @@ int e2d_get_reconstruction(e2d_handle* h, double* dWdx, double* dWdy, double* ph
 
 int e2d_rk_steps(e2d_handle* h, int n_steps, double* hist) {
   if (!h || n_steps < 0) return E2D_ERR_ARG;
+  if (!h->subs.empty()) {
+    const int C = h->B.ncase;
+    int rc = 0;
+    for (int s = 0; s < int(h->subs.size()); ++s) {
+      const std::vector<int> cs = sub_cases(h, s);
+      std::vector<double> hs(hist ? size_t(n_steps) * cs.size() * 4 : 0);
+      const int q = e2d_rk_steps(h->subs[s], n_steps, hist ? hs.data() : nullptr);
+      if (q < 0) return q;
+      if (q > 0 && rc == 0) rc = q;
+      if (hist)
+        for (int t = 0; t < n_steps; ++t)
+          for (size_t k = 0; k < cs.size(); ++k)
+            for (int f = 0; f < 4; ++f)
+              hist[(size_t(t) * C + cs[k]) * 4 + f] = hs[(size_t(t) * cs.size() + k) * 4 + f];
+    }
+    return rc;
+  }
   if (n_steps == 0) return 0;
   CK(cudaSetDevice(h->device));
   int rc = ensure_hist(h, n_steps + 1);  // the last step fills slot n_steps
@@ -945,6 +1131,16 @@ int e2d_rk_steps(e2d_handle* h, int n_steps, double* hist) {
 
 int e2d_norms(e2d_handle* h, double* out) {
   if (!h || !out) return E2D_ERR_ARG;
+  if (!h->subs.empty()) {
+    for (int s = 0; s < int(h->subs.size()); ++s) {
+      const std::vector<int> cs = sub_cases(h, s);
+      std::vector<double> o(3 * cs.size());
+      if (int rc = e2d_norms(h->subs[s], o.data())) return rc;
+      for (size_t k = 0; k < cs.size(); ++k)
+        for (int f = 0; f < 3; ++f) out[3 * size_t(cs[k]) + f] = o[3 * k + f];
+    }
+    return 0;
+  }
   CK(cudaSetDevice(h->device));
   CK(cudaMemsetAsync(h->step, 0, sizeof(int), h->stream));
   CK(launch_norms(h->B, h->part, h->hist, h->step, h->stream));
@@ -958,6 +1154,17 @@ int e2d_norms(e2d_handle* h, double* out) {
 
 int e2d_cfl(e2d_handle* h, double* dt, double* dtmin) {
   if (!h) return E2D_ERR_ARG;
+  if (!h->subs.empty()) {
+    for (int s = 0; s < int(h->subs.size()); ++s) {
+      const std::vector<int> cs = sub_cases(h, s);
+      std::vector<double> d(dt ? sub_total(h, s, h->size1) : 0), m(cs.size());
+      if (int rc = e2d_cfl(h->subs[s], dt ? d.data() : nullptr, m.data())) return rc;
+      if (dt) scatter_sub(h, s, d, h->off1, h->size1, dt);
+      if (dtmin)
+        for (size_t k = 0; k < cs.size(); ++k) dtmin[cs[k]] = m[k];
+    }
+    return 0;
+  }
   CK(cudaSetDevice(h->device));
   CK(cudaMemsetAsync(h->step, 0, sizeof(int), h->stream));
   CK(launch_slot_init(h->hist, h->step, 0, h->B.ncase, h->stream));
@@ -976,6 +1183,12 @@ int e2d_cfl(e2d_handle* h, double* dt, double* dtmin) {
 int e2d_set_precision(e2d_handle* h, int precision) {
   if (!h || (precision != E2D_PREC_FP64 && precision != E2D_PREC_FP32 && precision != E2D_PREC_FP64_EXACT))
     return E2D_ERR_ARG;
+  if (!h->subs.empty()) {
+    for (e2d_handle* s : h->subs)
+      if (int rc = e2d_set_precision(s, precision)) return rc;
+    h->sc.precision = precision;
+    return 0;
+  }
   if (precision == h->sc.precision) return 0;
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
@@ -992,6 +1205,7 @@ int e2d_set_precision(e2d_handle* h, int precision) {
 
 int e2d_stage_config(e2d_handle* h, int* kernel, int* rows, double* us) {
   if (!h) return E2D_ERR_ARG;
+  if (!h->subs.empty()) return e2d_stage_config(h->subs[0], kernel, rows, us);  // the first shape's
   if (kernel) *kernel = h->march ? 1 : 0;
   if (rows) *rows = h->march ? h->march_rows : 0;
   if (us) *us = h->tune_us;
@@ -1000,11 +1214,16 @@ int e2d_stage_config(e2d_handle* h, int* kernel, int* rows, double* us) {
 
 int e2d_status(e2d_handle* h) {
   if (!h) return E2D_ERR_ARG;
+  if (!h->subs.empty()) {
+    for (e2d_handle* s : h->subs)
+      if (int rc = e2d_status(s)) return rc;
+    return 0;
+  }
   return check_status(h);
 }
 
 int e2d_device_state(e2d_handle* h, double** W, double** U, double** dUdt) {
-  if (!h) return E2D_ERR_ARG;
+  if (!h || !h->subs.empty()) return E2D_ERR_ARG;
   if (W) *W = h->B.W;
   if (U) *U = h->B.U;
   if (dUdt) *dUdt = h->B.dUdt;
@@ -1013,6 +1232,11 @@ int e2d_device_state(e2d_handle* h, double** W, double** U, double** dUdt) {
 
 int e2d_set_stream(e2d_handle* h, void* stream) {
   if (!h) return E2D_ERR_ARG;
+  if (!h->subs.empty()) {
+    for (e2d_handle* s : h->subs)
+      if (int rc = e2d_set_stream(s, stream)) return rc;
+    return 0;
+  }
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
   if (!h->own_stream) {
@@ -1023,7 +1247,7 @@ int e2d_set_stream(e2d_handle* h, void* stream) {
 }
 
 int e2d_kernel_times(e2d_handle* h, int n_steps, double out[6]) {
-  if (!h || !out || n_steps < 1) return E2D_ERR_ARG;
+  if (!h || !out || n_steps < 1 || !h->subs.empty()) return E2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
   int rc = ensure_hist(h, n_steps + 1);
   if (rc) return rc;

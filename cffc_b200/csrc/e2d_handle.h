@@ -41,6 +41,14 @@ struct e2d_handle {
   double* geom = nullptr;
   unsigned char* gmask = nullptr;
   unsigned char* bcside = nullptr;  // per block: sides with face-setting BCs (marching kernel)
+  // A batch whose cases have different block shapes holds no blocks of its
+  // own: one uniform sub-batch per shape, every call dispatched to them.
+  // Per case (in the order given): its sub-batch and index there, and the
+  // offsets of its arrays in the callers' concatenated host arrays (cell
+  // arrays of 4 variables, scalar per-cell arrays).
+  std::vector<e2d_handle*> subs;
+  std::vector<int> sub_of, local_of;
+  std::vector<size_t> off4, size4, off1, size1;
   CUtensorMap tmU[2], tmR, tmGA, tmGF;  // marching kernel update inputs: U and U2, dUdt, geometry
   bool upd_ok = false;
   double* nodes_pad = nullptr;
@@ -80,6 +88,8 @@ template <class T> int dalloc(e2d_handle* h, T** p, size_t n) {
 int check_status(e2d_handle* h);
 cudaError_t launch_stage_any(e2d_handle* h, int mode, int fuse_next);
 cudaError_t launch_stage_args(e2d_handle* h, e2d::StageArgs& a);
+// Newton-Krylov over the sub-batches of a mixed-shape batch (e2d_nks).
+int composite_nks(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, int* n_steps);
 cudaError_t ghost_fill_for(e2d_handle* h, int mode);
 int ensure_hist(e2d_handle* h, int n);
 void nks_free(e2d_handle* h);

@@ -1261,6 +1261,7 @@ static bool params_ok(const e2d_nks_params& p) {
 // disabled): the solve runs without the freezing machinery.
 extern "C" int e2d_nks(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, int* n_steps) {
   if (!h) return nks_run(h, p, hist, n_steps);
+  if (!h->subs.empty()) return p ? composite_nks(h, p, hist, n_steps) : E2D_ERR_ARG;
   if (h->freeze && cudaMemset(h->freeze, 0, sizeof(int) * h->B.ncase) != cudaSuccess) return E2D_ERR_CUDA;
   const int* saved = h->B.freeze;
   h->B.freeze = nullptr;
@@ -1382,7 +1383,8 @@ static int nks_run(e2d_handle* h, const e2d_nks_params* p, e2d_nks_step* hist, i
 // rows, as in the reference's block matrix: ghost entries pass through.
 extern "C" int e2d_block_precon_apply(e2d_handle* h, const e2d_nks_params* p, double cfl, const double* v,
                                       double* z) {
-  if (!h || !p || !v || !z || !(cfl > 0.0) || !params_ok(*p) || p->gmres_restart < 1 || p->gmres_restart > 500)
+  if (!h || !h->subs.empty() || !p || !v || !z || !(cfl > 0.0) || !params_ok(*p) || p->gmres_restart < 1 ||
+      p->gmres_restart > 500)
     return E2D_ERR_ARG;
   if (cudaSetDevice(h->device) != cudaSuccess) return E2D_ERR_CUDA;
   int rc;

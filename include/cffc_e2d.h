@@ -133,12 +133,18 @@ e2d_handle *e2d_create(const e2d_blocks_desc *desc, const e2d_scheme *scheme,
                        int device, int *err);
 
 /* One handle over ncase independent cases (each its own block set, as
- * e2d_create takes it; block counts may differ, block dimensions must not).
+ * e2d_create takes it; block counts and block dimensions may differ).
  * Their blocks are laid end to end in case order; every entry point then
  * works on all cases at once, with per-case time-step minima, residual
  * norms, histories and Newton-Krylov solves, and gives each case the same
- * result bit for bit as a handle of that case alone.  No reference
- * counterpart: the reference runs one case per process. */
+ * result bit for bit as a handle of that case alone.  Cases of different
+ * block dimensions run as one batch per block shape behind this handle; the
+ * host arrays (states, residuals, local time steps) are then each case's
+ * array in its own shape, concatenated in case order, and
+ * e2d_get_reconstruction, e2d_device_state, e2d_kernel_times and
+ * e2d_block_precon_apply are not available (E2D_ERR_ARG); e2d_stage_config
+ * reports the first shape's kernel.  No reference counterpart: the
+ * reference runs one case per process. */
 e2d_handle *e2d_create_batch(const e2d_blocks_desc *cases, int ncase, const e2d_scheme *scheme,
                              int device, int *err);
 
