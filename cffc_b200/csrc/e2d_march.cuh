@@ -53,7 +53,6 @@ namespace mk {
 constexpr int MI = E2D_MARCH_COLS, MJ = 8, CH = 7;  // interior columns; rows of a chunk (at most; default)
 constexpr int WI = MI + 4, WJ = MJ + 4, NWI = MI + 6;  // staged window (cells, node columns)
 constexpr int RCI = MI + 2, RCJ = MJ + 2;          // reconstruction slots (cols, rows j0+1..j0+10)
-constexpr int FJ = MJ + 1;                         // j-face slots (faces j0+2-1/2 .. j0+10-1/2)
 #ifndef E2D_MARCH_NBUF
 #define E2D_MARCH_NBUF 2
 #endif
