@@ -191,19 +191,28 @@ __global__ void __launch_bounds__(VT) update_x_kernel(double* __restrict__ x, co
 
 // z = Minv v per cell, and eps[case] = eps0 / ||z|| over the case; grid =
 // nblk * ch CTAs, each a chunk of a block's cells.
-__global__ void __launch_bounds__(VT) precon_apply_kernel(const double* __restrict__ Minv, const double* __restrict__ v,
+// vscale (null: none): v is first divided in place by vscale[case] (the
+// dscal by ONE/H that closes the previous Arnoldi step, GMRES2D.h:1246,
+// done here instead of in its own pass: the same product f * v).
+__global__ void __launch_bounds__(VT) precon_apply_kernel(const double* __restrict__ Minv, double* __restrict__ v,
                                                           double* __restrict__ z, int cells_per_block, int ch,
                                                           double* partial, unsigned* counter, double* eps_out,
-                                                          double eps0, Blocks B) {
+                                                          double eps0, const double* vscale, Blocks B) {
   const int blk = blockIdx.x / ch, part = blockIdx.x % ch;
   const int cs = case_id(B, blk);
   if (!case_on(B, cs)) return;
   const int len = (cells_per_block + ch - 1) / ch, r0 = part * len, r1 = min(cells_per_block, r0 + len);
+  const double f = vscale ? 1.0 / vscale[cs] : 1.0;
   double s = 0.0;
   for (int r = r0 + threadIdx.x; r < r1; r += VT) {
     const size_t c = size_t(blk) * cells_per_block + r;
-    const double2* v2 = reinterpret_cast<const double2*>(v + 4 * c);
-    const double2 va = v2[0], vb = v2[1];
+    double2* v2 = reinterpret_cast<double2*>(v + 4 * c);
+    double2 va = v2[0], vb = v2[1];
+    if (vscale) {
+      va.x = f * va.x; va.y = f * va.y; vb.x = f * vb.x; vb.y = f * vb.y;
+      v2[0] = va;
+      v2[1] = vb;
+    }
     const double* M = Minv + 16 * c;
     double o[4];
 #pragma unroll
@@ -1089,8 +1098,11 @@ int arnoldi_step(e2d_handle* h, int j, double eps0, const Norm4& nm, bool ilu) {
     if ((rc = ilu_apply(h, Vj, Zj))) return rc;
     if ((rc = dot(h, Zj, Zj, s->eps, FIN_EPS, eps0))) return rc;
   } else {
+    // v_j = w_j / h(j, j-1) for j > 0 (the previous step's closing scale,
+    // deferred into this pass; h(j, j-1) is still in the column buffer)
     precon_apply_kernel<<<h->B.nblk * s->ch_cell, VT, 0, h->stream>>>(
-        s->Minv, Vj, Zj, h->B.NCi * h->B.NCj, s->ch_cell, s->partial, s->counter, s->eps, eps0, act(h));
+        s->Minv, Vj, Zj, h->B.NCi * h->B.NCj, s->ch_cell, s->partial, s->counter, s->eps, eps0,
+        j > 0 ? s->hcol + size_t(j) * C : nullptr, act(h));
     E2D_CK(cudaGetLastError());
   }
   if ((rc = matvec(h, Zj, Vn, nm))) return rc;
@@ -1105,7 +1117,10 @@ int arnoldi_step(e2d_handle* h, int j, double eps0, const Norm4& nm, bool ilu) {
                        last ? hn : s->hcol + size_t(k + 1) * C, last ? FIN_SQRT : FIN_SUM)))
       return rc;
   }
-  if ((rc = scale(h, Vn, hn, 1.0))) return rc;
+  // v_{j+1} = w / ||w||: here for ILU(k); the block-Jacobi apply of the next
+  // step does it in its own pass (a step that ends the cycle leaves the
+  // last vector unscaled, which nothing reads)
+  if (ilu && (rc = scale(h, Vn, hn, 1.0))) return rc;
   gmres_givens_kernel<<<1, VT, 0, h->stream>>>(s->gd, s->hcol, s->active, j);
   E2D_CK(cudaGetLastError());
   return 0;
@@ -1410,7 +1425,8 @@ extern "C" int e2d_block_precon_apply(e2d_handle* h, const e2d_nks_params* p, do
     if ((rc = ilu_apply(h, s->V, s->Z))) return rc;
   } else {
     precon_apply_kernel<<<B.nblk * s->ch_cell, VT, 0, h->stream>>>(s->Minv, s->V, s->Z, B.NCi * B.NCj, s->ch_cell,
-                                                                   s->partial, s->counter, s->eps, 1.0, act(h));
+                                                                   s->partial, s->counter, s->eps, 1.0, nullptr,
+                                                                   act(h));
     E2D_CK(cudaGetLastError());
   }
   E2D_CK(cudaMemcpyAsync(z, s->Z, nb, cudaMemcpyDeviceToHost, h->stream));
