@@ -59,79 +59,91 @@ __device__ __forceinline__ double sqrt_from_rsqrt(double x, double r) {
   return fma(0.5 * r, d, s);
 }
 
-__device__ __forceinline__ double harten_delta(double la, double ll, double lr) {
-  double delta = dmax(0.0, 2.0 * (lr - ll));
-  if (fabs(la) > delta || delta < TOLER) return 0.0;
-  return 0.5 * (la * la * rcp(delta) + delta) - fabs(la);
+// Single precision counterparts for the FP32 build (compiled with the
+// approximate single-precision division and square root).
+__device__ __forceinline__ float rcp(float x) { return 1.0f / x; }
+__device__ __forceinline__ float rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ float sqrt_from_rsqrt(float x, float r) {
+  const float s = x * r;
+  const float d = fmaf(-s, s, x);
+  return fmaf(0.5f * r, d, s);
 }
 
-// FluxRoe_n in the frame of the unit normal (c, s), division-lean form.
-__device__ __forceinline__ CState<double> flux_roe_n(const PState<double>& wl0, const PState<double>& wr0,
-                                                     double c, double s, double g, double gm1,
-                                                     double gm1i) {
-  const double dl = wl0.d, pl = wl0.p, dr = wr0.d, pr = wr0.p;
-  const double ul = wl0.u * c + wl0.v * s, vl = -wl0.u * s + wl0.v * c;
-  const double ur = wr0.u * c + wr0.v * s, vr = -wr0.u * s + wr0.v * c;
-  const double rsdl = rsqrt(dl), rsdr = rsqrt(dr);
-  const double sdl = sqrt_from_rsqrt(dl, rsdl), sdr = sqrt_from_rsqrt(dr, rsdr);
-  const double cl2 = g * pl * (rsdl * rsdl), cr2 = g * pr * (rsdr * rsdr);
-  const double hl = cl2 * gm1i + 0.5 * (ul * ul + vl * vl);
-  const double hr = cr2 * gm1i + 0.5 * (ur * ur + vr * vr);
-  const double inv = rcp(sdl + sdr);
-  const double ua = (sdl * ul + sdr * ur) * inv;
-  const double va = (sdl * vl + sdr * vr) * inv;
-  const double ha = (sdl * hl + sdr * hr) * inv;
-  const double qa2 = ua * ua + va * va;
-  const double aa2 = gm1 * (ha - 0.5 * qa2);
-  const double rca = rsqrt(aa2);
-  const double ca = sqrt_from_rsqrt(aa2, rca);
-  const double da = sdl * sdr;
-  const double dW1 = ur - ul, dW3 = pr - pl;
-  const bool up = ua >= 0.0;
-  const double d = up ? dl : dr, u = up ? ul : ur, v = up ? vl : vr, p = up ? pl : pr;
-  const double h = up ? hl : hr;
-  const double du = d * u;
-  double F0 = du, F1 = du * u + p, F2 = du * v, F3 = du * h;
-  const double la0 = ua - ca, la3 = ua + ca;
+template <class T>
+__device__ __forceinline__ T harten_delta(T la, T ll, T lr) {
+  T delta = dmax(T(0), T(2) * (lr - ll));
+  if (fabs(la) > delta || delta < T(TOLER)) return T(0);
+  return T(0.5) * (la * la * rcp(delta) + delta) - fabs(la);
+}
+
+// FluxRoe_n in the frame of the unit normal (c, s), division-lean form (T =
+// double for the fast FP64 build, float for the FP32 one).
+template <class T>
+__device__ __forceinline__ CState<T> flux_roe_n(const PState<T>& wl0, const PState<T>& wr0, T c, T s, T g, T gm1,
+                                                T gm1i) {
+  const T dl = wl0.d, pl = wl0.p, dr = wr0.d, pr = wr0.p;
+  const T ul = wl0.u * c + wl0.v * s, vl = -wl0.u * s + wl0.v * c;
+  const T ur = wr0.u * c + wr0.v * s, vr = -wr0.u * s + wr0.v * c;
+  const T rsdl = rsqrt(dl), rsdr = rsqrt(dr);
+  const T sdl = sqrt_from_rsqrt(dl, rsdl), sdr = sqrt_from_rsqrt(dr, rsdr);
+  const T cl2 = g * pl * (rsdl * rsdl), cr2 = g * pr * (rsdr * rsdr);
+  const T hl = cl2 * gm1i + T(0.5) * (ul * ul + vl * vl);
+  const T hr = cr2 * gm1i + T(0.5) * (ur * ur + vr * vr);
+  const T inv = rcp(sdl + sdr);
+  const T ua = (sdl * ul + sdr * ur) * inv;
+  const T va = (sdl * vl + sdr * vr) * inv;
+  const T ha = (sdl * hl + sdr * hr) * inv;
+  const T qa2 = ua * ua + va * va;
+  const T aa2 = gm1 * (ha - T(0.5) * qa2);
+  const T rca = rsqrt(aa2);
+  const T ca = sqrt_from_rsqrt(aa2, rca);
+  const T da = sdl * sdr;
+  const T dW1 = ur - ul, dW3 = pr - pl;
+  const bool up = ua >= T(0);
+  const T d = up ? dl : dr, u = up ? ul : ur, v = up ? vl : vr, p = up ? pl : pr;
+  const T h = up ? hl : hr;
+  const T du = d * u;
+  T F0 = du, F1 = du * u + p, F2 = du * v, F3 = du * h;
+  const T la0 = ua - ca, la3 = ua + ca;
   // Harten's fix acts on a wave only where |la| <= delta = max(0, 2 (lr - ll)),
   // lr - ll = (ur - ul) -+ (cr - cl).  Since |cr - cl| <= sqrt|cr^2 - cl^2|,
   // delta <= 2 (|ur - ul| + sqrt|cr^2 - cl^2|): faces whose wave speeds
   // exceed that bound (computed in single precision with a wide margin)
   // skip the exact sound speeds.
   const float dbound = 2.0f * (float(fabs(ur - ul)) + sqrtf(float(fabs(cr2 - cl2)))) * 1.001f + 1e-30f;
-  double d0 = 0.0, d3 = 0.0;
+  T d0 = T(0), d3 = T(0);
   if (!(float(fabs(la0)) > dbound) || !(float(fabs(la3)) > dbound)) {
-    const double cl = sqrt_from_rsqrt(cl2, rsqrt(cl2)), cr = sqrt_from_rsqrt(cr2, rsqrt(cr2));
+    const T cl = sqrt_from_rsqrt(cl2, rsqrt(cl2)), cr = sqrt_from_rsqrt(cr2, rsqrt(cr2));
     d0 = harten_delta(la0, ul - cl, ur - cr);
     d3 = harten_delta(la3, ul + cl, ur + cr);
   }
   // The entropy and shear waves travel at ua itself: with the upwind side
   // taken from the sign of ua their strengths (ua -+ |ua|) / 2 are exactly
   // zero, so only the two acoustic waves can contribute.
-  double ws0, ws3;
+  T ws0, ws3;
   if (up) {
-    ws0 = 0.5 * (la0 - fabs(la0) - d0);
-    ws3 = 0.5 * (la3 - fabs(la3) - d3);
+    ws0 = T(0.5) * (la0 - fabs(la0) - d0);
+    ws3 = T(0.5) * (la3 - fabs(la3) - d3);
   } else {
-    ws0 = 0.5 * (la0 + fabs(la0) + d0);
-    ws3 = 0.5 * (la3 + fabs(la3) + d3);
+    ws0 = T(0.5) * (la0 + fabs(la0) + d0);
+    ws3 = T(0.5) * (la3 + fabs(la3) + d3);
   }
-  const double sg = up ? 1.0 : -1.0;
-  const double rca2 = rca * rca;
-  const double hdr = 0.5 * da * rca * dW1, pdr = 0.5 * rca2 * dW3;
+  const T sg = up ? T(1) : T(-1);
+  const T rca2 = rca * rca;
+  const T hdr = T(0.5) * da * rca * dW1, pdr = T(0.5) * rca2 * dW3;
   // Each wave contributes only where the reference's upwind test selects it;
   // a wave speed of exactly zero contributes nothing either way.
-  const bool on0 = up ? (ws0 < 0.0) : (ws0 > 0.0);
-  const bool on3 = up ? (ws3 < 0.0) : (ws3 > 0.0);
+  const bool on0 = up ? (ws0 < T(0)) : (ws0 > T(0));
+  const bool on3 = up ? (ws3 < T(0)) : (ws3 > T(0));
   if (on0) {
-    const double k = sg * ws0 * (pdr - hdr);
+    const T k = sg * ws0 * (pdr - hdr);
     F0 += k; F1 += k * (ua - ca); F2 += k * va; F3 += k * (ha - ua * ca);
   }
   if (on3) {
-    const double k = sg * ws3 * (pdr + hdr);
+    const T k = sg * ws3 * (pdr + hdr);
     F0 += k; F1 += k * (ua + ca); F2 += k * va; F3 += k * (ha + ua * ca);
   }
-  CState<double> R;
+  CState<T> R;
   R.d = F0;
   R.mx = F1 * c - F2 * s;
   R.my = F1 * s + F2 * c;
@@ -147,7 +159,7 @@ __device__ __forceinline__ CState<double> flux_roe_n(const PState<double>& wl0, 
 // minimum is phi at the smallest y_q, capped at 1: the smallest ratio is found
 // by cross-multiplying |a| / |b| pairs and phi is evaluated once.
 __device__ __forceinline__ double rcp_t(double x) { return rcp(x); }
-__device__ __forceinline__ float rcp_t(float x) { return 1.0f / x; }
+__device__ __forceinline__ float rcp_t(float x) { return rcp(x); }
 template <class T>
 __device__ __forceinline__ T limiter(int kind, const T* uq, T u0, T umin, T umax) {
   if (kind == E2D_LIMITER_ONE) return T(1);

@@ -263,8 +263,8 @@ template <bool ROE>
 __device__ __forceinline__ CState<RT> face_flux(int kind, const PState<RT>& wl, const PState<RT>& wr, RT nx, RT ny,
                                                 RT g, RT gm1, RT gm1i) {
   if (!ROE) return flux_n(kind, wl, wr, nx, ny, g, gm1, gm1i);
-#if defined(E2D_FAST) && !defined(E2D_FP32)
-  return fm::flux_roe_n(wl, wr, nx, ny, g, gm1, gm1i);
+#if defined(E2D_FAST)
+  return fm::flux_roe_n<RT>(wl, wr, nx, ny, g, gm1, gm1i);
 #else
   return flux_roe_n(wl, wr, nx, ny, g, gm1, gm1i);
 #endif
