@@ -89,6 +89,40 @@ def fp32_leg(bs, rk_steps, device, steps=3):
             "l2_error_vs_fp64": dict(fp32_error(bs, rk_steps, device), steps=rk_steps)}
 
 
+def exact_leg(bs, rk_steps, device, steps=2):
+    """The exact FP64 path (the reference's arithmetic, bit-identical to its
+    residual and explicit steps: tests/test_gpu_parity.py,
+    tests/test_gpu_kernels.py) on the bench workload: throughput over `steps`
+    calls of rk_steps RK2 steps, the stage kernel its handle runs and that
+    kernel's mean CUDA-event time per launch."""
+    import dataclasses
+
+    import numpy as np
+    import torch
+
+    from cffc_b200 import capi
+    bx = dataclasses.replace(bs, scheme=dataclasses.replace(bs.scheme, precision=PRECISION["exact"]))
+    h = capi.Handle(bx, device=device)
+    h.set_state()
+    rc, _ = h.rk_steps(rk_steps, history=False)
+    assert rc == 0, rc
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        rc, _ = h.rk_steps(rk_steps, history=False)
+        assert rc == 0, rc
+    secs = (time.perf_counter() - t0) / steps
+    kt = np.zeros(6)
+    h.lib.e2d_kernel_times.argtypes = [capi.C.c_void_p, capi.C.c_int, capi._dp]
+    assert h.lib.e2d_kernel_times(h.h, 10, capi.ptr(kt)) == 0
+    kind, rows, _ = h.stage_config()
+    h.close()
+    return {"value": round(bs.n_interior * rk_steps / secs * 1e-6, 3), "unit": "Mcell-updates/s",
+            "timing": "host clock around e2d_rk_steps (returns after the device finished)",
+            "stage_kernel": f"march_kernel, {rows} rows per chunk" if kind == 1 else "stage_kernel (tiled)",
+            "stage_ms": [round(kt[1], 5), round(kt[2], 5)]}
+
+
 def parity_leg(bs, device):
     """Per-cell relative error of the fast FP64 residual (the benchmarked
     kernels) against the exact FP64 path, which reproduces the reference's
@@ -804,6 +838,7 @@ def main():
         elif world == 1:
             line["fp32"] = fp32_leg(bs, args.rk_steps, local)
         if world == 1:
+            line["exact"] = exact_leg(bs, args.rk_steps, local)
             line["parity"] = parity_leg(bs, local)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(bs)

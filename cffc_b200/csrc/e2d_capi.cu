@@ -142,10 +142,11 @@ void stage_buffers(e2d_handle* h, int k, double*& W, double*& U) {
 }
 
 // The stage kernel for a stage: the column-marching kernel where the handle
-// allows it (fast and FP32 paths, Roe flux, even block width, no degenerate
-// edges), else the tiled stage kernel.
+// allows it (Roe flux, even block width, no degenerate edges) and the
+// autotuner chose it, else the tiled stage kernel.
 cudaError_t launch_stage_args(e2d_handle* h, StageArgs& a) {
-  if (h->march && h->sc.precision != E2D_PREC_FP64_EXACT && a.B.flux == E2D_FLUX_ROE) {
+  if (h->march && a.B.flux == E2D_FLUX_ROE) {
+    const bool ex = h->sc.precision == E2D_PREC_FP64_EXACT;
     const CUtensorMap* tw = nullptr;
     if (a.Win == h->B.W) tw = &h->tmW[0];
     else if (a.Win == h->B.W2) tw = &h->tmW[1];
@@ -155,9 +156,9 @@ cudaError_t launch_stage_args(e2d_handle* h, StageArgs& a) {
       memset(&m, 0, sizeof(m));
       m.a = a;
       m.tmW = *tw;
-      m.tmG = h->tmG;
+      m.tmG = ex ? h->tmGx : h->tmG;
       m.tmN = h->tmN;
-      m.geom = h->geom;
+      m.geom = ex ? h->geomx : h->geom;
       m.mask = h->gmask;
       m.bcside = h->bcside;
       // update inputs by TMA: explicit stages over U or U2 whose second
@@ -168,8 +169,8 @@ cudaError_t launch_stage_args(e2d_handle* h, StageArgs& a) {
         m.upd = 1;
         m.tmU = a.Ubase == h->B.U ? h->tmU[0] : h->tmU[1];
         m.tmR = h->tmR;
-        m.tmGA = h->tmGA;
-        m.tmGF = h->tmGF;
+        m.tmGA = ex ? h->tmGAx : h->tmGA;
+        m.tmGF = ex ? h->tmGFx : h->tmGF;
       }
       const int mi = fast::march_strip_cols();
       m.strips = (h->B.nci + mi - 1) / mi;
@@ -177,6 +178,7 @@ cudaError_t launch_stage_args(e2d_handle* h, StageArgs& a) {
       m.cps = fast::march_chunks(h->B.ncj, m.ch);
       m.nchunk = (long long)m.strips * m.cps * h->B.nblk;
       const int grid = int(std::min<long long>(m.nchunk, h->march_grid));
+      if (ex) return exact::launch_march(m, grid, h->stream);
       return h->sc.precision == E2D_PREC_FP32 ? f32::launch_march(m, grid, h->stream)
                                               : fast::launch_march(m, grid, h->stream);
     }
@@ -226,8 +228,7 @@ bool encode3(CUtensorMap* map, void* base, uint64_t d0, uint64_t d1, uint64_t d2
 // Geometry, padded nodes and tensor maps of the marching kernel.  The handle
 // keeps the tiled stage kernel when the marching kernel does not apply:
 // another flux function, an odd block width (row strides of the tensor maps
-// must be multiples of 16 bytes) or a degenerate edge (and the exact path
-// always uses the tiled kernel).
+// must be multiples of 16 bytes) or a degenerate edge.
 int setup_march(e2d_handle* h) {
   h->march = h->march_ok = false;
   if (h->sc.flux != E2D_FLUX_ROE) return 0;
@@ -237,12 +238,16 @@ int setup_march(e2d_handle* h) {
   const int NNp = B.NNi + 1;  // NNi is odd for an even NCi
   int rc;
   int* degenerate = nullptr;
-  if ((rc = dalloc(h, &h->geom, size_t(GEOM_NF) * h->ncell)) || (rc = dalloc(h, &h->gmask, h->ncell)) ||
+  if ((rc = dalloc(h, &h->geom, size_t(GEOM_NF) * h->ncell)) || (rc = dalloc(h, &h->geomx, size_t(GEOM_NF) * h->ncell)) ||
+      (rc = dalloc(h, &h->gmask, h->ncell)) ||
       (rc = dalloc(h, &h->bcside, B.nblk)) || (rc = dalloc(h, &h->nodes_pad, size_t(B.nblk) * 2 * B.NNj * NNp)) ||
       (rc = dalloc(h, &degenerate, 1)))
     return rc;
   CK(cudaMemsetAsync(degenerate, 0, sizeof(int), h->stream));
   CK(cudaMemsetAsync(h->nodes_pad, 0, sizeof(double) * size_t(B.nblk) * 2 * B.NNj * NNp, h->stream));
+  // the exact build's geometry first: the fast one then writes the same mask,
+  // side bits and padded nodes again, and both flag degenerate edges
+  CK(exact::launch_geometry(B, h->geomx, h->gmask, h->bcside, degenerate, NNp, h->nodes_pad, h->stream));
   CK(fast::launch_geometry(B, h->geom, h->gmask, h->bcside, degenerate, NNp, h->nodes_pad, h->stream));
   int deg = 0;
   CK(cudaMemcpyAsync(&deg, degenerate, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -252,6 +257,7 @@ int setup_march(e2d_handle* h) {
   bool ok = encode3(&h->tmW[0], B.W, B.NCi, B.NCj, 4ull * B.nblk, wi, wj, 4) &&
             encode3(&h->tmW[1], B.W2, B.NCi, B.NCj, 4ull * B.nblk, wi, wj, 4) &&
             encode3(&h->tmG, h->geom, B.NCi, B.NCj, uint64_t(GEOM_NF) * B.nblk, wi, wj, G_K2 + 1) &&
+            encode3(&h->tmGx, h->geomx, B.NCi, B.NCj, uint64_t(GEOM_NF) * B.nblk, wi, wj, G_K2 + 1) &&
             encode3(&h->tmN, h->nodes_pad, NNp, B.NNj, 2ull * B.nblk, nwi, wj, 2);
   if (ok && h->W3) ok = encode3(&h->tmW[2], h->W3, B.NCi, B.NCj, 4ull * B.nblk, wi, wj, 4);
   if (!ok) return 0;
@@ -262,8 +268,11 @@ int setup_march(e2d_handle* h) {
               encode3(&h->tmU[1], B.U2, B.NCi, B.NCj, 4ull * B.nblk, mi, mj, 4) &&
               encode3(&h->tmR, B.dUdt, B.NCi, B.NCj, 4ull * B.nblk, mi, mj, 4) &&
               encode3(&h->tmGA, h->geom, B.NCi, B.NCj, uint64_t(GEOM_NF) * B.nblk, mi, mj, 1) &&
-              encode3(&h->tmGF, h->geom, B.NCi, B.NCj, uint64_t(GEOM_NF) * B.nblk, mi, mj, GEOM_NF - G_RA);
-  const int per_sm = std::min(f32::march_ctas_per_sm(), fast::march_ctas_per_sm());
+              encode3(&h->tmGF, h->geom, B.NCi, B.NCj, uint64_t(GEOM_NF) * B.nblk, mi, mj, GEOM_NF - G_RA) &&
+              encode3(&h->tmGAx, h->geomx, B.NCi, B.NCj, uint64_t(GEOM_NF) * B.nblk, mi, mj, 1) &&
+              encode3(&h->tmGFx, h->geomx, B.NCi, B.NCj, uint64_t(GEOM_NF) * B.nblk, mi, mj, GEOM_NF - G_RA);
+  const int per_sm =
+      std::min(std::min(f32::march_ctas_per_sm(), fast::march_ctas_per_sm()), exact::march_ctas_per_sm());
   int sms = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
   if (per_sm < 1 || sms < 1) return 0;
@@ -304,7 +313,7 @@ __global__ void uniform_state_kernel(Blocks B, long long ncell) {
   }
 }
 
-// Tunes one precision of the fast family (FP64 or FP32) into sel_*[prec].
+// Tunes one precision into sel_*[prec].
 int autotune_precision(e2d_handle* h, int prec) {
   const TuneKey key{h->B.nci, h->B.ncj, h->B.nblk, prec};
   {
@@ -367,7 +376,7 @@ int autotune_precision(e2d_handle* h, int prec) {
 // The kernel of the handle's current precision.
 void apply_selection(e2d_handle* h) {
   const int p = h->sc.precision;
-  if (!h->march_ok || p == E2D_PREC_FP64_EXACT) {
+  if (!h->march_ok) {
     h->march = false;
     return;
   }
@@ -376,17 +385,17 @@ void apply_selection(e2d_handle* h) {
   h->tune_us = h->sel_us[p];
 }
 
-// Both fast precisions are tuned when the handle is created (a handle may
-// switch between them, e2d_set_precision) on a uniform state in (W2, U2); the
-// state arrays are cleared afterwards.
+// Every precision is tuned when the handle is created (a handle may switch
+// between them, e2d_set_precision) on a uniform state in (W2, U2); the state
+// arrays are cleared afterwards.
 int autotune_stage(e2d_handle* h) {
   if (!h->march_ok) return 0;
   // "tiled" / "march": one kernel without tuning (tests and comparisons of
   // the two kernels; "march" with its default rows per chunk)
   const char* kind = getenv("CFFC_E2D_STAGE_KERNEL");
   if (kind && (strcmp(kind, "tiled") == 0 || strcmp(kind, "march") == 0)) {
-    h->sel_march[0] = h->sel_march[1] = strcmp(kind, "march") == 0;
-    h->sel_rows[0] = h->sel_rows[1] = fast::march_chunk_rows();
+    h->sel_march[0] = h->sel_march[1] = h->sel_march[2] = strcmp(kind, "march") == 0;
+    h->sel_rows[0] = h->sel_rows[1] = h->sel_rows[2] = fast::march_chunk_rows();
     apply_selection(h);
     return 0;
   }
@@ -398,7 +407,9 @@ int autotune_stage(e2d_handle* h) {
   CK(cudaGetLastError());
   CK(cudaMemsetAsync(h->hist, 0, sizeof(double) * 4 * size_t(h->hist_cap) * h->B.ncase, h->stream));
   int rc;
-  if ((rc = autotune_precision(h, E2D_PREC_FP64)) || (rc = autotune_precision(h, E2D_PREC_FP32))) return rc;
+  if ((rc = autotune_precision(h, E2D_PREC_FP64)) || (rc = autotune_precision(h, E2D_PREC_FP32)) ||
+      (rc = autotune_precision(h, E2D_PREC_FP64_EXACT)))
+    return rc;
   apply_selection(h);
   // the handle starts from a clean slate
   const size_t nb = sizeof(double) * 4 * h->ncell;

@@ -3,5 +3,10 @@
 // Also holds the ghost-fill, time-step and norm kernels, which every
 // precision path shares.
 #define E2D_NS exact
+// marching kernel: one staging buffer and the update inputs by TMA, as in
+// the fast builds
+#define E2D_MARCH_NBUF 1
+#define E2D_MARCH_UPD 1
 #include "e2d_stage.cuh"
 #include "e2d_aux.cuh"
+#include "e2d_march.cuh"

@@ -34,11 +34,13 @@ struct e2d_handle {
   int *freeze = nullptr, *first = nullptr;
   double* smooth_scratch = nullptr;
   size_t smooth_smem = 0;
-  // column-marching stage kernel of the fast and FP32 paths: per-cell
-  // geometry, padded nodes, tensor maps of the stage inputs (W, W2, W3), the
-  // geometry and the nodes, and the persistent grid size
+  // column-marching stage kernel: per-cell geometry (the fast builds' and
+  // the exact build's), padded nodes, tensor maps of the stage inputs (W, W2,
+  // W3), the geometry and the nodes, and the persistent grid size
   bool march = false;
   double* geom = nullptr;
+  double* geomx = nullptr;
+  CUtensorMap tmGx, tmGAx, tmGFx;  // the exact build's geometry: window, update inputs
   unsigned char* gmask = nullptr;
   unsigned char* bcside = nullptr;  // per block: sides with face-setting BCs (marching kernel)
   // A batch whose cases have different block shapes holds no blocks of its
@@ -57,10 +59,11 @@ struct e2d_handle {
   int march_rows = 7;  // rows of a chunk
   double tune_us = 0.0;  // the autotuner's time of one explicit stage with the chosen kernel
   bool march_ok = false;  // geometry and tensor maps set up
-  // the autotuner's choice per fast precision (E2D_PREC_FP64, E2D_PREC_FP32)
-  bool sel_march[2] = {false, false};
-  int sel_rows[2] = {7, 7};
-  double sel_us[2] = {0.0, 0.0};
+  // the autotuner's choice per precision (E2D_PREC_FP64, E2D_PREC_FP32,
+  // E2D_PREC_FP64_EXACT)
+  bool sel_march[3] = {false, false, false};
+  int sel_rows[3] = {7, 7, 7};
+  double sel_us[3] = {0.0, 0.0, 0.0};
   // captured explicit step
   cudaGraphExec_t step_graph = nullptr;
   e2d_nks_state* nks = nullptr;

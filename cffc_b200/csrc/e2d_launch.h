@@ -11,6 +11,11 @@ cudaError_t launch_stage(const StageArgs& a, cudaStream_t st);
 size_t stage_smem_bytes();
 int tile_i();
 int tile_j();
+// column-marching stage kernel in the reference's arithmetic and its geometry
+cudaError_t launch_march(const MarchArgs& m, int grid, cudaStream_t st);
+int march_ctas_per_sm();
+cudaError_t launch_geometry(const Blocks& B, double* geom, unsigned char* mask, unsigned char* bcside, int* degenerate,
+                            int NNp, double* nodes_pad, cudaStream_t st);
 }  // namespace exact
 namespace fast {
 cudaError_t launch_stage(const StageArgs& a, cudaStream_t st);

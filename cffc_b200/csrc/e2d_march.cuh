@@ -34,8 +34,17 @@
 //   once per handle (e2d_march_args.h); face normals and lengths come from
 //   the staged nodes with one reciprocal square root per face.
 //
+// The exact build (no E2D_FAST, compiled without FMA contraction) restates
+// the reference's arithmetic instead: the least-squares sums averaged over
+// the stencil and divided by the determinant, the limiter over the face-point
+// values, IEEE division and square root, the Roe flux of e2d_device.cuh, and
+// each face's flux times its length divided by the area in the reference's
+// order (so the faces keep flux and length apart).  Its per-handle geometry
+// holds the quantities the reference computes from the grid alone, in its
+// order (e2d_march_args.h), and its results equal stage_kernel's bit for bit.
+//
 // Used when the block set allows it (even nci, no degenerate edges, the Roe
-// flux); stage_kernel covers every other case and the exact path.
+// flux); stage_kernel covers every other case.
 #pragma once
 #include "e2d_march_args.h"
 #include "e2d_tc.cuh"
@@ -116,6 +125,9 @@ struct Smem {
   RT px[RR][4][RCI], py[RR][4][RCI];    // phi * gradient of the reconstructed cells
   double Fi[MJ][4][MI + 1];             // i-face flux x length, faces I-1/2, I = i0+2 .. i0+34
   double Fj[RR][4][MI];                 // j-face flux x length, face row J (face J-1/2)
+#ifndef E2D_FAST
+  double li[MJ][MI + 1], lj[RR][MI];    // exact build: face lengths (Fi, Fj hold the bare fluxes)
+#endif
   double red[4][NWARP];
   uint64_t full[2];
   uint64_t fullu;  // the update inputs
@@ -221,6 +233,8 @@ __device__ __forceinline__ void recon_cell(const MarchArgs& m, Smem& s, const Ti
     return;
   }
   const int wi = c + 1, wj = sl + 1;
+  // fast builds: the least-squares inverse; exact build: the averaged sums
+  // DxDx, DxDy, DyDy of the stencil
   const RT K0 = RT(T.G[G_K0][wj][wi]), K1 = RT(T.G[G_K1][wj][wi]), K2 = RT(T.G[G_K2][wj][wi]);
   const double xc0 = T.G[0][wj][wi], yc0 = T.G[1][wj][wi];
   RT w0[4], Sx[4], Sy[4], mn[4], mx[4];
@@ -262,6 +276,7 @@ __device__ __forceinline__ void recon_cell(const MarchArgs& m, Smem& s, const Ti
   const RT ofy[4] = {RT(HALF * (y10 + y11) - yc0), RT(HALF * (y00 + y01) - yc0), RT(HALF * (y01 + y11) - yc0),
                      RT(HALF * (y00 + y10) - yc0)};
   const int rs = rslot(k, sl);
+#ifdef E2D_FAST
   if (!frozen && !B.freeze && !B.dWdx && B.limiter == E2D_LIMITER_VENKATAKRISHNAN) {
     // the common case (uniform): Venkatakrishnan, no freezing, no export
 #pragma unroll
@@ -277,18 +292,44 @@ __device__ __forceinline__ void recon_cell(const MarchArgs& m, Smem& s, const Ti
     }
     return;
   }
+#else
+  // the reference's sums are averages over the stencil's n points (x / 8 and
+  // x * 0.125 round alike: both are the correctly rounded x / 8)
+  const int np = __popc(msk);
+  if (np == 8) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) { Sx[v] = Sx[v] * 0.125; Sy[v] = Sy[v] * 0.125; }
+  } else {
+    const double dn = double(np);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) { Sx[v] = Sx[v] / dn; Sy[v] = Sy[v] / dn; }
+  }
+  const double det = K0 * K2 - K1 * K1;
+#endif
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
+#ifdef E2D_FAST
     const RT gx = Sx[v] * K0 + Sy[v] * K1;
     const RT gy = Sx[v] * K1 + Sy[v] * K2;
     RT dq[4];  // unlimited change from the centroid to each face point
 #pragma unroll
     for (int q = 0; q < 4; ++q) dq[q] = gx * ofx[q] + gy * ofy[q];
+#else
+    const double gx = (Sx[v] * K2 - Sy[v] * K1) / det;
+    const double gy = (Sy[v] * K0 - Sx[v] * K1) / det;
+    double uq[4];  // unlimited state at each face point
+#pragma unroll
+    for (int q = 0; q < 4; ++q) uq[q] = w0[v] + gx * ofx[q] + gy * ofy[q];
+#endif
     RT phi;
     if (frozen) {
       phi = RT(B.phi_keep[cell_var(B, k.b, v, J, I)]);
     } else {
+#ifdef E2D_FAST
       phi = fm::limiter_diff<RT>(B.limiter, dq, mn[v] - w0[v], mx[v] - w0[v]);
+#else
+      phi = limiter(B.limiter, uq, w0[v], mn[v], mx[v]);
+#endif
       if (B.freeze) B.phi_keep[cell_var(B, k.b, v, J, I)] = double(phi);
     }
     s.px[rs][v][c] = phi * gx;
@@ -309,10 +350,16 @@ __device__ __forceinline__ FaceGeo face_geo(double ax, double ay, double cx, dou
   FaceGeo f;
   const double dx = ax - cx, dy = ay - cy;
   const double q = dx * dx + dy * dy;
+#ifdef E2D_FAST
   const double rn = fm::rsqrt(q);
   f.l = fm::sqrt_from_rsqrt(q, rn);
   f.nx = dy * rn;
   f.ny = -dx * rn;
+#else
+  f.l = sqrt(q);
+  f.nx = dy / f.l;
+  f.ny = -dx / f.l;
+#endif
   f.mx = HALF * (cx + ax);
   f.my = HALF * (cy + ay);
   return f;
@@ -332,6 +379,9 @@ __device__ __forceinline__ void face(const MarchArgs& m, Smem& s, const Tile& T,
   int aj, ai, cj, ci;  // window row and node column of the edge's ends a -> c
   double* out;         // flux x length, variable v at out[v * vs]
   int vs;
+#ifndef E2D_FAST
+  double* lout;        // exact build: the face length (out holds the bare flux)
+#endif
   int bcl = E2D_BC_NONE, bcr = E2D_BC_NONE;  // face-setting BC on the left (W, S) / right (E, N) edge
   const double *wol = nullptr, *wor = nullptr;
   int wlen = 0, widx = 0;
@@ -345,6 +395,9 @@ __device__ __forceinline__ void face(const MarchArgs& m, Smem& s, const Tile& T,
     aj = r + 3; ai = q + 2; cj = r + 2; ci = q + 2;
     out = &s.Fi[r][0][q];
     vs = MI + 1;
+#ifndef E2D_FAST
+    lout = &s.li[r][q];
+#endif
     if (BC) {  // BC codes matter at the block's west and east faces only
       if (I == NG) bcl = B.bcw[size_t(k.b) * B.NCj + J];
       if (I == B.nci + NG) bcr = B.bce[size_t(k.b) * B.NCj + J];
@@ -360,6 +413,9 @@ __device__ __forceinline__ void face(const MarchArgs& m, Smem& s, const Tile& T,
     aj = sl + 2; ai = q + 2; cj = sl + 2; ci = q + 3;
     out = &s.Fj[fslot(k, sl)][0][q];
     vs = MI;
+#ifndef E2D_FAST
+    lout = &s.lj[fslot(k, sl)][q];
+#endif
     if (BC) {
       if (J == NG) bcl = B.bcs[size_t(k.b) * B.NCi + I];
       if (J == B.ncj + NG) bcr = B.bcn[size_t(k.b) * B.NCi + I];
@@ -382,10 +438,18 @@ __device__ __forceinline__ void face(const MarchArgs& m, Smem& s, const Tile& T,
     wr = fstate(s, T, k, rs, rc, f.mx, f.my);
   }
   const CState<RT> F = face_flux<true>(B.flux, wl, wr, RT(f.nx), RT(f.ny), g, gm1, gm1i);
+#ifdef E2D_FAST
   out[0] = double(F.d) * f.l;
   out[vs] = double(F.mx) * f.l;
   out[2 * vs] = double(F.my) * f.l;
   out[3 * vs] = double(F.E) * f.l;
+#else
+  out[0] = F.d;
+  out[vs] = F.mx;
+  out[2 * vs] = F.my;
+  out[3 * vs] = F.E;
+  *lout = f.l;
+#endif
 }
 
 // Contributions of the CTA's cells to the next step's CFL minimum and
@@ -427,7 +491,18 @@ __device__ __forceinline__ double e_times_d2(const CState<double>& u) {
   return u.E * u.d - 0.5 * (u.mx * u.mx + u.my * u.my);
 }
 __device__ __forceinline__ bool not_positive(const CState<double>& u) {
+#ifdef E2D_FAST
   return u.d <= 0.0 || u.E <= 0.0 || e_times_d2(u) <= 0.0;
+#else
+  return u.d <= 0.0 || u.E <= 0.0 || e_of_U(u) <= 0.0;
+#endif
+}
+__device__ __forceinline__ bool positive(const CState<double>& u) {
+#ifdef E2D_FAST
+  return u.d > 0.0 && u.E > 0.0 && e_times_d2(u) > 0.0;
+#else
+  return u.d > 0.0 && u.E > 0.0 && e_of_U(u) > 0.0;
+#endif
 }
 
 // dtg: the case's global time step of this explicit step (modes 1, 2 with
@@ -452,10 +527,13 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
   const double* gp = m.geom + size_t(k.b) * GEOM_NF * plane + off;
   const bool su = PLAIN || up != nullptr;  // update inputs in shared memory
   const bool ldt = !PLAIN && B.local_dt;
-  const double rA = su ? up->G[0][r][q] : gp[G_RA * plane];
+  // plane G_RA: 1 / A (fast builds), A (exact build)
+  const double gA = su ? up->G[0][r][q] : gp[G_RA * plane];
   double kk = 1.0;
   if (MODE == 1 || MODE == 2) kk = B.cfl * (ldt ? B.dt[c] : dtg);
-  const double kA = kk * rA;
+#ifdef E2D_FAST
+  const double kA = kk * gA;
+#endif
   const int fs = fslot(k, r), fn = fslot(k, r + 1);
   double res[4];
 #pragma unroll
@@ -466,10 +544,25 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
       d = su ? up->R[v][r][q] : a.res_out[qv];
       if (!PLAIN && a.acc1) d = d + 2.0 * a.acc1[qv] + 2.0 * a.acc2[qv];
     }
+#ifdef E2D_FAST
     d += s.Fi[r][v][q] * kA;
     d -= s.Fi[r][v][q + 1] * kA;
     d += s.Fj[fs][v][q] * kA;
     d -= s.Fj[fn][v][q] * kA;
+#else
+    // faces W, E, S, N: (k F) l / A each, in the reference's order
+    if (MODE == 1 || MODE == 2) {
+      d += kk * s.Fi[r][v][q] * s.li[r][q] / gA;
+      d -= kk * s.Fi[r][v][q + 1] * s.li[r][q + 1] / gA;
+      d += kk * s.Fj[fs][v][q] * s.lj[fs][q] / gA;
+      d -= kk * s.Fj[fn][v][q] * s.lj[fn][q] / gA;
+    } else {
+      d += s.Fi[r][v][q] * s.li[r][q] / gA;
+      d -= s.Fi[r][v][q + 1] * s.li[r][q + 1] / gA;
+      d += s.Fj[fs][v][q] * s.lj[fs][q] / gA;
+      d -= s.Fj[fn][v][q] * s.lj[fn][q] / gA;
+    }
+#endif
     res[v] = d;
   }
   if (MODE == 0) {
@@ -515,7 +608,7 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
           for (int v = 0; v < 4; ++v) res[v] = rrf * res[v];
           u.d = uo.d + omega * res[0]; u.mx = uo.mx + omega * res[1];
           u.my = uo.my + omega * res[2]; u.E = uo.E + omega * res[3];
-          if (u.d > 0.0 && u.E > 0.0 && e_times_d2(u) > 0.0) break;
+          if (positive(u)) break;
         }
         B.dt[c] = dtc;
         if (not_positive(u)) set_status(B.status, ST_NEGATIVE, int(c));
@@ -523,22 +616,35 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
     }
 #pragma unroll
     for (int v = 0; v < 4; ++v) a.res_out[c0 + v * plane] = res[v];
+#ifdef E2D_FAST
     // W(U) (fm::W_of_U) with its reciprocal density kept for the CFL step
     const double rd = fm::rcp(u.d);
     PState<double> w;
     w.d = u.d; w.u = u.mx * rd; w.v = u.my * rd;
     w.p = gm1 * (u.E - 0.5 * (u.mx * u.mx + u.my * u.my) * rd);
+#else
+    const PState<double> w = W_of_U(u, gm1);
+#endif
     a.Uout[c0] = u.d; a.Uout[c0 + plane] = u.mx; a.Uout[c0 + 2 * plane] = u.my; a.Uout[c0 + 3 * plane] = u.E;
     a.Wout[c0] = w.d; a.Wout[c0 + plane] = w.u; a.Wout[c0 + 2 * plane] = w.v; a.Wout[c0 + 3 * plane] = w.p;
     if (FUSE) {
       // CFL of the updated cell (Euler2DQuadSingleBlock.cc:3019-3080)
       auto geo = [&](int f) { return su ? up->G[f - G_RA][r][q] : gp[f * plane]; };
+#ifdef E2D_FAST
       const double v_i = w.u * geo(G_VIX) + w.v * geo(G_VIY);
       const double v_j = w.u * geo(G_VJX) + w.v * geo(G_VJY);
       const double c2 = g * w.p * rd;
       const double snd = fm::sqrt_from_rsqrt(c2, fm::rsqrt(c2));
       const double ti = geo(G_DI) * fm::rcp(snd + fabs(v_i));
       const double tj = geo(G_DJ) * fm::rcp(snd + fabs(v_j));
+#else
+      // v_i = v.(n_E - n_W)/2, v_j = v.(n_N - n_S)/2; d_i / (a + |v_i|)
+      const double v_i = HALF * (w.u * geo(G_VIX) + w.v * geo(G_VIY));
+      const double v_j = HALF * (w.u * geo(G_VJX) + w.v * geo(G_VJY));
+      const double snd = a_of(w, g);
+      const double ti = geo(G_DI) / (snd + fabs(v_i));
+      const double tj = geo(G_DJ) / (snd + fabs(v_j));
+#endif
       const double dtc = dmin(ti, tj);
       if (ldt) B.dt[c] = dtc;
       dt_next = dmin(dt_next, dtc);
@@ -804,22 +910,34 @@ int march_chunks(int ncj, int ch) {
 }  // namespace E2D_NS
 }  // namespace e2d
 
-#if defined(E2D_FAST) && !defined(E2D_FP32)
-// ---- per-handle geometry of the marching kernel (fast-path arithmetic) ------
+#if !defined(E2D_FP32)
+// ---- per-handle geometry of the marching kernel ------------------------------
+// (the FP32 build shares the fast FP64 build's; the exact build computes its
+// own planes with the reference's arithmetic)
 namespace e2d {
 namespace E2D_NS {
 namespace mk {
 
 __device__ __forceinline__ void cell_geo(const Blocks& B, int b, int I, int J, double& xc, double& yc, double& A) {
+#ifdef E2D_FAST
   fm::quad_centroid(B.X[node_ix(B, b, J, I)], B.Y[node_ix(B, b, J, I)], B.X[node_ix(B, b, J, I + 1)],
                     B.Y[node_ix(B, b, J, I + 1)], B.X[node_ix(B, b, J + 1, I + 1)], B.Y[node_ix(B, b, J + 1, I + 1)],
                     B.X[node_ix(B, b, J + 1, I)], B.Y[node_ix(B, b, J + 1, I)], xc, yc, A);
+#else
+  quad_centroid(B.X[node_ix(B, b, J, I)], B.Y[node_ix(B, b, J, I)], B.X[node_ix(B, b, J, I + 1)],
+                B.Y[node_ix(B, b, J, I + 1)], B.X[node_ix(B, b, J + 1, I + 1)], B.Y[node_ix(B, b, J + 1, I + 1)],
+                B.X[node_ix(B, b, J + 1, I)], B.Y[node_ix(B, b, J + 1, I)], xc, yc, A);
+#endif
 }
 __device__ __forceinline__ double node_len(const Blocks& B, int b, int ai, int aj, int ci, int cj) {
   const double dx = B.X[node_ix(B, b, aj, ai)] - B.X[node_ix(B, b, cj, ci)];
   const double dy = B.Y[node_ix(B, b, aj, ai)] - B.Y[node_ix(B, b, cj, ci)];
   const double q = dx * dx + dy * dy;
+#ifdef E2D_FAST
   return fm::sqrt_from_rsqrt(q, fm::rsqrt(q));
+#else
+  return sqrt(q);
+#endif
 }
 
 // One thread per cell (ghosts included): centroid; for ring cells the
@@ -865,33 +983,62 @@ __global__ void geometry_kernel(Blocks B, double* geom, unsigned char* mask, int
     }
     mask[t] = (unsigned char)m;
     if (m) {
+#ifdef E2D_FAST
       const double rdet = fm::rcp(DxDx * DyDy - DxDy * DxDy);
       gp[G_K0 * plane] = DyDy * rdet;
       gp[G_K1 * plane] = -DxDy * rdet;
       gp[G_K2 * plane] = DxDx * rdet;
+#else
+      // the sums averaged over the stencil's points, as the reference
+      // divides them (Euler2DQuadSingleBlock.cc:4010-4019)
+      const double dn = double(__popc(m));
+      gp[G_K0 * plane] = DxDx / dn;
+      gp[G_K1 * plane] = DxDy / dn;
+      gp[G_K2 * plane] = DyDy / dn;
+#endif
     }
     if (I >= NG && I <= B.nci + 1 && J >= NG && J <= B.ncj + 1) {
+#ifdef E2D_FAST
       gp[G_RA * plane] = fm::rcp(A);
       gp[G_DI * plane] = 2.0 * A * fm::rcp(lE + lW);
       gp[G_DJ * plane] = 2.0 * A * fm::rcp(lN + lS);
+#else
+      gp[G_RA * plane] = A;
+      gp[G_DI * plane] = 2.0 * (A / (lE + lW));
+      gp[G_DJ * plane] = 2.0 * (A / (lN + lS));
+#endif
       // outward unit normals nfaceE/W/N/S of the cell (edges a -> c:
       // (dy, -dx) / |d|, d = a - c)
       auto nrm = [&](int ai, int aj, int ci, int cj, double& nx, double& ny) {
         const double dx = B.X[node_ix(B, b, aj, ai)] - B.X[node_ix(B, b, cj, ci)];
         const double dy = B.Y[node_ix(B, b, aj, ai)] - B.Y[node_ix(B, b, cj, ci)];
+#ifdef E2D_FAST
         const double rn = fm::rsqrt(dx * dx + dy * dy);
         nx = dy * rn;
         ny = -dx * rn;
+#else
+        const double n = sqrt(dx * dx + dy * dy);
+        nx = dy / n;
+        ny = -dx / n;
+#endif
       };
       double eX, eY, wX, wY, nX, nY, sX, sY;
       nrm(I + 1, J + 1, I + 1, J, eX, eY);
       nrm(I, J, I, J + 1, wX, wY);
       nrm(I, J + 1, I + 1, J + 1, nX, nY);
       nrm(I + 1, J, I, J, sX, sY);
+#ifdef E2D_FAST
       gp[G_VIX * plane] = HALF * (eX - wX);
       gp[G_VIY * plane] = HALF * (eY - wY);
       gp[G_VJX * plane] = HALF * (nX - sX);
       gp[G_VJY * plane] = HALF * (nY - sY);
+#else
+      // the differences alone: the stage halves their dot product with v
+      gp[G_VIX * plane] = eX - wX;
+      gp[G_VIY * plane] = eY - wY;
+      gp[G_VJX * plane] = nX - sX;
+      gp[G_VJY * plane] = nY - sY;
+#endif
     }
   }
 }

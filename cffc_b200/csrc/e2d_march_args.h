@@ -1,8 +1,9 @@
 // e2d_march_args.h — arguments of the column-marching stage kernel
 // (e2d_march.cuh) and the layout of the per-cell geometry it streams.
 //
-// Geometry (computed once per handle from the nodes, fast-path arithmetic):
-// an array [nblk][GEOM_NF][NCj][NCi] of doubles holding, per cell,
+// Geometry (computed once per handle from the nodes): an array
+// [nblk][GEOM_NF][NCj][NCi] of doubles holding, per cell, in the fast
+// builds' arithmetic
 //   0, 1  centroid xc, yc                         (every cell, ghosts included)
 //   2..4  least-squares inverse K0, K1, K2         (ring cells: the interior and
 //         one ghost layer); the gradient of a variable is
@@ -12,6 +13,11 @@
 //   6, 7  2 A / (lE + lW), 2 A / (lN + lS)          (interior cells, CFL step)
 //   8..11 (n_E - n_W) / 2 and (n_N - n_S) / 2, x then y, with the cell's own
 //         outward unit normals                      (interior cells, CFL step)
+// and, for the exact build (a second array of the same layout), the
+// quantities the reference derives from the grid alone, in its arithmetic:
+// planes 2..4 the averaged sums DxDx / n, DxDy / n, DyDy / n of the stencil,
+// plane 5 the area A, planes 6, 7 2 (A / (lE + lW)) and 2 (A / (lN + lS)),
+// planes 8..11 the normal differences n_E - n_W and n_N - n_S (not halved);
 // and a byte per cell naming the stencil's neighbours: bit k set when
 // neighbour k of (-1,-1) (0,-1) (1,-1) (-1,0) (1,0) (-1,1) (0,1) (1,1)
 // belongs to the least-squares stencil (the reference's stencils are all
