@@ -18,7 +18,9 @@
 namespace e2d {
 
 constexpr int AUX_THREADS = 256;
-constexpr int GHOST_THREADS = 1024;  // most threads of a ghost-fill CTA
+// most threads of a ghost-fill CTA; two such CTAs fit an SM (at most 56
+// registers a thread), so a launch over 256 blocks runs in one wave
+constexpr int GHOST_THREADS = 576;
 constexpr double MILLION = 1000000.0;
 
 // One edge-cell of the W or E (vertical) boundary: side 0 = W, 1 = E.
@@ -98,7 +100,7 @@ __device__ void bc_horizontal(const Blocks& B, int b, int i, int side) {
 // 8 neighbours and the block's BC codes are read together up front; a block
 // whose edges all have code BC_NONE (every edge exchanged) stops after the
 // exchange.
-__global__ void __launch_bounds__(GHOST_THREADS) ghost_fill_kernel(Blocks B) {
+__global__ void __launch_bounds__(GHOST_THREADS, 2) ghost_fill_kernel(Blocks B) {
   const int b = blockIdx.x;
   const int ICl = NG, ICu = B.nci + NG - 1, JCl = NG, JCu = B.ncj + NG - 1;
   __shared__ int failed, nb[8];
