@@ -51,7 +51,7 @@ def _newer(target, deps):
 def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in HEADERS]
-    objs = []
+    objs, cmds = [], []
     for src, flags in SOURCES.items():
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
@@ -62,7 +62,15 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
                 cmd += ["-Xptxas", "-v"]
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
+    # the translation units compile independently: run them side by side
+    # (the marching-kernel units dominate; one process each)
+    from concurrent.futures import ThreadPoolExecutor
+    workers = max(1, min(len(cmds), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        for r in list(pool.map(lambda c: subprocess.run(c), cmds)):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     # C++ host layer (include/cffc_euler2d.hpp): plain host code, without
     # contraction so the restart files' cell geometry is the reference's
     inc = os.path.join(ROOT_DIR, "include")
