@@ -142,10 +142,10 @@ void stage_buffers(e2d_handle* h, int k, double*& W, double*& U) {
 }
 
 // The stage kernel for a stage: the column-marching kernel where the handle
-// allows it (Roe flux, even block width, no degenerate edges) and the
-// autotuner chose it, else the tiled stage kernel.
+// allows it (even block width, no degenerate edges) and the autotuner chose
+// it, else the tiled stage kernel.
 cudaError_t launch_stage_args(e2d_handle* h, StageArgs& a) {
-  if (h->march && a.B.flux == E2D_FLUX_ROE) {
+  if (h->march) {
     const bool ex = h->sc.precision == E2D_PREC_FP64_EXACT;
     const CUtensorMap* tw = nullptr;
     if (a.Win == h->B.W) tw = &h->tmW[0];
@@ -226,12 +226,11 @@ bool encode3(CUtensorMap* map, void* base, uint64_t d0, uint64_t d1, uint64_t d2
 }
 
 // Geometry, padded nodes and tensor maps of the marching kernel.  The handle
-// keeps the tiled stage kernel when the marching kernel does not apply:
-// another flux function, an odd block width (row strides of the tensor maps
-// must be multiples of 16 bytes) or a degenerate edge.
+// keeps the tiled stage kernel when the marching kernel does not apply: an
+// odd block width (row strides of the tensor maps must be multiples of 16
+// bytes) or a degenerate edge.
 int setup_march(e2d_handle* h) {
   h->march = h->march_ok = false;
-  if (h->sc.flux != E2D_FLUX_ROE) return 0;
   const Blocks& B = h->B;
   if (B.NCi % 2 || !encode_fn()) return 0;
   const int mi = fast::march_strip_cols(), wj = fast::march_window_rows();
@@ -286,11 +285,12 @@ int setup_march(e2d_handle* h) {
 // rows per chunk -- are timed on the handle's own block set (a uniform
 // state, an explicit stage 1 per launch, one warm-up and three timed
 // launches each) when the handle is created; the fastest is kept.  Choices
-// are cached per (block shape, block count, precision) for the process.
+// are cached per (block shape, block count, precision, flux function) for
+// the process.
 struct TuneKey {
-  int nci, ncj, nblk, prec;
+  int nci, ncj, nblk, prec, flux;
   bool operator<(const TuneKey& o) const {
-    return std::tie(nci, ncj, nblk, prec) < std::tie(o.nci, o.ncj, o.nblk, o.prec);
+    return std::tie(nci, ncj, nblk, prec, flux) < std::tie(o.nci, o.ncj, o.nblk, o.prec, o.flux);
   }
 };
 struct TuneChoice {
@@ -315,7 +315,7 @@ __global__ void uniform_state_kernel(Blocks B, long long ncell) {
 
 // Tunes one precision into sel_*[prec].
 int autotune_precision(e2d_handle* h, int prec) {
-  const TuneKey key{h->B.nci, h->B.ncj, h->B.nblk, prec};
+  const TuneKey key{h->B.nci, h->B.ncj, h->B.nblk, prec, h->sc.flux};
   {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     auto it = g_tune.find(key);

@@ -43,8 +43,9 @@
 // holds the quantities the reference computes from the grid alone, in its
 // order (e2d_march_args.h), and its results equal stage_kernel's bit for bit.
 //
-// Used when the block set allows it (even nci, no degenerate edges, the Roe
-// flux); stage_kernel covers every other case.
+// Used when the block set allows it (even nci, no degenerate edges), for
+// every flux function (the Roe flux in an instance of its own);
+// stage_kernel covers the other block sets.
 #pragma once
 #include "e2d_march_args.h"
 #include "e2d_tc.cuh"
@@ -371,7 +372,7 @@ __device__ __forceinline__ FaceGeo face_geo(double ax, double ay, double cx, dou
 // flux evaluation; only the cells, the edge and the destination differ.  BC:
 // the chunk has faces on a block edge whose boundary condition sets the face
 // state (otherwise the BC codes are not read).
-template <bool BC>
+template <bool BC, bool ROE>
 __device__ __forceinline__ void face(const MarchArgs& m, Smem& s, const Tile& T, const Chunk& k, int t, int ni,
                                      int sf_lo) {
   const Blocks& B = m.a.B;
@@ -437,7 +438,7 @@ __device__ __forceinline__ void face(const MarchArgs& m, Smem& s, const Tile& T,
     wl = fstate(s, T, k, ls, lc, f.mx, f.my);
     wr = fstate(s, T, k, rs, rc, f.mx, f.my);
   }
-  const CState<RT> F = face_flux<true>(B.flux, wl, wr, RT(f.nx), RT(f.ny), g, gm1, gm1i);
+  const CState<RT> F = face_flux<ROE>(B.flux, wl, wr, RT(f.nx), RT(f.ny), g, gm1, gm1i);
 #ifdef E2D_FAST
   out[0] = double(F.d) * f.l;
   out[vs] = double(F.mx) * f.l;
@@ -659,7 +660,10 @@ __device__ __forceinline__ void update_cell(const MarchArgs& m, const Smem& s, c
 // reconstructs chunk c and updates chunk c-1 (whose face fluxes are complete),
 // then one phase that evaluates chunk c's faces; the last chunk's update runs
 // after the loop.  Two CTA barriers a chunk (and the staging wait).
-template <int MODE, bool FUSE>
+// ROE: the kernel instance of the Roe flux; the other instance dispatches
+// over the remaining flux functions (face_flux), so neither carries the
+// other's registers.
+template <int MODE, bool FUSE, bool ROE>
 __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_constant__ MarchArgs m) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // TMA destinations want 128-byte alignment: align the base by hand
@@ -816,9 +820,9 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
       const bool bc = ((sides & 1u) && k.i0 == 0) || ((sides & 2u) && k.i0 + MI >= B.nci) ||
                       ((sides & 4u) && k.c == 0) || ((sides & 8u) && k.c == m.cps - 1);
       if (bc) {
-        for (int t = tid; t < ni + nj; t += THREADS) face<true>(m, s, T, k, t, ni, sf_lo);
+        for (int t = tid; t < ni + nj; t += THREADS) face<true, ROE>(m, s, T, k, t, ni, sf_lo);
       } else {
-        for (int t = tid; t < ni + nj; t += THREADS) face<false>(m, s, T, k, t, ni, sf_lo);
+        for (int t = tid; t < ni + nj; t += THREADS) face<false, ROE>(m, s, T, k, t, ni, sf_lo);
       }
       pk = k;
       pcase = cs;
@@ -862,35 +866,39 @@ __global__ void __launch_bounds__(THREADS, MIN_CTAS) march_kernel(const __grid_c
 
 size_t march_smem_bytes() { return sizeof(mk::Smem) + 128; }
 
-template <int MODE, bool FUSE>
+template <int MODE, bool FUSE, bool ROE>
 cudaError_t march_one(const MarchArgs& m, int grid, cudaStream_t st) {
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(mk::march_kernel<MODE, FUSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(mk::march_kernel<MODE, FUSE, ROE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          int(march_smem_bytes()));
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  mk::march_kernel<MODE, FUSE><<<grid, mk::THREADS, march_smem_bytes(), st>>>(m);
+  mk::march_kernel<MODE, FUSE, ROE><<<grid, mk::THREADS, march_smem_bytes(), st>>>(m);
   return cudaGetLastError();
 }
 // grid: CTAs of the persistent launch (the caller sizes it to the SMs)
-cudaError_t launch_march(const MarchArgs& m, int grid, cudaStream_t st) {
+template <bool ROE>
+cudaError_t launch_march_flux(const MarchArgs& m, int grid, cudaStream_t st) {
   switch (m.a.mode * 2 + (m.a.fuse_next ? 1 : 0)) {
-    case 0: return march_one<0, false>(m, grid, st);
-    case 2: return march_one<1, false>(m, grid, st);
-    case 3: return march_one<1, true>(m, grid, st);
-    case 4: return march_one<2, false>(m, grid, st);
-    case 5: return march_one<2, true>(m, grid, st);
-    case 6: return march_one<3, false>(m, grid, st);
+    case 0: return march_one<0, false, ROE>(m, grid, st);
+    case 2: return march_one<1, false, ROE>(m, grid, st);
+    case 3: return march_one<1, true, ROE>(m, grid, st);
+    case 4: return march_one<2, false, ROE>(m, grid, st);
+    case 5: return march_one<2, true, ROE>(m, grid, st);
+    case 6: return march_one<3, false, ROE>(m, grid, st);
     default: return cudaErrorInvalidValue;
   }
 }
+cudaError_t launch_march(const MarchArgs& m, int grid, cudaStream_t st) {
+  return m.a.B.flux == E2D_FLUX_ROE ? launch_march_flux<true>(m, grid, st) : launch_march_flux<false>(m, grid, st);
+}
 int march_ctas_per_sm() {
   int n = 0;
-  if (cudaFuncSetAttribute(mk::march_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(mk::march_kernel<1, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            int(march_smem_bytes())) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mk::march_kernel<1, false>, mk::THREADS,
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mk::march_kernel<1, false, true>, mk::THREADS,
                                                     march_smem_bytes()) != cudaSuccess)
     return 0;
   return n;

@@ -355,8 +355,8 @@ int e2d_set_precision(e2d_handle *h, int precision);
 /* The stage kernel the handle's autotuner chose when the handle was created:
  * *kernel 0 = the tiled kernel, 1 = the column-marching kernel with *rows
  * rows per chunk; *us the tuner's time of one explicit stage with it (0 when
- * no tuning ran: a flux function other than Roe's, an odd block width,
- * a degenerate edge).  Any pointer may be NULL.  The environment variable
+ * no tuning ran: an odd block width or a degenerate edge, where the tiled
+ * kernel is the only one).  Any pointer may be NULL.  The environment variable
  * CFFC_E2D_STAGE_KERNEL=tiled or =march, read when a handle is created,
  * fixes the kernel without tuning (the marching kernel still only where it
  * applies).  No reference counterpart. */

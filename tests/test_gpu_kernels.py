@@ -1,8 +1,8 @@
 """Both stage kernels against the reference's golden vectors, whichever
 one the handle's autotuner would choose: CFFC_E2D_STAGE_KERNEL=tiled /
 march fixes the kernel when a handle is created.  The column-marching kernel
-serves the Roe flux on blocks of even width; other cases keep the tiled
-kernel whatever the setting.
+serves blocks of even width (every flux function); other block sets keep
+the tiled kernel whatever the setting.
 
 * fast FP64 precision: tolerances as tests/test_gpu_parity.py (residual per
   cell within helpers.rtol_fast and per value within 1e-12 (1 + scale /
@@ -30,7 +30,7 @@ def fast_handle(bs, kernel, monkeypatch, precision=FAST):
     h = capi.Handle(dataclasses.replace(bs, scheme=dataclasses.replace(bs.scheme, precision=precision)))
     monkeypatch.delenv("CFFC_E2D_STAGE_KERNEL")
     k, _, _ = h.stage_config()
-    marchable = bs.scheme.flux == cases.FLUX_ROE and bs.nci % 2 == 0
+    marchable = bs.nci % 2 == 0
     assert k == (KERNELS[kernel] if marchable else 0), (kernel, k)
     return h
 
