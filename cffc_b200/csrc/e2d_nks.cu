@@ -78,8 +78,19 @@ __device__ void partial_done(double s, double* partial, int slot, const Blocks& 
   if (!last || threadIdx.x >= 32) return;
   __threadfence();
   const int b0 = B.case_start ? B.case_start[c] : 0, b1 = B.case_start ? B.case_start[c + 1] : B.nblk;
+  // each lane sums partials lane, lane + 32, ... in that order; the loads of
+  // eight of them are issued together (from L2, where the other CTAs'
+  // fenced writes are), then added one after another
   double t = 0.0;
-  for (int q = b0 * ch + threadIdx.x; q < b1 * ch; q += 32) t += ((volatile double*)partial)[q];
+  const int q1 = b1 * ch;
+  for (int q = b0 * ch + threadIdx.x; q < q1; q += 32 * 8) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = q + 32 * u < q1 ? __ldcg(partial + q + 32 * u) : 0.0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (q + 32 * u < q1) t += v[u];
+  }
   for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
   if (threadIdx.x == 0) {
     out[c] = fin == FIN_SUM ? t : (fin == FIN_SQRT ? sqrt(t) : eps0 / sqrt(t));

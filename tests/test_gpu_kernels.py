@@ -104,3 +104,25 @@ def test_explicit_exact_each_kernel(name, kernel, monkeypatch):
         np.testing.assert_allclose(hist[:, 0], ref["hist"][:, 0], rtol=RTOL_POW)
     else:
         assert np.array_equal(hist[:, 0], ref["hist"][:, 0])
+
+
+@pytest.mark.parametrize("name", fixtures("residual")[:6])
+def test_switch_to_exact_on_a_live_handle(name, monkeypatch):
+    """A handle created in the fast precision and switched to the exact one
+    (e2d_set_precision) runs the exact build of its stage kernel with the
+    exact geometry: bit-identical to the reference; switched back, the fast
+    result again."""
+    bs, ref, _, lean = load(name)
+    h = fast_handle(bs, "march", monkeypatch)
+    h.set_state()
+    fast = h.residual().copy()
+    h.set_precision(EXACT)
+    h.set_state()
+    dUdt = h.residual()
+    h.set_precision(FAST)
+    h.set_state()
+    again = h.residual()
+    h.close()
+    r = ref["dUdt"] if lean else bs.interior(ref["dUdt"])
+    assert_exact(bs, bs.interior(dUdt), r)
+    assert np.array_equal(again, fast)
