@@ -117,10 +117,14 @@ def exact_leg(bs, rk_steps, device, steps=2):
     assert h.lib.e2d_kernel_times(h.h, 10, capi.ptr(kt)) == 0
     kind, rows, _ = h.stage_config()
     h.close()
+    hbm, peak_kind = peaks()
+    achieved = bs.n_interior * 0.5 * (80 + 112) / (0.5 * (kt[1] + kt[2]) * 1e-3) / 1e9
     return {"value": round(bs.n_interior * rk_steps / secs * 1e-6, 3), "unit": "Mcell-updates/s",
             "timing": "host clock around e2d_rk_steps (returns after the device finished)",
             "stage_kernel": f"march_kernel, {rows} rows per chunk" if kind == 1 else "stage_kernel (tiled)",
-            "stage_ms": [round(kt[1], 5), round(kt[2], 5)]}
+            "stage_ms": [round(kt[1], 5), round(kt[2], 5)],
+            "roofline": {"achieved": round(achieved, 2), "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4)}}
 
 
 def parity_leg(bs, device):
