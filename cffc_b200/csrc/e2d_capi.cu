@@ -687,11 +687,6 @@ static void scatter_sub(const e2d_handle* h, int s, const std::vector<double>& i
     q += size[c];
   }
 }
-static size_t total(const std::vector<size_t>& size) {
-  size_t t = 0;
-  for (size_t v : size) t += v;
-  return t;
-}
 static size_t sub_total(const e2d_handle* h, int s, const std::vector<size_t>& size) {
   size_t t = 0;
   for (int c : sub_cases(h, s)) t += size[c];
