@@ -77,7 +77,7 @@ constexpr int NBUF = E2D_MARCH_NBUF;  // staging buffers: 2 = the next chunk's c
 #define E2D_MARCH_UPD 0
 #endif
 // E2D_MARCH_UPD 1: the explicit stages' update inputs of a chunk (base state,
-// stage-1 residual, 1/A and the CFL geometry) arrive in shared memory by TMA
+// stage-1 residual, the area plane and the CFL geometry) arrive in shared memory by TMA
 // while the chunk's faces are evaluated, instead of as global loads in the
 // update (whose latency every warp meets at once after the phase barrier)
 constexpr bool UPD = E2D_MARCH_UPD;
@@ -110,7 +110,8 @@ static_assert(RR >= RCJ && RR >= MJ + 1, "ring holds the live rows");
 
 // Update inputs of a chunk's cells (rows j0+2 .., columns i0+2 ..): the base
 // conserved state, the residual RK stage 2 adds to, and geometry planes
-// G_RA .. G_VJY (1/A alone without the fused CFL step).
+// G_RA .. G_VJY (plane G_RA, 1/A or in the exact build A, alone without the
+// fused CFL step).
 struct UpdIn {
   double U[4][MJ][MI];
   double R[4][MJ][MI];
