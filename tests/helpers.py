@@ -13,7 +13,7 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 # Tolerance of the fast FP64 path (FMA contraction) against the reference:
 # per cell, |x - ref| <= RTOL * (|ref| + scale), scale = max |ref| of that
 # variable over the block set (so cells where the residual nearly cancels are
-# judged against the field's magnitude, not their own).
+# measured against the field's magnitude, not their own).
 RTOL_FP64 = 1e-12
 # The other flux functions have more cancellation in their dissipation terms
 # (differences of products, then scaled): FMA contraction moves their
@@ -79,7 +79,7 @@ def rel_err(x, ref, axis_var=1):
 
     scale_v = max(max |ref| of variable v, 1e-3 * max |ref| of all variables):
     a variable whose residual is pure round-off everywhere (e.g. the
-    y-momentum residual of a uniform-pressure, v = 0 state, ~1e-14) is judged
+    y-momentum residual of a uniform-pressure, v = 0 state, ~1e-14) is measured
     against the residual magnitude of the other variables, not itself."""
     x = np.asarray(x)
     ref = np.asarray(ref)
