@@ -27,7 +27,7 @@ constexpr int kThreads = 256;
 // The shared scratch: every call writes the slots [0, 3*nblk) before reading
 // them, so no slot needs clearing between calls.  Calls that overlap on the
 // GPU (two streams, or two host threads) use the same slots and race.
-__device__ __align__(256) double g_norm_scratch[3 * E2D_NORMS_STATIC_MAX_BLOCKS];
+static __device__ __align__(256) double g_norm_scratch[3 * E2D_NORMS_STATIC_MAX_BLOCKS];
 
 // Device address of g_norm_scratch per device (the symbol's name in host code
 // is a host-side stand-in, not a device address).
